@@ -1,0 +1,1485 @@
+/*
+ * hit3d_oracle.c -- TEST INFRASTRUCTURE ONLY.
+ *
+ * An FP64 CPU restatement of HIT3DP's pseudospectral timestep, written from the
+ * reference Fortran sources, used as the parity checker for the CUDA path.  It is
+ * loaded only by tests/, by __graft_entry__.smoke() and by bench.py's CPU-baseline
+ * leg; the product library never links or calls it.
+ *
+ * Parity status: UNPINNED against the reference's own build.  The reference is
+ * Fortran + MPI + FFTW3 and none of those toolchains exist on these machines, and
+ * the reference ships no golden vectors.  This restatement is pinned only by
+ *   - the analytic checks of the reference's (dead) test_rhs_velocity and
+ *     test_rhs_scalars routines (rhs_velocity.f90:430-553, rhs_scalars.f90:504-594),
+ *   - numpy.fft (pocketfft) for the transform conventions,
+ *   - exact integer arithmetic for RANDu.
+ *
+ * Layout follows the reference exactly: every field is a column-major
+ * (nx+2, ny, nz) real*8 array.  Physical space is (x, y, z); Fourier space is
+ * (kx re/im interleaved, kz, ky) (x_fftw.f90:321-327).  The forward transform is
+ * unnormalised, the inverse multiplies by 1/N^3 (x_fftw.f90:262,1070).
+ *
+ * Compile with -ffp-contract=off so that a*b+c is never fused, like gfortran -O2
+ * on x86-64 without -march flags.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define MAXS 8
+
+/* ------------------------------------------------------------------------- */
+/*  RANDu: L'Ecuyer with Bays-Durham shuffle (RANDu.f:12-52).                */
+/*  Quirk kept: idum = nint(idum3/987) is recomputed from the caller's seed   */
+/*  on every call (RANDu.f:27), so only idum2, iy and iv evolve.             */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    int64_t idum2, iy, iv[32];
+} randu_state;
+
+static int64_t nint_d(double x) { return (int64_t)llround(x); }
+
+void oracle_randu_reset(randu_state *s)
+{
+    s->idum2 = 123456789;
+    s->iy = 0;
+    for (int j = 0; j < 32; j++) s->iv[j] = 0;
+}
+
+double oracle_randu(randu_state *s, double idum3)
+{
+    const int64_t im1 = 2147483563, im2 = 2147483399, imm1 = im1 - 1;
+    const int64_t ia1 = 40014, ia2 = 40692, iq1 = 53668, iq2 = 52774;
+    const int64_t ir1 = 12211, ir2 = 3791, ntab = 32, ndiv = 1 + imm1 / ntab;
+    const double am = 1.0 / (double)im1, eps = 1.2e-7, rnmx = 1.0 - eps;
+    int64_t idum = nint_d(idum3 / 987.0);
+    int64_t k, j;
+    if (idum <= 0) {
+        idum = (-idum > 1) ? -idum : 1;
+        s->idum2 = idum;
+        for (j = ntab + 8; j >= 1; j--) {
+            k = idum / iq1;
+            idum = ia1 * (idum - k * iq1) - k * ir1;
+            if (idum < 0) idum += im1;
+            if (j <= ntab) s->iv[j - 1] = idum;
+        }
+    }
+    k = idum / iq1;
+    idum = ia1 * (idum - k * iq1) - k * ir1;
+    if (idum < 0) idum += im1;
+    k = s->idum2 / iq2;
+    s->idum2 = ia2 * (s->idum2 - k * iq2) - k * ir2;
+    if (s->idum2 < 0) s->idum2 += im2;
+    j = 1 + s->iy / ndiv;
+    s->iy = s->iv[j - 1] - s->idum2;
+    s->iv[j - 1] = idum;
+    if (s->iy < 1) s->iy += imm1;
+    double r = am * (double)s->iy;
+    return r < rnmx ? r : rnmx;
+}
+
+/* Fill out[0..count) with the stream that begins with random(-seed) and
+ * continues with random(seed), discarding the first value (init_velocity.f90:70-71). */
+void oracle_randu_stream(double seed, int64_t count, double *out)
+{
+    randu_state s;
+    oracle_randu_reset(&s);
+    (void)oracle_randu(&s, -seed);
+    for (int64_t i = 0; i < count; i++) out[i] = oracle_randu(&s, seed);
+}
+
+/* ------------------------------------------------------------------------- */
+/*  1-D complex FFT, mixed radix 2/3/4/5, Stockham autosort.                  */
+/*  Stands in for FFTW3's DFFTW_EXECUTE (x_fftw.f90:211-256).  Twiddles are  */
+/*  computed in long double and rounded once.                                 */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    int n, nf, fac[40];
+    double *tw; /* tw[2t], tw[2t+1] = cos(2 pi t/n), -sin(2 pi t/n) */
+} fftplan;
+
+static void plan_init(fftplan *p, int n)
+{
+    p->n = n;
+    p->nf = 0;
+    int m = n;
+    while (m % 4 == 0) { p->fac[p->nf++] = 4; m /= 4; }
+    while (m % 2 == 0) { p->fac[p->nf++] = 2; m /= 2; }
+    while (m % 3 == 0) { p->fac[p->nf++] = 3; m /= 3; }
+    while (m % 5 == 0) { p->fac[p->nf++] = 5; m /= 5; }
+    if (m != 1) { fprintf(stderr, "oracle: unsupported FFT length %d\n", n); abort(); }
+    p->tw = (double *)malloc(sizeof(double) * 2 * (size_t)n);
+    const long double twopi = 6.283185307179586476925286766559005768L;
+    for (int t = 0; t < n; t++) {
+        long double a = twopi * (long double)t / (long double)n;
+        p->tw[2 * t] = (double)cosl(a);
+        p->tw[2 * t + 1] = (double)(-sinl(a));
+    }
+}
+
+static void plan_free(fftplan *p) { free(p->tw); p->tw = NULL; }
+
+/* x: interleaved complex of length n; y: scratch of the same size.
+ * sign = -1 forward (e^{-i...}), +1 backward, both unnormalised. */
+static void fft1d(const fftplan *p, double *x, double *y, int sign)
+{
+    const int n = p->n;
+    double *src = x, *dst = y;
+    int Ns = 1;
+    for (int s = 0; s < p->nf; s++) {
+        const int R = p->fac[s], m = n / R, step = n / (Ns * R);
+        for (int j = 0; j < m; j++) {
+            const int k = j % Ns;
+            double ar[5], ai[5];
+            for (int r = 0; r < R; r++) {
+                double xr = src[2 * (j + r * m)], xi = src[2 * (j + r * m) + 1];
+                int t = (r * k * step) % n;
+                double wr = p->tw[2 * t], wi = p->tw[2 * t + 1];
+                if (sign > 0) wi = -wi;
+                ar[r] = xr * wr - xi * wi;
+                ai[r] = xr * wi + xi * wr;
+            }
+            double br[5], bi[5];
+            if (R == 2) {
+                br[0] = ar[0] + ar[1]; bi[0] = ai[0] + ai[1];
+                br[1] = ar[0] - ar[1]; bi[1] = ai[0] - ai[1];
+            } else if (R == 4) {
+                double s0r = ar[0] + ar[2], s0i = ai[0] + ai[2];
+                double d0r = ar[0] - ar[2], d0i = ai[0] - ai[2];
+                double s1r = ar[1] + ar[3], s1i = ai[1] + ai[3];
+                double d1r = ar[1] - ar[3], d1i = ai[1] - ai[3];
+                /* multiply d1 by -i*sign... forward: -i, backward: +i */
+                double er, ei;
+                if (sign < 0) { er = d1i; ei = -d1r; } else { er = -d1i; ei = d1r; }
+                br[0] = s0r + s1r; bi[0] = s0i + s1i;
+                br[2] = s0r - s1r; bi[2] = s0i - s1i;
+                br[1] = d0r + er;  bi[1] = d0i + ei;
+                br[3] = d0r - er;  bi[3] = d0i - ei;
+            } else {
+                /* direct DFT for radix 3 and 5 */
+                for (int q = 0; q < R; q++) {
+                    double sr = 0.0, si = 0.0;
+                    for (int r = 0; r < R; r++) {
+                        int t = ((q * r) % R) * (n / R);
+                        double wr = p->tw[2 * t], wi = p->tw[2 * t + 1];
+                        if (sign > 0) wi = -wi;
+                        sr += ar[r] * wr - ai[r] * wi;
+                        si += ar[r] * wi + ai[r] * wr;
+                    }
+                    br[q] = sr; bi[q] = si;
+                }
+            }
+            const int base = (j / Ns) * Ns * R + k;
+            for (int q = 0; q < R; q++) {
+                dst[2 * (base + q * Ns)] = br[q];
+                dst[2 * (base + q * Ns) + 1] = bi[q];
+            }
+        }
+        double *t = src; src = dst; dst = t;
+        Ns *= R;
+    }
+    if (src != x) memcpy(x, src, sizeof(double) * 2 * (size_t)n);
+}
+
+/* exported for the transform conventions test */
+void oracle_fft1d(int n, double *x, int sign)
+{
+    fftplan p;
+    plan_init(&p, n);
+    double *y = (double *)malloc(sizeof(double) * 2 * (size_t)n);
+    fft1d(&p, x, y, sign);
+    free(y);
+    plan_free(&p);
+}
+
+/* ------------------------------------------------------------------------- */
+/*  Oracle state: module globals of m_fields / m_work / x_fftw / m_force.    */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    int n, nscal, dealias, flow_type, force_type, kfmax, kmax, les_model, nwrk;
+    int isp_type;
+    double nu, dt, famp, dx, c_smag, les_delta, peak_wavenum, ir_exp;
+    double pe[MAXS];
+    int scalar_type[MAXS];
+    size_t fsz;               /* (n+2)*n*n */
+    double *fields, *rhs_old, *wrk, *turb_visc;
+    double *akx, *aky, *akz;
+    signed char *ialias;
+    int nfn, *fn_i, *fn_j, *fn_k;  /* forced nodes */
+    fftplan plan;
+    double courant, time;
+    int fov, fos, int_scalars;
+    double *scratch;          /* per-thread FFT scratch: nthreads * 4n doubles */
+    int nthreads;
+} oracle_t;
+
+#define IX(o, i, j, k) ((size_t)(i) + (size_t)((o)->n + 2) * ((size_t)(j) + (size_t)(o)->n * (size_t)(k)))
+#define F(o, m) ((o)->fields + (size_t)(m) * (o)->fsz)
+#define W(o, m) ((o)->wrk + (size_t)(m) * (o)->fsz)
+#define RO(o, m) ((o)->rhs_old + (size_t)(m) * (o)->fsz)
+
+static int nint_shell32(double k2)
+{
+    /* nint(sqrt(real(k2,4))) -- float32 sqrt (m_stats.f90:218, m_force.f90:270) */
+    float f = (float)k2;
+    float s = sqrtf(f);
+    return (int)lroundf(s);
+}
+
+static int nint_shell64(double k2)
+{
+    /* nint(sqrt(k2)) in FP64 (init_velocity.f90:127) */
+    return (int)llround(sqrt(k2));
+}
+
+static int tid(void)
+{
+#ifdef _OPENMP
+    return omp_get_thread_num();
+#else
+    return 0;
+#endif
+}
+
+/* x_fftw_init tables (x_fftw.f90:261-310) */
+static void tables_init(oracle_t *o)
+{
+    int n = o->n;
+    o->akx = (double *)calloc(n + 2, sizeof(double));
+    o->aky = (double *)calloc(n, sizeof(double));
+    o->akz = (double *)calloc(n, sizeof(double));
+    for (int i = 0; i < n + 2; i += 2) { o->akx[i] = (double)(i / 2); o->akx[i + 1] = o->akx[i]; }
+    for (int k = 0; k < n; k++) { double a = (double)k; if (a > 0.5 * n) a -= n; o->aky[k] = a; }
+    for (int j = 0; j < n; j++) { double a = (double)j; if (a > 0.5 * n) a -= n; o->akz[j] = a; }
+    o->ialias = (signed char *)calloc(o->fsz, 1);
+    double rnx3 = (double)(n / 3);
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 2; i++) {
+                int c = 0;
+                if (fabs(o->aky[k]) > rnx3) c++;
+                if (fabs(o->akz[j]) > rnx3) c++;
+                if (fabs(o->akx[i]) > rnx3) c++;
+                o->ialias[IX(o, i, j, k)] = (signed char)c;
+            }
+}
+
+/* ------------------------------------------------------------------------- */
+/*  3-D transforms on one (nx+2,ny,nz) array (x_fftw.f90:852-1085)           */
+/* ------------------------------------------------------------------------- */
+static void swap_yz(oracle_t *o, double *a)
+{
+    int n = o->n;
+#pragma omp parallel for schedule(dynamic)
+    for (int k = 0; k < n; k++)
+        for (int j = k + 1; j < n; j++)
+            for (int i = 0; i < n + 2; i++) {
+                double t = a[IX(o, i, j, k)];
+                a[IX(o, i, j, k)] = a[IX(o, i, k, j)];
+                a[IX(o, i, k, j)] = t;
+            }
+}
+
+/* complex FFT along dim 2 (index j) for every kx and every k */
+static void c2c_dim2(oracle_t *o, double *a, int sign)
+{
+    int n = o->n, nh = n / 2 + 1;
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n; k++) {
+        double *buf = o->scratch + (size_t)tid() * 4 * n;
+        double *y = buf + 2 * n;
+        for (int ix = 0; ix < nh; ix++) {
+            for (int j = 0; j < n; j++) {
+                buf[2 * j] = a[IX(o, 2 * ix, j, k)];
+                buf[2 * j + 1] = a[IX(o, 2 * ix + 1, j, k)];
+            }
+            fft1d(&o->plan, buf, y, sign);
+            for (int j = 0; j < n; j++) {
+                a[IX(o, 2 * ix, j, k)] = buf[2 * j];
+                a[IX(o, 2 * ix + 1, j, k)] = buf[2 * j + 1];
+            }
+        }
+    }
+}
+
+/* r2c along x for every (j,k): two real rows per complex transform */
+static void r2c_x(oracle_t *o, double *a)
+{
+    int n = o->n;
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n; k++) {
+        double *z = o->scratch + (size_t)tid() * 4 * n;
+        double *y = z + 2 * n;
+        for (int j = 0; j < n; j += 2) {
+            double *ra = a + IX(o, 0, j, k), *rb = a + IX(o, 0, j + 1, k);
+            for (int t = 0; t < n; t++) { z[2 * t] = ra[t]; z[2 * t + 1] = rb[t]; }
+            fft1d(&o->plan, z, y, -1);
+            for (int kx = 0; kx <= n / 2; kx++) {
+                int m = (n - kx) % n;
+                double zr = z[2 * kx], zi = z[2 * kx + 1];
+                double mr = z[2 * m], mi = -z[2 * m + 1];
+                ra[2 * kx] = 0.5 * (zr + mr);
+                ra[2 * kx + 1] = 0.5 * (zi + mi);
+                rb[2 * kx] = 0.5 * (zi - mi);
+                rb[2 * kx + 1] = -0.5 * (zr - mr);
+            }
+        }
+    }
+}
+
+/* c2r along x for every (j,k), times norm; imaginary parts of kx=0 and kx=N/2
+ * are ignored, as in FFTW's c2r. */
+static void c2r_x(oracle_t *o, double *a, double norm)
+{
+    int n = o->n;
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n; k++) {
+        double *z = o->scratch + (size_t)tid() * 4 * n;
+        double *y = z + 2 * n;
+        for (int j = 0; j < n; j += 2) {
+            double *ra = a + IX(o, 0, j, k), *rb = a + IX(o, 0, j + 1, k);
+            for (int kx = 0; kx <= n / 2; kx++) {
+                double xar = ra[2 * kx], xai = ra[2 * kx + 1];
+                double xbr = rb[2 * kx], xbi = rb[2 * kx + 1];
+                if (kx == 0 || kx == n / 2) { xai = 0.0; xbi = 0.0; }
+                z[2 * kx] = xar - xbi;
+                z[2 * kx + 1] = xai + xbr;
+                if (kx > 0 && kx < n / 2) {
+                    z[2 * (n - kx)] = xar + xbi;
+                    z[2 * (n - kx) + 1] = -xai + xbr;
+                }
+            }
+            fft1d(&o->plan, z, y, +1);
+            for (int t = 0; t < n; t++) { ra[t] = norm * z[2 * t]; rb[t] = norm * z[2 * t + 1]; }
+        }
+    }
+}
+
+static void xfft3d(oracle_t *o, int flag, double *a)
+{
+    int n = o->n;
+    if (flag == 1) {
+        r2c_x(o, a);
+        /* c2c along y within each z-plane: layout (kx, ky, z) */
+        c2c_dim2(o, a, -1);
+        swap_yz(o, a);
+        c2c_dim2(o, a, -1);
+    } else {
+        c2c_dim2(o, a, +1);
+        swap_yz(o, a);
+        c2c_dim2(o, a, +1);
+        c2r_x(o, a, 1.0 / ((double)n * (double)n * (double)n));
+    }
+}
+
+void oracle_fft3d(oracle_t *o, int flag, double *a) { xfft3d(o, flag, a); }
+
+/* ------------------------------------------------------------------------- */
+/*  create / destroy                                                          */
+/* ------------------------------------------------------------------------- */
+oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_type, int kfmax,
+                        double nu, double dt, double famp, int les_model, double c_smag,
+                        const double *sc, const int *scalar_type)
+{
+    if (nscal > MAXS) return NULL;
+    oracle_t *o = (oracle_t *)calloc(1, sizeof(oracle_t));
+    o->n = n; o->nscal = nscal; o->dealias = dealias; o->flow_type = flow_type;
+    o->force_type = force_type; o->kfmax = kfmax; o->nu = nu; o->dt = dt; o->famp = famp;
+    o->les_model = les_model; o->c_smag = c_smag;
+    o->dx = 2.0 * (4.0 * atan(1.0)) / (double)n;
+    o->les_delta = o->dx;
+    /* kmax (m_parameters.f90:123-131) */
+    if (dealias == 0) o->kmax = n / 3;
+    else o->kmax = (int)floor((double)n / 3.0 * sqrt(2.0));
+    for (int s = 0; s < nscal; s++) { o->pe[s] = nu / sc[s]; o->scalar_type[s] = scalar_type[s]; }
+    o->fsz = (size_t)(n + 2) * n * n;
+    o->nwrk = 7;
+    if (5 + nscal + 1 > o->nwrk) o->nwrk = 5 + nscal + 1;
+    o->fields = (double *)calloc(o->fsz * (3 + nscal), sizeof(double));
+    o->rhs_old = (double *)calloc(o->fsz * (3 + nscal), sizeof(double));
+    o->wrk = (double *)calloc(o->fsz * o->nwrk, sizeof(double));
+    if (les_model) o->turb_visc = (double *)calloc(o->fsz, sizeof(double));
+    if (!o->fields || !o->rhs_old || !o->wrk) return NULL;
+    tables_init(o);
+    plan_init(&o->plan, n);
+#ifdef _OPENMP
+    o->nthreads = omp_get_max_threads();
+#else
+    o->nthreads = 1;
+#endif
+    o->scratch = (double *)malloc(sizeof(double) * 4 * (size_t)n * o->nthreads);
+    /* forced node list (m_force.f90:13-97), loop order k, j, i over i<nx */
+    if (flow_type == 1) {
+        int cnt = 0;
+        for (int pass = 0; pass < 2; pass++) {
+            int m = 0;
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) {
+                        double k2 = o->akx[i] * o->akx[i] + o->aky[k] * o->aky[k] + o->akz[j] * o->akz[j];
+                        int sh = nint_shell32(k2);
+                        if (sh > 0 && sh <= kfmax) {
+                            if (pass == 1) { o->fn_i[m] = i; o->fn_j[m] = j; o->fn_k[m] = k; }
+                            m++;
+                        }
+                    }
+            if (pass == 0) {
+                cnt = m;
+                o->fn_i = (int *)malloc(sizeof(int) * (cnt + 1));
+                o->fn_j = (int *)malloc(sizeof(int) * (cnt + 1));
+                o->fn_k = (int *)malloc(sizeof(int) * (cnt + 1));
+            }
+        }
+        o->nfn = cnt;
+    }
+    o->fov = 1; o->fos = 1; o->int_scalars = nscal > 0;
+    return o;
+}
+
+void oracle_destroy(oracle_t *o)
+{
+    if (!o) return;
+    free(o->fields); free(o->rhs_old); free(o->wrk); free(o->turb_visc);
+    free(o->akx); free(o->aky); free(o->akz); free(o->ialias);
+    free(o->fn_i); free(o->fn_j); free(o->fn_k); free(o->scratch);
+    plan_free(&o->plan);
+    free(o);
+}
+
+double *oracle_fields(oracle_t *o) { return o->fields; }
+double *oracle_rhs_old(oracle_t *o) { return o->rhs_old; }
+double *oracle_wrk(oracle_t *o) { return o->wrk; }
+int oracle_kmax(oracle_t *o) { return o->kmax; }
+int oracle_nforced(oracle_t *o) { return o->nfn; }
+double oracle_courant(oracle_t *o) { return o->courant; }
+void oracle_set_dt(oracle_t *o, double dt) { o->dt = dt; }
+void oracle_set_flags(oracle_t *o, int fov, int fos, int int_scalars)
+{
+    o->fov = fov; o->fos = fos; o->int_scalars = int_scalars;
+}
+void oracle_get_flags(oracle_t *o, int *flags) { flags[0] = o->fov; flags[1] = o->fos; flags[2] = o->int_scalars; }
+
+/* ------------------------------------------------------------------------- */
+/*  dealias_all (dealias_all.f90:97-131)                                     */
+/* ------------------------------------------------------------------------- */
+void oracle_dealias_all(oracle_t *o)
+{
+    int n = o->n;
+    double akmax = (double)o->kmax;
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 2; i++)
+                if (fabs(o->akx[i]) > akmax || fabs(o->aky[k]) > akmax || fabs(o->akz[j]) > akmax)
+                    for (int m = 0; m < 3 + o->nscal; m++) F(o, m)[IX(o, i, j, k)] = 0.0;
+}
+
+/* ------------------------------------------------------------------------- */
+/*  Smagorinsky turbulent viscosity (m_les.f90:1142-1215)                    */
+/* ------------------------------------------------------------------------- */
+static void strain_first(oracle_t *o, int second)
+{
+    int n = o->n;
+    double *u = F(o, 0), *v = F(o, 1), *w = F(o, 2);
+    double *w4 = W(o, 4), *w5 = W(o, 5), *w6 = W(o, 6);
+    const double half = 0.5;
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 1; i += 2) {
+                size_t a = IX(o, i, j, k), b = a + 1;
+                double kx0 = o->akx[i], kx1 = o->akx[i + 1], ky = o->aky[k], kz = o->akz[j];
+                if (!second) {
+                    w4[a] = -kx1 * u[b];
+                    w4[b] = kx0 * u[a];
+                    w5[a] = -half * (ky * u[b] + kx1 * v[b]);
+                    w5[b] = half * (ky * u[a] + kx0 * v[a]);
+                    w6[a] = -half * (kz * u[b] + kx1 * w[b]);
+                    w6[b] = half * (kz * u[a] + kx0 * w[a]);
+                } else {
+                    w4[a] = -ky * v[b];
+                    w4[b] = ky * v[a];
+                    w5[a] = -half * (kz * v[b] + ky * w[b]);
+                    w5[b] = half * (kz * v[a] + ky * w[a]);
+                    w6[a] = -kz * w[b];
+                    w6[b] = kz * w[a];
+                }
+            }
+}
+
+static void les_get_turb_visc_smag(oracle_t *o)
+{
+    int n = o->n;
+    double *tv = o->turb_visc;
+    strain_first(o, 0);
+    for (int m = 4; m <= 6; m++) xfft3d(o, -1, W(o, m));
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                size_t a = IX(o, i, j, k);
+                double s4 = W(o, 4)[a], s5 = W(o, 5)[a], s6 = W(o, 6)[a];
+                double t = s4 * s4;
+                t = t + 2.0 * (s5 * s5);
+                t = t + 2.0 * (s6 * s6);
+                tv[a] = t;
+            }
+    strain_first(o, 1);
+    for (int m = 4; m <= 6; m++) xfft3d(o, -1, W(o, m));
+    double cd = o->c_smag * o->les_delta;
+    cd = cd * cd;
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                size_t a = IX(o, i, j, k);
+                double s4 = W(o, 4)[a], s5 = W(o, 5)[a], s6 = W(o, 6)[a];
+                double t = tv[a] + s4 * s4;
+                t = t + 2.0 * (s5 * s5);
+                t = t + s6 * s6;
+                t = sqrt(2.0 * t);
+                tv[a] = t * cd;
+            }
+}
+
+/* les_rhsv_turb_visc (m_les.f90:902-1018) followed by the ialias mask of
+ * les_rhs_velocity (m_les.f90:682-690) */
+static void les_rhs_velocity(oracle_t *o)
+{
+    int n = o->n;
+    double *tv = o->turb_visc;
+    for (int pass = 0; pass < 2; pass++) {
+        strain_first(o, pass);
+        for (int m = 4; m <= 6; m++) {
+            double *a = W(o, m);
+            xfft3d(o, -1, a);
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) {
+                        size_t q = IX(o, i, j, k);
+                        a[q] = -2.0 * tv[q] * a[q];
+                    }
+            xfft3d(o, 1, a);
+        }
+        double *r1 = W(o, 1), *r2 = W(o, 2), *r3 = W(o, 3);
+        double *w4 = W(o, 4), *w5 = W(o, 5), *w6 = W(o, 6);
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n + 1; i += 2) {
+                    size_t a = IX(o, i, j, k), b = a + 1;
+                    if (o->ialias[a] != 0) continue;
+                    double kx0 = o->akx[i], kx1 = o->akx[i + 1], ky = o->aky[k], kz = o->akz[j];
+                    if (pass == 0) {
+                        r1[a] = r1[a] + kx1 * w4[b] + ky * w5[b] + kz * w6[b];
+                        r1[b] = r1[b] - kx0 * w4[a] - ky * w5[a] - kz * w6[a];
+                        r2[a] = r2[a] + kx1 * w5[b];
+                        r2[b] = r2[b] - kx0 * w5[a];
+                        r3[a] = r3[a] + kx1 * w6[b];
+                        r3[b] = r3[b] - kx0 * w6[a];
+                    } else {
+                        r2[a] = r2[a] + ky * w4[b] + kz * w5[b];
+                        r2[b] = r2[b] - ky * w4[a] - kz * w5[a];
+                        r3[a] = r3[a] + ky * w5[b] + kz * w6[b];
+                        r3[b] = r3[b] - ky * w5[a] - kz * w6[a];
+                    }
+                }
+    }
+    for (size_t q = 0; q < o->fsz; q++)
+        if (o->ialias[q] != 0) { W(o, 1)[q] = 0.0; W(o, 2)[q] = 0.0; W(o, 3)[q] = 0.0; }
+}
+
+/* ------------------------------------------------------------------------- */
+/*  rhs_scalars (rhs_scalars.f90:1-402)                                      */
+/* ------------------------------------------------------------------------- */
+static void phase_factors(oracle_t *o)
+{
+    int n = o->n;
+    double *w0 = W(o, 0);
+    const double half = 0.5;
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 1; i += 2) {
+                size_t a = IX(o, i, j, k);
+                w0[a] = cos(half * (o->akx[i] + o->aky[k] + o->akz[j]) * o->dx);
+                w0[a + 1] = sin(half * (o->akx[i + 1] + o->aky[k] + o->akz[j]) * o->dx);
+            }
+}
+
+static void copy_field(oracle_t *o, double *dst, const double *src) { memcpy(dst, src, sizeof(double) * o->fsz); }
+
+static void mul3(oracle_t *o, double *dst, const double *a, const double *b)
+{
+#pragma omp parallel for schedule(static)
+    for (size_t q = 0; q < o->fsz; q++) dst[q] = a[q] * b[q];
+}
+
+static void oracle_rhs_scalars(oracle_t *o)
+{
+    int n = o->n, ns = o->nscal;
+    if (o->les_model) les_get_turb_visc_smag(o);
+    if (!o->int_scalars) {
+        for (int m = 0; m < 3; m++) { copy_field(o, W(o, 1 + m), F(o, m)); xfft3d(o, -1, W(o, 1 + m)); }
+        return;
+    }
+    for (int m = 4; m <= 3 + ns; m++) memset(W(o, m), 0, sizeof(double) * o->fsz);
+    if (o->dealias == 0) {
+        for (int m = 0; m < 3; m++) { copy_field(o, W(o, 1 + m), F(o, m)); xfft3d(o, -1, W(o, 1 + m)); }
+        for (int s = 1; s <= ns; s++) {
+            copy_field(o, W(o, 0), F(o, 2 + s));
+            xfft3d(o, -1, W(o, 0));
+            for (int c = 1; c <= 3; c++) {
+                mul3(o, W(o, s + 2 + c), W(o, 0), W(o, c));
+                xfft3d(o, 1, W(o, s + 2 + c));
+            }
+            double *r = W(o, 3 + s), *p2 = W(o, 4 + s), *p3 = W(o, 5 + s), *phi = F(o, 2 + s);
+            double pe = o->pe[s - 1];
+#pragma omp parallel for schedule(static)
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n + 1; i += 2) {
+                        size_t a = IX(o, i, j, k), b = a + 1;
+                        if (o->ialias[a] > 0) { r[a] = 0.0; r[b] = 0.0; continue; }
+                        double rt1 = o->akx[i + 1] * r[b] + o->aky[k] * p2[b] + o->akz[j] * p3[b];
+                        double rt2 = o->akx[i] * r[a] + o->aky[k] * p2[a] + o->akz[j] * p3[a];
+                        double wn2 = o->akx[i] * o->akx[i] + o->aky[k] * o->aky[k] + o->akz[j] * o->akz[j];
+                        r[a] = rt1 - pe * wn2 * phi[a];
+                        r[b] = -rt2 - pe * wn2 * phi[b];
+                    }
+        }
+    } else {
+        phase_factors(o);
+        double *w0 = W(o, 0);
+        for (int m = 1; m <= 3 + ns; m++) {
+            double *d = W(o, m), *f = F(o, m - 1);
+#pragma omp parallel for schedule(static)
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n + 1; i += 2) {
+                        size_t a = IX(o, i, j, k), b = a + 1;
+                        d[a] = f[a] * w0[a] - f[b] * w0[b];
+                        d[b] = f[b] * w0[a] + f[a] * w0[b];
+                    }
+            xfft3d(o, -1, d);
+        }
+        int n1 = ns + 4, n2 = ns + 5;
+        for (int m = 4; m <= 3 + ns; m++) {
+            mul3(o, W(o, n1), W(o, m), W(o, 1));
+            mul3(o, W(o, n2), W(o, m), W(o, 2));
+            mul3(o, W(o, m), W(o, m), W(o, 3));
+            xfft3d(o, 1, W(o, n1));
+            xfft3d(o, 1, W(o, n2));
+            xfft3d(o, 1, W(o, m));
+            double *A = W(o, n1), *B = W(o, n2), *C = W(o, m);
+#pragma omp parallel for schedule(static)
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n + 1; i += 2) {
+                        size_t a = IX(o, i, j, k), b = a + 1;
+                        if (o->ialias[a] > 1) { C[a] = 0.0; C[b] = 0.0; continue; }
+                        double r11 = A[a] * w0[a] + A[b] * w0[b];
+                        double r12 = A[b] * w0[a] - A[a] * w0[b];
+                        double r21 = B[a] * w0[a] + B[b] * w0[b];
+                        double r22 = B[b] * w0[a] - B[a] * w0[b];
+                        double r31 = C[a] * w0[a] + C[b] * w0[b];
+                        double r32 = C[b] * w0[a] - C[a] * w0[b];
+                        C[a] = +0.5 * (o->akx[i + 1] * r12 + o->aky[k] * r22 + o->akz[j] * r32);
+                        C[b] = -0.5 * (o->akx[i] * r11 + o->aky[k] * r21 + o->akz[j] * r31);
+                    }
+        }
+        for (int m = 0; m < 3; m++) { copy_field(o, W(o, 1 + m), F(o, m)); xfft3d(o, -1, W(o, 1 + m)); }
+        for (int m = 4; m <= 3 + ns; m++) {
+            copy_field(o, W(o, 0), F(o, m - 1));
+            xfft3d(o, -1, W(o, 0));
+            mul3(o, W(o, n1), W(o, 0), W(o, 1));
+            mul3(o, W(o, n2), W(o, 0), W(o, 2));
+            mul3(o, W(o, 0), W(o, 0), W(o, 3));
+            xfft3d(o, 1, W(o, n1));
+            xfft3d(o, 1, W(o, n2));
+            xfft3d(o, 1, W(o, 0));
+            double *A = W(o, n1), *B = W(o, n2), *C = W(o, 0), *r = W(o, m), *phi = F(o, m - 1);
+            double pe = o->pe[m - 4];
+#pragma omp parallel for schedule(static)
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n + 1; i += 2) {
+                        size_t a = IX(o, i, j, k), b = a + 1;
+                        if (o->ialias[a] < 2) {
+                            double rt1 = o->akx[i + 1] * A[b] + o->aky[k] * B[b] + o->akz[j] * C[b];
+                            double rt2 = o->akx[i] * A[a] + o->aky[k] * B[a] + o->akz[j] * C[a];
+                            double wn2 = o->akx[i] * o->akx[i] + o->aky[k] * o->aky[k] + o->akz[j] * o->akz[j];
+                            r[a] = r[a] + 0.5 * rt1 - pe * wn2 * phi[a];
+                            r[b] = r[b] - 0.5 * rt2 - pe * wn2 * phi[b];
+                        }
+                    }
+        }
+    }
+    /* uniform mean-gradient source for type-0 scalars (rhs_scalars.f90:387-389) */
+    for (int s = 1; s <= ns; s++)
+        if (o->scalar_type[s - 1] == 0) {
+            double *r = W(o, s + 3), *u = F(o, 0);
+            for (size_t q = 0; q < o->fsz; q++) r[q] = r[q] - u[q];
+        }
+}
+
+/* ------------------------------------------------------------------------- */
+/*  rhs_velocity (rhs_velocity.f90:1-419)                                    */
+/* ------------------------------------------------------------------------- */
+static void shift_back(oracle_t *o, double *a)
+{
+    int n = o->n;
+    double *w0 = W(o, 0);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 1; i += 2) {
+                size_t p = IX(o, i, j, k), q = p + 1;
+                double rt = a[p] * w0[p] + a[q] * w0[q];
+                a[q] = a[q] * w0[p] - a[p] * w0[q];
+                a[p] = rt;
+            }
+}
+
+static void shift_fwd(oracle_t *o, double *d, const double *f)
+{
+    int n = o->n;
+    double *w0 = W(o, 0);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 1; i += 2) {
+                size_t a = IX(o, i, j, k), b = a + 1;
+                d[a] = f[a] * w0[a] - f[b] * w0[b];
+                d[b] = f[b] * w0[a] + f[a] * w0[b];
+            }
+}
+
+static void oracle_rhs_velocity(oracle_t *o)
+{
+    int n = o->n;
+    double *w1 = W(o, 1), *w2 = W(o, 2), *w3 = W(o, 3), *w4 = W(o, 4), *w5 = W(o, 5), *w6 = W(o, 6);
+    /* Courant number (rhs_velocity.f90:31-38) */
+    double cmax = 0.0;
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                size_t a = IX(o, i, j, k);
+                double c = fabs(w1[a]) + fabs(w2[a]) + fabs(w3[a]);
+                if (c > cmax) cmax = c;
+            }
+    o->courant = cmax * o->dt / o->dx;
+
+    /* six products (both branches compute them identically) */
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                size_t a = IX(o, i, j, k);
+                double u = w1[a], v = w2[a], w = w3[a];
+                double t1 = u * u, t2 = u * v, t3 = u * w, t4 = v * v, t5 = v * w, t6 = w * w;
+                w1[a] = t1; w2[a] = t2; w3[a] = t3; w4[a] = t4; w5[a] = t5; w6[a] = t6;
+            }
+    for (int m = 1; m <= 6; m++) xfft3d(o, 1, W(o, m));
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 2; i++) {
+                size_t a = IX(o, i, j, k);
+                double kx = o->akx[i], ky = o->aky[k], kz = o->akz[j];
+                double t1 = -(kx * w1[a] + ky * w2[a] + kz * w3[a]);
+                double t2 = -(kx * w2[a] + ky * w4[a] + kz * w5[a]);
+                double t3 = -(kx * w3[a] + ky * w5[a] + kz * w6[a]);
+                double t4 = -o->nu * (kx * kx + ky * ky + kz * kz);
+                w1[a] = t1; w2[a] = t2; w3[a] = t3; w4[a] = t4;
+            }
+    double *fu[3] = {F(o, 0), F(o, 1), F(o, 2)};
+    double *wr[3] = {w1, w2, w3};
+    if (o->dealias == 0) {
+#pragma omp parallel for schedule(static)
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n + 1; i += 2) {
+                    size_t a = IX(o, i, j, k), b = a + 1;
+                    if (o->ialias[a] > 0) {
+                        for (int c = 0; c < 3; c++) { wr[c][a] = 0.0; wr[c][b] = 0.0; }
+                    } else {
+                        for (int c = 0; c < 3; c++) {
+                            double rt = -wr[c][b] + w4[a] * fu[c][a];
+                            wr[c][b] = wr[c][a] + w4[b] * fu[c][b];
+                            wr[c][a] = rt;
+                        }
+                    }
+                }
+    } else {
+        memset(W(o, 0), 0, sizeof(double) * o->fsz);
+#pragma omp parallel for schedule(static)
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n + 1; i += 2) {
+                    size_t a = IX(o, i, j, k), b = a + 1;
+                    if (o->ialias[a] > 1) {
+                        for (int c = 0; c < 3; c++) { wr[c][a] = 0.0; wr[c][b] = 0.0; }
+                    } else {
+                        for (int c = 0; c < 3; c++) {
+                            double rt = -0.5 * wr[c][b] + w4[a] * fu[c][a];
+                            wr[c][b] = 0.5 * wr[c][a] + w4[b] * fu[c][b];
+                            wr[c][a] = rt;
+                        }
+                    }
+                }
+        phase_factors(o);
+        shift_fwd(o, w4, fu[0]);
+        shift_fwd(o, w5, fu[1]);
+        xfft3d(o, -1, w4);
+        xfft3d(o, -1, w5);
+        /* (u+)(u+) */
+        mul3(o, w6, w4, w4);
+        xfft3d(o, 1, w6);
+        shift_back(o, w6);
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n + 1; i += 2) {
+                    size_t a = IX(o, i, j, k), b = a + 1;
+                    w1[a] = w1[a] + 0.5 * o->akx[i + 1] * w6[b];
+                    w1[b] = w1[b] - 0.5 * o->akx[i] * w6[a];
+                }
+        /* (u+)(v+) */
+        mul3(o, w6, w4, w5);
+        xfft3d(o, 1, w6);
+        shift_back(o, w6);
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n + 1; i += 2) {
+                    size_t a = IX(o, i, j, k), b = a + 1;
+                    w1[a] = w1[a] + 0.5 * o->aky[k] * w6[b];
+                    w1[b] = w1[b] - 0.5 * o->aky[k] * w6[a];
+                    w2[a] = w2[a] + 0.5 * o->akx[i + 1] * w6[b];
+                    w2[b] = w2[b] - 0.5 * o->akx[i] * w6[a];
+                }
+        /* (v+)(v+) */
+        mul3(o, w6, w5, w5);
+        xfft3d(o, 1, w6);
+        shift_back(o, w6);
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n + 1; i += 2) {
+                    size_t a = IX(o, i, j, k), b = a + 1;
+                    w2[a] = w2[a] + 0.5 * o->aky[k] * w6[b];
+                    w2[b] = w2[b] - 0.5 * o->aky[k] * w6[a];
+                }
+        /* w+ */
+        shift_fwd(o, w6, fu[2]);
+        xfft3d(o, -1, w6);
+        mul3(o, w4, w4, w6);
+        mul3(o, w5, w5, w6);
+        mul3(o, w6, w6, w6);
+        xfft3d(o, 1, w4);
+        xfft3d(o, 1, w5);
+        xfft3d(o, 1, w6);
+        shift_back(o, w4);
+        shift_back(o, w5);
+        shift_back(o, w6);
+#pragma omp parallel for schedule(static)
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n + 1; i += 2) {
+                    size_t a = IX(o, i, j, k), b = a + 1;
+                    double kx0 = o->akx[i], kx1 = o->akx[i + 1], ky = o->aky[k], kz = o->akz[j];
+                    if (o->ialias[a] < 2) {
+                        w1[a] = w1[a] + 0.5 * kz * w4[b];
+                        w1[b] = w1[b] - 0.5 * kz * w4[a];
+                        w2[a] = w2[a] + 0.5 * kz * w5[b];
+                        w2[b] = w2[b] - 0.5 * kz * w5[a];
+                        w3[a] = w3[a] + 0.5 * (kx1 * w4[b] + ky * w5[b] + kz * w6[b]);
+                        w3[b] = w3[b] - 0.5 * (kx0 * w4[a] + ky * w5[a] + kz * w6[a]);
+                    } else {
+                        w1[a] = 0.0; w1[b] = 0.0; w2[a] = 0.0; w2[b] = 0.0; w3[a] = 0.0; w3[b] = 0.0;
+                    }
+                }
+    }
+    if (o->les_model) les_rhs_velocity(o);
+}
+
+/* ------------------------------------------------------------------------- */
+/*  force_velocity (m_force.f90:101-182)                                     */
+/* ------------------------------------------------------------------------- */
+static double forcing_energy(oracle_t *o)
+{
+    int n = o->n;
+    double fac = 1.0 / (((double)n * n * n) * ((double)n * n * n));
+    double es[64] = {0};
+    double *u = F(o, 0), *v = F(o, 1), *w = F(o, 2);
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                double k2 = o->akx[i] * o->akx[i] + o->aky[k] * o->aky[k] + o->akz[j] * o->akz[j];
+                int sh = nint_shell32(k2);
+                if (sh > 0 && sh <= o->kfmax) {
+                    size_t a = IX(o, i, j, k);
+                    double f2 = fac * (u[a] * u[a] + v[a] * v[a] + w[a] * w[a]);
+                    if (o->akx[i] == 0.0) f2 = f2 * 0.5;
+                    es[sh - 1] = es[sh - 1] + f2;
+                }
+            }
+    double e = 0.0;
+    for (int s = 0; s < o->kfmax; s++) e = e + es[s];
+    return e;
+}
+
+double oracle_forcing_energy(oracle_t *o) { return forcing_energy(o); }
+
+static void force_velocity(oracle_t *o)
+{
+    double energy = forcing_energy(o);
+    double fac = o->famp / energy;
+    for (int m = 0; m < o->nfn; m++) {
+        size_t a = IX(o, o->fn_i[m], o->fn_j[m], o->fn_k[m]);
+        for (int c = 0; c < 3; c++) W(o, 1 + c)[a] = W(o, 1 + c)[a] + fac * F(o, c)[a];
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/*  pressure (pressure.f90:1-51)                                             */
+/* ------------------------------------------------------------------------- */
+static void pressure(oracle_t *o)
+{
+    int n = o->n;
+    double *u = F(o, 0), *v = F(o, 1), *w = F(o, 2);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 1; i += 2) {
+                size_t a = IX(o, i, j, k), b = a + 1;
+                double kx0 = o->akx[i], kx1 = o->akx[i + 1], ky = o->aky[k], kz = o->akz[j];
+                double div2 = kx0 * u[a] + ky * v[a] + kz * w[a];
+                double div1 = -(kx1 * u[b] + ky * v[b] + kz * w[b]);
+                double l1 = kx0 * kx0 + ky * ky + kz * kz;
+                double l2 = kx1 * kx1 + ky * ky + kz * kz;
+                if (l1 == 0.0) l1 = 9e20;
+                if (l2 == 0.0) l2 = 9e20;
+                double p1 = -div1 / l1, p2 = -div2 / l2;
+                u[a] = u[a] + p2 * kx1; u[b] = u[b] - p1 * kx0;
+                v[a] = v[a] + p2 * ky;  v[b] = v[b] - p1 * ky;
+                w[a] = w[a] + p2 * kz;  w[b] = w[b] - p1 * kz;
+            }
+}
+
+void oracle_pressure(oracle_t *o) { pressure(o); }
+
+/* ------------------------------------------------------------------------- */
+/*  one timestep of the hydro task (main.f90:124-170)                        */
+/* ------------------------------------------------------------------------- */
+void oracle_step(oracle_t *o, int nsteps)
+{
+    for (int it = 0; it < nsteps; it++) {
+        oracle_rhs_scalars(o);
+        if (o->int_scalars) {
+            int nlo = 3, nhi = 3 + o->nscal;
+            double dt = o->dt;
+            for (int m = nlo; m < nhi; m++) {
+                double *f = F(o, m), *r = RO(o, m), *w = W(o, m + 1);
+                if (o->fos) {
+                    for (size_t q = 0; q < o->fsz; q++) { r[q] = w[q]; f[q] = f[q] + dt * r[q]; }
+                } else {
+                    for (size_t q = 0; q < o->fsz; q++) {
+                        f[q] = f[q] + dt * (1.5 * w[q] - 0.5 * r[q]);
+                        r[q] = w[q];
+                    }
+                }
+            }
+            o->fos = 0;
+        }
+        oracle_rhs_velocity(o);
+        if (o->flow_type == 1) force_velocity(o);
+        double dt = o->dt;
+        for (int m = 0; m < 3; m++) {
+            double *f = F(o, m), *r = RO(o, m), *w = W(o, m + 1);
+            if (o->fov) {
+#pragma omp parallel for schedule(static)
+                for (size_t q = 0; q < o->fsz; q++) { r[q] = w[q]; f[q] = f[q] + dt * r[q]; }
+            } else {
+#pragma omp parallel for schedule(static)
+                for (size_t q = 0; q < o->fsz; q++) {
+                    f[q] = f[q] + dt * (1.5 * w[q] - 0.5 * r[q]);
+                    r[q] = w[q];
+                }
+            }
+        }
+        o->fov = 0;
+        pressure(o);
+        o->time += o->dt;
+    }
+}
+
+/* RHS only (no update): rhs_scalars + rhs_velocity + forcing; results in wrk1..3+ns */
+void oracle_rhs(oracle_t *o)
+{
+    oracle_rhs_scalars(o);
+    /* rhs_velocity reuses wrk4..; save scalar RHS first */
+    int ns = o->int_scalars ? o->nscal : 0;
+    double *save = NULL;
+    if (ns) {
+        save = (double *)malloc(sizeof(double) * o->fsz * ns);
+        memcpy(save, W(o, 4), sizeof(double) * o->fsz * ns);
+    }
+    oracle_rhs_velocity(o);
+    if (o->flow_type == 1) force_velocity(o);
+    if (ns) { memcpy(W(o, 4), save, sizeof(double) * o->fsz * ns); free(save); }
+}
+
+/* ------------------------------------------------------------------------- */
+/*  statistics (m_stats.f90:99-440) + velocity-derivative skewness (new)     */
+/*  out[0..kmax) = e_spec; out[kmax..] = energy, eps_v, eta, etakmax, uvar,  */
+/*  x_length, lambda, re_lambda, re_lambda1, tau_e, enstrophy, skewness      */
+/* ------------------------------------------------------------------------- */
+static void derivative(oracle_t *o, const double *src, char axis, double *dst)
+{
+    int n = o->n;
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 2; i++) {
+                size_t a = IX(o, i, j, k);
+                double kk = axis == 'x' ? o->akx[i] : axis == 'y' ? o->aky[k] : o->akz[j];
+                dst[a] = kk * src[a];
+            }
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 1; i += 2) {
+                size_t a = IX(o, i, j, k);
+                double rt = -dst[a + 1];
+                dst[a + 1] = dst[a];
+                dst[a] = rt;
+            }
+}
+
+void oracle_energy_spectrum(oracle_t *o, int field0, int ncomp, double *es)
+{
+    int n = o->n;
+    double fac = 1.0 / (((double)n * n * n) * ((double)n * n * n));
+    for (int s = 0; s < o->kmax; s++) es[s] = 0.0;
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                double k2 = o->akx[i] * o->akx[i] + o->aky[k] * o->aky[k] + o->akz[j] * o->akz[j];
+                int sh = nint_shell32(k2);
+                if (sh > 0 && sh <= o->kmax) {
+                    size_t a = IX(o, i, j, k);
+                    double sq = 0.0;
+                    for (int c = 0; c < ncomp; c++) {
+                        double x = F(o, field0 + c)[a];
+                        sq = (c == 0) ? x * x : sq + x * x;
+                    }
+                    double f2 = fac * sq;
+                    if (o->akx[i] == 0.0) f2 = 0.5 * f2;
+                    es[sh - 1] = es[sh - 1] + f2;
+                }
+            }
+}
+
+void oracle_stats(oracle_t *o, double *out)
+{
+    int n = o->n, kmax = o->kmax;
+    double PI = 4.0 * atan(1.0);
+    double *es = out;
+    double fac = 1.0 / ((double)n * n * n);
+    /* enstrophy (m_stats.f90:241-289) */
+    for (int m = 0; m < 3; m++) copy_field(o, W(o, 1 + m), F(o, m));
+    derivative(o, W(o, 3), 'y', W(o, 6));
+    derivative(o, W(o, 3), 'x', W(o, 5));
+    derivative(o, W(o, 2), 'z', W(o, 4));
+    derivative(o, W(o, 2), 'x', W(o, 3));
+    derivative(o, W(o, 1), 'z', W(o, 2));
+    derivative(o, W(o, 1), 'y', W(o, 1));
+    for (size_t q = 0; q < o->fsz; q++) {
+        W(o, 3)[q] = W(o, 3)[q] - W(o, 1)[q];
+        W(o, 2)[q] = W(o, 2)[q] - W(o, 5)[q];
+        W(o, 1)[q] = W(o, 6)[q] - W(o, 4)[q];
+    }
+    for (int m = 1; m <= 3; m++) xfft3d(o, -1, W(o, m));
+    double ens = 0.0;
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                size_t a = IX(o, i, j, k);
+                double x = W(o, 1)[a] * W(o, 1)[a] + W(o, 2)[a] * W(o, 2)[a] + W(o, 3)[a] * W(o, 3)[a];
+                ens += x;
+            }
+    ens = ens * fac;
+    /* skewness of the longitudinal derivatives (new statistic) */
+    double skew = 0.0;
+    for (int c = 0; c < 3; c++) {
+        derivative(o, F(o, c), c == 0 ? 'x' : c == 1 ? 'y' : 'z', W(o, 1));
+        xfft3d(o, -1, W(o, 1));
+        double m2 = 0.0, m3 = 0.0;
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n; i++) {
+                    double d = W(o, 1)[IX(o, i, j, k)];
+                    m2 += d * d;
+                    m3 += d * d * d;
+                }
+        m2 *= fac; m3 *= fac;
+        skew += m3 / pow(m2, 1.5);
+    }
+    skew /= 3.0;
+    /* spectrum and derived quantities (m_stats.f90:99-189) */
+    oracle_energy_spectrum(o, 0, 3, es);
+    double energy = 0.0;
+    for (int k = 0; k < kmax; k++) energy = energy + es[k];
+    double eps = 0.0;
+    for (int k = 1; k <= kmax; k++) eps = eps + es[k - 1] * (double)(k * k) * 2.0 * o->nu;
+    double eta = pow(o->nu * o->nu * o->nu / eps, 0.25);
+    double etakmax = eta * (double)kmax;
+    double uvar = 2.0 / 3.0 * energy;
+    double sct = 0.0;
+    for (int k = 1; k <= kmax; k++) sct = sct + es[k - 1] / (double)k;
+    double xl = PI / 2.0 * sct / uvar;
+    double lam = sqrt(15.0 * uvar * o->nu / eps);
+    double rel = uvar * sqrt(15.0 / eps * (1.0 / o->nu));
+    double rel1 = sqrt(uvar) * lam / o->nu;
+    double taue = xl / sqrt(uvar);
+    double *d = out + kmax;
+    d[0] = energy; d[1] = eps; d[2] = eta; d[3] = etakmax; d[4] = uvar; d[5] = xl;
+    d[6] = lam; d[7] = rel; d[8] = rel1; d[9] = taue; d[10] = ens; d[11] = skew;
+}
+
+/* scalar statistics (m_stats.f90:295-440): per scalar out[s*(kmax+5)+..] =
+ * spectrum (x2), dissipation, mean, variance, min, max */
+void oracle_scalar_stats(oracle_t *o, double *out)
+{
+    int n = o->n, kmax = o->kmax;
+    double fac = 1.0 / ((double)n * n * n);
+    for (int s = 0; s < o->nscal; s++) {
+        double *d = out + (size_t)s * (kmax + 5);
+        oracle_energy_spectrum(o, 3 + s, 1, d);
+        for (int k = 0; k < kmax; k++) d[k] = 2.0 * d[k];
+        copy_field(o, W(o, 0), F(o, 3 + s));
+        derivative(o, W(o, 0), 'x', W(o, 1));
+        derivative(o, W(o, 0), 'y', W(o, 2));
+        derivative(o, W(o, 0), 'z', W(o, 3));
+        for (int m = 1; m <= 3; m++) xfft3d(o, -1, W(o, m));
+        double q = 0.0;
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n; i++) {
+                    size_t a = IX(o, i, j, k);
+                    q += W(o, 1)[a] * W(o, 1)[a] + W(o, 2)[a] * W(o, 2)[a] + W(o, 3)[a] * W(o, 3)[a];
+                }
+        d[kmax] = 2.0 * o->pe[s] * q * fac;
+        xfft3d(o, -1, W(o, 0));
+        double m1 = 0.0, m2 = 0.0, mn = 1e300, mx = -1e300;
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n; i++) {
+                    double x = W(o, 0)[IX(o, i, j, k)];
+                    m1 += x; m2 += x * x;
+                    if (x < mn) mn = x;
+                    if (x > mx) mx = x;
+                }
+        m1 *= fac; m2 *= fac;
+        d[kmax + 1] = m1; d[kmax + 2] = m2 - m1 * m1; d[kmax + 3] = mn; d[kmax + 4] = mx;
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/*  initial velocity (init_velocity.f90:1-246); isp 0, 1, 3 as the reference */
+/*  and isp 2 = k^ir_exp * exp(-2 (k/k_p)^2), a spectrum the reference lacks */
+/* ------------------------------------------------------------------------- */
+int oracle_init_velocity(oracle_t *o, double rn1, int isp_type, double peak_wavenum, double ir_exp)
+{
+    int n = o->n, kmax = o->kmax;
+    double PI = 4.0 * atan(1.0), TWO_PI = 2.0 * PI;
+    if (isp_type == -1) {
+        /* Taylor-Green (init_velocity.f90:252-293) */
+        double dx = 2.0 * PI / (double)n;
+        for (int k = 0; k < n; k++) {
+            double zz = (double)k * dx;
+            for (int j = 0; j < n; j++) {
+                double yy = (double)j * dx;
+                for (int i = 0; i < n; i++) {
+                    double xx = (double)i * dx;
+                    size_t a = IX(o, i, j, k);
+                    W(o, 1)[a] = sin(xx) * cos(yy) * cos(zz);
+                    W(o, 2)[a] = -cos(xx) * sin(yy) * cos(zz);
+                    W(o, 3)[a] = 0.0;
+                }
+            }
+        }
+        for (int m = 1; m <= 3; m++) { xfft3d(o, 1, W(o, m)); copy_field(o, F(o, m - 1), W(o, m)); }
+        return 0;
+    }
+    /* random numbers over the full padded arrays, wrk1..6 in order */
+    randu_state st;
+    oracle_randu_reset(&st);
+    (void)oracle_randu(&st, -rn1);
+    for (int m = 1; m <= 6; m++) {
+        double *w = W(o, m);
+        for (size_t q = 0; q < o->fsz; q++) w[q] = oracle_randu(&st, rn1);
+    }
+    for (int m = 1; m <= 3; m++) {
+        double *a = W(o, m), *b = W(o, m + 3);
+        for (size_t q = 0; q < o->fsz; q++) a[q] = sqrt(-2.0 * log(a[q])) * sin(TWO_PI * b[q]);
+    }
+    for (int m = 1; m <= 3; m++) xfft3d(o, 1, W(o, m));
+    double *w1 = W(o, 1), *w2 = W(o, 2), *w3 = W(o, 3), *w4 = W(o, 4), *w5 = W(o, 5), *w6 = W(o, 6);
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 1; i += 2) {
+                size_t a = IX(o, i, j, k), b = a + 1;
+                double kx0 = o->akx[i], kx1 = o->akx[i + 1], ky = o->aky[k], kz = o->akz[j];
+                int sh = nint_shell64(kx0 * kx0 + ky * ky + kz * kz);
+                if (sh > 0 && sh <= kmax) {
+                    w4[a] = -(ky * w3[b] - kz * w2[b]);
+                    w4[b] = ky * w3[a] - kz * w2[a];
+                    w5[a] = -(kz * w1[b] - kx1 * w3[b]);
+                    w5[b] = kz * w1[a] - kx0 * w3[a];
+                    w6[a] = -(kx1 * w2[b] - ky * w1[b]);
+                    w6[b] = kx0 * w2[a] - ky * w1[a];
+                } else {
+                    w4[a] = w4[b] = w5[a] = w5[b] = w6[a] = w6[b] = 0.0;
+                }
+            }
+    for (int m = 0; m < 3; m++) copy_field(o, F(o, m), W(o, 4 + m));
+    double *es = (double *)calloc(kmax + 1, sizeof(double));
+    double *et = (double *)calloc(kmax + 1, sizeof(double));
+    oracle_energy_spectrum(o, 0, 3, es);
+    for (int k = 1; k <= kmax; k++) {
+        double wmag = (double)k, ratio = wmag / peak_wavenum;
+        if (isp_type == 0) et[k - 1] = pow(wmag, -5.0 / 3.0);
+        else if (isp_type == 1) et[k - 1] = ratio * ratio * ratio / peak_wavenum * exp(-3.0 * ratio);
+        else if (isp_type == 2) et[k - 1] = pow(wmag, ir_exp) * exp(-2.0 * ratio * ratio);
+        else if (isp_type == 3) {
+            double f = 2.0 * PI * ratio;
+            double f2 = f * f, d = 1.0 + f2;
+            et[k - 1] = (f2 * f2) / (d * d * d);
+        } else { free(es); free(et); return -1; }
+    }
+    double tot = 0.0;
+    for (int k = 0; k < kmax; k++) tot = tot + et[k];
+    for (int k = 0; k < kmax; k++) et[k] = et[k] / tot;
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 2; i++) {
+                double k2 = o->akx[i] * o->akx[i] + o->aky[k] * o->aky[k] + o->akz[j] * o->akz[j];
+                int sh = nint_shell32(k2);
+                size_t a = IX(o, i, j, k);
+                if (sh > 0 && sh <= kmax && es[sh - 1] > 0.0) {
+                    double r = sqrt(et[sh - 1] / es[sh - 1]);
+                    for (int c = 0; c < 3; c++) F(o, c)[a] = F(o, c)[a] * r;
+                } else {
+                    for (int c = 0; c < 3; c++) F(o, c)[a] = 0.0;
+                }
+            }
+    free(es); free(et);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/*  particles (m_particles.f90:815-1230, 1451-1508) on one periodic slab     */
+/*  uphys: three (nx+2,ny,nz) physical velocity arrays; xyzp/uvwp: 3*np,     */
+/*  particle-major like the reference's (3,np) arrays.                       */
+/* ------------------------------------------------------------------------- */
+static double cint1(double p1, double p2, double p3, double p4, const double *r)
+{
+    return (r[0] * p1 + r[1] * p2 + r[2] * p3 + r[3] * p4) / 6.0;
+}
+
+static void cint_r(double x, double *r)
+{
+    double s = (x - 1.0) * (x - 2.0);
+    r[0] = -x * s;
+    r[1] = 3.0 * (x + 1.0) * s;
+    s = (x + 1.0) * x;
+    r[2] = -3.0 * s * (x - 2.0);
+    r[3] = s * (x - 1.0);
+}
+
+static double cint_3d(const double a[4][4][4] /* [k][j][i] */, double x, double y, double z)
+{
+    double r[4], t2[4][4], t1[4];
+    cint_r(x, r);
+    for (int k = 0; k < 4; k++)
+        for (int j = 0; j < 4; j++) t2[k][j] = cint1(a[k][j][0], a[k][j][1], a[k][j][2], a[k][j][3], r);
+    cint_r(y, r);
+    for (int k = 0; k < 4; k++) t1[k] = cint1(t2[k][0], t2[k][1], t2[k][2], t2[k][3], r);
+    cint_r(z, r);
+    return cint1(t1[0], t1[1], t1[2], t1[3], r);
+}
+
+void oracle_particles_step(int n, double dt, const double *uphys, int64_t np, double *xyzp, double *uvwp,
+                           int scheme)
+{
+    size_t fsz = (size_t)(n + 2) * n * n;
+    double PI = 4.0 * atan(1.0);
+    double dx = 2.0 * PI / (double)n, dy = dx, dz = dx;
+    const double *U[3] = {uphys, uphys + fsz, uphys + 2 * fsz};
+#define PIX(i, j, k) ((size_t)((i) - 1) + (size_t)(n + 2) * ((size_t)((j) - 1) + (size_t)n * (size_t)((k) - 1)))
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < np; p++) {
+        double *X = xyzp + 3 * p, *V = uvwp + 3 * p;
+        int i = (int)floor(X[0]), j = (int)floor(X[1]), k = (int)floor(X[2]);
+        double xp = X[0] - (double)i, yp = X[1] - (double)j, zp = X[2] - (double)k;
+        double up[3];
+        if (scheme == 0) {
+            double c1 = (1.0 - xp) * (1.0 - yp) * (1.0 - zp);
+            double c2 = (xp) * (1.0 - yp) * (1.0 - zp);
+            double c3 = (1.0 - xp) * (yp) * (1.0 - zp);
+            double c4 = (xp) * (yp) * (1.0 - zp);
+            double c5 = (1.0 - xp) * (1.0 - yp) * (zp);
+            double c6 = (xp) * (1.0 - yp) * (zp);
+            double c7 = (1.0 - xp) * (yp) * (zp);
+            double c8 = (xp) * (yp) * (zp);
+            int i1 = (i == n) ? 1 : i + 1;
+            int j1 = (j == n) ? 1 : j + 1;
+            int k1 = (k == n) ? 1 : k + 1;
+            for (int c = 0; c < 3; c++) {
+                const double *f = U[c];
+                double s = c1 * f[PIX(i, j, k)] + c2 * f[PIX(i1, j, k)] + c3 * f[PIX(i, j1, k)] + c4 * f[PIX(i1, j1, k)];
+                s = s + c5 * f[PIX(i, j, k1)] + c6 * f[PIX(i1, j, k1)] + c7 * f[PIX(i, j1, k1)] + c8 * f[PIX(i1, j1, k1)];
+                up[c] = s;
+            }
+        } else {
+            double loc[3][4][4][4];
+            for (int kk = 0; kk < 4; kk++) {
+                int k1 = k - 2 + kk + 1;
+                if (k1 < 1) k1 += n;
+                if (k1 > n) k1 -= n;
+                for (int jj = 0; jj < 4; jj++) {
+                    int j1 = j - 2 + jj + 1;
+                    if (j1 < 1) j1 += n;
+                    if (j1 > n) j1 -= n;
+                    for (int ii = 0; ii < 4; ii++) {
+                        int i1 = i - 2 + ii + 1;
+                        if (i1 < 1) i1 += n;
+                        if (i1 > n) i1 -= n;
+                        for (int c = 0; c < 3; c++) loc[c][kk][jj][ii] = U[c][PIX(i1, j1, k1)];
+                    }
+                }
+            }
+            for (int c = 0; c < 3; c++) up[c] = cint_3d(loc[c], xp, yp, zp);
+        }
+        if (V[0] == -999.0) {
+            xp = xp + dt * up[0] / dx;
+            yp = yp + dt * up[1] / dy;
+            zp = zp + dt * up[2] / dz;
+        } else {
+            xp = xp + (1.50 * up[0] - 0.50 * V[0]) * dt / dx;
+            yp = yp + (1.50 * up[1] - 0.50 * V[1]) * dt / dy;
+            zp = zp + (1.50 * up[2] - 0.50 * V[2]) * dt / dz;
+        }
+        V[0] = up[0]; V[1] = up[1]; V[2] = up[2];
+        if (xp > 1.0) { xp = xp - 1.0; i = i + 1; if (i > n) i = i - n; }
+        if (xp < 0.0) { xp = xp + 1.0; i = i - 1; if (i < 1) i = i + n; }
+        if (yp > 1.0) { yp = yp - 1.0; j = j + 1; if (j > n) j = j - n; }
+        if (yp < 0.0) { yp = yp + 1.0; j = j - 1; if (j < 1) j = j + n; }
+        if (zp > 1.0) { zp = zp - 1.0; k = k + 1; }
+        if (zp < 0.0) { zp = zp + 1.0; k = k - 1; }
+        X[0] = xp + (double)i;
+        X[1] = yp + (double)j;
+        X[2] = zp + (double)k;
+        /* slab migration on a single periodic slab (m_particles.f90:1270-1319) */
+        if (X[2] >= (double)(n + 1)) X[2] = X[2] - (double)n;
+        else if (X[2] < 1.0) X[2] = X[2] + (double)n;
+    }
+#undef PIX
+}
+
+/* lattice initialisation (m_particles.f90:220-262, 314-319): returns nptot */
+int64_t oracle_particles_lattice(int n, int64_t nptot_in, double *xyzp /* may be NULL */)
+{
+    int64_t npt = (int64_t)((double)nptot_in > 0 ? pow((double)nptot_in, 1.0 / 3.0) : 0);
+    if (nptot_in - npt * npt * npt >= (npt + 1) * (npt + 1) * (npt + 1) - nptot_in) npt = npt + 1;
+    int64_t nptot = npt * npt * npt;
+    if (!xyzp) return nptot;
+    double PI = 4.0 * atan(1.0);
+    double sctmp = 2.0 * PI / (double)npt;
+    int64_t m = 0;
+    for (int64_t k = 1; k <= npt; k++)
+        for (int64_t j = 1; j <= npt; j++)
+            for (int64_t i = 1; i <= npt; i++) {
+                xyzp[3 * m + 0] = ((double)(i - 1) + 0.5) * sctmp;
+                xyzp[3 * m + 1] = ((double)(j - 1) + 0.5) * sctmp;
+                xyzp[3 * m + 2] = ((double)(k - 1) + 0.5) * sctmp;
+                m++;
+            }
+    for (int64_t p = 0; p < nptot * 3; p++) {
+        double x = xyzp[p];
+        if (x >= 2.0 * PI || x < 0.0) xyzp[p] = x - 2.0 * PI * floor(x / (2.0 * PI));
+    }
+    for (int64_t p = 0; p < nptot; p++) {
+        xyzp[3 * p + 0] = xyzp[3 * p + 0] / (2.0 * PI / (double)n) + 1.0;
+        xyzp[3 * p + 1] = xyzp[3 * p + 1] / (2.0 * PI / (double)n) + 1.0;
+        xyzp[3 * p + 2] = xyzp[3 * p + 2] / (2.0 * PI / (double)n) + 1.0;
+    }
+    return nptot;
+}
+
+/* ------------------------------------------------------------------------- */
+/*  filters (m_filter_xfftw.f90:121-286) and subgrid stress                  */
+/*  kind 2 = Gaussian (reference), kind 4 = box (new).  Returns filter_g in  */
+/*  the Fourier layout of one (nx+2,ny,nz) array.                            */
+/* ------------------------------------------------------------------------- */
+void oracle_filter_g(oracle_t *o, int kind, double delta, double *g)
+{
+    int n = o->n;
+    double PI = 4.0 * atan(1.0), dx = o->dx;
+    memset(g, 0, sizeof(double) * o->fsz);
+    if (kind == 2) {
+        double c1 = 6.0 / (delta * delta);
+        double sq = sqrt(c1 / PI);
+        double c2 = sq * sq * sq * (dx * dx * dx);
+        for (int k = 0; k < n; k++) {
+            int dk = k < n - k ? k : n - k;
+            double rz = dx * (double)dk;
+            for (int j = 0; j < n; j++) {
+                int dj = j < n - j ? j : n - j;
+                double ry = dx * (double)dj;
+                for (int i = 0; i < n; i++) {
+                    int di = i < n - i ? i : n - i;
+                    double rx = dx * (double)di;
+                    rx = rx * rx + ry * ry + rz * rz;
+                    double v = c2 * exp(-c1 * rx);
+                    if (v < 1.e-20) v = 0.0;
+                    g[IX(o, i, j, k)] = v;
+                }
+            }
+        }
+        xfft3d(o, 1, g);
+    } else {
+        /* box filter of width delta: spectral transfer function
+         * prod_a sin(k_a delta/2)/(k_a delta/2), real, stored in the re slots */
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n + 1; i += 2) {
+                    double h = 1.0;
+                    double ks[3] = {o->akx[i], o->aky[k], o->akz[j]};
+                    for (int a = 0; a < 3; a++) {
+                        double t = 0.5 * ks[a] * delta;
+                        h *= (t == 0.0) ? 1.0 : sin(t) / t;
+                    }
+                    g[IX(o, i, j, k)] = h;
+                    g[IX(o, i, j, k) + 1] = 0.0;
+                }
+    }
+}
+
+void oracle_apply_filter(oracle_t *o, const double *g, double *a)
+{
+    int n = o->n;
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 1; i += 2) {
+                size_t p = IX(o, i, j, k);
+                double x = a[p], y = a[p + 1], c = g[p], d = g[p + 1];
+                a[p] = x * c - y * d;
+                a[p + 1] = y * c + x * d;
+            }
+}
+
+int oracle_n(oracle_t *o) { return o->n; }
+size_t oracle_fsz(oracle_t *o) { return o->fsz; }
+double oracle_time(oracle_t *o) { return o->time; }
+void oracle_set_time(oracle_t *o, double t) { o->time = t; }
+double *oracle_turb_visc(oracle_t *o) { return o->turb_visc; }
