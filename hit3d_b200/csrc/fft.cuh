@@ -1,0 +1,260 @@
+// Radix-2/3/4/8 Stockham FFT on columns staged through shared memory.
+//
+// One CTA transforms TC independent sticks ("columns") of length L.  Stage 0 takes
+// its inputs straight from registers (loaded from HBM by the caller), the middle
+// stages exchange through shared memory, and the last stage leaves its outputs in
+// registers for the caller to store (or to combine with other fields first).  With
+// Stockham ordering the stage-0 inputs and the last-stage outputs of butterfly j
+// both sit at positions j + m*L/R, so a pass over HBM reads and writes the same
+// addresses and can run in place.
+//
+// Two shared-memory layouts:
+//   COLS (ROWS=false): element (c,p) at p*TC + c -- columns interleaved, used for
+//        the strided y/z passes where TC adjacent kx columns form one 128-byte row;
+//   ROWS (ROWS=true):  element (c,p) at c*(L+L/8) + p + p/8 -- each stick
+//        contiguous with one pad slot per 8 elements, used for the x passes.
+#pragma once
+#include "common.cuh"
+
+// ---------------------------------------------------------------------------
+// radix plans: forward order; the inverse x pass uses the reversed plan so that
+// its last radix equals the forward plan's first radix (register hand-off).
+// ---------------------------------------------------------------------------
+H3D_HD constexpr int plan_stages(int L)
+{
+    return L == 16 ? 2 : L == 32 ? 2 : L == 48 ? 3 : L == 64 ? 2 : L == 96 ? 3 : L == 128 ? 3 :
+           L == 192 ? 3 : L == 256 ? 3 : L == 384 ? 4 : L == 512 ? 3 : L == 768 ? 4 : L == 1024 ? 4 : 0;
+}
+
+H3D_HD constexpr int plan_radix_fwd(int L, int s)
+{
+    // 16=4.4 32=8.4 48=4.4.3 64=8.8 96=8.4.3 128=8.4.4 192=8.8.3 256=8.8.4
+    // 384=8.4.4.3 512=8.8.8 768=8.8.4.3 1024=8.8.4.4
+    return L == 16 ? 4 :
+           L == 32 ? (s == 0 ? 8 : 4) :
+           L == 48 ? (s < 2 ? 4 : 3) :
+           L == 64 ? 8 :
+           L == 96 ? (s == 0 ? 8 : s == 1 ? 4 : 3) :
+           L == 128 ? (s == 0 ? 8 : 4) :
+           L == 192 ? (s < 2 ? 8 : 3) :
+           L == 256 ? (s < 2 ? 8 : 4) :
+           L == 384 ? (s == 0 ? 8 : s < 3 ? 4 : 3) :
+           L == 512 ? 8 :
+           L == 768 ? (s < 2 ? 8 : s == 2 ? 4 : 3) :
+           L == 1024 ? (s < 2 ? 8 : 4) : 0;
+}
+
+template <int L, bool REV> struct Plan {
+    static constexpr int S = plan_stages(L);
+    static H3D_HD constexpr int R(int s) { return REV ? plan_radix_fwd(L, S - 1 - s) : plan_radix_fwd(L, s); }
+    // product of the radices of stages [0, s)
+    static H3D_HD constexpr int Ns(int s) { return s == 0 ? 1 : Ns(s - 1) * R(s - 1); }
+};
+
+// ---------------------------------------------------------------------------
+// small DFTs in registers, natural order in and out
+// ---------------------------------------------------------------------------
+template <typename T, bool FWD> H3D_D void dft2(cx<T> &a, cx<T> &b)
+{
+    cx<T> t = a;
+    a = t + b;
+    b = t - b;
+}
+
+template <typename T, bool FWD> H3D_D void dft4(cx<T> &a0, cx<T> &a1, cx<T> &a2, cx<T> &a3)
+{
+    cx<T> s0 = a0 + a2, d0 = a0 - a2, s1 = a1 + a3, d1 = mul_mi<FWD>(a1 - a3);
+    a0 = s0 + s1;
+    a2 = s0 - s1;
+    a1 = d0 + d1;
+    a3 = d0 - d1;
+}
+
+template <typename T, bool FWD> H3D_D void dft3(cx<T> &a0, cx<T> &a1, cx<T> &a2)
+{
+    const T h = (T)0.5;
+    const T s3 = (T)0.86602540378443864676372317075293618;  // sin(2 pi/3)
+    cx<T> s = a1 + a2, d = a1 - a2;
+    cx<T> m = mk<T>(a0.x - h * s.x, a0.y - h * s.y);
+    // forward: X1 = m - i s3 d, X2 = m + i s3 d
+    cx<T> r = mk<T>(s3 * d.y, -s3 * d.x);  // -i*s3*d
+    if (!FWD) r = mk<T>(-r.x, -r.y);
+    a0 = a0 + s;
+    a1 = m + r;
+    a2 = m - r;
+}
+
+template <typename T, bool FWD> H3D_D void dft8(cx<T> (&a)[8])
+{
+    const T r2 = (T)0.70710678118654752440084436210484904;
+    cx<T> e0 = a[0], e1 = a[2], e2 = a[4], e3 = a[6];
+    cx<T> o0 = a[1], o1 = a[3], o2 = a[5], o3 = a[7];
+    dft4<T, FWD>(e0, e1, e2, e3);
+    dft4<T, FWD>(o0, o1, o2, o3);
+    // twiddles w8^k, w8 = exp(-+ i pi/4)
+    cx<T> t1 = FWD ? mk<T>(r2 * (o1.x + o1.y), r2 * (o1.y - o1.x)) : mk<T>(r2 * (o1.x - o1.y), r2 * (o1.y + o1.x));
+    cx<T> t2 = mul_mi<FWD>(o2);
+    cx<T> t3 = FWD ? mk<T>(r2 * (-o3.x + o3.y), r2 * (-o3.y - o3.x)) : mk<T>(r2 * (-o3.x - o3.y), r2 * (-o3.y + o3.x));
+    a[0] = e0 + o0; a[4] = e0 - o0;
+    a[1] = e1 + t1; a[5] = e1 - t1;
+    a[2] = e2 + t2; a[6] = e2 - t2;
+    a[3] = e3 + t3; a[7] = e3 - t3;
+}
+
+template <typename T, int R, bool FWD> H3D_D void dft(cx<T> *a)
+{
+    if constexpr (R == 2) dft2<T, FWD>(a[0], a[1]);
+    else if constexpr (R == 3) dft3<T, FWD>(a[0], a[1], a[2]);
+    else if constexpr (R == 4) dft4<T, FWD>(a[0], a[1], a[2], a[3]);
+    else if constexpr (R == 8) {
+        cx<T> t[8];
+#pragma unroll
+        for (int m = 0; m < 8; m++) t[m] = a[m];
+        dft8<T, FWD>(t);
+#pragma unroll
+        for (int m = 0; m < 8; m++) a[m] = t[m];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// thread <-> butterfly mapping and shared-memory layout
+// ---------------------------------------------------------------------------
+template <int L, int TC, bool ROWS> struct Lay {
+    static constexpr int RS = L + L / 8;  // padded stick length in ROWS layout
+    static constexpr int elems = ROWS ? TC * RS : TC * L;
+    static H3D_D int idx(int c, int p) { return ROWS ? c * RS + p + (p >> 3) : p * TC + c; }
+    template <int R> static H3D_D void bf(int b, int &c, int &j)
+    {
+        constexpr int nbpc = L / R;
+        if (ROWS) { j = b % nbpc; c = b / nbpc; }
+        else { c = b % TC; j = b / TC; }
+    }
+};
+
+template <int L, int TC, int NT, int R> struct Cnt {
+    static constexpr int total = TC * (L / R);           // butterflies per stage per CTA
+    static constexpr int NB = (total + NT - 1) / NT;      // per thread
+};
+
+// twiddle w^(k*m) for a stage whose sub-transform length is Ns*R;
+// tw[t] = exp(-2 pi i t / L)
+template <typename T, bool FWD> H3D_D cx<T> twid(const cx<T> *__restrict__ tw, int t)
+{
+    cx<T> w = __ldg(tw + t);
+    if (!FWD) w.y = -w.y;
+    return w;
+}
+
+// ---------------------------------------------------------------------------
+// the column transform: in[] (stage-0 inputs) -> out[] (last-stage outputs)
+//   in[i*R0+m]  : column c, position j + m*L/R0 of butterfly b = tid + i*NT
+//   out[i*RL+m] : column c, position j + m*L/RL of butterfly b = tid + i*NT
+// The caller must __syncthreads() before reusing sm after this returns.
+// ---------------------------------------------------------------------------
+template <typename T, int L, int TC, int NT, bool ROWS, bool FWD, bool REV, int s>
+H3D_D void fft_mid_stage(cx<T> *sm, const cx<T> *__restrict__ tw)
+{
+    using P = Plan<L, REV>;
+    using LY = Lay<L, TC, ROWS>;
+    constexpr int R = P::R(s), Ns = P::Ns(s), nbpc = L / R;
+    using CN = Cnt<L, TC, NT, R>;
+    cx<T> a[CN::NB * R];
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int i = 0; i < CN::NB; i++) {
+        int b = tid + i * NT;
+        if (CN::total % NT == 0 || b < CN::total) {
+            int c, j;
+            LY::template bf<R>(b, c, j);
+            int k = j % Ns;
+#pragma unroll
+            for (int m = 0; m < R; m++) {
+                cx<T> v = sm[LY::idx(c, j + m * nbpc)];
+                if (m > 0) v = cmul(v, twid<T, FWD>(tw, k * m * (L / (Ns * R))));
+                a[i * R + m] = v;
+            }
+            dft<T, R, FWD>(a + i * R);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < CN::NB; i++) {
+        int b = tid + i * NT;
+        if (CN::total % NT == 0 || b < CN::total) {
+            int c, j;
+            LY::template bf<R>(b, c, j);
+            int k = j % Ns;
+            int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+            for (int m = 0; m < R; m++) sm[LY::idx(c, base + m * Ns)] = a[i * R + m];
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T, int L, int TC, int NT, bool ROWS, bool FWD, bool REV>
+struct ColFFT {
+    using P = Plan<L, REV>;
+    using LY = Lay<L, TC, ROWS>;
+    static constexpr int S = P::S;
+    static constexpr int R0 = P::R(0), RL = P::R(S - 1);
+    static constexpr int NB0 = Cnt<L, TC, NT, R0>::NB, NBL = Cnt<L, TC, NT, RL>::NB;
+    static constexpr int TOT0 = Cnt<L, TC, NT, R0>::total, TOTL = Cnt<L, TC, NT, RL>::total;
+    static constexpr int NIN = NB0 * R0, NOUT = NBL * RL;
+
+    // (c, position) of in[i*R0+m]; valid() false for idle slots
+    static H3D_D bool in_slot(int i, int m, int &c, int &p)
+    {
+        int b = threadIdx.x + i * NT;
+        int j;
+        LY::template bf<R0>(b, c, j);
+        p = j + m * (L / R0);
+        return TOT0 % NT == 0 || b < TOT0;
+    }
+    static H3D_D bool out_slot(int i, int m, int &c, int &p)
+    {
+        int b = threadIdx.x + i * NT;
+        int j;
+        LY::template bf<RL>(b, c, j);
+        p = j + m * (L / RL);
+        return TOTL % NT == 0 || b < TOTL;
+    }
+
+    static H3D_D void run(cx<T> (&in)[NIN], cx<T> *sm, cx<T> (&out)[NOUT], const cx<T> *__restrict__ tw)
+    {
+        const int tid = threadIdx.x;
+        // stage 0: no twiddles (Ns = 1)
+#pragma unroll
+        for (int i = 0; i < NB0; i++) {
+            int b = tid + i * NT;
+            if (TOT0 % NT == 0 || b < TOT0) {
+                int c, j;
+                LY::template bf<R0>(b, c, j);
+                dft<T, R0, FWD>(in + i * R0);
+#pragma unroll
+                for (int m = 0; m < R0; m++) sm[LY::idx(c, j * R0 + m)] = in[i * R0 + m];
+            }
+        }
+        __syncthreads();
+        if constexpr (S > 2) fft_mid_stage<T, L, TC, NT, ROWS, FWD, REV, 1>(sm, tw);
+        if constexpr (S > 3) fft_mid_stage<T, L, TC, NT, ROWS, FWD, REV, 2>(sm, tw);
+        // last stage: Ns*RL == L, outputs at j + m*L/RL
+        constexpr int NsL = P::Ns(S - 1), nbpc = L / RL;
+#pragma unroll
+        for (int i = 0; i < NBL; i++) {
+            int b = tid + i * NT;
+            if (TOTL % NT == 0 || b < TOTL) {
+                int c, j;
+                LY::template bf<RL>(b, c, j);
+                int k = j % NsL;
+#pragma unroll
+                for (int m = 0; m < RL; m++) {
+                    cx<T> v = sm[LY::idx(c, j + m * nbpc)];
+                    if (m > 0) v = cmul(v, twid<T, FWD>(tw, k * m * (L / (NsL * RL))));
+                    out[i * RL + m] = v;
+                }
+                dft<T, RL, FWD>(out + i * RL);
+            }
+        }
+    }
+};

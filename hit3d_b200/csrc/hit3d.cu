@@ -1,0 +1,919 @@
+// C-ABI of the B200 pseudospectral step (declared in include/hit3d_gpu.h):
+// device state, transform launchers dispatched on the grid size, the time step
+// pipeline, statistics, initial conditions and particles.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hit3d_gpu.h"
+#include "particles.cuh"
+#include "passes.cuh"
+#include "spectral.cuh"
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+int h3d_set_error(cudaError_t e, const char *what, const char *file, int line)
+{
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+    g_err = buf;
+    return -2;
+}
+int h3d_set_error_msg(int code, const char *msg)
+{
+    g_err = msg;
+    return code;
+}
+extern "C" const char *hit3d_gpu_last_error(void) { return g_err.c_str(); }
+
+#define H3D_LAUNCH_CHECK() H3D_CHECK(cudaGetLastError())
+#define H3D_TRY(x)            \
+    do {                      \
+        int rc__ = (x);       \
+        if (rc__ != 0) return rc__; \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// launch configurations per transform length
+// ---------------------------------------------------------------------------
+H3D_HD constexpr int plan_rmax(int L)
+{
+    int r = 0;
+    for (int s = 0; s < plan_stages(L); s++) r = plan_radix_fwd(L, s) > r ? plan_radix_fwd(L, s) : r;
+    return r;
+}
+template <typename T, int L> struct ColCfg {
+    static constexpr int TC = sizeof(T) == 8 ? 8 : 16;  // 128-byte rows of kx columns
+    static constexpr int NT0 = TC * L / plan_rmax(L);
+    static constexpr int NT = NT0 > 256 ? 256 : NT0;
+    static constexpr size_t SMEM = (size_t)Lay<L, TC, false>::elems * sizeof(cx<T>);
+};
+template <typename T, int L> struct RowCfg {
+    static constexpr int TC = L >= 1024 ? 1 : 1024 / L;  // row pairs per CTA
+    static constexpr int NT = 128;
+    static constexpr size_t SMEM = (size_t)Lay<L, TC, true>::elems * sizeof(cx<T>);
+};
+
+template <class K> static int set_smem(K kernel, size_t bytes)
+{
+    if (bytes > 48 * 1024) H3D_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return 0;
+}
+
+#define H3D_DISPATCH(n, CALL)                          \
+    switch (n) {                                       \
+    case 32: return CALL(32);                          \
+    case 48: return CALL(48);                          \
+    case 64: return CALL(64);                          \
+    case 128: return CALL(128);                        \
+    case 256: return CALL(256);                        \
+    case 512: return CALL(512);                        \
+    case 1024: return CALL(1024);                      \
+    default: return h3d_set_error_msg(-3, "unsupported grid size"); \
+    }
+
+static bool size_supported(int n)
+{
+    return n == 32 || n == 48 || n == 64 || n == 128 || n == 256 || n == 512 || n == 1024;
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct hit3d_ctx {
+    hit3d_params p;
+    int n, nh, P64, P32, nsc, dev, kmax, nsm;
+    int64_t fs64, fs32;
+    cudaStream_t st;
+    double2 *U, *RO, *RP, *SP;
+    void *W;             // work fields in the transform precision
+    int nw;
+    int64_t wfs;         // complex elements per work field
+    int wpitch;
+    double2 *W64;        // FP64 scratch (3 fields) for statistics and the transform API
+    double *phys;        // physical u,v,w [3][z][y][x] for particles
+    double2 *tw64;
+    float2 *tw32;
+    double *d_fen, *d_part, *d_red, *d_ratio;
+    unsigned long long *d_cmax;
+    double2 *stage;      // one field in the reference layout
+    double *d_xyz, *d_uvw;
+    int64_t np;
+    int pscheme;
+    int int_scalars;
+    double dx;
+    int pblocks;
+};
+
+static int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
+
+// ---------------------------------------------------------------------------
+// transform passes (templated on the compute precision T)
+// ---------------------------------------------------------------------------
+template <typename T> static const cx<T> *twid(const hit3d_ctx *c);
+template <> const double2 *twid<double>(const hit3d_ctx *c) { return c->tw64; }
+template <> const float2 *twid<float>(const hit3d_ctx *c) { return c->tw32; }
+
+// z pass reading the FP64 state with a spectral pre-operation, writing [z][ky][kx]
+template <typename T, int L>
+static int zinv_L(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src, int64_t src_fs, cx<T> *dst,
+                  int64_t dst_fs, int dpitch)
+{
+    using CF = ColCfg<T, L>;
+    IOSpec<T, T> io;
+    io.src = src; io.dst = dst; io.fs_src = src_fs; io.fs_dst = dst_fs;
+    io.n = c->n; io.psrc = c->P64; io.pdst = dpitch; io.ncol = c->nh; io.mode = mode; io.sfield = sfield;
+    io.dx = c->dx;
+    auto k = k_colfft<T, L, CF::TC, CF::NT, false, IOSpec<T, T>>;
+    H3D_TRY(set_smem(k, CF::SMEM));
+    dim3 g((c->nh + CF::TC - 1) / CF::TC, c->n, nf);
+    k<<<g, CF::NT, CF::SMEM, c->st>>>(io, twid<T>(c));
+    H3D_LAUNCH_CHECK();
+    return 0;
+}
+template <typename T>
+static int zinv(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src, int64_t src_fs, cx<T> *dst,
+                int64_t dst_fs, int dpitch)
+{
+#define CALL(L) zinv_L<T, L>(c, nf, mode, sfield, src, src_fs, dst, dst_fs, dpitch)
+    H3D_DISPATCH(c->n, CALL)
+#undef CALL
+}
+
+// in-place strided pass: axis 1 = y (stride pitch, outer z), axis 2 = z (stride n*pitch, outer ky)
+template <typename T, int L>
+static int spass_L(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, int pitch, int nf)
+{
+    using CF = ColCfg<T, L>;
+    IOPlain<T, T, T> io;
+    io.src = base; io.dst = base; io.fs_src = fs; io.fs_dst = fs; io.ncol = c->nh;
+    if (axis == 1) { io.sa_src = io.sa_dst = pitch; io.so_src = io.so_dst = (int64_t)c->n * pitch; }
+    else { io.sa_src = io.sa_dst = (int64_t)c->n * pitch; io.so_src = io.so_dst = pitch; }
+    dim3 g((c->nh + CF::TC - 1) / CF::TC, c->n, nf);
+    if (fwd) {
+        auto k = k_colfft<T, L, CF::TC, CF::NT, true, IOPlain<T, T, T>>;
+        H3D_TRY(set_smem(k, CF::SMEM));
+        k<<<g, CF::NT, CF::SMEM, c->st>>>(io, twid<T>(c));
+    } else {
+        auto k = k_colfft<T, L, CF::TC, CF::NT, false, IOPlain<T, T, T>>;
+        H3D_TRY(set_smem(k, CF::SMEM));
+        k<<<g, CF::NT, CF::SMEM, c->st>>>(io, twid<T>(c));
+    }
+    H3D_LAUNCH_CHECK();
+    return 0;
+}
+template <typename T> static int spass(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, int pitch, int nf)
+{
+#define CALL(L) spass_L<T, L>(c, axis, fwd, base, fs, pitch, nf)
+    H3D_DISPATCH(c->n, CALL)
+#undef CALL
+}
+
+template <typename T, int L> static int xc2r_L(hit3d_ctx *c, cx<T> *base, int64_t fs, int pitch, int nf)
+{
+    using RC = RowCfg<T, L>;
+    const int npairs = c->n * c->n / 2;
+    auto k = k_xc2r<T, L, RC::TC, RC::NT, T>;
+    H3D_TRY(set_smem(k, RC::SMEM));
+    const double n3 = (double)c->n * c->n * c->n;
+    k<<<dim3((npairs + RC::TC - 1) / RC::TC, 1, nf), RC::NT, RC::SMEM, c->st>>>(base, fs, pitch, npairs,
+                                                                                 (T)(1.0 / n3), twid<T>(c));
+    H3D_LAUNCH_CHECK();
+    return 0;
+}
+template <typename T> static int xc2r(hit3d_ctx *c, cx<T> *base, int64_t fs, int pitch, int nf)
+{
+#define CALL(L) xc2r_L<T, L>(c, base, fs, pitch, nf)
+    H3D_DISPATCH(c->n, CALL)
+#undef CALL
+}
+
+template <typename T, int L> static int xr2c_L(hit3d_ctx *c, cx<T> *base, int64_t fs, int pitch, int nf)
+{
+    using RC = RowCfg<T, L>;
+    const int npairs = c->n * c->n / 2;
+    auto k = k_xr2c<T, L, RC::TC, RC::NT, T>;
+    H3D_TRY(set_smem(k, RC::SMEM));
+    k<<<dim3((npairs + RC::TC - 1) / RC::TC, 1, nf), RC::NT, RC::SMEM, c->st>>>(base, fs, pitch, npairs, twid<T>(c));
+    H3D_LAUNCH_CHECK();
+    return 0;
+}
+template <typename T> static int xr2c(hit3d_ctx *c, cx<T> *base, int64_t fs, int pitch, int nf)
+{
+#define CALL(L) xr2c_L<T, L>(c, base, fs, pitch, nf)
+    H3D_DISPATCH(c->n, CALL)
+#undef CALL
+}
+
+template <typename T, template <class> class OP, int L> static int xfused_L(hit3d_ctx *c, FusedArgs a)
+{
+    using RC = RowCfg<T, L>;
+    auto k = k_xfused<T, L, RC::TC, RC::NT, T, OP<T>>;
+    H3D_TRY(set_smem(k, RC::SMEM));
+    k<<<dim3((a.npairs + RC::TC - 1) / RC::TC), RC::NT, RC::SMEM, c->st>>>(a, twid<T>(c));
+    H3D_LAUNCH_CHECK();
+    return 0;
+}
+template <typename T, template <class> class OP> static int xfused(hit3d_ctx *c, FusedArgs a)
+{
+    a.npairs = c->n * c->n / 2;
+    const double n3 = (double)c->n * c->n * c->n;
+    a.norm = 1.0 / n3;
+#define CALL(L) xfused_L<T, OP, L>(c, a)
+    H3D_DISPATCH(c->n, CALL)
+#undef CALL
+}
+
+static dim3 pw_grid(const hit3d_ctx *c) { return dim3(c->nsm * 4); }
+
+// full forward 3-D transform of nf FP64 scratch fields holding physical rows
+static int fwd3d64(hit3d_ctx *c, double2 *base, int nf)
+{
+    H3D_TRY(xr2c<double>(c, base, c->fs64, c->P64, nf));
+    H3D_TRY(spass<double>(c, 1, true, base, c->fs64, c->P64, nf));
+    H3D_TRY(spass<double>(c, 2, true, base, c->fs64, c->P64, nf));
+    return 0;
+}
+// full inverse of nf spectral FP64 fields in place
+static int inv3d64(hit3d_ctx *c, double2 *base, int nf)
+{
+    H3D_TRY(spass<double>(c, 2, false, base, c->fs64, c->P64, nf));
+    H3D_TRY(spass<double>(c, 1, false, base, c->fs64, c->P64, nf));
+    H3D_TRY(xc2r<double>(c, base, c->fs64, c->P64, nf));
+    return 0;
+}
+// inverse from the state with a pre-operation into W64[0..nf)
+static int inv_from_state(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src)
+{
+    H3D_TRY(zinv<double>(c, nf, mode, sfield, src, c->fs64, c->W64, c->fs64, c->P64));
+    H3D_TRY(spass<double>(c, 1, false, c->W64, c->fs64, c->P64, nf));
+    H3D_TRY(xc2r<double>(c, c->W64, c->fs64, c->P64, nf));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// one time step
+// ---------------------------------------------------------------------------
+template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_s)
+{
+    const hit3d_params &p = c->p;
+    cx<T> *W = reinterpret_cast<cx<T> *>(c->W);
+    const int64_t wfs = c->wfs;
+    const int wp = c->wpitch;
+    auto Wf = [&](int i) { return W + i * wfs; };
+    const int ns = c->int_scalars ? c->nsc : 0;
+    const int nprod = 6 + 3 * ns;
+    const bool les = p.les_model == 1;
+
+    StepArgs a;
+    memset(&a, 0, sizeof a);
+    a.n = c->n; a.nh = c->nh; a.pitch = c->P64; a.ppitch = wp; a.fs = c->fs64; a.pfs = wfs;
+    a.nu = p.nu; a.dt = p.dt; a.euler_v = euler_v; a.euler_s = euler_s;
+    a.flow_type = p.flow_type; a.kfmax = p.kfmax; a.famp = p.famp; a.fenergy = c->d_fen; a.nscal = ns;
+    for (int s = 0; s < c->nsc; s++) { a.pe[s] = p.nu / p.sc[s]; a.stype[s] = p.scalar_type[s]; }
+
+    if (p.flow_type == 1) {
+        k_forcing_energy<<<1, 32, 0, c->st>>>(c->n, c->P64, c->fs64, p.kfmax, c->U, c->d_fen);
+        H3D_LAUNCH_CHECK();
+    }
+    const int npass = p.dealias == 1 ? 2 : 1;
+    for (int pass = 0; pass < npass; pass++) {
+        const int mode = pass == 0 ? PRE_COPY : PRE_SHIFT;
+        H3D_TRY(zinv<T>(c, 3, mode, 0, c->U, c->fs64, Wf(0), wfs, wp));
+        for (int s = 0; s < ns; s++)
+            H3D_TRY(zinv<T>(c, 1, mode, 0, c->U + (3 + s) * c->fs64, c->fs64, Wf(6 + 3 * s), wfs, wp));
+        H3D_TRY(spass<T>(c, 1, false, Wf(0), wfs, wp, 3));
+        for (int s = 0; s < ns; s++) H3D_TRY(spass<T>(c, 1, false, Wf(6 + 3 * s), wfs, wp, 1));
+        if (pass == 0) H3D_CHECK(cudaMemsetAsync(c->d_cmax, 0, sizeof(unsigned long long), c->st));
+        for (int s = 0; s < ns; s++) {
+            FusedArgs fa;
+            memset(&fa, 0, sizeof fa);
+            fa.in[0] = Wf(0); fa.in[1] = Wf(1); fa.in[2] = Wf(2); fa.in[3] = Wf(6 + 3 * s);
+            fa.out[0] = Wf(6 + 3 * s); fa.out[1] = Wf(7 + 3 * s); fa.out[2] = Wf(8 + 3 * s);
+            fa.pitch = wp;
+            H3D_TRY((xfused<T, OpScal>(c, fa)));
+        }
+        {
+            FusedArgs fa;
+            memset(&fa, 0, sizeof fa);
+            for (int f = 0; f < 3; f++) fa.in[f] = Wf(f);
+            for (int o = 0; o < 6; o++) fa.out[o] = Wf(o);
+            fa.pitch = wp;
+            if (pass == 0) fa.cmax = c->d_cmax;
+            if (pass == 0 && c->np > 0) {
+                fa.phys = c->phys;
+                fa.phys_fs = (int64_t)c->n * c->n * c->n;
+                fa.phys_pitch = c->n;
+            }
+            H3D_TRY((xfused<T, OpVel>(c, fa)));
+        }
+        if (pass == 0 && c->np > 0) {
+            PartArgs pa;
+            pa.n = c->n; pa.scheme = c->pscheme; pa.np = c->np; pa.dt = p.dt; pa.dx = c->dx;
+            pa.U = c->phys; pa.fs = (int64_t)c->n * c->n * c->n; pa.xyz = c->d_xyz; pa.uvw = c->d_uvw;
+            k_particles<<<(unsigned)((c->np + 255) / 256), 256, 0, c->st>>>(pa);
+            H3D_LAUNCH_CHECK();
+        }
+        H3D_TRY(spass<T>(c, 1, true, Wf(0), wfs, wp, nprod));
+        H3D_TRY(spass<T>(c, 2, true, Wf(0), wfs, wp, nprod));
+
+        const cx<T> *tau = nullptr;
+        if (les) {
+            // Smagorinsky stress from the same state (m_les.f90:1142-1215, 902-1018)
+            const int t0 = nprod;
+            H3D_TRY(zinv<T>(c, 3, PRE_STRAIN_A, 0, c->U, c->fs64, Wf(t0), wfs, wp));
+            H3D_TRY(zinv<T>(c, 3, PRE_STRAIN_B, 0, c->U, c->fs64, Wf(t0 + 3), wfs, wp));
+            H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, 6));
+            FusedArgs fa;
+            memset(&fa, 0, sizeof fa);
+            for (int f = 0; f < 6; f++) { fa.in[f] = Wf(t0 + f); fa.out[f] = Wf(t0 + f); }
+            fa.pitch = wp;
+            double cd = p.c_smag * c->dx;
+            fa.p0 = cd * cd;
+            H3D_TRY((xfused<T, OpSmag>(c, fa)));
+            H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, 6));
+            H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, 6));
+            tau = Wf(t0);
+        }
+
+        if (p.dealias == 0) {
+            for (int s = 0; s < ns; s++) {
+                k_scalar<T><<<pw_grid(c), 256, 0, c->st>>>(a, 0, s, c->dx, Wf(6 + 3 * s), nullptr, c->U,
+                                                            c->U + (3 + s) * c->fs64, c->RO + (3 + s) * c->fs64);
+                H3D_LAUNCH_CHECK();
+            }
+            k_update_vel_23<T><<<pw_grid(c), 256, 0, c->st>>>(a, Wf(0), tau, c->U, c->RO);
+            H3D_LAUNCH_CHECK();
+        } else if (pass == 0) {
+            for (int s = 0; s < ns; s++) {
+                k_scalar<T><<<pw_grid(c), 256, 0, c->st>>>(a, 1, s, c->dx, Wf(6 + 3 * s), c->SP + s * c->fs64, c->U,
+                                                            c->U + (3 + s) * c->fs64, c->RO + (3 + s) * c->fs64);
+                H3D_LAUNCH_CHECK();
+            }
+            k_rhs_vel_ps1<T><<<pw_grid(c), 256, 0, c->st>>>(a, Wf(0), c->U, c->RP);
+            H3D_LAUNCH_CHECK();
+        } else {
+            for (int s = 0; s < ns; s++) {
+                k_scalar<T><<<pw_grid(c), 256, 0, c->st>>>(a, 2, s, c->dx, Wf(6 + 3 * s), c->SP + s * c->fs64, c->U,
+                                                            c->U + (3 + s) * c->fs64, c->RO + (3 + s) * c->fs64);
+                H3D_LAUNCH_CHECK();
+            }
+            k_update_vel_ps2<T><<<pw_grid(c), 256, 0, c->st>>>(a, c->dx, Wf(0), c->RP, c->U, c->RO);
+            H3D_LAUNCH_CHECK();
+        }
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// RANDu on the host (RANDu.f:12-52), bit-exact with the reference: the
+// initial-condition stream stays on the host as the reference generates it.
+// ---------------------------------------------------------------------------
+namespace {
+struct Randu {
+    int64_t idum2 = 123456789, iy = 0, iv[32] = {0};
+    double next(double idum3)
+    {
+        const int64_t im1 = 2147483563, im2 = 2147483399, imm1 = im1 - 1;
+        const int64_t ia1 = 40014, ia2 = 40692, iq1 = 53668, iq2 = 52774;
+        const int64_t ir1 = 12211, ir2 = 3791, ntab = 32, ndiv = 1 + imm1 / ntab;
+        const double am = 1.0 / (double)im1, eps = 1.2e-7, rnmx = 1.0 - eps;
+        int64_t idum = (int64_t)llround(idum3 / 987.0), k, j;
+        if (idum <= 0) {
+            idum = (-idum > 1) ? -idum : 1;
+            idum2 = idum;
+            for (j = ntab + 8; j >= 1; j--) {
+                k = idum / iq1;
+                idum = ia1 * (idum - k * iq1) - k * ir1;
+                if (idum < 0) idum += im1;
+                if (j <= ntab) iv[j - 1] = idum;
+            }
+        }
+        k = idum / iq1;
+        idum = ia1 * (idum - k * iq1) - k * ir1;
+        if (idum < 0) idum += im1;
+        k = idum2 / iq2;
+        idum2 = ia2 * (idum2 - k * iq2) - k * ir2;
+        if (idum2 < 0) idum2 += im2;
+        j = 1 + iy / ndiv;
+        iy = iv[j - 1] - idum2;
+        iv[j - 1] = idum;
+        if (iy < 1) iy += imm1;
+        double r = am * (double)iy;
+        return r < rnmx ? r : rnmx;
+    }
+};
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+static int ctx_alloc(void **p, size_t bytes)
+{
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return h3d_set_error(e, "cudaMalloc", __FILE__, __LINE__);
+    return 0;
+}
+
+extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
+{
+    if (!p || !out) return h3d_set_error_msg(-1, "hit3d_gpu_init: null argument");
+    *out = nullptr;
+    if (!size_supported(p->nx)) return h3d_set_error_msg(-3, "hit3d_gpu_init: grid size must be 32, 48, 64, 128, 256, 512 or 1024");
+    if (p->n_scalars < 0 || p->n_scalars > HIT3D_MAX_SCALARS) return h3d_set_error_msg(-1, "hit3d_gpu_init: bad n_scalars");
+    if (p->dealias != 0 && p->dealias != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: wrong dealias flag");
+    if (p->flow_type == 1 && p->force_type != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: WRONG FORCE TYPE");
+    if (p->flow_type == 1 && (p->kfmax < 1 || p->kfmax > 15)) return h3d_set_error_msg(-1, "hit3d_gpu_init: kfmax must be in 1..15");
+    if (p->les_model != 0 && p->les_model != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: only les_model 0 and 1 are supported");
+    if (p->les_model == 1 && p->n_scalars > 0) return h3d_set_error_msg(-1, "hit3d_gpu_init: LES with scalars is not supported");
+    if (p->precision != 0 && p->precision != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: precision must be 0 or 1");
+    for (int s = 0; s < p->n_scalars; s++) {
+        if (p->scalar_type[s] >= 100) return h3d_set_error_msg(-1, "hit3d_gpu_init: reacting scalars are not supported");
+        if (!(p->sc[s] > 0.0)) return h3d_set_error_msg(-1, "hit3d_gpu_init: Schmidt numbers must be > 0");
+    }
+    H3D_CHECK(cudaSetDevice(p->device));
+    hit3d_ctx *c = new hit3d_ctx();
+    memset(c, 0, sizeof *c);
+    c->p = *p;
+    if (c->p.dealias == 1 && c->p.les_model) c->p.dealias = 0;  // LES forces the 2/3 rule (m_parameters.f90:416-420)
+    c->dev = p->device;
+    c->n = p->nx;
+    c->nh = c->n / 2 + 1;
+    c->P64 = (int)round_up(c->nh, 8);
+    c->P32 = (int)round_up(c->nh, 16);
+    c->fs64 = (int64_t)c->n * c->n * c->P64;
+    c->fs32 = (int64_t)c->n * c->n * c->P32;
+    c->nsc = p->n_scalars;
+    c->kmax = c->p.dealias == 0 ? c->n / 3 : (int)floor((double)c->n / 3.0 * sqrt(2.0));
+    c->dx = 2.0 * (4.0 * atan(1.0)) / (double)c->n;
+    c->int_scalars = c->nsc > 0;
+    cudaDeviceProp prop;
+    H3D_CHECK(cudaGetDeviceProperties(&prop, c->dev));
+    c->nsm = prop.multiProcessorCount;
+    H3D_CHECK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    int rc = 0;
+    const int nf = 3 + c->nsc;
+    const size_t f64 = (size_t)c->fs64 * sizeof(double2);
+    c->nw = 6 + 3 * c->nsc + (c->p.les_model ? 6 : 0);
+    if (c->p.precision == 0) {
+        c->wpitch = c->P64;
+        c->wfs = c->fs64;
+    } else {
+        c->wpitch = c->P32;
+        c->wfs = c->fs32;
+    }
+    const size_t wbytes = (size_t)c->nw * c->wfs * (c->p.precision == 0 ? sizeof(double2) : sizeof(float2));
+    if ((rc = ctx_alloc((void **)&c->U, f64 * nf)) || (rc = ctx_alloc((void **)&c->RO, f64 * nf)) ||
+        (rc = ctx_alloc(&c->W, wbytes))) {
+        hit3d_gpu_finalize(c);
+        return rc;
+    }
+    if (c->p.dealias == 1) {
+        if ((rc = ctx_alloc((void **)&c->RP, f64 * 3)) || (c->nsc && (rc = ctx_alloc((void **)&c->SP, f64 * c->nsc)))) {
+            hit3d_gpu_finalize(c);
+            return rc;
+        }
+    }
+    if (c->p.precision == 0) c->W64 = reinterpret_cast<double2 *>(c->W);
+    else if ((rc = ctx_alloc((void **)&c->W64, f64 * 3))) { hit3d_gpu_finalize(c); return rc; }
+    c->pblocks = c->nsm * 2;
+    const int kpart = c->kmax > 4 ? c->kmax : 4;
+    if ((rc = ctx_alloc((void **)&c->tw64, sizeof(double2) * c->n)) || (rc = ctx_alloc((void **)&c->tw32, sizeof(float2) * c->n)) ||
+        (rc = ctx_alloc((void **)&c->d_fen, sizeof(double))) || (rc = ctx_alloc((void **)&c->d_cmax, sizeof(unsigned long long))) ||
+        (rc = ctx_alloc((void **)&c->d_part, sizeof(double) * (size_t)c->pblocks * kpart)) ||
+        (rc = ctx_alloc((void **)&c->d_red, sizeof(double) * (size_t)(kpart + 8))) ||
+        (rc = ctx_alloc((void **)&c->d_ratio, sizeof(double) * (size_t)kpart)) ||
+        (rc = ctx_alloc((void **)&c->stage, sizeof(double2) * (size_t)c->n * c->n * c->nh))) {
+        hit3d_gpu_finalize(c);
+        return rc;
+    }
+    // twiddles exp(-2 pi i t/N), computed in long double and rounded once
+    std::vector<double2> t64(c->n);
+    std::vector<float2> t32(c->n);
+    const long double twopi = 6.283185307179586476925286766559005768L;
+    for (int t = 0; t < c->n; t++) {
+        long double ang = twopi * (long double)t / (long double)c->n;
+        t64[t] = make_double2((double)cosl(ang), (double)(-sinl(ang)));
+        t32[t] = make_float2((float)cosl(ang), (float)(-sinl(ang)));
+    }
+    H3D_CHECK(cudaMemcpy(c->tw64, t64.data(), sizeof(double2) * c->n, cudaMemcpyHostToDevice));
+    H3D_CHECK(cudaMemcpy(c->tw32, t32.data(), sizeof(float2) * c->n, cudaMemcpyHostToDevice));
+    H3D_CHECK(cudaMemset(c->U, 0, f64 * nf));
+    H3D_CHECK(cudaMemset(c->RO, 0, f64 * nf));
+    H3D_CHECK(cudaMemset(c->W, 0, wbytes));
+    *out = c;
+    return 0;
+}
+
+extern "C" void hit3d_gpu_finalize(hit3d_ctx *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->dev);
+    if (c->st) cudaStreamSynchronize(c->st);
+    if (c->W64 && c->W64 != c->W) cudaFree(c->W64);
+    void *ptrs[] = {c->U, c->RO, c->RP, c->SP, c->W, c->phys, c->tw64, c->tw32, c->d_fen, c->d_part,
+                    c->d_red, c->d_ratio, c->d_cmax, c->stage, c->d_xyz, c->d_uvw};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+}
+
+static int transfer_fields(hit3d_ctx *c, double2 *dev, const double *hsrc, double *hdst, int64_t ld1, int nf)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    if (ld1 < c->n + 2) return h3d_set_error_msg(-1, "ld1 must be >= nx+2");
+    if (nf < 1 || nf > 3 + c->nsc) return h3d_set_error_msg(-1, "nfields out of range");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    const size_t width = (size_t)c->nh * sizeof(double2);
+    const size_t hp = (size_t)ld1 * sizeof(double);
+    const size_t rows = (size_t)c->n * c->n;
+    for (int f = 0; f < nf; f++) {
+        double2 *d = dev + f * c->fs64;
+        if (hsrc) {
+            const double *h = hsrc + (size_t)f * ld1 * rows;
+            H3D_CHECK(cudaMemcpy2DAsync(c->stage, width, h, hp, width, rows, cudaMemcpyHostToDevice, c->st));
+            k_ref_to_dev<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->stage, d);
+            H3D_LAUNCH_CHECK();
+        } else {
+            double *h = hdst + (size_t)f * ld1 * rows;
+            k_dev_to_ref<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, d, c->stage);
+            H3D_LAUNCH_CHECK();
+            H3D_CHECK(cudaMemcpy2DAsync(h, hp, c->stage, width, width, rows, cudaMemcpyDeviceToHost, c->st));
+        }
+    }
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+extern "C" int hit3d_gpu_upload_fields(hit3d_ctx *c, const double *fields, int64_t ld1, int32_t nf)
+{
+    if (!fields) return h3d_set_error_msg(-1, "null fields");
+    return transfer_fields(c, c ? c->U : nullptr, fields, nullptr, ld1, nf);
+}
+extern "C" int hit3d_gpu_download_fields(hit3d_ctx *c, double *fields, int64_t ld1, int32_t nf)
+{
+    if (!fields) return h3d_set_error_msg(-1, "null fields");
+    return transfer_fields(c, c ? c->U : nullptr, nullptr, fields, ld1, nf);
+}
+extern "C" int hit3d_gpu_upload_rhs_old(hit3d_ctx *c, const double *r, int64_t ld1, int32_t nf)
+{
+    if (!r) return h3d_set_error_msg(-1, "null rhs_old");
+    return transfer_fields(c, c ? c->RO : nullptr, r, nullptr, ld1, nf);
+}
+extern "C" int hit3d_gpu_download_rhs_old(hit3d_ctx *c, double *r, int64_t ld1, int32_t nf)
+{
+    if (!r) return h3d_set_error_msg(-1, "null rhs_old");
+    return transfer_fields(c, c ? c->RO : nullptr, nullptr, r, ld1, nf);
+}
+
+extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_t *fos, double *courant)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    if (nsteps < 0) return h3d_set_error_msg(-1, "nsteps < 0");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    int ev = fov ? (*fov != 0) : 0, es = fos ? (*fos != 0) : 0;
+    for (int it = 0; it < nsteps; it++) {
+        int rc = c->p.precision == 0 ? step_once<double>(c, ev, es) : step_once<float>(c, ev, es);
+        if (rc) return rc;
+        ev = 0;
+        if (c->int_scalars) es = 0;
+    }
+    if (fov) *fov = ev;
+    if (fos) *fos = es;
+    if (courant && nsteps > 0) {
+        unsigned long long bits = 0;
+        H3D_CHECK(cudaMemcpyAsync(&bits, c->d_cmax, sizeof bits, cudaMemcpyDeviceToHost, c->st));
+        H3D_CHECK(cudaStreamSynchronize(c->st));
+        double cm;
+        memcpy(&cm, &bits, sizeof cm);
+        *courant = cm * c->p.dt / c->dx;
+    }
+    H3D_CHECK(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int hit3d_gpu_set_dt(hit3d_ctx *c, double dt)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    if (!(dt > 0.0)) return h3d_set_error_msg(-1, "dt must be > 0");
+    c->p.dt = dt;
+    return 0;
+}
+
+extern "C" int hit3d_gpu_set_scalars_active(hit3d_ctx *c, int32_t on)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    c->int_scalars = (on != 0) && c->nsc > 0;
+    return 0;
+}
+
+extern "C" int hit3d_gpu_dealias_all(hit3d_ctx *c)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    k_dealias_all<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->fs64, 3 + c->nsc, c->kmax, c->U);
+    H3D_LAUNCH_CHECK();
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+// shell spectrum of nf state fields starting at src -> host es[0..kmax)
+static int shell_spectrum(hit3d_ctx *c, const double2 *src, int nf, double *es)
+{
+    const int kmax = c->kmax;
+    const int nw = 8;
+    k_shell_partial<<<c->pblocks, nw * 32, sizeof(double) * nw * kmax, c->st>>>(c->n, c->nh, c->P64, c->fs64, nf, kmax,
+                                                                               src, c->d_part);
+    H3D_LAUNCH_CHECK();
+    k_shell_final<<<(kmax + 127) / 128, 128, 0, c->st>>>(c->pblocks, kmax, c->d_part, c->d_red);
+    H3D_LAUNCH_CHECK();
+    H3D_CHECK(cudaMemcpyAsync(es, c->d_red, sizeof(double) * kmax, cudaMemcpyDeviceToHost, c->st));
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+// deterministic sums over physical points of W64 fields: returns 4 values
+static int phys_sums(hit3d_ctx *c, const double2 *base, int nf, int mode, double *out4)
+{
+    k_phys_partial<<<c->pblocks, 256, 0, c->st>>>(c->n, 2 * (int64_t)c->P64, 2 * c->fs64, nf, mode,
+                                                  reinterpret_cast<const double *>(base), c->d_part);
+    H3D_LAUNCH_CHECK();
+    k_phys_final<<<1, 1, 0, c->st>>>(c->pblocks, c->d_part, c->d_red);
+    H3D_LAUNCH_CHECK();
+    H3D_CHECK(cudaMemcpyAsync(out4, c->d_red, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+extern "C" int hit3d_gpu_stats(hit3d_ctx *c, double *e_spec, int32_t kmax, double *o)
+{
+    if (!c || !e_spec || !o) return h3d_set_error_msg(-1, "hit3d_gpu_stats: null argument");
+    if (kmax != c->kmax) return h3d_set_error_msg(-1, "hit3d_gpu_stats: kmax does not match the run");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    const int n = c->n;
+    const double fac = 1.0 / ((double)n * n * n);
+    double s4[4];
+    // enstrophy (m_stats.f90:241-289)
+    H3D_TRY(inv_from_state(c, 3, PRE_CURL, 0, c->U));
+    H3D_TRY(phys_sums(c, c->W64, 3, 0, s4));
+    const double ens = s4[0] * fac;
+    // skewness of the longitudinal derivatives
+    H3D_TRY(inv_from_state(c, 3, PRE_DLONG, 0, c->U));
+    double skew = 0.0;
+    for (int f = 0; f < 3; f++) {
+        H3D_TRY(phys_sums(c, c->W64 + f * c->fs64, 1, 1, s4));
+        double m2 = s4[0] * fac, m3 = s4[1] * fac;
+        skew += m3 / pow(m2, 1.5);
+    }
+    skew /= 3.0;
+    // spectrum and derived quantities (m_stats.f90:99-189), host arithmetic in the reference's order
+    H3D_TRY(shell_spectrum(c, c->U, 3, e_spec));
+    const double nu = c->p.nu, PI = 4.0 * atan(1.0);
+    double energy = 0.0;
+    for (int k = 0; k < kmax; k++) energy = energy + e_spec[k];
+    double eps = 0.0;
+    for (int k = 1; k <= kmax; k++) eps = eps + e_spec[k - 1] * (double)(k * k) * 2.0 * nu;
+    double eta = pow(nu * nu * nu / eps, 0.25);
+    double uvar = 2.0 / 3.0 * energy;
+    double sct = 0.0;
+    for (int k = 1; k <= kmax; k++) sct = sct + e_spec[k - 1] / (double)k;
+    double xl = PI / 2.0 * sct / uvar;
+    double lam = sqrt(15.0 * uvar * nu / eps);
+    o[0] = energy; o[1] = eps; o[2] = eta; o[3] = eta * (double)kmax; o[4] = uvar; o[5] = xl; o[6] = lam;
+    o[7] = uvar * sqrt(15.0 / eps * (1.0 / nu));
+    o[8] = sqrt(uvar) * lam / nu;
+    o[9] = xl / sqrt(uvar);
+    o[10] = ens;
+    o[11] = skew;
+    return 0;
+}
+
+extern "C" int hit3d_gpu_scalar_stats(hit3d_ctx *c, int32_t s, double *spec, int32_t kmax, double *o)
+{
+    if (!c || !spec || !o) return h3d_set_error_msg(-1, "hit3d_gpu_scalar_stats: null argument");
+    if (s < 0 || s >= c->nsc) return h3d_set_error_msg(-1, "hit3d_gpu_scalar_stats: no such scalar");
+    if (kmax != c->kmax) return h3d_set_error_msg(-1, "hit3d_gpu_scalar_stats: kmax does not match the run");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    const int n = c->n;
+    const double fac = 1.0 / ((double)n * n * n);
+    const double2 *phi = c->U + (3 + s) * c->fs64;
+    H3D_TRY(shell_spectrum(c, phi, 1, spec));
+    for (int k = 0; k < kmax; k++) spec[k] = 2.0 * spec[k];
+    double s4[4];
+    H3D_TRY(inv_from_state(c, 3, PRE_GRAD, 3 + s, c->U));
+    H3D_TRY(phys_sums(c, c->W64, 3, 0, s4));
+    o[0] = 2.0 * (c->p.nu / c->p.sc[s]) * s4[0] * fac;
+    H3D_TRY(inv_from_state(c, 1, PRE_COPY, 0, phi));
+    H3D_TRY(phys_sums(c, c->W64, 1, 2, s4));
+    double m1 = s4[0] * fac, m2 = s4[1] * fac;
+    o[1] = m1; o[2] = m2 - m1 * m1; o[3] = s4[2]; o[4] = s4[3];
+    return 0;
+}
+
+// upload nf host physical arrays (ld1, ny, nz) into W64 rows
+static int upload_phys(hit3d_ctx *c, const double *h, int64_t ld1, int nf)
+{
+    const size_t rows = (size_t)c->n * c->n;
+    for (int f = 0; f < nf; f++)
+        H3D_CHECK(cudaMemcpy2DAsync(reinterpret_cast<double *>(c->W64 + f * c->fs64), 2 * c->P64 * sizeof(double),
+                                    h + (size_t)f * ld1 * rows, ld1 * sizeof(double), c->n * sizeof(double), rows,
+                                    cudaMemcpyHostToDevice, c->st));
+    return 0;
+}
+
+extern "C" int hit3d_gpu_init_velocity(hit3d_ctx *c, double rn1, int32_t isp, double peak, double ir_exp)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    if (!(isp == -1 || isp == 0 || isp == 1 || isp == 2 || isp == 3))
+        return h3d_set_error_msg(-1, "ERROR: WRONG INITIAL SPECTRUM TYPE");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    const int n = c->n, kmax = c->kmax;
+    const size_t ld = (size_t)n + 2, fsz = ld * n * n;
+    const double PI = 4.0 * atan(1.0), TWO_PI = 2.0 * PI;
+    std::vector<double> g(3 * fsz);
+    if (isp == -1) {
+        // Taylor-Green (init_velocity.f90:252-293)
+        const double dx = 2.0 * PI / (double)n;
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n; i++) {
+                    double xx = (double)i * dx, yy = (double)j * dx, zz = (double)k * dx;
+                    size_t q = i + ld * (j + (size_t)n * k);
+                    g[q] = sin(xx) * cos(yy) * cos(zz);
+                    g[fsz + q] = -cos(xx) * sin(yy) * cos(zz);
+                    g[2 * fsz + q] = 0.0;
+                }
+        H3D_TRY(upload_phys(c, g.data(), (int64_t)ld, 3));
+        H3D_TRY(fwd3d64(c, c->W64, 3));
+        H3D_CHECK(cudaMemcpyAsync(c->U, c->W64, sizeof(double2) * 3 * c->fs64, cudaMemcpyDeviceToDevice, c->st));
+        H3D_CHECK(cudaStreamSynchronize(c->st));
+        return 0;
+    }
+    // RANDu over six full padded arrays in the reference's order, then Box-Muller
+    // (init_velocity.f90:67-113)
+    Randu r;
+    (void)r.next(-rn1);
+    for (size_t q = 0; q < 3 * fsz; q++) g[q] = r.next(rn1);
+    for (int f = 0; f < 3; f++)
+        for (size_t q = 0; q < fsz; q++) {
+            double u2 = r.next(rn1);
+            double &u1 = g[f * fsz + q];
+            u1 = sqrt(-2.0 * log(u1)) * sin(TWO_PI * u2);
+        }
+    H3D_TRY(upload_phys(c, g.data(), (int64_t)ld, 3));
+    H3D_TRY(fwd3d64(c, c->W64, 3));
+    k_init_curl<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, c->fs64, kmax, c->W64, c->U);
+    H3D_LAUNCH_CHECK();
+    std::vector<double> es(kmax), et(kmax), ratio(kmax);
+    H3D_TRY(shell_spectrum(c, c->U, 3, es.data()));
+    for (int k = 1; k <= kmax; k++) {
+        double wmag = (double)k, ratio_k = wmag / peak;
+        if (isp == 0) et[k - 1] = pow(wmag, -5.0 / 3.0);
+        else if (isp == 1) et[k - 1] = ratio_k * ratio_k * ratio_k / peak * exp(-3.0 * ratio_k);
+        else if (isp == 2) et[k - 1] = pow(wmag, ir_exp) * exp(-2.0 * ratio_k * ratio_k);
+        else {
+            double f = 2.0 * PI * ratio_k, f2 = f * f, d = 1.0 + f2;
+            et[k - 1] = (f2 * f2) / (d * d * d);
+        }
+    }
+    double tot = 0.0;
+    for (int k = 0; k < kmax; k++) tot = tot + et[k];
+    for (int k = 0; k < kmax; k++) {
+        et[k] = et[k] / tot;
+        ratio[k] = es[k] > 0.0 ? sqrt(et[k] / es[k]) : -1.0;
+    }
+    H3D_CHECK(cudaMemcpyAsync(c->d_ratio, ratio.data(), sizeof(double) * kmax, cudaMemcpyHostToDevice, c->st));
+    k_shell_scale<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, c->fs64, 3, kmax, c->d_ratio, c->U);
+    H3D_LAUNCH_CHECK();
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+extern "C" int hit3d_gpu_particles_upload(hit3d_ctx *c, const double *xyzp, const double *uvwp, int64_t np, int32_t scheme)
+{
+    if (!c || (np > 0 && !xyzp)) return h3d_set_error_msg(-1, "hit3d_gpu_particles_upload: null argument");
+    if (scheme != 0 && scheme != 1) return h3d_set_error_msg(-1, "particles_tracking_scheme must be 0 or 1");
+    if (np < 0) return h3d_set_error_msg(-1, "np < 0");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    if (c->d_xyz) { cudaFree(c->d_xyz); c->d_xyz = nullptr; }
+    if (c->d_uvw) { cudaFree(c->d_uvw); c->d_uvw = nullptr; }
+    c->np = 0;
+    if (np == 0) return 0;
+    int rc;
+    if ((rc = ctx_alloc((void **)&c->d_xyz, sizeof(double) * 3 * np)) || (rc = ctx_alloc((void **)&c->d_uvw, sizeof(double) * 3 * np)))
+        return rc;
+    if (!c->phys && (rc = ctx_alloc((void **)&c->phys, sizeof(double) * 3 * (size_t)c->n * c->n * c->n))) return rc;
+    H3D_CHECK(cudaMemcpy(c->d_xyz, xyzp, sizeof(double) * 3 * np, cudaMemcpyHostToDevice));
+    if (uvwp) H3D_CHECK(cudaMemcpy(c->d_uvw, uvwp, sizeof(double) * 3 * np, cudaMemcpyHostToDevice));
+    else {
+        std::vector<double> m(3 * np, -999.0);
+        H3D_CHECK(cudaMemcpy(c->d_uvw, m.data(), sizeof(double) * 3 * np, cudaMemcpyHostToDevice));
+    }
+    c->np = np;
+    c->pscheme = scheme;
+    return 0;
+}
+
+extern "C" int hit3d_gpu_particles_download(hit3d_ctx *c, double *xyzp, double *uvwp)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    if (c->np == 0) return 0;
+    if (xyzp) H3D_CHECK(cudaMemcpy(xyzp, c->d_xyz, sizeof(double) * 3 * c->np, cudaMemcpyDeviceToHost));
+    if (uvwp) H3D_CHECK(cudaMemcpy(uvwp, c->d_uvw, sizeof(double) * 3 * c->np, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+extern "C" int hit3d_gpu_xfft3d(hit3d_ctx *c, int32_t flag, const double *in, double *out, int64_t ld1)
+{
+    if (!c || !in || !out) return h3d_set_error_msg(-1, "hit3d_gpu_xfft3d: null argument");
+    if (flag != 1 && flag != -1) return h3d_set_error_msg(-1, "hit3d_gpu_xfft3d: flag must be 1 or -1");
+    if (ld1 < c->n + 2) return h3d_set_error_msg(-1, "ld1 must be >= nx+2");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    const size_t rows = (size_t)c->n * c->n;
+    const size_t width = (size_t)c->nh * sizeof(double2);
+    if (flag == 1) {
+        H3D_TRY(upload_phys(c, in, ld1, 1));
+        H3D_TRY(fwd3d64(c, c->W64, 1));
+        k_dev_to_ref<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->W64, c->stage);
+        H3D_LAUNCH_CHECK();
+        H3D_CHECK(cudaMemcpy2DAsync(out, ld1 * sizeof(double), c->stage, width, width, rows, cudaMemcpyDeviceToHost, c->st));
+    } else {
+        H3D_CHECK(cudaMemcpy2DAsync(c->stage, width, in, ld1 * sizeof(double), width, rows, cudaMemcpyHostToDevice, c->st));
+        k_ref_to_dev<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->stage, c->W64);
+        H3D_LAUNCH_CHECK();
+        H3D_TRY(inv3d64(c, c->W64, 1));
+        H3D_CHECK(cudaMemcpy2DAsync(out, ld1 * sizeof(double), reinterpret_cast<double *>(c->W64), 2 * c->P64 * sizeof(double),
+                                    c->n * sizeof(double), rows, cudaMemcpyDeviceToHost, c->st));
+    }
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+extern "C" int hit3d_gpu_filter_field(hit3d_ctx *c, int32_t kind, double delta, int32_t field)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    if (field < 0 || field >= 3 + c->nsc) return h3d_set_error_msg(-1, "hit3d_gpu_filter_field: no such field");
+    if (kind != 2 && kind != 4) return h3d_set_error_msg(-1, "hit3d_gpu_filter_field: kind must be 2 (Gaussian) or 4 (box)");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    const int n = c->n;
+    double2 *G = c->W64;
+    if (kind == 2) {
+        // Gaussian kernel in physical space, then its transform (m_filter_xfftw.f90:197-220, 259-271)
+        if (delta < 3.0 * c->dx) return h3d_set_error_msg(-1, "filter_xfftw_init: delta is too small");
+        const size_t ld = (size_t)n + 2;
+        std::vector<double> g(ld * n * n, 0.0);
+        const double PI = 4.0 * atan(1.0);
+        const double c1 = 6.0 / (delta * delta);
+        const double sq = sqrt(c1 / PI);
+        const double c2 = sq * sq * sq * (c->dx * c->dx * c->dx);
+        for (int k = 0; k < n; k++) {
+            int dk = k < n - k ? k : n - k;
+            double rz = c->dx * (double)dk;
+            for (int j = 0; j < n; j++) {
+                int dj = j < n - j ? j : n - j;
+                double ry = c->dx * (double)dj;
+                for (int i = 0; i < n; i++) {
+                    int di = i < n - i ? i : n - i;
+                    double rx = c->dx * (double)di;
+                    rx = rx * rx + ry * ry + rz * rz;
+                    double v = c2 * exp(-c1 * rx);
+                    if (v < 1.e-20) v = 0.0;
+                    g[i + ld * (j + (size_t)n * k)] = v;
+                }
+            }
+        }
+        H3D_TRY(upload_phys(c, g.data(), (int64_t)ld, 1));
+        H3D_TRY(fwd3d64(c, G, 1));
+    } else {
+        k_box_transfer<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, delta, G);
+        H3D_LAUNCH_CHECK();
+    }
+    k_filter_apply<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, G, c->U + field * c->fs64);
+    H3D_LAUNCH_CHECK();
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+extern "C" int hit3d_gpu_physical_velocity(hit3d_ctx *c, double *out, int64_t ld1)
+{
+    if (!c || !out) return h3d_set_error_msg(-1, "hit3d_gpu_physical_velocity: null argument");
+    if (ld1 < c->n + 2) return h3d_set_error_msg(-1, "ld1 must be >= nx+2");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    H3D_TRY(inv_from_state(c, 3, PRE_COPY, 0, c->U));
+    const size_t rows = (size_t)c->n * c->n;
+    for (int f = 0; f < 3; f++)
+        H3D_CHECK(cudaMemcpy2DAsync(out + (size_t)f * ld1 * rows, ld1 * sizeof(double),
+                                    reinterpret_cast<double *>(c->W64 + f * c->fs64), 2 * c->P64 * sizeof(double),
+                                    c->n * sizeof(double), rows, cudaMemcpyDeviceToHost, c->st));
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}

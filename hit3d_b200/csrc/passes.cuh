@@ -1,0 +1,421 @@
+// FFT passes over HBM: strided y/z passes and row (x) passes, plus the fused
+// x pass that turns inverse-transformed velocities into forward-transformed
+// products without a round trip through HBM.
+//
+// Replaces xFFT3d (x_fftw.f90:852-1085): the reference's per-plane 2-D r2c,
+// y<->z swap, MPI transpose and z-stick c2c become three in-place passes over
+// the whole field resident in HBM.
+#pragma once
+#include "fft.cuh"
+
+// ---------------------------------------------------------------------------
+// strided (y or z) pass:  CTA = TC adjacent kx columns x one outer index,
+// transform along an axis of stride `sa` (complex elements).
+// ---------------------------------------------------------------------------
+template <typename T, typename TI, typename TO> struct IOPlain {
+    const cx<TI> *src;
+    cx<TO> *dst;
+    int64_t fs_src, fs_dst;  // field strides
+    int64_t sa_src, so_src, sa_dst, so_dst;
+    int ncol;
+    H3D_D cx<T> load(int f, int o, int c, int p) const
+    {
+        if (c >= ncol) return mk<T>(0, 0);
+        return to_cx<T>(src[f * fs_src + p * sa_src + o * so_src + c]);
+    }
+    H3D_D void store(int f, int o, int c, int p, cx<T> v) const
+    {
+        if (c < ncol) dst[f * fs_dst + p * sa_dst + o * so_dst + c] = to_cx<TO>(v);
+    }
+};
+
+// Spectral pre-operations applied while reading the FP64 state in the first
+// inverse (z) pass: column c = kx, outer o = ky index, position p = kz index.
+enum PreMode : int {
+    PRE_COPY = 0,      // field f of the state
+    PRE_SHIFT = 1,     // field f times exp(i (kx+ky+kz) dx/2)   (rhs_velocity.f90:248-257)
+    PRE_CURL = 2,      // vorticity component f                 (m_stats.f90:260-274)
+    PRE_DLONG = 3,     // du_f/dx_f                              (new: skewness)
+    PRE_STRAIN_A = 4,  // S11, S12, S13 for f = 0,1,2            (m_les.f90:1153-1170)
+    PRE_STRAIN_B = 5,  // S22, S23, S33 for f = 0,1,2            (m_les.f90:1180-1198)
+    PRE_GRAD = 6,      // d phi/dx_f of state field `sfield`     (m_stats.f90:323-326)
+};
+
+template <typename T, typename TO> struct IOSpec {
+    const double2 *src;  // state fields, [kz][ky][kx] pitch psrc
+    cx<TO> *dst;         // [z][ky][kx] pitch pdst
+    int64_t fs_src, fs_dst;
+    int n, psrc, pdst, ncol, mode, sfield;
+    double dx;   // grid spacing, for PRE_SHIFT
+
+    H3D_D double2 U(int f, int o, int c, int p) const { return src[f * fs_src + ((int64_t)p * n + o) * psrc + c]; }
+    H3D_D cx<T> load(int f, int o, int c, int p) const
+    {
+        if (c >= ncol) return mk<T>(0, 0);
+        const double kx = c, ky = kwave(o, n), kz = kwave(p, n);
+        double2 r;
+        switch (mode) {
+        case PRE_SHIFT: {
+            double2 u = U(f, o, c, p);
+            double cs = cos((0.5 * ((kx + ky) + kz)) * dx);
+            double sn = sin((0.5 * ((kx + ky) + kz)) * dx);
+            r = make_double2(u.x * cs - u.y * sn, u.y * cs + u.x * sn);
+            break;
+        }
+        case PRE_CURL: {
+            // x_derivative: (a + ib) k -> (-k b, k a); omega as the reference forms it
+            double2 u = U(0, o, c, p), v = U(1, o, c, p), w = U(2, o, c, p);
+            if (f == 0) r = make_double2((-(ky * w.y)) - (-(kz * v.y)), (ky * w.x) - (kz * v.x));       // w_y - v_z
+            else if (f == 1) r = make_double2((-(kz * u.y)) - (-(kx * w.y)), (kz * u.x) - (kx * w.x));  // u_z - w_x
+            else r = make_double2((-(kx * v.y)) - (-(ky * u.y)), (kx * v.x) - (ky * u.x));              // v_x - u_y
+            break;
+        }
+        case PRE_DLONG: {
+            double2 u = U(f, o, c, p);
+            double k = f == 0 ? kx : f == 1 ? ky : kz;
+            r = make_double2(-(k * u.y), k * u.x);
+            break;
+        }
+        case PRE_STRAIN_A: {
+            double2 u = U(0, o, c, p);
+            if (f == 0) r = make_double2(-kx * u.y, kx * u.x);
+            else if (f == 1) { double2 v = U(1, o, c, p); r = make_double2(-0.5 * (ky * u.y + kx * v.y), 0.5 * (ky * u.x + kx * v.x)); }
+            else { double2 w = U(2, o, c, p); r = make_double2(-0.5 * (kz * u.y + kx * w.y), 0.5 * (kz * u.x + kx * w.x)); }
+            break;
+        }
+        case PRE_STRAIN_B: {
+            double2 v = U(1, o, c, p), w = U(2, o, c, p);
+            if (f == 0) r = make_double2(-ky * v.y, ky * v.x);
+            else if (f == 1) r = make_double2(-0.5 * (kz * v.y + ky * w.y), 0.5 * (kz * v.x + ky * w.x));
+            else r = make_double2(-kz * w.y, kz * w.x);
+            break;
+        }
+        case PRE_GRAD: {
+            double2 u = U(sfield, o, c, p);
+            double k = f == 0 ? kx : f == 1 ? ky : kz;
+            r = make_double2(-(k * u.y), k * u.x);
+            break;
+        }
+        default: r = U(f, o, c, p);
+        }
+        return to_cx<T>(r);
+    }
+    H3D_D void store(int f, int o, int c, int p, cx<T> v) const
+    {
+        if (c < ncol) dst[f * fs_dst + ((int64_t)p * n + o) * pdst + c] = to_cx<TO>(v);
+    }
+};
+
+template <typename T, int L, int TC, int NT, bool FWD, class IO>
+__global__ void __launch_bounds__(NT) k_colfft(const IO io, const cx<T> *__restrict__ tw)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
+    using F = ColFFT<T, L, TC, NT, false, FWD, false>;
+    const int col0 = blockIdx.x * TC, outer = blockIdx.y, f = blockIdx.z;
+    cx<T> in[F::NIN], out[F::NOUT];
+#pragma unroll
+    for (int i = 0; i < F::NB0; i++)
+#pragma unroll
+        for (int m = 0; m < F::R0; m++) {
+            int c, p;
+            if (F::in_slot(i, m, c, p)) in[i * F::R0 + m] = io.load(f, outer, col0 + c, p);
+        }
+    F::run(in, sm, out, tw);
+#pragma unroll
+    for (int i = 0; i < F::NBL; i++)
+#pragma unroll
+        for (int m = 0; m < F::RL; m++) {
+            int c, p;
+            if (F::out_slot(i, m, c, p)) io.store(f, outer, col0 + c, p, out[i * F::RL + m]);
+        }
+}
+
+// ---------------------------------------------------------------------------
+// row (x) passes.  A "column" of the FFT is a PAIR of physical rows (2q, 2q+1)
+// packed as z = a + i b; rows are numbered r = z*N + y over the whole field.
+//   complex row r: base + r*pitch            (N/2+1 modes used)
+//   real row r:    (T*)(base + r*pitch)       (N reals used)
+// ---------------------------------------------------------------------------
+template <typename T, int L, int TC, int NT, bool REV>
+using RowFFT = ColFFT<T, L, TC, NT, true, REV ? false : true, REV>;
+
+// Hermitian-extended packed spectrum Z[k] = Xa[k] + i Xb[k] of rows A, B at
+// k in [0, L); the imaginary parts of kx = 0 and kx = N/2 are ignored, as
+// FFTW's c2r does.
+template <typename T, int L, typename TS>
+H3D_D cx<T> load_packed(const cx<TS> *__restrict__ A, const cx<TS> *__restrict__ B, int k)
+{
+    if (k <= L / 2) {
+        cx<TS> a = A[k], b = B[k];
+        if (k == 0 || k == L / 2) { a.y = 0; b.y = 0; }
+        return mk<T>((T)(a.x - b.y), (T)(a.y + b.x));
+    }
+    cx<TS> a = A[L - k], b = B[L - k];
+    return mk<T>((T)(a.x + b.y), (T)(-a.y + b.x));
+}
+
+// After a forward row transform left Z (natural order) in shared memory: split
+// into the half spectra of the two packed rows and store them.
+template <typename T, int L, int TC, int NT, typename TS>
+H3D_D void store_split(const cx<T> *sm, cx<TS> *__restrict__ base, int64_t pitch, int pair0, int npairs)
+{
+    using LY = Lay<L, TC, true>;
+    constexpr int NH = L / 2 + 1;
+    for (int t = threadIdx.x; t < TC * NH; t += NT) {
+        int c = t / NH, k = t - c * NH;
+        if (pair0 + c >= npairs) continue;
+        cx<T> zk = sm[LY::idx(c, k)], zm = sm[LY::idx(c, k == 0 ? 0 : L - k)];
+        cx<TS> xa, xb;
+        xa.x = (TS)((T)0.5 * (zk.x + zm.x));
+        xa.y = (TS)((T)0.5 * (zk.y - zm.y));
+        xb.x = (TS)((T)0.5 * (zk.y + zm.y));
+        xb.y = (TS)((T)-0.5 * (zk.x - zm.x));
+        cx<TS> *A = base + (int64_t)(2 * (pair0 + c)) * pitch;
+        A[k] = xa;
+        A[pitch + k] = xb;
+    }
+}
+
+// plain c2r (inverse x pass) of one field; writes physical rows in place,
+// scaled by norm
+template <typename T, int L, int TC, int NT, typename TS>
+__global__ void __launch_bounds__(NT) k_xc2r(cx<TS> *base, int64_t fs, int64_t pitch, int npairs, T norm,
+                                             const cx<T> *__restrict__ tw)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
+    using F = RowFFT<T, L, TC, NT, true>;
+    const int pair0 = blockIdx.x * TC;
+    cx<TS> *fb = base + blockIdx.z * fs;
+    cx<T> in[F::NIN], out[F::NOUT];
+#pragma unroll
+    for (int i = 0; i < F::NB0; i++)
+#pragma unroll
+        for (int m = 0; m < F::R0; m++) {
+            int c, p;
+            if (F::in_slot(i, m, c, p) && pair0 + c < npairs) {
+                const cx<TS> *A = fb + (int64_t)(2 * (pair0 + c)) * pitch;
+                in[i * F::R0 + m] = load_packed<T, L, TS>(A, A + pitch, p);
+            } else in[i * F::R0 + m] = mk<T>(0, 0);
+        }
+    F::run(in, sm, out, tw);
+#pragma unroll
+    for (int i = 0; i < F::NBL; i++)
+#pragma unroll
+        for (int m = 0; m < F::RL; m++) {
+            int c, p;
+            if (F::out_slot(i, m, c, p) && pair0 + c < npairs) {
+                TS *A = reinterpret_cast<TS *>(fb + (int64_t)(2 * (pair0 + c)) * pitch);
+                A[p] = (TS)(out[i * F::RL + m].x * norm);
+                A[2 * pitch + p] = (TS)(out[i * F::RL + m].y * norm);
+            }
+        }
+}
+
+// plain r2c (forward x pass) of one field, in place
+template <typename T, int L, int TC, int NT, typename TS>
+__global__ void __launch_bounds__(NT) k_xr2c(cx<TS> *base, int64_t fs, int64_t pitch, int npairs,
+                                             const cx<T> *__restrict__ tw)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
+    using F = RowFFT<T, L, TC, NT, false>;
+    const int pair0 = blockIdx.x * TC;
+    cx<TS> *fb = base + blockIdx.z * fs;
+    cx<T> in[F::NIN], out[F::NOUT];
+#pragma unroll
+    for (int i = 0; i < F::NB0; i++)
+#pragma unroll
+        for (int m = 0; m < F::R0; m++) {
+            int c, p;
+            if (F::in_slot(i, m, c, p) && pair0 + c < npairs) {
+                const TS *A = reinterpret_cast<const TS *>(fb + (int64_t)(2 * (pair0 + c)) * pitch);
+                in[i * F::R0 + m] = mk<T>((T)A[p], (T)A[2 * pitch + p]);
+            } else in[i * F::R0 + m] = mk<T>(0, 0);
+        }
+    F::run(in, sm, out, tw);
+    __syncthreads();
+    using LY = typename F::LY;
+#pragma unroll
+    for (int i = 0; i < F::NBL; i++)
+#pragma unroll
+        for (int m = 0; m < F::RL; m++) {
+            int c, p;
+            if (F::out_slot(i, m, c, p)) sm[LY::idx(c, p)] = out[i * F::RL + m];
+        }
+    __syncthreads();
+    store_split<T, L, TC, NT, TS>(sm, fb, pitch, pair0, npairs);
+}
+
+// ---------------------------------------------------------------------------
+// fused x pass:  NIN spectral inputs (after their z and y inverse passes) ->
+// c2r in registers -> per-point operator -> NOUT forward r2c outputs.
+// The inverse uses the reversed radix plan so its output slots are exactly the
+// forward plan's input slots: products never leave registers.
+// OP provides NIN, NOUT, aux(in) and out(o, in, aux).
+// ---------------------------------------------------------------------------
+struct FusedArgs {
+    const void *in[6];   // cx<TS>* of the NIN input fields
+    void *out[6];        // cx<TS>* of the NOUT output fields (may alias inputs)
+    int64_t pitch;
+    int npairs;
+    double norm;
+    unsigned long long *cmax;  // optional: max over points of OP::cour(in) (bit pattern of a double >= 0)
+    double *phys;        // optional: physical copies of the first OP::NPHYS inputs, [f][row][x]
+    int64_t phys_fs, phys_pitch;
+    double p0, p1;       // operator parameters
+};
+
+template <typename T, int L, int TC, int NT, typename TS, class OP>
+__global__ void __launch_bounds__(NT) k_xfused(const FusedArgs a, const cx<T> *__restrict__ tw)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
+    using FI = RowFFT<T, L, TC, NT, true>;
+    using FF = RowFFT<T, L, TC, NT, false>;
+    static_assert(FI::NOUT == FF::NIN, "slot hand-off mismatch");
+    constexpr int NP = FI::NOUT;
+    const int pair0 = blockIdx.x * TC;
+    const T norm = (T)a.norm;
+    OP op{(T)a.p0, (T)a.p1};
+
+    cx<T> phys[OP::NIN][NP];
+#pragma unroll
+    for (int f = 0; f < OP::NIN; f++) {
+        cx<T> in[FI::NIN];
+        const cx<TS> *fb = reinterpret_cast<const cx<TS> *>(a.in[f]);
+#pragma unroll
+        for (int i = 0; i < FI::NB0; i++)
+#pragma unroll
+            for (int m = 0; m < FI::R0; m++) {
+                int c, p;
+                if (FI::in_slot(i, m, c, p) && pair0 + c < a.npairs) {
+                    const cx<TS> *A = fb + (int64_t)(2 * (pair0 + c)) * a.pitch;
+                    in[i * FI::R0 + m] = load_packed<T, L, TS>(A, A + a.pitch, p);
+                } else in[i * FI::R0 + m] = mk<T>(0, 0);
+            }
+        // slots of idle butterflies are never written by run(): keep them zero so
+        // that the Courant maximum and the products never see stale registers
+#pragma unroll
+        for (int q = 0; q < NP; q++) phys[f][q] = mk<T>(0, 0);
+        FI::run(in, sm, phys[f], tw);
+#pragma unroll
+        for (int q = 0; q < NP; q++) phys[f][q] = mk<T>(phys[f][q].x * norm, phys[f][q].y * norm);
+        __syncthreads();
+    }
+    // optional physical copies and the Courant maximum
+    if (a.phys != nullptr) {
+        double *pb = a.phys;
+#pragma unroll
+        for (int i = 0; i < FI::NBL; i++)
+#pragma unroll
+            for (int m = 0; m < FI::RL; m++) {
+                int c, p;
+                if (FI::out_slot(i, m, c, p) && pair0 + c < a.npairs) {
+                    int64_t r = 2 * (pair0 + c);
+#pragma unroll
+                    for (int f = 0; f < OP::NPHYS; f++) {
+                        pb[f * a.phys_fs + r * a.phys_pitch + p] = (double)phys[f][i * FI::RL + m].x;
+                        pb[f * a.phys_fs + (r + 1) * a.phys_pitch + p] = (double)phys[f][i * FI::RL + m].y;
+                    }
+                }
+            }
+    }
+    if (a.cmax != nullptr) {
+        double cm = 0.0;
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            T va[OP::NIN], vb[OP::NIN];
+#pragma unroll
+            for (int f = 0; f < OP::NIN; f++) { va[f] = phys[f][q].x; vb[f] = phys[f][q].y; }
+            cm = fmax(cm, (double)op.cour(va));
+            cm = fmax(cm, (double)op.cour(vb));
+        }
+        // padding slots hold zeros, so they never raise the maximum
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, off));
+        if ((threadIdx.x & 31) == 0) atomicMax(a.cmax, (unsigned long long)__double_as_longlong(cm));
+    }
+    // per-point auxiliary (e.g. eddy viscosity)
+    cx<T> aux[NP];
+#pragma unroll
+    for (int q = 0; q < NP; q++) {
+        T va[OP::NIN], vb[OP::NIN];
+#pragma unroll
+        for (int f = 0; f < OP::NIN; f++) { va[f] = phys[f][q].x; vb[f] = phys[f][q].y; }
+        aux[q] = mk<T>(op.aux(va), op.aux(vb));
+    }
+    using LY = typename FF::LY;
+#pragma unroll 1
+    for (int o = 0; o < OP::NOUT; o++) {
+        cx<T> in[FF::NIN], out[FF::NOUT];
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            T va[OP::NIN], vb[OP::NIN];
+#pragma unroll
+            for (int f = 0; f < OP::NIN; f++) { va[f] = phys[f][q].x; vb[f] = phys[f][q].y; }
+            in[q] = mk<T>(op.out(o, va, aux[q].x), op.out(o, vb, aux[q].y));
+        }
+        FF::run(in, sm, out, tw);
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < FF::NBL; i++)
+#pragma unroll
+            for (int m = 0; m < FF::RL; m++) {
+                int c, p;
+                if (FF::out_slot(i, m, c, p)) sm[LY::idx(c, p)] = out[i * FF::RL + m];
+            }
+        __syncthreads();
+        store_split<T, L, TC, NT, TS>(sm, reinterpret_cast<cx<TS> *>(a.out[o]), a.pitch, pair0, a.npairs);
+        __syncthreads();
+    }
+}
+
+// velocity products (rhs_velocity.f90:56-72): uu uv uw vv vw ww; Courant |u|+|v|+|w|
+template <typename T> struct OpVel {
+    static constexpr int NIN = 3, NOUT = 6, NPHYS = 3;
+    T p0, p1;
+    H3D_D T cour(const T *v) const { return fabs(v[0]) + fabs(v[1]) + fabs(v[2]); }
+    H3D_D T aux(const T *) const { return (T)0; }
+    H3D_D T out(int o, const T *v, T) const
+    {
+        switch (o) {
+        case 0: return v[0] * v[0];
+        case 1: return v[0] * v[1];
+        case 2: return v[0] * v[2];
+        case 3: return v[1] * v[1];
+        case 4: return v[1] * v[2];
+        default: return v[2] * v[2];
+        }
+    }
+};
+
+// scalar fluxes (rhs_scalars.f90:82-85): phi*u, phi*v, phi*w from (u, v, w, phi)
+template <typename T> struct OpScal {
+    static constexpr int NIN = 4, NOUT = 3, NPHYS = 0;
+    T p0, p1;
+    H3D_D T cour(const T *v) const { return fabs(v[0]) + fabs(v[1]) + fabs(v[2]); }
+    H3D_D T aux(const T *) const { return (T)0; }
+    H3D_D T out(int o, const T *v, T) const { return v[3] * v[o]; }
+};
+
+// Smagorinsky: inputs S11 S12 S13 S22 S23 S33, aux = nu_t = (Cs Delta)^2 sqrt(2 S:S)
+// (m_les.f90:1176-1212), outputs tau_ij = -2 nu_t S_ij (m_les.f90:935,989).
+// p0 = (Cs Delta)^2
+template <typename T> struct OpSmag {
+    static constexpr int NIN = 6, NOUT = 6, NPHYS = 0;
+    T p0, p1;
+    H3D_D T cour(const T *) const { return (T)0; }
+    H3D_D T aux(const T *s) const
+    {
+        T t = s[0] * s[0];
+        t = t + (T)2 * (s[1] * s[1]);
+        t = t + (T)2 * (s[2] * s[2]);
+        t = t + s[3] * s[3];
+        t = t + (T)2 * (s[4] * s[4]);
+        t = t + s[5] * s[5];
+        return sqrt((T)2 * t) * p0;
+    }
+    H3D_D T out(int o, const T *s, T nut) const { return ((T)-2 * nut) * s[o]; }
+};

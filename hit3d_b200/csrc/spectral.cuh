@@ -1,0 +1,550 @@
+// Pointwise spectral kernels of the step: RHS assembly with dealiasing masks,
+// band forcing, Adams-Bashforth update and pressure projection fused in one
+// pass over the modes; plus forcing energy, dealias, shell spectra, reductions
+// and initial-condition shaping.
+#pragma once
+#include "common.cuh"
+
+struct ModeIdx {
+    int kx, kyi, kzi;       // kx in [0, N/2], ky/kz storage indices
+    double ax, ay, az;      // signed wavenumbers akx, aky, akz
+    int ialias;             // number of |k_i| > N/3 (x_fftw.f90:298-310)
+};
+
+H3D_D ModeIdx mode_of(int64_t t, int n, int nh)
+{
+    ModeIdx m;
+    m.kx = (int)(t % nh);
+    int64_t r = t / nh;
+    m.kyi = (int)(r % n);
+    m.kzi = (int)(r / n);
+    m.ax = m.kx;
+    m.ay = kwave(m.kyi, n);
+    m.az = kwave(m.kzi, n);
+    const double rn3 = (double)(n / 3);
+    m.ialias = (fabs(m.ay) > rn3) + (fabs(m.az) > rn3) + (fabs(m.ax) > rn3);
+    return m;
+}
+H3D_D int64_t soff(const ModeIdx &m, int n, int pitch) { return ((int64_t)m.kzi * n + m.kyi) * pitch + m.kx; }
+
+// Machiels band forcing: a mode takes part when kx < N/2 (the reference loops
+// over real indices 1..nx) and its float32 shell index is in [1, kfmax]
+// (m_force.f90:166-209).
+H3D_D bool forced(const ModeIdx &m, int n, int kfmax)
+{
+    if (kfmax <= 0 || m.kx >= n / 2) return false;
+    double k2 = m.ax * m.ax + m.ay * m.ay + m.az * m.az;
+    if (k2 > (kfmax + 1.0) * (kfmax + 1.0)) return false;
+    int sh = shell32(k2);
+    return sh > 0 && sh <= kfmax;
+}
+
+// pressure projection of one mode (pressure.f90:13-47)
+H3D_D void project(const ModeIdx &m, double2 &u, double2 &v, double2 &w)
+{
+    double kx = m.ax, ky = m.ay, kz = m.az;
+    double div2 = kx * u.x + ky * v.x + kz * w.x;
+    double div1 = -(kx * u.y + ky * v.y + kz * w.y);
+    double l = kx * kx + ky * ky + kz * kz;
+    if (l == 0.0) l = 9e20;
+    double p1 = -div1 / l, p2 = -div2 / l;
+    u.x = u.x + p2 * kx; u.y = u.y - p1 * kx;
+    v.x = v.x + p2 * ky; v.y = v.y - p1 * ky;
+    w.x = w.x + p2 * kz; w.y = w.y - p1 * kz;
+}
+
+// Adams-Bashforth 2 (Euler on the first step) of one mode (main.f90:156-164)
+H3D_D void ab2(double2 &f, double2 &ro, double2 r, double dt, bool euler)
+{
+    if (euler) {
+        ro = r;
+        f.x = f.x + dt * ro.x;
+        f.y = f.y + dt * ro.y;
+    } else {
+        f.x = f.x + dt * (1.5 * r.x - 0.5 * ro.x);
+        f.y = f.y + dt * (1.5 * r.y - 0.5 * ro.y);
+        ro = r;
+    }
+}
+
+template <typename TP> H3D_D double2 ld2(const cx<TP> *p, int64_t i)
+{
+    cx<TP> v = p[i];
+    return make_double2((double)v.x, (double)v.y);
+}
+
+struct StepArgs {
+    int n, nh, pitch, ppitch;  // state pitch, product pitch
+    int64_t fs, pfs;           // state / product field strides (complex elements)
+    double nu, dt;
+    int euler_v, euler_s;
+    int flow_type, kfmax;
+    double famp;
+    const double *fenergy;     // device: energy in the forcing band
+    int nscal;
+    double pe[8];
+    int stype[8];
+};
+
+// 2/3 rule (rhs_velocity.f90:85-142) + forcing + AB2 + pressure.
+// P: six product spectra [uu uv uw vv vw ww]; U, RO: velocity state and old RHS
+// TAU (optional, Smagorinsky): six subgrid-stress spectra [t11 t12 t13 t22 t23 t33]
+// added where ialias == 0 (les_rhsv_turb_visc, m_les.f90:941-1015)
+template <typename TP>
+__global__ void k_update_vel_23(const StepArgs a, const cx<TP> *__restrict__ P, const cx<TP> *__restrict__ TAU,
+                                double2 *__restrict__ U, double2 *__restrict__ RO)
+{
+    const int64_t nm = (int64_t)a.n * a.n * a.nh;
+    const double fac = (a.flow_type == 1) ? a.famp / *a.fenergy : 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        ModeIdx m = mode_of(t, a.n, a.nh);
+        int64_t o = soff(m, a.n, a.pitch), po = soff(m, a.n, a.ppitch);
+        double2 u[3] = {U[o], U[o + a.fs], U[o + 2 * a.fs]};
+        double2 r[3];
+        if (m.ialias > 0) {
+            r[0] = r[1] = r[2] = make_double2(0.0, 0.0);
+        } else {
+            double2 p11 = ld2<TP>(P, po), p12 = ld2<TP>(P, po + a.pfs), p13 = ld2<TP>(P, po + 2 * a.pfs);
+            double2 p22 = ld2<TP>(P, po + 3 * a.pfs), p23 = ld2<TP>(P, po + 4 * a.pfs), p33 = ld2<TP>(P, po + 5 * a.pfs);
+            double kx = m.ax, ky = m.ay, kz = m.az;
+            double2 t1 = make_double2(-(kx * p11.x + ky * p12.x + kz * p13.x), -(kx * p11.y + ky * p12.y + kz * p13.y));
+            double2 t2 = make_double2(-(kx * p12.x + ky * p22.x + kz * p23.x), -(kx * p12.y + ky * p22.y + kz * p23.y));
+            double2 t3 = make_double2(-(kx * p13.x + ky * p23.x + kz * p33.x), -(kx * p13.y + ky * p23.y + kz * p33.y));
+            double t4 = -a.nu * (kx * kx + ky * ky + kz * kz);
+            double2 tt[3] = {t1, t2, t3};
+#pragma unroll
+            for (int c = 0; c < 3; c++) r[c] = make_double2(-tt[c].y + t4 * u[c].x, tt[c].x + t4 * u[c].y);
+            if (TAU != nullptr) {
+                double2 s11 = ld2<TP>(TAU, po), s12 = ld2<TP>(TAU, po + a.pfs), s13 = ld2<TP>(TAU, po + 2 * a.pfs);
+                double2 s22 = ld2<TP>(TAU, po + 3 * a.pfs), s23 = ld2<TP>(TAU, po + 4 * a.pfs), s33 = ld2<TP>(TAU, po + 5 * a.pfs);
+                r[0].x = r[0].x + kx * s11.y + ky * s12.y + kz * s13.y;
+                r[0].y = r[0].y - kx * s11.x - ky * s12.x - kz * s13.x;
+                r[1].x = r[1].x + kx * s12.y;
+                r[1].y = r[1].y - kx * s12.x;
+                r[2].x = r[2].x + kx * s13.y;
+                r[2].y = r[2].y - kx * s13.x;
+                r[1].x = r[1].x + ky * s22.y + kz * s23.y;
+                r[1].y = r[1].y - ky * s22.x - kz * s23.x;
+                r[2].x = r[2].x + ky * s23.y + kz * s33.y;
+                r[2].y = r[2].y - ky * s23.x - kz * s33.x;
+            }
+        }
+        if (a.flow_type == 1 && forced(m, a.n, a.kfmax)) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) { r[c].x = r[c].x + fac * u[c].x; r[c].y = r[c].y + fac * u[c].y; }
+        }
+        double2 ro[3] = {RO[o], RO[o + a.fs], RO[o + 2 * a.fs]};
+#pragma unroll
+        for (int c = 0; c < 3; c++) ab2(u[c], ro[c], r[c], a.dt, a.euler_v);
+        project(m, u[0], u[1], u[2]);
+#pragma unroll
+        for (int c = 0; c < 3; c++) { U[o + c * a.fs] = u[c]; RO[o + c * a.fs] = ro[c]; }
+    }
+}
+
+// phase shift, first half (rhs_velocity.f90:183-232): partial RHS into RP
+template <typename TP>
+__global__ void k_rhs_vel_ps1(const StepArgs a, const cx<TP> *__restrict__ P, const double2 *__restrict__ U,
+                              double2 *__restrict__ RP)
+{
+    const int64_t nm = (int64_t)a.n * a.n * a.nh;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        ModeIdx m = mode_of(t, a.n, a.nh);
+        int64_t o = soff(m, a.n, a.pitch), po = soff(m, a.n, a.ppitch);
+        double2 r[3];
+        if (m.ialias > 1) {
+            r[0] = r[1] = r[2] = make_double2(0.0, 0.0);
+        } else {
+            double2 u[3] = {U[o], U[o + a.fs], U[o + 2 * a.fs]};
+            double2 p11 = ld2<TP>(P, po), p12 = ld2<TP>(P, po + a.pfs), p13 = ld2<TP>(P, po + 2 * a.pfs);
+            double2 p22 = ld2<TP>(P, po + 3 * a.pfs), p23 = ld2<TP>(P, po + 4 * a.pfs), p33 = ld2<TP>(P, po + 5 * a.pfs);
+            double kx = m.ax, ky = m.ay, kz = m.az;
+            double2 t1 = make_double2(-(kx * p11.x + ky * p12.x + kz * p13.x), -(kx * p11.y + ky * p12.y + kz * p13.y));
+            double2 t2 = make_double2(-(kx * p12.x + ky * p22.x + kz * p23.x), -(kx * p12.y + ky * p22.y + kz * p23.y));
+            double2 t3 = make_double2(-(kx * p13.x + ky * p23.x + kz * p33.x), -(kx * p13.y + ky * p23.y + kz * p33.y));
+            double t4 = -a.nu * (kx * kx + ky * ky + kz * kz);
+            double2 tt[3] = {t1, t2, t3};
+#pragma unroll
+            for (int c = 0; c < 3; c++) r[c] = make_double2(-0.5 * tt[c].y + t4 * u[c].x, 0.5 * tt[c].x + t4 * u[c].y);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) RP[o + c * a.fs] = r[c];
+    }
+}
+
+// shift back by exp(-i k.delta) (rhs_velocity.f90:276-278)
+H3D_D double2 shift_back(double2 v, double cs, double sn)
+{
+    return make_double2(v.x * cs + v.y * sn, v.y * cs - v.x * sn);
+}
+
+// phase shift, second half (rhs_velocity.f90:242-408) + forcing + AB2 + pressure.
+// Q: six shifted product spectra [u+u+ u+v+ u+w+ v+v+ v+w+ w+w+]
+template <typename TP>
+__global__ void k_update_vel_ps2(const StepArgs a, double dx, const cx<TP> *__restrict__ Q,
+                                 const double2 *__restrict__ RP, double2 *__restrict__ U, double2 *__restrict__ RO)
+{
+    const int64_t nm = (int64_t)a.n * a.n * a.nh;
+    const double fac = (a.flow_type == 1) ? a.famp / *a.fenergy : 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        ModeIdx m = mode_of(t, a.n, a.nh);
+        int64_t o = soff(m, a.n, a.pitch), po = soff(m, a.n, a.ppitch);
+        double2 u[3] = {U[o], U[o + a.fs], U[o + 2 * a.fs]};
+        double2 r[3];
+        double kx = m.ax, ky = m.ay, kz = m.az;
+        if (m.ialias < 2) {
+            double cs = cos((0.5 * ((kx + ky) + kz)) * dx), sn = sin((0.5 * ((kx + ky) + kz)) * dx);
+            r[0] = RP[o]; r[1] = RP[o + a.fs]; r[2] = RP[o + 2 * a.fs];
+            double2 A = shift_back(ld2<TP>(Q, po), cs, sn);                // u+u+
+            r[0].x = r[0].x + 0.5 * kx * A.y; r[0].y = r[0].y - 0.5 * kx * A.x;
+            double2 B = shift_back(ld2<TP>(Q, po + a.pfs), cs, sn);        // u+v+
+            r[0].x = r[0].x + 0.5 * ky * B.y; r[0].y = r[0].y - 0.5 * ky * B.x;
+            r[1].x = r[1].x + 0.5 * kx * B.y; r[1].y = r[1].y - 0.5 * kx * B.x;
+            double2 Cc = shift_back(ld2<TP>(Q, po + 3 * a.pfs), cs, sn);   // v+v+
+            r[1].x = r[1].x + 0.5 * ky * Cc.y; r[1].y = r[1].y - 0.5 * ky * Cc.x;
+            double2 D4 = shift_back(ld2<TP>(Q, po + 2 * a.pfs), cs, sn);   // u+w+
+            double2 D5 = shift_back(ld2<TP>(Q, po + 4 * a.pfs), cs, sn);   // v+w+
+            double2 D6 = shift_back(ld2<TP>(Q, po + 5 * a.pfs), cs, sn);   // w+w+
+            r[0].x = r[0].x + 0.5 * kz * D4.y; r[0].y = r[0].y - 0.5 * kz * D4.x;
+            r[1].x = r[1].x + 0.5 * kz * D5.y; r[1].y = r[1].y - 0.5 * kz * D5.x;
+            r[2].x = r[2].x + 0.5 * (kx * D4.y + ky * D5.y + kz * D6.y);
+            r[2].y = r[2].y - 0.5 * (kx * D4.x + ky * D5.x + kz * D6.x);
+        } else {
+            r[0] = r[1] = r[2] = make_double2(0.0, 0.0);
+        }
+        if (a.flow_type == 1 && forced(m, a.n, a.kfmax)) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) { r[c].x = r[c].x + fac * u[c].x; r[c].y = r[c].y + fac * u[c].y; }
+        }
+        double2 ro[3] = {RO[o], RO[o + a.fs], RO[o + 2 * a.fs]};
+#pragma unroll
+        for (int c = 0; c < 3; c++) ab2(u[c], ro[c], r[c], a.dt, a.euler_v);
+        project(m, u[0], u[1], u[2]);
+#pragma unroll
+        for (int c = 0; c < 3; c++) { U[o + c * a.fs] = u[c]; RO[o + c * a.fs] = ro[c]; }
+    }
+}
+
+// Scalar RHS + AB2 for scalar s.
+//  mode 0 (2/3 rule, rhs_scalars.f90:88-121):     P = fluxes [phi u, phi v, phi w]
+//  mode 1 (phase shift, first = unshifted half):  writes SP = 0.5 * flux term (masked)
+//  mode 2 (phase shift, final = shifted half):    P = shifted fluxes, adds SP and diffusion
+// The uniform-gradient source -u is added over all modes for type 0 scalars
+// (rhs_scalars.f90:387-389).
+template <typename TP>
+__global__ void k_scalar(const StepArgs a, int mode, int s, double dx, const cx<TP> *__restrict__ P,
+                         double2 *__restrict__ SP, const double2 *__restrict__ Uvel, double2 *__restrict__ PHI,
+                         double2 *__restrict__ RO)
+{
+    const int64_t nm = (int64_t)a.n * a.n * a.nh;
+    const double pe = a.pe[s];
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        ModeIdx m = mode_of(t, a.n, a.nh);
+        int64_t o = soff(m, a.n, a.pitch), po = soff(m, a.n, a.ppitch);
+        double kx = m.ax, ky = m.ay, kz = m.az;
+        double2 pu = ld2<TP>(P, po), pv = ld2<TP>(P, po + a.pfs), pw = ld2<TP>(P, po + 2 * a.pfs);
+        if (mode == 1) {
+            double2 sp = make_double2(0.0, 0.0);
+            if (m.ialias < 2) {
+                double rt1 = kx * pu.y + ky * pv.y + kz * pw.y;
+                double rt2 = kx * pu.x + ky * pv.x + kz * pw.x;
+                sp = make_double2(0.5 * rt1, -(0.5 * rt2));
+            }
+            SP[o] = sp;
+            continue;
+        }
+        double2 phi = PHI[o];
+        double2 r;
+        double wn2 = kx * kx + ky * ky + kz * kz;
+        if (mode == 0) {
+            if (m.ialias > 0) r = make_double2(0.0, 0.0);
+            else {
+                double rt1 = kx * pu.y + ky * pv.y + kz * pw.y;
+                double rt2 = kx * pu.x + ky * pv.x + kz * pw.x;
+                r = make_double2(rt1 - pe * wn2 * phi.x, -rt2 - pe * wn2 * phi.y);
+            }
+        } else {
+            if (m.ialias > 1) r = make_double2(0.0, 0.0);
+            else {
+                double cs = cos((0.5 * ((kx + ky) + kz)) * dx), sn = sin((0.5 * ((kx + ky) + kz)) * dx);
+                double2 a1 = shift_back(pu, cs, sn), a2 = shift_back(pv, cs, sn), a3 = shift_back(pw, cs, sn);
+                r = make_double2(+0.5 * (kx * a1.y + ky * a2.y + kz * a3.y), -0.5 * (kx * a1.x + ky * a2.x + kz * a3.x));
+                double2 sp = SP[o];
+                r.x = r.x + sp.x - pe * wn2 * phi.x;
+                r.y = r.y + sp.y - pe * wn2 * phi.y;
+            }
+        }
+        if (a.stype[s] == 0) {
+            double2 u = Uvel[o];
+            r.x = r.x - u.x;
+            r.y = r.y - u.y;
+        }
+        double2 ro = RO[o];
+        ab2(phi, ro, r, a.dt, a.euler_s);
+        PHI[o] = phi;
+        RO[o] = ro;
+    }
+}
+
+// Energy in the forcing band, summed by one thread in the reference's loop
+// order (m_force.f90:266-284) so that the result is reproducible to the bit.
+__global__ void k_forcing_energy(int n, int pitch, int64_t fs, int kfmax, const double2 *__restrict__ U,
+                                 double *out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double es[16];
+    for (int s = 0; s < 16; s++) es[s] = 0.0;
+    const double n3 = (double)n * n * n;
+    const double fac = 1.0 / (n3 * n3);
+    const int km = kfmax + 1;
+    // storage indices in increasing order whose |wavenumber| <= km: 0..km, n-km..n-1
+    for (int kq = 0; kq < n; kq++) {
+        if (kq > km && kq < n - km) { kq = n - km - 1; continue; }
+        const int ky = kwave(kq, n);
+        for (int jq = 0; jq < n; jq++) {
+            if (jq > km && jq < n - km) { jq = n - km - 1; continue; }
+            const int kz = kwave(jq, n);
+            for (int kx = 0; kx <= km && kx < n / 2; kx++) {
+                double k2 = (double)kx * kx + (double)ky * ky + (double)kz * kz;
+                int sh = shell32(k2);
+                if (sh <= 0 || sh > kfmax) continue;
+                const int64_t o = ((int64_t)jq * n + kq) * pitch + kx;
+                double2 u = U[o], v = U[fs + o], w = U[2 * fs + o];
+                // real entry then imaginary entry, each added on its own
+                double f2 = __dmul_rn(fac, __dadd_rn(__dadd_rn(__dmul_rn(u.x, u.x), __dmul_rn(v.x, v.x)), __dmul_rn(w.x, w.x)));
+                if (kx == 0) f2 = __dmul_rn(f2, 0.5);
+                es[sh - 1] = __dadd_rn(es[sh - 1], f2);
+                f2 = __dmul_rn(fac, __dadd_rn(__dadd_rn(__dmul_rn(u.y, u.y), __dmul_rn(v.y, v.y)), __dmul_rn(w.y, w.y)));
+                if (kx == 0) f2 = __dmul_rn(f2, 0.5);
+                es[sh - 1] = __dadd_rn(es[sh - 1], f2);
+            }
+        }
+    }
+    double e = 0.0;
+    for (int s = 0; s < kfmax; s++) e = __dadd_rn(e, es[s]);
+    *out = e;
+}
+
+// dealias_all (dealias_all.f90:97-131): zero modes with any |k_i| > kmax
+__global__ void k_dealias_all(int n, int nh, int pitch, int64_t fs, int nf, int kmax, double2 *U)
+{
+    const int64_t nm = (int64_t)n * n * nh;
+    const double ak = (double)kmax;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        ModeIdx m = mode_of(t, n, nh);
+        if (fabs(m.ax) > ak || fabs(m.ay) > ak || fabs(m.az) > ak) {
+            int64_t o = soff(m, n, pitch);
+            for (int f = 0; f < nf; f++) U[o + f * fs] = make_double2(0.0, 0.0);
+        }
+    }
+}
+
+// Shell spectrum sum_{shell} fac * |f|^2 (kx = 0 halved, kx = N/2 excluded),
+// float32 shell index (m_stats.f90:195-235).  Deterministic: each warp owns a
+// private histogram, lane L accumulates the shells congruent to L mod 32 in a
+// fixed element order; warps and blocks are combined in index order.
+__global__ void k_shell_partial(int n, int nh, int pitch, int64_t fs, int nf, int kmax, const double2 *__restrict__ U,
+                                double *__restrict__ part /* [gridDim.x][kmax] */)
+{
+    extern __shared__ double hist[];  // [warps][kmax]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = threadIdx.x; i < nw * kmax; i += blockDim.x) hist[i] = 0.0;
+    __syncthreads();
+    const double n3 = (double)n * n * n;
+    const double fac = 1.0 / (n3 * n3);
+    const int64_t nm = (int64_t)n * n * nh;
+    const int64_t per_block = (nm + gridDim.x - 1) / gridDim.x;
+    const int64_t b0 = blockIdx.x * per_block, b1 = min(nm, b0 + per_block);
+    double *h = hist + warp * kmax;
+    for (int64_t base = b0 + warp * 32; base < b1; base += nw * 32) {
+        int64_t t = base + lane;
+        int sh = -1;
+        double e = 0.0;
+        if (t < b1) {
+            ModeIdx m = mode_of(t, n, nh);
+            if (m.kx < n / 2) {
+                double k2 = m.ax * m.ax + m.ay * m.ay + m.az * m.az;
+                int s = shell32(k2);
+                if (s > 0 && s <= kmax) {
+                    int64_t o = soff(m, n, pitch);
+                    double re = 0.0, im = 0.0;
+                    for (int f = 0; f < nf; f++) {
+                        double2 v = U[o + f * fs];
+                        re = (f == 0) ? v.x * v.x : re + v.x * v.x;
+                        im = (f == 0) ? v.y * v.y : im + v.y * v.y;
+                    }
+                    double e1 = fac * re, e2 = fac * im;
+                    if (m.kx == 0) { e1 *= 0.5; e2 *= 0.5; }
+                    e = e1 + e2;
+                    sh = s - 1;
+                }
+            }
+        }
+        for (int l = 0; l < 32; l++) {
+            int s = __shfl_sync(0xffffffffu, sh, l);
+            double v = __shfl_sync(0xffffffffu, e, l);
+            if (s >= 0 && (s & 31) == lane) h[s] += v;
+        }
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < kmax; s += blockDim.x) {
+        double acc = 0.0;
+        for (int w = 0; w < nw; w++) acc += hist[w * kmax + s];
+        part[(int64_t)blockIdx.x * kmax + s] = acc;
+    }
+}
+
+__global__ void k_shell_final(int nblk, int kmax, const double *__restrict__ part, double *__restrict__ out)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < kmax; s += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int b = 0; b < nblk; b++) acc += part[(int64_t)b * kmax + s];
+        out[s] = acc;
+    }
+}
+
+// Deterministic sums over physical points of the fields:
+// mode 0: sum_f x_f^2;  mode 1: x_0^2 and x_0^3 (two sums);  mode 2: x, x^2, min, max of x_0
+__global__ void k_phys_partial(int n, int64_t rpitch, int64_t fs, int nf, int mode, const double *__restrict__ X,
+                               double *__restrict__ part /* [gridDim.x][4] */)
+{
+    __shared__ double sh[4][32];
+    const int64_t np = (int64_t)n * n * n;
+    double s0 = 0.0, s1 = 0.0, mn = 1e300, mx = -1e300;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t row = t / n, x = t - row * n;
+        const double *p = X + row * rpitch + x;
+        if (mode == 0) {
+            double q = 0.0;
+            for (int f = 0; f < nf; f++) { double v = p[f * fs]; q = (f == 0) ? v * v : q + v * v; }
+            s0 += q;
+        } else if (mode == 1) {
+            double v = p[0];
+            s0 += v * v;
+            s1 += v * v * v;
+        } else {
+            double v = p[0];
+            s0 += v;
+            s1 += v * v;
+            mn = fmin(mn, v);
+            mx = fmax(mx, v);
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, off));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (l == 0) { sh[0][w] = s0; sh[1][w] = s1; sh[2][w] = mn; sh[3][w] = mx; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a0 = 0.0, a1 = 0.0, a2 = 1e300, a3 = -1e300;
+        for (int i = 0; i < nw; i++) { a0 += sh[0][i]; a1 += sh[1][i]; a2 = fmin(a2, sh[2][i]); a3 = fmax(a3, sh[3][i]); }
+        part[blockIdx.x * 4 + 0] = a0; part[blockIdx.x * 4 + 1] = a1;
+        part[blockIdx.x * 4 + 2] = a2; part[blockIdx.x * 4 + 3] = a3;
+    }
+}
+
+__global__ void k_phys_final(int nblk, const double *__restrict__ part, double *__restrict__ out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double a0 = 0.0, a1 = 0.0, a2 = 1e300, a3 = -1e300;
+    for (int b = 0; b < nblk; b++) {
+        a0 += part[b * 4]; a1 += part[b * 4 + 1];
+        a2 = fmin(a2, part[b * 4 + 2]); a3 = fmax(a3, part[b * 4 + 3]);
+    }
+    out[0] = a0; out[1] = a1; out[2] = a2; out[3] = a3;
+}
+
+// initial velocity: solenoidal curl of the transformed Gaussian noise G restricted
+// to shells 1..kmax with an FP64 shell index (init_velocity.f90:123-149)
+__global__ void k_init_curl(int n, int nh, int pitch, int64_t fs, int kmax, const double2 *__restrict__ G,
+                            double2 *__restrict__ U)
+{
+    const int64_t nm = (int64_t)n * n * nh;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        ModeIdx m = mode_of(t, n, nh);
+        int64_t o = soff(m, n, pitch);
+        double kx = m.ax, ky = m.ay, kz = m.az;
+        int sh = (int)llround(sqrt(kx * kx + ky * ky + kz * kz));
+        double2 r4 = make_double2(0, 0), r5 = r4, r6 = r4;
+        if (sh > 0 && sh <= kmax) {
+            double2 g1 = G[o], g2 = G[o + fs], g3 = G[o + 2 * fs];
+            r4 = make_double2(-(ky * g3.y - kz * g2.y), ky * g3.x - kz * g2.x);
+            r5 = make_double2(-(kz * g1.y - kx * g3.y), kz * g1.x - kx * g3.x);
+            r6 = make_double2(-(kx * g2.y - ky * g1.y), kx * g2.x - ky * g1.x);
+        }
+        U[o] = r4; U[o + fs] = r5; U[o + 2 * fs] = r6;
+    }
+}
+
+// multiply modes of shells 1..kmax by ratio[shell] and zero the rest
+// (init_velocity.f90:224-237); ratio[s] < 0 marks an empty shell
+__global__ void k_shell_scale(int n, int nh, int pitch, int64_t fs, int nf, int kmax, const double *__restrict__ ratio,
+                              double2 *__restrict__ U)
+{
+    const int64_t nm = (int64_t)n * n * nh;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        ModeIdx m = mode_of(t, n, nh);
+        int64_t o = soff(m, n, pitch);
+        int sh = shell32(m.ax * m.ax + m.ay * m.ay + m.az * m.az);
+        bool keep = sh > 0 && sh <= kmax && ratio[sh - 1] >= 0.0;
+        for (int f = 0; f < nf; f++) {
+            double2 v = U[o + f * fs];
+            if (keep) { double r = ratio[sh - 1]; v.x = v.x * r; v.y = v.y * r; }
+            else v = make_double2(0.0, 0.0);
+            U[o + f * fs] = v;
+        }
+    }
+}
+
+// spectral filter f <- f * G as a complex product (m_filter_xfftw.f90:92-104);
+// G is the transfer function in the device spectral layout
+__global__ void k_filter_apply(int n, int nh, int pitch, const double2 *__restrict__ G, double2 *__restrict__ F)
+{
+    const int64_t nm = (int64_t)n * n * nh;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        ModeIdx m = mode_of(t, n, nh);
+        int64_t o = soff(m, n, pitch);
+        double2 f = F[o], g = G[o];
+        F[o] = make_double2(f.x * g.x - f.y * g.y, f.y * g.x + f.x * g.y);
+    }
+}
+
+// box filter of width delta: G = prod_a sin(k_a delta/2)/(k_a delta/2), real
+__global__ void k_box_transfer(int n, int nh, int pitch, double delta, double2 *__restrict__ G)
+{
+    const int64_t nm = (int64_t)n * n * nh;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        ModeIdx m = mode_of(t, n, nh);
+        double g = 1.0;
+        double ks[3] = {m.ax, m.ay, m.az};
+        for (int q = 0; q < 3; q++) { double h = 0.5 * ks[q] * delta; g *= (h == 0.0) ? 1.0 : sin(h) / h; }
+        G[soff(m, n, pitch)] = make_double2(g, 0.0);
+    }
+}
+
+// layout conversion between the reference's (nx+2, ny, nz) Fourier array
+// [ky][kz][kx] (pitch nh) and the device layout [kz][ky][kx] (pitch P)
+__global__ void k_ref_to_dev(int n, int nh, int pitch, const double2 *__restrict__ R, double2 *__restrict__ D)
+{
+    const int64_t nm = (int64_t)n * n * nh;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        int kx = (int)(t % nh);
+        int64_t r = t / nh;
+        int kzi = (int)(r % n), kyi = (int)(r / n);
+        D[((int64_t)kzi * n + kyi) * pitch + kx] = R[t];
+    }
+}
+__global__ void k_dev_to_ref(int n, int nh, int pitch, const double2 *__restrict__ D, double2 *__restrict__ R)
+{
+    const int64_t nm = (int64_t)n * n * nh;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        int kx = (int)(t % nh);
+        int64_t r = t / nh;
+        int kzi = (int)(r % n), kyi = (int)(r / n);
+        R[t] = D[((int64_t)kzi * n + kyi) * pitch + kx];
+    }
+}

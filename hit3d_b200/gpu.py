@@ -1,0 +1,257 @@
+"""ctypes binding of libhit3d_gpu.so (the C-ABI of include/hit3d_gpu.h).
+
+This is the Python counterpart of the ISO_C_BINDING interfaces a Fortran host
+would declare: every call maps 1:1 onto an ``extern "C"`` entry point, arrays are
+passed as plain pointers in the reference's (nx+2, ny, nz, nfields) layout, and a
+non-zero return code raises :class:`Hit3dError` (the reference stops through
+``my_exit(-1)``, my_exit.f90:23-62).
+
+There is no CPU fallback: if the shared library is missing this module raises on
+import of :func:`lib`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhit3d_gpu.so")
+MAX_SCALARS = 8
+_lib = None
+
+
+class Hit3dError(RuntimeError):
+    pass
+
+
+class _Params(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("dealias", C.c_int32), ("flow_type", C.c_int32), ("force_type", C.c_int32),
+        ("kfmax", C.c_int32), ("n_scalars", C.c_int32), ("precision", C.c_int32), ("les_model", C.c_int32),
+        ("scalar_type", C.c_int32 * MAX_SCALARS), ("device", C.c_int32), ("reserved", C.c_int32),
+        ("nu", C.c_double), ("dt", C.c_double), ("famp", C.c_double), ("c_smag", C.c_double),
+        ("sc", C.c_double * MAX_SCALARS),
+    ]
+
+
+@dataclass
+class Params:
+    """Run parameters (the values of <run_name>.in, m_parameters.f90:172-512)."""
+    nx: int = 64
+    dealias: int = 0
+    flow_type: int = 0
+    force_type: int = 1
+    kfmax: int = 2
+    n_scalars: int = 0
+    precision: int = 0
+    les_model: int = 0
+    scalar_type: Sequence[int] = field(default_factory=list)
+    device: int = 0
+    nu: float = 1.0 / 400.0
+    dt: float = 0.005
+    famp: float = 0.5
+    c_smag: float = 0.18
+    sc: Sequence[float] = field(default_factory=list)
+
+    @property
+    def kmax(self) -> int:
+        """Largest resolved shell (m_parameters.f90:123-131)."""
+        dealias = 0 if self.les_model else self.dealias
+        if dealias == 0:
+            return self.nx // 3
+        return int(np.floor(self.nx / 3.0 * np.sqrt(2.0)))
+
+    def to_c(self) -> _Params:
+        p = _Params()
+        for k in ("nx", "dealias", "flow_type", "force_type", "kfmax", "n_scalars", "precision", "les_model",
+                  "device"):
+            setattr(p, k, int(getattr(self, k)))
+        for k in ("nu", "dt", "famp", "c_smag"):
+            setattr(p, k, float(getattr(self, k)))
+        st = list(self.scalar_type) + [0] * MAX_SCALARS
+        sc = list(self.sc) + [1.0] * MAX_SCALARS
+        for i in range(MAX_SCALARS):
+            p.scalar_type[i] = int(st[i])
+            p.sc[i] = float(sc[i])
+        return p
+
+
+# (name, restype, argtypes) of every entry point of include/hit3d_gpu.h
+_vp, _dp, _i32, _i64, _d = C.c_void_p, C.POINTER(C.c_double), C.c_int32, C.c_int64, C.c_double
+SIGNATURES = [
+    ("hit3d_gpu_init", C.c_int, [C.POINTER(_Params), C.POINTER(C.c_void_p)]),
+    ("hit3d_gpu_finalize", None, [_vp]),
+    ("hit3d_gpu_last_error", C.c_char_p, []),
+    ("hit3d_gpu_upload_fields", C.c_int, [_vp, _dp, _i64, _i32]),
+    ("hit3d_gpu_download_fields", C.c_int, [_vp, _dp, _i64, _i32]),
+    ("hit3d_gpu_upload_rhs_old", C.c_int, [_vp, _dp, _i64, _i32]),
+    ("hit3d_gpu_download_rhs_old", C.c_int, [_vp, _dp, _i64, _i32]),
+    ("hit3d_gpu_step", C.c_int, [_vp, _i32, C.POINTER(_i32), C.POINTER(_i32), _dp]),
+    ("hit3d_gpu_set_dt", C.c_int, [_vp, _d]),
+    ("hit3d_gpu_set_scalars_active", C.c_int, [_vp, _i32]),
+    ("hit3d_gpu_dealias_all", C.c_int, [_vp]),
+    ("hit3d_gpu_init_velocity", C.c_int, [_vp, _d, _i32, _d, _d]),
+    ("hit3d_gpu_stats", C.c_int, [_vp, _dp, _i32, _dp]),
+    ("hit3d_gpu_scalar_stats", C.c_int, [_vp, _i32, _dp, _i32, _dp]),
+    ("hit3d_gpu_particles_upload", C.c_int, [_vp, _dp, _dp, _i64, _i32]),
+    ("hit3d_gpu_particles_download", C.c_int, [_vp, _dp, _dp]),
+    ("hit3d_gpu_xfft3d", C.c_int, [_vp, _i32, _dp, _dp, _i64]),
+    ("hit3d_gpu_filter_field", C.c_int, [_vp, _i32, _d, _i32]),
+    ("hit3d_gpu_physical_velocity", C.c_int, [_vp, _dp, _i64]),
+]
+
+
+def lib():
+    """Load the in-tree library; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise Hit3dError(f"{LIB_PATH} is missing: build it with `python -m hit3d_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        msg = lib().hit3d_gpu_last_error().decode(errors="replace")
+        raise Hit3dError(f"{what}: code {rc}: {msg}")
+
+
+def _ptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise TypeError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(_dp)
+
+
+class Context:
+    """One simulation resident on one GPU (a hydro task of the reference).
+
+    Field arrays use the reference layout: a numpy array of shape
+    (nfields, nz, ny, nx+2) in C order is exactly Fortran's fields(nx+2, ny, nz, nfields).
+    """
+
+    STAT_KEYS = ["energy", "eps_v", "eta", "etakmax", "uvar", "x_length", "lambda", "re_lambda",
+                 "re_lambda1", "tau_e", "enstrophy", "skewness"]
+
+    def __init__(self, params: Params):
+        self.params = params
+        self.n = params.nx
+        self.nfields = 3 + params.n_scalars
+        self.kmax = params.kmax
+        h = C.c_void_p()
+        cp = params.to_c()
+        _check(lib().hit3d_gpu_init(C.byref(cp), C.byref(h)), "hit3d_gpu_init")
+        self._h = h
+        self.fov = 1
+        self.fos = 1
+        self.courant = 0.0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().hit3d_gpu_finalize(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def field_shape(self, nf=None):
+        return (self.nfields if nf is None else nf, self.n, self.n, self.n + 2)
+
+    def upload_fields(self, fields: np.ndarray):
+        nf = fields.shape[0]
+        _check(lib().hit3d_gpu_upload_fields(self._h, _ptr(fields), self.n + 2, nf), "upload_fields")
+
+    def download_fields(self, nf=None) -> np.ndarray:
+        out = np.empty(self.field_shape(nf))
+        _check(lib().hit3d_gpu_download_fields(self._h, _ptr(out), self.n + 2, out.shape[0]), "download_fields")
+        return out
+
+    def upload_rhs_old(self, r: np.ndarray):
+        _check(lib().hit3d_gpu_upload_rhs_old(self._h, _ptr(r), self.n + 2, r.shape[0]), "upload_rhs_old")
+
+    def download_rhs_old(self, nf=None) -> np.ndarray:
+        out = np.empty(self.field_shape(nf))
+        _check(lib().hit3d_gpu_download_rhs_old(self._h, _ptr(out), self.n + 2, out.shape[0]), "download_rhs_old")
+        return out
+
+    def step(self, nsteps: int = 1) -> float:
+        fov, fos, cour = C.c_int32(self.fov), C.c_int32(self.fos), C.c_double(0.0)
+        _check(lib().hit3d_gpu_step(self._h, int(nsteps), C.byref(fov), C.byref(fos), C.byref(cour)), "step")
+        self.fov, self.fos, self.courant = fov.value, fos.value, cour.value
+        return self.courant
+
+    def set_dt(self, dt: float):
+        _check(lib().hit3d_gpu_set_dt(self._h, float(dt)), "set_dt")
+        self.params.dt = dt
+
+    def set_scalars_active(self, on: bool):
+        _check(lib().hit3d_gpu_set_scalars_active(self._h, int(bool(on))), "set_scalars_active")
+
+    def dealias_all(self):
+        _check(lib().hit3d_gpu_dealias_all(self._h), "dealias_all")
+
+    def init_velocity(self, rn1: float, isp_type: int = 1, peak_wavenum: float = 4.0, ir_exp: float = 2.0):
+        _check(lib().hit3d_gpu_init_velocity(self._h, float(rn1), int(isp_type), float(peak_wavenum),
+                                             float(ir_exp)), "init_velocity")
+
+    def stats(self):
+        es = np.zeros(self.kmax)
+        out = np.zeros(12)
+        _check(lib().hit3d_gpu_stats(self._h, _ptr(es), self.kmax, _ptr(out)), "stats")
+        return es, dict(zip(self.STAT_KEYS, out.tolist()))
+
+    def scalar_stats(self, s: int):
+        sp = np.zeros(self.kmax)
+        out = np.zeros(5)
+        _check(lib().hit3d_gpu_scalar_stats(self._h, int(s), _ptr(sp), self.kmax, _ptr(out)), "scalar_stats")
+        return dict(spectrum=sp, diss=out[0], mean=out[1], variance=out[2], min=out[3], max=out[4])
+
+    def particles_upload(self, xyzp: np.ndarray, uvwp: np.ndarray | None = None, scheme: int = 1):
+        xyzp = np.ascontiguousarray(xyzp, dtype=np.float64)
+        u = None if uvwp is None else np.ascontiguousarray(uvwp, dtype=np.float64)
+        _check(lib().hit3d_gpu_particles_upload(self._h, _ptr(xyzp), None if u is None else _ptr(u),
+                                                xyzp.shape[0], int(scheme)), "particles_upload")
+        self._np = xyzp.shape[0]
+
+    def particles_download(self):
+        x = np.zeros((self._np, 3))
+        u = np.zeros((self._np, 3))
+        _check(lib().hit3d_gpu_particles_download(self._h, _ptr(x), _ptr(u)), "particles_download")
+        return x, u
+
+    def xfft3d(self, flag: int, a: np.ndarray) -> np.ndarray:
+        """xFFT3d on one (nz, ny, nx+2) host array; returns a new array."""
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        out = np.zeros_like(a)
+        _check(lib().hit3d_gpu_xfft3d(self._h, int(flag), _ptr(a), _ptr(out), self.n + 2), "xfft3d")
+        return out
+
+    def filter_field(self, kind: int, delta: float, field: int):
+        _check(lib().hit3d_gpu_filter_field(self._h, int(kind), float(delta), int(field)), "filter_field")
+
+    def physical_velocity(self) -> np.ndarray:
+        out = np.zeros((3, self.n, self.n, self.n + 2))
+        _check(lib().hit3d_gpu_physical_velocity(self._h, _ptr(out), self.n + 2), "physical_velocity")
+        return out

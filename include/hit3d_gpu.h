@@ -1,0 +1,145 @@
+/*
+ * hit3d_gpu.h -- C-ABI of the B200 pseudospectral step for HIT3DP.
+ *
+ * The reference has no plugin API: its hot path is a set of argument-less
+ * Fortran subroutines acting on module globals (call sites main.f90:124-167).
+ * Each entry point below replaces one of those calls or module set-ups, takes
+ * plain pointers and fixed-width integers (the reference compiles with -i8 -r8,
+ * Makefile:11-12,53-56, so a binding must use c_int32_t/c_int64_t/c_double
+ * explicitly, never default INTEGER/REAL), and returns 0 on success or a
+ * negative code; hit3d_gpu_last_error() then describes the failure (the
+ * reference's equivalent is call my_exit(-1), my_exit.f90:23-62).
+ *
+ * Layouts at the boundary are the reference's:
+ *   fields(nx+2, ny, nz, nfields) real*8, column-major.  Fourier space is
+ *   (kx re/im interleaved, kz, ky) (x_fftw.f90:321-327); physical space is
+ *   (x, y, z) with two padding entries per x row.
+ * Inside the library the state lives in HBM in a transposed, row-padded layout;
+ * it is converted only on upload/download.
+ *
+ * One context = one simulation on one GPU, driven from one host thread, on one
+ * CUDA stream.  Contexts are independent; calls on one context are not
+ * thread-safe.
+ */
+#ifndef HIT3D_GPU_H
+#define HIT3D_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hit3d_ctx hit3d_ctx;
+
+#define HIT3D_MAX_SCALARS 8
+
+/* Run parameters; the values the reference reads from <run_name>.in
+ * (m_parameters.f90:172-512) and derives at start-up. */
+typedef struct hit3d_params {
+    int32_t nx;          /* cubic grid size N = nx = ny = nz_all (m_parameters.f90:202)  */
+    int32_t dealias;     /* 0: 2/3 rule, 1: phase shift + truncation (m_parameters.f90:330) */
+    int32_t flow_type;   /* 0: decaying, 1: forced (m_parameters.f90:264)                 */
+    int32_t force_type;  /* 1: Machiels band forcing (m_force.f90:158)                     */
+    int32_t kfmax;       /* forced shells 1..kfmax (m_parameters.f90:309)                  */
+    int32_t n_scalars;   /* passive scalars, <= HIT3D_MAX_SCALARS (m_parameters.f90:424)   */
+    int32_t precision;   /* 0: FP64 transforms; 1: FP32 nonlinear-term transforms with FP64
+                            state, integrator and reductions (no reference counterpart)    */
+    int32_t les_model;   /* 0: none; 1: Smagorinsky (m_les.f90:94-106)                     */
+    int32_t scalar_type[HIT3D_MAX_SCALARS]; /* 0 = uniform mean gradient source            */
+    int32_t device;      /* CUDA device ordinal                                            */
+    int32_t reserved;
+    double nu;           /* 1/RE (m_parameters.f90:275)                                    */
+    double dt;           /* time step > 0 (m_parameters.f90:277-284)                       */
+    double famp;         /* FAMP (m_parameters.f90:312)                                    */
+    double c_smag;       /* Smagorinsky constant; the reference hard-codes 0.18 (m_les.f90:1148) */
+    double sc[HIT3D_MAX_SCALARS]; /* Schmidt numbers; PE = nu/sc (m_parameters.f90:451)    */
+} hit3d_params;
+
+/* Allocate the device state, transform plans and wavenumber tables.
+ * Replaces m_fields_init, m_work_init, x_fftw_allocate(1), x_fftw_init and
+ * m_force_init (main.f90:27-36; x_fftw.f90:81-317; m_force.f90:13-97). */
+int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out);
+
+/* Release everything (x_fftw_allocate(-1), x_fftw.f90:134-142). */
+void hit3d_gpu_finalize(hit3d_ctx *ctx);
+
+/* Message of the last failure on this thread. */
+const char *hit3d_gpu_last_error(void);
+
+/* Copy nfields Fourier-space fields between the host array fields(ld1, ny, nz, nfields)
+ * (ld1 >= nx+2 reals) and the device.  nfields = 3 + n_scalars covers the state of
+ * m_fields.f90:21.  Used where the reference reads or writes `fields` on the host:
+ * begin_new/begin_restart (main.f90:56-60), restart_write_parallel (main.f90:173). */
+int hit3d_gpu_upload_fields(hit3d_ctx *ctx, const double *fields, int64_t ld1, int32_t nfields);
+int hit3d_gpu_download_fields(hit3d_ctx *ctx, double *fields, int64_t ld1, int32_t nfields);
+
+/* Same for the AB2 history rhs_old (m_work.f90:109), so that a run can be moved
+ * between host and device without restarting the integrator. */
+int hit3d_gpu_upload_rhs_old(hit3d_ctx *ctx, const double *rhs_old, int64_t ld1, int32_t nfields);
+int hit3d_gpu_download_rhs_old(hit3d_ctx *ctx, double *rhs_old, int64_t ld1, int32_t nfields);
+
+/* Advance nsteps time steps, all on the device: rhs_scalars, AB2 scalars,
+ * rhs_velocity (2/3 rule or phase shift, + Smagorinsky), force_velocity, AB2
+ * velocities, pressure (main.f90:124-167).  *fov / *fos are the reference's
+ * first-order flags (main.f90:71-72): non-zero means "take an Euler step"; both
+ * are cleared on return as the reference clears them.  *courant receives the
+ * Courant number of the last step (rhs_velocity.f90:31-38).  Particles, if
+ * uploaded, move with the level-n velocity of every step (main.f90:235-247). */
+int hit3d_gpu_step(hit3d_ctx *ctx, int32_t nsteps, int32_t *fov, int32_t *fos, double *courant);
+
+/* Change dt (my_dt.f90) and start/stop advancing scalars (int_scalars, main.f90:199-204). */
+int hit3d_gpu_set_dt(hit3d_ctx *ctx, double dt);
+int hit3d_gpu_set_scalars_active(hit3d_ctx *ctx, int32_t active);
+
+/* Zero every mode with some |k_i| > kmax (dealias_all.f90:97-131). */
+int hit3d_gpu_dealias_all(hit3d_ctx *ctx);
+
+/* Initial velocity (init_velocity.f90:1-246): RANDu stream seeded with rn1 and
+ * Box-Muller on the host (bit-exact with the reference), transform, curl and
+ * shell rescale on the device.  isp_type -1 Taylor-Green, 0 Kolmogorov,
+ * 1 exponential (peak_wavenum), 3 von Karman as the reference; 2 =
+ * k^ir_exp exp(-2 (k/peak_wavenum)^2), a spectrum the reference does not have. */
+int hit3d_gpu_init_velocity(hit3d_ctx *ctx, double rn1, int32_t isp_type, double peak_wavenum, double ir_exp);
+
+/* Velocity statistics (m_stats.f90:99-289): e_spec[0..kmax) and
+ * out[12] = energy, eps_v, eta, etakmax, uvar, x_length, lambda, re_lambda,
+ * re_lambda1, tau_e, enstrophy, and the velocity-derivative skewness
+ * (mean over a of <(du_a/dx_a)^3>/<(du_a/dx_a)^2>^{3/2}; no reference counterpart). */
+int hit3d_gpu_stats(hit3d_ctx *ctx, double *e_spec, int32_t kmax, double *out12);
+
+/* Scalar statistics for scalar s (m_stats.f90:295-440): spectrum[0..kmax)
+ * (already doubled like the reference) and out5 = dissipation, mean, variance,
+ * min, max. */
+int hit3d_gpu_scalar_stats(hit3d_ctx *ctx, int32_t s, double *spectrum, int32_t kmax, double *out5);
+
+/* Lagrangian particles (m_particles.f90:157-337, 815-1230).  xyzp(3, np) in the
+ * reference's grid units (x/dx + 1); uvwp(3, np) starts at -999 (Euler first
+ * step).  scheme 0 = trilinear, 1 = 4-point cubic (CINT).  The whole field is
+ * resident, so the slab halos and migration of the reference become periodic
+ * wrap-around on one slab. */
+int hit3d_gpu_particles_upload(hit3d_ctx *ctx, const double *xyzp, const double *uvwp, int64_t np, int32_t scheme);
+int hit3d_gpu_particles_download(hit3d_ctx *ctx, double *xyzp, double *uvwp);
+
+/* One 3-D transform of a single host array in the reference layout
+ * (xFFT3d(flag, n), x_fftw.f90:852-1085): flag 1 physical -> Fourier
+ * (unnormalised), flag -1 Fourier -> physical (times 1/N^3).  in and out are
+ * (ld1, ny, nz) host arrays and may alias. */
+int hit3d_gpu_xfft3d(hit3d_ctx *ctx, int32_t flag, const double *in, double *out, int64_t ld1);
+
+/* Filter Fourier-space field `field` of the state in place
+ * (filter_xfftw_fields, m_filter_xfftw.f90:74-110).  kind 2 = Gaussian kernel
+ * built in physical space and transformed as the reference does
+ * (m_filter_xfftw.f90:197-220); kind 4 = box filter of width delta, transfer
+ * function prod sin(k delta/2)/(k delta/2) (no reference counterpart). */
+int hit3d_gpu_filter_field(hit3d_ctx *ctx, int32_t kind, double delta, int32_t field);
+
+/* Physical-space velocity (x, y, z) of the current state, as the reference's
+ * wrk1..3 after rhs_scalars (main.f90:126): out(ld1, ny, nz, 3). */
+int hit3d_gpu_physical_velocity(hit3d_ctx *ctx, double *out, int64_t ld1);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HIT3D_GPU_H */

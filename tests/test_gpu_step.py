@@ -1,0 +1,150 @@
+"""Whole-step parity of the CUDA path against the oracle (main.f90:124-170):
+rhs_scalars -> AB2 scalars -> rhs_velocity -> force_velocity -> AB2 -> pressure.
+
+Tolerance: 1e-10 relative on the Fourier-space fields (FP64 transforms differ
+from the oracle's only by rounding; the differences grow slowly with steps)."""
+import numpy as np
+import pytest
+
+from _cases import RN1, make_pair, relerr, seed_scalars
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def _compare(o, g, nf, tol=TOL):
+    f = g.download_fields()
+    for m in range(nf):
+        e = relerr(f[m], o.fields[m])
+        assert e < tol, f"field {m}: relative error {e:.3e}"
+
+
+@pytest.mark.parametrize("n,isp", [(32, 1), (64, 1), (48, 2), (32, 0), (32, 3), (32, -1)])
+def test_init_velocity_matches_oracle(n, isp):
+    o, g = make_pair(n, isp_type=isp, init="gpu")
+    import oracle
+    o2 = oracle.Oracle(n)
+    o2.init_velocity(RN1, isp_type=isp, peak_wavenum=4.0, ir_exp=2.0)
+    o2.dealias_all()
+    f = g.download_fields()
+    for m in range(3):
+        assert relerr(f[m], o2.fields[m]) < 1e-12
+    # solenoidal and unit energy (isp != -1)
+    es, st = g.stats()
+    if isp != -1:
+        assert abs(st["energy"] - 1.0) < 1e-12
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_decaying_two_thirds(n):
+    o, g = make_pair(n, dealias=0, flow_type=0, nu=1.0 / 400.0, dt=0.005)
+    for _ in range(2):
+        o.step(5)
+        g.step(5)
+        _compare(o, g, 3)
+    assert abs(g.courant - o.courant) < 1e-12 * max(1.0, o.courant)
+
+
+def test_forced_two_thirds():
+    o, g = make_pair(32, dealias=0, flow_type=1, kfmax=2, famp=0.5, nu=1.0 / 100.0, dt=0.005)
+    o.step(10)
+    g.step(10)
+    _compare(o, g, 3)
+
+
+def test_forcing_band_energy():
+    """Energy in the forcing band (m_force.f90:258-284) agrees with the oracle."""
+    o, g = make_pair(32, dealias=0, flow_type=1, kfmax=2)
+    assert o.nforced() > 0
+    e_or = o.forcing_energy()
+    es, _ = g.stats()
+    assert abs(es[0] + es[1] - e_or) <= 1e-13 * e_or
+
+
+@pytest.mark.parametrize("dealias", [0, 1])
+def test_forced_with_scalars(dealias):
+    rng = np.random.default_rng(3)
+    o, g = make_pair(32, dealias=dealias, flow_type=1, kfmax=2, nu=1.0 / 200.0, dt=0.004, nscal=2,
+                     sc=(0.7, 1.0), scalar_type=(0, 1))
+    seed_scalars(o, g, 2, rng)
+    o.step(6)
+    g.step(6)
+    _compare(o, g, 5)
+
+
+def test_phase_shift_decaying_64():
+    o, g = make_pair(64, dealias=1, flow_type=0, nu=1.0 / 400.0, dt=0.005)
+    o.step(5)
+    g.step(5)
+    _compare(o, g, 3)
+
+
+def test_smagorinsky_les():
+    o, g = make_pair(32, dealias=0, flow_type=1, kfmax=2, nu=1.0 / 6000.0, dt=0.004, les_model=1, c_smag=0.18)
+    o.step(6)
+    g.step(6)
+    _compare(o, g, 3)
+
+
+def test_rhs_old_round_trip():
+    o, g = make_pair(32)
+    g.step(2)
+    r = g.download_rhs_old()
+    g.upload_rhs_old(r)
+    assert np.array_equal(g.download_rhs_old(), r)
+
+
+def test_stats_match_oracle():
+    o, g = make_pair(64, dealias=0, flow_type=0)
+    o.step(4)
+    g.step(4)
+    es_o, st_o = o.stats()
+    es_g, st_g = g.stats()
+    assert relerr(es_g, es_o) < 1e-10
+    for k in st_o:
+        assert abs(st_g[k] - st_o[k]) <= 1e-9 * max(1.0, abs(st_o[k])), k
+
+
+def test_scalar_stats_match_oracle():
+    rng = np.random.default_rng(5)
+    o, g = make_pair(32, dealias=0, flow_type=1, nscal=1, sc=(0.7,), scalar_type=(0,))
+    seed_scalars(o, g, 1, rng)
+    o.step(3)
+    g.step(3)
+    so = o.scalar_stats()[0]
+    sg = g.scalar_stats(0)
+    assert relerr(sg["spectrum"], so["spectrum"]) < 1e-10
+    for k in ("diss", "mean", "variance", "min", "max"):
+        assert abs(sg[k] - so[k]) <= 1e-9 * max(1.0, abs(so[k])), k
+
+
+def test_dealias_all_matches():
+    import oracle
+    o = oracle.Oracle(32, dealias=1)
+    rng = np.random.default_rng(1)
+    o.fields[:] = rng.standard_normal(o.fields.shape)
+    from hit3d_b200 import Context, Params
+    g = Context(Params(nx=32, dealias=1))
+    g.upload_fields(np.ascontiguousarray(o.fields))
+    o.dealias_all()
+    g.dealias_all()
+    assert np.array_equal(g.download_fields(), o.fields)
+
+
+def test_physical_velocity_matches_oracle():
+    o, g = make_pair(32)
+    up = g.physical_velocity()
+    for c in range(3):
+        a = np.ascontiguousarray(o.fields[c]).copy()
+        o.fft3d(-1, a)
+        assert relerr(up[c][:, :, :32], a[:, :, :32]) < 1e-13
+
+
+def test_filter_gaussian_matches_oracle():
+    o, g = make_pair(32)
+    delta = 4 * 2 * np.pi / 32
+    gf = o.filter_g(2, delta)
+    a = np.ascontiguousarray(o.fields[0]).copy()
+    o.apply_filter(gf, a)
+    g.filter_field(2, delta, 0)
+    assert relerr(g.download_fields()[0], a) < 1e-12
