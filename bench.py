@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Benchmark of the HIT3DP pseudospectral timestep on B200.
+
+Workload: forced DNS on a 512^3 grid (flow_type=1, Machiels band forcing KFMAX=2,
+FAMP=0.5), Re = 3000, fixed dt, 2/3-rule dealiasing, FP64 spectral state, no
+scalars or particles; initial velocity from the reference's RANDu/Box-Muller
+generator (RN1 of scripts/00_example.in) shaped to E(k) ~ k^2 exp(-2 (k/4)^2).
+Data are synthetic (generated in place); every field is ~1.1 GB, far larger than
+the 126 MB L2, so no flush is needed between steps.
+
+`value` = timesteps/s of the FP64 path with the state resident in HBM, timed
+with CUDA events on the library's stream; `e2e` = the same through the C-ABI
+with the host owning the fields (pinned host -> device upload, step, device ->
+host download every step).  The FP32-nonlinear-term form is timed on the same
+initial state and its E(k) is compared with the FP64 run.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank advances its own independent replica (the
+single-GPU path does not shard); value = all ranks' steps / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT = 512
+RE = 3000.0
+DT = 0.001
+RN1 = 67748937.0
+METRIC = "timesteps/s at 512^3 FP64 (forced DNS, 2/3 rule)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-transform form")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_context(n, precision, device):
+    from hit3d_b200 import Context, Params
+    p = Params(nx=n, dealias=0, flow_type=1, force_type=1, kfmax=2, famp=0.5, nu=1.0 / RE, dt=DT,
+               precision=precision, device=device)
+    return Context(p)
+
+
+# algorithmic bytes per step of each stage, in units of one unpadded complex
+# half-spectrum field B1 = N^2 (N/2+1) * 16 bytes (FP64) -- velocity only, 2/3 rule
+STAGE_UNITS = {
+    0: {"z_inverse": 6, "y_inverse": 6, "x_fused": 9, "y_forward": 12, "z_forward": 12, "update": 18},
+    1: {"z_inverse": 4.5, "y_inverse": 3, "x_fused": 4.5, "y_forward": 6, "z_forward": 6, "update": 15},
+}
+# single launches per step of each stage (velocity only, 2/3 rule)
+STAGE_LAUNCHES = {"z_inverse": 1, "y_inverse": 1, "x_fused": 1, "y_forward": 1, "z_forward": 1, "update": 1}
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of each stage from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def timed_steps(torch, ctx, steps):
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    ctx.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1000.0
+
+
+def cpu_sample(n_gpu, fields0):
+    """Oracle (C/OpenMP FP64 restatement) on the host cores: one step at 256^3 if
+    the workload is 512^3, scaled by the N^3 log N work ratio to the 512^3 unit."""
+    import oracle
+    cores = os.cpu_count() or 1
+    n_s = 256 if n_gpu >= 256 else n_gpu
+    o = oracle.Oracle(n_s, nscal=0, dealias=0, flow_type=1, kfmax=2, nu=1.0 / RE, dt=DT, famp=0.5)
+    o.init_velocity(RN1, isp_type=2, peak_wavenum=4.0, ir_exp=2.0)
+    o.dealias_all()
+    o.step(1)  # warm-up: page in and first-order step
+    t0 = time.perf_counter()
+    nst = 0
+    while True:
+        o.step(1)
+        nst += 1
+        el = time.perf_counter() - t0
+        if el > 10.0 or nst >= 5:
+            break
+    rate = nst / el
+    scale = (n_gpu ** 3 * np.log2(n_gpu ** 3)) / (n_s ** 3 * np.log2(n_s ** 3))
+    return {"value": rate / scale, "unit": "timesteps/s", "cores": cores, "kind": "port",
+            "sample": f"{nst} oracle steps at {n_s}^3 ({el:.1f} s, OpenMP on {cores} threads), scaled by the "
+                      f"N^3 log2 N^3 work ratio {scale:.2f} to {n_gpu}^3"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    cs = cpu_sample(args.n, None)
+    line = {"impl": "reference", "metric": METRIC, "value": cs["value"], "unit": "timesteps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"forced DNS {args.n}^3, Re={RE:g}, dt={DT}, 2/3 rule, KFMAX=2, FAMP=0.5",
+                       "grid": args.n},
+            "cpu_baseline": cs,
+            "e2e": {"value": cs["value"], "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    n = args.n
+    B1 = n * n * (n // 2 + 1) * 16.0
+    peak, peak_kind = peaks()
+
+    ctx = make_context(n, 0, local)
+    ctx.init_velocity(RN1, 2, 4.0, 2.0)
+    ctx.dealias_all()
+    fields0 = ctx.download_fields()
+
+    # warm-up, then the timed region
+    ctx.step(args.warmup)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launches
+    with ClockSampler(local) as clk:
+        t = timed_steps(torch, ctx, args.steps)
+    launches = ctx.launches - launches0
+    if dist:
+        tt = torch.tensor([t], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    value = world * args.steps / t
+    ms = 1000.0 * t / args.steps
+    es64, st64 = ctx.stats()
+
+    # per-stage device time (separate, untimed steps) -> roofline of the dominant stage
+    prof = ctx.step_profile(3)
+    prof = {k: v / 3 for k, v in prof.items()}
+    units = STAGE_UNITS[0]
+    top = max(units, key=lambda k: prof.get(k, 0.0))
+    ach = units[top] * B1 / (prof[top] / 1000.0) / 1e9
+    traffic = load_traffic().get(f"{n}:{top}")
+    stage_gbs = {k: round(units[k] * B1 / (prof[k] / 1000.0) / 1e9, 1) for k in units if prof.get(k, 0) > 0}
+    ideal = 240.0 * n ** 3  # bytes per step of the ideal single-pass model
+    # e2e through the C-ABI with host-owned fields
+    e2e = None
+    if not args.no_e2e:
+        h = torch.empty(fields0.size, dtype=torch.float64).pin_memory()
+        hv = h.numpy().reshape(fields0.shape)
+        hv[:] = fields0
+        ho = torch.empty(fields0.size, dtype=torch.float64).pin_memory()
+        hov = ho.numpy().reshape(fields0.shape)
+        ctx.upload_fields(hv)
+        ctx.step(1)
+        stream = torch.cuda.ExternalStream(ctx.stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            ctx.upload_fields(hv)
+            ctx.step(1)
+            out = ctx.download_fields(out=hov)
+        e1.record(stream)
+        e1.synchronize()
+        te = e0.elapsed_time(e1) / 1000.0
+        if dist:
+            tt = torch.tensor([te], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        nbytes = fields0.nbytes
+        e2e = {"value": world * args.e2e_steps / te, "unit": "timesteps/s", "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps}
+        del out
+    ctx.close()
+
+    # FP32 nonlinear-term transforms, same initial state and step count
+    fp32 = None
+    if not args.no_fp32:
+        c32 = make_context(n, 1, local)
+        c32.upload_fields(fields0)
+        c32.step(args.warmup)
+        if dist:
+            dist.barrier()
+        t32 = timed_steps(torch, c32, args.steps)
+        if dist:
+            tt = torch.tensor([t32], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t32 = float(tt.item())
+        es32, st32 = c32.stats()
+        prof32 = c32.step_profile(3)
+        mask = es64 > 1e-12 * es64.max()
+        ek_err = float(np.max(np.abs(es32[mask] - es64[mask]) / es64[mask]))
+        fp32 = {"value": world * args.steps / t32, "unit": "timesteps/s", "speedup_vs_fp64": (world * args.steps / t32) / value,
+                "ek_max_rel_err_vs_fp64": ek_err, "eps_rel_err": abs(st32["eps_v"] - st64["eps_v"]) / st64["eps_v"],
+                "skew_abs_err": abs(st32["skewness"] - st64["skewness"]),
+                "stage_ms": {k: round(v / 3, 3) for k, v in prof32.items() if v > 0}}
+        c32.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_sample(n, fields0)
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "error": str(e)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"forced DNS {n}^3, Re={RE:g}, dt={DT}, 2/3 rule, KFMAX=2, FAMP=0.5, "
+                                   "E(k)~k^2 exp(-2(k/4)^2) RANDu init",
+                       "grid": n, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs > L2 (1.1 GB per field), no flush"},
+            "grid_points_steps_per_s": value * n ** 3,
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "peak_kind": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": units[top] * B1},
+            "step_roofline": {"ideal_bytes_per_step": ideal, "achieved_GBs": ideal / (ms / 1000.0) / 1e9,
+                              "frac_of_peak": ideal / (ms / 1000.0) / 1e9 / peak},
+            "stage_ms": {k: round(v, 3) for k, v in prof.items() if v > 0},
+            "stage_GBs": stage_gbs,
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "fp32_fft": fp32,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

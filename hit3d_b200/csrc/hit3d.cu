@@ -32,7 +32,12 @@ int h3d_set_error_msg(int code, const char *msg)
 }
 extern "C" const char *hit3d_gpu_last_error(void) { return g_err.c_str(); }
 
-#define H3D_LAUNCH_CHECK() H3D_CHECK(cudaGetLastError())
+// every launch site has the context `c` in scope and counts its kernels
+#define H3D_LAUNCH_CHECK()                 \
+    do {                                   \
+        c->nlaunch++;                      \
+        H3D_CHECK(cudaGetLastError());     \
+    } while (0)
 #define H3D_TRY(x)            \
     do {                      \
         int rc__ = (x);       \
@@ -109,6 +114,7 @@ struct hit3d_ctx {
     int int_scalars;
     double dx;
     int pblocks;
+    int64_t nlaunch;
 };
 
 static int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
@@ -258,9 +264,31 @@ static int inv_from_state(hit3d_ctx *c, int nf, int mode, int sfield, const doub
 }
 
 // ---------------------------------------------------------------------------
+// optional per-stage event markers (hit3d_gpu_step_profile)
+// ---------------------------------------------------------------------------
+struct Prof {
+    static constexpr int MAXM = 64;
+    cudaEvent_t ev[MAXM];
+    int stage[MAXM];
+    int n = 0;
+    void mark(cudaStream_t st, int s)
+    {
+        if (n < MAXM) {
+            cudaEventRecord(ev[n], st);
+            stage[n] = s;
+            n++;
+        }
+    }
+};
+#define MARK(s) \
+    do {        \
+        if (prof) prof->mark(c->st, (s)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
 // one time step
 // ---------------------------------------------------------------------------
-template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_s)
+template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_s, Prof *prof = nullptr)
 {
     const hit3d_params &p = c->p;
     cx<T> *W = reinterpret_cast<cx<T> *>(c->W);
@@ -278,6 +306,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     a.flow_type = p.flow_type; a.kfmax = p.kfmax; a.famp = p.famp; a.fenergy = c->d_fen; a.nscal = ns;
     for (int s = 0; s < c->nsc; s++) { a.pe[s] = p.nu / p.sc[s]; a.stype[s] = p.scalar_type[s]; }
 
+    MARK(7);
     if (p.flow_type == 1) {
         k_forcing_energy<<<1, 32, 0, c->st>>>(c->n, c->P64, c->fs64, p.kfmax, c->U, c->d_fen);
         H3D_LAUNCH_CHECK();
@@ -285,11 +314,14 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     const int npass = p.dealias == 1 ? 2 : 1;
     for (int pass = 0; pass < npass; pass++) {
         const int mode = pass == 0 ? PRE_COPY : PRE_SHIFT;
+        MARK(0);
         H3D_TRY(zinv<T>(c, 3, mode, 0, c->U, c->fs64, Wf(0), wfs, wp));
         for (int s = 0; s < ns; s++)
             H3D_TRY(zinv<T>(c, 1, mode, 0, c->U + (3 + s) * c->fs64, c->fs64, Wf(6 + 3 * s), wfs, wp));
+        MARK(1);
         H3D_TRY(spass<T>(c, 1, false, Wf(0), wfs, wp, 3));
         for (int s = 0; s < ns; s++) H3D_TRY(spass<T>(c, 1, false, Wf(6 + 3 * s), wfs, wp, 1));
+        MARK(2);
         if (pass == 0) H3D_CHECK(cudaMemsetAsync(c->d_cmax, 0, sizeof(unsigned long long), c->st));
         for (int s = 0; s < ns; s++) {
             FusedArgs fa;
@@ -314,17 +346,21 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
             H3D_TRY((xfused<T, OpVel>(c, fa)));
         }
         if (pass == 0 && c->np > 0) {
+            MARK(7);
             PartArgs pa;
             pa.n = c->n; pa.scheme = c->pscheme; pa.np = c->np; pa.dt = p.dt; pa.dx = c->dx;
             pa.U = c->phys; pa.fs = (int64_t)c->n * c->n * c->n; pa.xyz = c->d_xyz; pa.uvw = c->d_uvw;
             k_particles<<<(unsigned)((c->np + 255) / 256), 256, 0, c->st>>>(pa);
             H3D_LAUNCH_CHECK();
         }
+        MARK(3);
         H3D_TRY(spass<T>(c, 1, true, Wf(0), wfs, wp, nprod));
+        MARK(4);
         H3D_TRY(spass<T>(c, 2, true, Wf(0), wfs, wp, nprod));
 
         const cx<T> *tau = nullptr;
         if (les) {
+            MARK(6);
             // Smagorinsky stress from the same state (m_les.f90:1142-1215, 902-1018)
             const int t0 = nprod;
             H3D_TRY(zinv<T>(c, 3, PRE_STRAIN_A, 0, c->U, c->fs64, Wf(t0), wfs, wp));
@@ -342,6 +378,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
             tau = Wf(t0);
         }
 
+        MARK(5);
         if (p.dealias == 0) {
             for (int s = 0; s < ns; s++) {
                 k_scalar<T><<<pw_grid(c), 256, 0, c->st>>>(a, 0, s, c->dx, Wf(6 + 3 * s), nullptr, c->U,
@@ -368,6 +405,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
             H3D_LAUNCH_CHECK();
         }
     }
+    MARK(7);
     return 0;
 }
 
@@ -596,6 +634,38 @@ extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_
         *courant = cm * c->p.dt / c->dx;
     }
     H3D_CHECK(cudaGetLastError());
+    return 0;
+}
+
+extern "C" void *hit3d_gpu_stream(hit3d_ctx *c) { return c ? (void *)c->st : nullptr; }
+extern "C" int64_t hit3d_gpu_launch_count(hit3d_ctx *c) { return c ? c->nlaunch : -1; }
+
+extern "C" int hit3d_gpu_step_profile(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_t *fos, double *ms)
+{
+    if (!c || !ms) return h3d_set_error_msg(-1, "hit3d_gpu_step_profile: null argument");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    Prof prof;
+    for (int i = 0; i < Prof::MAXM; i++) H3D_CHECK(cudaEventCreate(&prof.ev[i]));
+    int ev = fov ? (*fov != 0) : 0, es = fos ? (*fos != 0) : 0;
+    int rc = 0;
+    for (int it = 0; it < nsteps && rc == 0; it++) {
+        prof.n = 0;
+        rc = c->p.precision == 0 ? step_once<double>(c, ev, es, &prof) : step_once<float>(c, ev, es, &prof);
+        if (rc) break;
+        ev = 0;
+        if (c->int_scalars) es = 0;
+        cudaError_t e = cudaEventSynchronize(prof.ev[prof.n - 1]);
+        if (e != cudaSuccess) { rc = h3d_set_error(e, "cudaEventSynchronize", __FILE__, __LINE__); break; }
+        for (int i = 0; i + 1 < prof.n; i++) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, prof.ev[i], prof.ev[i + 1]);
+            ms[prof.stage[i]] += t;
+        }
+    }
+    for (int i = 0; i < Prof::MAXM; i++) cudaEventDestroy(prof.ev[i]);
+    if (rc) return rc;
+    if (fov) *fov = ev;
+    if (fos) *fos = es;
     return 0;
 }
 

@@ -91,6 +91,9 @@ SIGNATURES = [
     ("hit3d_gpu_upload_rhs_old", C.c_int, [_vp, _dp, _i64, _i32]),
     ("hit3d_gpu_download_rhs_old", C.c_int, [_vp, _dp, _i64, _i32]),
     ("hit3d_gpu_step", C.c_int, [_vp, _i32, C.POINTER(_i32), C.POINTER(_i32), _dp]),
+    ("hit3d_gpu_stream", C.c_void_p, [_vp]),
+    ("hit3d_gpu_launch_count", C.c_int64, [_vp]),
+    ("hit3d_gpu_step_profile", C.c_int, [_vp, _i32, C.POINTER(_i32), C.POINTER(_i32), _dp]),
     ("hit3d_gpu_set_dt", C.c_int, [_vp, _d]),
     ("hit3d_gpu_set_scalars_active", C.c_int, [_vp, _i32]),
     ("hit3d_gpu_dealias_all", C.c_int, [_vp]),
@@ -183,8 +186,9 @@ class Context:
         nf = fields.shape[0]
         _check(lib().hit3d_gpu_upload_fields(self._h, _ptr(fields), self.n + 2, nf), "upload_fields")
 
-    def download_fields(self, nf=None) -> np.ndarray:
-        out = np.empty(self.field_shape(nf))
+    def download_fields(self, nf=None, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.field_shape(nf))
         _check(lib().hit3d_gpu_download_fields(self._h, _ptr(out), self.n + 2, out.shape[0]), "download_fields")
         return out
 
@@ -201,6 +205,27 @@ class Context:
         _check(lib().hit3d_gpu_step(self._h, int(nsteps), C.byref(fov), C.byref(fos), C.byref(cour)), "step")
         self.fov, self.fos, self.courant = fov.value, fos.value, cour.value
         return self.courant
+
+    STAGES = ["z_inverse", "y_inverse", "x_fused", "y_forward", "z_forward", "update", "smagorinsky", "other"]
+
+    def step_profile(self, nsteps: int = 1) -> dict:
+        """Advance nsteps and return device milliseconds per stage (events between stages)."""
+        fov, fos = C.c_int32(self.fov), C.c_int32(self.fos)
+        ms = np.zeros(8)
+        _check(lib().hit3d_gpu_step_profile(self._h, int(nsteps), C.byref(fov), C.byref(fos), _ptr(ms)),
+               "step_profile")
+        self.fov, self.fos = fov.value, fos.value
+        return dict(zip(self.STAGES, ms.tolist()))
+
+    @property
+    def launches(self) -> int:
+        """Kernels launched by this context so far."""
+        return int(lib().hit3d_gpu_launch_count(self._h))
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of this context (as an integer handle)."""
+        return lib().hit3d_gpu_stream(self._h) or 0
 
     def set_dt(self, dt: float):
         _check(lib().hit3d_gpu_set_dt(self._h, float(dt)), "set_dt")

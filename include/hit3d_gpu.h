@@ -88,6 +88,23 @@ int hit3d_gpu_download_rhs_old(hit3d_ctx *ctx, double *rhs_old, int64_t ld1, int
  * uploaded, move with the level-n velocity of every step (main.f90:235-247). */
 int hit3d_gpu_step(hit3d_ctx *ctx, int32_t nsteps, int32_t *fov, int32_t *fos, double *courant);
 
+/* The CUDA stream (cudaStream_t) every kernel of this context runs on, for
+ * callers that time or order work around the library (the reference's
+ * system_clock stage timers, m_timing.f90:48-73, x_fftw.f90:871-889). */
+void *hit3d_gpu_stream(hit3d_ctx *ctx);
+
+/* hit3d_gpu_step with CUDA events between the stages of every step;
+ * ms[0..8) accumulates device time per stage: 0 inverse z pass (with spectral
+ * pre-operation), 1 inverse y pass, 2 fused x pass (c2r, products, r2c),
+ * 3 forward y pass, 4 forward z pass, 5 RHS/forcing/AB2/pressure update,
+ * 6 Smagorinsky stress, 7 everything else (forcing energy, particles).  The
+ * replacement of the reference's benchmark counters bm(1..12)
+ * (main.f90:307-356). */
+int hit3d_gpu_step_profile(hit3d_ctx *ctx, int32_t nsteps, int32_t *fov, int32_t *fos, double *ms);
+
+/* Number of kernels this context has launched since hit3d_gpu_init. */
+int64_t hit3d_gpu_launch_count(hit3d_ctx *ctx);
+
 /* Change dt (my_dt.f90) and start/stop advancing scalars (int_scalars, main.f90:199-204). */
 int hit3d_gpu_set_dt(hit3d_ctx *ctx, double dt);
 int hit3d_gpu_set_scalars_active(hit3d_ctx *ctx, int32_t active);
