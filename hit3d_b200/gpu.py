@@ -104,6 +104,7 @@ SIGNATURES = [
     ("hit3d_gpu_particles_download", C.c_int, [_vp, _dp, _dp]),
     ("hit3d_gpu_xfft3d", C.c_int, [_vp, _i32, _dp, _dp, _i64]),
     ("hit3d_gpu_filter_field", C.c_int, [_vp, _i32, _d, _i32]),
+    ("hit3d_gpu_xfft3d_static", C.c_int, [_i32, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("hit3d_gpu_physical_velocity", C.c_int, [_vp, _dp, _i64]),
 ]
 

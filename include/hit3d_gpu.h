@@ -144,6 +144,22 @@ int hit3d_gpu_particles_download(hit3d_ctx *ctx, double *xyzp, double *uvwp);
  * (ld1, ny, nz) host arrays and may alias. */
 int hit3d_gpu_xfft3d(hit3d_ctx *ctx, int32_t flag, const double *in, double *out, int64_t ld1);
 
+/* Forward 3-D transform (as hit3d_gpu_xfft3d with flag 1) of one DEVICE array
+ * that allocates nothing, for callers that cannot call cudaMalloc (a host whose
+ * device memory is all handed out by its own pool allocator, or a loop that must
+ * not risk the device-wide synchronisation of cudaMalloc/cudaFree).  No
+ * counterpart in the reference.  `in` is a physical (nx+2, ny, nz) device array,
+ * `out` receives the Fourier (nx+2, ny, nz) array; both belong to the caller,
+ * must be 16-byte aligned and must not alias.  Work is queued on `stream`
+ * (a cudaStream_t, NULL = default stream) and the caller synchronises.  Grid
+ * sizes 32, 48, 64 and 128 only: the one scratch field lives in a file-scope
+ * __device__ array (17 MB, held on every GPU that loads the library until the
+ * process exits).  The first call on a device resolves that array's address and
+ * uploads twiddle tables, so make it before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race and must be serialised by the
+ * caller. */
+int hit3d_gpu_xfft3d_static(int32_t n, const double *in, double *out, void *stream);
+
 /* Filter Fourier-space field `field` of the state in place
  * (filter_xfftw_fields, m_filter_xfftw.f90:74-110).  kind 2 = Gaussian kernel
  * built in physical space and transformed as the reference does
