@@ -226,6 +226,7 @@ def main():
     ctx.init_velocity(RN1, 2, 4.0, 2.0)
     ctx.dealias_all()
     fields0 = ctx.download_fields()
+    variant, variant_ms = ctx.autotune()
 
     # warm-up, then the timed region
     ctx.step(args.warmup)
@@ -290,6 +291,7 @@ def main():
     if not args.no_fp32:
         c32 = make_context(n, 1, local)
         c32.upload_fields(fields0)
+        v32, v32_ms = c32.autotune()
         c32.step(args.warmup)
         if dist:
             dist.barrier()
@@ -305,7 +307,8 @@ def main():
         fp32 = {"value": world * args.steps / t32, "unit": "timesteps/s", "speedup_vs_fp64": (world * args.steps / t32) / value,
                 "ek_max_rel_err_vs_fp64": ek_err, "eps_rel_err": abs(st32["eps_v"] - st64["eps_v"]) / st64["eps_v"],
                 "skew_abs_err": abs(st32["skewness"] - st64["skewness"]),
-                "stage_ms": {k: round(v / 3, 3) for k, v in prof32.items() if v > 0}}
+                "stage_ms": {k: round(v / 3, 3) for k, v in prof32.items() if v > 0},
+                "tuned_variant": v32, "variant_ms": [round(x, 3) for x in v32_ms]}
         c32.close()
 
     cpu = None
@@ -333,6 +336,7 @@ def main():
                               "frac_of_peak": ideal / (ms / 1000.0) / 1e9 / peak},
             "stage_ms": {k: round(v, 3) for k, v in prof.items() if v > 0},
             "stage_GBs": stage_gbs,
+            "tuned_variant": variant, "variant_ms": [round(x, 3) for x in variant_ms],
             "clocks": clk.summary(),
             "e2e": e2e,
             "fp32_fft": fp32,

@@ -151,8 +151,22 @@ template <typename T, bool FWD> H3D_D cx<T> twid(const cx<T> *__restrict__ tw, i
 //   out[i*RL+m] : column c, position j + m*L/RL of butterfly b = tid + i*NT
 // The caller must __syncthreads() before reusing sm after this returns.
 // ---------------------------------------------------------------------------
-template <typename T, int L, int TC, int NT, bool ROWS, bool FWD, bool REV, int s>
-H3D_D void fft_mid_stage(cx<T> *sm, const cx<T> *__restrict__ tw)
+// Twiddle sources.  GlobalTw reads the table for every butterfly; CachedTw holds
+// the twiddles of this thread's butterflies in registers (they depend only on
+// the thread's fixed position in each stage, so a kernel that runs many
+// transforms with the same mapping loads them once).  Both return the forward
+// twiddle w^(k m) of stage s, butterfly slot i; conjugated for inverse transforms.
+template <typename T> struct GlobalTw {
+    const cx<T> *__restrict__ tw;
+    template <int L, int Ns, int R, bool FWD, int s>
+    H3D_D cx<T> get(int i, int m, int k) const
+    {
+        (void)i;
+        return twid<T, FWD>(tw, k * m * (L / (Ns * R)));
+    }
+};
+template <typename T, int L, int TC, int NT, bool ROWS, bool FWD, bool REV, int s, class TWS>
+H3D_D void fft_mid_stage(cx<T> *sm, const TWS &tws)
 {
     using P = Plan<L, REV>;
     using LY = Lay<L, TC, ROWS>;
@@ -170,7 +184,7 @@ H3D_D void fft_mid_stage(cx<T> *sm, const cx<T> *__restrict__ tw)
 #pragma unroll
             for (int m = 0; m < R; m++) {
                 cx<T> v = sm[LY::idx(c, j + m * nbpc)];
-                if (m > 0) v = cmul(v, twid<T, FWD>(tw, k * m * (L / (Ns * R))));
+                if (m > 0) v = cmul(v, tws.template get<L, Ns, R, FWD, s>(i, m, k));
                 a[i * R + m] = v;
             }
             dft<T, R, FWD>(a + i * R);
@@ -202,6 +216,48 @@ struct ColFFT {
     static constexpr int TOT0 = Cnt<L, TC, NT, R0>::total, TOTL = Cnt<L, TC, NT, RL>::total;
     static constexpr int NIN = NB0 * R0, NOUT = NBL * RL;
 
+    // register twiddle cache: stages 1..S-1, NB_s butterflies, R_s - 1 twiddles each
+    static H3D_HD constexpr int tw_count(int s)
+    {
+        return ((TC * (L / P::R(s)) + NT - 1) / NT) * (P::R(s) - 1);
+    }
+    static H3D_HD constexpr int tw_off(int s) { return s <= 1 ? 0 : tw_off(s - 1) + tw_count(s - 1); }
+    static constexpr int TWN = tw_off(S);
+    struct CachedTw {
+        cx<T> w[TWN > 0 ? TWN : 1];  // forward twiddles
+        template <int L_, int Ns, int R, bool FWD_, int s>
+        H3D_D cx<T> get(int i, int m, int) const
+        {
+            cx<T> v = w[tw_off(s) + i * (R - 1) + (m - 1)];
+            if (!FWD_) v.y = -v.y;
+            return v;
+        }
+    };
+    // fill the cache for this thread's butterflies (same mapping in every transform)
+    static H3D_D void load_twiddles(CachedTw &c, const cx<T> *__restrict__ tw)
+    {
+        load_tw_stage<1>(c, tw);
+    }
+    template <int s> static H3D_D void load_tw_stage(CachedTw &cache, const cx<T> *__restrict__ tw)
+    {
+        if constexpr (s < S) {
+            constexpr int R = P::R(s), Ns = P::Ns(s);
+            using CN = Cnt<L, TC, NT, R>;
+#pragma unroll
+            for (int i = 0; i < CN::NB; i++) {
+                int b = threadIdx.x + i * NT;
+                int c, j;
+                LY::template bf<R>(b, c, j);
+                int k = j % Ns;
+#pragma unroll
+                for (int m = 1; m < R; m++)
+                    cache.w[tw_off(s) + i * (R - 1) + (m - 1)] =
+                        (CN::total % NT == 0 || b < CN::total) ? __ldg(tw + k * m * (L / (Ns * R))) : mk<T>(1, 0);
+            }
+            load_tw_stage<s + 1>(cache, tw);
+        }
+    }
+
     // (c, position) of in[i*R0+m]; valid() false for idle slots
     static H3D_D bool in_slot(int i, int m, int &c, int &p)
     {
@@ -220,10 +276,10 @@ struct ColFFT {
         return TOTL % NT == 0 || b < TOTL;
     }
 
-    static H3D_D void run(cx<T> (&in)[NIN], cx<T> *sm, cx<T> (&out)[NOUT], const cx<T> *__restrict__ tw)
+    // stage 0 and the middle stages; afterwards sm holds the input of the last stage
+    template <class TWS> static H3D_D void stages_to_last_t(cx<T> (&in)[NIN], cx<T> *sm, const TWS &tws)
     {
         const int tid = threadIdx.x;
-        // stage 0: no twiddles (Ns = 1)
 #pragma unroll
         for (int i = 0; i < NB0; i++) {
             int b = tid + i * NT;
@@ -236,10 +292,81 @@ struct ColFFT {
             }
         }
         __syncthreads();
-        if constexpr (S > 2) fft_mid_stage<T, L, TC, NT, ROWS, FWD, REV, 1>(sm, tw);
-        if constexpr (S > 3) fft_mid_stage<T, L, TC, NT, ROWS, FWD, REV, 2>(sm, tw);
-        // last stage: Ns*RL == L, outputs at j + m*L/RL
+        if constexpr (S > 2) fft_mid_stage<T, L, TC, NT, ROWS, FWD, REV, 1>(sm, tws);
+        if constexpr (S > 3) fft_mid_stage<T, L, TC, NT, ROWS, FWD, REV, 2>(sm, tws);
+    }
+
+    // the transform, handing each last-stage butterfly to st(c, p, v) as soon as
+    // it is computed so that its outputs need not stay live in registers
+    template <class TWS, class ST>
+    static H3D_D void run_store_t(cx<T> (&in)[NIN], cx<T> *sm, const TWS &tws, ST &&st)
+    {
+        stages_to_last_t(in, sm, tws);
         constexpr int NsL = P::Ns(S - 1), nbpc = L / RL;
+        const int tid = threadIdx.x;
+#pragma unroll
+        for (int i = 0; i < NBL; i++) {
+            int b = tid + i * NT;
+            if (TOTL % NT == 0 || b < TOTL) {
+                int c, j;
+                LY::template bf<RL>(b, c, j);
+                int k = j % NsL;
+                cx<T> v[RL];
+#pragma unroll
+                for (int m = 0; m < RL; m++) {
+                    cx<T> x = sm[LY::idx(c, j + m * nbpc)];
+                    if (m > 0) x = cmul(x, tws.template get<L, NsL, RL, FWD, S - 1>(i, m, k));
+                    v[m] = x;
+                }
+                dft<T, RL, FWD>(v);
+#pragma unroll
+                for (int m = 0; m < RL; m++) st(c, j + m * nbpc, v[m]);
+            }
+        }
+    }
+
+    // as run_store_t, but st(i, m, c, p, v) also receives the output slot (i, m)
+    // so that callers can keep per-slot accumulators in registers
+    template <class TWS, class ST>
+    static H3D_D void run_slots_t(cx<T> (&in)[NIN], cx<T> *sm, const TWS &tws, ST &&st)
+    {
+        stages_to_last_t(in, sm, tws);
+        constexpr int NsL = P::Ns(S - 1), nbpc = L / RL;
+        const int tid = threadIdx.x;
+#pragma unroll
+        for (int i = 0; i < NBL; i++) {
+            int b = tid + i * NT;
+            if (TOTL % NT == 0 || b < TOTL) {
+                int c, j;
+                LY::template bf<RL>(b, c, j);
+                int k = j % NsL;
+                cx<T> v[RL];
+#pragma unroll
+                for (int m = 0; m < RL; m++) {
+                    cx<T> x = sm[LY::idx(c, j + m * nbpc)];
+                    if (m > 0) x = cmul(x, tws.template get<L, NsL, RL, FWD, S - 1>(i, m, k));
+                    v[m] = x;
+                }
+                dft<T, RL, FWD>(v);
+#pragma unroll
+                for (int m = 0; m < RL; m++) st(i, m, c, j + m * nbpc, v[m]);
+            }
+        }
+    }
+
+    template <class ST>
+    static H3D_D void run_store(cx<T> (&in)[NIN], cx<T> *sm, const cx<T> *__restrict__ tw, ST &&st)
+    {
+        run_store_t(in, sm, GlobalTw<T>{tw}, st);
+    }
+
+    // the transform with the last-stage outputs left in out[i*RL+m]
+    static H3D_D void run(cx<T> (&in)[NIN], cx<T> *sm, cx<T> (&out)[NOUT], const cx<T> *__restrict__ tw)
+    {
+        const GlobalTw<T> tws{tw};
+        stages_to_last_t(in, sm, tws);
+        constexpr int NsL = P::Ns(S - 1), nbpc = L / RL;
+        const int tid = threadIdx.x;
 #pragma unroll
         for (int i = 0; i < NBL; i++) {
             int b = tid + i * NT;
@@ -249,9 +376,9 @@ struct ColFFT {
                 int k = j % NsL;
 #pragma unroll
                 for (int m = 0; m < RL; m++) {
-                    cx<T> v = sm[LY::idx(c, j + m * nbpc)];
-                    if (m > 0) v = cmul(v, twid<T, FWD>(tw, k * m * (L / (NsL * RL))));
-                    out[i * RL + m] = v;
+                    cx<T> x = sm[LY::idx(c, j + m * nbpc)];
+                    if (m > 0) x = cmul(x, tws.template get<L, NsL, RL, FWD, S - 1>(i, m, k));
+                    out[i * RL + m] = x;
                 }
                 dft<T, RL, FWD>(out + i * RL);
             }

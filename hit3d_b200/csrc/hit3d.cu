@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/hit3d_gpu.h"
@@ -56,7 +57,8 @@ H3D_HD constexpr int plan_rmax(int L)
 template <typename T, int L> struct ColCfg {
     static constexpr int TC = sizeof(T) == 8 ? 8 : 16;  // 128-byte rows of kx columns
     static constexpr int NT0 = TC * L / plan_rmax(L);
-    static constexpr int NT = NT0 > 256 ? 256 : NT0;
+    static constexpr int NTMAX = sizeof(T) == 8 ? 256 : 512;
+    static constexpr int NT = NT0 > NTMAX ? NTMAX : NT0;
     static constexpr size_t SMEM = (size_t)Lay<L, TC, false>::elems * sizeof(cx<T>);
 };
 template <typename T, int L> struct RowCfg {
@@ -64,6 +66,17 @@ template <typename T, int L> struct RowCfg {
     static constexpr int NT = 128;
     static constexpr size_t SMEM = (size_t)Lay<L, TC, true>::elems * sizeof(cx<T>);
 };
+// launch-shape variants of the fused x pass (picked by the tuner):
+//   0: 1024/L pairs x 128 threads   1: 2048/L pairs x 128 threads
+//   2: 1024/L pairs x  64 threads   3: 512/L pairs x 64 threads
+template <typename T, int L, int V> struct RowCfgV {
+    static constexpr int W = V == 1 ? 2048 : V == 3 ? 512 : 1024;
+    static constexpr int TC = L >= W ? 1 : W / L;
+    static constexpr int NT = (V >= 2) ? 64 : 128;
+    static constexpr size_t SMEM = (size_t)Lay<L, TC, true>::elems * sizeof(cx<T>);
+};
+//   4: register-resident kernel (k_xfused_reg), 1024/L pairs x 128 threads
+constexpr int kFusedVariants = 5;
 
 template <class K> static int set_smem(K kernel, size_t bytes)
 {
@@ -115,6 +128,7 @@ struct hit3d_ctx {
     double dx;
     int pblocks;
     int64_t nlaunch;
+    int xcfg;            // launch-shape variant of the fused x pass
 };
 
 static int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
@@ -127,21 +141,44 @@ template <> const double2 *twid<double>(const hit3d_ctx *c) { return c->tw64; }
 template <> const float2 *twid<float>(const hit3d_ctx *c) { return c->tw32; }
 
 // z pass reading the FP64 state with a spectral pre-operation, writing [z][ky][kx]
-template <typename T, int L>
-static int zinv_L(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src, int64_t src_fs, cx<T> *dst,
-                  int64_t dst_fs, int dpitch)
+template <typename T, int L, int MODE>
+static int zinv_LM(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_t src_fs, cx<T> *dst,
+                   int64_t dst_fs, int dpitch)
 {
     using CF = ColCfg<T, L>;
-    IOSpec<T, T> io;
+    using IO = IOSpec<T, T, MODE>;
+    IO io;
     io.src = src; io.dst = dst; io.fs_src = src_fs; io.fs_dst = dst_fs;
-    io.n = c->n; io.psrc = c->P64; io.pdst = dpitch; io.ncol = c->nh; io.mode = mode; io.sfield = sfield;
+    io.n = c->n; io.psrc = c->P64; io.pdst = dpitch; io.ncol = c->nh; io.sfield = sfield;
     io.dx = c->dx;
-    auto k = k_colfft<T, L, CF::TC, CF::NT, false, IOSpec<T, T>>;
+    auto k = k_colfft<T, L, CF::TC, CF::NT, false, IO>;
     H3D_TRY(set_smem(k, CF::SMEM));
     dim3 g((c->nh + CF::TC - 1) / CF::TC, c->n, nf);
     k<<<g, CF::NT, CF::SMEM, c->st>>>(io, twid<T>(c));
     H3D_LAUNCH_CHECK();
     return 0;
+}
+template <typename T, int L>
+static int zinv_L(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src, int64_t src_fs, cx<T> *dst,
+                  int64_t dst_fs, int dpitch)
+{
+    switch (mode) {
+    case PRE_COPY: return zinv_LM<T, L, PRE_COPY>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+    case PRE_SHIFT: return zinv_LM<T, L, PRE_SHIFT>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+    case PRE_STRAIN_A: return zinv_LM<T, L, PRE_STRAIN_A>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+    case PRE_STRAIN_B: return zinv_LM<T, L, PRE_STRAIN_B>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+    default: break;
+    }
+    if constexpr (std::is_same<T, double>::value) {
+        // statistics pre-operations run in FP64 only
+        switch (mode) {
+        case PRE_CURL: return zinv_LM<T, L, PRE_CURL>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+        case PRE_DLONG: return zinv_LM<T, L, PRE_DLONG>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+        case PRE_GRAD: return zinv_LM<T, L, PRE_GRAD>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+        default: break;
+        }
+    }
+    return h3d_set_error_msg(-1, "unsupported spectral pre-operation");
 }
 template <typename T>
 static int zinv(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src, int64_t src_fs, cx<T> *dst,
@@ -217,14 +254,39 @@ template <typename T> static int xr2c(hit3d_ctx *c, cx<T> *base, int64_t fs, int
 #undef CALL
 }
 
-template <typename T, template <class> class OP, int L> static int xfused_L(hit3d_ctx *c, FusedArgs a)
+template <typename T, template <class> class OP, int L, int V> static int xfused_LV(hit3d_ctx *c, FusedArgs a)
+{
+    using RC = RowCfgV<T, L, V>;
+    auto k = k_xfused<T, L, RC::TC, RC::NT, T, OP<T>>;
+    // transform buffer + the CTA's physical field; one cluster of NIN CTAs per tile
+    const size_t smem = 2 * RC::SMEM;
+    H3D_TRY(set_smem(k, smem));
+    const int tiles = (a.npairs + RC::TC - 1) / RC::TC;
+    k<<<dim3(tiles * OP<T>::NIN), RC::NT, smem, c->st>>>(a, twid<T>(c));
+    H3D_LAUNCH_CHECK();
+    return 0;
+}
+template <typename T, template <class> class OP, int L> static int xfused_reg_L(hit3d_ctx *c, FusedArgs a)
 {
     using RC = RowCfg<T, L>;
-    auto k = k_xfused<T, L, RC::TC, RC::NT, T, OP<T>>;
+    auto k = k_xfused_reg<T, L, RC::TC, RC::NT, T, OP<T>>;
     H3D_TRY(set_smem(k, RC::SMEM));
     k<<<dim3((a.npairs + RC::TC - 1) / RC::TC), RC::NT, RC::SMEM, c->st>>>(a, twid<T>(c));
     H3D_LAUNCH_CHECK();
     return 0;
+}
+template <typename T, template <class> class OP, int L> static int xfused_L(hit3d_ctx *c, FusedArgs a)
+{
+    if (c->xcfg == 4) return xfused_reg_L<T, OP, L>(c, a);
+    if constexpr (L >= 128) {
+        switch (c->xcfg) {
+        case 1: return xfused_LV<T, OP, L, 1>(c, a);
+        case 2: return xfused_LV<T, OP, L, 2>(c, a);
+        case 3: return xfused_LV<T, OP, L, 3>(c, a);
+        default: break;
+        }
+    }
+    return xfused_LV<T, OP, L, 0>(c, a);
 }
 template <typename T, template <class> class OP> static int xfused(hit3d_ctx *c, FusedArgs a)
 {
@@ -666,6 +728,56 @@ extern "C" int hit3d_gpu_step_profile(hit3d_ctx *c, int32_t nsteps, int32_t *fov
     if (rc) return rc;
     if (fov) *fov = ev;
     if (fos) *fos = es;
+    return 0;
+}
+
+// time one fused x pass (velocity products) in the current variant; W is scratch
+template <typename T> static int time_fused(hit3d_ctx *c, float *ms)
+{
+    cx<T> *W = reinterpret_cast<cx<T> *>(c->W);
+    FusedArgs fa;
+    memset(&fa, 0, sizeof fa);
+    for (int f = 0; f < 3; f++) fa.in[f] = W + f * c->wfs;
+    for (int o = 0; o < 6; o++) fa.out[o] = W + o * c->wfs;
+    fa.pitch = c->wpitch;
+    cudaEvent_t e0, e1;
+    H3D_CHECK(cudaEventCreate(&e0));
+    H3D_CHECK(cudaEventCreate(&e1));
+    H3D_TRY((xfused<T, OpVel>(c, fa)));  // warm-up
+    H3D_CHECK(cudaEventRecord(e0, c->st));
+    for (int r = 0; r < 3; r++) H3D_TRY((xfused<T, OpVel>(c, fa)));
+    H3D_CHECK(cudaEventRecord(e1, c->st));
+    H3D_CHECK(cudaEventSynchronize(e1));
+    H3D_CHECK(cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return 0;
+}
+
+extern "C" int hit3d_gpu_autotune(hit3d_ctx *c, int32_t *variant, double *ms_out)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    int best = 0;
+    float bt = 1e30f;
+    for (int v = 0; v < kFusedVariants; v++) {
+        c->xcfg = v;
+        float ms = 0.f;
+        int rc = c->p.precision == 0 ? time_fused<double>(c, &ms) : time_fused<float>(c, &ms);
+        if (rc) return rc;
+        if (ms_out) ms_out[v] = ms / 3.0;
+        if (ms < bt) { bt = ms; best = v; }
+    }
+    c->xcfg = best;
+    if (variant) *variant = best;
+    return 0;
+}
+
+extern "C" int hit3d_gpu_set_variant(hit3d_ctx *c, int32_t v)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    if (v < 0 || v >= kFusedVariants) return h3d_set_error_msg(-1, "hit3d_gpu_set_variant: no such variant");
+    c->xcfg = v;
     return 0;
 }
 

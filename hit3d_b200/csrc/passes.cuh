@@ -6,6 +6,8 @@
 // y<->z swap, MPI transpose and z-stick c2c become three in-place passes over
 // the whole field resident in HBM.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "fft.cuh"
 
 // ---------------------------------------------------------------------------
@@ -41,20 +43,23 @@ enum PreMode : int {
     PRE_GRAD = 6,      // d phi/dx_f of state field `sfield`     (m_stats.f90:323-326)
 };
 
-template <typename T, typename TO> struct IOSpec {
+// MODE is a compile-time PreMode so that the plain copy carries no per-element
+// branching or wavenumber arithmetic
+template <typename T, typename TO, int MODE> struct IOSpec {
     const double2 *src;  // state fields, [kz][ky][kx] pitch psrc
     cx<TO> *dst;         // [z][ky][kx] pitch pdst
     int64_t fs_src, fs_dst;
-    int n, psrc, pdst, ncol, mode, sfield;
+    int n, psrc, pdst, ncol, sfield;
     double dx;   // grid spacing, for PRE_SHIFT
 
     H3D_D double2 U(int f, int o, int c, int p) const { return src[f * fs_src + ((int64_t)p * n + o) * psrc + c]; }
     H3D_D cx<T> load(int f, int o, int c, int p) const
     {
         if (c >= ncol) return mk<T>(0, 0);
+        if constexpr (MODE == PRE_COPY) return to_cx<T>(U(f, o, c, p));
         const double kx = c, ky = kwave(o, n), kz = kwave(p, n);
         double2 r;
-        switch (mode) {
+        switch (MODE) {
         case PRE_SHIFT: {
             double2 u = U(f, o, c, p);
             double cs = cos((0.5 * ((kx + ky) + kz)) * dx);
@@ -106,14 +111,20 @@ template <typename T, typename TO> struct IOSpec {
     }
 };
 
+// two resident CTAs per SM for lengths up to 512, so that one CTA's loads
+// overlap another's shared-memory stages
+template <int L, int NT> struct ColMinBlocks {
+    static constexpr int value = (L <= 512 && NT >= 128) ? 2 : 1;
+};
+
 template <typename T, int L, int TC, int NT, bool FWD, class IO>
-__global__ void __launch_bounds__(NT) k_colfft(const IO io, const cx<T> *__restrict__ tw)
+__global__ void __launch_bounds__(NT, (ColMinBlocks<L, NT>::value)) k_colfft(const IO io, const cx<T> *__restrict__ tw)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
     using F = ColFFT<T, L, TC, NT, false, FWD, false>;
     const int col0 = blockIdx.x * TC, outer = blockIdx.y, f = blockIdx.z;
-    cx<T> in[F::NIN], out[F::NOUT];
+    cx<T> in[F::NIN];
 #pragma unroll
     for (int i = 0; i < F::NB0; i++)
 #pragma unroll
@@ -121,14 +132,7 @@ __global__ void __launch_bounds__(NT) k_colfft(const IO io, const cx<T> *__restr
             int c, p;
             if (F::in_slot(i, m, c, p)) in[i * F::R0 + m] = io.load(f, outer, col0 + c, p);
         }
-    F::run(in, sm, out, tw);
-#pragma unroll
-    for (int i = 0; i < F::NBL; i++)
-#pragma unroll
-        for (int m = 0; m < F::RL; m++) {
-            int c, p;
-            if (F::out_slot(i, m, c, p)) io.store(f, outer, col0 + c, p, out[i * F::RL + m]);
-        }
+    F::run_store(in, sm, tw, [&](int c, int p, cx<T> v) { io.store(f, outer, col0 + c, p, v); });
 }
 
 // ---------------------------------------------------------------------------
@@ -250,10 +254,15 @@ __global__ void __launch_bounds__(NT) k_xr2c(cx<TS> *base, int64_t fs, int64_t p
 
 // ---------------------------------------------------------------------------
 // fused x pass:  NIN spectral inputs (after their z and y inverse passes) ->
-// c2r in registers -> per-point operator -> NOUT forward r2c outputs.
-// The inverse uses the reversed radix plan so its output slots are exactly the
-// forward plan's input slots: products never leave registers.
-// OP provides NIN, NOUT, aux(in) and out(o, in, aux).
+// c2r -> per-point operator -> NOUT forward r2c outputs, in one kernel.
+// One thread-block cluster of NIN CTAs owns a tile of TC row pairs.  CTA r
+// inverse-transforms input r and keeps the physical rows in its own shared
+// memory; after a cluster barrier every CTA reads the fields it needs from its
+// peers' shared memory (distributed shared memory) and forward-transforms the
+// outputs o with o % NIN == r.  Inputs are fully consumed before the barrier, so
+// outputs may overwrite inputs.
+// OP provides NIN, NOUT, NPHYS, NEED_AUX, uses(o, f), cour(in), aux(in) and
+// out(o, in, aux).
 // ---------------------------------------------------------------------------
 struct FusedArgs {
     const void *in[6];   // cx<TS>* of the NIN input fields
@@ -262,13 +271,125 @@ struct FusedArgs {
     int npairs;
     double norm;
     unsigned long long *cmax;  // optional: max over points of OP::cour(in) (bit pattern of a double >= 0)
-    double *phys;        // optional: physical copies of the first OP::NPHYS inputs, [f][row][x]
+    double *phys;        // optional: FP64 physical copies of the first OP::NPHYS inputs, [f][row][x]
     int64_t phys_fs, phys_pitch;
     double p0, p1;       // operator parameters
 };
 
 template <typename T, int L, int TC, int NT, typename TS, class OP>
-__global__ void __launch_bounds__(NT) k_xfused(const FusedArgs a, const cx<T> *__restrict__ tw)
+__global__ void __cluster_dims__(OP::NIN, 1, 1) __launch_bounds__(NT, 256 / NT)
+    k_xfused(const FusedArgs a, const cx<T> *__restrict__ tw)
+{
+    namespace cg = cooperative_groups;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    // inverse and forward share one plan (and so one set of per-thread twiddles)
+    using FI = ColFFT<T, L, TC, NT, true, false, false>;
+    using FF = ColFFT<T, L, TC, NT, true, true, false>;
+    using LY = typename FF::LY;
+    typename FF::CachedTw twc;
+    FF::load_twiddles(twc, tw);
+    cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);  // transform work buffer
+    cx<T> *ph = sm + LY::elems;                      // this CTA's physical field (a + i b packed)
+    cg::cluster_group cl = cg::this_cluster();
+    const int r = (int)cl.block_rank();
+    const int pair0 = (int)(blockIdx.x / OP::NIN) * TC;
+    const T norm = (T)a.norm;
+    OP op{(T)a.p0, (T)a.p1};
+
+    // ---- phase 1: input r to physical space, kept in shared memory ----
+    {
+        cx<T> in[FI::NIN];
+        const cx<TS> *fb = reinterpret_cast<const cx<TS> *>(a.in[r]);
+#pragma unroll
+        for (int i = 0; i < FI::NB0; i++)
+#pragma unroll
+            for (int m = 0; m < FI::R0; m++) {
+                int c, p;
+                if (FI::in_slot(i, m, c, p) && pair0 + c < a.npairs) {
+                    const cx<TS> *A = fb + (int64_t)(2 * (pair0 + c)) * a.pitch;
+                    in[i * FI::R0 + m] = load_packed<T, L, TS>(A, A + a.pitch, p);
+                } else in[i * FI::R0 + m] = mk<T>(0, 0);
+            }
+        FI::run_store_t(in, sm, twc, [&](int c, int p, cx<T> v) {
+            // round through the storage type so that every precision sees the
+            // same physical values as a separate c2r pass would produce
+            const cx<T> x = mk<T>((T)(TS)(v.x * norm), (T)(TS)(v.y * norm));
+            ph[LY::idx(c, p)] = x;
+            if (a.phys != nullptr && r < OP::NPHYS && pair0 + c < a.npairs) {
+                const int64_t row = 2 * (pair0 + c);
+                a.phys[r * a.phys_fs + row * a.phys_pitch + p] = (double)x.x;
+                a.phys[r * a.phys_fs + (row + 1) * a.phys_pitch + p] = (double)x.y;
+            }
+        });
+    }
+    cl.sync();
+    const cx<T> *fp[OP::NIN];
+#pragma unroll
+    for (int f = 0; f < OP::NIN; f++) fp[f] = cl.map_shared_rank(ph, f);
+
+    // ---- Courant maximum (rank 0 scans the whole tile) ----
+    if (a.cmax != nullptr && r == 0) {
+        double cm = 0.0;
+        for (int t = threadIdx.x; t < TC * L; t += NT) {
+            const int c = t / L, p = t - c * L;
+            if (pair0 + c >= a.npairs) continue;
+            T va[OP::NIN], vb[OP::NIN];
+#pragma unroll
+            for (int f = 0; f < OP::NIN; f++) {
+                const cx<T> v = fp[f][LY::idx(c, p)];
+                va[f] = v.x;
+                vb[f] = v.y;
+            }
+            cm = fmax(cm, fmax((double)op.cour(va), (double)op.cour(vb)));
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, off));
+        if ((threadIdx.x & 31) == 0) atomicMax(a.cmax, (unsigned long long)__double_as_longlong(cm));
+    }
+
+    // ---- phase 2: outputs o = r, r + NIN, ... ----
+#pragma unroll 1
+    for (int o = r; o < OP::NOUT; o += OP::NIN) {
+        cx<T> in[FF::NIN];
+#pragma unroll
+        for (int i = 0; i < FF::NB0; i++)
+#pragma unroll
+            for (int m = 0; m < FF::R0; m++) {
+                int c, p;
+                const int q = i * FF::R0 + m;
+                in[q] = mk<T>(0, 0);
+                if (FF::in_slot(i, m, c, p) && pair0 + c < a.npairs) {
+                    T va[OP::NIN], vb[OP::NIN];
+#pragma unroll
+                    for (int f = 0; f < OP::NIN; f++) {
+                        if (OP::NEED_AUX || OP::uses(o, f)) {
+                            const cx<T> v = fp[f][LY::idx(c, p)];
+                            va[f] = v.x;
+                            vb[f] = v.y;
+                        } else va[f] = vb[f] = (T)0;
+                    }
+                    T xa = (T)0, xb = (T)0;
+                    if (OP::NEED_AUX) { xa = op.aux(va); xb = op.aux(vb); }
+                    in[q] = mk<T>(op.out(o, va, xa), op.out(o, vb, xb));
+                }
+            }
+        // each last-stage butterfly reads and writes only its own positions, so
+        // its outputs can go straight back into the work buffer
+        FF::run_store_t(in, sm, twc, [&](int c, int p, cx<T> v) { sm[LY::idx(c, p)] = v; });
+        __syncthreads();
+        store_split<T, L, TC, NT, TS>(sm, reinterpret_cast<cx<TS> *>(a.out[o]), a.pitch, pair0, a.npairs);
+        __syncthreads();
+    }
+    cl.sync();  // peers may still be reading this CTA's physical field
+}
+
+// Register-resident variant of the fused x pass (one CTA per tile): the three
+// physical inputs stay in registers between the inverse and forward
+// transforms, handed over slot for slot because the inverse uses the reversed
+// radix plan.  Fewer warps per SM than the cluster variant but no shared-memory
+// round trip for the physical fields; the tuner picks between them.
+template <typename T, int L, int TC, int NT, typename TS, class OP>
+__global__ void __launch_bounds__(NT) k_xfused_reg(const FusedArgs a, const cx<T> *__restrict__ tw)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
@@ -372,9 +493,15 @@ __global__ void __launch_bounds__(NT) k_xfused(const FusedArgs a, const cx<T> *_
     }
 }
 
+
 // velocity products (rhs_velocity.f90:56-72): uu uv uw vv vw ww; Courant |u|+|v|+|w|
 template <typename T> struct OpVel {
     static constexpr int NIN = 3, NOUT = 6, NPHYS = 3;
+    static constexpr bool NEED_AUX = false;
+    static H3D_HD constexpr bool uses(int o, int f)
+    {
+        return o == 0 ? f == 0 : o == 1 ? f <= 1 : o == 2 ? (f == 0 || f == 2) : o == 3 ? f == 1 : o == 4 ? f >= 1 : f == 2;
+    }
     T p0, p1;
     H3D_D T cour(const T *v) const { return fabs(v[0]) + fabs(v[1]) + fabs(v[2]); }
     H3D_D T aux(const T *) const { return (T)0; }
@@ -394,6 +521,8 @@ template <typename T> struct OpVel {
 // scalar fluxes (rhs_scalars.f90:82-85): phi*u, phi*v, phi*w from (u, v, w, phi)
 template <typename T> struct OpScal {
     static constexpr int NIN = 4, NOUT = 3, NPHYS = 0;
+    static constexpr bool NEED_AUX = false;
+    static H3D_HD constexpr bool uses(int o, int f) { return f == o || f == 3; }
     T p0, p1;
     H3D_D T cour(const T *v) const { return fabs(v[0]) + fabs(v[1]) + fabs(v[2]); }
     H3D_D T aux(const T *) const { return (T)0; }
@@ -405,6 +534,8 @@ template <typename T> struct OpScal {
 // p0 = (Cs Delta)^2
 template <typename T> struct OpSmag {
     static constexpr int NIN = 6, NOUT = 6, NPHYS = 0;
+    static constexpr bool NEED_AUX = true;
+    static H3D_HD constexpr bool uses(int o, int f) { return f == o; }
     T p0, p1;
     H3D_D T cour(const T *) const { return (T)0; }
     H3D_D T aux(const T *s) const

@@ -93,6 +93,8 @@ SIGNATURES = [
     ("hit3d_gpu_step", C.c_int, [_vp, _i32, C.POINTER(_i32), C.POINTER(_i32), _dp]),
     ("hit3d_gpu_stream", C.c_void_p, [_vp]),
     ("hit3d_gpu_launch_count", C.c_int64, [_vp]),
+    ("hit3d_gpu_autotune", C.c_int, [_vp, C.POINTER(_i32), _dp]),
+    ("hit3d_gpu_set_variant", C.c_int, [_vp, _i32]),
     ("hit3d_gpu_step_profile", C.c_int, [_vp, _i32, C.POINTER(_i32), C.POINTER(_i32), _dp]),
     ("hit3d_gpu_set_dt", C.c_int, [_vp, _d]),
     ("hit3d_gpu_set_scalars_active", C.c_int, [_vp, _i32]),
@@ -217,6 +219,16 @@ class Context:
                "step_profile")
         self.fov, self.fos = fov.value, fos.value
         return dict(zip(self.STAGES, ms.tolist()))
+
+    def autotune(self):
+        """Pick the fastest launch shape of the fused x pass; returns (variant, ms per variant)."""
+        v = C.c_int32(0)
+        ms = np.full(8, np.nan)
+        _check(lib().hit3d_gpu_autotune(self._h, C.byref(v), _ptr(ms)), "autotune")
+        return v.value, [x for x in ms.tolist() if x == x]
+
+    def set_variant(self, v: int):
+        _check(lib().hit3d_gpu_set_variant(self._h, int(v)), "set_variant")
 
     @property
     def launches(self) -> int:

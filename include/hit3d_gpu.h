@@ -102,6 +102,15 @@ void *hit3d_gpu_stream(hit3d_ctx *ctx);
  * (main.f90:307-356). */
 int hit3d_gpu_step_profile(hit3d_ctx *ctx, int32_t nsteps, int32_t *fov, int32_t *fos, double *ms);
 
+/* Launch-shape tuner (no reference counterpart): times every launch-shape
+ * variant of the fused x pass (row pairs per CTA, threads per CTA) on this
+ * context's own work buffers and keeps the fastest; the state is not touched.
+ * *variant receives the choice, ms[0..8) the time of each variant (unused
+ * entries are left untouched).
+ * hit3d_gpu_set_variant fixes a variant by hand. */
+int hit3d_gpu_autotune(hit3d_ctx *ctx, int32_t *variant, double *ms);
+int hit3d_gpu_set_variant(hit3d_ctx *ctx, int32_t variant);
+
 /* Number of kernels this context has launched since hit3d_gpu_init. */
 int64_t hit3d_gpu_launch_count(hit3d_ctx *ctx);
 
