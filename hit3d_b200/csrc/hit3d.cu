@@ -129,6 +129,7 @@ struct hit3d_ctx {
     int pblocks;
     int64_t nlaunch;
     int xcfg;            // launch-shape variant of the fused x pass
+    double k2max;        // truncation radius squared of PRE_TRUNC
 };
 
 static int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
@@ -151,6 +152,7 @@ static int zinv_LM(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_t
     io.src = src; io.dst = dst; io.fs_src = src_fs; io.fs_dst = dst_fs;
     io.n = c->n; io.psrc = c->P64; io.pdst = dpitch; io.ncol = c->nh; io.sfield = sfield;
     io.dx = c->dx;
+    io.k2max = c->k2max;
     auto k = k_colfft<T, L, CF::TC, CF::NT, false, IO>;
     H3D_TRY(set_smem(k, CF::SMEM));
     dim3 g((c->nh + CF::TC - 1) / CF::TC, c->n, nf);
@@ -175,6 +177,7 @@ static int zinv_L(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src
         case PRE_CURL: return zinv_LM<T, L, PRE_CURL>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         case PRE_DLONG: return zinv_LM<T, L, PRE_DLONG>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         case PRE_GRAD: return zinv_LM<T, L, PRE_GRAD>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+        case PRE_TRUNC: return zinv_LM<T, L, PRE_TRUNC>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         default: break;
         }
     }
@@ -807,12 +810,12 @@ extern "C" int hit3d_gpu_dealias_all(hit3d_ctx *c)
 }
 
 // shell spectrum of nf state fields starting at src -> host es[0..kmax)
-static int shell_spectrum(hit3d_ctx *c, const double2 *src, int nf, double *es)
+static int shell_spectrum(hit3d_ctx *c, const double2 *src, int nf, double *es, double w0 = 0.5)
 {
     const int kmax = c->kmax;
     const int nw = 8;
     k_shell_partial<<<c->pblocks, nw * 32, sizeof(double) * nw * kmax, c->st>>>(c->n, c->nh, c->P64, c->fs64, nf, kmax,
-                                                                               src, c->d_part);
+                                                                               w0, src, c->d_part);
     H3D_LAUNCH_CHECK();
     k_shell_final<<<(kmax + 127) / 128, 128, 0, c->st>>>(c->pblocks, kmax, c->d_part, c->d_red);
     H3D_LAUNCH_CHECK();
@@ -910,6 +913,8 @@ static int upload_phys(hit3d_ctx *c, const double *h, int64_t ld1, int nf)
     return 0;
 }
 
+static int target_spectrum(int isp, double peak, double ir_exp, int kmax, std::vector<double> &et);
+
 extern "C" int hit3d_gpu_init_velocity(hit3d_ctx *c, double rn1, int32_t isp, double peak, double ir_exp)
 {
     if (!c) return h3d_set_error_msg(-1, "null context");
@@ -953,24 +958,10 @@ extern "C" int hit3d_gpu_init_velocity(hit3d_ctx *c, double rn1, int32_t isp, do
     H3D_TRY(fwd3d64(c, c->W64, 3));
     k_init_curl<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, c->fs64, kmax, c->W64, c->U);
     H3D_LAUNCH_CHECK();
-    std::vector<double> es(kmax), et(kmax), ratio(kmax);
+    std::vector<double> es(kmax), et, ratio(kmax);
     H3D_TRY(shell_spectrum(c, c->U, 3, es.data()));
-    for (int k = 1; k <= kmax; k++) {
-        double wmag = (double)k, ratio_k = wmag / peak;
-        if (isp == 0) et[k - 1] = pow(wmag, -5.0 / 3.0);
-        else if (isp == 1) et[k - 1] = ratio_k * ratio_k * ratio_k / peak * exp(-3.0 * ratio_k);
-        else if (isp == 2) et[k - 1] = pow(wmag, ir_exp) * exp(-2.0 * ratio_k * ratio_k);
-        else {
-            double f = 2.0 * PI * ratio_k, f2 = f * f, d = 1.0 + f2;
-            et[k - 1] = (f2 * f2) / (d * d * d);
-        }
-    }
-    double tot = 0.0;
-    for (int k = 0; k < kmax; k++) tot = tot + et[k];
-    for (int k = 0; k < kmax; k++) {
-        et[k] = et[k] / tot;
-        ratio[k] = es[k] > 0.0 ? sqrt(et[k] / es[k]) : -1.0;
-    }
+    target_spectrum(isp, peak, ir_exp, kmax, et);
+    for (int k = 0; k < kmax; k++) ratio[k] = es[k] > 0.0 ? sqrt(et[k] / es[k]) : -1.0;
     H3D_CHECK(cudaMemcpyAsync(c->d_ratio, ratio.data(), sizeof(double) * kmax, cudaMemcpyHostToDevice, c->st));
     k_shell_scale<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, c->fs64, 3, kmax, c->d_ratio, c->U);
     H3D_LAUNCH_CHECK();
@@ -1080,6 +1071,87 @@ extern "C" int hit3d_gpu_filter_field(hit3d_ctx *c, int32_t kind, double delta, 
         H3D_LAUNCH_CHECK();
     }
     k_filter_apply<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, G, c->U + field * c->fs64);
+    H3D_LAUNCH_CHECK();
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+extern "C" int hit3d_gpu_physical_fields(hit3d_ctx *c, int32_t nf, double k2max, double *out, int64_t ld1)
+{
+    if (!c || !out) return h3d_set_error_msg(-1, "hit3d_gpu_physical_fields: null argument");
+    if (ld1 < c->n + 2) return h3d_set_error_msg(-1, "ld1 must be >= nx+2");
+    if (nf < 1 || nf > 3 + c->nsc) return h3d_set_error_msg(-1, "hit3d_gpu_physical_fields: nfields out of range");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    const size_t rows = (size_t)c->n * c->n;
+    c->k2max = k2max;
+    for (int f0 = 0; f0 < nf; f0 += 3) {
+        const int m = nf - f0 < 3 ? nf - f0 : 3;
+        H3D_TRY(inv_from_state(c, m, k2max > 0.0 ? PRE_TRUNC : PRE_COPY, 0, c->U + f0 * c->fs64));
+        for (int f = 0; f < m; f++)
+            H3D_CHECK(cudaMemcpy2DAsync(out + (size_t)(f0 + f) * ld1 * rows, ld1 * sizeof(double),
+                                        reinterpret_cast<double *>(c->W64 + f * c->fs64), 2 * c->P64 * sizeof(double),
+                                        c->n * sizeof(double), rows, cudaMemcpyDeviceToHost, c->st));
+    }
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+// target spectra of init_velocity.f90:193-220 (isp 2 added by this library)
+static int target_spectrum(int isp, double peak, double ir_exp, int kmax, std::vector<double> &et)
+{
+    const double PI = 4.0 * atan(1.0);
+    et.assign(kmax, 0.0);
+    for (int k = 1; k <= kmax; k++) {
+        double wmag = (double)k, ratio_k = wmag / peak;
+        if (isp == 0) et[k - 1] = pow(wmag, -5.0 / 3.0);
+        else if (isp == 1) et[k - 1] = ratio_k * ratio_k * ratio_k / peak * exp(-3.0 * ratio_k);
+        else if (isp == 2) et[k - 1] = pow(wmag, ir_exp) * exp(-2.0 * ratio_k * ratio_k);
+        else if (isp == 3) {
+            double f = 2.0 * PI * ratio_k, f2 = f * f, d = 1.0 + f2;
+            et[k - 1] = (f2 * f2) / (d * d * d);
+        } else return -1;
+    }
+    double tot = 0.0;
+    for (int k = 0; k < kmax; k++) tot = tot + et[k];
+    for (int k = 0; k < kmax; k++) et[k] = et[k] / tot;
+    return 0;
+}
+
+extern "C" int hit3d_gpu_velocity_rescale(hit3d_ctx *c, int32_t isp, double peak, double ir_exp)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    if (isp == -1) return 0;  // Taylor-Green runs are never rescaled (velocity_rescale.f90:24)
+    const int n = c->n, kmax = c->kmax;
+    std::vector<double> et;
+    if (target_spectrum(isp, peak, ir_exp, kmax, et)) return h3d_set_error_msg(-1, "ERROR: WRONG INITIAL SPECTRUM TYPE");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    // shell energies without the kx = 0 half weight; hits = real entries per shell
+    // (velocity_rescale.f90:42-60)
+    std::vector<double> es(kmax);
+    H3D_TRY(shell_spectrum(c, c->U, 3, es.data(), 1.0));
+    std::vector<int64_t> hits(kmax, 0);
+    for (int kq = 0; kq < n; kq++) {
+        const double ky = kwave(kq, n);
+        for (int jq = 0; jq < n; jq++) {
+            const double kz = kwave(jq, n);
+            for (int kx = 0; kx < n / 2; kx++) {
+                const double k2 = (double)kx * kx + ky * ky + kz * kz;
+                const int sh = (int)lroundf(sqrtf((float)k2));
+                if (sh > 0 && sh <= kmax) hits[sh - 1] += 2;
+            }
+        }
+    }
+    const double PI = 4.0 * atan(1.0);
+    const double fac = 4.0 / 3.0 * PI / 2.0;
+    std::vector<double> ratio(kmax);
+    for (int k = 1; k <= kmax; k++) {
+        double r1 = (double)k + 0.5, r2 = (double)k - 0.5;
+        if (k == 1) r2 = 0.0;
+        double e = hits[k - 1] > 0 ? es[k - 1] / (double)hits[k - 1] * fac * (r1 * r1 * r1 - r2 * r2 * r2) : 0.0;
+        ratio[k - 1] = e > 0.0 ? sqrt(et[k - 1] / e) : -1.0;
+    }
+    H3D_CHECK(cudaMemcpyAsync(c->d_ratio, ratio.data(), sizeof(double) * kmax, cudaMemcpyHostToDevice, c->st));
+    k_shell_scale<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, c->fs64, 3, kmax, c->d_ratio, c->U);
     H3D_LAUNCH_CHECK();
     H3D_CHECK(cudaStreamSynchronize(c->st));
     return 0;

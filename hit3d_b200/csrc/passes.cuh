@@ -41,6 +41,7 @@ enum PreMode : int {
     PRE_STRAIN_A = 4,  // S11, S12, S13 for f = 0,1,2            (m_les.f90:1153-1170)
     PRE_STRAIN_B = 5,  // S22, S23, S33 for f = 0,1,2            (m_les.f90:1180-1198)
     PRE_GRAD = 6,      // d phi/dx_f of state field `sfield`     (m_stats.f90:323-326)
+    PRE_TRUNC = 7,     // field f with |k|^2 > k2max zeroed       (io_write_4.f90:21-42)
 };
 
 // MODE is a compile-time PreMode so that the plain copy carries no per-element
@@ -50,7 +51,8 @@ template <typename T, typename TO, int MODE> struct IOSpec {
     cx<TO> *dst;         // [z][ky][kx] pitch pdst
     int64_t fs_src, fs_dst;
     int n, psrc, pdst, ncol, sfield;
-    double dx;   // grid spacing, for PRE_SHIFT
+    double dx;     // grid spacing, for PRE_SHIFT
+    double k2max;  // truncation radius squared, for PRE_TRUNC
 
     H3D_D double2 U(int f, int o, int c, int p) const { return src[f * fs_src + ((int64_t)p * n + o) * psrc + c]; }
     H3D_D cx<T> load(int f, int o, int c, int p) const
@@ -99,6 +101,11 @@ template <typename T, typename TO, int MODE> struct IOSpec {
             double2 u = U(sfield, o, c, p);
             double k = f == 0 ? kx : f == 1 ? ky : kz;
             r = make_double2(-(k * u.y), k * u.x);
+            break;
+        }
+        case PRE_TRUNC: {
+            const double k2 = kx * kx + ky * ky + kz * kz;
+            r = k2 > k2max ? make_double2(0.0, 0.0) : U(f, o, c, p);
             break;
         }
         default: r = U(f, o, c, p);

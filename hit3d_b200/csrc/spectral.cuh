@@ -343,8 +343,10 @@ __global__ void k_dealias_all(int n, int nh, int pitch, int64_t fs, int nf, int 
 // float32 shell index (m_stats.f90:195-235).  Deterministic: each warp owns a
 // private histogram, lane L accumulates the shells congruent to L mod 32 in a
 // fixed element order; warps and blocks are combined in index order.
-__global__ void k_shell_partial(int n, int nh, int pitch, int64_t fs, int nf, int kmax, const double2 *__restrict__ U,
-                                double *__restrict__ part /* [gridDim.x][kmax] */)
+// w0 is the weight of the kx = 0 plane: 0.5 for the statistics (m_stats.f90:222),
+// 1 for the decaying-run rescale (velocity_rescale.f90:47-55)
+__global__ void k_shell_partial(int n, int nh, int pitch, int64_t fs, int nf, int kmax, double w0,
+                                const double2 *__restrict__ U, double *__restrict__ part /* [gridDim.x][kmax] */)
 {
     extern __shared__ double hist[];  // [warps][kmax]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -374,7 +376,7 @@ __global__ void k_shell_partial(int n, int nh, int pitch, int64_t fs, int nf, in
                         im = (f == 0) ? v.y * v.y : im + v.y * v.y;
                     }
                     double e1 = fac * re, e2 = fac * im;
-                    if (m.kx == 0) { e1 *= 0.5; e2 *= 0.5; }
+                    if (m.kx == 0) { e1 *= w0; e2 *= w0; }
                     e = e1 + e2;
                     sh = s - 1;
                 }

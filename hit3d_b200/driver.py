@@ -1,0 +1,214 @@
+"""Host main loop of the hydro task over the C-ABI (restates main.f90:22-300).
+
+The reference's Fortran host keeps the input file, the restart layout, the seeds
+and the statistics files; here the same host logic drives the device through
+hit3d_b200.gpu.  Output files keep the reference's names and formats:
+stat1.gp / stat2.gp / es.gp (m_stats.f90:150-185), scNN.gp / es_NN.gp
+(m_stats.f90:66-80, 420-432), u./v./w./scNN. real*4 files (io_write_4.f90) and
+<run_name>.64.<itime> restart files (restart_io.f90).  Exit reasons follow
+my_exit.f90:23-62: 0 normal, 1 TMAX, 2 run limit, 3 user 'stop' file.
+"""
+from __future__ import annotations
+
+import math
+import os
+import time as _time
+
+import numpy as np
+
+from .gpu import Context
+from .params import RunConfig, read_input_file
+from .restart import read_restart, restart_name, write_real4, write_restart
+
+
+def _fmt_e(x: float, w: int = 15, d: int = 6) -> str:
+    """Fortran Ew.d edit descriptor (0.dddddE+xx form)."""
+    if x == 0.0 or not math.isfinite(x):
+        m, e = 0.0, 0
+    else:
+        e = int(math.floor(math.log10(abs(x)))) + 1
+        m = x / 10.0 ** e
+        if round(abs(m), d) >= 1.0:
+            m /= 10.0
+            e += 1
+    s = f"{'-' if m < 0 else ''}0.{int(round(abs(m) * 10 ** d)):0{d}d}E{'+' if e >= 0 else '-'}{abs(e):02d}"
+    return s.rjust(w)
+
+
+class Simulation:
+    """One run: the reference's hydro task with the state resident on the GPU."""
+
+    def __init__(self, run_name: str, workdir: str = ".", cfg: RunConfig | None = None, precision: int = 0,
+                 device: int = 0, job_runlimit_min: float = 12 * 60):
+        self.run_name = run_name
+        self.wd = workdir
+        self.cfg = cfg or read_input_file(os.path.join(workdir, run_name + ".in"))
+        self.ctx = Context(self.cfg.to_params(precision=precision, device=device))
+        self.time = 0.0
+        self.itime = self.cfg.itmin
+        self.int_scalars = False
+        self.t0 = _time.time()
+        self.job_runlimit = job_runlimit_min
+        p = os.path.join(workdir, "job_parameters.txt")
+        if os.path.exists(p):
+            try:
+                self.job_runlimit = float(open(p).read().split()[0])
+            except (ValueError, IndexError):
+                pass
+        self.exit_reason = None
+        self.log = []
+
+    # -- start-up (begin_new.f90 / begin_restart.f90) ---------------------------
+    def begin(self):
+        c = self.cfg
+        if c.itmin == 0:
+            self.time = 0.0
+            self.itime = 0
+            if c.tscalar <= 0.0 and c.n_scalars > 0:
+                self.int_scalars = True
+            self.ctx.init_velocity(c.rn1, c.isp_type, c.peak_wavenum, float(c.ir_exp))
+            if c.n_scalars:
+                self._init_scalars()
+            self.io_write_4()
+        else:
+            self.itime = c.itmin
+            f, self.time, dt, nums1, _ = read_restart(
+                os.path.join(self.wd, restart_name(self.run_name, c.itmin)), c.nx, c.n_scalars)
+            self.ctx.upload_fields(f)
+            if nums1 > 0 or c.tscalar <= self.time:
+                self.int_scalars = c.n_scalars > 0
+            if c.variable_dt:
+                c.dt = 0.5 * dt
+                self.ctx.set_dt(c.dt)
+        self.ctx.set_scalars_active(self.int_scalars)
+        self.ctx.fov = self.ctx.fos = 1
+        self.ctx.dealias_all()
+
+    def _init_scalars(self):
+        """init_scalars.f90: only type-0 (uniform mean gradient, zero initial field) is generated."""
+        for t in self.cfg.scalar_type:
+            if t % 100 != 0:
+                raise NotImplementedError("only scalars of initial type 0 are generated on this path")
+        f = self.ctx.download_fields()
+        f[3:] = 0.0
+        self.ctx.upload_fields(f)
+
+    # -- outputs ---------------------------------------------------------------
+    def file_ext(self):
+        return f"{self.itime:06d}"
+
+    def io_write_4(self):
+        c = self.cfg
+        nout = 3 + (c.n_scalars if self.int_scalars else 0)
+        phys = self.ctx.physical_fields(nout, float(c.kmax) ** 2)
+        names = ["u", "v", "w"] + [f"sc{n + 1:02d}" for n in range(nout - 3)]
+        for n, nm in enumerate(names):
+            write_real4(os.path.join(self.wd, f"{nm}.{self.file_ext()}"), phys[n])
+
+    def write_restart(self):
+        nums = self.cfg.n_scalars if self.int_scalars else 0
+        f = self.ctx.download_fields(3 + nums)
+        write_restart(os.path.join(self.wd, restart_name(self.run_name, self.itime)), f, self.time, self.cfg.dt,
+                      nums)
+
+    def stat_main(self):
+        es, st = self.ctx.stats()
+        wd, it, t = self.wd, self.itime, self.time
+
+        def append(name, header, line):
+            path = os.path.join(wd, name)
+            new = not os.path.exists(path)
+            with open(path, "a") as fh:
+                if new and header:
+                    fh.write(header + "\n")
+                fh.write(line + "\n")
+
+        append("stat1.gp", " # 1.itime 2.time         3.energy       4.diss         5.eta          6.enstrophy    7.R_lambda",
+               f"{it:8d}" + "".join(_fmt_e(x) for x in (t, st["energy"], st["eps_v"], st["eta"], st["enstrophy"],
+                                                         st["re_lambda"])))
+        append("stat2.gp", "# 1.itime  2.time         3.int LS       4. lambda      5.R_lambda1    6.tau_e        7.etakmax",
+               f"{it:8d}" + "".join(_fmt_e(x) for x in (t, st["x_length"], st["lambda"], st["re_lambda1"],
+                                                         st["tau_e"], st["etakmax"])))
+        e1 = es * np.arange(1, len(es) + 1) ** 2 * 2.0 * self.cfg.nu
+        with open(os.path.join(wd, "es.gp"), "a") as fh:
+            fh.write("\n\n" + f"# ITIME={it:7d} TIME={_fmt_e(t, 17, 8)}\n")
+            for k in range(len(es)):
+                fh.write(f"{k + 1:4d}{_fmt_e(es[k])}{_fmt_e(e1[k])}\n")
+        if self.int_scalars:
+            for s in range(self.cfg.n_scalars):
+                ss = self.ctx.scalar_stats(s)
+                append(f"sc{s + 1:02d}.gp",
+                       "# 1.itime 2.time          3.sc.diss       4. mean      5.variance    6.min     7.max",
+                       f"{it:7d}" + "".join(_fmt_e(x) for x in (t, ss["diss"], ss["mean"], ss["variance"], ss["min"],
+                                                                ss["max"])))
+                with open(os.path.join(wd, f"es_{s + 1:02d}.gp"), "a") as fh:
+                    fh.write("\n\n" + f"# ITIME={it:7d} TIME={_fmt_e(t, 17, 8)}\n")
+                    for k, v in enumerate(ss["spectrum"]):
+                        fh.write(f"{k + 1:4d}{_fmt_e(v)}\n")
+        return es, st
+
+    # -- time step control (my_dt.f90) ------------------------------------------
+    def my_dt(self, courant):
+        c = self.cfg
+        courant_max = 0.1
+        if c.flow_type <= 1:
+            if courant < courant_max:
+                c.dt = min(c.dt * 1.01, 0.01)
+            else:
+                c.dt = c.dt / 1.05
+            if self.int_scalars and courant > 0.0:
+                for s in c.sc:
+                    c.dt = min(c.dt, c.dt * courant_max / courant / s)
+        self.ctx.set_dt(c.dt)
+
+    # -- main cycle (main.f90:87-288) -------------------------------------------
+    def run(self, max_steps: int | None = None):
+        c = self.cfg
+        last = c.itmax if max_steps is None else min(c.itmax, self.itime + max_steps)
+        while self.itime < last:
+            self.itime += 1
+            it = self.itime
+            t = self.time
+            if c.flow_type == 0 and c.trescale > 0.0 and \
+                    math.floor((t - c.dt) / c.trescale) < math.floor(t / c.trescale):
+                if math.floor(t / c.trescale) <= c.nrescale and it != 1:
+                    self.ctx.velocity_rescale(c.isp_type, c.peak_wavenum, float(c.ir_exp))
+                    self.ctx.fov = self.ctx.fos = 1
+                    if it % c.iprint1 == 0:
+                        self.stat_main()
+            courant = self.ctx.step(1)
+            self.time += c.dt
+            if it % c.iprint2 == 0:
+                self.write_restart()
+            if c.variable_dt:
+                self.my_dt(courant)
+            if it % c.iprint1 == 0:
+                el = int(_time.time() - self.t0)
+                self.log.append(f"ITIME={it:6d}   TIME={self.time:8.4f}    DT={c.dt:8.5f}   Courn= {courant:6.4f}  "
+                                f"CPU:({el // 3600:04d}:{el // 60 % 60:02d}:{el % 60:02d})")
+            if it % c.iprint1 == 0 or it % c.iwrite4 == 0:
+                if self.time > c.tmax:
+                    return self.exit(1)
+                if c.n_scalars > 0 and not self.int_scalars and self.time > c.tscalar:
+                    self.int_scalars = True
+                    self._init_scalars()
+                    self.ctx.set_scalars_active(True)
+                if it % c.iprint1 == 0:
+                    self.stat_main()
+                if it % c.iwrite4 == 0:
+                    self.io_write_4()
+            if it % 10 == 0:
+                if (_time.time() - self.t0) / 60.0 + 5 > self.job_runlimit:
+                    return self.exit(2)
+                if os.path.exists(os.path.join(self.wd, "stop")):
+                    return self.exit(3)
+        if max_steps is None or self.itime >= c.itmax:
+            return self.exit(0)
+        return None
+
+    def exit(self, reason: int):
+        """my_exit: a restart file is written for every reason >= 0."""
+        self.exit_reason = reason
+        if reason >= 0:
+            self.write_restart()
+        return reason

@@ -108,6 +108,8 @@ SIGNATURES = [
     ("hit3d_gpu_filter_field", C.c_int, [_vp, _i32, _d, _i32]),
     ("hit3d_gpu_xfft3d_static", C.c_int, [_i32, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("hit3d_gpu_physical_velocity", C.c_int, [_vp, _dp, _i64]),
+    ("hit3d_gpu_physical_fields", C.c_int, [_vp, _i32, _d, _dp, _i64]),
+    ("hit3d_gpu_velocity_rescale", C.c_int, [_vp, _i32, _d, _d]),
 ]
 
 
@@ -288,6 +290,17 @@ class Context:
 
     def filter_field(self, kind: int, delta: float, field: int):
         _check(lib().hit3d_gpu_filter_field(self._h, int(kind), float(delta), int(field)), "filter_field")
+
+    def physical_fields(self, nf: int, k2max: float = 0.0) -> np.ndarray:
+        """Inverse transforms of the first nf state fields, optionally spherically truncated."""
+        out = np.zeros((nf, self.n, self.n, self.n + 2))
+        _check(lib().hit3d_gpu_physical_fields(self._h, int(nf), float(k2max), _ptr(out), self.n + 2),
+               "physical_fields")
+        return out
+
+    def velocity_rescale(self, isp_type: int, peak_wavenum: float, ir_exp: float = 2.0):
+        _check(lib().hit3d_gpu_velocity_rescale(self._h, int(isp_type), float(peak_wavenum), float(ir_exp)),
+               "velocity_rescale")
 
     def physical_velocity(self) -> np.ndarray:
         out = np.zeros((3, self.n, self.n, self.n + 2))

@@ -176,6 +176,17 @@ int hit3d_gpu_xfft3d_static(int32_t n, const double *in, double *out, void *stre
  * function prod sin(k delta/2)/(k delta/2) (no reference counterpart). */
 int hit3d_gpu_filter_field(hit3d_ctx *ctx, int32_t kind, double delta, int32_t field);
 
+/* Physical-space copies of the first nf state fields, out(ld1, ny, nz, nf), with
+ * every mode of |k|^2 > k2max zeroed first when k2max > 0 (the spherical
+ * truncation and inverse transforms of io_write_4, io_write_4.f90:21-90; the
+ * caller converts to real*4 and writes the files). */
+int hit3d_gpu_physical_fields(hit3d_ctx *ctx, int32_t nf, double k2max, double *out, int64_t ld1);
+
+/* Rescale the velocity to the initial spectrum of type isp_type for decaying
+ * runs (velocity_rescale.f90:1-159); called by the host every TRESCALE in time
+ * (main.f90:111-121). */
+int hit3d_gpu_velocity_rescale(hit3d_ctx *ctx, int32_t isp_type, double peak_wavenum, double ir_exp);
+
 /* Physical-space velocity (x, y, z) of the current state, as the reference's
  * wrk1..3 after rhs_scalars (main.f90:126): out(ld1, ny, nz, 3). */
 int hit3d_gpu_physical_velocity(hit3d_ctx *ctx, double *out, int64_t ld1);

@@ -77,6 +77,8 @@ def lib():
         L.oracle_init_velocity.restype = C.c_int
         L.oracle_init_velocity.argtypes = [vp, C.c_double, C.c_int, C.c_double, C.c_double]
         L.oracle_randu_stream.argtypes = [C.c_double, C.c_int64, dp]
+        L.oracle_velocity_rescale.restype = C.c_int
+        L.oracle_velocity_rescale.argtypes = [vp, C.c_int, C.c_double, C.c_double]
         L.oracle_particles_step.argtypes = [C.c_int, C.c_double, dp, C.c_int64, dp, dp, C.c_int]
         L.oracle_particles_lattice.restype = C.c_int64
         L.oracle_particles_lattice.argtypes = [C.c_int, C.c_int64, dp]
@@ -162,6 +164,10 @@ class Oracle:
 
     def dealias_all(self):
         lib().oracle_dealias_all(self._p)
+
+    def velocity_rescale(self, isp_type, peak_wavenum, ir_exp=2.0):
+        if lib().oracle_velocity_rescale(self._p, int(isp_type), float(peak_wavenum), float(ir_exp)) != 0:
+            raise ValueError(f"unsupported isp_type {isp_type}")
 
     def step(self, nsteps=1):
         lib().oracle_step(self._p, int(nsteps))

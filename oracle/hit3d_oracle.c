@@ -1277,6 +1277,69 @@ int oracle_init_velocity(oracle_t *o, double rn1, int isp_type, double peak_wave
 }
 
 /* ------------------------------------------------------------------------- */
+/*  velocity_rescale (velocity_rescale.f90:1-159): shell energies without the */
+/*  kx=0 half weight, averaged by hits and scaled by the shell volume, then   */
+/*  the velocity is rescaled to the target spectrum                           */
+/* ------------------------------------------------------------------------- */
+int oracle_velocity_rescale(oracle_t *o, int isp_type, double peak_wavenum, double ir_exp)
+{
+    int n = o->n, kmax = o->kmax;
+    double PI = 4.0 * atan(1.0);
+    if (isp_type == -1) return 0;
+    double fac = 1.0 / (((double)n * n * n) * ((double)n * n * n));
+    double *es = (double *)calloc(kmax, sizeof(double));
+    double *et = (double *)calloc(kmax, sizeof(double));
+    int64_t *hits = (int64_t *)calloc(kmax, sizeof(int64_t));
+    double *u = F(o, 0), *v = F(o, 1), *w = F(o, 2);
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                double k2 = o->akx[i] * o->akx[i] + o->aky[k] * o->aky[k] + o->akz[j] * o->akz[j];
+                int sh = nint_shell32(k2);
+                if (sh > 0 && sh <= kmax) {
+                    size_t a = IX(o, i, j, k);
+                    hits[sh - 1] += 1;
+                    es[sh - 1] = es[sh - 1] + fac * (u[a] * u[a] + v[a] * v[a] + w[a] * w[a]);
+                }
+            }
+    double fv = 4.0 / 3.0 * PI / 2.0;
+    for (int k = 1; k <= kmax; k++) {
+        double r1 = (double)k + 0.5, r2 = (double)k - 0.5;
+        if (k == 1) r2 = 0.0;
+        if (hits[k - 1] > 0) es[k - 1] = es[k - 1] / (double)hits[k - 1] * fv * (r1 * r1 * r1 - r2 * r2 * r2);
+        else es[k - 1] = 0.0;
+    }
+    for (int k = 1; k <= kmax; k++) {
+        double wmag = (double)k, ratio = wmag / peak_wavenum;
+        if (isp_type == 0) et[k - 1] = pow(wmag, -5.0 / 3.0);
+        else if (isp_type == 1) et[k - 1] = ratio * ratio * ratio / peak_wavenum * exp(-3.0 * ratio);
+        else if (isp_type == 2) et[k - 1] = pow(wmag, ir_exp) * exp(-2.0 * ratio * ratio);
+        else if (isp_type == 3) {
+            double f = 2.0 * PI * ratio, f2 = f * f, d = 1.0 + f2;
+            et[k - 1] = (f2 * f2) / (d * d * d);
+        } else { free(es); free(et); free(hits); return -1; }
+    }
+    double tot = 0.0;
+    for (int k = 0; k < kmax; k++) tot = tot + et[k];
+    for (int k = 0; k < kmax; k++) et[k] = et[k] / tot;
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 2; i++) {
+                double k2 = o->akx[i] * o->akx[i] + o->aky[k] * o->aky[k] + o->akz[j] * o->akz[j];
+                int sh = nint_shell32(k2);
+                size_t a = IX(o, i, j, k);
+                if (sh > 0 && sh <= kmax && es[sh - 1] > 0.0) {
+                    double r = sqrt(et[sh - 1] / es[sh - 1]);
+                    for (int c = 0; c < 3; c++) F(o, c)[a] = F(o, c)[a] * r;
+                } else {
+                    for (int c = 0; c < 3; c++) F(o, c)[a] = 0.0;
+                }
+            }
+    free(es); free(et); free(hits);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
 /*  particles (m_particles.f90:815-1230, 1451-1508) on one periodic slab     */
 /*  uphys: three (nx+2,ny,nz) physical velocity arrays; xyzp/uvwp: 3*np,     */
 /*  particle-major like the reference's (3,np) arrays.                       */

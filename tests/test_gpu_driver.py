@@ -1,0 +1,73 @@
+"""The host main loop over the C-ABI (main.f90) and the device pieces it needs:
+velocity_rescale, the truncated physical output of io_write_4, restart files."""
+import os
+import shutil
+
+import numpy as np
+import pytest
+
+from _cases import make_pair, relerr
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.mark.parametrize("isp", [0, 1, 3])
+def test_velocity_rescale_matches_oracle(isp):
+    o, g = make_pair(32, dealias=0, flow_type=0)
+    o.step(3)
+    g.step(3)
+    o.velocity_rescale(isp, 4.0)
+    g.velocity_rescale(isp, 4.0)
+    f = g.download_fields()
+    for m in range(3):
+        assert relerr(f[m], o.fields[m]) < 1e-10
+
+
+def test_truncated_physical_fields_match_oracle():
+    o, g = make_pair(32)
+    kmax = 32 // 3
+    phys = g.physical_fields(3, float(kmax) ** 2)
+    n = 32
+    ky = np.fft.fftfreq(n, 1.0 / n)
+    ky[n // 2] = n // 2
+    kx = np.repeat(np.arange(n // 2 + 1), 2)
+    k2 = ky[:, None, None] ** 2 + ky[None, :, None] ** 2 + kx[None, None, :] ** 2
+    for c in range(3):
+        a = np.ascontiguousarray(o.fields[c]).copy()
+        a[k2 > kmax ** 2] = 0.0
+        o.fft3d(-1, a)
+        assert relerr(phys[c][:, :, :n], a[:, :, :n]) < 1e-13
+
+
+def test_driver_run_writes_reference_files(tmp_path):
+    from hit3d_b200.driver import Simulation
+    from hit3d_b200.restart import read_real4, read_restart
+    wd = str(tmp_path)
+    shutil.copy(os.path.join(GOLDEN, "decay64_.in"), os.path.join(wd, "decay64_.in"))
+    sim = Simulation("decay64_", wd)
+    sim.begin()
+    reason = sim.run()
+    assert reason == 0 and sim.itime == 20
+    lines = [ln for ln in open(os.path.join(wd, "stat1.gp")) if not ln.lstrip().startswith("#")]
+    assert len(lines) == 2 and lines[0].split()[0] == "10"
+    es_blocks = open(os.path.join(wd, "es.gp")).read().count("# ITIME=")
+    assert es_blocks == 2
+    assert os.path.exists(os.path.join(wd, "sc01.gp")) and os.path.exists(os.path.join(wd, "es_02.gp"))
+    u0 = read_real4(os.path.join(wd, "u.000000"))
+    assert u0.shape == (64, 64, 64) and np.isfinite(u0).all()
+    f, t, dt, nums, nles = read_restart(os.path.join(wd, "decay64_.64.000020"), 64, 2)
+    assert nums == 2 and abs(t - 20 * 0.005) < 1e-12
+    g = sim.ctx.download_fields()
+    assert np.array_equal(f[..., :64], g[..., :64])
+
+
+def test_stop_file_ends_the_run_with_a_restart(tmp_path):
+    from hit3d_b200.driver import Simulation
+    wd = str(tmp_path)
+    shutil.copy(os.path.join(GOLDEN, "decay64_.in"), os.path.join(wd, "decay64_.in"))
+    open(os.path.join(wd, "stop"), "w").close()
+    sim = Simulation("decay64_", wd)
+    sim.begin()
+    assert sim.run() == 3 and sim.itime == 10
+    assert os.path.exists(os.path.join(wd, "decay64_.64.000010"))

@@ -1,0 +1,98 @@
+"""Host-side pieces that need no GPU: the input-file reader, restart and real*4
+file layouts, and their failure paths (my_exit(-1) conditions of the reference)."""
+import os
+import struct
+
+import numpy as np
+import pytest
+
+from hit3d_b200.params import InputFileError, parse_input, read_input_file
+from hit3d_b200.restart import RestartError, read_real4, read_restart, write_real4, write_restart
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_reads_sample_input():
+    c = read_input_file(os.path.join(GOLDEN, "decay64_.in"))
+    assert (c.nx, c.ny, c.nz_all) == (64, 64, 64)
+    assert (c.itmin, c.itmax, c.iprint1, c.iprint2, c.iwrite4) == (0, 20, 10, 20, 20)
+    assert c.trescale == 0.05 and c.nrescale == 2
+    assert c.flow_type == 0 and c.re == 400.0 and c.nu == 1.0 / 400.0
+    assert c.dt == 0.005 and not c.variable_dt
+    assert (c.isp_type, c.ir_exp, c.peak_wavenum) == (1, 2, 4.0)
+    assert c.rn1 == 67748937.0 and c.kmax == 21
+    assert c.n_scalars == 2 and c.scalar_type == [0, 0] and c.sc == [0.7, 1.0]
+    assert c.pe == [c.nu / 0.7, c.nu / 1.0]
+
+
+def test_list_directed_reads_span_lines():
+    """A scalar line with four values takes the fifth from the next line."""
+    text = open(os.path.join(GOLDEN, "decay64_.in")).read()
+    text = text.replace("0      0.7     4.0    2.    0.0\n0      1.0     4.0    4.    0.0",
+                        "0      0.7     4.0    2.\n 0.25\n0      1.0     4.0    4.    0.0")
+    c = parse_input(text)
+    assert c.reac_sc == [0.25, 0.0] and c.sc == [0.7, 1.0]
+
+
+def test_missing_nrescale_defaults_to_one():
+    text = open(os.path.join(GOLDEN, "decay64_.in")).read().replace("0.05 2          TRESCALE", "0.05            TRESCALE")
+    assert parse_input(text).nrescale == 1
+
+
+def test_les_forces_two_thirds_rule_and_dealias_kmax():
+    text = open(os.path.join(GOLDEN, "decay64_.in")).read()
+    c = parse_input(text.replace("0		dealias", "1		dealias"))
+    assert c.dealias == 1 and c.kmax == int(np.floor(64 / 3 * np.sqrt(2)))
+    c = parse_input(text.replace("0		dealias", "1		dealias").replace("0               les_model", "1               les_model"))
+    assert c.dealias == 0
+
+
+def test_truncated_input_is_an_error():
+    text = open(os.path.join(GOLDEN, "decay64_.in")).read()
+    with pytest.raises(InputFileError):
+        parse_input("\n".join(text.splitlines()[:20]))
+    with pytest.raises(InputFileError):
+        parse_input(text, numprocs=3)
+
+
+def test_restart_round_trip(tmp_path):
+    rng = np.random.default_rng(0)
+    f = rng.standard_normal((5, 8, 8, 10))
+    p = str(tmp_path / "run_000001.64.000010")
+    write_restart(p, f, 1.25, 0.005, nums=2)
+    assert os.path.getsize(p) == 36 + 5 * 8 * 8 * 8 * 8
+    with open(p, "rb") as fh:
+        assert struct.unpack("<5i2d", fh.read(36)) == (8, 8, 8, 2, 0, 1.25, 0.005)
+    g, t, dt, nums, nles = read_restart(p, 8, n_scalars=2)
+    assert (t, dt, nums, nles) == (1.25, 0.005, 2, 0)
+    assert np.array_equal(g[..., :8], f[..., :8]) and np.all(g[..., 8:] == 0)
+    # the input file prevails: fewer scalars drop, more scalars come back as zeros
+    g1, *_ = read_restart(p, 8, n_scalars=1)
+    assert g1.shape[0] == 4 and np.array_equal(g1[3, ..., :8], f[3, ..., :8])
+    g3, *_ = read_restart(p, 8, n_scalars=3)
+    assert g3.shape[0] == 6 and np.all(g3[5] == 0)
+
+
+def test_corrupt_restarts_are_rejected(tmp_path):
+    f = np.zeros((3, 8, 8, 10))
+    p = str(tmp_path / "r.64.000001")
+    write_restart(p, f, 0.0, 0.01, nums=0)
+    with pytest.raises(RestartError, match="Dimensions"):
+        read_restart(p, 16, 0)
+    with open(p, "r+b") as fh:
+        fh.truncate(100)
+    with pytest.raises(RestartError, match="size"):
+        read_restart(p, 8, 0)
+    with open(p, "wb") as fh:
+        fh.write(b"\x00" * 10)
+    with pytest.raises(RestartError, match="truncated"):
+        read_restart(p, 8, 0)
+
+
+def test_real4_layout(tmp_path):
+    a = np.arange(4 * 4 * 6, dtype=np.float64).reshape(4, 4, 6)
+    p = str(tmp_path / "u.000000")
+    write_real4(p, a)
+    assert os.path.getsize(p) == 12 + 4 * 4 * 4 * 4
+    b = read_real4(p)
+    assert np.array_equal(b, a[:, :, :4].astype(np.float32))
