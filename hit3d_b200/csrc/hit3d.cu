@@ -6,7 +6,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <mutex>
+#include <set>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "../../include/hit3d_gpu.h"
@@ -78,9 +81,20 @@ template <typename T, int L, int V> struct RowCfgV {
 //   4: register-resident kernel (k_xfused_reg), 1024/L pairs x 128 threads
 constexpr int kFusedVariants = 5;
 
+// Raise a kernel's dynamic shared-memory limit once per kernel and device, so
+// that steps recorded into a CUDA graph later make no attribute calls.
 template <class K> static int set_smem(K kernel, size_t bytes)
 {
-    if (bytes > 48 * 1024) H3D_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    if (bytes <= 48 * 1024) return 0;
+    static std::mutex mu;
+    static std::set<std::pair<const void *, int>> done;
+    int dev = 0;
+    H3D_CHECK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_pair((const void *)kernel, dev);
+    if (done.count(key)) return 0;
+    H3D_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    done.insert(key);
     return 0;
 }
 
@@ -115,6 +129,7 @@ struct hit3d_ctx {
     int64_t wfs;         // complex elements per work field
     int wpitch;
     double2 *W64;        // FP64 scratch (3 fields) for statistics and the transform API
+    double2 *sgs;        // FP64 scratch (9 fields) of the subgrid-stress data path, on first use
     double *phys;        // physical u,v,w [3][z][y][x] for particles
     double2 *tw64;
     float2 *tw32;
@@ -621,7 +636,7 @@ extern "C" void hit3d_gpu_finalize(hit3d_ctx *c)
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->W64 && c->W64 != c->W) cudaFree(c->W64);
     void *ptrs[] = {c->U, c->RO, c->RP, c->SP, c->W, c->phys, c->tw64, c->tw32, c->d_fen, c->d_part,
-                    c->d_red, c->d_ratio, c->d_cmax, c->stage, c->d_xyz, c->d_uvw};
+                    c->d_red, c->d_ratio, c->d_cmax, c->stage, c->d_xyz, c->d_uvw, c->sgs};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
@@ -1031,12 +1046,12 @@ extern "C" int hit3d_gpu_xfft3d(hit3d_ctx *c, int32_t flag, const double *in, do
     return 0;
 }
 
-extern "C" int hit3d_gpu_filter_field(hit3d_ctx *c, int32_t kind, double delta, int32_t field)
+// filter transfer function into the FP64 scratch field W64[0]: kind 2 Gaussian
+// (kernel built in physical space and transformed, m_filter_xfftw.f90:197-271),
+// kind 4 box of width delta (analytic sinc product)
+static int filter_transfer(hit3d_ctx *c, int kind, double delta)
 {
-    if (!c) return h3d_set_error_msg(-1, "null context");
-    if (field < 0 || field >= 3 + c->nsc) return h3d_set_error_msg(-1, "hit3d_gpu_filter_field: no such field");
-    if (kind != 2 && kind != 4) return h3d_set_error_msg(-1, "hit3d_gpu_filter_field: kind must be 2 (Gaussian) or 4 (box)");
-    H3D_CHECK(cudaSetDevice(c->dev));
+    if (kind != 2 && kind != 4) return h3d_set_error_msg(-1, "filter kind must be 2 (Gaussian) or 4 (box)");
     const int n = c->n;
     double2 *G = c->W64;
     if (kind == 2) {
@@ -1070,9 +1085,95 @@ extern "C" int hit3d_gpu_filter_field(hit3d_ctx *c, int32_t kind, double delta, 
         k_box_transfer<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, delta, G);
         H3D_LAUNCH_CHECK();
     }
-    k_filter_apply<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, G, c->U + field * c->fs64);
+    return 0;
+}
+
+extern "C" int hit3d_gpu_filter_field(hit3d_ctx *c, int32_t kind, double delta, int32_t field)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    if (field < 0 || field >= 3 + c->nsc) return h3d_set_error_msg(-1, "hit3d_gpu_filter_field: no such field");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    H3D_TRY(filter_transfer(c, kind, delta));
+    k_filter_apply<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->W64, c->U + field * c->fs64);
     H3D_LAUNCH_CHECK();
     H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+// download physical rows of nf FP64 fields as compact FP32 [f][z][y][x]
+static int download_f32(hit3d_ctx *c, const double2 *base, int nf, float *out)
+{
+    const int64_t np = (int64_t)c->n * c->n * c->n;
+    float *st = reinterpret_cast<float *>(c->stage);  // n*n*nh double2 >= n^3 floats
+    for (int f = 0; f < nf; f++) {
+        k_phys_to_f32<<<pw_grid(c), 256, 0, c->st>>>(c->n, 2 * (int64_t)c->P64,
+                                                     reinterpret_cast<const double *>(base + f * c->fs64), st);
+        H3D_LAUNCH_CHECK();
+        H3D_CHECK(cudaMemcpyAsync(out + f * np, st, sizeof(float) * np, cudaMemcpyDeviceToHost, c->st));
+        H3D_CHECK(cudaStreamSynchronize(c->st));
+    }
+    return 0;
+}
+
+extern "C" int hit3d_gpu_sgs_fields(hit3d_ctx *c, int32_t kind, double delta, float *out)
+{
+    if (!c || !out) return h3d_set_error_msg(-1, "hit3d_gpu_sgs_fields: null argument");
+    if (c->p.precision != 0) return h3d_set_error_msg(-1, "hit3d_gpu_sgs_fields: needs a context with FP64 transforms");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    const int64_t np = (int64_t)c->n * c->n * c->n;
+    if (!c->sgs) H3D_TRY(ctx_alloc((void **)&c->sgs, sizeof(double2) * 6 * (size_t)c->fs64));
+    double2 *W = reinterpret_cast<double2 *>(c->W);
+    const int64_t fs = c->fs64;
+    const int P = c->P64;
+    // 1. products of the resolved velocity, transformed forward: W0..5 = (u_i u_j)^
+    H3D_TRY(zinv<double>(c, 3, PRE_COPY, 0, c->U, fs, W, fs, P));
+    H3D_TRY(spass<double>(c, 1, false, W, fs, P, 3));
+    {
+        FusedArgs fa;
+        memset(&fa, 0, sizeof fa);
+        for (int f = 0; f < 3; f++) fa.in[f] = W + f * fs;
+        for (int o = 0; o < 6; o++) fa.out[o] = W + o * fs;
+        fa.pitch = P;
+        H3D_TRY((xfused<double, OpVel>(c, fa)));
+    }
+    H3D_TRY(spass<double>(c, 1, true, W, fs, P, 6));
+    H3D_TRY(spass<double>(c, 2, true, W, fs, P, 6));
+    // 2. the filter; W64 is W's first field in FP64 mode, so build G in sgs[5]
+    double2 *G = c->sgs + 5 * fs;
+    {
+        double2 *save = c->W64;
+        c->W64 = G;
+        int rc = filter_transfer(c, kind, delta);
+        c->W64 = save;
+        if (rc) return rc;
+    }
+    // 3. filtered velocity (sgs0..2) and filtered products (W0..5), spectral
+    H3D_CHECK(cudaMemcpyAsync(c->sgs, c->U, sizeof(double2) * 3 * fs, cudaMemcpyDeviceToDevice, c->st));
+    for (int f = 0; f < 3; f++) {
+        k_filter_apply<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, P, G, c->sgs + f * fs);
+        H3D_LAUNCH_CHECK();
+    }
+    for (int f = 0; f < 6; f++) {
+        k_filter_apply<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, P, G, W + f * fs);
+        H3D_LAUNCH_CHECK();
+    }
+    // 4. filtered velocity gradients A_ij = d ubar_i / dx_j, nine fields (i-major);
+    //    G is no longer needed, so sgs3..5 serve as scratch
+    double2 *tmp = c->sgs + 3 * fs;
+    for (int i = 0; i < 3; i++) {
+        H3D_TRY(zinv<double>(c, 3, PRE_GRAD, i, c->sgs, fs, tmp, fs, P));
+        H3D_TRY(spass<double>(c, 1, false, tmp, fs, P, 3));
+        H3D_TRY(xc2r<double>(c, tmp, fs, P, 3));
+        H3D_TRY(download_f32(c, tmp, 3, out + (9 + 3 * i) * np));
+    }
+    // 5. physical filtered velocity and products; tau in place of the products
+    H3D_TRY(inv3d64(c, c->sgs, 3));
+    H3D_TRY(inv3d64(c, W, 6));
+    k_sgs_tau<<<pw_grid(c), 256, 0, c->st>>>(c->n, 2 * (int64_t)P, 2 * fs, reinterpret_cast<const double *>(c->sgs),
+                                             reinterpret_cast<double *>(W));
+    H3D_LAUNCH_CHECK();
+    H3D_TRY(download_f32(c, c->sgs, 3, out));
+    H3D_TRY(download_f32(c, W, 6, out + 3 * np));
     return 0;
 }
 
@@ -1171,3 +1272,150 @@ extern "C" int hit3d_gpu_physical_velocity(hit3d_ctx *c, double *out, int64_t ld
     H3D_CHECK(cudaStreamSynchronize(c->st));
     return 0;
 }
+
+// ---------------------------------------------------------------------------
+// batched form: many independent runs (uneven sizes, own parameters and seeds)
+// advanced together.  After an eager first-order step, chunks of `graph_steps`
+// Adams-Bashforth steps of all runs are recorded once into a CUDA graph -- one
+// branch per run on its own stream, forked from and joined back into a root
+// stream -- and replayed with a single launch per chunk.
+// ---------------------------------------------------------------------------
+struct hit3d_batch {
+    std::vector<hit3d_ctx *> runs;
+    std::vector<int> fov, fos;
+    int dev = 0;
+    cudaStream_t root = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int graph_steps = 0;
+    int64_t launches = 0;
+};
+
+static int run_step(hit3d_ctx *c, int ev, int es)
+{
+    return c->p.precision == 0 ? step_once<double>(c, ev, es) : step_once<float>(c, ev, es);
+}
+
+extern "C" void hit3d_batch_destroy(hit3d_batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->dev);
+    if (b->root) cudaStreamSynchronize(b->root);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (cudaEvent_t e : b->join) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->root) cudaStreamDestroy(b->root);
+    for (hit3d_ctx *c : b->runs) hit3d_gpu_finalize(c);
+    delete b;
+}
+
+extern "C" int hit3d_batch_create(const hit3d_params *p, int32_t nruns, hit3d_batch **out)
+{
+    if (!p || !out || nruns < 1) return h3d_set_error_msg(-1, "hit3d_batch_create: bad arguments");
+    *out = nullptr;
+    for (int r = 1; r < nruns; r++)
+        if (p[r].device != p[0].device) return h3d_set_error_msg(-1, "hit3d_batch_create: all runs must share one device");
+    hit3d_batch *b = new hit3d_batch();
+    b->dev = p[0].device;
+    for (int r = 0; r < nruns; r++) {
+        hit3d_ctx *c = nullptr;
+        int rc = hit3d_gpu_init(&p[r], &c);
+        if (rc) { hit3d_batch_destroy(b); return rc; }
+        b->runs.push_back(c);
+        b->fov.push_back(1);
+        b->fos.push_back(1);
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    b->join.resize(nruns, nullptr);
+    for (int r = 0; r < nruns && e == cudaSuccess; r++) e = cudaEventCreateWithFlags(&b->join[r], cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        hit3d_batch_destroy(b);
+        return h3d_set_error(e, "hit3d_batch_create", __FILE__, __LINE__);
+    }
+    *out = b;
+    return 0;
+}
+
+extern "C" int hit3d_batch_context(hit3d_batch *b, int32_t r, hit3d_ctx **ctx)
+{
+    if (!b || !ctx || r < 0 || r >= (int)b->runs.size()) return h3d_set_error_msg(-1, "hit3d_batch_context: no such run");
+    *ctx = b->runs[r];
+    return 0;
+}
+
+// record `steps` Adams-Bashforth steps of every run into one graph
+static int batch_capture(hit3d_batch *b, int steps)
+{
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    hit3d_ctx *c = b->runs[0];  // for the error macros
+    H3D_CHECK(cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal));
+    int rc = 0;
+    for (int s = 0; s < steps && rc == 0; s++) {
+        cudaEventRecord(b->fork, b->root);
+        for (size_t r = 0; r < b->runs.size() && rc == 0; r++) {
+            hit3d_ctx *cr = b->runs[r];
+            cudaStreamWaitEvent(cr->st, b->fork, 0);
+            rc = run_step(cr, 0, 0);
+            cudaEventRecord(b->join[r], cr->st);
+            cudaStreamWaitEvent(b->root, b->join[r], 0);
+        }
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->root, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return h3d_set_error(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    b->graph = g;
+    H3D_CHECK(cudaGraphInstantiate(&b->exec, g, 0));
+    b->graph_steps = steps;
+    (void)c;
+    return 0;
+}
+
+extern "C" int hit3d_batch_step(hit3d_batch *b, int32_t nsteps, int32_t graph_steps)
+{
+    if (!b || nsteps < 0) return h3d_set_error_msg(-1, "hit3d_batch_step: bad arguments");
+    if (graph_steps < 1) graph_steps = 1;
+    hit3d_ctx *c = b->runs[0];
+    H3D_CHECK(cudaSetDevice(b->dev));
+    int left = nsteps;
+    // first-order step of runs that need one, outside the graph
+    bool any_first = false;
+    for (size_t r = 0; r < b->runs.size(); r++) any_first |= b->fov[r] || (b->fos[r] && b->runs[r]->int_scalars);
+    if (any_first && left > 0) {
+        for (size_t r = 0; r < b->runs.size(); r++) {
+            H3D_TRY(run_step(b->runs[r], b->fov[r], b->fos[r]));
+            b->fov[r] = 0;
+            if (b->runs[r]->int_scalars) b->fos[r] = 0;
+        }
+        left--;
+    }
+    if (left >= graph_steps) {
+        if (!b->exec || b->graph_steps != graph_steps) {
+            for (hit3d_ctx *cr : b->runs) H3D_CHECK(cudaStreamSynchronize(cr->st));
+            H3D_TRY(batch_capture(b, graph_steps));
+        }
+        // order the replay after any eager work on the run streams
+        for (size_t r = 0; r < b->runs.size(); r++) {
+            H3D_CHECK(cudaEventRecord(b->join[r], b->runs[r]->st));
+            H3D_CHECK(cudaStreamWaitEvent(b->root, b->join[r], 0));
+        }
+        while (left >= graph_steps) {
+            H3D_CHECK(cudaGraphLaunch(b->exec, b->root));
+            b->launches++;
+            left -= graph_steps;
+        }
+        H3D_CHECK(cudaStreamSynchronize(b->root));
+    }
+    for (; left > 0; left--)
+        for (hit3d_ctx *cr : b->runs) H3D_TRY(run_step(cr, 0, 0));
+    for (hit3d_ctx *cr : b->runs) H3D_CHECK(cudaStreamSynchronize(cr->st));
+    (void)c;
+    return 0;
+}
+
+extern "C" int64_t hit3d_batch_graph_launches(hit3d_batch *b) { return b ? b->launches : -1; }

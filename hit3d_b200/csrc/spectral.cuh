@@ -528,6 +528,35 @@ __global__ void k_box_transfer(int n, int nh, int pitch, double delta, double2 *
     }
 }
 
+// physical rows (pitch rp reals) -> compact FP32 [z][y][x]
+__global__ void k_phys_to_f32(int n, int64_t rp, const double *__restrict__ src, float *__restrict__ dst)
+{
+    const int64_t np = (int64_t)n * n * n;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t row = t / n, x = t - row * n;
+        dst[t] = (float)src[row * rp + x];
+    }
+}
+
+// subgrid stress tau_ij = filter(u_i u_j) - filter(u_i) filter(u_j) in physical
+// space, in place over the six filtered products P (pitch rp reals, field stride
+// fs reals); UB = the three filtered velocities
+__global__ void k_sgs_tau(int n, int64_t rp, int64_t fs, const double *__restrict__ UB, double *__restrict__ P)
+{
+    const int64_t np = (int64_t)n * n * n;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t row = t / n, x = t - row * n;
+        const int64_t o = row * rp + x;
+        const double u = UB[o], v = UB[fs + o], w = UB[2 * fs + o];
+        P[o] -= u * u;
+        P[fs + o] -= u * v;
+        P[2 * fs + o] -= u * w;
+        P[3 * fs + o] -= v * v;
+        P[4 * fs + o] -= v * w;
+        P[5 * fs + o] -= w * w;
+    }
+}
+
 // layout conversion between the reference's (nx+2, ny, nz) Fourier array
 // [ky][kz][kx] (pitch nh) and the device layout [kz][ky][kx] (pitch P)
 __global__ void k_ref_to_dev(int n, int nh, int pitch, const double2 *__restrict__ R, double2 *__restrict__ D)

@@ -110,6 +110,12 @@ SIGNATURES = [
     ("hit3d_gpu_physical_velocity", C.c_int, [_vp, _dp, _i64]),
     ("hit3d_gpu_physical_fields", C.c_int, [_vp, _i32, _d, _dp, _i64]),
     ("hit3d_gpu_velocity_rescale", C.c_int, [_vp, _i32, _d, _d]),
+    ("hit3d_gpu_sgs_fields", C.c_int, [_vp, _i32, _d, C.POINTER(C.c_float)]),
+    ("hit3d_batch_create", C.c_int, [C.POINTER(_Params), _i32, C.POINTER(C.c_void_p)]),
+    ("hit3d_batch_context", C.c_int, [_vp, _i32, C.POINTER(C.c_void_p)]),
+    ("hit3d_batch_step", C.c_int, [_vp, _i32, _i32]),
+    ("hit3d_batch_graph_launches", C.c_int64, [_vp]),
+    ("hit3d_batch_destroy", None, [_vp]),
 ]
 
 
@@ -150,14 +156,18 @@ class Context:
     STAT_KEYS = ["energy", "eps_v", "eta", "etakmax", "uvar", "x_length", "lambda", "re_lambda",
                  "re_lambda1", "tau_e", "enstrophy", "skewness"]
 
-    def __init__(self, params: Params):
+    def __init__(self, params: Params, _handle: C.c_void_p | None = None):
         self.params = params
         self.n = params.nx
         self.nfields = 3 + params.n_scalars
         self.kmax = params.kmax
-        h = C.c_void_p()
-        cp = params.to_c()
-        _check(lib().hit3d_gpu_init(C.byref(cp), C.byref(h)), "hit3d_gpu_init")
+        self._owned = _handle is None
+        if _handle is None:
+            h = C.c_void_p()
+            cp = params.to_c()
+            _check(lib().hit3d_gpu_init(C.byref(cp), C.byref(h)), "hit3d_gpu_init")
+        else:
+            h = _handle
         self._h = h
         self.fov = 1
         self.fos = 1
@@ -165,7 +175,8 @@ class Context:
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().hit3d_gpu_finalize(self._h)
+            if self._owned:
+                lib().hit3d_gpu_finalize(self._h)
             self._h = None
 
     def __del__(self):
@@ -296,6 +307,15 @@ class Context:
         out = np.zeros((nf, self.n, self.n, self.n + 2))
         _check(lib().hit3d_gpu_physical_fields(self._h, int(nf), float(k2max), _ptr(out), self.n + 2),
                "physical_fields")
+        return out
+
+    def sgs_fields(self, kind: int = 4, delta: float | None = None) -> np.ndarray:
+        """(18, nz, ny, nx) float32: filtered velocity, exact subgrid stress, filtered gradients."""
+        if delta is None:
+            delta = 4.0 * 2.0 * np.pi / self.n
+        out = np.empty((18, self.n, self.n, self.n), dtype=np.float32)
+        _check(lib().hit3d_gpu_sgs_fields(self._h, int(kind), float(delta),
+                                          out.ctypes.data_as(C.POINTER(C.c_float))), "sgs_fields")
         return out
 
     def velocity_rescale(self, isp_type: int, peak_wavenum: float, ir_exp: float = 2.0):

@@ -176,6 +176,17 @@ int hit3d_gpu_xfft3d_static(int32_t n, const double *in, double *out, void *stre
  * function prod sin(k delta/2)/(k delta/2) (no reference counterpart). */
 int hit3d_gpu_filter_field(hit3d_ctx *ctx, int32_t kind, double delta, int32_t field);
 
+/* Training data of a learned subgrid closure from the current (DNS) state: with
+ * the filter of hit3d_gpu_filter_field (kind 2 Gaussian, 4 box of width delta),
+ * out receives 18 compact float32 fields (nx, ny, nz) in this order:
+ *   ubar_1..3   filtered velocity,
+ *   tau_11, tau_12, tau_13, tau_22, tau_23, tau_33   exact subgrid stress
+ *               filter(u_i u_j) - ubar_i ubar_j (the Leonard-stress formula of
+ *               m_les.f90:1847-1865 applied to the DNS field),
+ *   A_ij = d ubar_i / dx_j, i-major (9 fields).
+ * Needs FP64 transforms (precision 0); uses 6 extra fields of device memory. */
+int hit3d_gpu_sgs_fields(hit3d_ctx *ctx, int32_t kind, double delta, float *out);
+
 /* Physical-space copies of the first nf state fields, out(ld1, ny, nz, nf), with
  * every mode of |k|^2 > k2max zeroed first when k2max > 0 (the spherical
  * truncation and inverse transforms of io_write_4, io_write_4.f90:21-90; the
@@ -190,6 +201,24 @@ int hit3d_gpu_velocity_rescale(hit3d_ctx *ctx, int32_t isp_type, double peak_wav
 /* Physical-space velocity (x, y, z) of the current state, as the reference's
  * wrk1..3 after rhs_scalars (main.f90:126): out(ld1, ny, nz, 3). */
 int hit3d_gpu_physical_velocity(hit3d_ctx *ctx, double *out, int64_t ld1);
+
+/* ---------------------------------------------------------------------------
+ * Batched form (no reference counterpart: the reference runs one simulation per
+ * MPI job).  Many independent runs of uneven sizes, each with its own
+ * parameters (Re, seeds), on one GPU.  hit3d_batch_step takes the first-order
+ * step of new runs eagerly, then records `graph_steps` Adams-Bashforth steps of
+ * all runs into one CUDA graph (a branch per run) and replays it, one launch per
+ * chunk.  dt and the scalar switch are baked into the recording: change them
+ * only between calls (the graph is re-recorded when graph_steps changes).
+ * ------------------------------------------------------------------------- */
+typedef struct hit3d_batch hit3d_batch;
+int hit3d_batch_create(const hit3d_params *p /* [nruns] */, int32_t nruns, hit3d_batch **out);
+/* The context of run r, for initial conditions, transfers and statistics. */
+int hit3d_batch_context(hit3d_batch *b, int32_t r, hit3d_ctx **ctx);
+int hit3d_batch_step(hit3d_batch *b, int32_t nsteps, int32_t graph_steps);
+/* Number of graph launches so far. */
+int64_t hit3d_batch_graph_launches(hit3d_batch *b);
+void hit3d_batch_destroy(hit3d_batch *b);
 
 #ifdef __cplusplus
 }
