@@ -37,7 +37,7 @@ sys.path.insert(0, ROOT)
 
 N_DEFAULT = 512
 RE = 3000.0
-DT = 0.001
+DT = 0.0002  # Courant number about 0.1 in the developed flow, as the reference keeps it (my_dt.f90)
 RN1 = 67748937.0
 METRIC = "timesteps/s at 512^3 FP64 (forced DNS, 2/3 rule)"
 

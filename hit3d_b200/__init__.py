@@ -5,6 +5,6 @@ from ``csrc/`` for sm_100a.  This package binds it (``gpu``), parses the
 reference's input file (``params``) and restates the reference's host main loop
 over the C-ABI (``driver``).
 """
-from .gpu import Context, Hit3dError, Params, lib  # noqa: F401
+from .gpu import Context, Hit3dError, Mlp, Params, lib  # noqa: F401
 
-__all__ = ["Context", "Hit3dError", "Params", "lib"]
+__all__ = ["Context", "Hit3dError", "Mlp", "Params", "lib"]

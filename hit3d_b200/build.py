@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhit3d_gpu.so")
-SOURCES = ["hit3d.cu", "noalloc.cu"]
+SOURCES = ["hit3d.cu", "noalloc.cu", "mlp.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

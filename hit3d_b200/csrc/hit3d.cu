@@ -145,7 +145,13 @@ struct hit3d_ctx {
     int64_t nlaunch;
     int xcfg;            // launch-shape variant of the fused x pass
     double k2max;        // truncation radius squared of PRE_TRUNC
+    void *mlp_wb;        // bf16 weights of the learned closure (les_model 2)
+    double mlp_delta;    // filter width the closure was trained for
+    int mlp_clip;        // zero the stress where its dissipation is negative
 };
+
+int h3d_mlp_apply(cudaStream_t st, int fp64, int64_t np, int64_t n, int64_t rp, int64_t fs, double delta, int clip,
+                  const void *wb, void *G);
 
 static int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 
@@ -184,6 +190,7 @@ static int zinv_L(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src
     case PRE_SHIFT: return zinv_LM<T, L, PRE_SHIFT>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
     case PRE_STRAIN_A: return zinv_LM<T, L, PRE_STRAIN_A>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
     case PRE_STRAIN_B: return zinv_LM<T, L, PRE_STRAIN_B>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+    case PRE_GRAD: return zinv_LM<T, L, PRE_GRAD>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
     default: break;
     }
     if constexpr (std::is_same<T, double>::value) {
@@ -191,7 +198,6 @@ static int zinv_L(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src
         switch (mode) {
         case PRE_CURL: return zinv_LM<T, L, PRE_CURL>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         case PRE_DLONG: return zinv_LM<T, L, PRE_DLONG>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
-        case PRE_GRAD: return zinv_LM<T, L, PRE_GRAD>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         case PRE_TRUNC: return zinv_LM<T, L, PRE_TRUNC>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         default: break;
         }
@@ -377,7 +383,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     auto Wf = [&](int i) { return W + i * wfs; };
     const int ns = c->int_scalars ? c->nsc : 0;
     const int nprod = 6 + 3 * ns;
-    const bool les = p.les_model == 1;
+    const bool les = p.les_model == 1, les_mlp = p.les_model == 2;
 
     StepArgs a;
     memset(&a, 0, sizeof a);
@@ -453,6 +459,22 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
             double cd = p.c_smag * c->dx;
             fa.p0 = cd * cd;
             H3D_TRY((xfused<T, OpSmag>(c, fa)));
+            H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, 6));
+            H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, 6));
+            tau = Wf(t0);
+        }
+        if (les_mlp) {
+            MARK(6);
+            // learned closure: the nine velocity gradients in physical space, the
+            // network per point, the six stresses back to spectral space
+            const int t0 = nprod;
+            for (int i = 0; i < 3; i++) H3D_TRY(zinv<T>(c, 3, PRE_GRAD, i, c->U, c->fs64, Wf(t0 + 3 * i), wfs, wp));
+            H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, 9));
+            H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, 9));
+            H3D_TRY(h3d_mlp_apply(c->st, sizeof(T) == 8, (int64_t)c->n * c->n * c->n, c->n, 2 * (int64_t)wp, 2 * wfs,
+                                  c->mlp_delta, c->mlp_clip, c->mlp_wb, Wf(t0)));
+            c->nlaunch++;
+            H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, 6));
             H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, 6));
             H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, 6));
             tau = Wf(t0);
@@ -548,8 +570,8 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     if (p->dealias != 0 && p->dealias != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: wrong dealias flag");
     if (p->flow_type == 1 && p->force_type != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: WRONG FORCE TYPE");
     if (p->flow_type == 1 && (p->kfmax < 1 || p->kfmax > 15)) return h3d_set_error_msg(-1, "hit3d_gpu_init: kfmax must be in 1..15");
-    if (p->les_model != 0 && p->les_model != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: only les_model 0 and 1 are supported");
-    if (p->les_model == 1 && p->n_scalars > 0) return h3d_set_error_msg(-1, "hit3d_gpu_init: LES with scalars is not supported");
+    if (p->les_model < 0 || p->les_model > 2) return h3d_set_error_msg(-1, "hit3d_gpu_init: only les_model 0, 1 and 2 are supported");
+    if (p->les_model != 0 && p->n_scalars > 0) return h3d_set_error_msg(-1, "hit3d_gpu_init: LES with scalars is not supported");
     if (p->precision != 0 && p->precision != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: precision must be 0 or 1");
     for (int s = 0; s < p->n_scalars; s++) {
         if (p->scalar_type[s] >= 100) return h3d_set_error_msg(-1, "hit3d_gpu_init: reacting scalars are not supported");
@@ -578,7 +600,7 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     int rc = 0;
     const int nf = 3 + c->nsc;
     const size_t f64 = (size_t)c->fs64 * sizeof(double2);
-    c->nw = 6 + 3 * c->nsc + (c->p.les_model ? 6 : 0);
+    c->nw = 6 + 3 * c->nsc + (c->p.les_model == 1 ? 6 : c->p.les_model == 2 ? 9 : 0);
     if (c->p.precision == 0) {
         c->wpitch = c->P64;
         c->wfs = c->fs64;
@@ -636,7 +658,7 @@ extern "C" void hit3d_gpu_finalize(hit3d_ctx *c)
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->W64 && c->W64 != c->W) cudaFree(c->W64);
     void *ptrs[] = {c->U, c->RO, c->RP, c->SP, c->W, c->phys, c->tw64, c->tw32, c->d_fen, c->d_part,
-                    c->d_red, c->d_ratio, c->d_cmax, c->stage, c->d_xyz, c->d_uvw, c->sgs};
+                    c->d_red, c->d_ratio, c->d_cmax, c->stage, c->d_xyz, c->d_uvw, c->sgs, c->mlp_wb};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
@@ -695,6 +717,8 @@ extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_
 {
     if (!c) return h3d_set_error_msg(-1, "null context");
     if (nsteps < 0) return h3d_set_error_msg(-1, "nsteps < 0");
+    if (c->p.les_model == 2 && !c->mlp_wb)
+        return h3d_set_error_msg(-1, "hit3d_gpu_step: les_model 2 needs weights (hit3d_gpu_les_set_mlp)");
     H3D_CHECK(cudaSetDevice(c->dev));
     int ev = fov ? (*fov != 0) : 0, es = fos ? (*fos != 0) : 0;
     for (int it = 0; it < nsteps; it++) {
@@ -714,6 +738,22 @@ extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_
         *courant = cm * c->p.dt / c->dx;
     }
     H3D_CHECK(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int hit3d_mlp_nparam(void);
+extern "C" int hit3d_gpu_les_set_mlp(hit3d_ctx *c, const uint16_t *wb, int64_t nparam, double delta, int32_t clip)
+{
+    if (!c || !wb) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: null argument");
+    if (c->p.les_model != 2) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: the context needs les_model 2");
+    if (nparam != hit3d_mlp_nparam()) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: wrong parameter count");
+    if (!(delta > 0.0)) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: filter width must be positive");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    if (!c->mlp_wb) H3D_TRY(ctx_alloc(&c->mlp_wb, sizeof(uint16_t) * (size_t)nparam));
+    H3D_CHECK(cudaMemcpyAsync(c->mlp_wb, wb, sizeof(uint16_t) * (size_t)nparam, cudaMemcpyHostToDevice, c->st));
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    c->mlp_delta = delta;
+    c->mlp_clip = clip != 0;
     return 0;
 }
 
@@ -1101,12 +1141,12 @@ extern "C" int hit3d_gpu_filter_field(hit3d_ctx *c, int32_t kind, double delta, 
 }
 
 // download physical rows of nf FP64 fields as compact FP32 [f][z][y][x]
-static int download_f32(hit3d_ctx *c, const double2 *base, int nf, float *out)
+static int download_f32(hit3d_ctx *c, const double2 *base, int nf, float *out, int stride = 1)
 {
-    const int64_t np = (int64_t)c->n * c->n * c->n;
+    const int64_t m = c->n / stride, np = m * m * m;
     float *st = reinterpret_cast<float *>(c->stage);  // n*n*nh double2 >= n^3 floats
     for (int f = 0; f < nf; f++) {
-        k_phys_to_f32<<<pw_grid(c), 256, 0, c->st>>>(c->n, 2 * (int64_t)c->P64,
+        k_phys_to_f32<<<pw_grid(c), 256, 0, c->st>>>(c->n, 2 * (int64_t)c->P64, stride,
                                                      reinterpret_cast<const double *>(base + f * c->fs64), st);
         H3D_LAUNCH_CHECK();
         H3D_CHECK(cudaMemcpyAsync(out + f * np, st, sizeof(float) * np, cudaMemcpyDeviceToHost, c->st));
@@ -1115,12 +1155,13 @@ static int download_f32(hit3d_ctx *c, const double2 *base, int nf, float *out)
     return 0;
 }
 
-extern "C" int hit3d_gpu_sgs_fields(hit3d_ctx *c, int32_t kind, double delta, float *out)
+extern "C" int hit3d_gpu_sgs_samples(hit3d_ctx *c, int32_t kind, double delta, int32_t stride, float *out)
 {
     if (!c || !out) return h3d_set_error_msg(-1, "hit3d_gpu_sgs_fields: null argument");
     if (c->p.precision != 0) return h3d_set_error_msg(-1, "hit3d_gpu_sgs_fields: needs a context with FP64 transforms");
+    if (stride < 1 || c->n % stride != 0) return h3d_set_error_msg(-1, "hit3d_gpu_sgs_samples: stride must divide nx");
     H3D_CHECK(cudaSetDevice(c->dev));
-    const int64_t np = (int64_t)c->n * c->n * c->n;
+    const int64_t m = c->n / stride, np = m * m * m;
     if (!c->sgs) H3D_TRY(ctx_alloc((void **)&c->sgs, sizeof(double2) * 6 * (size_t)c->fs64));
     double2 *W = reinterpret_cast<double2 *>(c->W);
     const int64_t fs = c->fs64;
@@ -1164,7 +1205,7 @@ extern "C" int hit3d_gpu_sgs_fields(hit3d_ctx *c, int32_t kind, double delta, fl
         H3D_TRY(zinv<double>(c, 3, PRE_GRAD, i, c->sgs, fs, tmp, fs, P));
         H3D_TRY(spass<double>(c, 1, false, tmp, fs, P, 3));
         H3D_TRY(xc2r<double>(c, tmp, fs, P, 3));
-        H3D_TRY(download_f32(c, tmp, 3, out + (9 + 3 * i) * np));
+        H3D_TRY(download_f32(c, tmp, 3, out + (9 + 3 * i) * np, stride));
     }
     // 5. physical filtered velocity and products; tau in place of the products
     H3D_TRY(inv3d64(c, c->sgs, 3));
@@ -1172,9 +1213,14 @@ extern "C" int hit3d_gpu_sgs_fields(hit3d_ctx *c, int32_t kind, double delta, fl
     k_sgs_tau<<<pw_grid(c), 256, 0, c->st>>>(c->n, 2 * (int64_t)P, 2 * fs, reinterpret_cast<const double *>(c->sgs),
                                              reinterpret_cast<double *>(W));
     H3D_LAUNCH_CHECK();
-    H3D_TRY(download_f32(c, c->sgs, 3, out));
-    H3D_TRY(download_f32(c, W, 6, out + 3 * np));
+    H3D_TRY(download_f32(c, c->sgs, 3, out, stride));
+    H3D_TRY(download_f32(c, W, 6, out + 3 * np, stride));
     return 0;
+}
+
+extern "C" int hit3d_gpu_sgs_fields(hit3d_ctx *c, int32_t kind, double delta, float *out)
+{
+    return hit3d_gpu_sgs_samples(c, kind, delta, 1, out);
 }
 
 extern "C" int hit3d_gpu_physical_fields(hit3d_ctx *c, int32_t nf, double k2max, double *out, int64_t ld1)
@@ -1291,6 +1337,8 @@ struct hit3d_batch {
     cudaGraphExec_t exec = nullptr;
     int graph_steps = 0;
     int64_t launches = 0;
+    std::vector<double> cap_dt;  // dt and scalar switch of every run when the graph was recorded
+    std::vector<int> cap_scal;
 };
 
 static int run_step(hit3d_ctx *c, int ev, int es)
@@ -1372,6 +1420,12 @@ static int batch_capture(hit3d_batch *b, int steps)
     b->graph = g;
     H3D_CHECK(cudaGraphInstantiate(&b->exec, g, 0));
     b->graph_steps = steps;
+    b->cap_dt.clear();
+    b->cap_scal.clear();
+    for (hit3d_ctx *cr : b->runs) {
+        b->cap_dt.push_back(cr->p.dt);
+        b->cap_scal.push_back(cr->int_scalars);
+    }
     (void)c;
     return 0;
 }
@@ -1395,7 +1449,10 @@ extern "C" int hit3d_batch_step(hit3d_batch *b, int32_t nsteps, int32_t graph_st
         left--;
     }
     if (left >= graph_steps) {
-        if (!b->exec || b->graph_steps != graph_steps) {
+        bool stale = !b->exec || b->graph_steps != graph_steps || b->cap_dt.size() != b->runs.size();
+        for (size_t r = 0; !stale && r < b->runs.size(); r++)
+            stale = b->cap_dt[r] != b->runs[r]->p.dt || b->cap_scal[r] != b->runs[r]->int_scalars;
+        if (stale) {
             for (hit3d_ctx *cr : b->runs) H3D_CHECK(cudaStreamSynchronize(cr->st));
             H3D_TRY(batch_capture(b, graph_steps));
         }

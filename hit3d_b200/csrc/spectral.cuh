@@ -529,12 +529,14 @@ __global__ void k_box_transfer(int n, int nh, int pitch, double delta, double2 *
 }
 
 // physical rows (pitch rp reals) -> compact FP32 [z][y][x]
-__global__ void k_phys_to_f32(int n, int64_t rp, const double *__restrict__ src, float *__restrict__ dst)
+// every stride-th point per axis of a physical field (m = n / stride points per axis)
+__global__ void k_phys_to_f32(int n, int64_t rp, int stride, const double *__restrict__ src, float *__restrict__ dst)
 {
-    const int64_t np = (int64_t)n * n * n;
+    const int m = n / stride;
+    const int64_t np = (int64_t)m * m * m;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
-        int64_t row = t / n, x = t - row * n;
-        dst[t] = (float)src[row * rp + x];
+        const int64_t row = t / m, x = t - row * m, z = row / m, y = row - z * m;
+        dst[t] = (float)src[(z * stride * n + y * stride) * rp + x * stride];
     }
 }
 

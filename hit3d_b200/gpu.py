@@ -82,6 +82,7 @@ class Params:
 
 # (name, restype, argtypes) of every entry point of include/hit3d_gpu.h
 _vp, _dp, _i32, _i64, _d = C.c_void_p, C.POINTER(C.c_double), C.c_int32, C.c_int64, C.c_double
+_fp = C.POINTER(C.c_float)
 SIGNATURES = [
     ("hit3d_gpu_init", C.c_int, [C.POINTER(_Params), C.POINTER(C.c_void_p)]),
     ("hit3d_gpu_finalize", None, [_vp]),
@@ -111,11 +112,24 @@ SIGNATURES = [
     ("hit3d_gpu_physical_fields", C.c_int, [_vp, _i32, _d, _dp, _i64]),
     ("hit3d_gpu_velocity_rescale", C.c_int, [_vp, _i32, _d, _d]),
     ("hit3d_gpu_sgs_fields", C.c_int, [_vp, _i32, _d, C.POINTER(C.c_float)]),
+    ("hit3d_gpu_sgs_samples", C.c_int, [_vp, _i32, _d, _i32, C.POINTER(C.c_float)]),
     ("hit3d_batch_create", C.c_int, [C.POINTER(_Params), _i32, C.POINTER(C.c_void_p)]),
     ("hit3d_batch_context", C.c_int, [_vp, _i32, C.POINTER(C.c_void_p)]),
     ("hit3d_batch_step", C.c_int, [_vp, _i32, _i32]),
     ("hit3d_batch_graph_launches", C.c_int64, [_vp]),
     ("hit3d_batch_destroy", None, [_vp]),
+    ("hit3d_mlp_nparam", C.c_int, []),
+    ("hit3d_mlp_create", C.c_int, [_i32, C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("hit3d_mlp_destroy", C.c_int, [_vp]),
+    ("hit3d_mlp_set_params", C.c_int, [_vp, _fp]),
+    ("hit3d_mlp_get_params", C.c_int, [_vp, _fp]),
+    ("hit3d_mlp_get_bf16", C.c_int, [_vp, C.POINTER(C.c_uint16)]),
+    ("hit3d_mlp_set_data", C.c_int, [_vp, _fp, _fp, _i64, _d]),
+    ("hit3d_mlp_norms", C.c_int, [_vp, _dp]),
+    ("hit3d_mlp_loss_grad", C.c_int, [_vp, C.POINTER(_i32), _i64, _d, _fp, _fp]),
+    ("hit3d_mlp_train", C.c_int, [_vp, _i32, _i64, _d, _d, C.c_uint64, _fp]),
+    ("hit3d_mlp_predict", C.c_int, [_vp, _fp, _i64, _d, _i32, _fp]),
+    ("hit3d_gpu_les_set_mlp", C.c_int, [_vp, C.POINTER(C.c_uint16), _i64, _d, _i32]),
 ]
 
 
@@ -318,6 +332,14 @@ class Context:
                                           out.ctypes.data_as(C.POINTER(C.c_float))), "sgs_fields")
         return out
 
+    def sgs_samples(self, kind: int, delta: float, stride: int) -> np.ndarray:
+        """sgs_fields on every stride-th point per axis: (18, m, m, m), m = nx / stride."""
+        m = self.n // stride
+        out = np.empty((18, m, m, m), dtype=np.float32)
+        _check(lib().hit3d_gpu_sgs_samples(self._h, int(kind), float(delta), int(stride),
+                                           out.ctypes.data_as(C.POINTER(C.c_float))), "sgs_samples")
+        return out
+
     def velocity_rescale(self, isp_type: int, peak_wavenum: float, ir_exp: float = 2.0):
         _check(lib().hit3d_gpu_velocity_rescale(self._h, int(isp_type), float(peak_wavenum), float(ir_exp)),
                "velocity_rescale")
@@ -325,4 +347,96 @@ class Context:
     def physical_velocity(self) -> np.ndarray:
         out = np.zeros((3, self.n, self.n, self.n + 2))
         _check(lib().hit3d_gpu_physical_velocity(self._h, _ptr(out), self.n + 2), "physical_velocity")
+        return out
+
+    def les_set_mlp(self, bf16_weights: np.ndarray, delta: float, clip: bool = True):
+        """Use trained bf16 weights (uint16 bit patterns) as this context's subgrid model
+        (les_model 2); delta is the filter width the network was trained for."""
+        w = np.ascontiguousarray(bf16_weights, dtype=np.uint16)
+        _check(lib().hit3d_gpu_les_set_mlp(self._h, w.ctypes.data_as(C.POINTER(C.c_uint16)), w.size, float(delta),
+                                           int(bool(clip))), "les_set_mlp")
+
+
+def _f32(a: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a
+
+
+class Mlp:
+    """The learned subgrid closure on one GPU: parameters, training data, the
+    training step and inference (hit3d_mlp_* in the C-ABI)."""
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        h = C.c_void_p()
+        _check(lib().hit3d_mlp_create(int(device), int(seed) & (2**64 - 1), C.byref(h)), "hit3d_mlp_create")
+        self._h = h
+        self.nparam = int(lib().hit3d_mlp_nparam())
+        self.delta = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().hit3d_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> np.ndarray:
+        w = np.empty(self.nparam, dtype=np.float32)
+        _check(lib().hit3d_mlp_get_params(self._h, w.ctypes.data_as(_fp)), "hit3d_mlp_get_params")
+        return w
+
+    @params.setter
+    def params(self, w: np.ndarray):
+        w = _f32(w)
+        if w.size != self.nparam:
+            raise ValueError(f"expected {self.nparam} parameters")
+        _check(lib().hit3d_mlp_set_params(self._h, w.ctypes.data_as(_fp)), "hit3d_mlp_set_params")
+
+    def bf16(self) -> np.ndarray:
+        w = np.empty(self.nparam, dtype=np.uint16)
+        _check(lib().hit3d_mlp_get_bf16(self._h, w.ctypes.data_as(C.POINTER(C.c_uint16))), "hit3d_mlp_get_bf16")
+        return w
+
+    def set_data(self, A: np.ndarray, tau: np.ndarray, delta: float):
+        """A: (9, P) gradients d u_i/d x_j at row 3i+j; tau: (6, P) stresses (11 12 13 22 23 33)."""
+        A = _f32(A).reshape(9, -1)
+        tau = _f32(tau).reshape(6, -1)
+        if A.shape[1] != tau.shape[1]:
+            raise ValueError("A and tau disagree on the number of points")
+        _check(lib().hit3d_mlp_set_data(self._h, A.ctypes.data_as(_fp), tau.ctypes.data_as(_fp), A.shape[1],
+                                        float(delta)), "hit3d_mlp_set_data")
+        self.delta = float(delta)
+
+    def norms(self):
+        out = np.zeros(2)
+        _check(lib().hit3d_mlp_norms(self._h, _ptr(out)), "hit3d_mlp_norms")
+        return float(out[0]), float(out[1])
+
+    def loss_grad(self, idx: np.ndarray, lam: float = 0.0):
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        loss = C.c_float()
+        g = np.empty(self.nparam, dtype=np.float32)
+        _check(lib().hit3d_mlp_loss_grad(self._h, idx.ctypes.data_as(C.POINTER(_i32)), idx.size, float(lam),
+                                         C.byref(loss), g.ctypes.data_as(_fp)), "hit3d_mlp_loss_grad")
+        return float(loss.value), g
+
+    def train(self, nsteps: int, batch: int = 16384, lr: float = 1e-3, lam: float = 0.0, seed: int = 1) -> np.ndarray:
+        losses = np.empty(max(int(nsteps), 1), dtype=np.float32)
+        _check(lib().hit3d_mlp_train(self._h, int(nsteps), int(batch), float(lr), float(lam),
+                                     int(seed) & (2**64 - 1), losses.ctypes.data_as(_fp)), "hit3d_mlp_train")
+        return losses[:nsteps]
+
+    def predict(self, A: np.ndarray, delta: float | None = None, clip: bool = False) -> np.ndarray:
+        A = _f32(A).reshape(9, -1)
+        d = self.delta if delta is None else delta
+        if d is None:
+            raise ValueError("no filter width")
+        out = np.empty((6, A.shape[1]), dtype=np.float32)
+        _check(lib().hit3d_mlp_predict(self._h, A.ctypes.data_as(_fp), A.shape[1], float(d), int(bool(clip)),
+                                       out.ctypes.data_as(_fp)), "hit3d_mlp_predict")
         return out

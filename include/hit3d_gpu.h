@@ -45,7 +45,8 @@ typedef struct hit3d_params {
     int32_t n_scalars;   /* passive scalars, <= HIT3D_MAX_SCALARS (m_parameters.f90:424)   */
     int32_t precision;   /* 0: FP64 transforms; 1: FP32 nonlinear-term transforms with FP64
                             state, integrator and reductions (no reference counterpart)    */
-    int32_t les_model;   /* 0: none; 1: Smagorinsky (m_les.f90:94-106)                     */
+    int32_t les_model;   /* 0: none; 1: Smagorinsky (m_les.f90:94-106); 2: learned closure
+                            (hit3d_gpu_les_set_mlp; no reference counterpart)              */
     int32_t scalar_type[HIT3D_MAX_SCALARS]; /* 0 = uniform mean gradient source            */
     int32_t device;      /* CUDA device ordinal                                            */
     int32_t reserved;
@@ -186,6 +187,9 @@ int hit3d_gpu_filter_field(hit3d_ctx *ctx, int32_t kind, double delta, int32_t f
  *   A_ij = d ubar_i / dx_j, i-major (9 fields).
  * Needs FP64 transforms (precision 0); uses 6 extra fields of device memory. */
 int hit3d_gpu_sgs_fields(hit3d_ctx *ctx, int32_t kind, double delta, float *out);
+/* The same on every stride-th point per axis (stride divides nx):
+ * out(18, m, m, m) with m = nx / stride. */
+int hit3d_gpu_sgs_samples(hit3d_ctx *ctx, int32_t kind, double delta, int32_t stride, float *out);
 
 /* Physical-space copies of the first nf state fields, out(ld1, ny, nz, nf), with
  * every mode of |k|^2 > k2max zeroed first when k2max > 0 (the spherical
@@ -209,7 +213,9 @@ int hit3d_gpu_physical_velocity(hit3d_ctx *ctx, double *out, int64_t ld1);
  * step of new runs eagerly, then records `graph_steps` Adams-Bashforth steps of
  * all runs into one CUDA graph (a branch per run) and replays it, one launch per
  * chunk.  dt and the scalar switch are baked into the recording: change them
- * only between calls (the graph is re-recorded when graph_steps changes).
+ * (hit3d_gpu_set_dt, hit3d_gpu_set_scalars_active on a run's context) only
+ * between calls; the next call re-records the graph when either, or
+ * graph_steps, has changed.
  * ------------------------------------------------------------------------- */
 typedef struct hit3d_batch hit3d_batch;
 int hit3d_batch_create(const hit3d_params *p /* [nruns] */, int32_t nruns, hit3d_batch **out);
@@ -219,6 +225,48 @@ int hit3d_batch_step(hit3d_batch *b, int32_t nsteps, int32_t graph_steps);
 /* Number of graph launches so far. */
 int64_t hit3d_batch_graph_launches(hit3d_batch *b);
 void hit3d_batch_destroy(hit3d_batch *b);
+
+/* ---------------------------------------------------------------------------
+ * Learned subgrid closure (no reference counterpart; the reference's LES models
+ * are in m_les.f90, and its Smagorinsky model, m_les.f90:1142-1215, is the
+ * fallback).  A network g = MLP(x), 6 -> 64 -> 64 -> 64 -> 5 with GELU, maps
+ * five invariants of the normalised filtered velocity gradient and the filter
+ * width to the coefficients of a five-tensor basis, and
+ *     tau_ij = Delta^2 |S|^2 sum_n g_n T^(n)_ij      (deviatoric).
+ * Weights are bf16, every product is accumulated in fp32.  Parameters are a
+ * flat fp32 vector of hit3d_mlp_nparam() values: W1[64][6] b1[64] W2[64][64]
+ * b2[64] W3[64][64] b3[64] W4[5][64] b4[5].  Gradient fields A are [9][P]
+ * with A[3i+j] = d u_i / d x_j; stresses are [6][P] in the order
+ * 11 12 13 22 23 33.
+ * ------------------------------------------------------------------------- */
+typedef struct hit3d_mlp hit3d_mlp;
+int hit3d_mlp_nparam(void);
+/* Glorot-uniform initial weights from `seed`. */
+int hit3d_mlp_create(int32_t device, uint64_t seed, hit3d_mlp **out);
+int hit3d_mlp_destroy(hit3d_mlp *m);
+/* fp32 master parameters; setting them also resets the Adam moments. */
+int hit3d_mlp_set_params(hit3d_mlp *m, const float *w);
+int hit3d_mlp_get_params(hit3d_mlp *m, float *w);
+/* the bf16 weights the kernels use (raw bf16 bit patterns) */
+int hit3d_mlp_get_bf16(hit3d_mlp *m, uint16_t *wb);
+/* Training data from filtered DNS (hit3d_gpu_sgs_fields): gradients and
+ * stresses at P points, filter width delta.  Stresses are made deviatoric. */
+int hit3d_mlp_set_data(hit3d_mlp *m, const float *A, const float *tau, int64_t P, double delta);
+/* out2 = {1 / mean |tau|_F^2, 1 / mean (tau:S)^2} over the data set */
+int hit3d_mlp_norms(hit3d_mlp *m, double *out2);
+/* Loss and its gradient with respect to the parameters (evaluated at the bf16
+ * weights) for the data points idx[0..np):
+ *   L = n1/np sum |tau_pred - tau|_F^2 + lam n2/np sum (tau_pred:S - tau:S)^2 */
+int hit3d_mlp_loss_grad(hit3d_mlp *m, const int32_t *idx, int64_t np, double lam, float *loss, float *grad);
+/* nsteps Adam steps (lr, betas 0.9/0.999) on minibatches of `batch` points
+ * drawn from the data set by a hash of (seed, step); losses[nsteps] may be null. */
+int hit3d_mlp_train(hit3d_mlp *m, int32_t nsteps, int64_t batch, double lr, double lam, uint64_t seed, float *losses);
+/* Stresses predicted at np points; with clip, points whose predicted
+ * dissipation -tau:S is negative get tau = 0. */
+int hit3d_mlp_predict(hit3d_mlp *m, const float *A, int64_t np, double delta, int32_t clip, float *tau);
+/* Use a trained network as the context's subgrid model (les_model 2): nparam
+ * bf16 weights, the filter width they were trained for, the clip switch. */
+int hit3d_gpu_les_set_mlp(hit3d_ctx *ctx, const uint16_t *bf16_weights, int64_t nparam, double delta, int32_t clip);
 
 #ifdef __cplusplus
 }

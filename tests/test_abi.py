@@ -14,7 +14,7 @@ HEADER = os.path.join(ROOT, "include", "hit3d_gpu.h")
 
 def declared_functions():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"\b(hit3d_(?:gpu|batch)_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(hit3d_(?:gpu|batch|mlp)_\w+)\s*\(", text)))
 
 
 def test_header_declares_every_binding():

@@ -69,3 +69,28 @@ def test_sgs_fields_match_oracle():
     ref = ub + tau + A
     for q in range(18):
         assert relerr(out[q], ref[q]) < 2e-6, q
+
+
+def test_batch_rerecords_graph_after_dt_change():
+    """dt is baked into the recorded graph; changing it on a run's context between
+    calls must take effect (the graph is re-recorded)."""
+    from hit3d_b200 import Context, Params
+    from hit3d_b200.batch import Batch, run_seed
+    ps = [Params(nx=32, flow_type=1, kfmax=2, nu=1.0 / 300, dt=0.004) for _ in range(2)]
+    b = Batch(ps)
+    b.init()
+    b.step(6, graph_steps=5)
+    for c in b.contexts:
+        c.set_dt(0.002)
+    b.step(10, graph_steps=5)
+    assert b.graph_launches == 3
+    for r, p in enumerate(ps):
+        c = Context(Params(nx=32, flow_type=1, kfmax=2, nu=1.0 / 300, dt=0.004))
+        c.init_velocity(run_seed(r), 2, 4.0, 2.0)
+        c.dealias_all()
+        c.step(6)
+        c.set_dt(0.002)
+        c.step(10)
+        assert np.array_equal(b.contexts[r].download_fields(), c.download_fields())
+        c.close()
+    b.close()

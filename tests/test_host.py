@@ -96,3 +96,29 @@ def test_real4_layout(tmp_path):
     assert os.path.getsize(p) == 12 + 4 * 4 * 4 * 4
     b = read_real4(p)
     assert np.array_equal(b, a[:, :, :4].astype(np.float32))
+
+
+def test_spectral_truncate_maps_modes_between_grids():
+    """A field made of modes |k_i| < n/2 has the same (rescaled) coefficients on an
+    N^3 and an n^3 grid; the reference layout is [ky][kz][kx re/im]."""
+    from hit3d_b200.les import spectral_truncate
+    rng = np.random.default_rng(0)
+    N, n = 16, 8
+    modes = [(int(a), int(b), int(c), rng.standard_normal(), rng.standard_normal())
+             for a, b, c in rng.integers(-3, 4, size=(12, 3))]
+
+    def ref_layout(m):
+        x = np.arange(m) * 2 * np.pi / m
+        Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
+        f = sum(a * np.cos(kx * X + ky * Y + kz * Z) + b * np.sin(kx * X + ky * Y + kz * Z)
+                for kx, ky, kz, a, b in modes)
+        F = np.fft.rfftn(f)                # [kz][ky][kx], unnormalised, e^{-i}
+        F = F.transpose(1, 0, 2)           # [ky][kz][kx]
+        out = np.zeros((1, m, m, m + 2))
+        out[0, ..., 0::2], out[0, ..., 1::2] = F.real, F.imag
+        return out
+
+    got = spectral_truncate(ref_layout(N), n)
+    want = ref_layout(n)
+    want[..., n // 2 * 2:] = 0.0  # kx Nyquist column is not carried over
+    assert np.abs(got - want).max() < 1e-9 * np.abs(want).max()
