@@ -45,7 +45,7 @@ METRIC = "timesteps/s at 512^3 FP64 (forced DNS, 2/3 rule)"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
@@ -53,6 +53,14 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-transform form")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-les", action="store_true", help="skip the learned-LES leg")
+    ap.add_argument("--les-full", action="store_true",
+                    help="a-posteriori test at 512^3 DNS -> 128^3 LES (minutes) instead of 128^3 -> 32^3")
+    ap.add_argument("--les-only", action="store_true", help="only the learned-LES step rates (profiling runs)")
+    ap.add_argument("--cmp-every", type=int, default=50, help="FP32 vs FP64 statistics every this many steps")
+    ap.add_argument("--cmp-points", type=int, default=4)
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="fix the fused x-pass launch shape instead of tuning (profiling runs)")
     return ap.parse_args()
 
 
@@ -190,6 +198,67 @@ def cpu_sample(n_gpu, fields0):
                       f"N^3 log2 N^3 work ratio {scale:.2f} to {n_gpu}^3"}
 
 
+def les_leg(torch, args, dns_rate, dns32_rate, device):
+    """Learned-closure LES at 128^3 against the 512^3 DNS: step rates, the
+    simulated-time speedup at equal Courant number (dt_les = 4 dt_dns), and an
+    a-posteriori spectrum test against filtered DNS."""
+    from hit3d_b200 import Context, Params
+    from hit3d_b200.les import LesExperiment, run_experiment
+    from hit3d_b200 import gpu
+    n_les, ratio = 128, 2.0
+    dt_les = DT * args.n / n_les
+    delta = ratio * 2.0 * np.pi / n_les
+    out = {"grid": n_les, "dt_les": dt_les, "dt_dns": DT, "filter_width": delta}
+    # step cost does not depend on the weight values: time with the Smagorinsky-
+    # equivalent network g = (-2 Cs^2 dx^2 / Delta^2, 0, 0, 0, 0)
+    nparam = int(gpu.lib().hit3d_mlp_nparam())
+    w = np.zeros(nparam, dtype=np.float32)
+    dx = 2.0 * np.pi / n_les
+    w[nparam - 5] = -2.0 * 0.18 ** 2 * dx * dx / (delta * delta)
+    bits = ((w.view(np.uint32).astype(np.uint64) + 0x7FFF + ((w.view(np.uint32) >> 16) & 1)) >> 16).astype(np.uint16)
+    rates = {}
+    for name, model, kernel in (("learned", 2, 1), ("learned_cuda_cores", 2, 0), ("smagorinsky", 1, 0)):
+        c = Context(Params(nx=n_les, dealias=0, flow_type=1, force_type=1, kfmax=2, famp=0.5, nu=1.0 / RE, dt=dt_les,
+                           les_model=model, device=device))
+        if model == 2:
+            c.les_set_mlp(bits, delta, clip=True, kernel=kernel)
+        c.init_velocity(RN1, 2, 4.0, 2.0)
+        c.dealias_all()
+        if args.variant >= 0:
+            c.set_variant(args.variant)
+        else:
+            c.autotune()
+        c.step(args.warmup)
+        steps = max(args.steps, 50)
+        t = timed_steps(torch, c, steps)
+        rates[name] = steps / t
+        if model == 2:
+            prof = c.step_profile(3)
+            out[name + "_stage_ms"] = {("closure" if k == "smagorinsky" else k): round(v / 3, 4)
+                                       for k, v in prof.items() if v > 0}
+        c.close()
+    out["steps_per_s"] = rates
+    if dns_rate:
+        out["speedup_vs_dns_fp64"] = rates["learned"] * dt_les / (dns_rate * DT)
+    if dns32_rate:
+        out["speedup_vs_dns_fp32"] = rates["learned"] * dt_les / (dns32_rate * DT)
+    if args.les_only:
+        return out
+    ex = (LesExperiment(n_dns=512, n_les=128, re=RE, dt_dns=0.00025, nruns=1, spinup=2.0, collect=0.5, nsnap=4,
+                        window=1.0, nsample=5, stride=4, train_steps=2000) if args.les_full else
+          LesExperiment(n_dns=128, n_les=32, re=1000.0, dt_dns=0.002, nruns=2, spinup=2.0, collect=1.0, nsnap=4,
+                        window=1.5, nsample=6, stride=2, train_steps=1500))
+    try:
+        r = run_experiment(ex, device=device, log=lambda *a: None)
+        out["aposteriori"] = {"dns_to_les": f"{ex.n_dns}^3 -> {ex.n_les}^3", "re": ex.re,
+                              "mean_abs_log_spectrum_error": r["spectrum_error"],
+                              "apriori_stress_error": r["apriori_stress_error"],
+                              "speedup_vs_dns": r["speedup_vs_dns"]}
+    except Exception as e:  # reported, never fatal to the bench line
+        out["aposteriori"] = {"error": str(e)}
+    return out
+
+
 def run_reference(args):
     rank, world, _ = dist_info()
     if rank != 0:
@@ -213,6 +282,9 @@ def main():
     import torch
     rank, world, local = dist_info()
     torch.cuda.set_device(local)
+    if args.les_only:
+        print(json.dumps({"learned_les": les_leg(torch, args, None, None, local)}), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime
@@ -226,7 +298,11 @@ def main():
     ctx.init_velocity(RN1, 2, 4.0, 2.0)
     ctx.dealias_all()
     fields0 = ctx.download_fields()
-    variant, variant_ms = ctx.autotune()
+    if args.variant >= 0:
+        ctx.set_variant(args.variant)
+        variant, variant_ms = args.variant, []
+    else:
+        variant, variant_ms = ctx.autotune()
 
     # warm-up, then the timed region
     ctx.step(args.warmup)
@@ -284,14 +360,17 @@ def main():
         e2e = {"value": world * args.e2e_steps / te, "unit": "timesteps/s", "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps}
         del out
-    ctx.close()
 
     # FP32 nonlinear-term transforms, same initial state and step count
     fp32 = None
     if not args.no_fp32:
         c32 = make_context(n, 1, local)
         c32.upload_fields(fields0)
-        v32, v32_ms = c32.autotune()
+        if args.variant >= 0:
+            c32.set_variant(args.variant)
+            v32, v32_ms = args.variant, []
+        else:
+            v32, v32_ms = c32.autotune()
         c32.step(args.warmup)
         if dist:
             dist.barrier()
@@ -309,7 +388,31 @@ def main():
                 "skew_abs_err": abs(st32["skewness"] - st64["skewness"]),
                 "stage_ms": {k: round(v / 3, 3) for k, v in prof32.items() if v > 0},
                 "tuned_variant": v32, "variant_ms": [round(x, 3) for x in v32_ms]}
+        # error per statistic against the FP64 path every cmp_every steps from the same state
+        ctx.upload_fields(fields0)
+        c32.upload_fields(fields0)
+        ctx.fov = ctx.fos = c32.fov = c32.fos = 1
+        cmp = []
+        for k in range(args.cmp_points):
+            ctx.step(args.cmp_every)
+            c32.step(args.cmp_every)
+            e64, s64 = ctx.stats()
+            e32, s32 = c32.stats()
+            mk = e64 > 1e-12 * e64.max()
+            cmp.append({"step": (k + 1) * args.cmp_every,
+                        "ek_max_rel_err": float(np.max(np.abs(e32[mk] - e64[mk]) / e64[mk])),
+                        "energy_rel_err": abs(s32["energy"] - s64["energy"]) / s64["energy"],
+                        "eps_rel_err": abs(s32["eps_v"] - s64["eps_v"]) / s64["eps_v"],
+                        "skew_abs_err": abs(s32["skewness"] - s64["skewness"]),
+                        "courant": c32.courant})
+        fp32["vs_fp64_every_%d_steps" % args.cmp_every] = cmp
+        fp32["ek_max_rel_err_over_run"] = max(c["ek_max_rel_err"] for c in cmp)
         c32.close()
+    ctx.close()
+
+    les = None
+    if not args.no_les and world == 1:
+        les = les_leg(torch, args, value, fp32["value"] if fp32 else None, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -340,6 +443,7 @@ def main():
             "clocks": clk.summary(),
             "e2e": e2e,
             "fp32_fft": fp32,
+            "learned_les": les,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

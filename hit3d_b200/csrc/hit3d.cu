@@ -148,10 +148,12 @@ struct hit3d_ctx {
     void *mlp_wb;        // bf16 weights of the learned closure (les_model 2)
     double mlp_delta;    // filter width the closure was trained for
     int mlp_clip;        // zero the stress where its dissipation is negative
+    int mlp_kernel;      // 0: CUDA cores, 1: tensor cores for the hidden layers
+    int *d_mlp_err;      // set by the tensor-core kernel when a completion wait runs out
 };
 
 int h3d_mlp_apply(cudaStream_t st, int fp64, int64_t np, int64_t n, int64_t rp, int64_t fs, double delta, int clip,
-                  const void *wb, void *G);
+                  int kernel, const void *wb, void *G, int *err);
 
 static int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 
@@ -472,7 +474,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
             H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, 9));
             H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, 9));
             H3D_TRY(h3d_mlp_apply(c->st, sizeof(T) == 8, (int64_t)c->n * c->n * c->n, c->n, 2 * (int64_t)wp, 2 * wfs,
-                                  c->mlp_delta, c->mlp_clip, c->mlp_wb, Wf(t0)));
+                                  c->mlp_delta, c->mlp_clip, c->mlp_kernel, c->mlp_wb, Wf(t0), c->d_mlp_err));
             c->nlaunch++;
             H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, 6));
             H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, 6));
@@ -593,6 +595,7 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     c->kmax = c->p.dealias == 0 ? c->n / 3 : (int)floor((double)c->n / 3.0 * sqrt(2.0));
     c->dx = 2.0 * (4.0 * atan(1.0)) / (double)c->n;
     c->int_scalars = c->nsc > 0;
+    c->xcfg = 4;  // register-resident fused x pass, the tuner's usual pick
     cudaDeviceProp prop;
     H3D_CHECK(cudaGetDeviceProperties(&prop, c->dev));
     c->nsm = prop.multiProcessorCount;
@@ -658,7 +661,8 @@ extern "C" void hit3d_gpu_finalize(hit3d_ctx *c)
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->W64 && c->W64 != c->W) cudaFree(c->W64);
     void *ptrs[] = {c->U, c->RO, c->RP, c->SP, c->W, c->phys, c->tw64, c->tw32, c->d_fen, c->d_part,
-                    c->d_red, c->d_ratio, c->d_cmax, c->stage, c->d_xyz, c->d_uvw, c->sgs, c->mlp_wb};
+                    c->d_red, c->d_ratio, c->d_cmax, c->stage, c->d_xyz, c->d_uvw, c->sgs, c->mlp_wb,
+                    c->d_mlp_err};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
@@ -729,6 +733,12 @@ extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_
     }
     if (fov) *fov = ev;
     if (fos) *fos = es;
+    if (c->p.les_model == 2 && c->mlp_kernel == 1 && nsteps > 0) {
+        int herr = 0;
+        H3D_CHECK(cudaMemcpyAsync(&herr, c->d_mlp_err, sizeof herr, cudaMemcpyDeviceToHost, c->st));
+        H3D_CHECK(cudaStreamSynchronize(c->st));
+        if (herr) return h3d_set_error_msg(-5, "hit3d_gpu_step: a tensor-core completion wait of the closure ran out");
+    }
     if (courant && nsteps > 0) {
         unsigned long long bits = 0;
         H3D_CHECK(cudaMemcpyAsync(&bits, c->d_cmax, sizeof bits, cudaMemcpyDeviceToHost, c->st));
@@ -742,14 +752,19 @@ extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_
 }
 
 extern "C" int hit3d_mlp_nparam(void);
-extern "C" int hit3d_gpu_les_set_mlp(hit3d_ctx *c, const uint16_t *wb, int64_t nparam, double delta, int32_t clip)
+extern "C" int hit3d_gpu_les_set_mlp(hit3d_ctx *c, const uint16_t *wb, int64_t nparam, double delta, int32_t clip,
+                                     int32_t kernel)
 {
     if (!c || !wb) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: null argument");
+    if (kernel != 0 && kernel != 1) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: kernel must be 0 or 1");
     if (c->p.les_model != 2) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: the context needs les_model 2");
     if (nparam != hit3d_mlp_nparam()) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: wrong parameter count");
     if (!(delta > 0.0)) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: filter width must be positive");
     H3D_CHECK(cudaSetDevice(c->dev));
     if (!c->mlp_wb) H3D_TRY(ctx_alloc(&c->mlp_wb, sizeof(uint16_t) * (size_t)nparam));
+    if (!c->d_mlp_err) H3D_TRY(ctx_alloc((void **)&c->d_mlp_err, sizeof(int)));
+    H3D_CHECK(cudaMemsetAsync(c->d_mlp_err, 0, sizeof(int), c->st));
+    c->mlp_kernel = kernel;
     H3D_CHECK(cudaMemcpyAsync(c->mlp_wb, wb, sizeof(uint16_t) * (size_t)nparam, cudaMemcpyHostToDevice, c->st));
     H3D_CHECK(cudaStreamSynchronize(c->st));
     c->mlp_delta = delta;

@@ -9,7 +9,7 @@
 #include <vector>
 
 #include "../../include/hit3d_gpu.h"
-#include "mlp.cuh"
+#include "mlp_tc.cuh"
 
 #define M_TRY(x)                    \
     do {                            \
@@ -297,14 +297,40 @@ extern "C" int hit3d_mlp_train(hit3d_mlp *m, int32_t nsteps, int64_t batch, doub
     return 0;
 }
 
+static int sm_count()
+{
+    static int cache[64] = {0};
+    int dev = 0;
+    H3D_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return 148;
+    if (!cache[dev]) H3D_CHECK(cudaDeviceGetAttribute(&cache[dev], cudaDevAttrMultiProcessorCount, dev));
+    return cache[dev];
+}
+
 // one launch of the inference kernel on fields in device memory (used by the
-// LES step as well)
+// LES step as well): kernel 0 = fp32 activations on the CUDA cores, 1 = hidden
+// layers on the tensor cores (bf16 activations); err receives 1 if a
+// tensor-core completion wait ran out
 int h3d_mlp_apply(cudaStream_t st, int fp64, int64_t np, int64_t n, int64_t rp, int64_t fs, double delta, int clip,
-                  const void *wb, void *G)
+                  int kernel, const void *wb, void *G, int *err)
 {
     if ((np + MLP_NT - 1) / MLP_NT > INT32_MAX) return h3d_set_error_msg(-1, "h3d_mlp_apply: too many points");
-    const int nblk = (int)((np + MLP_NT - 1) / MLP_NT);
     const __nv_bfloat16 *w = static_cast<const __nv_bfloat16 *>(wb);
+    if (kernel == 1) {
+        if (!err) return h3d_set_error_msg(-1, "h3d_mlp_apply: the tensor-core kernel needs an error flag");
+        const int64_t ntile = (np + TC_TILE - 1) / TC_TILE;
+        const int nsm = sm_count();
+        if (nsm <= 0) return nsm;
+        const int nblk = (int)std::min<int64_t>(ntile, (int64_t)nsm * 4);
+        if (fp64)
+            k_mlp_apply_tc<double><<<nblk, TC_TILE, TC_SMEM, st>>>(np, n, rp, fs, (float)delta, clip, w, (double *)G, err);
+        else
+            k_mlp_apply_tc<float><<<nblk, TC_TILE, TC_SMEM, st>>>(np, n, rp, fs, (float)delta, clip, w, (float *)G, err);
+        H3D_CHECK(cudaGetLastError());
+        return 0;
+    }
+    if (kernel != 0) return h3d_set_error_msg(-1, "h3d_mlp_apply: kernel must be 0 or 1");
+    const int nblk = (int)((np + MLP_NT - 1) / MLP_NT);
     if (fp64) {
         M_TRY(mlp_smem((const void *)k_mlp_apply<double>));
         k_mlp_apply<double><<<nblk, MLP_NT, MLP_SMEM, st>>>(np, n, rp, fs, (float)delta, clip, w, (double *)G);
@@ -316,20 +342,30 @@ int h3d_mlp_apply(cudaStream_t st, int fp64, int64_t np, int64_t n, int64_t rp, 
     return 0;
 }
 
-extern "C" int hit3d_mlp_predict(hit3d_mlp *m, const float *A, int64_t np, double delta, int32_t clip, float *tau)
+extern "C" int hit3d_mlp_predict(hit3d_mlp *m, const float *A, int64_t np, double delta, int32_t clip, int32_t kernel,
+                                 float *tau)
 {
     if (!m || !A || !tau) return h3d_set_error_msg(-1, "hit3d_mlp_predict: null argument");
     if (np <= 0) return h3d_set_error_msg(-1, "hit3d_mlp_predict: empty input");
+    if (kernel != 0 && kernel != 1) return h3d_set_error_msg(-1, "hit3d_mlp_predict: kernel must be 0 or 1");
     H3D_CHECK(cudaSetDevice(m->dev));
     float *G = nullptr;
-    if (cudaMalloc(&G, sizeof(float) * 9 * np) != cudaSuccess) return h3d_set_error_msg(-4, "hit3d_mlp_predict: out of device memory");
-    int rc = 0;
-    if (cudaMemcpyAsync(G, A, sizeof(float) * 9 * np, cudaMemcpyHostToDevice, m->st) != cudaSuccess)
+    int *err = nullptr;
+    if (cudaMalloc(&G, sizeof(float) * 9 * np) != cudaSuccess || cudaMalloc(&err, sizeof(int)) != cudaSuccess) {
+        mfree(G);
+        return h3d_set_error_msg(-4, "hit3d_mlp_predict: out of device memory");
+    }
+    int rc = 0, herr = 0;
+    if (cudaMemsetAsync(err, 0, sizeof(int), m->st) != cudaSuccess ||
+        cudaMemcpyAsync(G, A, sizeof(float) * 9 * np, cudaMemcpyHostToDevice, m->st) != cudaSuccess)
         rc = h3d_set_error_msg(-2, "hit3d_mlp_predict: upload failed");
-    if (!rc) rc = h3d_mlp_apply(m->st, 0, np, np, np, np, delta, clip, m->wb, G);
-    if (!rc && cudaMemcpyAsync(tau, G, sizeof(float) * 6 * np, cudaMemcpyDeviceToHost, m->st) != cudaSuccess)
+    if (!rc) rc = h3d_mlp_apply(m->st, 0, np, np, np, np, delta, clip, kernel, m->wb, G, err);
+    if (!rc && (cudaMemcpyAsync(tau, G, sizeof(float) * 6 * np, cudaMemcpyDeviceToHost, m->st) != cudaSuccess ||
+                cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, m->st) != cudaSuccess))
         rc = h3d_set_error_msg(-2, "hit3d_mlp_predict: download failed");
     if (!rc && cudaStreamSynchronize(m->st) != cudaSuccess) rc = h3d_set_error_msg(-2, "hit3d_mlp_predict: kernel failed");
+    if (!rc && herr) rc = h3d_set_error_msg(-5, "hit3d_mlp_predict: a tensor-core completion wait ran out");
     cudaFree(G);
+    cudaFree(err);
     return rc;
 }

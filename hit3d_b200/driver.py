@@ -212,3 +212,23 @@ class Simulation:
         if reason >= 0:
             self.write_restart()
         return reason
+
+
+def main(argv=None):
+    """`python -m hit3d_b200.driver <run_name> [--workdir D] [--precision 0|1]`:
+    read <run_name>.in, run to ITMAX/TMAX/stop/runlimit, write the reference's files."""
+    import argparse
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("run_name")
+    ap.add_argument("--workdir", default=".")
+    ap.add_argument("--precision", type=int, default=0)
+    a = ap.parse_args(argv)
+    sim = Simulation(a.run_name, workdir=a.workdir, precision=a.precision)
+    sim.begin()
+    reason = sim.run()
+    print(f"exit reason {reason} at ITIME={sim.itime}, TIME={sim.time:.6f}")
+    return 0 if reason is not None and reason >= 0 else 1
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -128,8 +128,8 @@ SIGNATURES = [
     ("hit3d_mlp_norms", C.c_int, [_vp, _dp]),
     ("hit3d_mlp_loss_grad", C.c_int, [_vp, C.POINTER(_i32), _i64, _d, _fp, _fp]),
     ("hit3d_mlp_train", C.c_int, [_vp, _i32, _i64, _d, _d, C.c_uint64, _fp]),
-    ("hit3d_mlp_predict", C.c_int, [_vp, _fp, _i64, _d, _i32, _fp]),
-    ("hit3d_gpu_les_set_mlp", C.c_int, [_vp, C.POINTER(C.c_uint16), _i64, _d, _i32]),
+    ("hit3d_mlp_predict", C.c_int, [_vp, _fp, _i64, _d, _i32, _i32, _fp]),
+    ("hit3d_gpu_les_set_mlp", C.c_int, [_vp, C.POINTER(C.c_uint16), _i64, _d, _i32, _i32]),
 ]
 
 
@@ -349,12 +349,13 @@ class Context:
         _check(lib().hit3d_gpu_physical_velocity(self._h, _ptr(out), self.n + 2), "physical_velocity")
         return out
 
-    def les_set_mlp(self, bf16_weights: np.ndarray, delta: float, clip: bool = True):
+    def les_set_mlp(self, bf16_weights: np.ndarray, delta: float, clip: bool = True, kernel: int = 1):
         """Use trained bf16 weights (uint16 bit patterns) as this context's subgrid model
-        (les_model 2); delta is the filter width the network was trained for."""
+        (les_model 2); delta is the filter width the network was trained for; kernel 1
+        runs the hidden layers on the tensor cores, 0 on the CUDA cores in fp32."""
         w = np.ascontiguousarray(bf16_weights, dtype=np.uint16)
         _check(lib().hit3d_gpu_les_set_mlp(self._h, w.ctypes.data_as(C.POINTER(C.c_uint16)), w.size, float(delta),
-                                           int(bool(clip))), "les_set_mlp")
+                                           int(bool(clip)), int(kernel)), "les_set_mlp")
 
 
 def _f32(a: np.ndarray) -> np.ndarray:
@@ -431,12 +432,12 @@ class Mlp:
                                      int(seed) & (2**64 - 1), losses.ctypes.data_as(_fp)), "hit3d_mlp_train")
         return losses[:nsteps]
 
-    def predict(self, A: np.ndarray, delta: float | None = None, clip: bool = False) -> np.ndarray:
+    def predict(self, A: np.ndarray, delta: float | None = None, clip: bool = False, kernel: int = 0) -> np.ndarray:
         A = _f32(A).reshape(9, -1)
         d = self.delta if delta is None else delta
         if d is None:
             raise ValueError("no filter width")
         out = np.empty((6, A.shape[1]), dtype=np.float32)
         _check(lib().hit3d_mlp_predict(self._h, A.ctypes.data_as(_fp), A.shape[1], float(d), int(bool(clip)),
-                                       out.ctypes.data_as(_fp)), "hit3d_mlp_predict")
+                                       int(kernel), out.ctypes.data_as(_fp)), "hit3d_mlp_predict")
         return out

@@ -122,6 +122,7 @@ class LesExperiment:
     lr: float = 1e-3
     lam: float = 1.0            # weight of the dissipation term of the loss
     clip: bool = True
+    kernel: int = 1             # inference on the tensor cores (1) or the CUDA cores (0)
     cs: float = 0.18
     seed: int = 5
     graph_steps: int = 20
@@ -199,7 +200,7 @@ def run_experiment(ex: LesExperiment, device: int = 0, log=print) -> Dict:
     for name, model in models.items():
         c = Context(ex.les_params(model))
         if model == 2:
-            c.les_set_mlp(w16, ex.delta, clip=ex.clip)
+            c.les_set_mlp(w16, ex.delta, clip=ex.clip, kernel=ex.kernel)
         filtered_state(f0, c, ex.delta)
         les[name] = c
 
@@ -208,14 +209,19 @@ def run_experiment(ex: LesExperiment, device: int = 0, log=print) -> Dict:
     errs: Dict[str, List[float]] = {k: [] for k in models}
     spectra: Dict[str, List[List[float]]] = {k: [] for k in list(models) + ["filtered_dns"]}
     kc = ref.kmax
+    wall = {k: 0.0 for k in list(models) + ["dns"]}
     for s in range(ex.nsample):
+        t0 = time.perf_counter()
         dns.step(dns_per)
+        wall["dns"] += time.perf_counter() - t0
         filtered_state(dns.download_fields(), ref, ex.delta)
         e_ref, _ = ref.stats()
         spectra["filtered_dns"].append(e_ref.tolist())
         for name, c in les.items():
             try:
+                t0 = time.perf_counter()
                 c.step(les_per)
+                wall[name] += time.perf_counter() - t0
                 e, _ = c.stats()
                 ok = bool(np.all(np.isfinite(e)))
             except Exception as exc:  # a blown-up LES is reported, not raised
@@ -226,7 +232,7 @@ def run_experiment(ex: LesExperiment, device: int = 0, log=print) -> Dict:
 
     # a-priori errors on held-out data: the DNS at the end of the window
     Ah, th = sgs_samples(dns, ex.delta, ex.stride)
-    pred = m.predict(Ah, ex.delta, clip=ex.clip)
+    pred = m.predict(Ah, ex.delta, clip=ex.clip, kernel=ex.kernel)
     dx_les = 2.0 * np.pi / ex.n_les
     apriori = {
         "learned": stress_error(pred, th),
@@ -249,11 +255,18 @@ def run_experiment(ex: LesExperiment, device: int = 0, log=print) -> Dict:
         "train_loss_first": float(np.mean(losses[:20])),
         "train_loss_last": float(np.mean(losses[-50:])),
         "train_seconds": t_train,
+        "ms_per_step": {k: 1000.0 * v / ((dns_per if k == "dns" else les_per) * ex.nsample) for k, v in wall.items()},
         "spectra": spectra,
     }
+    # simulated time per wall-clock second, LES over DNS
+    res["speedup_vs_dns"] = {k: (ex.dt_les / res["ms_per_step"][k]) / (ex.dt_dns / res["ms_per_step"]["dns"])
+                             for k in models}
     log("a-posteriori mean |ln E/E_fdns| over k=1..%d: " % kc +
         ", ".join(f"{k} {v:.4f}" for k, v in res["spectrum_error"].items()))
     log("a-priori stress error: " + ", ".join(f"{k} {v:.4f}" for k, v in apriori.items()))
+    log("ms per step: " + ", ".join(f"{k} {v:.3f}" for k, v in res["ms_per_step"].items()) +
+        "; speedup vs DNS (simulated time per second): " +
+        ", ".join(f"{k} {v:.1f}" for k, v in res["speedup_vs_dns"].items()))
     return res
 
 

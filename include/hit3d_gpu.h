@@ -262,11 +262,17 @@ int hit3d_mlp_loss_grad(hit3d_mlp *m, const int32_t *idx, int64_t np, double lam
  * drawn from the data set by a hash of (seed, step); losses[nsteps] may be null. */
 int hit3d_mlp_train(hit3d_mlp *m, int32_t nsteps, int64_t batch, double lr, double lam, uint64_t seed, float *losses);
 /* Stresses predicted at np points; with clip, points whose predicted
- * dissipation -tau:S is negative get tau = 0. */
-int hit3d_mlp_predict(hit3d_mlp *m, const float *A, int64_t np, double delta, int32_t clip, float *tau);
+ * dissipation -tau:S is negative get tau = 0.  kernel 0 keeps every
+ * activation in fp32 on the CUDA cores (the training kernels' arithmetic);
+ * kernel 1 runs the two hidden 64x64 layers on the tensor cores (tcgen05,
+ * TMEM accumulators) with their inputs rounded to bf16. */
+int hit3d_mlp_predict(hit3d_mlp *m, const float *A, int64_t np, double delta, int32_t clip, int32_t kernel,
+                      float *tau);
 /* Use a trained network as the context's subgrid model (les_model 2): nparam
- * bf16 weights, the filter width they were trained for, the clip switch. */
-int hit3d_gpu_les_set_mlp(hit3d_ctx *ctx, const uint16_t *bf16_weights, int64_t nparam, double delta, int32_t clip);
+ * bf16 weights, the filter width they were trained for, the clip switch and
+ * the inference kernel (as in hit3d_mlp_predict). */
+int hit3d_gpu_les_set_mlp(hit3d_ctx *ctx, const uint16_t *bf16_weights, int64_t nparam, double delta, int32_t clip,
+                          int32_t kernel);
 
 #ifdef __cplusplus
 }

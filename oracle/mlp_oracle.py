@@ -84,21 +84,31 @@ def features(A, delta):
     return x, T, sbar, pref
 
 
-def forward(w, x):
+def _bf16_act(a):
+    return bf16_round(a.astype(np.float32)).astype(np.float64)
+
+
+def forward(w, x, act_bf16=False):
+    """act_bf16: the inputs of the two hidden 64x64 layers rounded to bf16, as the
+    tensor-core inference kernel feeds them to the MMA."""
     p = unpack(w)
     z1 = p["W1"] @ x + p["b1"][:, None]
     a1 = gelu(z1)
+    if act_bf16:
+        a1 = _bf16_act(a1)
     z2 = p["W2"] @ a1 + p["b2"][:, None]
     a2 = gelu(z2)
+    if act_bf16:
+        a2 = _bf16_act(a2)
     z3 = p["W3"] @ a2 + p["b3"][:, None]
     a3 = gelu(z3)
     g = p["W4"] @ a3 + p["b4"][:, None]
     return g, (x, z1, a1, z2, a2, z3, a3)
 
 
-def predict(w, A, delta, clip=False):
+def predict(w, A, delta, clip=False, act_bf16=False):
     x, T, sbar, pref = features(A, delta)
-    g, _ = forward(w, x)
+    g, _ = forward(w, x, act_bf16)
     tau = pref * np.einsum("np,ncp->cp", g, T)
     if clip:
         diss = -np.einsum("c,cp,cp->p", FROB, tau, sbar)

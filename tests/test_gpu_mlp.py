@@ -56,6 +56,31 @@ def test_predict_matches_oracle(clip):
     m.close()
 
 
+def test_tensor_core_predict_matches_oracle():
+    """Hidden layers on the tensor cores (bf16 activations, fp32 accumulation in
+    TMEM): against the oracle with the same bf16 rounding of the activations, on a
+    ragged point count that spans several tiles per CTA."""
+    np_ = 300001
+    A, _ = mo.synthetic_data(np_, seed=13)
+    w = mo.bf16_round(mo.init_params(21)).astype(np.float64)
+    m = _mlp(w)
+    got = m.predict(A, DELTA, clip=False, kernel=1)
+    ref = mo.predict(w, A, DELTA, act_bf16=True)
+    scale = np.abs(ref).max()
+    err = np.abs(got - ref).max(axis=0) / scale
+    # a bf16 rounding decided differently by the last fp32 bit of an activation
+    # moves a point by about one bf16 step; everything else agrees to fp32 accuracy
+    assert np.quantile(err, 0.999) < 2e-5 and err.max() < 5e-3, (np.quantile(err, 0.999), err.max())
+    # and the fp32-activation kernel agrees to bf16 accuracy
+    exact = m.predict(A, DELTA, clip=False, kernel=0)
+    assert np.abs(exact - got).max() < 2e-2 * scale
+    got_clip = m.predict(A, DELTA, clip=True, kernel=1)
+    ref_clip = mo.predict(w, A, DELTA, clip=True, act_bf16=True)
+    agree = np.all(np.abs(got_clip - ref_clip) <= 5e-3 * scale, axis=0)
+    assert agree.mean() > 0.999
+    m.close()
+
+
 def test_training_reduces_loss_and_is_deterministic():
     A, tau = mo.synthetic_data(50000, seed=9)
     runs = []
@@ -71,7 +96,8 @@ def test_training_reduces_loss_and_is_deterministic():
     assert np.array_equal(runs[0][0], runs[1][0]) and np.array_equal(runs[0][1], runs[1][1])
 
 
-def test_les_step_with_smagorinsky_weights_matches_smagorinsky():
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_les_step_with_smagorinsky_weights_matches_smagorinsky(kernel):
     """With g = (g1, 0, 0, 0, 0) the network is the Smagorinsky model; the LES step
     through the network must match les_model 1 with the same coefficient."""
     from _cases import RN1, relerr
@@ -85,7 +111,7 @@ def test_les_step_with_smagorinsky_weights_matches_smagorinsky():
     b = Context(Params(les_model=2, **common))
     w = mo.smagorinsky_params(0.0, dx, DELTA)
     w[-5] = g1
-    b.les_set_mlp(mo.bf16_bits(w), DELTA, clip=True)
+    b.les_set_mlp(mo.bf16_bits(w), DELTA, clip=True, kernel=kernel)
     for c in (a, b):
         c.init_velocity(RN1, 2, 4.0, 2.0)
         c.dealias_all()
