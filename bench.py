@@ -141,24 +141,45 @@ def make_context(n, precision, device):
     return Context(p)
 
 
-# algorithmic bytes per step of each stage, in units of one unpadded complex
-# half-spectrum field B1 = N^2 (N/2+1) * 16 bytes (FP64) -- velocity only, 2/3 rule
-STAGE_UNITS = {
-    0: {"z_inverse": 6, "y_inverse": 6, "x_fused": 9, "y_forward": 12, "z_forward": 12, "update": 18},
-    1: {"z_inverse": 4.5, "y_inverse": 3, "x_fused": 4.5, "y_forward": 6, "z_forward": 6, "update": 15},
-}
+def stage_units(n, precision, pruned):
+    """Algorithmic bytes per step of each stage, in units of one unpadded complex
+    half-spectrum field B1 = N^2 (N/2+1) * 16 bytes, velocity only, 2/3 rule.
+
+    With 2/3-rule pruning a = (kc+1)/(N/2+1) of the kx columns and b = (2 kc+1)/N of
+    the ky (or kz) indices are kept (kc = N/3): inverse passes read only kept
+    indices along their axis and forward passes store only kept indices.  The
+    update reads the products only at kept modes (a b^2) in either case.  Work
+    fields are half size in the FP32 form; the state stays FP64."""
+    kc = n // 3
+    a0, b0 = (kc + 1) / (n // 2 + 1), (2 * kc + 1) / n
+    a, b = (a0, b0) if pruned else (1.0, 1.0)
+    w = 0.5 if precision else 1.0
+    return {
+        "z_inverse": 3 * a * b * b + w * 3 * a * b,
+        "y_inverse": w * (3 * a * b + 3 * a),
+        "x_fused": w * (3 * a + 6 * a),
+        "y_forward": w * (6 * a + 6 * a * b),
+        "z_forward": w * (6 * a * b + 6 * a * b * b),
+        "update": 12 + w * 6 * a0 * b0 * b0,
+    }
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of the dominant stage from the committed ncu summary."""
+    out = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.txt")) as f:
+            for line in f:
+                line = line.split("#")[0].split()
+                if len(line) == 2:
+                    out[line[0]] = float(line[1])
+    except OSError:
+        pass
+    return out
 # single launches per step of each stage (velocity only, 2/3 rule)
 STAGE_LAUNCHES = {"z_inverse": 1, "y_inverse": 1, "x_fused": 1, "y_forward": 1, "z_forward": 1, "update": 1}
 
 
-def load_traffic():
-    """Per-launch DRAM bytes of each stage from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    try:
-        with open(path) as f:
-            return json.load(f)
-    except Exception:
-        return {}
 
 
 def timed_steps(torch, ctx, steps):
@@ -322,9 +343,10 @@ def main():
     es64, st64 = ctx.stats()
 
     # per-stage device time (separate, untimed steps) -> roofline of the dominant stage
+    pruned = ctx.pruned
     prof = ctx.step_profile(3)
     prof = {k: v / 3 for k, v in prof.items()}
-    units = STAGE_UNITS[0]
+    units = stage_units(n, 0, pruned)
     top = max(units, key=lambda k: prof.get(k, 0.0))
     ach = units[top] * B1 / (prof[top] / 1000.0) / 1e9
     traffic = load_traffic().get(f"{n}:{top}")
@@ -434,9 +456,12 @@ def main():
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": top, "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "peak_kind": peak_kind, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": units[top] * B1},
+                         "algorithmic_bytes_per_launch": units[top] * B1, "pruned_transforms": pruned},
             "step_roofline": {"ideal_bytes_per_step": ideal, "achieved_GBs": ideal / (ms / 1000.0) / 1e9,
-                              "frac_of_peak": ideal / (ms / 1000.0) / 1e9 / peak},
+                              "frac_of_peak": ideal / (ms / 1000.0) / 1e9 / peak,
+                              "stage_model_bytes_per_step": sum(units.values()) * B1,
+                              "stage_model_GBs": sum(units.values()) * B1 / (ms / 1000.0) / 1e9,
+                              "stage_model_frac_of_peak": sum(units.values()) * B1 / (ms / 1000.0) / 1e9 / peak},
             "stage_ms": {k: round(v, 3) for k, v in prof.items() if v > 0},
             "stage_GBs": stage_gbs,
             "tuned_variant": variant, "variant_ms": [round(x, 3) for x in variant_ms],

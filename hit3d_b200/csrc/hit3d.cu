@@ -150,6 +150,10 @@ struct hit3d_ctx {
     int mlp_clip;        // zero the stress where its dissipation is negative
     int mlp_kernel;      // 0: CUDA cores, 1: tensor cores for the hidden layers
     int *d_mlp_err;      // set by the tensor-core kernel when a completion wait runs out
+    int prune_on;        // allow 2/3-rule pruning of the step's transforms
+    int pruned;          // the state is zero beyond N/3 (checked), so pruning is exact
+    int alias_known;     // `pruned` is up to date with the state
+    int kc_active;       // >= 0 while a pruned step is being issued: the cutoff N/3
 };
 
 int h3d_mlp_apply(cudaStream_t st, int fp64, int64_t np, int64_t n, int64_t rp, int64_t fs, double delta, int clip,
@@ -176,9 +180,15 @@ static int zinv_LM(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_t
     io.n = c->n; io.psrc = c->P64; io.pdst = dpitch; io.ncol = c->nh; io.sfield = sfield;
     io.dx = c->dx;
     io.k2max = c->k2max;
+    int rows = c->n;
+    if (c->kc_active >= 0) {
+        io.kl = io.ko = c->kc_active;
+        io.ncol = c->kc_active + 1;
+        rows = 2 * c->kc_active + 1;
+    }
     auto k = k_colfft<T, L, CF::TC, CF::NT, false, IO>;
     H3D_TRY(set_smem(k, CF::SMEM));
-    dim3 g((c->nh + CF::TC - 1) / CF::TC, c->n, nf);
+    dim3 g((io.ncol + CF::TC - 1) / CF::TC, rows, nf);
     k<<<g, CF::NT, CF::SMEM, c->st>>>(io, twid<T>(c));
     H3D_LAUNCH_CHECK();
     return 0;
@@ -224,7 +234,20 @@ static int spass_L(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, in
     io.src = base; io.dst = base; io.fs_src = fs; io.fs_dst = fs; io.ncol = c->nh;
     if (axis == 1) { io.sa_src = io.sa_dst = pitch; io.so_src = io.so_dst = (int64_t)c->n * pitch; }
     else { io.sa_src = io.sa_dst = (int64_t)c->n * pitch; io.so_src = io.so_dst = pitch; }
-    dim3 g((c->nh + CF::TC - 1) / CF::TC, c->n, nf);
+    int rows = c->n;
+    if (c->kc_active >= 0) {
+        // kx <= kc only; inverse passes read |k| <= kc along the axis, forward
+        // passes store |k| <= kc; the z pass visits only the kept ky rows
+        io.n = c->n;
+        io.ncol = c->kc_active + 1;
+        if (fwd) io.ks = c->kc_active;
+        else io.kl = c->kc_active;
+        if (axis == 2) {
+            io.ko = c->kc_active;
+            rows = 2 * c->kc_active + 1;
+        }
+    }
+    dim3 g((io.ncol + CF::TC - 1) / CF::TC, rows, nf);
     if (fwd) {
         auto k = k_colfft<T, L, CF::TC, CF::NT, true, IOPlain<T, T, T>>;
         H3D_TRY(set_smem(k, CF::SMEM));
@@ -251,8 +274,8 @@ template <typename T, int L> static int xc2r_L(hit3d_ctx *c, cx<T> *base, int64_
     auto k = k_xc2r<T, L, RC::TC, RC::NT, T>;
     H3D_TRY(set_smem(k, RC::SMEM));
     const double n3 = (double)c->n * c->n * c->n;
-    k<<<dim3((npairs + RC::TC - 1) / RC::TC, 1, nf), RC::NT, RC::SMEM, c->st>>>(base, fs, pitch, npairs,
-                                                                                 (T)(1.0 / n3), twid<T>(c));
+    k<<<dim3((npairs + RC::TC - 1) / RC::TC, 1, nf), RC::NT, RC::SMEM, c->st>>>(
+        base, fs, pitch, npairs, (T)(1.0 / n3), twid<T>(c), c->kc_active >= 0 ? c->kc_active + 1 : 0);
     H3D_LAUNCH_CHECK();
     return 0;
 }
@@ -269,7 +292,8 @@ template <typename T, int L> static int xr2c_L(hit3d_ctx *c, cx<T> *base, int64_
     const int npairs = c->n * c->n / 2;
     auto k = k_xr2c<T, L, RC::TC, RC::NT, T>;
     H3D_TRY(set_smem(k, RC::SMEM));
-    k<<<dim3((npairs + RC::TC - 1) / RC::TC, 1, nf), RC::NT, RC::SMEM, c->st>>>(base, fs, pitch, npairs, twid<T>(c));
+    k<<<dim3((npairs + RC::TC - 1) / RC::TC, 1, nf), RC::NT, RC::SMEM, c->st>>>(
+        base, fs, pitch, npairs, twid<T>(c), c->kc_active >= 0 ? c->kc_active + 1 : 0);
     H3D_LAUNCH_CHECK();
     return 0;
 }
@@ -319,6 +343,7 @@ template <typename T, template <class> class OP> static int xfused(hit3d_ctx *c,
     a.npairs = c->n * c->n / 2;
     const double n3 = (double)c->n * c->n * c->n;
     a.norm = 1.0 / n3;
+    a.kx_lim = c->kc_active >= 0 ? c->kc_active + 1 : 0;
 #define CALL(L) xfused_L<T, OP, L>(c, a)
     H3D_DISPATCH(c->n, CALL)
 #undef CALL
@@ -376,8 +401,39 @@ struct Prof {
 // ---------------------------------------------------------------------------
 // one time step
 // ---------------------------------------------------------------------------
+// 2/3-rule pruning for the duration of one step (reset on every exit path)
+struct PruneScope {
+    hit3d_ctx *c;
+    explicit PruneScope(hit3d_ctx *cc) : c(cc)
+    {
+        c->kc_active = (c->prune_on && c->pruned && c->p.dealias == 0) ? c->n / 3 : -1;
+    }
+    ~PruneScope() { c->kc_active = -1; }
+};
+
+// bring `pruned` up to date with the state (one pass over U and RO, only after
+// the state changed); never called while a graph is being recorded
+static int ensure_alias_state(hit3d_ctx *c)
+{
+    if (c->alias_known) return 0;
+    c->pruned = 0;
+    if (c->p.dealias == 0 && c->prune_on) {
+        unsigned long long *d = reinterpret_cast<unsigned long long *>(c->d_red);
+        H3D_CHECK(cudaMemsetAsync(d, 0, sizeof(unsigned long long), c->st));
+        k_alias_max<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->fs64, 3 + c->nsc, c->U, c->RO, d);
+        H3D_LAUNCH_CHECK();
+        unsigned long long bits = 1;
+        H3D_CHECK(cudaMemcpyAsync(&bits, d, sizeof bits, cudaMemcpyDeviceToHost, c->st));
+        H3D_CHECK(cudaStreamSynchronize(c->st));
+        c->pruned = bits == 0;
+    }
+    c->alias_known = 1;
+    return 0;
+}
+
 template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_s, Prof *prof = nullptr)
 {
+    PruneScope prune_scope(c);
     const hit3d_params &p = c->p;
     cx<T> *W = reinterpret_cast<cx<T> *>(c->W);
     const int64_t wfs = c->wfs;
@@ -596,6 +652,8 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     c->dx = 2.0 * (4.0 * atan(1.0)) / (double)c->n;
     c->int_scalars = c->nsc > 0;
     c->xcfg = 4;  // register-resident fused x pass, the tuner's usual pick
+    c->prune_on = 1;
+    c->kc_active = -1;
     cudaDeviceProp prop;
     H3D_CHECK(cudaGetDeviceProperties(&prop, c->dev));
     c->nsm = prop.multiProcessorCount;
@@ -678,6 +736,7 @@ static int transfer_fields(hit3d_ctx *c, double2 *dev, const double *hsrc, doubl
     const size_t width = (size_t)c->nh * sizeof(double2);
     const size_t hp = (size_t)ld1 * sizeof(double);
     const size_t rows = (size_t)c->n * c->n;
+    if (hsrc) c->alias_known = 0;
     for (int f = 0; f < nf; f++) {
         double2 *d = dev + f * c->fs64;
         if (hsrc) {
@@ -724,6 +783,7 @@ extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_
     if (c->p.les_model == 2 && !c->mlp_wb)
         return h3d_set_error_msg(-1, "hit3d_gpu_step: les_model 2 needs weights (hit3d_gpu_les_set_mlp)");
     H3D_CHECK(cudaSetDevice(c->dev));
+    H3D_TRY(ensure_alias_state(c));
     int ev = fov ? (*fov != 0) : 0, es = fos ? (*fos != 0) : 0;
     for (int it = 0; it < nsteps; it++) {
         int rc = c->p.precision == 0 ? step_once<double>(c, ev, es) : step_once<float>(c, ev, es);
@@ -779,6 +839,7 @@ extern "C" int hit3d_gpu_step_profile(hit3d_ctx *c, int32_t nsteps, int32_t *fov
 {
     if (!c || !ms) return h3d_set_error_msg(-1, "hit3d_gpu_step_profile: null argument");
     H3D_CHECK(cudaSetDevice(c->dev));
+    H3D_TRY(ensure_alias_state(c));
     Prof prof;
     for (int i = 0; i < Prof::MAXM; i++) H3D_CHECK(cudaEventCreate(&prof.ev[i]));
     int ev = fov ? (*fov != 0) : 0, es = fos ? (*fos != 0) : 0;
@@ -807,6 +868,7 @@ extern "C" int hit3d_gpu_step_profile(hit3d_ctx *c, int32_t nsteps, int32_t *fov
 // time one fused x pass (velocity products) in the current variant; W is scratch
 template <typename T> static int time_fused(hit3d_ctx *c, float *ms)
 {
+    PruneScope prune_scope(c);  // time the launch shape the step will use
     cx<T> *W = reinterpret_cast<cx<T> *>(c->W);
     FusedArgs fa;
     memset(&fa, 0, sizeof fa);
@@ -831,6 +893,7 @@ extern "C" int hit3d_gpu_autotune(hit3d_ctx *c, int32_t *variant, double *ms_out
 {
     if (!c) return h3d_set_error_msg(-1, "null context");
     H3D_CHECK(cudaSetDevice(c->dev));
+    H3D_TRY(ensure_alias_state(c));
     int best = 0;
     float bt = 1e30f;
     for (int v = 0; v < kFusedVariants; v++) {
@@ -844,6 +907,22 @@ extern "C" int hit3d_gpu_autotune(hit3d_ctx *c, int32_t *variant, double *ms_out
     c->xcfg = best;
     if (variant) *variant = best;
     return 0;
+}
+
+extern "C" int hit3d_gpu_set_pruning(hit3d_ctx *c, int32_t on)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    c->prune_on = on != 0;
+    c->alias_known = 0;
+    return 0;
+}
+
+extern "C" int hit3d_gpu_pruned(hit3d_ctx *c)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    H3D_TRY(ensure_alias_state(c));
+    return c->pruned ? 1 : 0;
 }
 
 extern "C" int hit3d_gpu_set_variant(hit3d_ctx *c, int32_t v)
@@ -876,6 +955,7 @@ extern "C" int hit3d_gpu_dealias_all(hit3d_ctx *c)
     k_dealias_all<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->fs64, 3 + c->nsc, c->kmax, c->U);
     H3D_LAUNCH_CHECK();
     H3D_CHECK(cudaStreamSynchronize(c->st));
+    c->alias_known = 0;
     return 0;
 }
 
@@ -1026,6 +1106,7 @@ extern "C" int hit3d_gpu_init_velocity(hit3d_ctx *c, double rn1, int32_t isp, do
         }
     H3D_TRY(upload_phys(c, g.data(), (int64_t)ld, 3));
     H3D_TRY(fwd3d64(c, c->W64, 3));
+    c->alias_known = 0;
     k_init_curl<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, c->fs64, kmax, c->W64, c->U);
     H3D_LAUNCH_CHECK();
     std::vector<double> es(kmax), et, ratio(kmax);
@@ -1033,6 +1114,7 @@ extern "C" int hit3d_gpu_init_velocity(hit3d_ctx *c, double rn1, int32_t isp, do
     target_spectrum(isp, peak, ir_exp, kmax, et);
     for (int k = 0; k < kmax; k++) ratio[k] = es[k] > 0.0 ? sqrt(et[k] / es[k]) : -1.0;
     H3D_CHECK(cudaMemcpyAsync(c->d_ratio, ratio.data(), sizeof(double) * kmax, cudaMemcpyHostToDevice, c->st));
+    c->alias_known = 0;
     k_shell_scale<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, c->fs64, 3, kmax, c->d_ratio, c->U);
     H3D_LAUNCH_CHECK();
     H3D_CHECK(cudaStreamSynchronize(c->st));
@@ -1149,6 +1231,7 @@ extern "C" int hit3d_gpu_filter_field(hit3d_ctx *c, int32_t kind, double delta, 
     if (field < 0 || field >= 3 + c->nsc) return h3d_set_error_msg(-1, "hit3d_gpu_filter_field: no such field");
     H3D_CHECK(cudaSetDevice(c->dev));
     H3D_TRY(filter_transfer(c, kind, delta));
+    c->alias_known = 0;
     k_filter_apply<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->W64, c->U + field * c->fs64);
     H3D_LAUNCH_CHECK();
     H3D_CHECK(cudaStreamSynchronize(c->st));
@@ -1313,6 +1396,7 @@ extern "C" int hit3d_gpu_velocity_rescale(hit3d_ctx *c, int32_t isp, double peak
         ratio[k - 1] = e > 0.0 ? sqrt(et[k - 1] / e) : -1.0;
     }
     H3D_CHECK(cudaMemcpyAsync(c->d_ratio, ratio.data(), sizeof(double) * kmax, cudaMemcpyHostToDevice, c->st));
+    c->alias_known = 0;
     k_shell_scale<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, c->fs64, 3, kmax, c->d_ratio, c->U);
     H3D_LAUNCH_CHECK();
     H3D_CHECK(cudaStreamSynchronize(c->st));
@@ -1352,8 +1436,8 @@ struct hit3d_batch {
     cudaGraphExec_t exec = nullptr;
     int graph_steps = 0;
     int64_t launches = 0;
-    std::vector<double> cap_dt;  // dt and scalar switch of every run when the graph was recorded
-    std::vector<int> cap_scal;
+    std::vector<double> cap_dt;  // dt, scalar switch and pruning of every run when the graph was recorded
+    std::vector<int> cap_scal, cap_prune;
 };
 
 static int run_step(hit3d_ctx *c, int ev, int es)
@@ -1437,9 +1521,11 @@ static int batch_capture(hit3d_batch *b, int steps)
     b->graph_steps = steps;
     b->cap_dt.clear();
     b->cap_scal.clear();
+    b->cap_prune.clear();
     for (hit3d_ctx *cr : b->runs) {
         b->cap_dt.push_back(cr->p.dt);
         b->cap_scal.push_back(cr->int_scalars);
+        b->cap_prune.push_back(cr->prune_on && cr->pruned);
     }
     (void)c;
     return 0;
@@ -1451,6 +1537,7 @@ extern "C" int hit3d_batch_step(hit3d_batch *b, int32_t nsteps, int32_t graph_st
     if (graph_steps < 1) graph_steps = 1;
     hit3d_ctx *c = b->runs[0];
     H3D_CHECK(cudaSetDevice(b->dev));
+    for (hit3d_ctx *cr : b->runs) H3D_TRY(ensure_alias_state(cr));
     int left = nsteps;
     // first-order step of runs that need one, outside the graph
     bool any_first = false;
@@ -1466,7 +1553,8 @@ extern "C" int hit3d_batch_step(hit3d_batch *b, int32_t nsteps, int32_t graph_st
     if (left >= graph_steps) {
         bool stale = !b->exec || b->graph_steps != graph_steps || b->cap_dt.size() != b->runs.size();
         for (size_t r = 0; !stale && r < b->runs.size(); r++)
-            stale = b->cap_dt[r] != b->runs[r]->p.dt || b->cap_scal[r] != b->runs[r]->int_scalars;
+            stale = b->cap_dt[r] != b->runs[r]->p.dt || b->cap_scal[r] != b->runs[r]->int_scalars ||
+                    b->cap_prune[r] != (b->runs[r]->prune_on && b->runs[r]->pruned);
         if (stale) {
             for (hit3d_ctx *cr : b->runs) H3D_CHECK(cudaStreamSynchronize(cr->st));
             H3D_TRY(batch_capture(b, graph_steps));

@@ -95,7 +95,7 @@ template <int L> int run(const DevState &s, const double *in, double *out, cudaS
         constexpr int TC = L >= 1024 ? 1 : 1024 / L, NT = 128;
         const int npairs = n * n / 2;
         k_xr2c<double, L, TC, NT, double><<<(npairs + TC - 1) / TC, NT, Lay<L, TC, true>::elems * sizeof(double2), st>>>(
-            w, 0, nh, npairs, tw);
+            w, 0, nh, npairs, tw, 0);
     }
     constexpr int TC = 8;
     constexpr int RMAX = L == 48 ? 4 : 8;  // largest radix of the plan

@@ -11,8 +11,24 @@
 #include "fft.cuh"
 
 // ---------------------------------------------------------------------------
+// 2/3-rule pruning.  When every mode with some |k_i| > kc = N/3 is zero in the
+// state (the reference dealiases at start, dealias_all.f90, and the update
+// keeps those modes at zero), the passes of a time step skip what cannot
+// change the result: inverse passes read only |k| <= kc and leave whole
+// columns or rows of zeros untouched, forward passes store only |k| <= kc, the
+// modes the update reads (rhs_velocity.f90:85-142 masks the rest).  Index idx
+// of an axis of n points holds the signed wavenumber idx (idx <= n/2) or
+// idx - n; n/2 counts as +n/2.
+// ---------------------------------------------------------------------------
+H3D_HD bool kept(int idx, int n, int kc) { return (idx <= n / 2 ? idx : n - idx) <= kc; }
+// outer index y in [0, 2 kc] -> the kept axis index (0..kc, n-kc..n-1)
+H3D_HD int kept_index(int y, int n, int kc) { return y <= kc ? y : n - (2 * kc + 1 - y); }
+
+// ---------------------------------------------------------------------------
 // strided (y or z) pass:  CTA = TC adjacent kx columns x one outer index,
-// transform along an axis of stride `sa` (complex elements).
+// transform along an axis of stride `sa` (complex elements).  kl/ks >= 0 prune
+// the loads/stores along the transform axis; ko >= 0 maps the outer grid index
+// onto the kept indices of the outer axis.
 // ---------------------------------------------------------------------------
 template <typename T, typename TI, typename TO> struct IOPlain {
     const cx<TI> *src;
@@ -20,14 +36,16 @@ template <typename T, typename TI, typename TO> struct IOPlain {
     int64_t fs_src, fs_dst;  // field strides
     int64_t sa_src, so_src, sa_dst, so_dst;
     int ncol;
+    int n = 0, kl = -1, ks = -1, ko = -1;
+    H3D_D int outer(int y) const { return ko >= 0 ? kept_index(y, n, ko) : y; }
     H3D_D cx<T> load(int f, int o, int c, int p) const
     {
-        if (c >= ncol) return mk<T>(0, 0);
+        if (c >= ncol || (kl >= 0 && !kept(p, n, kl))) return mk<T>(0, 0);
         return to_cx<T>(src[f * fs_src + p * sa_src + o * so_src + c]);
     }
     H3D_D void store(int f, int o, int c, int p, cx<T> v) const
     {
-        if (c < ncol) dst[f * fs_dst + p * sa_dst + o * so_dst + c] = to_cx<TO>(v);
+        if (c < ncol && (ks < 0 || kept(p, n, ks))) dst[f * fs_dst + p * sa_dst + o * so_dst + c] = to_cx<TO>(v);
     }
 };
 
@@ -53,11 +71,13 @@ template <typename T, typename TO, int MODE> struct IOSpec {
     int n, psrc, pdst, ncol, sfield;
     double dx;     // grid spacing, for PRE_SHIFT
     double k2max;  // truncation radius squared, for PRE_TRUNC
+    int kl = -1, ko = -1;  // 2/3-rule pruning of the kz loads and the ky rows
+    H3D_D int outer(int y) const { return ko >= 0 ? kept_index(y, n, ko) : y; }
 
     H3D_D double2 U(int f, int o, int c, int p) const { return src[f * fs_src + ((int64_t)p * n + o) * psrc + c]; }
     H3D_D cx<T> load(int f, int o, int c, int p) const
     {
-        if (c >= ncol) return mk<T>(0, 0);
+        if (c >= ncol || (kl >= 0 && !kept(p, n, kl))) return mk<T>(0, 0);
         if constexpr (MODE == PRE_COPY) return to_cx<T>(U(f, o, c, p));
         const double kx = c, ky = kwave(o, n), kz = kwave(p, n);
         double2 r;
@@ -130,7 +150,7 @@ __global__ void __launch_bounds__(NT, (ColMinBlocks<L, NT>::value)) k_colfft(con
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
     using F = ColFFT<T, L, TC, NT, false, FWD, false>;
-    const int col0 = blockIdx.x * TC, outer = blockIdx.y, f = blockIdx.z;
+    const int col0 = blockIdx.x * TC, outer = io.outer(blockIdx.y), f = blockIdx.z;
     cx<T> in[F::NIN];
 #pragma unroll
     for (int i = 0; i < F::NB0; i++)
@@ -153,26 +173,29 @@ using RowFFT = ColFFT<T, L, TC, NT, true, REV ? false : true, REV>;
 
 // Hermitian-extended packed spectrum Z[k] = Xa[k] + i Xb[k] of rows A, B at
 // k in [0, L); the imaginary parts of kx = 0 and kx = N/2 are ignored, as
-// FFTW's c2r does.
+// FFTW's c2r does.  Only kx < lim is read (2/3-rule pruning; the rest is zero).
 template <typename T, int L, typename TS>
-H3D_D cx<T> load_packed(const cx<TS> *__restrict__ A, const cx<TS> *__restrict__ B, int k)
+H3D_D cx<T> load_packed(const cx<TS> *__restrict__ A, const cx<TS> *__restrict__ B, int k, int lim = L / 2 + 1)
 {
     if (k <= L / 2) {
+        if (k >= lim) return mk<T>(0, 0);
         cx<TS> a = A[k], b = B[k];
         if (k == 0 || k == L / 2) { a.y = 0; b.y = 0; }
         return mk<T>((T)(a.x - b.y), (T)(a.y + b.x));
     }
+    if (L - k >= lim) return mk<T>(0, 0);
     cx<TS> a = A[L - k], b = B[L - k];
     return mk<T>((T)(a.x + b.y), (T)(-a.y + b.x));
 }
 
 // After a forward row transform left Z (natural order) in shared memory: split
-// into the half spectra of the two packed rows and store them.
+// into the half spectra of the two packed rows and store kx < lim of them.
 template <typename T, int L, int TC, int NT, typename TS>
-H3D_D void store_split(const cx<T> *sm, cx<TS> *__restrict__ base, int64_t pitch, int pair0, int npairs)
+H3D_D void store_split(const cx<T> *sm, cx<TS> *__restrict__ base, int64_t pitch, int pair0, int npairs,
+                       int lim = L / 2 + 1)
 {
     using LY = Lay<L, TC, true>;
-    constexpr int NH = L / 2 + 1;
+    const int NH = lim < L / 2 + 1 ? lim : L / 2 + 1;
     for (int t = threadIdx.x; t < TC * NH; t += NT) {
         int c = t / NH, k = t - c * NH;
         if (pair0 + c >= npairs) continue;
@@ -192,7 +215,7 @@ H3D_D void store_split(const cx<T> *sm, cx<TS> *__restrict__ base, int64_t pitch
 // scaled by norm
 template <typename T, int L, int TC, int NT, typename TS>
 __global__ void __launch_bounds__(NT) k_xc2r(cx<TS> *base, int64_t fs, int64_t pitch, int npairs, T norm,
-                                             const cx<T> *__restrict__ tw)
+                                             const cx<T> *__restrict__ tw, int kx_lim)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
@@ -207,7 +230,7 @@ __global__ void __launch_bounds__(NT) k_xc2r(cx<TS> *base, int64_t fs, int64_t p
             int c, p;
             if (F::in_slot(i, m, c, p) && pair0 + c < npairs) {
                 const cx<TS> *A = fb + (int64_t)(2 * (pair0 + c)) * pitch;
-                in[i * F::R0 + m] = load_packed<T, L, TS>(A, A + pitch, p);
+                in[i * F::R0 + m] = load_packed<T, L, TS>(A, A + pitch, p, kx_lim > 0 ? kx_lim : L / 2 + 1);
             } else in[i * F::R0 + m] = mk<T>(0, 0);
         }
     F::run(in, sm, out, tw);
@@ -227,7 +250,7 @@ __global__ void __launch_bounds__(NT) k_xc2r(cx<TS> *base, int64_t fs, int64_t p
 // plain r2c (forward x pass) of one field, in place
 template <typename T, int L, int TC, int NT, typename TS>
 __global__ void __launch_bounds__(NT) k_xr2c(cx<TS> *base, int64_t fs, int64_t pitch, int npairs,
-                                             const cx<T> *__restrict__ tw)
+                                             const cx<T> *__restrict__ tw, int kx_lim)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
@@ -256,7 +279,7 @@ __global__ void __launch_bounds__(NT) k_xr2c(cx<TS> *base, int64_t fs, int64_t p
             if (F::out_slot(i, m, c, p)) sm[LY::idx(c, p)] = out[i * F::RL + m];
         }
     __syncthreads();
-    store_split<T, L, TC, NT, TS>(sm, fb, pitch, pair0, npairs);
+    store_split<T, L, TC, NT, TS>(sm, fb, pitch, pair0, npairs, kx_lim > 0 ? kx_lim : L / 2 + 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -281,6 +304,7 @@ struct FusedArgs {
     double *phys;        // optional: FP64 physical copies of the first OP::NPHYS inputs, [f][row][x]
     int64_t phys_fs, phys_pitch;
     double p0, p1;       // operator parameters
+    int kx_lim;          // > 0: only kx < kx_lim is read and stored (2/3-rule pruning)
 };
 
 template <typename T, int L, int TC, int NT, typename TS, class OP>
@@ -314,7 +338,7 @@ __global__ void __cluster_dims__(OP::NIN, 1, 1) __launch_bounds__(NT, 256 / NT)
                 int c, p;
                 if (FI::in_slot(i, m, c, p) && pair0 + c < a.npairs) {
                     const cx<TS> *A = fb + (int64_t)(2 * (pair0 + c)) * a.pitch;
-                    in[i * FI::R0 + m] = load_packed<T, L, TS>(A, A + a.pitch, p);
+                    in[i * FI::R0 + m] = load_packed<T, L, TS>(A, A + a.pitch, p, a.kx_lim > 0 ? a.kx_lim : L / 2 + 1);
                 } else in[i * FI::R0 + m] = mk<T>(0, 0);
             }
         FI::run_store_t(in, sm, twc, [&](int c, int p, cx<T> v) {
@@ -384,7 +408,8 @@ __global__ void __cluster_dims__(OP::NIN, 1, 1) __launch_bounds__(NT, 256 / NT)
         // its outputs can go straight back into the work buffer
         FF::run_store_t(in, sm, twc, [&](int c, int p, cx<T> v) { sm[LY::idx(c, p)] = v; });
         __syncthreads();
-        store_split<T, L, TC, NT, TS>(sm, reinterpret_cast<cx<TS> *>(a.out[o]), a.pitch, pair0, a.npairs);
+        store_split<T, L, TC, NT, TS>(sm, reinterpret_cast<cx<TS> *>(a.out[o]), a.pitch, pair0, a.npairs,
+                                      a.kx_lim > 0 ? a.kx_lim : L / 2 + 1);
         __syncthreads();
     }
     cl.sync();  // peers may still be reading this CTA's physical field
@@ -420,7 +445,7 @@ __global__ void __launch_bounds__(NT) k_xfused_reg(const FusedArgs a, const cx<T
                 int c, p;
                 if (FI::in_slot(i, m, c, p) && pair0 + c < a.npairs) {
                     const cx<TS> *A = fb + (int64_t)(2 * (pair0 + c)) * a.pitch;
-                    in[i * FI::R0 + m] = load_packed<T, L, TS>(A, A + a.pitch, p);
+                    in[i * FI::R0 + m] = load_packed<T, L, TS>(A, A + a.pitch, p, a.kx_lim > 0 ? a.kx_lim : L / 2 + 1);
                 } else in[i * FI::R0 + m] = mk<T>(0, 0);
             }
         // slots of idle butterflies are never written by run(): keep them zero so
@@ -495,7 +520,8 @@ __global__ void __launch_bounds__(NT) k_xfused_reg(const FusedArgs a, const cx<T
                 if (FF::out_slot(i, m, c, p)) sm[LY::idx(c, p)] = out[i * FF::RL + m];
             }
         __syncthreads();
-        store_split<T, L, TC, NT, TS>(sm, reinterpret_cast<cx<TS> *>(a.out[o]), a.pitch, pair0, a.npairs);
+        store_split<T, L, TC, NT, TS>(sm, reinterpret_cast<cx<TS> *>(a.out[o]), a.pitch, pair0, a.npairs,
+                                      a.kx_lim > 0 ? a.kx_lim : L / 2 + 1);
         __syncthreads();
     }
 }

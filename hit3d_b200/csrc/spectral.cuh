@@ -242,7 +242,13 @@ __global__ void k_scalar(const StepArgs a, int mode, int s, double dx, const cx<
         ModeIdx m = mode_of(t, a.n, a.nh);
         int64_t o = soff(m, a.n, a.pitch), po = soff(m, a.n, a.ppitch);
         double kx = m.ax, ky = m.ay, kz = m.az;
-        double2 pu = ld2<TP>(P, po), pv = ld2<TP>(P, po + a.pfs), pw = ld2<TP>(P, po + 2 * a.pfs);
+        // the products are read only where they are used (the 2/3 rule masks the rest)
+        double2 pu = make_double2(0.0, 0.0), pv = pu, pw = pu;
+        if (mode != 0 || m.ialias == 0) {
+            pu = ld2<TP>(P, po);
+            pv = ld2<TP>(P, po + a.pfs);
+            pw = ld2<TP>(P, po + 2 * a.pfs);
+        }
         if (mode == 1) {
             double2 sp = make_double2(0.0, 0.0);
             if (m.ialias < 2) {
@@ -337,6 +343,28 @@ __global__ void k_dealias_all(int n, int nh, int pitch, int64_t fs, int nf, int 
             for (int f = 0; f < nf; f++) U[o + f * fs] = make_double2(0.0, 0.0);
         }
     }
+}
+
+// max |component| of nf fields of A and B over the modes the 2/3 rule removes
+// (some |k_i| > N/3), as the bit pattern of a non-negative double: zero means
+// the transforms of a time step may skip those modes exactly
+__global__ void k_alias_max(int n, int nh, int pitch, int64_t fs, int nf, const double2 *__restrict__ A,
+                            const double2 *__restrict__ B, unsigned long long *out)
+{
+    const int64_t nm = (int64_t)n * n * nh;
+    double mx = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        ModeIdx m = mode_of(t, n, nh);
+        if (m.ialias > 0) {
+            const int64_t o = soff(m, n, pitch);
+            for (int f = 0; f < nf; f++) {
+                const double2 a = A[o + f * fs], b = B[o + f * fs];
+                mx = fmax(mx, fmax(fmax(fabs(a.x), fabs(a.y)), fmax(fabs(b.x), fabs(b.y))));
+            }
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if ((threadIdx.x & 31) == 0 && mx > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(mx));
 }
 
 // Shell spectrum sum_{shell} fac * |f|^2 (kx = 0 halved, kx = N/2 excluded),

@@ -96,6 +96,8 @@ SIGNATURES = [
     ("hit3d_gpu_launch_count", C.c_int64, [_vp]),
     ("hit3d_gpu_autotune", C.c_int, [_vp, C.POINTER(_i32), _dp]),
     ("hit3d_gpu_set_variant", C.c_int, [_vp, _i32]),
+    ("hit3d_gpu_set_pruning", C.c_int, [_vp, _i32]),
+    ("hit3d_gpu_pruned", C.c_int, [_vp]),
     ("hit3d_gpu_step_profile", C.c_int, [_vp, _i32, C.POINTER(_i32), C.POINTER(_i32), _dp]),
     ("hit3d_gpu_set_dt", C.c_int, [_vp, _d]),
     ("hit3d_gpu_set_scalars_active", C.c_int, [_vp, _i32]),
@@ -256,6 +258,18 @@ class Context:
 
     def set_variant(self, v: int):
         _check(lib().hit3d_gpu_set_variant(self._h, int(v)), "set_variant")
+
+    def set_pruning(self, on: bool):
+        """Allow (default) or forbid 2/3-rule pruning of the step's transforms."""
+        _check(lib().hit3d_gpu_set_pruning(self._h, int(bool(on))), "set_pruning")
+
+    @property
+    def pruned(self) -> bool:
+        """Whether the next step runs pruned transforms (checks the state on the device)."""
+        r = lib().hit3d_gpu_pruned(self._h)
+        if r < 0:
+            _check(r, "pruned")
+        return bool(r)
 
     @property
     def launches(self) -> int:

@@ -112,6 +112,17 @@ int hit3d_gpu_step_profile(hit3d_ctx *ctx, int32_t nsteps, int32_t *fov, int32_t
 int hit3d_gpu_autotune(hit3d_ctx *ctx, int32_t *variant, double *ms);
 int hit3d_gpu_set_variant(hit3d_ctx *ctx, int32_t variant);
 
+/* 2/3-rule pruning (no reference counterpart; on by default).  With the 2/3
+ * rule, when every mode with some |k_i| > N/3 is zero in the state (the
+ * reference dealiases at start, dealias_all.f90, and its update keeps those
+ * modes zero), the transforms of a step skip the columns, rows and outputs
+ * that are zero or that the update masks (rhs_velocity.f90:85-142).  The
+ * result is bit-identical; the state is checked on the device before the
+ * first step after every change, and a state with energy beyond N/3 runs the
+ * full transforms.  hit3d_gpu_pruned returns 1 if the next step is pruned. */
+int hit3d_gpu_set_pruning(hit3d_ctx *ctx, int32_t on);
+int hit3d_gpu_pruned(hit3d_ctx *ctx);
+
 /* Number of kernels this context has launched since hit3d_gpu_init. */
 int64_t hit3d_gpu_launch_count(hit3d_ctx *ctx);
 
