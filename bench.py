@@ -147,8 +147,9 @@ def stage_units(n, precision, pruned):
 
     With 2/3-rule pruning a = (kc+1)/(N/2+1) of the kx columns and b = (2 kc+1)/N of
     the ky (or kz) indices are kept (kc = N/3): inverse passes read only kept
-    indices along their axis and forward passes store only kept indices.  The
-    update reads the products only at kept modes (a b^2) in either case.  Work
+    indices along their axis and forward passes store only kept indices, and the
+    update visits only the kept modes (a b^2).  Unpruned, the update still reads
+    the products only at kept modes.  Work
     fields are half size in the FP32 form; the state stays FP64."""
     kc = n // 3
     a0, b0 = (kc + 1) / (n // 2 + 1), (2 * kc + 1) / n
@@ -160,7 +161,8 @@ def stage_units(n, precision, pruned):
         "x_fused": w * (3 * a + 6 * a),
         "y_forward": w * (6 * a + 6 * a * b),
         "z_forward": w * (6 * a * b + 6 * a * b * b),
-        "update": 12 + w * 6 * a0 * b0 * b0,
+        # U, RO read and written, products read: at the kept modes only when pruned
+        "update": (12 if not pruned else 12 * a0 * b0 * b0) + w * 6 * a0 * b0 * b0,
     }
 
 

@@ -360,6 +360,99 @@ struct ColFFT {
         run_store_t(in, sm, GlobalTw<T>{tw}, st);
     }
 
+    // NF independent transforms in lockstep: field f uses the shared-memory
+    // buffer sm + f * LY::elems, all fields share one barrier per stage and one
+    // twiddle load per butterfly.  Last-stage outputs are left in out[f][...].
+    // The caller must __syncthreads() before reusing sm after this returns.
+    template <int NF>
+    static H3D_D void run_multi(cx<T> (&in)[NF][NIN], cx<T> *sm, cx<T> (&out)[NF][NOUT], const cx<T> *__restrict__ tw)
+    {
+        constexpr int E = LY::elems;
+        const int tid = threadIdx.x;
+#pragma unroll
+        for (int i = 0; i < NB0; i++) {
+            int b = tid + i * NT;
+            if (TOT0 % NT == 0 || b < TOT0) {
+                int c, j;
+                LY::template bf<R0>(b, c, j);
+#pragma unroll
+                for (int f = 0; f < NF; f++) {
+                    dft<T, R0, FWD>(in[f] + i * R0);
+#pragma unroll
+                    for (int m = 0; m < R0; m++) sm[f * E + LY::idx(c, j * R0 + m)] = in[f][i * R0 + m];
+                }
+            }
+        }
+        __syncthreads();
+        if constexpr (S > 2) mid_multi<NF, 1>(sm, tw);
+        if constexpr (S > 3) mid_multi<NF, 2>(sm, tw);
+        constexpr int NsL = P::Ns(S - 1), nbpc = L / RL;
+#pragma unroll
+        for (int i = 0; i < NBL; i++) {
+            int b = tid + i * NT;
+            if (TOTL % NT == 0 || b < TOTL) {
+                int c, j;
+                LY::template bf<RL>(b, c, j);
+                const int k = j % NsL;
+#pragma unroll
+                for (int m = 0; m < RL; m++) {
+                    const cx<T> w = m > 0 ? twid<T, FWD>(tw, k * m * (L / (NsL * RL))) : mk<T>(1, 0);
+#pragma unroll
+                    for (int f = 0; f < NF; f++) {
+                        cx<T> x = sm[f * E + LY::idx(c, j + m * nbpc)];
+                        out[f][i * RL + m] = m > 0 ? cmul(x, w) : x;
+                    }
+                }
+#pragma unroll
+                for (int f = 0; f < NF; f++) dft<T, RL, FWD>(out[f] + i * RL);
+            }
+        }
+    }
+    template <int NF, int s> static H3D_D void mid_multi(cx<T> *sm, const cx<T> *__restrict__ tw)
+    {
+        constexpr int E = LY::elems;
+        constexpr int R = P::R(s), Ns = P::Ns(s), nbpc = L / R;
+        using CN = Cnt<L, TC, NT, R>;
+        cx<T> a[NF][CN::NB * R];
+        const int tid = threadIdx.x;
+#pragma unroll
+        for (int i = 0; i < CN::NB; i++) {
+            int b = tid + i * NT;
+            if (CN::total % NT == 0 || b < CN::total) {
+                int c, j;
+                LY::template bf<R>(b, c, j);
+                const int k = j % Ns;
+#pragma unroll
+                for (int m = 0; m < R; m++) {
+                    const cx<T> w = m > 0 ? twid<T, FWD>(tw, k * m * (L / (Ns * R))) : mk<T>(1, 0);
+#pragma unroll
+                    for (int f = 0; f < NF; f++) {
+                        cx<T> v = sm[f * E + LY::idx(c, j + m * nbpc)];
+                        a[f][i * R + m] = m > 0 ? cmul(v, w) : v;
+                    }
+                }
+#pragma unroll
+                for (int f = 0; f < NF; f++) dft<T, R, FWD>(a[f] + i * R);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < CN::NB; i++) {
+            int b = tid + i * NT;
+            if (CN::total % NT == 0 || b < CN::total) {
+                int c, j;
+                LY::template bf<R>(b, c, j);
+                const int k = j % Ns;
+                const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+                for (int f = 0; f < NF; f++)
+#pragma unroll
+                    for (int m = 0; m < R; m++) sm[f * E + LY::idx(c, base + m * Ns)] = a[f][i * R + m];
+            }
+        }
+        __syncthreads();
+    }
+
     // the transform with the last-stage outputs left in out[i*RL+m]
     static H3D_D void run(cx<T> (&in)[NIN], cx<T> *sm, cx<T> (&out)[NOUT], const cx<T> *__restrict__ tw)
     {

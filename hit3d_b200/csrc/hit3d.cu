@@ -79,7 +79,8 @@ template <typename T, int L, int V> struct RowCfgV {
     static constexpr size_t SMEM = (size_t)Lay<L, TC, true>::elems * sizeof(cx<T>);
 };
 //   4: register-resident kernel (k_xfused_reg), 1024/L pairs x 128 threads
-constexpr int kFusedVariants = 5;
+//   5, 6: lockstep kernel (k_xfused_ms), forward transforms in groups of 3 / 2
+constexpr int kFusedVariants = 7;
 
 // Raise a kernel's dynamic shared-memory limit once per kernel and device, so
 // that steps recorded into a CUDA graph later make no attribute calls.
@@ -325,9 +326,23 @@ template <typename T, template <class> class OP, int L> static int xfused_reg_L(
     H3D_LAUNCH_CHECK();
     return 0;
 }
+template <typename T, template <class> class OP, int L, int GF> static int xfused_ms_L(hit3d_ctx *c, FusedArgs a)
+{
+    using RC = RowCfg<T, L>;
+    constexpr int NB = OP<T>::NIN > GF ? OP<T>::NIN : GF;  // shared-memory buffers
+    auto k = k_xfused_ms<T, L, RC::TC, RC::NT, T, OP<T>, GF>;
+    H3D_TRY(set_smem(k, NB * RC::SMEM));
+    k<<<dim3((a.npairs + RC::TC - 1) / RC::TC), RC::NT, NB * RC::SMEM, c->st>>>(a, twid<T>(c));
+    H3D_LAUNCH_CHECK();
+    return 0;
+}
 template <typename T, template <class> class OP, int L> static int xfused_L(hit3d_ctx *c, FusedArgs a)
 {
-    if (c->xcfg == 4) return xfused_reg_L<T, OP, L>(c, a);
+    if constexpr (OP<T>::NIN <= 3) {
+        if (c->xcfg == 5) return xfused_ms_L<T, OP, L, 3>(c, a);
+        if (c->xcfg == 6) return xfused_ms_L<T, OP, L, 2>(c, a);
+    }
+    if (c->xcfg >= 4) return xfused_reg_L<T, OP, L>(c, a);
     if constexpr (L >= 128) {
         switch (c->xcfg) {
         case 1: return xfused_LV<T, OP, L, 1>(c, a);
@@ -448,6 +463,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     a.n = c->n; a.nh = c->nh; a.pitch = c->P64; a.ppitch = wp; a.fs = c->fs64; a.pfs = wfs;
     a.nu = p.nu; a.dt = p.dt; a.euler_v = euler_v; a.euler_s = euler_s;
     a.flow_type = p.flow_type; a.kfmax = p.kfmax; a.famp = p.famp; a.fenergy = c->d_fen; a.nscal = ns;
+    a.kc = c->kc_active;  // pruned state: the updates visit only the kept modes
     for (int s = 0; s < c->nsc; s++) { a.pe[s] = p.nu / p.sc[s]; a.stype[s] = p.scalar_type[s]; }
 
     MARK(7);

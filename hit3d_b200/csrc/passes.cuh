@@ -527,6 +527,131 @@ __global__ void __launch_bounds__(NT) k_xfused_reg(const FusedArgs a, const cx<T
 }
 
 
+// Lockstep form of the fused x pass: the NIN inverse transforms advance
+// together (one barrier per radix stage for all of them, one twiddle load per
+// butterfly) and the NOUT forward transforms in groups of GF, each transform
+// with its own shared-memory buffer.  More independent work between barriers
+// than k_xfused_reg at the same register budget per transform; the tuner picks.
+template <typename T, int L, int TC, int NT, typename TS, class OP, int GF>
+__global__ void __launch_bounds__(NT) k_xfused_ms(const FusedArgs a, const cx<T> *__restrict__ tw)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
+    using FI = RowFFT<T, L, TC, NT, true>;
+    using FF = RowFFT<T, L, TC, NT, false>;
+    static_assert(FI::NOUT == FF::NIN, "slot hand-off mismatch");
+    constexpr int NP = FI::NOUT;
+    constexpr int E = Lay<L, TC, true>::elems;
+    const int pair0 = blockIdx.x * TC;
+    const T norm = (T)a.norm;
+    const int lim = a.kx_lim > 0 ? a.kx_lim : L / 2 + 1;
+    OP op{(T)a.p0, (T)a.p1};
+
+    cx<T> phys[OP::NIN][NP];
+    {
+        cx<T> in[OP::NIN][FI::NIN];
+#pragma unroll
+        for (int f = 0; f < OP::NIN; f++) {
+            const cx<TS> *fb = reinterpret_cast<const cx<TS> *>(a.in[f]);
+#pragma unroll
+            for (int i = 0; i < FI::NB0; i++)
+#pragma unroll
+                for (int m = 0; m < FI::R0; m++) {
+                    int c, p;
+                    if (FI::in_slot(i, m, c, p) && pair0 + c < a.npairs) {
+                        const cx<TS> *A = fb + (int64_t)(2 * (pair0 + c)) * a.pitch;
+                        in[f][i * FI::R0 + m] = load_packed<T, L, TS>(A, A + a.pitch, p, lim);
+                    } else in[f][i * FI::R0 + m] = mk<T>(0, 0);
+                }
+            // idle butterflies never write their slots: keep them zero
+#pragma unroll
+            for (int q = 0; q < NP; q++) phys[f][q] = mk<T>(0, 0);
+        }
+        FI::template run_multi<OP::NIN>(in, sm, phys, tw);
+    }
+#pragma unroll
+    for (int f = 0; f < OP::NIN; f++)
+#pragma unroll
+        for (int q = 0; q < NP; q++) phys[f][q] = mk<T>(phys[f][q].x * norm, phys[f][q].y * norm);
+    __syncthreads();
+    if (a.phys != nullptr) {
+        double *pb = a.phys;
+#pragma unroll
+        for (int i = 0; i < FI::NBL; i++)
+#pragma unroll
+            for (int m = 0; m < FI::RL; m++) {
+                int c, p;
+                if (FI::out_slot(i, m, c, p) && pair0 + c < a.npairs) {
+                    int64_t r = 2 * (pair0 + c);
+#pragma unroll
+                    for (int f = 0; f < OP::NPHYS; f++) {
+                        pb[f * a.phys_fs + r * a.phys_pitch + p] = (double)phys[f][i * FI::RL + m].x;
+                        pb[f * a.phys_fs + (r + 1) * a.phys_pitch + p] = (double)phys[f][i * FI::RL + m].y;
+                    }
+                }
+            }
+    }
+    if (a.cmax != nullptr) {
+        double cm = 0.0;
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            T va[OP::NIN], vb[OP::NIN];
+#pragma unroll
+            for (int f = 0; f < OP::NIN; f++) { va[f] = phys[f][q].x; vb[f] = phys[f][q].y; }
+            cm = fmax(cm, (double)op.cour(va));
+            cm = fmax(cm, (double)op.cour(vb));
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, off));
+        if ((threadIdx.x & 31) == 0) atomicMax(a.cmax, (unsigned long long)__double_as_longlong(cm));
+    }
+    cx<T> aux[NP];
+#pragma unroll
+    for (int q = 0; q < NP; q++) {
+        T va[OP::NIN], vb[OP::NIN];
+#pragma unroll
+        for (int f = 0; f < OP::NIN; f++) { va[f] = phys[f][q].x; vb[f] = phys[f][q].y; }
+        aux[q] = mk<T>(op.aux(va), op.aux(vb));
+    }
+    using LY = typename FF::LY;
+    constexpr int NG = (OP::NOUT + GF - 1) / GF;
+#pragma unroll 1
+    for (int g = 0; g < NG; g++) {
+        cx<T> in[GF][FF::NIN], out[GF][FF::NOUT];
+#pragma unroll
+        for (int gf = 0; gf < GF; gf++) {
+            const int o = g * GF + gf;
+#pragma unroll
+            for (int q = 0; q < NP; q++) {
+                T va[OP::NIN], vb[OP::NIN];
+#pragma unroll
+                for (int f = 0; f < OP::NIN; f++) { va[f] = phys[f][q].x; vb[f] = phys[f][q].y; }
+                in[gf][q] = o < OP::NOUT ? mk<T>(op.out(o, va, aux[q].x), op.out(o, vb, aux[q].y)) : mk<T>(0, 0);
+            }
+        }
+        FF::template run_multi<GF>(in, sm, out, tw);
+        __syncthreads();
+#pragma unroll
+        for (int gf = 0; gf < GF; gf++)
+#pragma unroll
+            for (int i = 0; i < FF::NBL; i++)
+#pragma unroll
+                for (int m = 0; m < FF::RL; m++) {
+                    int c, p;
+                    if (FF::out_slot(i, m, c, p)) sm[gf * E + LY::idx(c, p)] = out[gf][i * FF::RL + m];
+                }
+        __syncthreads();
+#pragma unroll
+        for (int gf = 0; gf < GF; gf++) {
+            const int o = g * GF + gf;
+            if (o < OP::NOUT)
+                store_split<T, L, TC, NT, TS>(sm + gf * E, reinterpret_cast<cx<TS> *>(a.out[o]), a.pitch, pair0,
+                                              a.npairs, lim);
+        }
+        __syncthreads();
+    }
+}
+
 // velocity products (rhs_velocity.f90:56-72): uu uv uw vv vw ww; Courant |u|+|v|+|w|
 template <typename T> struct OpVel {
     static constexpr int NIN = 3, NOUT = 6, NPHYS = 3;

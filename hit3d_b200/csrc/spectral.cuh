@@ -27,6 +27,26 @@ H3D_D ModeIdx mode_of(int64_t t, int n, int nh)
 }
 H3D_D int64_t soff(const ModeIdx &m, int n, int pitch) { return ((int64_t)m.kzi * n + m.kyi) * pitch + m.kx; }
 
+// Mode loops of the 2/3-rule updates.  kc < 0: every mode (index t over
+// N x N x (N/2+1)).  kc >= 0 (pruned state: U and RO are zero wherever some
+// |k_i| > kc and the update keeps them zero): only the kept modes, t over
+// (kc+1) x (2kc+1)^2 with kx fastest, so that masked modes are neither read nor
+// written.
+H3D_D int64_t mode_count(int n, int nh, int kc)
+{
+    return kc < 0 ? (int64_t)n * n * nh : (int64_t)(kc + 1) * (2 * kc + 1) * (2 * kc + 1);
+}
+H3D_D ModeIdx mode_at(int64_t t, int n, int nh, int kc)
+{
+    if (kc < 0) return mode_of(t, n, nh);
+    const int nk = 2 * kc + 1;
+    const int kx = (int)(t % (kc + 1));
+    const int64_t r = t / (kc + 1);
+    const int yc = (int)(r % nk), zc = (int)(r / nk);
+    const int kyi = yc <= kc ? yc : n - (nk - yc), kzi = zc <= kc ? zc : n - (nk - zc);
+    return mode_of(((int64_t)kzi * n + kyi) * nh + kx, n, nh);
+}
+
 // Machiels band forcing: a mode takes part when kx < N/2 (the reference loops
 // over real indices 1..nx) and its float32 shell index is in [1, kfmax]
 // (m_force.f90:166-209).
@@ -84,6 +104,7 @@ struct StepArgs {
     int nscal;
     double pe[8];
     int stype[8];
+    int kc;                    // >= 0: visit only the modes the 2/3 rule keeps (pruned state)
 };
 
 // 2/3 rule (rhs_velocity.f90:85-142) + forcing + AB2 + pressure.
@@ -94,10 +115,10 @@ template <typename TP>
 __global__ void k_update_vel_23(const StepArgs a, const cx<TP> *__restrict__ P, const cx<TP> *__restrict__ TAU,
                                 double2 *__restrict__ U, double2 *__restrict__ RO)
 {
-    const int64_t nm = (int64_t)a.n * a.n * a.nh;
+    const int64_t nm = mode_count(a.n, a.nh, a.kc);
     const double fac = (a.flow_type == 1) ? a.famp / *a.fenergy : 0.0;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
-        ModeIdx m = mode_of(t, a.n, a.nh);
+        ModeIdx m = mode_at(t, a.n, a.nh, a.kc);
         int64_t o = soff(m, a.n, a.pitch), po = soff(m, a.n, a.ppitch);
         double2 u[3] = {U[o], U[o + a.fs], U[o + 2 * a.fs]};
         double2 r[3];
@@ -236,10 +257,11 @@ __global__ void k_scalar(const StepArgs a, int mode, int s, double dx, const cx<
                          double2 *__restrict__ SP, const double2 *__restrict__ Uvel, double2 *__restrict__ PHI,
                          double2 *__restrict__ RO)
 {
-    const int64_t nm = (int64_t)a.n * a.n * a.nh;
+    const int kc = mode == 0 ? a.kc : -1;
+    const int64_t nm = mode_count(a.n, a.nh, kc);
     const double pe = a.pe[s];
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
-        ModeIdx m = mode_of(t, a.n, a.nh);
+        ModeIdx m = mode_at(t, a.n, a.nh, kc);
         int64_t o = soff(m, a.n, a.pitch), po = soff(m, a.n, a.ppitch);
         double kx = m.ax, ky = m.ay, kz = m.az;
         // the products are read only where they are used (the 2/3 rule masks the rest)
