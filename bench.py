@@ -240,10 +240,10 @@ def les_leg(torch, args, dns_rate, dns32_rate, device):
     w[nparam - 5] = -2.0 * 0.18 ** 2 * dx * dx / (delta * delta)
     bits = ((w.view(np.uint32).astype(np.uint64) + 0x7FFF + ((w.view(np.uint32) >> 16) & 1)) >> 16).astype(np.uint16)
     rates = {}
-    for name, model, kernel in (("learned", 2, 1), ("learned_cuda_cores", 2, 0), ("smagorinsky", 1, 0)):
+    for name, model, kernel in (("learned", 20, 1), ("learned_cuda_cores", 20, 0), ("smagorinsky", 1, 0)):
         c = Context(Params(nx=n_les, dealias=0, flow_type=1, force_type=1, kfmax=2, famp=0.5, nu=1.0 / RE, dt=dt_les,
                            les_model=model, device=device))
-        if model == 2:
+        if model == 20:
             c.les_set_mlp(bits, delta, clip=True, kernel=kernel)
         c.init_velocity(RN1, 2, 4.0, 2.0)
         c.dealias_all()
@@ -255,7 +255,7 @@ def les_leg(torch, args, dns_rate, dns32_rate, device):
         steps = max(args.steps, 50)
         t = timed_steps(torch, c, steps)
         rates[name] = steps / t
-        if model == 2:
+        if model == 20:
             prof = c.step_profile(3)
             out[name + "_stage_ms"] = {("closure" if k == "smagorinsky" else k): round(v / 3, 4)
                                        for k, v in prof.items() if v > 0}

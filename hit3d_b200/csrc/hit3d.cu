@@ -146,7 +146,7 @@ struct hit3d_ctx {
     int64_t nlaunch;
     int xcfg;            // launch-shape variant of the fused x pass
     double k2max;        // truncation radius squared of PRE_TRUNC
-    void *mlp_wb;        // bf16 weights of the learned closure (les_model 2)
+    void *mlp_wb;        // bf16 weights of the learned closure (les_model HIT3D_LES_LEARNED)
     double mlp_delta;    // filter width the closure was trained for
     int mlp_clip;        // zero the stress where its dissipation is negative
     int mlp_kernel;      // 0: CUDA cores, 1: tensor cores for the hidden layers
@@ -456,7 +456,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     auto Wf = [&](int i) { return W + i * wfs; };
     const int ns = c->int_scalars ? c->nsc : 0;
     const int nprod = 6 + 3 * ns;
-    const bool les = p.les_model == 1, les_mlp = p.les_model == 2;
+    const bool les = p.les_model == 1, les_mlp = p.les_model == HIT3D_LES_LEARNED;
 
     StepArgs a;
     memset(&a, 0, sizeof a);
@@ -644,7 +644,9 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     if (p->dealias != 0 && p->dealias != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: wrong dealias flag");
     if (p->flow_type == 1 && p->force_type != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: WRONG FORCE TYPE");
     if (p->flow_type == 1 && (p->kfmax < 1 || p->kfmax > 15)) return h3d_set_error_msg(-1, "hit3d_gpu_init: kfmax must be in 1..15");
-    if (p->les_model < 0 || p->les_model > 2) return h3d_set_error_msg(-1, "hit3d_gpu_init: only les_model 0, 1 and 2 are supported");
+    if (p->les_model != 0 && p->les_model != 1 && p->les_model != HIT3D_LES_LEARNED)
+        return h3d_set_error_msg(-1, "hit3d_gpu_init: les_model must be 0 (none), 1 (Smagorinsky) or 20 (learned closure); "
+                                     "the reference's models 2-10 are not supported");
     if (p->les_model != 0 && p->n_scalars > 0) return h3d_set_error_msg(-1, "hit3d_gpu_init: LES with scalars is not supported");
     if (p->precision != 0 && p->precision != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: precision must be 0 or 1");
     for (int s = 0; s < p->n_scalars; s++) {
@@ -677,7 +679,7 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     int rc = 0;
     const int nf = 3 + c->nsc;
     const size_t f64 = (size_t)c->fs64 * sizeof(double2);
-    c->nw = 6 + 3 * c->nsc + (c->p.les_model == 1 ? 6 : c->p.les_model == 2 ? 9 : 0);
+    c->nw = 6 + 3 * c->nsc + (c->p.les_model == 1 ? 6 : c->p.les_model == HIT3D_LES_LEARNED ? 9 : 0);
     if (c->p.precision == 0) {
         c->wpitch = c->P64;
         c->wfs = c->fs64;
@@ -796,8 +798,8 @@ extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_
 {
     if (!c) return h3d_set_error_msg(-1, "null context");
     if (nsteps < 0) return h3d_set_error_msg(-1, "nsteps < 0");
-    if (c->p.les_model == 2 && !c->mlp_wb)
-        return h3d_set_error_msg(-1, "hit3d_gpu_step: les_model 2 needs weights (hit3d_gpu_les_set_mlp)");
+    if (c->p.les_model == HIT3D_LES_LEARNED && !c->mlp_wb)
+        return h3d_set_error_msg(-1, "hit3d_gpu_step: the learned closure (les_model 20) needs weights (hit3d_gpu_les_set_mlp)");
     H3D_CHECK(cudaSetDevice(c->dev));
     H3D_TRY(ensure_alias_state(c));
     int ev = fov ? (*fov != 0) : 0, es = fos ? (*fos != 0) : 0;
@@ -809,7 +811,7 @@ extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_
     }
     if (fov) *fov = ev;
     if (fos) *fos = es;
-    if (c->p.les_model == 2 && c->mlp_kernel == 1 && nsteps > 0) {
+    if (c->p.les_model == HIT3D_LES_LEARNED && c->mlp_kernel == 1 && nsteps > 0) {
         int herr = 0;
         H3D_CHECK(cudaMemcpyAsync(&herr, c->d_mlp_err, sizeof herr, cudaMemcpyDeviceToHost, c->st));
         H3D_CHECK(cudaStreamSynchronize(c->st));
@@ -833,7 +835,8 @@ extern "C" int hit3d_gpu_les_set_mlp(hit3d_ctx *c, const uint16_t *wb, int64_t n
 {
     if (!c || !wb) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: null argument");
     if (kernel != 0 && kernel != 1) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: kernel must be 0 or 1");
-    if (c->p.les_model != 2) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: the context needs les_model 2");
+    if (c->p.les_model != HIT3D_LES_LEARNED)
+        return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: the context needs les_model 20 (learned closure)");
     if (nparam != hit3d_mlp_nparam()) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: wrong parameter count");
     if (!(delta > 0.0)) return h3d_set_error_msg(-1, "hit3d_gpu_les_set_mlp: filter width must be positive");
     H3D_CHECK(cudaSetDevice(c->dev));

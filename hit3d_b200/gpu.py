@@ -21,6 +21,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libhit3d_gpu.so")
 MAX_SCALARS = 8
+LES_LEARNED = 20  # les_model of the learned closure (HIT3D_LES_LEARNED)
 _lib = None
 
 
@@ -365,7 +366,7 @@ class Context:
 
     def les_set_mlp(self, bf16_weights: np.ndarray, delta: float, clip: bool = True, kernel: int = 1):
         """Use trained bf16 weights (uint16 bit patterns) as this context's subgrid model
-        (les_model 2); delta is the filter width the network was trained for; kernel 1
+        (les_model LES_LEARNED = 20); delta is the filter width the network was trained for; kernel 1
         runs the hidden layers on the tensor cores, 0 on the CUDA cores in fp32."""
         w = np.ascontiguousarray(bf16_weights, dtype=np.uint16)
         _check(lib().hit3d_gpu_les_set_mlp(self._h, w.ctypes.data_as(C.POINTER(C.c_uint16)), w.size, float(delta),

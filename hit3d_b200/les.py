@@ -16,7 +16,7 @@ from typing import Dict, List, Optional
 import numpy as np
 
 from .batch import Batch, run_seed
-from .gpu import Context, Mlp, Params
+from .gpu import LES_LEARNED, Context, Mlp, Params
 
 PAIRS = [(0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2)]
 FROB = np.array([1.0, 2.0, 2.0, 1.0, 2.0, 1.0])
@@ -195,11 +195,11 @@ def run_experiment(ex: LesExperiment, device: int = 0, log=print) -> Dict:
     dns.upload_rhs_old(r0)
     dns.fov = 0
     ref = Context(ex.les_params(0))
-    models = {"learned": 2, "smagorinsky": 1, "none": 0}
+    models = {"learned": LES_LEARNED, "smagorinsky": 1, "none": 0}
     les = {}
     for name, model in models.items():
         c = Context(ex.les_params(model))
-        if model == 2:
+        if model == LES_LEARNED:
             c.les_set_mlp(w16, ex.delta, clip=ex.clip, kernel=ex.kernel)
         filtered_state(f0, c, ex.delta)
         les[name] = c

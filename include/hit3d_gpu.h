@@ -33,6 +33,8 @@ extern "C" {
 typedef struct hit3d_ctx hit3d_ctx;
 
 #define HIT3D_MAX_SCALARS 8
+/* les_model of the learned closure; outside the reference's model numbers 0-10 */
+#define HIT3D_LES_LEARNED 20
 
 /* Run parameters; the values the reference reads from <run_name>.in
  * (m_parameters.f90:172-512) and derives at start-up. */
@@ -45,8 +47,9 @@ typedef struct hit3d_params {
     int32_t n_scalars;   /* passive scalars, <= HIT3D_MAX_SCALARS (m_parameters.f90:424)   */
     int32_t precision;   /* 0: FP64 transforms; 1: FP32 nonlinear-term transforms with FP64
                             state, integrator and reductions (no reference counterpart)    */
-    int32_t les_model;   /* 0: none; 1: Smagorinsky (m_les.f90:94-106); 2: learned closure
-                            (hit3d_gpu_les_set_mlp; no reference counterpart)              */
+    int32_t les_model;   /* 0: none; 1: Smagorinsky (m_les.f90:94-106); HIT3D_LES_LEARNED (20):
+                            learned closure (hit3d_gpu_les_set_mlp; no reference
+                            counterpart).  The reference's models 2-10 are rejected.       */
     int32_t scalar_type[HIT3D_MAX_SCALARS]; /* 0 = uniform mean gradient source            */
     int32_t device;      /* CUDA device ordinal                                            */
     int32_t reserved;
@@ -279,7 +282,7 @@ int hit3d_mlp_train(hit3d_mlp *m, int32_t nsteps, int64_t batch, double lr, doub
  * TMEM accumulators) with their inputs rounded to bf16. */
 int hit3d_mlp_predict(hit3d_mlp *m, const float *A, int64_t np, double delta, int32_t clip, int32_t kernel,
                       float *tau);
-/* Use a trained network as the context's subgrid model (les_model 2): nparam
+/* Use a trained network as the context's subgrid model (les_model 20): nparam
  * bf16 weights, the filter width they were trained for, the clip switch and
  * the inference kernel (as in hit3d_mlp_predict). */
 int hit3d_gpu_les_set_mlp(hit3d_ctx *ctx, const uint16_t *bf16_weights, int64_t nparam, double delta, int32_t clip,

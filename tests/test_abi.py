@@ -61,3 +61,12 @@ def test_unsupported_size_rejected_before_device_use():
     from hit3d_b200 import Hit3dError, Params, Context
     with pytest.raises(Hit3dError, match="grid size"):
         Context(Params(nx=100))
+
+
+def test_reference_les_models_without_a_port_are_rejected():
+    """The reference's LES models 2-10 (DLM, DSTM, mixed) are not built: an input
+    asking for one fails at init instead of running another model."""
+    from hit3d_b200 import Hit3dError, Params, Context
+    for m in (2, 3, 4, 5, 6, 7, 10):
+        with pytest.raises(Hit3dError, match="les_model"):
+            Context(Params(nx=32, les_model=m))

@@ -108,7 +108,7 @@ def test_les_step_with_smagorinsky_weights_matches_smagorinsky(kernel):
     cs = np.sqrt(-g1 * DELTA ** 2 / (2 * dx * dx))
     common = dict(nx=n, flow_type=1, kfmax=2, nu=1.0 / 2000.0, dt=0.005)
     a = Context(Params(les_model=1, c_smag=cs, **common))
-    b = Context(Params(les_model=2, **common))
+    b = Context(Params(les_model=20, **common))
     w = mo.smagorinsky_params(0.0, dx, DELTA)
     w[-5] = g1
     b.les_set_mlp(mo.bf16_bits(w), DELTA, clip=True, kernel=kernel)
@@ -128,11 +128,11 @@ def test_les_step_with_smagorinsky_weights_matches_smagorinsky(kernel):
 
 def test_learned_les_needs_weights():
     from hit3d_b200 import Context, Hit3dError, Params
-    c = Context(Params(nx=32, les_model=2))
+    c = Context(Params(nx=32, les_model=20))
     with pytest.raises(Hit3dError, match="weights"):
         c.step(1)
     d = Context(Params(nx=32, les_model=1))
-    with pytest.raises(Hit3dError, match="les_model 2"):
+    with pytest.raises(Hit3dError, match="les_model 20"):
         d.les_set_mlp(np.zeros(mo.NPARAM, np.uint16), DELTA)
 
 

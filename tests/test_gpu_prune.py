@@ -15,8 +15,8 @@ CASES = [
     (64, 1, dict(n_scalars=1, sc=[0.7], scalar_type=[0])),
     (128, 1, {}),
     (32, 0, dict(les_model=1)),
-    (32, 0, dict(les_model=2)),
-    (64, 1, dict(les_model=2)),
+    (32, 0, dict(les_model=20)),
+    (64, 1, dict(les_model=20)),
 ]
 
 
@@ -24,7 +24,7 @@ def _run(n, precision, extra, prune, steps=5):
     from hit3d_b200 import Context, Params
     from oracle import mlp_oracle as mo
     c = Context(Params(nx=n, flow_type=1, kfmax=2, nu=1.0 / 800.0, dt=0.002, precision=precision, **extra))
-    if extra.get("les_model") == 2:
+    if extra.get("les_model") == 20:
         c.les_set_mlp(mo.bf16_bits(mo.bf16_round(mo.init_params(4) * 0.05)), 4 * np.pi / n, clip=True, kernel=1)
     c.set_pruning(prune)
     c.init_velocity(RN1, 2, 4.0, 2.0)
