@@ -151,6 +151,7 @@ struct hit3d_ctx {
     int mlp_clip;        // zero the stress where its dissipation is negative
     int mlp_kernel;      // 0: CUDA cores, 1: tensor cores for the hidden layers
     int *d_mlp_err;      // set by the tensor-core kernel when a completion wait runs out
+    double *d_kmin;      // dynamic localization model: minimum of k_sgs in the current step (slot 2)
     int prune_on;        // allow 2/3-rule pruning of the step's transforms
     int pruned;          // the state is zero beyond N/3 (checked), so pruning is exact
     int alias_known;     // `pruned` is up to date with the state
@@ -212,6 +213,7 @@ static int zinv_L(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src
         case PRE_CURL: return zinv_LM<T, L, PRE_CURL>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         case PRE_DLONG: return zinv_LM<T, L, PRE_DLONG>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         case PRE_TRUNC: return zinv_LM<T, L, PRE_TRUNC>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+        case PRE_CUBE: return zinv_LM<T, L, PRE_CUBE>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         default: break;
         }
     }
@@ -456,7 +458,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     auto Wf = [&](int i) { return W + i * wfs; };
     const int ns = c->int_scalars ? c->nsc : 0;
     const int nprod = 6 + 3 * ns;
-    const bool les = p.les_model == 1, les_mlp = p.les_model == HIT3D_LES_LEARNED;
+    const bool les = p.les_model == 1, les_mlp = p.les_model == HIT3D_LES_LEARNED, dlm = p.les_model == 2;
 
     StepArgs a;
     memset(&a, 0, sizeof a);
@@ -464,9 +466,44 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     a.nu = p.nu; a.dt = p.dt; a.euler_v = euler_v; a.euler_s = euler_s;
     a.flow_type = p.flow_type; a.kfmax = p.kfmax; a.famp = p.famp; a.fenergy = c->d_fen; a.nscal = ns;
     a.kc = c->kc_active;  // pruned state: the updates visit only the kept modes
-    for (int s = 0; s < c->nsc; s++) { a.pe[s] = p.nu / p.sc[s]; a.stype[s] = p.scalar_type[s]; }
+    for (int s = 0; s < p.n_scalars; s++) { a.pe[s] = p.nu / p.sc[s]; a.stype[s] = p.scalar_type[s]; }
+    if (dlm) {
+        // k_sgs: Schmidt number one (m_les.f90:372-391), no mean-gradient source
+        a.pe[p.n_scalars] = p.nu / 1.0;
+        a.stype[p.n_scalars] = -1;
+    }
 
     MARK(7);
+    if constexpr (std::is_same<T, double>::value) {
+        if (dlm) {
+            // nu_t from k_sgs truncated to |k| <= kmax, clipped at zero; the clipped
+            // field replaces the state when its minimum is negative
+            // (les_get_turb_visc_dlm, m_les.f90:1313-1388)
+            MARK(6);
+            const int kf = nprod + 10, nutf = nprod + 11;
+            double2 *K = c->U + 3 * c->fs64;
+            c->k2max = (double)c->kmax * (double)c->kmax;
+            H3D_TRY(zinv<T>(c, 1, PRE_TRUNC, 0, K, c->fs64, Wf(kf), wfs, wp));
+            H3D_TRY(spass<T>(c, 1, false, Wf(kf), wfs, wp, 1));
+            H3D_TRY(xc2r<T>(c, Wf(kf), wfs, wp, 1));
+            k_phys_partial<<<c->pblocks, 256, 0, c->st>>>(c->n, 2 * (int64_t)wp, 2 * wfs, 1, 2,
+                                                          reinterpret_cast<const double *>(Wf(kf)), c->d_part);
+            H3D_LAUNCH_CHECK();
+            k_phys_final<<<1, 1, 0, c->st>>>(c->pblocks, c->d_part, c->d_kmin);
+            H3D_LAUNCH_CHECK();
+            k_dlm_nut<<<pw_grid(c), 256, 0, c->st>>>(c->n, 2 * (int64_t)wp, 0.1 * c->dx,
+                                                     reinterpret_cast<double *>(Wf(kf)),
+                                                     reinterpret_cast<double *>(Wf(nutf)));
+            H3D_LAUNCH_CHECK();
+            H3D_TRY(xr2c<T>(c, Wf(kf), wfs, wp, 1));
+            H3D_TRY(spass<T>(c, 1, true, Wf(kf), wfs, wp, 1));
+            H3D_TRY(spass<T>(c, 2, true, Wf(kf), wfs, wp, 1));
+            k_dlm_commit<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->d_kmin + 2,
+                                                        reinterpret_cast<const double2 *>(Wf(kf)), K);
+            H3D_LAUNCH_CHECK();
+            MARK(7);
+        }
+    }
     if (p.flow_type == 1) {
         k_forcing_energy<<<1, 32, 0, c->st>>>(c->n, c->P64, c->fs64, p.kfmax, c->U, c->d_fen);
         H3D_LAUNCH_CHECK();
@@ -537,6 +574,34 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
             H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, 6));
             tau = Wf(t0);
         }
+        const cx<T> *les_src = nullptr, *les_flux = nullptr;
+        if constexpr (std::is_same<T, double>::value) {
+            if (dlm) {
+                // dynamic localization model: tau = -2 nu_t S for the velocities, and
+                // for k_sgs the production 2 nu_t S:S, the dissipation k^(3/2)/Delta
+                // and the turbulent fluxes nu_t dk/dx_i (m_les.f90:902-1018,
+                // 1422-1621, 1041-1091), all from the physical fields of this state
+                MARK(6);
+                const int t0 = nprod;
+                H3D_TRY(zinv<T>(c, 3, PRE_STRAIN_A, 0, c->U, c->fs64, Wf(t0), wfs, wp));
+                H3D_TRY(zinv<T>(c, 3, PRE_STRAIN_B, 0, c->U, c->fs64, Wf(t0 + 3), wfs, wp));
+                H3D_TRY(zinv<T>(c, 1, PRE_CUBE, 0, c->U + 3 * c->fs64, c->fs64, Wf(t0 + 6), wfs, wp));
+                H3D_TRY(zinv<T>(c, 3, PRE_GRAD, 3, c->U, c->fs64, Wf(t0 + 7), wfs, wp));
+                H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, 10));
+                H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, 10));
+                k_dlm_phys<<<pw_grid(c), 256, 0, c->st>>>(
+                    c->n, 2 * (int64_t)wp, 2 * wfs, c->dx, reinterpret_cast<const double *>(Wf(nprod + 11)),
+                    reinterpret_cast<double *>(Wf(t0)), reinterpret_cast<double *>(Wf(t0 + 6)),
+                    reinterpret_cast<double *>(Wf(t0 + 7)));
+                H3D_LAUNCH_CHECK();
+                H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, 10));
+                H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, 10));
+                H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, 10));
+                tau = Wf(t0);
+                les_src = Wf(t0 + 6);
+                les_flux = Wf(t0 + 7);
+            }
+        }
         if (les_mlp) {
             MARK(6);
             // learned closure: the nine velocity gradients in physical space, the
@@ -557,8 +622,10 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
         MARK(5);
         if (p.dealias == 0) {
             for (int s = 0; s < ns; s++) {
+                const bool kles = dlm && s == p.n_scalars;
                 k_scalar<T><<<pw_grid(c), 256, 0, c->st>>>(a, 0, s, c->dx, Wf(6 + 3 * s), nullptr, c->U,
-                                                            c->U + (3 + s) * c->fs64, c->RO + (3 + s) * c->fs64);
+                                                            c->U + (3 + s) * c->fs64, c->RO + (3 + s) * c->fs64,
+                                                            kles ? les_src : nullptr, kles ? les_flux : nullptr);
                 H3D_LAUNCH_CHECK();
             }
             k_update_vel_23<T><<<pw_grid(c), 256, 0, c->st>>>(a, Wf(0), tau, c->U, c->RO);
@@ -644,9 +711,11 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     if (p->dealias != 0 && p->dealias != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: wrong dealias flag");
     if (p->flow_type == 1 && p->force_type != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: WRONG FORCE TYPE");
     if (p->flow_type == 1 && (p->kfmax < 1 || p->kfmax > 15)) return h3d_set_error_msg(-1, "hit3d_gpu_init: kfmax must be in 1..15");
-    if (p->les_model != 0 && p->les_model != 1 && p->les_model != HIT3D_LES_LEARNED)
-        return h3d_set_error_msg(-1, "hit3d_gpu_init: les_model must be 0 (none), 1 (Smagorinsky) or 20 (learned closure); "
-                                     "the reference's models 2-10 are not supported");
+    if (p->les_model != 0 && p->les_model != 1 && p->les_model != 2 && p->les_model != HIT3D_LES_LEARNED)
+        return h3d_set_error_msg(-1, "hit3d_gpu_init: les_model must be 0 (none), 1 (Smagorinsky), 2 (dynamic "
+                                     "localization) or 20 (learned closure); the reference's models 3-10 are not supported");
+    if (p->les_model == 2 && p->precision != 0)
+        return h3d_set_error_msg(-1, "hit3d_gpu_init: the dynamic localization model (les_model 2) runs with FP64 transforms");
     if (p->les_model != 0 && p->n_scalars > 0) return h3d_set_error_msg(-1, "hit3d_gpu_init: LES with scalars is not supported");
     if (p->precision != 0 && p->precision != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: precision must be 0 or 1");
     for (int s = 0; s < p->n_scalars; s++) {
@@ -665,12 +734,14 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     c->P32 = (int)round_up(c->nh, 16);
     c->fs64 = (int64_t)c->n * c->n * c->P64;
     c->fs32 = (int64_t)c->n * c->n * c->P32;
-    c->nsc = p->n_scalars;
+    // transported fields beyond velocity: passive scalars, then k_sgs of the
+    // dynamic localization model (m_les.f90:111-123, n_les = 1)
+    c->nsc = p->n_scalars + (p->les_model == 2 ? 1 : 0);
     c->kmax = c->p.dealias == 0 ? c->n / 3 : (int)floor((double)c->n / 3.0 * sqrt(2.0));
     c->dx = 2.0 * (4.0 * atan(1.0)) / (double)c->n;
     c->int_scalars = c->nsc > 0;
     c->xcfg = 4;  // register-resident fused x pass, the tuner's usual pick
-    c->prune_on = 1;
+    c->prune_on = p->les_model != 2;  // a clipped k_sgs brings modes beyond N/3 into the state
     c->kc_active = -1;
     cudaDeviceProp prop;
     H3D_CHECK(cudaGetDeviceProperties(&prop, c->dev));
@@ -679,7 +750,8 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     int rc = 0;
     const int nf = 3 + c->nsc;
     const size_t f64 = (size_t)c->fs64 * sizeof(double2);
-    c->nw = 6 + 3 * c->nsc + (c->p.les_model == 1 ? 6 : c->p.les_model == HIT3D_LES_LEARNED ? 9 : 0);
+    c->nw = 6 + 3 * c->nsc +
+            (c->p.les_model == 1 ? 6 : c->p.les_model == HIT3D_LES_LEARNED ? 9 : c->p.les_model == 2 ? 12 : 0);
     if (c->p.precision == 0) {
         c->wpitch = c->P64;
         c->wfs = c->fs64;
@@ -726,6 +798,13 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     H3D_CHECK(cudaMemset(c->U, 0, f64 * nf));
     H3D_CHECK(cudaMemset(c->RO, 0, f64 * nf));
     H3D_CHECK(cudaMemset(c->W, 0, wbytes));
+    if (c->p.les_model == 2) {
+        if ((rc = ctx_alloc((void **)&c->d_kmin, sizeof(double) * 4))) { hit3d_gpu_finalize(c); return rc; }
+        // m_les_dlm_k_init (m_les.f90:1394-1413): k_sgs = 0.1 in physical space, so
+        // only the (0,0,0) mode, 0.1 N^3 after the unnormalised transform
+        const double2 k0 = make_double2(0.1 * (double)c->n * (double)c->n * (double)c->n, 0.0);
+        H3D_CHECK(cudaMemcpy(c->U + 3 * c->fs64, &k0, sizeof k0, cudaMemcpyHostToDevice));
+    }
     *out = c;
     return 0;
 }
@@ -738,7 +817,7 @@ extern "C" void hit3d_gpu_finalize(hit3d_ctx *c)
     if (c->W64 && c->W64 != c->W) cudaFree(c->W64);
     void *ptrs[] = {c->U, c->RO, c->RP, c->SP, c->W, c->phys, c->tw64, c->tw32, c->d_fen, c->d_part,
                     c->d_red, c->d_ratio, c->d_cmax, c->stage, c->d_xyz, c->d_uvw, c->sgs, c->mlp_wb,
-                    c->d_mlp_err};
+                    c->d_mlp_err, c->d_kmin};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
@@ -963,7 +1042,8 @@ extern "C" int hit3d_gpu_set_dt(hit3d_ctx *c, double dt)
 extern "C" int hit3d_gpu_set_scalars_active(hit3d_ctx *c, int32_t on)
 {
     if (!c) return h3d_set_error_msg(-1, "null context");
-    c->int_scalars = (on != 0) && c->nsc > 0;
+    // k_sgs of the dynamic localization model is always transported (rhs_scalars.f90:72-74)
+    c->int_scalars = ((on != 0) && c->nsc > 0) || c->p.les_model == 2;
     return 0;
 }
 
@@ -971,7 +1051,8 @@ extern "C" int hit3d_gpu_dealias_all(hit3d_ctx *c)
 {
     if (!c) return h3d_set_error_msg(-1, "null context");
     H3D_CHECK(cudaSetDevice(c->dev));
-    k_dealias_all<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->fs64, 3 + c->nsc, c->kmax, c->U);
+    // velocity and passive scalars (dealias_all.f90:27), not k_sgs
+    k_dealias_all<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->fs64, 3 + c->p.n_scalars, c->kmax, c->U);
     H3D_LAUNCH_CHECK();
     H3D_CHECK(cudaStreamSynchronize(c->st));
     c->alias_known = 0;

@@ -60,6 +60,7 @@ enum PreMode : int {
     PRE_STRAIN_B = 5,  // S22, S23, S33 for f = 0,1,2            (m_les.f90:1180-1198)
     PRE_GRAD = 6,      // d phi/dx_f of state field `sfield`     (m_stats.f90:323-326)
     PRE_TRUNC = 7,     // field f with |k|^2 > k2max zeroed       (io_write_4.f90:21-42)
+    PRE_CUBE = 8,      // field f with some |k_i| > N/3 zeroed    (m_les.f90:1579-1586)
 };
 
 // MODE is a compile-time PreMode so that the plain copy carries no per-element
@@ -126,6 +127,11 @@ template <typename T, typename TO, int MODE> struct IOSpec {
         case PRE_TRUNC: {
             const double k2 = kx * kx + ky * ky + kz * kz;
             r = k2 > k2max ? make_double2(0.0, 0.0) : U(f, o, c, p);
+            break;
+        }
+        case PRE_CUBE: {
+            const double k3 = (double)(n / 3);
+            r = (fabs(kx) > k3 || fabs(ky) > k3 || fabs(kz) > k3) ? make_double2(0.0, 0.0) : U(f, o, c, p);
             break;
         }
         default: r = U(f, o, c, p);

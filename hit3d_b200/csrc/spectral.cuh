@@ -253,9 +253,13 @@ __global__ void k_update_vel_ps2(const StepArgs a, double dx, const cx<TP> *__re
 // The uniform-gradient source -u is added over all modes for type 0 scalars
 // (rhs_scalars.f90:387-389).
 template <typename TP>
+// LS, LF (optional, dynamic localization model): spectra of the k_sgs source
+// 2 nu_t S:S - k^(3/2)/Delta and of the three fluxes nu_t dk/dx_i, added to the
+// RHS where ialias == 0 as LS + i k . LF (m_les.f90:1540-1546, 1609-1615, 1080-1086)
 __global__ void k_scalar(const StepArgs a, int mode, int s, double dx, const cx<TP> *__restrict__ P,
                          double2 *__restrict__ SP, const double2 *__restrict__ Uvel, double2 *__restrict__ PHI,
-                         double2 *__restrict__ RO)
+                         double2 *__restrict__ RO, const cx<TP> *__restrict__ LS = nullptr,
+                         const cx<TP> *__restrict__ LF = nullptr)
 {
     const int kc = mode == 0 ? a.kc : -1;
     const int64_t nm = mode_count(a.n, a.nh, kc);
@@ -306,6 +310,12 @@ __global__ void k_scalar(const StepArgs a, int mode, int s, double dx, const cx<
             double2 u = Uvel[o];
             r.x = r.x - u.x;
             r.y = r.y - u.y;
+        }
+        if (LS != nullptr && m.ialias == 0) {
+            const double2 sv = ld2<TP>(LS, po), f1 = ld2<TP>(LF, po), f2 = ld2<TP>(LF, po + a.pfs),
+                          f3 = ld2<TP>(LF, po + 2 * a.pfs);
+            r.x = r.x + sv.x - (kx * f1.y + ky * f2.y + kz * f3.y);
+            r.y = r.y + sv.y + (kx * f1.x + ky * f2.x + kz * f3.x);
         }
         double2 ro = RO[o];
         ab2(phi, ro, r, a.dt, a.euler_s);
@@ -508,6 +518,66 @@ __global__ void k_phys_final(int nblk, const double *__restrict__ part, double *
         a2 = fmin(a2, part[b * 4 + 2]); a3 = fmax(a3, part[b * 4 + 3]);
     }
     out[0] = a0; out[1] = a1; out[2] = a2; out[3] = a3;
+}
+
+// ---------------------------------------------------------------------------
+// dynamic localization model (m_les.f90:1313-1621, 1041-1091)
+// ---------------------------------------------------------------------------
+// nu_t = C_k Delta sqrt(k) from the truncated k_sgs in physical space, with k
+// clipped at zero in place (les_get_turb_visc_dlm, m_les.f90:1313-1388: the
+// reference clips only when the minimum is negative, which gives the same
+// values).  coef = C_k Delta.
+__global__ void k_dlm_nut(int n, int64_t rp, double coef, double *__restrict__ K, double *__restrict__ NUT)
+{
+    const int64_t np = (int64_t)n * n * n;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / n, o = row * rp + (t - row * n);
+        const double k = K[o] > 0.0 ? K[o] : 0.0;
+        K[o] = k;
+        NUT[o] = coef * sqrt(k);
+    }
+}
+
+// the clipped k_sgs W replaces the state field when the minimum was negative
+__global__ void k_dlm_commit(int n, int nh, int pitch, const double *__restrict__ kmin,
+                             const double2 *__restrict__ W, double2 *__restrict__ U)
+{
+    if (!(*kmin < 0.0)) return;
+    const int64_t nm = (int64_t)n * n * nh;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / nh, o = row * pitch + (t - row * nh);
+        U[o] = W[o];
+    }
+}
+
+// physical-space terms, in place, on rows of pitch rp (reals), fields fs reals apart:
+//   S[0..6) (S11 S12 S13 S22 S23 S33) -> tau_ij = -2 nu_t S_ij      (m_les.f90:902-1018)
+//   KC (k_sgs with the 2/3 rule)      -> 2 nu_t S_ij S_ij - max(KC,0)^1.5 / Delta
+//                                                                    (m_les.f90:1422-1621)
+//   G[0..3) (dk/dx_i)                 -> nu_t dk/dx_i                (m_les.f90:1041-1091)
+__global__ void k_dlm_phys(int n, int64_t rp, int64_t fs, double delta, const double *__restrict__ NUT,
+                           double *__restrict__ S, double *__restrict__ KC, double *__restrict__ G)
+{
+    const int64_t np = (int64_t)n * n * n;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / n, o = row * rp + (t - row * n);
+        const double nut = NUT[o];
+        double sv[6];
+#pragma unroll
+        for (int c = 0; c < 6; c++) sv[c] = S[o + c * fs];
+        double ss = sv[0] * sv[0];
+        ss = ss + 2.0 * (sv[1] * sv[1]);
+        ss = ss + 2.0 * (sv[2] * sv[2]);
+        ss = ss + sv[3] * sv[3];
+        ss = ss + 2.0 * (sv[4] * sv[4]);
+        ss = ss + sv[5] * sv[5];
+        const double kc = KC[o] > 0.0 ? KC[o] : 0.0;
+        KC[o] = (2.0 * ss) * nut - pow(kc, 1.5) / delta;
+#pragma unroll
+        for (int c = 0; c < 6; c++) S[o + c * fs] = (-2.0 * nut) * sv[c];
+#pragma unroll
+        for (int d = 0; d < 3; d++) G[o + d * fs] = G[o + d * fs] * nut;
+    }
 }
 
 // initial velocity: solenoidal curl of the transformed Gaussian noise G restricted

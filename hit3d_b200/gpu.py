@@ -176,7 +176,8 @@ class Context:
     def __init__(self, params: Params, _handle: C.c_void_p | None = None):
         self.params = params
         self.n = params.nx
-        self.nfields = 3 + params.n_scalars
+        # k_sgs of the dynamic localization model is state field 3 + n_scalars
+        self.nfields = 3 + params.n_scalars + (1 if params.les_model == 2 else 0)
         self.kmax = params.kmax
         self._owned = _handle is None
         if _handle is None:

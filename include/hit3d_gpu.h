@@ -47,9 +47,11 @@ typedef struct hit3d_params {
     int32_t n_scalars;   /* passive scalars, <= HIT3D_MAX_SCALARS (m_parameters.f90:424)   */
     int32_t precision;   /* 0: FP64 transforms; 1: FP32 nonlinear-term transforms with FP64
                             state, integrator and reductions (no reference counterpart)    */
-    int32_t les_model;   /* 0: none; 1: Smagorinsky (m_les.f90:94-106); HIT3D_LES_LEARNED (20):
-                            learned closure (hit3d_gpu_les_set_mlp; no reference
-                            counterpart).  The reference's models 2-10 are rejected.       */
+    int32_t les_model;   /* 0: none; 1: Smagorinsky (m_les.f90:94-106); 2: dynamic localization
+                            model (m_les.f90:111-123), with k_sgs as state field 3+n_scalars,
+                            FP64 only, no passive scalars; HIT3D_LES_LEARNED (20): learned
+                            closure (hit3d_gpu_les_set_mlp; no reference counterpart).
+                            The reference's models 3-10 are rejected.                      */
     int32_t scalar_type[HIT3D_MAX_SCALARS]; /* 0 = uniform mean gradient source            */
     int32_t device;      /* CUDA device ordinal                                            */
     int32_t reserved;

@@ -138,15 +138,16 @@ class Oracle:
         if not self._p:
             raise MemoryError("oracle_create failed")
         self.n, self.nscal = n, nscal
+        self.nles = 1 if les_model == 2 else 0   # k_sgs of the dynamic localization model
         self.nu = nu
         self.kmax = L.oracle_kmax(self._p)
         self.fsz = (n + 2) * n * n
-        nf = 3 + nscal
+        nf = 3 + nscal + self.nles
         self.fields = np.ctypeslib.as_array(L.oracle_fields(self._p), shape=(nf * self.fsz,)).reshape(
             nf, n, n, n + 2)
         self.rhs_old = np.ctypeslib.as_array(L.oracle_rhs_old(self._p), shape=(nf * self.fsz,)).reshape(
             nf, n, n, n + 2)
-        nw = max(7, 6 + nscal)
+        nw = max(7, 6 + nscal + self.nles)
         self.wrk = np.ctypeslib.as_array(L.oracle_wrk(self._p), shape=(nw * self.fsz,)).reshape(
             nw, n, n, n + 2)
 

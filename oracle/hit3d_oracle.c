@@ -201,10 +201,10 @@ void oracle_fft1d(int n, double *x, int sign)
 /*  Oracle state: module globals of m_fields / m_work / x_fftw / m_force.    */
 /* ------------------------------------------------------------------------- */
 typedef struct {
-    int n, nscal, dealias, flow_type, force_type, kfmax, kmax, les_model, nwrk;
+    int n, nscal, nles, dealias, flow_type, force_type, kfmax, kmax, les_model, nwrk;
     int isp_type;
     double nu, dt, famp, dx, c_smag, les_delta, peak_wavenum, ir_exp;
-    double pe[MAXS];
+    double pe[MAXS + 1];
     int scalar_type[MAXS];
     size_t fsz;               /* (n+2)*n*n */
     double *fields, *rhs_old, *wrk, *turb_visc;
@@ -393,15 +393,20 @@ oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_
     o->les_model = les_model; o->c_smag = c_smag;
     o->dx = 2.0 * (4.0 * atan(1.0)) / (double)n;
     o->les_delta = o->dx;
+    /* LES-related transported quantities: k_sgs for the DLM (m_les.f90:111-123),
+     * with Schmidt number one (m_les.f90:372-391) */
+    o->nles = les_model == 2 ? 1 : 0;
+    if (o->nles && nscal > 0) { free(o); return NULL; }
     /* kmax (m_parameters.f90:123-131) */
     if (dealias == 0) o->kmax = n / 3;
     else o->kmax = (int)floor((double)n / 3.0 * sqrt(2.0));
     for (int s = 0; s < nscal; s++) { o->pe[s] = nu / sc[s]; o->scalar_type[s] = scalar_type[s]; }
+    if (o->nles) o->pe[nscal] = nu / 1.0;
     o->fsz = (size_t)(n + 2) * n * n;
     o->nwrk = 7;
-    if (5 + nscal + 1 > o->nwrk) o->nwrk = 5 + nscal + 1;
-    o->fields = (double *)calloc(o->fsz * (3 + nscal), sizeof(double));
-    o->rhs_old = (double *)calloc(o->fsz * (3 + nscal), sizeof(double));
+    if (6 + nscal + o->nles > o->nwrk) o->nwrk = 6 + nscal + o->nles;
+    o->fields = (double *)calloc(o->fsz * (3 + nscal + o->nles), sizeof(double));
+    o->rhs_old = (double *)calloc(o->fsz * (3 + nscal + o->nles), sizeof(double));
     o->wrk = (double *)calloc(o->fsz * o->nwrk, sizeof(double));
     if (les_model) o->turb_visc = (double *)calloc(o->fsz, sizeof(double));
     if (!o->fields || !o->rhs_old || !o->wrk) return NULL;
@@ -438,6 +443,9 @@ oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_
         o->nfn = cnt;
     }
     o->fov = 1; o->fos = 1; o->int_scalars = nscal > 0;
+    /* m_les_dlm_k_init (m_les.f90:1394-1413): k_sgs = 0.1 in physical space,
+     * i.e. only the (0,0,0) mode, 0.1 N^3 after the unnormalised transform */
+    if (o->nles) F(o, 3 + nscal)[0] = 0.1 * (double)n * (double)n * (double)n;
     return o;
 }
 
@@ -591,6 +599,172 @@ static void les_rhs_velocity(oracle_t *o)
 }
 
 /* ------------------------------------------------------------------------- */
+/*  Dynamic localization model (les_model 2)                                  */
+/* ------------------------------------------------------------------------- */
+static void copy_field(oracle_t *o, double *dst, const double *src);
+
+/* les_get_turb_visc_dlm (m_les.f90:1313-1388): nu_t = C_k Delta sqrt(k_sgs)
+ * from k_sgs truncated to |k|^2 <= kmax^2; if k_sgs < 0 anywhere, the clipped
+ * field replaces the state. */
+static void les_get_turb_visc_dlm(oracle_t *o)
+{
+    int n = o->n, nk = 3 + o->nscal;
+    const double C_k = 0.1;
+    double *w0 = W(o, 0), *tv = o->turb_visc;
+    copy_field(o, w0, F(o, nk));
+    const double rkmax2 = (double)(o->kmax * o->kmax);
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 2; i++) {
+                double wmag2 = o->akx[i] * o->akx[i] + o->aky[k] * o->aky[k] + o->akz[j] * o->akz[j];
+                if (wmag2 > rkmax2) w0[IX(o, i, j, k)] = 0.0;
+            }
+    xfft3d(o, -1, w0);
+    double mn = w0[0];
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                double v = w0[IX(o, i, j, k)];
+                if (v < mn) mn = v;
+            }
+    if (mn < 0.0)
+        for (size_t q = 0; q < o->fsz; q++) w0[q] = w0[q] > 0.0 ? w0[q] : 0.0;
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                size_t a = IX(o, i, j, k);
+                tv[a] = C_k * o->les_delta * sqrt(w0[a]);
+            }
+    if (mn < 0.0) {
+        xfft3d(o, 1, w0);
+        copy_field(o, F(o, nk), w0);
+    }
+}
+
+/* m_les_k_src_dlm (m_les.f90:1422-1561): production 2 nu_t S_ij S_ij of
+ * k_sgs, added to its RHS where ialias == 0.  The strain components are taken
+ * where ialias == 0 and zero elsewhere.  (The reference zeroes its two work
+ * arrays only before the first of the three passes, so from the second pass on
+ * their aliased entries still hold the previous pass's physical values; that
+ * content depends on what the transform library leaves in the row padding and
+ * cannot be reproduced.  Every pass starts from zero here.) */
+static void strain_pair(oracle_t *o, int pass, double *s1, double *s2)
+{
+    int n = o->n;
+    double *u = F(o, 0), *v = F(o, 1), *w = F(o, 2);
+    const double half = 0.5;
+    memset(s1, 0, sizeof(double) * o->fsz);
+    memset(s2, 0, sizeof(double) * o->fsz);
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n + 1; i += 2) {
+                size_t a = IX(o, i, j, k), b = a + 1;
+                if (o->ialias[a] != 0) continue;
+                double kx0 = o->akx[i], kx1 = o->akx[i + 1], ky = o->aky[k], kz = o->akz[j];
+                if (pass == 0) {
+                    s1[a] = -kx1 * u[b];  s1[b] = kx0 * u[a];                         /* S11 */
+                    s2[a] = -half * (ky * u[b] + kx1 * v[b]);                         /* S12 */
+                    s2[b] = half * (ky * u[a] + kx0 * v[a]);
+                } else if (pass == 1) {
+                    s1[a] = -half * (kz * u[b] + kx1 * w[b]);                         /* S13 */
+                    s1[b] = half * (kz * u[a] + kx0 * w[a]);
+                    s2[a] = -ky * v[b];  s2[b] = ky * v[a];                           /* S22 */
+                } else {
+                    s1[a] = -half * (kz * v[b] + ky * w[b]);                          /* S23 */
+                    s1[b] = half * (kz * v[a] + ky * w[a]);
+                    s2[a] = -kz * w[b];  s2[b] = kz * w[a];                           /* S33 */
+                }
+            }
+}
+
+static void les_k_src_dlm(oracle_t *o)
+{
+    int n1 = 3 + o->nscal + o->nles + 1, n2 = n1 + 1, kn = 3 + o->nscal + 1;
+    double *w0 = W(o, 0), *a1 = W(o, n1), *a2 = W(o, n2), *tv = o->turb_visc;
+    memset(w0, 0, sizeof(double) * o->fsz);
+    for (int pass = 0; pass < 3; pass++) {
+        strain_pair(o, pass, a1, a2);
+        xfft3d(o, -1, a1);
+        xfft3d(o, -1, a2);
+        /* S11^2 + 2 S12^2, then 2 S13^2 + S22^2, then 2 S23^2 + S33^2 */
+        const double c1 = pass == 0 ? 1.0 : 2.0, c2 = pass == 0 ? 2.0 : 1.0;
+        for (size_t q = 0; q < o->fsz; q++) {
+            double t = w0[q];
+            t = t + (pass == 0 ? a1[q] * a1[q] : c1 * (a1[q] * a1[q]));
+            t = t + (pass == 0 ? c2 * (a2[q] * a2[q]) : a2[q] * a2[q]);
+            w0[q] = t;
+        }
+    }
+    for (size_t q = 0; q < o->fsz; q++) w0[q] = 2.0 * w0[q];
+    int n = o->n;
+    for (size_t q = 0; q < o->fsz; q++) a1[q] = w0[q];
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                size_t a = IX(o, i, j, k);
+                a1[a] = a1[a] * tv[a];
+            }
+    xfft3d(o, 1, a1);
+    double *r = W(o, kn);
+    for (size_t q = 0; q < o->fsz; q++)
+        if (o->ialias[q] == 0) r[q] = r[q] + a1[q];
+}
+
+/* m_les_k_diss_algebraic (m_les.f90:1567-1621): dissipation k^(3/2)/Delta of
+ * the dealiased, clipped k_sgs, subtracted where ialias == 0 */
+static void les_k_diss_algebraic(oracle_t *o)
+{
+    int n = o->n, kn = 3 + o->nscal + 1;
+    double *w0 = W(o, 0);
+    copy_field(o, w0, F(o, kn - 1));
+    for (size_t q = 0; q < o->fsz; q++)
+        if (o->ialias[q] > 0) w0[q] = 0.0;
+    xfft3d(o, -1, w0);
+    for (size_t q = 0; q < o->fsz; q++) {
+        double v = w0[q] > 0.0 ? w0[q] : 0.0;
+        w0[q] = pow(v, 1.5) / o->les_delta;
+    }
+    xfft3d(o, 1, w0);
+    double *r = W(o, kn);
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                size_t a = IX(o, i, j, k);
+                if (o->ialias[a] == 0) r[a] = r[a] - w0[a];
+            }
+}
+
+static void derivative(oracle_t *o, const double *src, char axis, double *dst);
+
+/* m_les_rhss_turb_visc1 (m_les.f90:1041-1091): sum_i d/dx_i (nu_t d phi/dx_i)
+ * added to the RHS of field m where ialias == 0 */
+static void les_rhss_turb_visc1(oracle_t *o, int m)
+{
+    int n = o->n;
+    int t1 = 3 + o->nscal + o->nles + 1, t2 = t1 + 1;
+    double *w0 = W(o, 0), *a1 = W(o, t1), *a2 = W(o, t2), *tv = o->turb_visc;
+    copy_field(o, a1, F(o, m - 1));
+    memset(w0, 0, sizeof(double) * o->fsz);
+    const char dirs[3] = {'x', 'y', 'z'};
+    for (int d = 0; d < 3; d++) {
+        derivative(o, a1, dirs[d], a2);
+        xfft3d(o, -1, a2);
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n; i++) {
+                    size_t a = IX(o, i, j, k);
+                    a2[a] = a2[a] * tv[a];
+                }
+        xfft3d(o, 1, a2);
+        derivative(o, a2, dirs[d], a2);
+        for (size_t q = 0; q < o->fsz; q++) w0[q] = w0[q] + a2[q];
+    }
+    double *r = W(o, m);
+    for (size_t q = 0; q < o->fsz; q++)
+        if (o->ialias[q] == 0) r[q] = r[q] + w0[q];
+}
+
+/* ------------------------------------------------------------------------- */
 /*  rhs_scalars (rhs_scalars.f90:1-402)                                      */
 /* ------------------------------------------------------------------------- */
 static void phase_factors(oracle_t *o)
@@ -618,16 +792,19 @@ static void mul3(oracle_t *o, double *dst, const double *a, const double *b)
 
 static void oracle_rhs_scalars(oracle_t *o)
 {
-    int n = o->n, ns = o->nscal;
-    if (o->les_model) les_get_turb_visc_smag(o);
-    if (!o->int_scalars) {
+    int n = o->n, ns = o->nscal, nl = o->nles;
+    if (o->les_model == 1) les_get_turb_visc_smag(o);
+    if (o->les_model == 2) les_get_turb_visc_dlm(o);
+    if (!o->int_scalars && nl == 0) {
         for (int m = 0; m < 3; m++) { copy_field(o, W(o, 1 + m), F(o, m)); xfft3d(o, -1, W(o, 1 + m)); }
         return;
     }
-    for (int m = 4; m <= 3 + ns; m++) memset(W(o, m), 0, sizeof(double) * o->fsz);
+    for (int m = 4; m <= 3 + ns + nl; m++) memset(W(o, m), 0, sizeof(double) * o->fsz);
     if (o->dealias == 0) {
         for (int m = 0; m < 3; m++) { copy_field(o, W(o, 1 + m), F(o, m)); xfft3d(o, -1, W(o, 1 + m)); }
-        for (int s = 1; s <= ns; s++) {
+        /* passive scalars only once they are switched on; LES quantities always
+         * (rhs_scalars.f90:72-74) */
+        for (int s = o->int_scalars ? 1 : ns + 1; s <= ns + nl; s++) {
             copy_field(o, W(o, 0), F(o, 2 + s));
             xfft3d(o, -1, W(o, 0));
             for (int c = 1; c <= 3; c++) {
@@ -722,6 +899,12 @@ static void oracle_rhs_scalars(oracle_t *o)
             double *r = W(o, s + 3), *u = F(o, 0);
             for (size_t q = 0; q < o->fsz; q++) r[q] = r[q] - u[q];
         }
+    /* les_rhs_scalars, DLM branch (m_les.f90:714-719) */
+    if (o->les_model == 2) {
+        les_k_src_dlm(o);
+        les_k_diss_algebraic(o);
+        for (int m = 4; m <= 3 + ns + nl; m++) les_rhss_turb_visc1(o, m);
+    }
 }
 
 /* ------------------------------------------------------------------------- */
@@ -975,8 +1158,8 @@ void oracle_step(oracle_t *o, int nsteps)
 {
     for (int it = 0; it < nsteps; it++) {
         oracle_rhs_scalars(o);
-        if (o->int_scalars) {
-            int nlo = 3, nhi = 3 + o->nscal;
+        if (o->int_scalars || o->nles > 0) {
+            int nlo = 3, nhi = 3 + o->nscal + o->nles;
             double dt = o->dt;
             for (int m = nlo; m < nhi; m++) {
                 double *f = F(o, m), *r = RO(o, m), *w = W(o, m + 1);
@@ -1018,7 +1201,7 @@ void oracle_rhs(oracle_t *o)
 {
     oracle_rhs_scalars(o);
     /* rhs_velocity reuses wrk4..; save scalar RHS first */
-    int ns = o->int_scalars ? o->nscal : 0;
+    int ns = (o->int_scalars ? o->nscal : 0) + o->nles;
     double *save = NULL;
     if (ns) {
         save = (double *)malloc(sizeof(double) * o->fsz * ns);
@@ -1036,6 +1219,7 @@ void oracle_rhs(oracle_t *o)
 /* ------------------------------------------------------------------------- */
 static void derivative(oracle_t *o, const double *src, char axis, double *dst)
 {
+    /* x_derivative (x_fftw.f90:637-682); src and dst may be the same array */
     int n = o->n;
     for (int k = 0; k < n; k++)
         for (int j = 0; j < n; j++)

@@ -1,0 +1,53 @@
+"""Dynamic localization model (les_model 2, m_les.f90:111-123, 1313-1621,
+1041-1091): k_sgs transported as state field 3, nu_t = 0.1 Delta sqrt(k_sgs),
+production, dissipation and turbulent diffusion of k_sgs, -2 nu_t S in the
+velocity RHS; against the oracle, including the clipping of a negative k_sgs."""
+import numpy as np
+import pytest
+
+from _cases import make_pair, relerr
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n", [32, 48])
+def test_dlm_matches_oracle(n):
+    o, g = make_pair(n, flow_type=1, les_model=2, nu=1.0 / 2000.0, dt=0.004, isp_type=2)
+    assert g.download_fields().shape[0] == 4
+    # m_les_dlm_k_init: k_sgs = 0.1 everywhere
+    assert g.download_fields()[3, 0, 0, 0] == pytest.approx(0.1 * n ** 3, rel=1e-15)
+    for _ in range(3):
+        o.step(4)
+        g.step(4)
+        f = g.download_fields()
+        assert relerr(f[:3], o.fields[:3]) < 1e-10
+        assert relerr(f[3], o.fields[3]) < 1e-10
+    assert relerr(g.download_rhs_old(), o.rhs_old) < 1e-9
+
+
+def test_dlm_clips_negative_k_sgs_like_the_oracle():
+    n = 32
+    o, g = make_pair(n, flow_type=1, les_model=2, nu=1.0 / 2000.0, dt=0.004, isp_type=2)
+    f = g.download_fields()
+    f[3] = 0.0
+    f[3, 0, 0, 0] = 0.1 * n ** 3
+    f[3, 0, 0, 2] = 0.15 * n ** 3      # + 0.3 cos(x): k_sgs < 0 on part of the domain
+    g.upload_fields(f)
+    o.fields[:] = f
+    o.step(1)
+    g.step(1)
+    got = g.download_fields()
+    # the clipped field replaced the state: it now has modes beyond kx = 1
+    assert np.abs(got[3, 0, 0, 4:8]).max() > 1e-3 * n ** 3
+    assert relerr(got, o.fields) < 1e-10
+    o.step(5)
+    g.step(5)
+    assert relerr(g.download_fields(), o.fields) < 1e-10
+
+
+def test_dlm_rejects_what_it_does_not_support():
+    from hit3d_b200 import Context, Hit3dError, Params
+    with pytest.raises(Hit3dError, match="FP64"):
+        Context(Params(nx=32, les_model=2, precision=1))
+    with pytest.raises(Hit3dError, match="scalars"):
+        Context(Params(nx=32, les_model=2, n_scalars=1, sc=[1.0], scalar_type=[0]))

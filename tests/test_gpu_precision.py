@@ -23,7 +23,10 @@ def test_fp32_transforms_track_fp64(n, dealias):
         for c in ctx:
             c.step(25)
         (e64, s64), (e32, s32) = ctx[0].stats(), ctx[1].stats()
-        mask = e64 > 1e-12 * e64.max()
+        # shells holding more than 1e-8 of the peak: the nearly empty top shells of
+        # this initial spectrum (1e-12 of the peak at 128^3) sit at the FP32
+        # round-off floor, where a relative error says nothing
+        mask = e64 > 1e-8 * e64.max()
         assert np.max(np.abs(e32[mask] - e64[mask]) / e64[mask]) < 1e-4
         assert abs(s32["energy"] - s64["energy"]) < 1e-8 * s64["energy"]
         assert abs(s32["eps_v"] - s64["eps_v"]) < 1e-7 * s64["eps_v"]
