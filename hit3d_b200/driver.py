@@ -73,7 +73,7 @@ class Simulation:
         else:
             self.itime = c.itmin
             f, self.time, dt, nums1, _ = read_restart(
-                os.path.join(self.wd, restart_name(self.run_name, c.itmin)), c.nx, c.n_scalars)
+                os.path.join(self.wd, restart_name(self.run_name, c.itmin)), c.nx, c.n_scalars, self.n_les)
             self.ctx.upload_fields(f)
             if nums1 > 0 or c.tscalar <= self.time:
                 self.int_scalars = c.n_scalars > 0
@@ -105,11 +105,17 @@ class Simulation:
         for n, nm in enumerate(names):
             write_real4(os.path.join(self.wd, f"{nm}.{self.file_ext()}"), phys[n])
 
+    @property
+    def n_les(self) -> int:
+        """LES-related transported fields: k_sgs of the dynamic localization model."""
+        return 1 if self.cfg.les_model == 2 else 0
+
     def write_restart(self):
         nums = self.cfg.n_scalars if self.int_scalars else 0
-        f = self.ctx.download_fields(3 + nums)
-        write_restart(os.path.join(self.wd, restart_name(self.run_name, self.itime)), f, self.time, self.cfg.dt,
-                      nums)
+        f = self.ctx.download_fields(self.ctx.nfields)
+        keep = list(range(3 + nums)) + list(range(3 + self.cfg.n_scalars, 3 + self.cfg.n_scalars + self.n_les))
+        write_restart(os.path.join(self.wd, restart_name(self.run_name, self.itime)),
+                      np.ascontiguousarray(f[keep]), self.time, self.cfg.dt, nums, self.n_les)
 
     def stat_main(self):
         es, st = self.ctx.stats()

@@ -71,3 +71,27 @@ def test_stop_file_ends_the_run_with_a_restart(tmp_path):
     sim.begin()
     assert sim.run() == 3 and sim.itime == 10
     assert os.path.exists(os.path.join(wd, "decay64_.64.000010"))
+
+
+def test_dlm_run_restarts_with_k_sgs(tmp_path):
+    """The dynamic localization model through the host loop: the restart file
+    carries k_sgs (nles = 1, as restart_io.f90 writes it) and a run restarted
+    from it continues with the same state."""
+    from dataclasses import replace
+    from hit3d_b200.driver import Simulation
+    from hit3d_b200.params import read_input_file
+    from hit3d_b200.restart import read_restart
+    wd = str(tmp_path)
+    cfg = read_input_file(os.path.join(GOLDEN, "decay64_.in"))
+    cfg = replace(cfg, les_model=2, n_scalars=0, scalar_type=[], sc=[], ir_exp_sc=[], peak_wavenum_sc=[],
+                  reac_sc=[], itmax=6, iprint1=3, iprint2=3, iwrite4=100, tmax=10.0)
+    sim = Simulation("dlm64", wd, cfg=cfg)
+    sim.begin()
+    assert sim.run() == 0 and sim.itime == 6
+    f, t, dt, nums, nles = read_restart(os.path.join(wd, "dlm64.64.000006"), 64, 0, 1)
+    assert nums == 0 and nles == 1 and f.shape[0] == 4
+    g = sim.ctx.download_fields()
+    assert np.array_equal(f[..., :64], g[..., :64])
+    sim2 = Simulation("dlm64", wd, cfg=replace(cfg, itmin=6))
+    sim2.begin()
+    assert np.array_equal(sim2.ctx.download_fields()[..., :64], g[..., :64])
