@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--les-full", action="store_true",
                     help="a-posteriori test at 512^3 DNS -> 128^3 LES (minutes) instead of 128^3 -> 32^3")
     ap.add_argument("--les-only", action="store_true", help="only the learned-LES step rates (profiling runs)")
+    ap.add_argument("--no-configs", action="store_true", help="skip the step rates of the other configurations")
+    ap.add_argument("--configs-only", action="store_true", help="only the step rates of the other configurations")
     ap.add_argument("--cmp-every", type=int, default=50, help="FP32 vs FP64 statistics every this many steps")
     ap.add_argument("--cmp-points", type=int, default=4)
     ap.add_argument("--variant", type=int, default=-1,
@@ -282,6 +284,80 @@ def les_leg(torch, args, dns_rate, dns32_rate, device):
     return out
 
 
+def configs_leg(torch, args, device):
+    """Step rates of the other configurations of the path (the per-configuration
+    parity lives in tests/): 64^3 decaying; 256^3 forced with phase-shift
+    dealiasing, two scalars and 10^6 CINT particles; the batched 96-run set;
+    128^3 LES with each closure."""
+    from hit3d_b200 import Context, Params
+    from hit3d_b200.batch import Batch, batched_runs
+    out = {}
+
+    def rate(c, steps):
+        c.init_velocity(RN1, 2, 4.0, 2.0)
+        c.dealias_all()
+        if args.variant >= 0:
+            c.set_variant(args.variant)
+        else:
+            c.autotune()
+        c.step(args.warmup)
+        t = timed_steps(torch, c, steps)
+        return steps / t
+
+    c = Context(Params(nx=64, dealias=0, flow_type=0, nu=1.0 / 400.0, dt=0.005, device=device))
+    r = rate(c, 100)
+    out["decaying_64"] = {"workload": "decaying DNS 64^3, Re=400, dt=0.005, 2/3 rule", "steps_per_s": r,
+                          "grid_points_steps_per_s": r * 64 ** 3}
+    c.close()
+
+    n = 256
+    c = Context(Params(nx=n, dealias=1, flow_type=1, force_type=1, kfmax=2, famp=0.5, nu=1.0 / 1000.0, dt=0.001,
+                       n_scalars=2, sc=[0.7, 1.0], scalar_type=[0, 0], device=device))
+    c.set_scalars_active(True)
+    # 100^3 = 10^6 particles on the reference's lattice of cell centres, in its
+    # 1-based grid units (m_particles.f90:220-262, 314-319)
+    g = (np.arange(100) + 0.5) * n / 100.0 + 1.0
+    Z, Y, X = np.meshgrid(g, g, g, indexing="ij")
+    c.particles_upload(np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1), None, scheme=1)
+    r = rate(c, 20)
+    out["forced_256_phase_shift_2_scalars_1e6_particles"] = {
+        "workload": "forced DNS 256^3, Re=1000, dt=0.001, phase shift, 2 scalars (Sc 0.7, 1.0), 10^6 CINT particles",
+        "steps_per_s": r, "grid_points_steps_per_s": r * n ** 3}
+    c.close()
+
+    ps = batched_runs()
+    b = Batch(ps)
+    b.init()
+    b.step(args.warmup + 1, graph_steps=10)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.step(50, graph_steps=10)
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    pts = sum(p.nx ** 3 for p in ps)
+    out["batched_96_runs"] = {"workload": "96 forced runs: 32 x 32^3, 32 x 48^3, 28 x 64^3, 4 x 128^3, one recorded graph",
+                              "run_steps_per_s": len(ps) * 50 / t, "grid_points_steps_per_s": pts * 50 / t,
+                              "graph_launches": b.graph_launches, "timing": "host clock around 50 steps (5 graph launches)"}
+    b.close()
+
+    les = {}
+    nparam = None
+    for name, model in (("smagorinsky", 1), ("dynamic_localization", 2), ("learned", 20)):
+        c = Context(Params(nx=128, dealias=0, flow_type=1, force_type=1, kfmax=2, famp=0.5, nu=1.0 / 6000.0,
+                           dt=0.002, les_model=model, device=device))
+        if model == 20:
+            from hit3d_b200 import gpu
+            nparam = int(gpu.lib().hit3d_mlp_nparam())
+            w = np.zeros(nparam, dtype=np.float32)
+            w[nparam - 5] = -2.0 * 0.18 ** 2 / 4.0
+            bits = ((w.view(np.uint32).astype(np.uint64) + 0x7FFF + ((w.view(np.uint32) >> 16) & 1)) >> 16).astype(np.uint16)
+            c.les_set_mlp(bits, 2 * 2.0 * np.pi / 128, clip=True, kernel=1)
+        les[name] = rate(c, 50)
+        c.close()
+    out["les_128"] = {"workload": "LES 128^3, Re=6000, 2/3 rule", "steps_per_s": les}
+    return out
+
+
 def run_reference(args):
     rank, world, _ = dist_info()
     if rank != 0:
@@ -307,6 +383,9 @@ def main():
     torch.cuda.set_device(local)
     if args.les_only:
         print(json.dumps({"learned_les": les_leg(torch, args, None, None, local)}), flush=True)
+        return
+    if args.configs_only:
+        print(json.dumps({"other_configs": configs_leg(torch, args, local)}), flush=True)
         return
     dist = None
     if world > 1:
@@ -385,6 +464,18 @@ def main():
                "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps}
         del out
 
+    # the FP64 trajectory for the per-statistic comparison, recorded before the
+    # FP32 context is created so that only one context is resident at a time
+    # (1024^3 does not hold both)
+    ref_traj = []
+    if not args.no_fp32:
+        ctx.upload_fields(fields0)
+        ctx.fov = ctx.fos = 1
+        for k in range(args.cmp_points):
+            ctx.step(args.cmp_every)
+            ref_traj.append(ctx.stats())
+    ctx.close()
+
     # FP32 nonlinear-term transforms, same initial state and step count
     fp32 = None
     if not args.no_fp32:
@@ -413,14 +504,11 @@ def main():
                 "stage_ms": {k: round(v / 3, 3) for k, v in prof32.items() if v > 0},
                 "tuned_variant": v32, "variant_ms": [round(x, 3) for x in v32_ms]}
         # error per statistic against the FP64 path every cmp_every steps from the same state
-        ctx.upload_fields(fields0)
         c32.upload_fields(fields0)
-        ctx.fov = ctx.fos = c32.fov = c32.fos = 1
+        c32.fov = c32.fos = 1
         cmp = []
-        for k in range(args.cmp_points):
-            ctx.step(args.cmp_every)
+        for k, (e64, s64) in enumerate(ref_traj):
             c32.step(args.cmp_every)
-            e64, s64 = ctx.stats()
             e32, s32 = c32.stats()
             mk = e64 > 1e-12 * e64.max()
             cmp.append({"step": (k + 1) * args.cmp_every,
@@ -430,13 +518,18 @@ def main():
                         "skew_abs_err": abs(s32["skewness"] - s64["skewness"]),
                         "courant": c32.courant})
         fp32["vs_fp64_every_%d_steps" % args.cmp_every] = cmp
-        fp32["ek_max_rel_err_over_run"] = max(c["ek_max_rel_err"] for c in cmp)
+        fp32["ek_max_rel_err_over_run"] = max(c["ek_max_rel_err"] for c in cmp) if cmp else None
         c32.close()
-    ctx.close()
 
     les = None
     if not args.no_les and world == 1:
         les = les_leg(torch, args, value, fp32["value"] if fp32 else None, local)
+    configs = None
+    if not args.no_configs and world == 1:
+        try:
+            configs = configs_leg(torch, args, local)
+        except Exception as e:  # reported, never fatal to the bench line
+            configs = {"error": str(e)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -471,6 +564,7 @@ def main():
             "e2e": e2e,
             "fp32_fft": fp32,
             "learned_les": les,
+            "other_configs": configs,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
