@@ -79,8 +79,9 @@ template <typename T, int L, int V> struct RowCfgV {
     static constexpr size_t SMEM = (size_t)Lay<L, TC, true>::elems * sizeof(cx<T>);
 };
 //   4: register-resident kernel (k_xfused_reg), 1024/L pairs x 128 threads
-//   5, 6: lockstep kernel (k_xfused_ms), forward transforms in groups of 3 / 2
-constexpr int kFusedVariants = 7;
+//   5, 6, 7: lockstep kernel (k_xfused_ms), forward transforms in groups of 3 / 2 / 1,
+//            the last with registers capped for 3 (FP64) or 4 (FP32) CTAs per SM
+constexpr int kFusedVariants = 8;
 
 // Raise a kernel's dynamic shared-memory limit once per kernel and device, so
 // that steps recorded into a CUDA graph later make no attribute calls.
@@ -328,11 +329,12 @@ template <typename T, template <class> class OP, int L> static int xfused_reg_L(
     H3D_LAUNCH_CHECK();
     return 0;
 }
-template <typename T, template <class> class OP, int L, int GF> static int xfused_ms_L(hit3d_ctx *c, FusedArgs a)
+template <typename T, template <class> class OP, int L, int GF, int MINB = 1>
+static int xfused_ms_L(hit3d_ctx *c, FusedArgs a)
 {
     using RC = RowCfg<T, L>;
     constexpr int NB = OP<T>::NIN > GF ? OP<T>::NIN : GF;  // shared-memory buffers
-    auto k = k_xfused_ms<T, L, RC::TC, RC::NT, T, OP<T>, GF>;
+    auto k = k_xfused_ms<T, L, RC::TC, RC::NT, T, OP<T>, GF, MINB>;
     H3D_TRY(set_smem(k, NB * RC::SMEM));
     k<<<dim3((a.npairs + RC::TC - 1) / RC::TC), RC::NT, NB * RC::SMEM, c->st>>>(a, twid<T>(c));
     H3D_LAUNCH_CHECK();
@@ -343,6 +345,7 @@ template <typename T, template <class> class OP, int L> static int xfused_L(hit3
     if constexpr (OP<T>::NIN <= 3) {
         if (c->xcfg == 5) return xfused_ms_L<T, OP, L, 3>(c, a);
         if (c->xcfg == 6) return xfused_ms_L<T, OP, L, 2>(c, a);
+        if (c->xcfg == 7) return xfused_ms_L<T, OP, L, 1, sizeof(T) == 4 ? 4 : 3>(c, a);
     }
     if (c->xcfg >= 4) return xfused_reg_L<T, OP, L>(c, a);
     if constexpr (L >= 128) {

@@ -538,8 +538,9 @@ __global__ void __launch_bounds__(NT) k_xfused_reg(const FusedArgs a, const cx<T
 // butterfly) and the NOUT forward transforms in groups of GF, each transform
 // with its own shared-memory buffer.  More independent work between barriers
 // than k_xfused_reg at the same register budget per transform; the tuner picks.
-template <typename T, int L, int TC, int NT, typename TS, class OP, int GF>
-__global__ void __launch_bounds__(NT) k_xfused_ms(const FusedArgs a, const cx<T> *__restrict__ tw)
+// MINB > 1 caps the registers so that MINB CTAs share an SM.
+template <typename T, int L, int TC, int NT, typename TS, class OP, int GF, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) k_xfused_ms(const FusedArgs a, const cx<T> *__restrict__ tw)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);

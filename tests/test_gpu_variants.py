@@ -19,7 +19,7 @@ def test_variants_agree(n, precision, case):
     else:
         kw.update(les_model=1)
     outs = []
-    for v in range(7):
+    for v in range(8):
         c = Context(Params(**kw))
         c.set_variant(v)
         c.init_velocity(RN1, 2, 4.0, 2.0)
@@ -28,7 +28,7 @@ def test_variants_agree(n, precision, case):
         outs.append(c.download_fields())
         c.close()
     tol = 1e-13 if precision == 0 else 1e-6
-    for v in range(1, 7):
+    for v in range(1, 8):
         assert relerr(outs[v], outs[0]) < tol, (v, relerr(outs[v], outs[0]))
 
 
@@ -36,5 +36,5 @@ def test_tuner_picks_a_valid_variant():
     from hit3d_b200 import Context, Params
     c = Context(Params(nx=64, flow_type=1, kfmax=2, nu=1.0 / 800.0, dt=0.002))
     v, ms = c.autotune()
-    assert 0 <= v < 7 and len(ms) == 7 and all(x > 0 for x in ms)
+    assert 0 <= v < 8 and len(ms) == 8 and all(x > 0 for x in ms)
     assert ms[v] == min(ms)
