@@ -57,8 +57,11 @@ H3D_HD constexpr int plan_rmax(int L)
     for (int s = 0; s < plan_stages(L); s++) r = plan_radix_fwd(L, s) > r ? plan_radix_fwd(L, s) : r;
     return r;
 }
-template <typename T, int L> struct ColCfg {
-    static constexpr int TC = sizeof(T) == 8 ? 8 : 16;  // 128-byte rows of kx columns
+template <typename T, int L, bool YPASS = false> struct ColCfg {
+    // 128-byte rows of kx columns; the FP64 y passes at L = 1024 take 64-byte
+    // rows, so that a CTA's shared memory (TC x L elements) leaves room for two
+    // CTAs per SM (measured faster there, slower for the z passes and FP32)
+    static constexpr int TC = sizeof(T) == 8 ? ((L >= 1024 && YPASS) ? 4 : 8) : 16;
     static constexpr int NT0 = TC * L / plan_rmax(L);
     static constexpr int NTMAX = sizeof(T) == 8 ? 256 : 512;
     static constexpr int NT = NT0 > NTMAX ? NTMAX : NT0;
@@ -230,10 +233,10 @@ static int zinv(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src, 
 }
 
 // in-place strided pass: axis 1 = y (stride pitch, outer z), axis 2 = z (stride n*pitch, outer ky)
-template <typename T, int L>
-static int spass_L(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, int pitch, int nf)
+template <typename T, int L, bool YPASS>
+static int spass_LA(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, int pitch, int nf)
 {
-    using CF = ColCfg<T, L>;
+    using CF = ColCfg<T, L, YPASS>;
     IOPlain<T, T, T> io;
     io.src = base; io.dst = base; io.fs_src = fs; io.fs_dst = fs; io.ncol = c->nh;
     if (axis == 1) { io.sa_src = io.sa_dst = pitch; io.so_src = io.so_dst = (int64_t)c->n * pitch; }
@@ -263,6 +266,12 @@ static int spass_L(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, in
     }
     H3D_LAUNCH_CHECK();
     return 0;
+}
+template <typename T, int L>
+static int spass_L(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, int pitch, int nf)
+{
+    return axis == 1 ? spass_LA<T, L, true>(c, axis, fwd, base, fs, pitch, nf)
+                     : spass_LA<T, L, false>(c, axis, fwd, base, fs, pitch, nf);
 }
 template <typename T> static int spass(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, int pitch, int nf)
 {

@@ -144,14 +144,14 @@ template <typename T, typename TO, int MODE> struct IOSpec {
     }
 };
 
-// two resident CTAs per SM for lengths up to 512, so that one CTA's loads
-// overlap another's shared-memory stages
-template <int L, int NT> struct ColMinBlocks {
-    static constexpr int value = (L <= 512 && NT >= 128) ? 2 : 1;
+// two resident CTAs per SM where two tiles fit in shared memory, so that one
+// CTA's loads overlap another's shared-memory stages
+template <typename T, int L, int TC, int NT> struct ColMinBlocks {
+    static constexpr int value = (NT >= 128 && (size_t)TC * L * sizeof(cx<T>) <= 112 * 1024) ? 2 : 1;
 };
 
 template <typename T, int L, int TC, int NT, bool FWD, class IO>
-__global__ void __launch_bounds__(NT, (ColMinBlocks<L, NT>::value)) k_colfft(const IO io, const cx<T> *__restrict__ tw)
+__global__ void __launch_bounds__(NT, (ColMinBlocks<T, L, TC, NT>::value)) k_colfft(const IO io, const cx<T> *__restrict__ tw)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
