@@ -850,14 +850,22 @@ static int transfer_fields(hit3d_ctx *c, double2 *dev, const double *hsrc, doubl
         double2 *d = dev + f * c->fs64;
         if (hsrc) {
             const double *h = hsrc + (size_t)f * ld1 * rows;
-            H3D_CHECK(cudaMemcpy2DAsync(c->stage, width, h, hp, width, rows, cudaMemcpyHostToDevice, c->st));
+            // ld1 = nx+2 makes a field one contiguous block: one linear copy, which
+            // runs at the full host-to-device rate where the pitched copy does not
+            if (hp == width)
+                H3D_CHECK(cudaMemcpyAsync(c->stage, h, width * rows, cudaMemcpyHostToDevice, c->st));
+            else
+                H3D_CHECK(cudaMemcpy2DAsync(c->stage, width, h, hp, width, rows, cudaMemcpyHostToDevice, c->st));
             k_ref_to_dev<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->stage, d);
             H3D_LAUNCH_CHECK();
         } else {
             double *h = hdst + (size_t)f * ld1 * rows;
             k_dev_to_ref<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, d, c->stage);
             H3D_LAUNCH_CHECK();
-            H3D_CHECK(cudaMemcpy2DAsync(h, hp, c->stage, width, width, rows, cudaMemcpyDeviceToHost, c->st));
+            if (hp == width)
+                H3D_CHECK(cudaMemcpyAsync(h, c->stage, width * rows, cudaMemcpyDeviceToHost, c->st));
+            else
+                H3D_CHECK(cudaMemcpy2DAsync(h, hp, c->stage, width, width, rows, cudaMemcpyDeviceToHost, c->st));
         }
     }
     H3D_CHECK(cudaStreamSynchronize(c->st));
@@ -1646,6 +1654,10 @@ static int batch_capture(hit3d_batch *b, int steps)
 extern "C" int hit3d_batch_step(hit3d_batch *b, int32_t nsteps, int32_t graph_steps)
 {
     if (!b || nsteps < 0) return h3d_set_error_msg(-1, "hit3d_batch_step: bad arguments");
+    for (hit3d_ctx *cr : b->runs)
+        if (cr->p.les_model == HIT3D_LES_LEARNED && !cr->mlp_wb)
+            return h3d_set_error_msg(-1, "hit3d_batch_step: a run with the learned closure (les_model 20) needs weights "
+                                         "(hit3d_gpu_les_set_mlp)");
     if (graph_steps < 1) graph_steps = 1;
     hit3d_ctx *c = b->runs[0];
     H3D_CHECK(cudaSetDevice(b->dev));
@@ -1686,6 +1698,14 @@ extern "C" int hit3d_batch_step(hit3d_batch *b, int32_t nsteps, int32_t graph_st
     for (; left > 0; left--)
         for (hit3d_ctx *cr : b->runs) H3D_TRY(run_step(cr, 0, 0));
     for (hit3d_ctx *cr : b->runs) H3D_CHECK(cudaStreamSynchronize(cr->st));
+    // a run with the learned closure on the tensor cores reports a completion
+    // wait that ran out, as hit3d_gpu_step does
+    for (hit3d_ctx *cr : b->runs)
+        if (cr->p.les_model == HIT3D_LES_LEARNED && cr->mlp_kernel == 1 && nsteps > 0) {
+            int herr = 0;
+            H3D_CHECK(cudaMemcpy(&herr, cr->d_mlp_err, sizeof herr, cudaMemcpyDeviceToHost));
+            if (herr) return h3d_set_error_msg(-5, "hit3d_batch_step: a tensor-core completion wait of the closure ran out");
+        }
     (void)c;
     return 0;
 }

@@ -94,3 +94,14 @@ def test_batch_rerecords_graph_after_dt_change():
         assert np.array_equal(b.contexts[r].download_fields(), c.download_fields())
         c.close()
     b.close()
+
+
+def test_batch_refuses_a_learned_closure_run_without_weights():
+    from hit3d_b200 import Hit3dError, Params
+    from hit3d_b200.batch import Batch
+    b = Batch([Params(nx=32, flow_type=1, kfmax=2, nu=1.0 / 300, dt=0.004),
+               Params(nx=32, flow_type=1, kfmax=2, nu=1.0 / 300, dt=0.004, les_model=20)])
+    b.init()
+    with pytest.raises(Hit3dError, match="weights"):
+        b.step(3, graph_steps=2)
+    b.close()
