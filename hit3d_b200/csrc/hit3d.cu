@@ -604,7 +604,10 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 k_dlm_phys<<<pw_grid(c), 256, 0, c->st>>>(
                     c->n, 2 * (int64_t)wp, 2 * wfs, c->dx, reinterpret_cast<const double *>(Wf(nprod + 11)),
                     reinterpret_cast<double *>(Wf(t0)), reinterpret_cast<double *>(Wf(t0 + 6)),
-                    reinterpret_cast<double *>(Wf(t0 + 7)));
+                    reinterpret_cast<double *>(Wf(t0 + 7)), c->d_kmin + 8);
+                H3D_LAUNCH_CHECK();
+                k_dlm_stats<<<1, 32, 0, c->st>>>((int)pw_grid(c).x, 1.0 / ((double)c->n * c->n * c->n),
+                                                 c->U + 3 * c->fs64, c->d_kmin + 8, c->d_kmin + 4);
                 H3D_LAUNCH_CHECK();
                 H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, 10));
                 H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, 10));
@@ -811,7 +814,12 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     H3D_CHECK(cudaMemset(c->RO, 0, f64 * nf));
     H3D_CHECK(cudaMemset(c->W, 0, wbytes));
     if (c->p.les_model == 2) {
-        if ((rc = ctx_alloc((void **)&c->d_kmin, sizeof(double) * 4))) { hit3d_gpu_finalize(c); return rc; }
+        // [2] the minimum of k_sgs, [4..8) the les.gp means, [8..) block partial sums
+        if ((rc = ctx_alloc((void **)&c->d_kmin, sizeof(double) * (8 + 2 * (size_t)pw_grid(c).x)))) {
+            hit3d_gpu_finalize(c);
+            return rc;
+        }
+        H3D_CHECK(cudaMemset(c->d_kmin, 0, sizeof(double) * 8));
         // m_les_dlm_k_init (m_les.f90:1394-1413): k_sgs = 0.1 in physical space, so
         // only the (0,0,0) mode, 0.1 N^3 after the unnormalised transform
         const double2 k0 = make_double2(0.1 * (double)c->n * (double)c->n * (double)c->n, 0.0);
@@ -1024,6 +1032,35 @@ extern "C" int hit3d_gpu_autotune(hit3d_ctx *c, int32_t *variant, double *ms_out
     }
     c->xcfg = best;
     if (variant) *variant = best;
+    return 0;
+}
+
+extern "C" int hit3d_gpu_check_finite(hit3d_ctx *c, int64_t *nonfinite)
+{
+    if (!c || !nonfinite) return h3d_set_error_msg(-1, "hit3d_gpu_check_finite: null argument");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    unsigned long long *d = reinterpret_cast<unsigned long long *>(c->d_red);
+    H3D_CHECK(cudaMemsetAsync(d, 0, sizeof(unsigned long long), c->st));
+    const int nf = 3 + c->nsc;
+    k_count_nonfinite<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->fs64, nf, c->U, d);
+    H3D_LAUNCH_CHECK();
+    k_count_nonfinite<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->fs64, nf, c->RO, d);
+    H3D_LAUNCH_CHECK();
+    unsigned long long h = 0;
+    H3D_CHECK(cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, c->st));
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    *nonfinite = (int64_t)h;
+    return 0;
+}
+
+extern "C" int hit3d_gpu_les_stats(hit3d_ctx *c, double *out4)
+{
+    if (!c || !out4) return h3d_set_error_msg(-1, "hit3d_gpu_les_stats: null argument");
+    if (c->p.les_model != 2)
+        return h3d_set_error_msg(-1, "hit3d_gpu_les_stats: les.gp quantities exist for les_model 2 only");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    H3D_CHECK(cudaMemcpyAsync(out4, c->d_kmin + 4, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
+    H3D_CHECK(cudaStreamSynchronize(c->st));
     return 0;
 }
 

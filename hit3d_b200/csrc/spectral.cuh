@@ -399,6 +399,25 @@ __global__ void k_alias_max(int n, int nh, int pitch, int64_t fs, int nf, const 
     if ((threadIdx.x & 31) == 0 && mx > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(mx));
 }
 
+// number of non-finite components among the N^2 (N/2+1) modes of nf fields of
+// A (state layout, row pitch `pitch` complex, field stride fs)
+__global__ void k_count_nonfinite(int n, int nh, int pitch, int64_t fs, int nf, const double2 *__restrict__ A,
+                                  unsigned long long *out)
+{
+    const int64_t nm = (int64_t)n * n * nh;
+    unsigned long long cnt = 0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / nh, o = row * pitch + (t - row * nh);
+        for (int f = 0; f < nf; f++) {
+            const double2 v = A[o + f * fs];
+            cnt += !isfinite(v.x);
+            cnt += !isfinite(v.y);
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
+}
+
 // Shell spectrum sum_{shell} fac * |f|^2 (kx = 0 halved, kx = N/2 excluded),
 // float32 shell index (m_stats.f90:195-235).  Deterministic: each warp owns a
 // private histogram, lane L accumulates the shells congruent to L mod 32 in a
@@ -555,10 +574,15 @@ __global__ void k_dlm_commit(int n, int nh, int pitch, const double *__restrict_
 //   KC (k_sgs with the 2/3 rule)      -> 2 nu_t S_ij S_ij - max(KC,0)^1.5 / Delta
 //                                                                    (m_les.f90:1422-1621)
 //   G[0..3) (dk/dx_i)                 -> nu_t dk/dx_i                (m_les.f90:1041-1091)
-__global__ void k_dlm_phys(int n, int64_t rp, int64_t fs, double delta, const double *__restrict__ NUT,
-                           double *__restrict__ S, double *__restrict__ KC, double *__restrict__ G)
+// part[2 b], part[2 b + 1]: block b's sums of the production and of the
+// dissipation, for the domain means that les.gp reports (m_les.f90:1536,1617)
+__global__ void __launch_bounds__(256) k_dlm_phys(int n, int64_t rp, int64_t fs, double delta,
+                                                  const double *__restrict__ NUT, double *__restrict__ S,
+                                                  double *__restrict__ KC, double *__restrict__ G,
+                                                  double *__restrict__ part)
 {
     const int64_t np = (int64_t)n * n * n;
+    double psum = 0.0, dsum = 0.0;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t row = t / n, o = row * rp + (t - row * n);
         const double nut = NUT[o];
@@ -572,11 +596,47 @@ __global__ void k_dlm_phys(int n, int64_t rp, int64_t fs, double delta, const do
         ss = ss + 2.0 * (sv[4] * sv[4]);
         ss = ss + sv[5] * sv[5];
         const double kc = KC[o] > 0.0 ? KC[o] : 0.0;
-        KC[o] = (2.0 * ss) * nut - pow(kc, 1.5) / delta;
+        const double prod = (2.0 * ss) * nut, diss = pow(kc, 1.5) / delta;
+        KC[o] = prod - diss;
+        psum += prod;
+        dsum += diss;
 #pragma unroll
         for (int c = 0; c < 6; c++) S[o + c * fs] = (-2.0 * nut) * sv[c];
 #pragma unroll
         for (int d = 0; d < 3; d++) G[o + d * fs] = G[o + d * fs] * nut;
+    }
+    __shared__ double sh[2][8];
+    for (int off = 16; off > 0; off >>= 1) {
+        psum += __shfl_xor_sync(0xffffffffu, psum, off);
+        dsum += __shfl_xor_sync(0xffffffffu, dsum, off);
+    }
+    if ((threadIdx.x & 31) == 0) { sh[0][threadIdx.x >> 5] = psum; sh[1][threadIdx.x >> 5] = dsum; }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += sh[threadIdx.x][w];
+        part[2 * blockIdx.x + threadIdx.x] = v;
+    }
+}
+
+// out[0..3] = energy, production, B, dissipation of les.gp (m_les.f90:876-892):
+// the mean k_sgs from its zero mode K0 (unnormalised forward transform), the
+// block sums of k_dlm_phys divided by N^3, and B = 0 (no lag model); one warp,
+// fixed summation order
+__global__ void k_dlm_stats(int nblk, double inv_n3, const double2 *__restrict__ K0, const double *__restrict__ part,
+                            double *__restrict__ out)
+{
+    double p = 0.0, d = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += 32) { p += part[2 * b]; d += part[2 * b + 1]; }
+    for (int off = 16; off > 0; off >>= 1) {
+        p += __shfl_xor_sync(0xffffffffu, p, off);
+        d += __shfl_xor_sync(0xffffffffu, d, off);
+    }
+    if (threadIdx.x == 0) {
+        out[0] = K0[0].x * inv_n3;
+        out[1] = p * inv_n3;
+        out[2] = 0.0;
+        out[3] = d * inv_n3;
     }
 }
 

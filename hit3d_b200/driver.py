@@ -6,7 +6,10 @@ hit3d_b200.gpu.  Output files keep the reference's names and formats:
 stat1.gp / stat2.gp / es.gp (m_stats.f90:150-185), scNN.gp / es_NN.gp
 (m_stats.f90:66-80, 420-432), u./v./w./scNN. real*4 files (io_write_4.f90) and
 <run_name>.64.<itime> restart files (restart_io.f90).  Exit reasons follow
-my_exit.f90:23-62: 0 normal, 1 TMAX, 2 run limit, 3 user 'stop' file.
+my_exit.f90:23-62: 0 normal, 1 TMAX, 2 run limit, 3 user 'stop' file.  One
+reason is added, -2: the state turned non-finite (a non-finite Courant number,
+or the device count of non-finite modes at a statistics step); as for every
+negative reason of my_exit.f90:58-61, no restart is written over good ones.
 """
 from __future__ import annotations
 
@@ -153,6 +156,14 @@ class Simulation:
                         fh.write(f"{k + 1:4d}{_fmt_e(v)}\n")
         return es, st
 
+    def _les_gp(self, it, t):
+        """les.gp (m_les.f90:876-892): itime, the time at the start of the step,
+        mean k_sgs, production, B and dissipation of that step's RHS."""
+        ls = self.ctx.les_stats()
+        vals = (t, ls["energy"], ls["production"], ls["B"], ls["dissipation"])
+        with open(os.path.join(self.wd, "les.gp"), "a") as fh:
+            fh.write(f"{it:6d} " + "".join(_fmt_e(x) for x in vals) + "\n")
+
     # -- time step control (my_dt.f90) ------------------------------------------
     def my_dt(self, courant):
         c = self.cfg
@@ -183,7 +194,12 @@ class Simulation:
                     if it % c.iprint1 == 0:
                         self.stat_main()
             courant = self.ctx.step(1)
+            if c.les_model == 2 and it % c.iprint1 == 0:
+                self._les_gp(it, t)
             self.time += c.dt
+            if not math.isfinite(courant) or (it % c.iprint1 == 0 and self.ctx.nonfinite() > 0):
+                self.log.append(f"ITIME={it:6d}   non-finite state")
+                return self.exit(-2)
             if it % c.iprint2 == 0:
                 self.write_restart()
             if c.variable_dt:

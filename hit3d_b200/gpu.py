@@ -98,6 +98,8 @@ SIGNATURES = [
     ("hit3d_gpu_autotune", C.c_int, [_vp, C.POINTER(_i32), _dp]),
     ("hit3d_gpu_set_variant", C.c_int, [_vp, _i32]),
     ("hit3d_gpu_set_pruning", C.c_int, [_vp, _i32]),
+    ("hit3d_gpu_check_finite", C.c_int, [_vp, C.POINTER(_i64)]),
+    ("hit3d_gpu_les_stats", C.c_int, [_vp, _dp]),
     ("hit3d_gpu_pruned", C.c_int, [_vp]),
     ("hit3d_gpu_step_profile", C.c_int, [_vp, _i32, C.POINTER(_i32), C.POINTER(_i32), _dp]),
     ("hit3d_gpu_set_dt", C.c_int, [_vp, _d]),
@@ -260,6 +262,18 @@ class Context:
 
     def set_variant(self, v: int):
         _check(lib().hit3d_gpu_set_variant(self._h, int(v)), "set_variant")
+
+    def nonfinite(self) -> int:
+        """Number of non-finite components of the state and the AB2 history (on the device)."""
+        v = C.c_int64(0)
+        _check(lib().hit3d_gpu_check_finite(self._h, C.byref(v)), "check_finite")
+        return int(v.value)
+
+    def les_stats(self) -> dict:
+        """les.gp quantities of the last step (dynamic localization model only)."""
+        out = np.zeros(4)
+        _check(lib().hit3d_gpu_les_stats(self._h, _ptr(out)), "les_stats")
+        return dict(zip(("energy", "production", "B", "dissipation"), out.tolist()))
 
     def set_pruning(self, on: bool):
         """Allow (default) or forbid 2/3-rule pruning of the step's transforms."""

@@ -128,6 +128,20 @@ int hit3d_gpu_set_variant(hit3d_ctx *ctx, int32_t variant);
 int hit3d_gpu_set_pruning(hit3d_ctx *ctx, int32_t on);
 int hit3d_gpu_pruned(hit3d_ctx *ctx);
 
+/* Failure detection (no reference counterpart: a diverged run of the
+ * reference carries NaN into its files).  Counts, on the device, the
+ * non-finite components of the state and the AB2 history; the host loop
+ * checks it with the statistics and ends the run with an error status. */
+int hit3d_gpu_check_finite(hit3d_ctx *ctx, int64_t *nonfinite);
+
+/* The les.gp quantities of the last step of a dynamic-localization run
+ * (les_model 2; m_les.f90:876-892, the write of les_rhs_scalars):
+ * out4 = {mean k_sgs, mean production 2 nu_t S:S, B (0: no lag model),
+ * mean dissipation k^(3/2)/Delta}, all from the state at the start of that
+ * step.  An error for any other les_model, as the reference writes les.gp
+ * only when n_les > 0. */
+int hit3d_gpu_les_stats(hit3d_ctx *ctx, double *out4);
+
 /* Number of kernels this context has launched since hit3d_gpu_init. */
 int64_t hit3d_gpu_launch_count(hit3d_ctx *ctx);
 

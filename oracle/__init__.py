@@ -70,6 +70,7 @@ def lib():
         L.oracle_fft3d.argtypes = [vp, C.c_int, dp]
         L.oracle_fft1d.argtypes = [C.c_int, dp, C.c_int]
         L.oracle_stats.argtypes = [vp, dp]
+        L.oracle_les_stats.argtypes = [vp, dp]
         L.oracle_scalar_stats.argtypes = [vp, dp]
         L.oracle_energy_spectrum.argtypes = [vp, C.c_int, C.c_int, dp]
         L.oracle_forcing_energy.restype = C.c_double
@@ -215,6 +216,12 @@ class Oracle:
         keys = ["energy", "eps_v", "eta", "etakmax", "uvar", "x_length", "lambda", "re_lambda",
                 "re_lambda1", "tau_e", "enstrophy", "skewness"]
         return out[: self.kmax].copy(), dict(zip(keys, out[self.kmax:].tolist()))
+
+    def les_stats(self):
+        """les.gp quantities of the last RHS evaluation (dynamic localization model)."""
+        out = np.zeros(4)
+        lib().oracle_les_stats(self._p, _dp(out))
+        return dict(zip(("energy", "production", "B", "dissipation"), out.tolist()))
 
     def scalar_stats(self):
         out = np.zeros(self.nscal * (self.kmax + 5))

@@ -213,6 +213,7 @@ typedef struct {
     int nfn, *fn_i, *fn_j, *fn_k;  /* forced nodes */
     fftplan plan;
     double courant, time;
+    double les_stat[4];       /* les.gp: mean k_sgs, production, B, dissipation */
     int fov, fos, int_scalars;
     double *scratch;          /* per-thread FFT scratch: nthreads * 4n doubles */
     int nthreads;
@@ -705,6 +706,8 @@ static void les_k_src_dlm(oracle_t *o)
                 a1[a] = a1[a] * tv[a];
             }
     xfft3d(o, 1, a1);
+    /* saved for les.gp (m_les.f90:1536): the zero mode over N^3 */
+    o->les_stat[1] = a1[0] / ((double)n * n * n);
     double *r = W(o, kn);
     for (size_t q = 0; q < o->fsz; q++)
         if (o->ialias[q] == 0) r[q] = r[q] + a1[q];
@@ -725,6 +728,7 @@ static void les_k_diss_algebraic(oracle_t *o)
         w0[q] = pow(v, 1.5) / o->les_delta;
     }
     xfft3d(o, 1, w0);
+    o->les_stat[3] = w0[0] / ((double)n * n * n);    /* m_les.f90:1617 */
     double *r = W(o, kn);
     for (int k = 0; k < n; k++)
         for (int j = 0; j < n; j++)
@@ -901,6 +905,9 @@ static void oracle_rhs_scalars(oracle_t *o)
         }
     /* les_rhs_scalars, DLM branch (m_les.f90:714-719) */
     if (o->les_model == 2) {
+        /* les.gp energy and B (m_les.f90:880-885; no lag model, so B = 0) */
+        o->les_stat[0] = F(o, 3 + ns)[0] / ((double)o->n * o->n * o->n);
+        o->les_stat[2] = 0.0;
         les_k_src_dlm(o);
         les_k_diss_algebraic(o);
         for (int m = 4; m <= 3 + ns + nl; m++) les_rhss_turb_visc1(o, m);
@@ -1726,6 +1733,10 @@ void oracle_apply_filter(oracle_t *o, const double *g, double *a)
 }
 
 int oracle_n(oracle_t *o) { return o->n; }
+void oracle_les_stats(oracle_t *o, double *out)
+{
+    for (int q = 0; q < 4; q++) out[q] = o->les_stat[q];
+}
 size_t oracle_fsz(oracle_t *o) { return o->fsz; }
 double oracle_time(oracle_t *o) { return o->time; }
 void oracle_set_time(oracle_t *o, double t) { o->time = t; }

@@ -22,6 +22,11 @@ def test_dlm_matches_oracle(n):
         f = g.download_fields()
         assert relerr(f[:3], o.fields[:3]) < 1e-10
         assert relerr(f[3], o.fields[3]) < 1e-10
+        # les.gp means of the last step (device block sums against the oracle's zero modes)
+        gs, os_ = g.les_stats(), o.les_stats()
+        assert gs["B"] == 0.0
+        for k in ("energy", "production", "dissipation"):
+            assert gs[k] == pytest.approx(os_[k], rel=1e-11), k
     assert relerr(g.download_rhs_old(), o.rhs_old) < 1e-9
 
 
@@ -43,6 +48,13 @@ def test_dlm_clips_negative_k_sgs_like_the_oracle():
     o.step(5)
     g.step(5)
     assert relerr(g.download_fields(), o.fields) < 1e-10
+
+
+def test_les_stats_only_for_the_dynamic_localization_model():
+    from hit3d_b200 import Context, Hit3dError, Params
+    with Context(Params(nx=32, les_model=1)) as c:
+        with pytest.raises(Hit3dError, match="les_model 2"):
+            c.les_stats()
 
 
 def test_dlm_rejects_what_it_does_not_support():

@@ -88,6 +88,11 @@ def test_dlm_run_restarts_with_k_sgs(tmp_path):
     sim = Simulation("dlm64", wd, cfg=cfg)
     sim.begin()
     assert sim.run() == 0 and sim.itime == 6
+    # les.gp at every statistics step: itime, time, mean k_sgs, production, B, dissipation
+    rows = [ln.split() for ln in open(os.path.join(wd, "les.gp"))]
+    assert [int(r[0]) for r in rows] == [3, 6] and all(len(r) == 6 for r in rows)
+    assert float(rows[1][1]) == pytest.approx(5 * 0.005, rel=1e-6) and float(rows[1][4]) == 0.0
+    assert float(rows[1][3]) > 0 and float(rows[1][5]) > 0
     f, t, dt, nums, nles = read_restart(os.path.join(wd, "dlm64.64.000006"), 64, 0, 1)
     assert nums == 0 and nles == 1 and f.shape[0] == 4
     g = sim.ctx.download_fields()
@@ -95,3 +100,44 @@ def test_dlm_run_restarts_with_k_sgs(tmp_path):
     sim2 = Simulation("dlm64", wd, cfg=replace(cfg, itmin=6))
     sim2.begin()
     assert np.array_equal(sim2.ctx.download_fields()[..., :64], g[..., :64])
+
+
+def test_run_limit_ends_the_run_with_a_restart(tmp_path):
+    """job_parameters.txt gives the run limit in minutes; the loop leaves with
+    reason 2 at the first 10-step check within 5 minutes of it (main.f90)."""
+    from hit3d_b200.driver import Simulation
+    wd = str(tmp_path)
+    shutil.copy(os.path.join(GOLDEN, "decay64_.in"), os.path.join(wd, "decay64_.in"))
+    with open(os.path.join(wd, "job_parameters.txt"), "w") as fh:
+        fh.write("4.0\n")
+    sim = Simulation("decay64_", wd)
+    assert sim.job_runlimit == 4.0
+    sim.begin()
+    assert sim.run() == 2 and sim.itime == 10
+    assert os.path.exists(os.path.join(wd, "decay64_.64.000010"))
+
+
+def test_non_finite_state_is_detected_on_the_device(tmp_path):
+    """NaN and Inf planted in a host copy of the state are counted by the
+    device reduction, and the host loop then ends with reason -2 and writes
+    no restart."""
+    from hit3d_b200.driver import Simulation
+    wd = str(tmp_path)
+    shutil.copy(os.path.join(GOLDEN, "decay64_.in"), os.path.join(wd, "decay64_.in"))
+    sim = Simulation("decay64_", wd)
+    sim.begin()
+    assert sim.ctx.nonfinite() == 0
+    f = sim.ctx.download_fields()
+    good = f.copy()
+    f[1, 5, 7, 9] = np.nan
+    f[4, 0, 0, 0] = np.inf
+    f[0, 63, 63, 65] = -np.inf
+    sim.ctx.upload_fields(f)
+    assert sim.ctx.nonfinite() == 3
+    sim.ctx.upload_fields(good)
+    assert sim.ctx.nonfinite() == 0
+    f[2, 3, 3, 3] = np.nan
+    sim.ctx.upload_fields(f)
+    # the Courant maximum (fmax) passes over NaN, so the statistics step finds it
+    assert sim.run() == -2 and sim.itime == 10
+    assert not any(n.startswith("decay64_.64.") for n in os.listdir(wd))

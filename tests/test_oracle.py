@@ -1,0 +1,294 @@
+"""Pins of the FP64 CPU oracle, on the CPU.  The reference cannot be built here
+and ships no golden vectors, so the oracle is checked against what can be
+stated independently of it:
+
+- the analytic RHS checks of the reference's own (uncalled) test routines,
+  test_rhs_velocity (rhs_velocity.f90:430-553) and test_rhs_scalars
+  (rhs_scalars.f90:504-594);
+- numpy.fft for the 3-D real transform and the 1-D complex transform;
+- a pure-Python integer restatement of RANDu (RANDu.f:12-52);
+- the target spectra that init_velocity imposes (init_velocity.f90:150-237);
+- the band forcing of force_velocity (m_force.f90:101-182) restated in numpy;
+- exact properties: the 2/3-rule nonlinear term conserves energy, the pressure
+  projection leaves a divergence-free field, and the les.gp means of the
+  dynamic localization model for a uniform k_sgs (m_les.f90:876-892)."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from _cases import RN1
+
+
+def _grid(n):
+    x = np.arange(n) * 2 * np.pi / n
+    Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
+    return X, Y, Z
+
+
+def _phys(n, f):
+    """A physical field in the reference's array: [z][y][x] with two padding entries."""
+    a = np.zeros((n, n, n + 2))
+    a[..., :n] = f
+    return a
+
+
+def _wavenumbers(n):
+    """akx per real entry (pairs), aky / akz per index (m_fields.f90 layout)."""
+    akx = (np.arange(n + 2) // 2).astype(np.float64)
+    k = np.arange(n, dtype=np.float64)
+    aky = np.where(k <= n // 2, k, k - n)
+    return akx, aky, aky.copy()
+
+
+def _to_complex(f):
+    """Reference Fourier layout [ky][kz][kx re/im] -> complex [ky][kz][kx]."""
+    return f[..., 0::2] + 1j * f[..., 1::2]
+
+
+def _shell32(k2):
+    """nint(sqrt(real(k2, 4))): the single-precision shell index of the reference."""
+    r = np.sqrt(np.asarray(k2, dtype=np.float32)).astype(np.float64)
+    return np.floor(r + 0.5).astype(np.int64)
+
+
+# --- transforms -----------------------------------------------------------------
+
+@pytest.mark.parametrize("n", [16, 24, 40, 48])
+def test_fft3d_matches_numpy(n):
+    """xFFT3d(+1): unnormalised forward, e^{-i}, result in [ky][kz][kx re/im];
+    xFFT3d(-1): the inverse with 1/N^3 (x_fftw.f90:850-1090)."""
+    o = oracle.Oracle(n)
+    rng = np.random.default_rng(n)
+    f = rng.standard_normal((n, n, n))
+    a = _phys(n, f)
+    o.fft3d(1, a)
+    want = np.fft.rfftn(f).transpose(1, 0, 2)
+    got = _to_complex(a)
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    o.fft3d(-1, a)
+    assert np.abs(a[..., :n] - f).max() <= 1e-13 * np.abs(f).max()
+
+
+@pytest.mark.parametrize("n", [8, 12, 20, 48, 96, 160])
+def test_fft1d_matches_numpy(n):
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    assert np.abs(oracle.fft1d(x, -1) - np.fft.fft(x)).max() <= 1e-13 * n
+    assert np.abs(oracle.fft1d(x, 1) - n * np.fft.ifft(x)).max() <= 1e-13 * n
+
+
+# --- random numbers ---------------------------------------------------------------
+
+def _randu_python(seed, count):
+    """RANDu.f:12-52 in Python integers.  idum is recomputed from the caller's
+    argument on every call; iv, iy and idum2 are saved between calls."""
+    im1, im2, ia1, ia2, iq1, iq2, ir1, ir2, ntab = 2147483563, 2147483399, 40014, 40692, 53668, 52774, 12211, 3791, 32
+    imm1 = im1 - 1
+    ndiv = 1 + imm1 // ntab
+    am, rnmx = 1.0 / im1, 1.0 - 1.2e-7
+    st = {"idum2": 123456789, "iy": 0, "iv": [0] * ntab}
+
+    def fdiv(a, b):                      # Fortran integer division truncates toward zero
+        q = abs(a) // abs(b)
+        return q if (a >= 0) == (b >= 0) else -q
+
+    def rnd(idum3):
+        idum = int(math.floor(abs(idum3 / 987.0) + 0.5)) * (1 if idum3 >= 0 else -1)
+        if idum <= 0:
+            idum = max(-idum, 1)
+            st["idum2"] = idum
+            for j in range(ntab + 8, 0, -1):
+                k = fdiv(idum, iq1)
+                idum = ia1 * (idum - k * iq1) - k * ir1
+                if idum < 0:
+                    idum += im1
+                if j <= ntab:
+                    st["iv"][j - 1] = idum
+        k = fdiv(idum, iq1)
+        idum = ia1 * (idum - k * iq1) - k * ir1
+        if idum < 0:
+            idum += im1
+        k = fdiv(st["idum2"], iq2)
+        st["idum2"] = ia2 * (st["idum2"] - k * iq2) - k * ir2
+        if st["idum2"] < 0:
+            st["idum2"] += im2
+        j = 1 + fdiv(st["iy"], ndiv)
+        st["iy"] = st["iv"][j - 1] - st["idum2"]
+        st["iv"][j - 1] = idum
+        if st["iy"] < 1:
+            st["iy"] += imm1
+        return min(am * st["iy"], rnmx)
+
+    rnd(-seed)
+    return np.array([rnd(seed) for _ in range(count)])
+
+
+@pytest.mark.parametrize("seed", [RN1, 93712139.0, 10765397.0, 987.0 * 5])
+def test_randu_stream_is_exact(seed):
+    got = oracle.randu_stream(seed, 3000)
+    want = _randu_python(seed, 3000)
+    assert np.array_equal(got, want)
+    assert (got > 0).all() and (got < 1).all()
+
+
+# --- initial spectrum -------------------------------------------------------------
+
+@pytest.mark.parametrize("isp", [0, 1, 3])
+def test_init_velocity_imposes_the_target_spectrum(isp):
+    """init_velocity.f90:150-237: every shell 1..kmax carries the normalised
+    target spectrum, binned as the reference bins it (real entries i < nx,
+    kx = 0 halved, single-precision shell index)."""
+    n, peak = 32, 4.0
+    o = oracle.Oracle(n)
+    o.init_velocity(RN1, isp_type=isp, peak_wavenum=peak)
+    akx, aky, akz = _wavenumbers(n)
+    k2 = akx[None, None, :] ** 2 + aky[:, None, None] ** 2 + akz[None, :, None] ** 2
+    sh = _shell32(k2)[..., :n]
+    w = np.where(akx[:n] == 0, 0.5, 1.0)[None, None, :]
+    e = (o.fields[:3, ..., :n] ** 2).sum(axis=0) * w / float(n) ** 6
+    kmax = o.kmax
+    got = np.bincount(sh.ravel(), weights=e.ravel(), minlength=kmax + 2)[1:kmax + 1]
+    k = np.arange(1, kmax + 1, dtype=np.float64)
+    r = k / peak
+    tgt = {0: k ** (-5.0 / 3.0), 1: r ** 3 / peak * np.exp(-3.0 * r),
+           3: (2 * np.pi * r) ** 4 / (1 + (2 * np.pi * r) ** 2) ** 3}[isp]
+    tgt = tgt / tgt.sum()
+    assert np.abs(got - tgt).max() <= 1e-13
+    # nothing outside shells 1..kmax, and the field is solenoidal
+    full_sh = _shell32(k2)
+    assert np.abs(o.fields[:3][:, (full_sh == 0) | (full_sh > kmax)]).max() == 0.0
+    u = _to_complex(o.fields[:3])
+    div = akx[0::2][None, None, :] * u[0] + aky[:, None, None] * u[1] + akz[None, :, None] * u[2]
+    assert np.abs(div).max() <= 1e-12 * np.abs(u).max()
+
+
+# --- right-hand sides -------------------------------------------------------------
+
+@pytest.mark.parametrize("nu", [0.0, 0.01])
+def test_rhs_velocity_analytic(nu):
+    """test_rhs_velocity (rhs_velocity.f90:430-553): for u = (sin x, sin y, sin z)
+    the RHS is -sin(x) (2 cos x + cos y + cos z + nu), and cyclically."""
+    n = 16
+    o = oracle.Oracle(n, nu=nu, flow_type=0)
+    X, Y, Z = _grid(n)
+    for m, f in enumerate((np.sin(X), np.sin(Y), np.sin(Z))):
+        a = _phys(n, f)
+        o.fft3d(1, a)
+        o.fields[m] = a
+    o.rhs()
+    got = o.wrk[1:4].copy()
+    for m in range(3):
+        o.fft3d(-1, got[m])
+    s = np.cos(X) + np.cos(Y) + np.cos(Z)
+    want = [-np.sin(X) * (np.cos(X) + s + nu), -np.sin(Y) * (np.cos(Y) + s + nu),
+            -np.sin(Z) * (np.cos(Z) + s + nu)]
+    for m in range(3):
+        assert np.abs(got[m][..., :n] - want[m]).max() <= 1e-13
+
+
+def test_rhs_scalars_analytic():
+    """test_rhs_scalars (rhs_scalars.f90:504-594): u = (sin x, sin 5y, sin 17z),
+    phi = cos x, Sc = 1, nu = 0.5: RHS = -cos 2x - cos x (5 cos 5y + 17 cos 17z + nu).
+    A scalar of initial type 1 carries no mean-gradient source."""
+    n, nu = 54, 0.5
+    o = oracle.Oracle(n, nu=nu, nscal=1, sc=(1.0,), scalar_type=(1,))
+    o.set_flags(1, 1, 1)
+    X, Y, Z = _grid(n)
+    for m, f in enumerate((np.sin(X), np.sin(5 * Y), np.sin(17 * Z), np.cos(X))):
+        a = _phys(n, f)
+        o.fft3d(1, a)
+        o.fields[m] = a
+    o.rhs()
+    r = o.wrk[4].copy()
+    o.fft3d(-1, r)
+    want = -np.cos(2 * X) - np.cos(X) * (5 * np.cos(5 * Y) + 17 * np.cos(17 * Z) + nu)
+    assert np.abs(r[..., :n] - want).max() <= 1e-12
+
+
+def test_two_thirds_nonlinear_term_conserves_energy():
+    """For a solenoidal, 2/3-rule-truncated u the products are alias-free on the
+    kept modes, so sum_k Re(u* . N) = 0 (N = -d(u_i u_j)/dx_j, nu = 0)."""
+    n = 32
+    o = oracle.Oracle(n, nu=0.0, flow_type=0)
+    o.init_velocity(RN1, isp_type=1, peak_wavenum=4.0)
+    o.dealias_all()
+    o.rhs()
+    akx, _, _ = _wavenumbers(n)
+    w = np.where(akx == 0, 1.0, 2.0)[None, None, None, :]
+    dot = (o.fields[:3] * o.wrk[1:4] * w).sum()
+    scale = (np.abs(o.fields[:3]) * np.abs(o.wrk[1:4]) * w).sum()
+    assert scale > 0 and abs(dot) <= 1e-13 * scale
+
+
+def test_pressure_projection_is_divergence_free():
+    """pressure.f90: u <- u - k (k.u)/k^2 leaves k.u = 0 and is idempotent."""
+    n = 24
+    o = oracle.Oracle(n)
+    rng = np.random.default_rng(5)
+    for m in range(3):
+        a = _phys(n, rng.standard_normal((n, n, n)))
+        o.fft3d(1, a)
+        o.fields[m] = a
+    o.pressure()
+    akx, aky, akz = _wavenumbers(n)
+    u = _to_complex(o.fields[:3])
+    div = akx[0::2][None, None, :] * u[0] + aky[:, None, None] * u[1] + akz[None, :, None] * u[2]
+    # the Nyquist planes carry modes whose +-N/2 ambiguity the projection does not resolve
+    inner = (np.abs(aky) < n // 2)[:, None, None] & (np.abs(akz) < n // 2)[None, :, None] \
+        & (akx[0::2] < n // 2)[None, None, :]
+    assert np.abs(div[inner]).max() <= 1e-12 * np.abs(u).max()
+    before = o.fields[:3].copy()
+    o.pressure()
+    assert np.abs(o.fields[:3] - before).max() <= 1e-13 * np.abs(before).max()
+
+
+def test_band_forcing_matches_numpy_restatement():
+    """force_velocity (m_force.f90:101-182): every real entry of shells 1..kfmax
+    gains FAMP / E_band times itself, E_band binned as in the reference."""
+    n, famp, kfmax = 32, 0.5, 2
+    o0 = oracle.Oracle(n, flow_type=0, kfmax=kfmax, famp=famp)
+    o1 = oracle.Oracle(n, flow_type=1, kfmax=kfmax, famp=famp)
+    o0.init_velocity(RN1, isp_type=1, peak_wavenum=3.0)
+    o0.dealias_all()
+    o1.fields[:] = o0.fields
+    o0.rhs()
+    o1.rhs()
+    akx, aky, akz = _wavenumbers(n)
+    sh = _shell32(akx[None, None, :] ** 2 + aky[:, None, None] ** 2 + akz[None, :, None] ** 2)
+    band = (sh > 0) & (sh <= kfmax)
+    band[..., n:] = False
+    w = np.where(akx == 0, 0.5, 1.0)[None, None, :]
+    e_band = ((o0.fields[:3] ** 2).sum(axis=0) * w)[band].sum() / float(n) ** 6
+    want = np.where(band[None], famp / e_band * o0.fields[:3], 0.0)
+    got = o1.wrk[1:4] - o0.wrk[1:4]
+    assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
+    assert o1.nforced() == int(band.sum())
+
+
+def test_dlm_les_means_for_uniform_k_sgs():
+    """les.gp of the dynamic localization model (m_les.f90:876-892) for k_sgs =
+    0.1 everywhere: energy 0.1, dissipation 0.1^1.5 / Delta, B = 0 and production
+    2 nu_t <S:S> with nu_t = 0.1 Delta sqrt(0.1) (Delta = dx)."""
+    n = 32
+    o = oracle.Oracle(n, les_model=2, flow_type=0, nu=1.0 / 2000.0)
+    o.init_velocity(RN1, isp_type=1, peak_wavenum=4.0)
+    o.dealias_all()
+    o.fields[3] = 0.0
+    o.fields[3, 0, 0, 0] = 0.1 * n ** 3
+    o.rhs()
+    st = o.les_stats()
+    dx = 2 * np.pi / n
+    u = _to_complex(o.fields[:3]).transpose(0, 2, 1, 3)            # [c][kz][ky][kx]
+    kz = np.fft.fftfreq(n, 1.0 / n)[:, None, None]
+    ky = np.fft.fftfreq(n, 1.0 / n)[None, :, None]
+    kx = np.arange(n // 2 + 1)[None, None, :]
+    kk = (kx, ky, kz)
+    grad = [[np.fft.irfftn(1j * kk[j] * u[i], s=(n, n, n), axes=(0, 1, 2)) for j in range(3)] for i in range(3)]
+    ss = sum((0.5 * (grad[i][j] + grad[j][i])) ** 2 for i in range(3) for j in range(3)).mean()
+    nut = 0.1 * dx * math.sqrt(0.1)
+    assert st["energy"] == pytest.approx(0.1, rel=1e-14)
+    assert st["B"] == 0.0
+    assert st["dissipation"] == pytest.approx(0.1 ** 1.5 / dx, rel=1e-13)
+    assert st["production"] == pytest.approx(2 * nut * ss, rel=1e-12)
