@@ -22,6 +22,7 @@ import numpy as np
 from .gpu import Context
 from .params import RunConfig, read_input_file
 from .restart import read_restart, restart_name, write_real4, write_restart
+from .sidecar import GpuSettings, SidecarError, read_sidecar
 
 
 def _fmt_e(x: float, w: int = 15, d: int = 6) -> str:
@@ -41,12 +42,32 @@ def _fmt_e(x: float, w: int = 15, d: int = 6) -> str:
 class Simulation:
     """One run: the reference's hydro task with the state resident on the GPU."""
 
-    def __init__(self, run_name: str, workdir: str = ".", cfg: RunConfig | None = None, precision: int = 0,
-                 device: int = 0, job_runlimit_min: float = 12 * 60):
+    def __init__(self, run_name: str, workdir: str = ".", cfg: RunConfig | None = None,
+                 precision: int | None = None, device: int | None = None, job_runlimit_min: float = 12 * 60,
+                 settings: GpuSettings | None = None):
+        """cfg: the `.in` settings (read from workdir if None); settings: those of
+        `<run_name>.gpu.in` (read from workdir if None); precision and device, when
+        given, override the settings."""
         self.run_name = run_name
         self.wd = workdir
         self.cfg = cfg or read_input_file(os.path.join(workdir, run_name + ".in"))
-        self.ctx = Context(self.cfg.to_params(precision=precision, device=device))
+        s = settings if settings is not None else read_sidecar(workdir, run_name)
+        if precision is not None:
+            s.precision = precision
+        if device is not None:
+            s.device = device
+        self.settings = s
+        if s.les_model is not None:
+            self.cfg.les_model = s.les_model
+            if s.les_model > 0:
+                self.cfg.dealias = 0  # every LES model runs with the 2/3 rule (m_parameters.f90:416-420)
+        self.ctx = Context(self.cfg.to_params(precision=s.precision, device=s.device, c_smag=s.c_smag))
+        if not s.pruning:
+            self.ctx.set_pruning(False)
+        if s.variant is not None:
+            self.ctx.set_variant(s.variant)
+        if self.cfg.les_model == 20:
+            self._load_closure()
         self.time = 0.0
         self.itime = self.cfg.itmin
         self.int_scalars = False
@@ -60,6 +81,17 @@ class Simulation:
                 pass
         self.exit_reason = None
         self.log = []
+
+    def _load_closure(self):
+        s = self.settings
+        if s.les_mlp is None:
+            raise SidecarError("les_model 20 (learned closure) needs les_mlp weights")
+        path = s.les_mlp if os.path.isabs(s.les_mlp) else os.path.join(self.wd, s.les_mlp)
+        w = np.load(path)
+        if w.dtype != np.uint16:
+            raise SidecarError(f"{path}: the closure weights must be bf16 bit patterns (uint16), got {w.dtype}")
+        delta = s.les_mlp_delta if s.les_mlp_delta is not None else 2.0 * self.cfg.dx
+        self.ctx.les_set_mlp(w, delta, clip=s.les_mlp_clip, kernel=s.les_mlp_kernel)
 
     # -- start-up (begin_new.f90 / begin_restart.f90) ---------------------------
     def begin(self):
@@ -86,6 +118,8 @@ class Simulation:
         self.ctx.set_scalars_active(self.int_scalars)
         self.ctx.fov = self.ctx.fos = 1
         self.ctx.dealias_all()
+        if self.settings.variant is None:
+            self.ctx.autotune()
 
     def _init_scalars(self):
         """init_scalars.f90: only type-0 (uniform mean gradient, zero initial field) is generated."""
@@ -197,7 +231,8 @@ class Simulation:
             if c.les_model == 2 and it % c.iprint1 == 0:
                 self._les_gp(it, t)
             self.time += c.dt
-            if not math.isfinite(courant) or (it % c.iprint1 == 0 and self.ctx.nonfinite() > 0):
+            if not math.isfinite(courant) or \
+                    (self.settings.nonfinite_check and it % c.iprint1 == 0 and self.ctx.nonfinite() > 0):
                 self.log.append(f"ITIME={it:6d}   non-finite state")
                 return self.exit(-2)
             if it % c.iprint2 == 0:
@@ -237,15 +272,17 @@ class Simulation:
 
 
 def main(argv=None):
-    """`python -m hit3d_b200.driver <run_name> [--workdir D] [--precision 0|1]`:
-    read <run_name>.in, run to ITMAX/TMAX/stop/runlimit, write the reference's files."""
+    """`python -m hit3d_b200.driver <run_name> [--workdir D] [--precision 0|1] [--device I]`:
+    read <run_name>.in and <run_name>.gpu.in, run to ITMAX/TMAX/stop/runlimit,
+    write the reference's files.  --precision and --device override the .gpu.in file."""
     import argparse
     ap = argparse.ArgumentParser(description=main.__doc__)
     ap.add_argument("run_name")
     ap.add_argument("--workdir", default=".")
-    ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--precision", type=int, choices=(0, 1), default=None)
+    ap.add_argument("--device", type=int, default=None)
     a = ap.parse_args(argv)
-    sim = Simulation(a.run_name, workdir=a.workdir, precision=a.precision)
+    sim = Simulation(a.run_name, workdir=a.workdir, precision=a.precision, device=a.device)
     sim.begin()
     reason = sim.run()
     print(f"exit reason {reason} at ITIME={sim.itime}, TIME={sim.time:.6f}")

@@ -141,3 +141,45 @@ def test_non_finite_state_is_detected_on_the_device(tmp_path):
     # the Courant maximum (fmax) passes over NaN, so the statistics step finds it
     assert sim.run() == -2 and sim.itime == 10
     assert not any(n.startswith("decay64_.64.") for n in os.listdir(wd))
+
+
+def test_sidecar_runs_the_learned_closure_with_fixed_settings(tmp_path):
+    """<run>.gpu.in turns an unmodified .in file into a learned-closure run in
+    the FP32 form with a fixed launch shape and no pruning; the state equals a
+    Context driven with the same settings directly."""
+    from hit3d_b200 import Context
+    from hit3d_b200.driver import Simulation
+    from hit3d_b200.params import read_input_file
+    from oracle import mlp_oracle as mo
+    wd = str(tmp_path)
+    # the sample input without its passive scalars (LES runs here carry none)
+    text = open(os.path.join(GOLDEN, "decay64_.in")).read()
+    text = text.replace("2\t\tnums, # of passive scalars", "0\t\tnums, # of passive scalars")
+    with open(os.path.join(wd, "decay64_.in"), "w") as fh:
+        fh.write(text)
+    w = mo.bf16_bits(mo.bf16_round(mo.init_params(4) * 0.05))
+    np.save(os.path.join(wd, "closure.npy"), w)
+    delta = 4 * np.pi / 64
+    with open(os.path.join(wd, "decay64_.gpu.in"), "w") as fh:
+        fh.write(f"precision = 1\npruning = off\nvariant = 5\nles_model = 20\nles_mlp = closure.npy\n"
+                 f"les_mlp_delta = {delta!r}\nles_mlp_kernel = 1\n")
+    sim = Simulation("decay64_", wd)
+    assert sim.cfg.les_model == 20 and sim.settings.precision == 1 and not sim.ctx.pruned
+    sim.begin()
+    assert sim.run(max_steps=4) is None and sim.itime == 4
+    got = sim.ctx.download_fields()
+    assert np.isfinite(got).all()
+
+    cfg = read_input_file(os.path.join(wd, "decay64_.in"))
+    cfg.les_model = 20
+    c = Context(cfg.to_params(precision=1))
+    c.set_pruning(False)
+    c.set_variant(5)
+    c.les_set_mlp(w, delta, clip=True, kernel=1)
+    assert cfg.n_scalars == 0
+    c.init_velocity(cfg.rn1, cfg.isp_type, cfg.peak_wavenum, float(cfg.ir_exp))
+    c.fov = c.fos = 1
+    c.dealias_all()
+    c.step(4)
+    assert np.array_equal(c.download_fields(), got)
+    c.close()

@@ -122,3 +122,43 @@ def test_spectral_truncate_maps_modes_between_grids():
     want = ref_layout(n)
     want[..., n // 2 * 2:] = 0.0  # kx Nyquist column is not carried over
     assert np.abs(got - want).max() < 1e-9 * np.abs(want).max()
+
+
+def test_sidecar_keys_and_defaults(tmp_path):
+    from hit3d_b200.sidecar import GpuSettings, parse_sidecar, read_sidecar
+    assert read_sidecar(str(tmp_path), "nosuchrun") == GpuSettings()
+    s = parse_sidecar("""
+        # settings beyond the .in file
+        precision = 1
+        Pruning = off       # keys are case-insensitive
+        variant = 5
+        device = 0
+        c_smag = 0.16
+        les_model = 20
+        les_mlp = closure.npy
+        les_mlp_delta = 0.39
+        les_mlp_clip = off
+        les_mlp_kernel = 0
+        nonfinite_check = off
+    """)
+    assert (s.precision, s.pruning, s.variant, s.c_smag, s.les_model, s.les_mlp) == (1, False, 5, 0.16, 20, "closure.npy")
+    assert (s.les_mlp_delta, s.les_mlp_clip, s.les_mlp_kernel, s.nonfinite_check) == (0.39, False, 0, False)
+    assert parse_sidecar("variant = auto").variant is None
+
+
+@pytest.mark.parametrize("text,msg", [
+    ("precision = 2", "precision"),
+    ("speed = 11", "unknown key"),
+    ("variant = 8", "variant"),
+    ("pruning = maybe", "on/off"),
+    ("precision", "key = value"),
+    ("precision = 1\nprecision = 0", "twice"),
+    ("c_smag = -0.1", "positive"),
+    ("les_model = 3", "not supported"),
+    ("les_model = 20", "les_mlp"),
+    ("device =", "no value"),
+])
+def test_sidecar_errors_name_the_line(text, msg):
+    from hit3d_b200.sidecar import SidecarError, parse_sidecar
+    with pytest.raises(SidecarError, match=msg):
+        parse_sidecar(text, "run.gpu.in")
