@@ -84,7 +84,9 @@ template <typename T, int L, int V> struct RowCfgV {
 //   4: register-resident kernel (k_xfused_reg), 1024/L pairs x 128 threads
 //   5, 6, 7: lockstep kernel (k_xfused_ms), forward transforms in groups of 3 / 2 / 1,
 //            the last with registers capped for 3 (FP64) or 4 (FP32) CTAs per SM
-constexpr int kFusedVariants = 8;
+//   8, 9, 10: staged lockstep kernel (k_xfused_st), the same three groupings,
+//            each CTA walking tiles with the next tile's input prefetched
+constexpr int kFusedVariants = HIT3D_FUSED_VARIANTS;
 
 // Raise a kernel's dynamic shared-memory limit once per kernel and device, so
 // that steps recorded into a CUDA graph later make no attribute calls.
@@ -349,9 +351,45 @@ static int xfused_ms_L(hit3d_ctx *c, FusedArgs a)
     H3D_LAUNCH_CHECK();
     return 0;
 }
+// staged lockstep kernel: a grid of the CTAs that fit at once, each walking tiles
+// with the next tile's input rows prefetched into shared memory
+template <typename T, template <class> class OP, int L, int GF, int MINB>
+static int xfused_st_L(hit3d_ctx *c, FusedArgs a)
+{
+    using RC = RowCfg<T, L>;
+    constexpr int NIN = OP<T>::NIN;
+    constexpr int NB = NIN > GF ? NIN : GF;
+    auto k = k_xfused_st<T, L, RC::TC, RC::NT, T, OP<T>, GF, MINB>;
+    for (int f = 0; f < NIN; f++)
+        if (reinterpret_cast<uintptr_t>(a.in[f]) % 16 != 0)
+            return h3d_set_error_msg(-1, "fused x pass: input field not 16-byte aligned");
+    if ((a.pitch * (int64_t)sizeof(cx<T>)) % 16 != 0)
+        return h3d_set_error_msg(-1, "fused x pass: row pitch not a multiple of 16 bytes");
+    auto stage_bytes = [&](int lim) {
+        return (size_t)NIN * 2 * RC::TC * StageRow<T>::chunks(lim) * StageRow<T>::PER * sizeof(cx<T>);
+    };
+    const int lim = a.kx_lim > 0 ? a.kx_lim : L / 2 + 1;
+    const size_t soff = (NB * RC::SMEM + 15) / 16 * 16;  // the stage starts on a 16-byte boundary
+    const size_t smax = soff + stage_bytes(L / 2 + 1), smem = soff + stage_bytes(lim);
+    H3D_TRY(set_smem(k, smax));
+    // CTAs per SM: the register cap of the kernel, or fewer if shared memory says so
+    // (233472 bytes per SM, 1 KB reserved per CTA)
+    int per_sm = (int)(233472 / (smem + 1024));
+    per_sm = per_sm < MINB ? per_sm : MINB;
+    if (per_sm < 1) return h3d_set_error_msg(-1, "fused x pass: stage does not fit in shared memory");
+    const int tiles = (a.npairs + RC::TC - 1) / RC::TC;
+    int grid = c->nsm * per_sm;
+    grid = grid < tiles ? grid : tiles;
+    k<<<dim3(grid), RC::NT, smem, c->st>>>(a, twid<T>(c));
+    H3D_LAUNCH_CHECK();
+    return 0;
+}
 template <typename T, template <class> class OP, int L> static int xfused_L(hit3d_ctx *c, FusedArgs a)
 {
     if constexpr (OP<T>::NIN <= 3) {
+        if (c->xcfg == 8) return xfused_st_L<T, OP, L, 3, 2>(c, a);
+        if (c->xcfg == 9) return xfused_st_L<T, OP, L, 2, 2>(c, a);
+        if (c->xcfg == 10) return xfused_st_L<T, OP, L, 1, sizeof(T) == 4 ? 4 : 3>(c, a);
         if (c->xcfg == 5) return xfused_ms_L<T, OP, L, 3>(c, a);
         if (c->xcfg == 6) return xfused_ms_L<T, OP, L, 2>(c, a);
         if (c->xcfg == 7) return xfused_ms_L<T, OP, L, 1, sizeof(T) == 4 ? 4 : 3>(c, a);

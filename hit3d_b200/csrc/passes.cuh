@@ -659,6 +659,176 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_ms(const FusedArgs a, const
     }
 }
 
+// Staged lockstep form: each CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x,
+// ... (grid = the CTAs resident at once).  The kx < lim columns of the next
+// tile's input rows are copied into a shared-memory stage with cp.async while
+// the current tile is transformed, so the global-load latency that dominates
+// k_xfused_ms at its low occupancy overlaps the FFT work.  Stage layout:
+// [f][row 0..2 TC)[RS elements], RS = 16-byte chunks per row; rows of a pair
+// beyond npairs are neither copied nor read.  Requires 16-byte aligned input
+// fields and a pitch that is a multiple of 16 bytes (checked by the host).
+H3D_D void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+H3D_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+H3D_D void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <typename TS> struct StageRow {
+    static constexpr int PER = 16 / (int)sizeof(cx<TS>);  // elements per 16-byte chunk
+    static H3D_HD int chunks(int lim) { return (lim + PER - 1) / PER; }
+};
+
+template <typename TS, int NIN, int TC, int NT>
+H3D_D void stage_issue(const FusedArgs &a, cx<TS> *st, int pair0, int nch)
+{
+    constexpr int PER = StageRow<TS>::PER;
+    const int rs = nch * PER;
+    const int total = NIN * 2 * TC * nch;
+    for (int q = threadIdx.x; q < total; q += NT) {
+        const int ch = q % nch, rr = q / nch;
+        const int r = rr % (2 * TC), f = rr / (2 * TC);
+        if (pair0 + r / 2 >= a.npairs) continue;
+        const cx<TS> *src = reinterpret_cast<const cx<TS> *>(a.in[f]) + (int64_t)(2 * pair0 + r) * a.pitch + ch * PER;
+        cp_async16(st + (f * 2 * TC + r) * rs + ch * PER, src);
+    }
+    cp_async_commit();
+}
+
+template <typename T, int L, int TC, int NT, typename TS, class OP, int GF, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) k_xfused_st(const FusedArgs a, const cx<T> *__restrict__ tw)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    using FI = RowFFT<T, L, TC, NT, true>;
+    using FF = RowFFT<T, L, TC, NT, false>;
+    static_assert(FI::NOUT == FF::NIN, "slot hand-off mismatch");
+    constexpr int NP = FI::NOUT;
+    constexpr int E = Lay<L, TC, true>::elems;
+    constexpr int NB = OP::NIN > GF ? OP::NIN : GF;
+    constexpr size_t SOFF = ((size_t)NB * E * sizeof(cx<T>) + 15) / 16 * 16;  // cp.async wants 16-byte targets
+    cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
+    cx<TS> *st = reinterpret_cast<cx<TS> *>(smraw + SOFF);
+    const T norm = (T)a.norm;
+    const int lim = a.kx_lim > 0 ? a.kx_lim : L / 2 + 1;
+    const int nch = StageRow<TS>::chunks(lim);
+    const int rs = nch * StageRow<TS>::PER;
+    const int ntiles = (a.npairs + TC - 1) / TC;
+    OP op{(T)a.p0, (T)a.p1};
+    if ((int)blockIdx.x < ntiles) stage_issue<TS, OP::NIN, TC, NT>(a, st, blockIdx.x * TC, nch);
+
+#pragma unroll 1
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int pair0 = tile * TC;
+        cx<T> phys[OP::NIN][NP];
+        {
+            cp_async_wait_all();
+            __syncthreads();
+            cx<T> in[OP::NIN][FI::NIN];
+#pragma unroll
+            for (int f = 0; f < OP::NIN; f++) {
+#pragma unroll
+                for (int i = 0; i < FI::NB0; i++)
+#pragma unroll
+                    for (int m = 0; m < FI::R0; m++) {
+                        int c, p;
+                        if (FI::in_slot(i, m, c, p) && pair0 + c < a.npairs) {
+                            const cx<TS> *A = st + (f * 2 * TC + 2 * c) * rs;
+                            in[f][i * FI::R0 + m] = load_packed<T, L, TS>(A, A + rs, p, lim);
+                        } else in[f][i * FI::R0 + m] = mk<T>(0, 0);
+                    }
+#pragma unroll
+                for (int q = 0; q < NP; q++) phys[f][q] = mk<T>(0, 0);
+            }
+            __syncthreads();  // the stage is free: prefetch the next tile
+            if (tile + (int)gridDim.x < ntiles) stage_issue<TS, OP::NIN, TC, NT>(a, st, pair0 + gridDim.x * TC, nch);
+            FI::template run_multi<OP::NIN>(in, sm, phys, tw);
+        }
+#pragma unroll
+        for (int f = 0; f < OP::NIN; f++)
+#pragma unroll
+            for (int q = 0; q < NP; q++) phys[f][q] = mk<T>(phys[f][q].x * norm, phys[f][q].y * norm);
+        __syncthreads();
+        if (a.phys != nullptr) {
+            double *pb = a.phys;
+#pragma unroll
+            for (int i = 0; i < FI::NBL; i++)
+#pragma unroll
+                for (int m = 0; m < FI::RL; m++) {
+                    int c, p;
+                    if (FI::out_slot(i, m, c, p) && pair0 + c < a.npairs) {
+                        int64_t r = 2 * (pair0 + c);
+#pragma unroll
+                        for (int f = 0; f < OP::NPHYS; f++) {
+                            pb[f * a.phys_fs + r * a.phys_pitch + p] = (double)phys[f][i * FI::RL + m].x;
+                            pb[f * a.phys_fs + (r + 1) * a.phys_pitch + p] = (double)phys[f][i * FI::RL + m].y;
+                        }
+                    }
+                }
+        }
+        if (a.cmax != nullptr) {
+            double cm = 0.0;
+#pragma unroll
+            for (int q = 0; q < NP; q++) {
+                T va[OP::NIN], vb[OP::NIN];
+#pragma unroll
+                for (int f = 0; f < OP::NIN; f++) { va[f] = phys[f][q].x; vb[f] = phys[f][q].y; }
+                cm = fmax(cm, (double)op.cour(va));
+                cm = fmax(cm, (double)op.cour(vb));
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, off));
+            if ((threadIdx.x & 31) == 0) atomicMax(a.cmax, (unsigned long long)__double_as_longlong(cm));
+        }
+        cx<T> aux[NP];
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+            T va[OP::NIN], vb[OP::NIN];
+#pragma unroll
+            for (int f = 0; f < OP::NIN; f++) { va[f] = phys[f][q].x; vb[f] = phys[f][q].y; }
+            aux[q] = mk<T>(op.aux(va), op.aux(vb));
+        }
+        using LY = typename FF::LY;
+        constexpr int NG = (OP::NOUT + GF - 1) / GF;
+#pragma unroll 1
+        for (int g = 0; g < NG; g++) {
+            cx<T> in[GF][FF::NIN], out[GF][FF::NOUT];
+#pragma unroll
+            for (int gf = 0; gf < GF; gf++) {
+                const int o = g * GF + gf;
+#pragma unroll
+                for (int q = 0; q < NP; q++) {
+                    T va[OP::NIN], vb[OP::NIN];
+#pragma unroll
+                    for (int f = 0; f < OP::NIN; f++) { va[f] = phys[f][q].x; vb[f] = phys[f][q].y; }
+                    in[gf][q] = o < OP::NOUT ? mk<T>(op.out(o, va, aux[q].x), op.out(o, vb, aux[q].y)) : mk<T>(0, 0);
+                }
+            }
+            FF::template run_multi<GF>(in, sm, out, tw);
+            __syncthreads();
+#pragma unroll
+            for (int gf = 0; gf < GF; gf++)
+#pragma unroll
+                for (int i = 0; i < FF::NBL; i++)
+#pragma unroll
+                    for (int m = 0; m < FF::RL; m++) {
+                        int c, p;
+                        if (FF::out_slot(i, m, c, p)) sm[gf * E + LY::idx(c, p)] = out[gf][i * FF::RL + m];
+                    }
+            __syncthreads();
+#pragma unroll
+            for (int gf = 0; gf < GF; gf++) {
+                const int o = g * GF + gf;
+                if (o < OP::NOUT)
+                    store_split<T, L, TC, NT, TS>(sm + gf * E, reinterpret_cast<cx<TS> *>(a.out[o]), a.pitch, pair0,
+                                                  a.npairs, lim);
+            }
+            __syncthreads();
+        }
+    }
+    cp_async_wait_all();
+}
+
 // velocity products (rhs_velocity.f90:56-72): uu uv uw vv vw ww; Courant |u|+|v|+|w|
 template <typename T> struct OpVel {
     static constexpr int NIN = 3, NOUT = 6, NPHYS = 3;

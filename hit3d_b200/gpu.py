@@ -22,6 +22,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libhit3d_gpu.so")
 MAX_SCALARS = 8
 LES_LEARNED = 20  # les_model of the learned closure (HIT3D_LES_LEARNED)
+N_VARIANTS = 11  # launch-shape variants of the fused x pass (HIT3D_FUSED_VARIANTS)
 _lib = None
 
 
@@ -256,7 +257,7 @@ class Context:
     def autotune(self):
         """Pick the fastest launch shape of the fused x pass; returns (variant, ms per variant)."""
         v = C.c_int32(0)
-        ms = np.full(8, np.nan)
+        ms = np.full(N_VARIANTS, np.nan)
         _check(lib().hit3d_gpu_autotune(self._h, C.byref(v), _ptr(ms)), "autotune")
         return v.value, [x for x in ms.tolist() if x == x]
 

@@ -12,7 +12,7 @@ error that names the line, as a bad `.in` line is in the reference.
 
   precision       0 | 1        FP64 transforms | FP32 transforms (FP64 state)
   pruning         on | off     skip work on the modes the 2/3 rule discards
-  variant         auto | 0..7  launch shape of the fused row pass; auto tunes
+  variant         auto | 0..10 launch shape of the fused row pass; auto tunes
   device          int          CUDA device ordinal
   c_smag          float        Smagorinsky constant (the reference fixes 0.18)
   les_model       int          overrides the `.in` LES model; 20 is the learned
@@ -77,7 +77,8 @@ def _choice(*allowed):
 def _variant(v: str) -> Optional[int]:
     if v.lower() == "auto":
         return None
-    return _choice(*range(8))(v)
+    from .gpu import N_VARIANTS
+    return _choice(*range(N_VARIANTS))(v)
 
 
 def _les_model(v: str) -> int:

@@ -111,9 +111,10 @@ int hit3d_gpu_step_profile(hit3d_ctx *ctx, int32_t nsteps, int32_t *fov, int32_t
 /* Launch-shape tuner (no reference counterpart): times every launch-shape
  * variant of the fused x pass (row pairs per CTA, threads per CTA) on this
  * context's own work buffers and keeps the fastest; the state is not touched.
- * *variant receives the choice, ms[0..8) the time of each variant (unused
- * entries are left untouched).
+ * *variant receives the choice, ms[0..HIT3D_FUSED_VARIANTS) the time of each
+ * variant (unused entries are left untouched).
  * hit3d_gpu_set_variant fixes a variant by hand. */
+#define HIT3D_FUSED_VARIANTS 11
 int hit3d_gpu_autotune(hit3d_ctx *ctx, int32_t *variant, double *ms);
 int hit3d_gpu_set_variant(hit3d_ctx *ctx, int32_t variant);
 

@@ -19,7 +19,8 @@ def test_variants_agree(n, precision, case):
     else:
         kw.update(les_model=1)
     outs = []
-    for v in range(8):
+    from hit3d_b200.gpu import N_VARIANTS
+    for v in range(N_VARIANTS):
         c = Context(Params(**kw))
         c.set_variant(v)
         c.init_velocity(RN1, 2, 4.0, 2.0)
@@ -35,6 +36,7 @@ def test_variants_agree(n, precision, case):
 def test_tuner_picks_a_valid_variant():
     from hit3d_b200 import Context, Params
     c = Context(Params(nx=64, flow_type=1, kfmax=2, nu=1.0 / 800.0, dt=0.002))
+    from hit3d_b200.gpu import N_VARIANTS
     v, ms = c.autotune()
-    assert 0 <= v < 8 and len(ms) == 8 and all(x > 0 for x in ms)
+    assert 0 <= v < N_VARIANTS and len(ms) == N_VARIANTS and all(x > 0 for x in ms)
     assert ms[v] == min(ms)
