@@ -467,6 +467,11 @@ struct Prof {
 
 // ---------------------------------------------------------------------------
 // one time step
+// LES-related transported fields (m_les.f90:111-137): k_sgs for the dynamic
+// localization model (2); k_sgs, (B T_B) and (eps T_eps) with the lag model (3)
+static int les_nles(int model) { return model == 2 ? 1 : model == 3 ? 3 : 0; }
+static bool les_dlm(int model) { return model == 2 || model == 3; }
+
 // ---------------------------------------------------------------------------
 // 2/3-rule pruning for the duration of one step (reset on every exit path)
 struct PruneScope {
@@ -508,7 +513,8 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     auto Wf = [&](int i) { return W + i * wfs; };
     const int ns = c->int_scalars ? c->nsc : 0;
     const int nprod = 6 + 3 * ns;
-    const bool les = p.les_model == 1, les_mlp = p.les_model == HIT3D_LES_LEARNED, dlm = p.les_model == 2;
+    const bool les = p.les_model == 1, les_mlp = p.les_model == HIT3D_LES_LEARNED, dlm = les_dlm(p.les_model);
+    const bool lag = p.les_model == 3;
 
     StepArgs a;
     memset(&a, 0, sizeof a);
@@ -517,11 +523,17 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     a.flow_type = p.flow_type; a.kfmax = p.kfmax; a.famp = p.famp; a.fenergy = c->d_fen; a.nscal = ns;
     a.kc = c->kc_active;  // pruned state: the updates visit only the kept modes
     for (int s = 0; s < p.n_scalars; s++) { a.pe[s] = p.nu / p.sc[s]; a.stype[s] = p.scalar_type[s]; }
-    if (dlm) {
-        // k_sgs: Schmidt number one (m_les.f90:372-391), no mean-gradient source
-        a.pe[p.n_scalars] = p.nu / 1.0;
-        a.stype[p.n_scalars] = -1;
+    for (int j = 0; j < les_nles(p.les_model); j++) {
+        // LES fields: Schmidt number one (m_les.f90:372-391), no mean-gradient source
+        a.pe[p.n_scalars + j] = p.nu / 1.0;
+        a.stype[p.n_scalars + j] = -1;
     }
+    // work fields of the dynamic localization models after the nprod products:
+    // model 2: [0,6) strain -> tau, [6] k cube -> k source, [7,10) grad k -> fluxes
+    // model 3: [0,6) strain -> tau, [6] (B T_B) -> k source, [7] (eps T_eps) -> B T_B
+    //          source, [8,17) gradients of the three -> fluxes, [17] eps T_eps source
+    // then k_sgs truncated (kf) and nu_t (nutf)
+    const int kf = nprod + (lag ? 18 : 10), nutf = kf + 1;
 
     MARK(7);
     if constexpr (std::is_same<T, double>::value) {
@@ -530,7 +542,6 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
             // field replaces the state when its minimum is negative
             // (les_get_turb_visc_dlm, m_les.f90:1313-1388)
             MARK(6);
-            const int kf = nprod + 10, nutf = nprod + 11;
             double2 *K = c->U + 3 * c->fs64;
             c->k2max = (double)c->kmax * (double)c->kmax;
             H3D_TRY(zinv<T>(c, 1, PRE_TRUNC, 0, K, c->fs64, Wf(kf), wfs, wp));
@@ -626,7 +637,32 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
         }
         const cx<T> *les_src = nullptr, *les_flux = nullptr;
         if constexpr (std::is_same<T, double>::value) {
-            if (dlm) {
+            if (lag) {
+                // dynamic localization model with the lag model for the dissipation
+                // (les_model 3; m_les.f90:720-724, 1422-1561, 1629-1684, 1041-1091)
+                MARK(6);
+                const int t0 = nprod;
+                H3D_TRY(zinv<T>(c, 3, PRE_STRAIN_A, 0, c->U, c->fs64, Wf(t0), wfs, wp));
+                H3D_TRY(zinv<T>(c, 3, PRE_STRAIN_B, 0, c->U, c->fs64, Wf(t0 + 3), wfs, wp));
+                H3D_TRY(zinv<T>(c, 2, PRE_COPY, 0, c->U + 4 * c->fs64, c->fs64, Wf(t0 + 6), wfs, wp));
+                for (int j = 0; j < 3; j++)
+                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, 3 + j, c->U, c->fs64, Wf(t0 + 8 + 3 * j), wfs, wp));
+                H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, 17));
+                H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, 17));
+                k_dll_phys<<<pw_grid(c), 256, 0, c->st>>>(
+                    c->n, 2 * (int64_t)wp, 2 * wfs, c->dx, 1.0, reinterpret_cast<const double *>(Wf(nutf)),
+                    reinterpret_cast<double *>(Wf(t0)), reinterpret_cast<double *>(Wf(t0 + 6)),
+                    reinterpret_cast<double *>(Wf(t0 + 7)), reinterpret_cast<double *>(Wf(t0 + 8)),
+                    reinterpret_cast<double *>(Wf(t0 + 17)), c->d_kmin + 8);
+                H3D_LAUNCH_CHECK();
+                k_dlm_stats<<<1, 32, 0, c->st>>>((int)pw_grid(c).x, 1.0 / ((double)c->n * c->n * c->n),
+                                                 c->U + 3 * c->fs64, c->d_kmin + 8, c->d_kmin + 4);
+                H3D_LAUNCH_CHECK();
+                H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, 18));
+                H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, 18));
+                H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, 18));
+                tau = Wf(t0);
+            } else if (dlm) {
                 // dynamic localization model: tau = -2 nu_t S for the velocities, and
                 // for k_sgs the production 2 nu_t S:S, the dissipation k^(3/2)/Delta
                 // and the turbulent fluxes nu_t dk/dx_i (m_les.f90:902-1018,
@@ -640,7 +676,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, 10));
                 H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, 10));
                 k_dlm_phys<<<pw_grid(c), 256, 0, c->st>>>(
-                    c->n, 2 * (int64_t)wp, 2 * wfs, c->dx, reinterpret_cast<const double *>(Wf(nprod + 11)),
+                    c->n, 2 * (int64_t)wp, 2 * wfs, c->dx, reinterpret_cast<const double *>(Wf(nutf)),
                     reinterpret_cast<double *>(Wf(t0)), reinterpret_cast<double *>(Wf(t0 + 6)),
                     reinterpret_cast<double *>(Wf(t0 + 7)), c->d_kmin + 8);
                 H3D_LAUNCH_CHECK();
@@ -675,10 +711,19 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
         MARK(5);
         if (p.dealias == 0) {
             for (int s = 0; s < ns; s++) {
-                const bool kles = dlm && s == p.n_scalars;
+                // sources and turbulent fluxes of the LES fields (layout above)
+                const int j = s - p.n_scalars;
+                const cx<T> *src = nullptr, *flux = nullptr;
+                if (lag && j >= 0) {
+                    src = Wf(nprod + (j == 0 ? 6 : j == 1 ? 7 : 17));
+                    flux = Wf(nprod + 8 + 3 * j);
+                } else if (dlm && j == 0) {
+                    src = les_src;
+                    flux = les_flux;
+                }
                 k_scalar<T><<<pw_grid(c), 256, 0, c->st>>>(a, 0, s, c->dx, Wf(6 + 3 * s), nullptr, c->U,
                                                             c->U + (3 + s) * c->fs64, c->RO + (3 + s) * c->fs64,
-                                                            kles ? les_src : nullptr, kles ? les_flux : nullptr);
+                                                            src, flux);
                 H3D_LAUNCH_CHECK();
             }
             k_update_vel_23<T><<<pw_grid(c), 256, 0, c->st>>>(a, Wf(0), tau, c->U, c->RO);
@@ -764,11 +809,12 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     if (p->dealias != 0 && p->dealias != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: wrong dealias flag");
     if (p->flow_type == 1 && p->force_type != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: WRONG FORCE TYPE");
     if (p->flow_type == 1 && (p->kfmax < 1 || p->kfmax > 15)) return h3d_set_error_msg(-1, "hit3d_gpu_init: kfmax must be in 1..15");
-    if (p->les_model != 0 && p->les_model != 1 && p->les_model != 2 && p->les_model != HIT3D_LES_LEARNED)
+    if (p->les_model != 0 && p->les_model != 1 && !les_dlm(p->les_model) && p->les_model != HIT3D_LES_LEARNED)
         return h3d_set_error_msg(-1, "hit3d_gpu_init: les_model must be 0 (none), 1 (Smagorinsky), 2 (dynamic "
-                                     "localization) or 20 (learned closure); the reference's models 3-10 are not supported");
-    if (p->les_model == 2 && p->precision != 0)
-        return h3d_set_error_msg(-1, "hit3d_gpu_init: the dynamic localization model (les_model 2) runs with FP64 transforms");
+                                     "localization), 3 (dynamic localization with the lag model) or 20 (learned "
+                                     "closure); the reference's models 4-10 are not supported");
+    if (les_dlm(p->les_model) && p->precision != 0)
+        return h3d_set_error_msg(-1, "hit3d_gpu_init: the dynamic localization models (les_model 2, 3) run with FP64 transforms");
     if (p->les_model != 0 && p->n_scalars > 0) return h3d_set_error_msg(-1, "hit3d_gpu_init: LES with scalars is not supported");
     if (p->precision != 0 && p->precision != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: precision must be 0 or 1");
     for (int s = 0; s < p->n_scalars; s++) {
@@ -787,14 +833,13 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     c->P32 = (int)round_up(c->nh, 16);
     c->fs64 = (int64_t)c->n * c->n * c->P64;
     c->fs32 = (int64_t)c->n * c->n * c->P32;
-    // transported fields beyond velocity: passive scalars, then k_sgs of the
-    // dynamic localization model (m_les.f90:111-123, n_les = 1)
-    c->nsc = p->n_scalars + (p->les_model == 2 ? 1 : 0);
+    // transported fields beyond velocity: passive scalars, then the LES fields
+    c->nsc = p->n_scalars + les_nles(p->les_model);
     c->kmax = c->p.dealias == 0 ? c->n / 3 : (int)floor((double)c->n / 3.0 * sqrt(2.0));
     c->dx = 2.0 * (4.0 * atan(1.0)) / (double)c->n;
     c->int_scalars = c->nsc > 0;
     c->xcfg = 4;  // register-resident fused x pass, the tuner's usual pick
-    c->prune_on = p->les_model != 2;  // a clipped k_sgs brings modes beyond N/3 into the state
+    c->prune_on = !les_dlm(p->les_model);  // a clipped k_sgs brings modes beyond N/3 into the state
     c->kc_active = -1;
     cudaDeviceProp prop;
     H3D_CHECK(cudaGetDeviceProperties(&prop, c->dev));
@@ -804,7 +849,8 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     const int nf = 3 + c->nsc;
     const size_t f64 = (size_t)c->fs64 * sizeof(double2);
     c->nw = 6 + 3 * c->nsc +
-            (c->p.les_model == 1 ? 6 : c->p.les_model == HIT3D_LES_LEARNED ? 9 : c->p.les_model == 2 ? 12 : 0);
+            (c->p.les_model == 1 ? 6 : c->p.les_model == HIT3D_LES_LEARNED ? 9 : c->p.les_model == 2 ? 12
+                                                                               : c->p.les_model == 3 ? 20 : 0);
     if (c->p.precision == 0) {
         c->wpitch = c->P64;
         c->wfs = c->fs64;
@@ -851,9 +897,9 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     H3D_CHECK(cudaMemset(c->U, 0, f64 * nf));
     H3D_CHECK(cudaMemset(c->RO, 0, f64 * nf));
     H3D_CHECK(cudaMemset(c->W, 0, wbytes));
-    if (c->p.les_model == 2) {
+    if (les_dlm(c->p.les_model)) {
         // [2] the minimum of k_sgs, [4..8) the les.gp means, [8..) block partial sums
-        if ((rc = ctx_alloc((void **)&c->d_kmin, sizeof(double) * (8 + 2 * (size_t)pw_grid(c).x)))) {
+        if ((rc = ctx_alloc((void **)&c->d_kmin, sizeof(double) * (8 + 3 * (size_t)pw_grid(c).x)))) {
             hit3d_gpu_finalize(c);
             return rc;
         }
@@ -862,6 +908,12 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
         // only the (0,0,0) mode, 0.1 N^3 after the unnormalised transform
         const double2 k0 = make_double2(0.1 * (double)c->n * (double)c->n * (double)c->n, 0.0);
         H3D_CHECK(cudaMemcpy(c->U + 3 * c->fs64, &k0, sizeof k0, cudaMemcpyHostToDevice));
+        if (c->p.les_model == 3) {
+            // (B T_B) = (eps T_eps) = 0.5 k_sgs (m_les.f90:474-479)
+            const double2 h0 = make_double2(0.5 * k0.x, 0.0);
+            H3D_CHECK(cudaMemcpy(c->U + 4 * c->fs64, &h0, sizeof h0, cudaMemcpyHostToDevice));
+            H3D_CHECK(cudaMemcpy(c->U + 5 * c->fs64, &h0, sizeof h0, cudaMemcpyHostToDevice));
+        }
     }
     *out = c;
     return 0;
@@ -1094,8 +1146,8 @@ extern "C" int hit3d_gpu_check_finite(hit3d_ctx *c, int64_t *nonfinite)
 extern "C" int hit3d_gpu_les_stats(hit3d_ctx *c, double *out4)
 {
     if (!c || !out4) return h3d_set_error_msg(-1, "hit3d_gpu_les_stats: null argument");
-    if (c->p.les_model != 2)
-        return h3d_set_error_msg(-1, "hit3d_gpu_les_stats: les.gp quantities exist for les_model 2 only");
+    if (!les_dlm(c->p.les_model))
+        return h3d_set_error_msg(-1, "hit3d_gpu_les_stats: les.gp quantities exist for les_model 2 and 3 only");
     H3D_CHECK(cudaSetDevice(c->dev));
     H3D_CHECK(cudaMemcpyAsync(out4, c->d_kmin + 4, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
     H3D_CHECK(cudaStreamSynchronize(c->st));
@@ -1137,8 +1189,8 @@ extern "C" int hit3d_gpu_set_dt(hit3d_ctx *c, double dt)
 extern "C" int hit3d_gpu_set_scalars_active(hit3d_ctx *c, int32_t on)
 {
     if (!c) return h3d_set_error_msg(-1, "null context");
-    // k_sgs of the dynamic localization model is always transported (rhs_scalars.f90:72-74)
-    c->int_scalars = ((on != 0) && c->nsc > 0) || c->p.les_model == 2;
+    // the LES fields are always transported (rhs_scalars.f90:72-74)
+    c->int_scalars = ((on != 0) && c->nsc > 0) || les_dlm(c->p.les_model);
     return 0;
 }
 

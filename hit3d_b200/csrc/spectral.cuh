@@ -574,8 +574,31 @@ __global__ void k_dlm_commit(int n, int nh, int pitch, const double *__restrict_
 //   KC (k_sgs with the 2/3 rule)      -> 2 nu_t S_ij S_ij - max(KC,0)^1.5 / Delta
 //                                                                    (m_les.f90:1422-1621)
 //   G[0..3) (dk/dx_i)                 -> nu_t dk/dx_i                (m_les.f90:1041-1091)
-// part[2 b], part[2 b + 1]: block b's sums of the production and of the
-// dissipation, for the domain means that les.gp reports (m_les.f90:1536,1617)
+// the three sums of a 256-thread block into part[3 blockIdx.x + 0, 1, 2]
+H3D_D void block_sums3(double a, double b, double d, double *__restrict__ part)
+{
+    __shared__ double sh[3][8];
+    for (int off = 16; off > 0; off >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, off);
+        b += __shfl_xor_sync(0xffffffffu, b, off);
+        d += __shfl_xor_sync(0xffffffffu, d, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sh[0][threadIdx.x >> 5] = a;
+        sh[1][threadIdx.x >> 5] = b;
+        sh[2][threadIdx.x >> 5] = d;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += sh[threadIdx.x][w];
+        part[3 * blockIdx.x + threadIdx.x] = v;
+    }
+}
+
+// part[3 b + 0, 1, 2]: block b's sums of the production, of B (zero here) and
+// of the dissipation, for the domain means that les.gp reports
+// (m_les.f90:1536,1617)
 __global__ void __launch_bounds__(256) k_dlm_phys(int n, int64_t rp, int64_t fs, double delta,
                                                   const double *__restrict__ NUT, double *__restrict__ S,
                                                   double *__restrict__ KC, double *__restrict__ G,
@@ -605,37 +628,79 @@ __global__ void __launch_bounds__(256) k_dlm_phys(int n, int64_t rp, int64_t fs,
 #pragma unroll
         for (int d = 0; d < 3; d++) G[o + d * fs] = G[o + d * fs] * nut;
     }
-    __shared__ double sh[2][8];
-    for (int off = 16; off > 0; off >>= 1) {
-        psum += __shfl_xor_sync(0xffffffffu, psum, off);
-        dsum += __shfl_xor_sync(0xffffffffu, dsum, off);
+    block_sums3(psum, 0.0, dsum, part);
+}
+
+// Dynamic localization model with the lag model for the dissipation
+// (les_model 3; m_les.f90:1422-1561, 1629-1684): per point, from nu_t, the six
+// strain components S, the physical (B T_B) and (eps T_eps) in BT and ET, and
+// the gradients G of k_sgs, (B T_B), (eps T_eps):
+//   |S| = sqrt(2 S:S), B = (B T_B) |S|, eps = max(eps T_eps, 0)^1.5 / (Delta C_T^1.5),
+//   production Pi = 2 nu_t S:S;
+//   sources  k: Pi - eps  -> BT,   B T_B: Pi - B  -> ET,   eps T_eps: B - eps -> S3;
+//   tau = -2 nu_t S in S, fluxes nu_t grad in G (nine fields).
+// part[3 b + 0, 1, 2]: block sums of Pi, B and eps.
+__global__ void __launch_bounds__(256) k_dll_phys(int n, int64_t rp, int64_t fs, double delta, double c_t,
+                                                  const double *__restrict__ NUT, double *__restrict__ S,
+                                                  double *__restrict__ BT, double *__restrict__ ET,
+                                                  double *__restrict__ G, double *__restrict__ S3,
+                                                  double *__restrict__ part)
+{
+    const int64_t np = (int64_t)n * n * n;
+    const double den = delta * pow(c_t, 1.5);
+    double psum = 0.0, bsum = 0.0, dsum = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / n, o = row * rp + (t - row * n);
+        const double nut = NUT[o];
+        double sv[6];
+#pragma unroll
+        for (int c = 0; c < 6; c++) sv[c] = S[o + c * fs];
+        double ss = sv[0] * sv[0];
+        ss = ss + 2.0 * (sv[1] * sv[1]);
+        ss = ss + 2.0 * (sv[2] * sv[2]);
+        ss = ss + sv[3] * sv[3];
+        ss = ss + 2.0 * (sv[4] * sv[4]);
+        ss = ss + sv[5] * sv[5];
+        const double s2 = 2.0 * ss;
+        const double prod = s2 * nut;
+        const double bb = BT[o] * sqrt(s2);
+        const double et = ET[o] > 0.0 ? ET[o] : 0.0;
+        const double eps = pow(et, 1.5) / den;
+        BT[o] = prod - eps;
+        ET[o] = prod - bb;
+        S3[o] = bb - eps;
+        psum += prod;
+        bsum += bb;
+        dsum += eps;
+#pragma unroll
+        for (int c = 0; c < 6; c++) S[o + c * fs] = (-2.0 * nut) * sv[c];
+#pragma unroll
+        for (int d = 0; d < 9; d++) G[o + d * fs] = G[o + d * fs] * nut;
     }
-    if ((threadIdx.x & 31) == 0) { sh[0][threadIdx.x >> 5] = psum; sh[1][threadIdx.x >> 5] = dsum; }
-    __syncthreads();
-    if (threadIdx.x < 2) {
-        double v = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += sh[threadIdx.x][w];
-        part[2 * blockIdx.x + threadIdx.x] = v;
-    }
+    block_sums3(psum, bsum, dsum, part);
 }
 
 // out[0..3] = energy, production, B, dissipation of les.gp (m_les.f90:876-892):
-// the mean k_sgs from its zero mode K0 (unnormalised forward transform), the
-// block sums of k_dlm_phys divided by N^3, and B = 0 (no lag model); one warp,
-// fixed summation order
+// the mean k_sgs from its zero mode K0 (unnormalised forward transform) and the
+// block sums divided by N^3; one warp, fixed summation order
 __global__ void k_dlm_stats(int nblk, double inv_n3, const double2 *__restrict__ K0, const double *__restrict__ part,
                             double *__restrict__ out)
 {
-    double p = 0.0, d = 0.0;
-    for (int b = threadIdx.x; b < nblk; b += 32) { p += part[2 * b]; d += part[2 * b + 1]; }
+    double p = 0.0, b = 0.0, d = 0.0;
+    for (int q = threadIdx.x; q < nblk; q += 32) {
+        p += part[3 * q];
+        b += part[3 * q + 1];
+        d += part[3 * q + 2];
+    }
     for (int off = 16; off > 0; off >>= 1) {
         p += __shfl_xor_sync(0xffffffffu, p, off);
+        b += __shfl_xor_sync(0xffffffffu, b, off);
         d += __shfl_xor_sync(0xffffffffu, d, off);
     }
     if (threadIdx.x == 0) {
         out[0] = K0[0].x * inv_n3;
         out[1] = p * inv_n3;
-        out[2] = 0.0;
+        out[2] = b * inv_n3;
         out[3] = d * inv_n3;
     }
 }

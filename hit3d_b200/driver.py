@@ -19,7 +19,7 @@ import time as _time
 
 import numpy as np
 
-from .gpu import Context
+from .gpu import Context, les_fields
 from .params import RunConfig, read_input_file
 from .restart import read_restart, restart_name, write_real4, write_restart
 from .sidecar import GpuSettings, SidecarError, read_sidecar
@@ -144,8 +144,8 @@ class Simulation:
 
     @property
     def n_les(self) -> int:
-        """LES-related transported fields: k_sgs of the dynamic localization model."""
-        return 1 if self.cfg.les_model == 2 else 0
+        """LES-related transported fields of the dynamic localization models."""
+        return les_fields(self.cfg.les_model)
 
     def write_restart(self):
         nums = self.cfg.n_scalars if self.int_scalars else 0
@@ -228,7 +228,7 @@ class Simulation:
                     if it % c.iprint1 == 0:
                         self.stat_main()
             courant = self.ctx.step(1)
-            if c.les_model == 2 and it % c.iprint1 == 0:
+            if self.n_les > 0 and it % c.iprint1 == 0:
                 self._les_gp(it, t)
             self.time += c.dt
             if not math.isfinite(courant) or \

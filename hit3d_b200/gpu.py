@@ -23,6 +23,14 @@ LIB_PATH = os.path.join(_HERE, "libhit3d_gpu.so")
 MAX_SCALARS = 8
 LES_LEARNED = 20  # les_model of the learned closure (HIT3D_LES_LEARNED)
 N_VARIANTS = 11  # launch-shape variants of the fused x pass (HIT3D_FUSED_VARIANTS)
+
+
+def les_fields(les_model: int) -> int:
+    """LES-related transported fields (m_les.f90:111-137): k_sgs for the dynamic
+    localization model (2); k_sgs, (B T_B), (eps T_eps) with the lag model (3)."""
+    return {2: 1, 3: 3}.get(int(les_model), 0)
+
+
 _lib = None
 
 
@@ -180,7 +188,7 @@ class Context:
         self.params = params
         self.n = params.nx
         # k_sgs of the dynamic localization model is state field 3 + n_scalars
-        self.nfields = 3 + params.n_scalars + (1 if params.les_model == 2 else 0)
+        self.nfields = 3 + params.n_scalars + les_fields(params.les_model)
         self.kmax = params.kmax
         self._owned = _handle is None
         if _handle is None:

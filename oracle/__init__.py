@@ -139,7 +139,7 @@ class Oracle:
         if not self._p:
             raise MemoryError("oracle_create failed")
         self.n, self.nscal = n, nscal
-        self.nles = 1 if les_model == 2 else 0   # k_sgs of the dynamic localization model
+        self.nles = {2: 1, 3: 3}.get(les_model, 0)   # LES fields of the dynamic localization models
         self.nu = nu
         self.kmax = L.oracle_kmax(self._p)
         self.fsz = (n + 2) * n * n

@@ -394,15 +394,16 @@ oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_
     o->les_model = les_model; o->c_smag = c_smag;
     o->dx = 2.0 * (4.0 * atan(1.0)) / (double)n;
     o->les_delta = o->dx;
-    /* LES-related transported quantities: k_sgs for the DLM (m_les.f90:111-123),
+    /* LES-related transported quantities: k_sgs for the DLM (m_les.f90:111-123);
+     * k_sgs, (B T_B), (eps T_eps) with the lag model (m_les.f90:124-137); all
      * with Schmidt number one (m_les.f90:372-391) */
-    o->nles = les_model == 2 ? 1 : 0;
+    o->nles = les_model == 2 ? 1 : les_model == 3 ? 3 : 0;
     if (o->nles && nscal > 0) { free(o); return NULL; }
     /* kmax (m_parameters.f90:123-131) */
     if (dealias == 0) o->kmax = n / 3;
     else o->kmax = (int)floor((double)n / 3.0 * sqrt(2.0));
     for (int s = 0; s < nscal; s++) { o->pe[s] = nu / sc[s]; o->scalar_type[s] = scalar_type[s]; }
-    if (o->nles) o->pe[nscal] = nu / 1.0;
+    for (int j = 0; j < o->nles; j++) o->pe[nscal + j] = nu / 1.0;
     o->fsz = (size_t)(n + 2) * n * n;
     o->nwrk = 7;
     if (6 + nscal + o->nles > o->nwrk) o->nwrk = 6 + nscal + o->nles;
@@ -447,6 +448,8 @@ oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_
     /* m_les_dlm_k_init (m_les.f90:1394-1413): k_sgs = 0.1 in physical space,
      * i.e. only the (0,0,0) mode, 0.1 N^3 after the unnormalised transform */
     if (o->nles) F(o, 3 + nscal)[0] = 0.1 * (double)n * (double)n * (double)n;
+    /* lag model: (B T_B) = (eps T_eps) = 0.5 k_sgs (m_les.f90:474-479) */
+    if (o->nles == 3) F(o, 4 + nscal)[0] = F(o, 5 + nscal)[0] = 0.5 * F(o, 3 + nscal)[0];
     return o;
 }
 
@@ -711,6 +714,44 @@ static void les_k_src_dlm(oracle_t *o)
     double *r = W(o, kn);
     for (size_t q = 0; q < o->fsz; q++)
         if (o->ialias[q] == 0) r[q] = r[q] + a1[q];
+    /* with the lag model the transfer term is also a source for (B T_B)
+     * (m_les.f90:1547-1557) */
+    if (o->les_model == 3) {
+        double *rb = W(o, kn + 1);
+        for (size_t q = 0; q < o->fsz; q++)
+            if (o->ialias[q] == 0) rb[q] = rb[q] + a1[q];
+    }
+}
+
+/* m_les_lag_model_sources (m_les.f90:1629-1684): B = (B T_B) |S| with
+ * |S|^2 = 2 S_ij S_ij left in wrk0 by les_k_src_dlm, eps = max(eps T_eps, 0)^1.5
+ * / (Delta C_T^1.5); where ialias == 0 the RHS of k_sgs loses eps, that of
+ * (B T_B) loses B and that of (eps T_eps) gains B - eps. */
+static void les_lag_model_sources(oracle_t *o)
+{
+    const double C_T = 1.0;   /* m_les.f90:43-44 */
+    int n = o->n, nk = 3 + o->nscal + 1, n1 = 3 + o->nscal + o->nles + 1, n2 = n1 + 1;
+    double *w0 = W(o, 0), *b = W(o, n1), *e = W(o, n2);
+    copy_field(o, b, F(o, nk));            /* (B T_B): field nk+1 in the 1-based count */
+    xfft3d(o, -1, b);
+    for (size_t q = 0; q < o->fsz; q++) b[q] = b[q] * sqrt(w0[q]);
+    xfft3d(o, 1, b);
+    copy_field(o, e, F(o, nk + 1));        /* (eps T_eps) */
+    xfft3d(o, -1, e);
+    for (size_t q = 0; q < o->fsz; q++) {
+        double v = e[q] > 0.0 ? e[q] : 0.0;
+        e[q] = pow(v, 1.5) / (o->les_delta * pow(C_T, 1.5));
+    }
+    xfft3d(o, 1, e);
+    o->les_stat[2] = b[0] / ((double)n * n * n);
+    o->les_stat[3] = e[0] / ((double)n * n * n);
+    double *rk = W(o, nk), *rb = W(o, nk + 1), *re = W(o, nk + 2);
+    for (size_t q = 0; q < o->fsz; q++)
+        if (o->ialias[q] == 0) {
+            rk[q] = rk[q] - e[q];
+            rb[q] = rb[q] - b[q];
+            re[q] = re[q] + b[q] - e[q];
+        }
 }
 
 /* m_les_k_diss_algebraic (m_les.f90:1567-1621): dissipation k^(3/2)/Delta of
@@ -798,7 +839,7 @@ static void oracle_rhs_scalars(oracle_t *o)
 {
     int n = o->n, ns = o->nscal, nl = o->nles;
     if (o->les_model == 1) les_get_turb_visc_smag(o);
-    if (o->les_model == 2) les_get_turb_visc_dlm(o);
+    if (o->les_model == 2 || o->les_model == 3) les_get_turb_visc_dlm(o);
     if (!o->int_scalars && nl == 0) {
         for (int m = 0; m < 3; m++) { copy_field(o, W(o, 1 + m), F(o, m)); xfft3d(o, -1, W(o, 1 + m)); }
         return;
@@ -904,12 +945,13 @@ static void oracle_rhs_scalars(oracle_t *o)
             for (size_t q = 0; q < o->fsz; q++) r[q] = r[q] - u[q];
         }
     /* les_rhs_scalars, DLM branch (m_les.f90:714-719) */
-    if (o->les_model == 2) {
-        /* les.gp energy and B (m_les.f90:880-885; no lag model, so B = 0) */
+    if (o->les_model == 2 || o->les_model == 3) {
+        /* les.gp energy (m_les.f90:880-885); B stays 0 without the lag model */
         o->les_stat[0] = F(o, 3 + ns)[0] / ((double)o->n * o->n * o->n);
         o->les_stat[2] = 0.0;
         les_k_src_dlm(o);
-        les_k_diss_algebraic(o);
+        if (o->les_model == 2) les_k_diss_algebraic(o);
+        else les_lag_model_sources(o);
         for (int m = 4; m <= 3 + ns + nl; m++) les_rhss_turb_visc1(o, m);
     }
 }

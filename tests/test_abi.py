@@ -64,9 +64,9 @@ def test_unsupported_size_rejected_before_device_use():
 
 
 def test_reference_les_models_without_a_port_are_rejected():
-    """The reference's LES models 3-10 (DLM with lag model, DSTM, mixed) are not
-    built: an input asking for one fails at init instead of running another model."""
+    """The reference's LES models 4-10 (DSTM, mixed) are not built: an input
+    asking for one fails at init instead of running another model."""
     from hit3d_b200 import Hit3dError, Params, Context
-    for m in (3, 4, 5, 6, 7, 10):
+    for m in (4, 5, 6, 7, 10):
         with pytest.raises(Hit3dError, match="les_model"):
             Context(Params(nx=32, les_model=m))

@@ -50,6 +50,27 @@ def test_dlm_clips_negative_k_sgs_like_the_oracle():
     assert relerr(g.download_fields(), o.fields) < 1e-10
 
 
+@pytest.mark.parametrize("n", [32, 48])
+def test_lag_model_matches_oracle(n):
+    """les_model 3: the DLM with the lag model for the dissipation; k_sgs,
+    (B T_B) and (eps T_eps) are state fields 3, 4, 5."""
+    o, g = make_pair(n, flow_type=1, les_model=3, nu=1.0 / 2000.0, dt=0.004, isp_type=2)
+    f0 = g.download_fields()
+    assert f0.shape[0] == 6
+    assert f0[3, 0, 0, 0] == pytest.approx(0.1 * n ** 3, rel=1e-15)
+    assert f0[4, 0, 0, 0] == f0[5, 0, 0, 0] == pytest.approx(0.05 * n ** 3, rel=1e-15)
+    for _ in range(3):
+        o.step(4)
+        g.step(4)
+        f = g.download_fields()
+        for m in range(6):
+            assert relerr(f[m], o.fields[m]) < 1e-10, m
+        gs, os_ = g.les_stats(), o.les_stats()
+        for k in ("energy", "production", "B", "dissipation"):
+            assert gs[k] == pytest.approx(os_[k], rel=1e-11), k
+    assert relerr(g.download_rhs_old(), o.rhs_old) < 1e-9
+
+
 def test_les_stats_only_for_the_dynamic_localization_model():
     from hit3d_b200 import Context, Hit3dError, Params
     with Context(Params(nx=32, les_model=1)) as c:

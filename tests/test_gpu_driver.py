@@ -73,17 +73,18 @@ def test_stop_file_ends_the_run_with_a_restart(tmp_path):
     assert os.path.exists(os.path.join(wd, "decay64_.64.000010"))
 
 
-def test_dlm_run_restarts_with_k_sgs(tmp_path):
-    """The dynamic localization model through the host loop: the restart file
-    carries k_sgs (nles = 1, as restart_io.f90 writes it) and a run restarted
-    from it continues with the same state."""
+@pytest.mark.parametrize("model,nles", [(2, 1), (3, 3)])
+def test_dlm_run_restarts_with_k_sgs(tmp_path, model, nles):
+    """The dynamic localization models through the host loop: the restart file
+    carries the LES fields (nles = 1 or 3, as restart_io.f90 writes them) and a
+    run restarted from it continues with the same state."""
     from dataclasses import replace
     from hit3d_b200.driver import Simulation
     from hit3d_b200.params import read_input_file
     from hit3d_b200.restart import read_restart
     wd = str(tmp_path)
     cfg = read_input_file(os.path.join(GOLDEN, "decay64_.in"))
-    cfg = replace(cfg, les_model=2, n_scalars=0, scalar_type=[], sc=[], ir_exp_sc=[], peak_wavenum_sc=[],
+    cfg = replace(cfg, les_model=model, n_scalars=0, scalar_type=[], sc=[], ir_exp_sc=[], peak_wavenum_sc=[],
                   reac_sc=[], itmax=6, iprint1=3, iprint2=3, iwrite4=100, tmax=10.0)
     sim = Simulation("dlm64", wd, cfg=cfg)
     sim.begin()
@@ -91,10 +92,11 @@ def test_dlm_run_restarts_with_k_sgs(tmp_path):
     # les.gp at every statistics step: itime, time, mean k_sgs, production, B, dissipation
     rows = [ln.split() for ln in open(os.path.join(wd, "les.gp"))]
     assert [int(r[0]) for r in rows] == [3, 6] and all(len(r) == 6 for r in rows)
-    assert float(rows[1][1]) == pytest.approx(5 * 0.005, rel=1e-6) and float(rows[1][4]) == 0.0
+    assert float(rows[1][1]) == pytest.approx(5 * 0.005, rel=1e-6)
+    assert (float(rows[1][4]) == 0.0) == (model == 2)       # B: only with the lag model
     assert float(rows[1][3]) > 0 and float(rows[1][5]) > 0
-    f, t, dt, nums, nles = read_restart(os.path.join(wd, "dlm64.64.000006"), 64, 0, 1)
-    assert nums == 0 and nles == 1 and f.shape[0] == 4
+    f, t, dt, nums, nles_read = read_restart(os.path.join(wd, "dlm64.64.000006"), 64, 0, nles)
+    assert nums == 0 and nles_read == nles and f.shape[0] == 3 + nles
     g = sim.ctx.download_fields()
     assert np.array_equal(f[..., :64], g[..., :64])
     sim2 = Simulation("dlm64", wd, cfg=replace(cfg, itmin=6))

@@ -292,3 +292,31 @@ def test_dlm_les_means_for_uniform_k_sgs():
     assert st["B"] == 0.0
     assert st["dissipation"] == pytest.approx(0.1 ** 1.5 / dx, rel=1e-13)
     assert st["production"] == pytest.approx(2 * nut * ss, rel=1e-12)
+
+
+def test_lag_model_les_means_for_uniform_fields():
+    """The lag model (les_model 3, m_les.f90:1629-1684) from its initial state
+    k_sgs = 0.1, (B T_B) = (eps T_eps) = 0.05 (m_les.f90:474-479): B = 0.05 <|S|>
+    with |S| = sqrt(2 S:S), eps = 0.05^1.5 / Delta (C_T = 1), production as for
+    the DLM."""
+    n = 32
+    o = oracle.Oracle(n, les_model=3, flow_type=0, nu=1.0 / 2000.0)
+    assert o.fields.shape[0] == 6
+    assert o.fields[4, 0, 0, 0] == o.fields[5, 0, 0, 0] == 0.05 * n ** 3
+    o.init_velocity(RN1, isp_type=1, peak_wavenum=4.0)
+    o.dealias_all()
+    o.rhs()
+    st = o.les_stats()
+    dx = 2 * np.pi / n
+    u = _to_complex(o.fields[:3]).transpose(0, 2, 1, 3)
+    kz = np.fft.fftfreq(n, 1.0 / n)[:, None, None]
+    ky = np.fft.fftfreq(n, 1.0 / n)[None, :, None]
+    kx = np.arange(n // 2 + 1)[None, None, :]
+    kk = (kx, ky, kz)
+    grad = [[np.fft.irfftn(1j * kk[j] * u[i], s=(n, n, n), axes=(0, 1, 2)) for j in range(3)] for i in range(3)]
+    ss = sum((0.5 * (grad[i][j] + grad[j][i])) ** 2 for i in range(3) for j in range(3))
+    nut = 0.1 * dx * math.sqrt(0.1)
+    assert st["energy"] == pytest.approx(0.1, rel=1e-14)
+    assert st["production"] == pytest.approx(2 * nut * ss.mean(), rel=1e-12)
+    assert st["B"] == pytest.approx(0.05 * np.sqrt(2 * ss).mean(), rel=1e-12)
+    assert st["dissipation"] == pytest.approx(0.05 ** 1.5 / dx, rel=1e-13)
