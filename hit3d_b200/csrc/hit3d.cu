@@ -157,7 +157,8 @@ struct hit3d_ctx {
     int mlp_clip;        // zero the stress where its dissipation is negative
     int mlp_kernel;      // 0: CUDA cores, 1: tensor cores for the hidden layers
     int *d_mlp_err;      // set by the tensor-core kernel when a completion wait runs out
-    double *d_kmin;      // dynamic localization model: minimum of k_sgs in the current step (slot 2)
+    double *d_kmin;      // LES with k_sgs: minimum of k_sgs (slot 2), les.gp means, block sums
+    double2 *gfilt;      // test filter transfer function of the Dynamic Structure models
     int prune_on;        // allow 2/3-rule pruning of the step's transforms
     int pruned;          // the state is zero beyond N/3 (checked), so pruning is exact
     int alias_known;     // `pruned` is up to date with the state
@@ -188,6 +189,7 @@ static int zinv_LM(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_t
     io.n = c->n; io.psrc = c->P64; io.pdst = dpitch; io.ncol = c->nh; io.sfield = sfield;
     io.dx = c->dx;
     io.k2max = c->k2max;
+    io.g = c->gfilt;
     int rows = c->n;
     if (c->kc_active >= 0) {
         io.kl = io.ko = c->kc_active;
@@ -220,6 +222,7 @@ static int zinv_L(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src
         case PRE_DLONG: return zinv_LM<T, L, PRE_DLONG>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         case PRE_TRUNC: return zinv_LM<T, L, PRE_TRUNC>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         case PRE_CUBE: return zinv_LM<T, L, PRE_CUBE>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+        case PRE_FILT: return zinv_LM<T, L, PRE_FILT>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         default: break;
         }
     }
@@ -467,10 +470,18 @@ struct Prof {
 
 // ---------------------------------------------------------------------------
 // one time step
-// LES-related transported fields (m_les.f90:111-137): k_sgs for the dynamic
-// localization model (2); k_sgs, (B T_B) and (eps T_eps) with the lag model (3)
-static int les_nles(int model) { return model == 2 ? 1 : model == 3 ? 3 : 0; }
+// LES-related transported fields (m_les.f90:111-300): k_sgs for the models with
+// an algebraic dissipation (2, 4, 6); k_sgs, (B T_B) and (eps T_eps) with the
+// lag model (3, 5, 7)
+static int les_nles(int model)
+{
+    return (model == 2 || model == 4 || model == 6) ? 1 : (model == 3 || model == 5 || model == 7) ? 3 : 0;
+}
 static bool les_dlm(int model) { return model == 2 || model == 3; }
+static bool les_dstm(int model) { return model >= 4 && model <= 7; }
+// work fields of the Dynamic Structure models past the products (k_dstm_phys layout)
+static int dstm_fields(int nles) { return (nles == 3 ? 21 : 20) + 3 * nles; }
+static int filter_transfer(hit3d_ctx *c, int kind, double delta);
 
 // ---------------------------------------------------------------------------
 // 2/3-rule pruning for the duration of one step (reset on every exit path)
@@ -514,7 +525,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     const int ns = c->int_scalars ? c->nsc : 0;
     const int nprod = 6 + 3 * ns;
     const bool les = p.les_model == 1, les_mlp = p.les_model == HIT3D_LES_LEARNED, dlm = les_dlm(p.les_model);
-    const bool lag = p.les_model == 3;
+    const bool lag = p.les_model == 3, dstm = les_dstm(p.les_model);
 
     StepArgs a;
     memset(&a, 0, sizeof a);
@@ -637,7 +648,47 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
         }
         const cx<T> *les_src = nullptr, *les_flux = nullptr;
         if constexpr (std::is_same<T, double>::value) {
-            if (lag) {
+            if (dstm) {
+                // Dynamic Structure Model family (les_models 4-7): test-filtered
+                // products (of the forward products above) and velocity, the nine
+                // velocity gradients, k_sgs and the LES fields in physical space;
+                // one kernel forms tau, the sources and the fluxes
+                MARK(6);
+                const int t0 = nprod, nl = les_nles(p.les_model);
+                const bool lagm = nl == 3;
+                const int g0 = lagm ? 21 : 20, nfld = dstm_fields(nl);
+                H3D_TRY(zinv<T>(c, 6, PRE_FILT, 0, reinterpret_cast<const double2 *>(Wf(0)), wfs, Wf(t0), wfs, wp));
+                H3D_TRY(zinv<T>(c, 3, PRE_FILT, 0, c->U, c->fs64, Wf(t0 + 6), wfs, wp));
+                for (int i = 0; i < 3; i++)
+                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, i, c->U, c->fs64, Wf(t0 + 9 + 3 * i), wfs, wp));
+                H3D_TRY(zinv<T>(c, 1, PRE_COPY, 0, c->U + 3 * c->fs64, c->fs64, Wf(t0 + 18), wfs, wp));
+                if (lagm) H3D_TRY(zinv<T>(c, 2, PRE_COPY, 0, c->U + 4 * c->fs64, c->fs64, Wf(t0 + 19), wfs, wp));
+                else H3D_TRY(zinv<T>(c, 1, PRE_CUBE, 0, c->U + 3 * c->fs64, c->fs64, Wf(t0 + 19), wfs, wp));
+                for (int j = 0; j < nl; j++)
+                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, 3 + j, c->U, c->fs64, Wf(t0 + g0 + 3 * j), wfs, wp));
+                H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, nfld));
+                H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, nfld));
+                DstmArgs da;
+                da.n = c->n; da.rp = 2 * (int64_t)wp; da.fs = 2 * wfs;
+                da.lag = lagm; da.mixed = p.les_model >= 6; da.g0 = g0;
+                const double cd = p.c_smag * c->dx;
+                da.cs2 = cd * cd;
+                da.cmix = p.les_model >= 6 ? p.c_mixed : 1.0;
+                da.delta = c->dx;
+                da.c_t = p.les_model == 5 ? p.c_t : 1.0;
+                k_dstm_phys<<<pw_grid(c), 256, 0, c->st>>>(da, reinterpret_cast<double *>(Wf(t0)), c->d_kmin + 8);
+                H3D_LAUNCH_CHECK();
+                k_dlm_stats<<<1, 32, 0, c->st>>>((int)pw_grid(c).x, 1.0 / ((double)c->n * c->n * c->n),
+                                                 c->U + 3 * c->fs64, c->d_kmin + 8, c->d_kmin + 4);
+                H3D_LAUNCH_CHECK();
+                H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, 6 + nl));
+                H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, 6 + nl));
+                H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, 6 + nl));
+                H3D_TRY(xr2c<T>(c, Wf(t0 + g0), wfs, wp, 3 * nl));
+                H3D_TRY(spass<T>(c, 1, true, Wf(t0 + g0), wfs, wp, 3 * nl));
+                H3D_TRY(spass<T>(c, 2, true, Wf(t0 + g0), wfs, wp, 3 * nl));
+                tau = Wf(t0);
+            } else if (lag) {
                 // dynamic localization model with the lag model for the dissipation
                 // (les_model 3; m_les.f90:720-724, 1422-1561, 1629-1684, 1041-1091)
                 MARK(6);
@@ -714,7 +765,10 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 // sources and turbulent fluxes of the LES fields (layout above)
                 const int j = s - p.n_scalars;
                 const cx<T> *src = nullptr, *flux = nullptr;
-                if (lag && j >= 0) {
+                if (dstm && j >= 0) {
+                    src = Wf(nprod + 6 + j);
+                    flux = Wf(nprod + (les_nles(p.les_model) == 3 ? 21 : 20) + 3 * j);
+                } else if (lag && j >= 0) {
                     src = Wf(nprod + (j == 0 ? 6 : j == 1 ? 7 : 17));
                     flux = Wf(nprod + 8 + 3 * j);
                 } else if (dlm && j == 0) {
@@ -809,12 +863,17 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     if (p->dealias != 0 && p->dealias != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: wrong dealias flag");
     if (p->flow_type == 1 && p->force_type != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: WRONG FORCE TYPE");
     if (p->flow_type == 1 && (p->kfmax < 1 || p->kfmax > 15)) return h3d_set_error_msg(-1, "hit3d_gpu_init: kfmax must be in 1..15");
-    if (p->les_model != 0 && p->les_model != 1 && !les_dlm(p->les_model) && p->les_model != HIT3D_LES_LEARNED)
-        return h3d_set_error_msg(-1, "hit3d_gpu_init: les_model must be 0 (none), 1 (Smagorinsky), 2 (dynamic "
-                                     "localization), 3 (dynamic localization with the lag model) or 20 (learned "
-                                     "closure); the reference's models 4-10 are not supported");
-    if (les_dlm(p->les_model) && p->precision != 0)
-        return h3d_set_error_msg(-1, "hit3d_gpu_init: the dynamic localization models (les_model 2, 3) run with FP64 transforms");
+    if (!(p->les_model >= 0 && p->les_model <= 7) && p->les_model != HIT3D_LES_LEARNED)
+        return h3d_set_error_msg(-1, "hit3d_gpu_init: les_model must be 0 (none), 1 (Smagorinsky), 2-3 (dynamic "
+                                     "localization), 4-7 (dynamic structure, mixed) or 20 (learned closure); the "
+                                     "reference's model 10 is not supported");
+    if (les_nles(p->les_model) > 0 && p->precision != 0)
+        return h3d_set_error_msg(-1, "hit3d_gpu_init: the LES models with k_sgs (les_model 2-7) run with FP64 transforms");
+    if (p->les_model == 5 && !(p->c_t > 0.0))
+        return h3d_set_error_msg(-1, "hit3d_gpu_init: les_model 5 needs C_T > 0 (the reference reads it from c_t.in)");
+    if ((p->les_model == 6 || p->les_model == 7) && !(p->c_mixed > 0.0))
+        return h3d_set_error_msg(-1, "hit3d_gpu_init: les_models 6 and 7 need C_mixed > 0 (the reference reads it "
+                                     "from c_mixed.in)");
     if (p->les_model != 0 && p->n_scalars > 0) return h3d_set_error_msg(-1, "hit3d_gpu_init: LES with scalars is not supported");
     if (p->precision != 0 && p->precision != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: precision must be 0 or 1");
     for (int s = 0; s < p->n_scalars; s++) {
@@ -839,7 +898,9 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     c->dx = 2.0 * (4.0 * atan(1.0)) / (double)c->n;
     c->int_scalars = c->nsc > 0;
     c->xcfg = 4;  // register-resident fused x pass, the tuner's usual pick
-    c->prune_on = !les_dlm(p->les_model);  // a clipped k_sgs brings modes beyond N/3 into the state
+    // a clipped k_sgs brings modes beyond N/3 into the state; the LES fields keep
+    // the unpruned transforms throughout
+    c->prune_on = les_nles(p->les_model) == 0;
     c->kc_active = -1;
     cudaDeviceProp prop;
     H3D_CHECK(cudaGetDeviceProperties(&prop, c->dev));
@@ -850,7 +911,10 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     const size_t f64 = (size_t)c->fs64 * sizeof(double2);
     c->nw = 6 + 3 * c->nsc +
             (c->p.les_model == 1 ? 6 : c->p.les_model == HIT3D_LES_LEARNED ? 9 : c->p.les_model == 2 ? 12
-                                                                               : c->p.les_model == 3 ? 20 : 0);
+                                                                               : c->p.les_model == 3 ? 20
+                                                                               : les_dstm(c->p.les_model)
+                                                                                   ? dstm_fields(les_nles(c->p.les_model))
+                                                                                   : 0);
     if (c->p.precision == 0) {
         c->wpitch = c->P64;
         c->wfs = c->fs64;
@@ -897,7 +961,7 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     H3D_CHECK(cudaMemset(c->U, 0, f64 * nf));
     H3D_CHECK(cudaMemset(c->RO, 0, f64 * nf));
     H3D_CHECK(cudaMemset(c->W, 0, wbytes));
-    if (les_dlm(c->p.les_model)) {
+    if (les_nles(c->p.les_model) > 0) {
         // [2] the minimum of k_sgs, [4..8) the les.gp means, [8..) block partial sums
         if ((rc = ctx_alloc((void **)&c->d_kmin, sizeof(double) * (8 + 3 * (size_t)pw_grid(c).x)))) {
             hit3d_gpu_finalize(c);
@@ -906,13 +970,32 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
         H3D_CHECK(cudaMemset(c->d_kmin, 0, sizeof(double) * 8));
         // m_les_dlm_k_init (m_les.f90:1394-1413): k_sgs = 0.1 in physical space, so
         // only the (0,0,0) mode, 0.1 N^3 after the unnormalised transform
-        const double2 k0 = make_double2(0.1 * (double)c->n * (double)c->n * (double)c->n, 0.0);
+        // m_les_begin (m_les.f90:430-570): k_sgs = 0.2 for les_model 4, 0.5 for
+        // 5-7; with the lag model (B T_B) = (eps T_eps) = 0.5 k_sgs (3), or
+        // (B T_B) = k_sgs and (eps T_eps) = 0 (5, 7)
+        const int m = c->p.les_model;
+        const double n3 = (double)c->n * (double)c->n * (double)c->n;
+        const double2 k0 = make_double2((m <= 3 ? 0.1 : m == 4 ? 0.2 : 0.5) * n3, 0.0);
         H3D_CHECK(cudaMemcpy(c->U + 3 * c->fs64, &k0, sizeof k0, cudaMemcpyHostToDevice));
-        if (c->p.les_model == 3) {
-            // (B T_B) = (eps T_eps) = 0.5 k_sgs (m_les.f90:474-479)
-            const double2 h0 = make_double2(0.5 * k0.x, 0.0);
-            H3D_CHECK(cudaMemcpy(c->U + 4 * c->fs64, &h0, sizeof h0, cudaMemcpyHostToDevice));
-            H3D_CHECK(cudaMemcpy(c->U + 5 * c->fs64, &h0, sizeof h0, cudaMemcpyHostToDevice));
+        if (les_nles(m) == 3) {
+            const double2 b0 = make_double2(m == 3 ? 0.5 * k0.x : k0.x, 0.0);
+            const double2 e0 = make_double2(m == 3 ? 0.5 * k0.x : 0.0, 0.0);
+            H3D_CHECK(cudaMemcpy(c->U + 4 * c->fs64, &b0, sizeof b0, cudaMemcpyHostToDevice));
+            H3D_CHECK(cudaMemcpy(c->U + 5 * c->fs64, &e0, sizeof e0, cudaMemcpyHostToDevice));
+        }
+        if (les_dstm(m)) {
+            // the test filter: Gaussian of width 4 dx (m_filter_xfftw.f90:140-150, 197-220)
+            if ((rc = ctx_alloc((void **)&c->gfilt, sizeof(double2) * (size_t)c->fs64))) {
+                hit3d_gpu_finalize(c);
+                return rc;
+            }
+            if ((rc = filter_transfer(c, 2, 4.0 * c->dx))) {
+                hit3d_gpu_finalize(c);
+                return rc;
+            }
+            H3D_CHECK(cudaMemcpyAsync(c->gfilt, c->W64, sizeof(double2) * (size_t)c->fs64, cudaMemcpyDeviceToDevice,
+                                      c->st));
+            H3D_CHECK(cudaStreamSynchronize(c->st));
         }
     }
     *out = c;
@@ -927,7 +1010,7 @@ extern "C" void hit3d_gpu_finalize(hit3d_ctx *c)
     if (c->W64 && c->W64 != c->W) cudaFree(c->W64);
     void *ptrs[] = {c->U, c->RO, c->RP, c->SP, c->W, c->phys, c->tw64, c->tw32, c->d_fen, c->d_part,
                     c->d_red, c->d_ratio, c->d_cmax, c->stage, c->d_xyz, c->d_uvw, c->sgs, c->mlp_wb,
-                    c->d_mlp_err, c->d_kmin};
+                    c->d_mlp_err, c->d_kmin, c->gfilt};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
@@ -1146,8 +1229,8 @@ extern "C" int hit3d_gpu_check_finite(hit3d_ctx *c, int64_t *nonfinite)
 extern "C" int hit3d_gpu_les_stats(hit3d_ctx *c, double *out4)
 {
     if (!c || !out4) return h3d_set_error_msg(-1, "hit3d_gpu_les_stats: null argument");
-    if (!les_dlm(c->p.les_model))
-        return h3d_set_error_msg(-1, "hit3d_gpu_les_stats: les.gp quantities exist for les_model 2 and 3 only");
+    if (les_nles(c->p.les_model) == 0)
+        return h3d_set_error_msg(-1, "hit3d_gpu_les_stats: les.gp quantities exist for les_models 2-7 only");
     H3D_CHECK(cudaSetDevice(c->dev));
     H3D_CHECK(cudaMemcpyAsync(out4, c->d_kmin + 4, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
     H3D_CHECK(cudaStreamSynchronize(c->st));
@@ -1190,7 +1273,7 @@ extern "C" int hit3d_gpu_set_scalars_active(hit3d_ctx *c, int32_t on)
 {
     if (!c) return h3d_set_error_msg(-1, "null context");
     // the LES fields are always transported (rhs_scalars.f90:72-74)
-    c->int_scalars = ((on != 0) && c->nsc > 0) || les_dlm(c->p.les_model);
+    c->int_scalars = ((on != 0) && c->nsc > 0) || les_nles(c->p.les_model) > 0;
     return 0;
 }
 

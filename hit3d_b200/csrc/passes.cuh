@@ -61,6 +61,7 @@ enum PreMode : int {
     PRE_GRAD = 6,      // d phi/dx_f of state field `sfield`     (m_stats.f90:323-326)
     PRE_TRUNC = 7,     // field f with |k|^2 > k2max zeroed       (io_write_4.f90:21-42)
     PRE_CUBE = 8,      // field f with some |k_i| > N/3 zeroed    (m_les.f90:1579-1586)
+    PRE_FILT = 9,      // field f times the test filter g         (m_filter_xfftw.f90:81-100)
 };
 
 // MODE is a compile-time PreMode so that the plain copy carries no per-element
@@ -72,6 +73,7 @@ template <typename T, typename TO, int MODE> struct IOSpec {
     int n, psrc, pdst, ncol, sfield;
     double dx;     // grid spacing, for PRE_SHIFT
     double k2max;  // truncation radius squared, for PRE_TRUNC
+    const double2 *g = nullptr;  // test filter transfer function, for PRE_FILT (pitch psrc)
     int kl = -1, ko = -1;  // 2/3-rule pruning of the kz loads and the ky rows
     H3D_D int outer(int y) const { return ko >= 0 ? kept_index(y, n, ko) : y; }
 
@@ -132,6 +134,12 @@ template <typename T, typename TO, int MODE> struct IOSpec {
         case PRE_CUBE: {
             const double k3 = (double)(n / 3);
             r = (fabs(kx) > k3 || fabs(ky) > k3 || fabs(kz) > k3) ? make_double2(0.0, 0.0) : U(f, o, c, p);
+            break;
+        }
+        case PRE_FILT: {
+            // filter_xfftw: (a + ib)(c + id) with the transfer function in (c, d)
+            const double2 u = U(f, o, c, p), gg = g[((int64_t)p * n + o) * psrc + c];
+            r = make_double2(u.x * gg.x - u.y * gg.y, u.y * gg.x + u.x * gg.y);
             break;
         }
         default: r = U(f, o, c, p);

@@ -680,6 +680,101 @@ __global__ void __launch_bounds__(256) k_dll_phys(int n, int64_t rp, int64_t fs,
     block_sums3(psum, bsum, dsum, part);
 }
 
+// Dynamic Structure Model family (les_models 4-7; m_les.f90:1697-1960 with
+// 1096-1137, 1422-1621, 1629-1684, 1041-1091), per point of the physical
+// fields W (row pitch rp, field stride fs):
+//   W[0..6)  test-filtered products (u_i u_j)~ (uu uv uw vv vw ww) -> tau_ij
+//   W[6..9)  test-filtered velocity u~_i                            -> sources
+//   W[9..18) du_i/dx_j at 9 + 3 i + j
+//   W[18]    k_sgs;  W[19] the 2/3-rule k_sgs (algebraic dissipation) or
+//   (B T_B);  W[20] (eps T_eps);  W[g0 ..) gradients of the LES fields -> fluxes
+// tau_D = 2 max(k, 0) / max(L_kk, 1e-15) L_ij, L_ij = (u_i u_j)~ - u~_i u~_j;
+// Pi_D = -tau_ij du_i/dx_j;  nu_t = cmix (c_s dx)^2 sqrt(2 S:S) (cmix = 1 for
+// 4, 5, C_mixed for 6, 7); the mixed models add -2 nu_t S to tau and the
+// transfer Pi_L = 2 nu_t S:S.  Sources: k: Pi_D + Pi_L - eps;  (B T_B):
+// Pi_D + Pi_L - B;  (eps T_eps): B - eps, with eps = max(k~, 0)^1.5 / Delta
+// (algebraic, 4 and 6) or max(eps T_eps, 0)^1.5 / (Delta C_T^1.5) and
+// B = (B T_B) sqrt(2 S:S) (lag model, 5 and 7).  Fluxes nu_t grad(phi).
+struct DstmArgs {
+    int n;
+    int64_t rp, fs;
+    int lag, mixed, g0;
+    double cs2, cmix, delta, c_t;
+};
+__global__ void __launch_bounds__(256) k_dstm_phys(const DstmArgs a, double *__restrict__ W, double *__restrict__ part)
+{
+    const int64_t np = (int64_t)a.n * a.n * a.n;
+    const int nl = a.lag ? 3 : 1;
+    const double den = a.delta * (a.lag ? pow(a.c_t, 1.5) : 1.0);
+    double psum = 0.0, bsum = 0.0, dsum = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / a.n, o = row * a.rp + (t - row * a.n);
+        double g[9], fu[3], fp[6];
+#pragma unroll
+        for (int q = 0; q < 9; q++) g[q] = W[o + (9 + q) * a.fs];
+#pragma unroll
+        for (int q = 0; q < 3; q++) fu[q] = W[o + (6 + q) * a.fs];
+#pragma unroll
+        for (int q = 0; q < 6; q++) fp[q] = W[o + q * a.fs];
+        const double kr = W[o + 18 * a.fs];
+        // products in the order uu uv uw vv vw ww: (i, j) -> index
+        const int pi[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+        double lkk = (fp[0] + fp[3]) + fp[5];
+        lkk = lkk - fu[0] * fu[0];
+        lkk = lkk - fu[1] * fu[1];
+        lkk = lkk - fu[2] * fu[2];
+        const double cf = 2.0 * (kr > 0.0 ? kr : 0.0) / (lkk > 1.e-15 ? lkk : 1.e-15);
+        double tau[6];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = i; j < 3; j++) tau[pi[i][j]] = (fp[pi[i][j]] - fu[i] * fu[j]) * cf;
+        double pid = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) pid -= g[3 * i + j] * tau[pi[i][j]];
+        double sv[6];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = i; j < 3; j++) sv[pi[i][j]] = 0.5 * (g[3 * i + j] + g[3 * j + i]);
+        double ss = sv[0] * sv[0];
+        ss = ss + 2.0 * (sv[1] * sv[1]);
+        ss = ss + 2.0 * (sv[2] * sv[2]);
+        ss = ss + sv[3] * sv[3];
+        ss = ss + 2.0 * (sv[4] * sv[4]);
+        ss = ss + sv[5] * sv[5];
+        const double s2 = 2.0 * ss;
+        const double nut = a.cmix * (sqrt(s2) * a.cs2);
+        double pil = 0.0;
+        if (a.mixed) {
+            pil = s2 * nut;
+#pragma unroll
+            for (int q = 0; q < 6; q++) tau[q] = tau[q] + (-2.0 * nut) * sv[q];
+        }
+        double eps, bb = 0.0;
+        if (a.lag) {
+            const double et = W[o + 20 * a.fs];
+            bb = W[o + 19 * a.fs] * sqrt(s2);
+            eps = pow(et > 0.0 ? et : 0.0, 1.5) / den;
+            W[o + 7 * a.fs] = (pid + pil) - bb;
+            W[o + 8 * a.fs] = bb - eps;
+        } else {
+            const double kc = W[o + 19 * a.fs];
+            eps = pow(kc > 0.0 ? kc : 0.0, 1.5) / den;
+        }
+        W[o + 6 * a.fs] = (pid + pil) - eps;
+#pragma unroll
+        for (int q = 0; q < 6; q++) W[o + q * a.fs] = tau[q];
+        for (int q = 0; q < 3 * nl; q++) W[o + (a.g0 + q) * a.fs] = W[o + (a.g0 + q) * a.fs] * nut;
+        psum += pid + pil;
+        bsum += bb;
+        dsum += eps;
+    }
+    block_sums3(psum, bsum, dsum, part);
+}
+
 // out[0..3] = energy, production, B, dissipation of les.gp (m_les.f90:876-892):
 // the mean k_sgs from its zero mode K0 (unnormalised forward transform) and the
 // block sums divided by N^3; one warp, fixed summation order

@@ -20,7 +20,7 @@ import time as _time
 import numpy as np
 
 from .gpu import Context, les_fields
-from .params import RunConfig, read_input_file
+from .params import InputFileError, RunConfig, read_input_file
 from .restart import read_restart, restart_name, write_real4, write_restart
 from .sidecar import GpuSettings, SidecarError, read_sidecar
 
@@ -61,7 +61,9 @@ class Simulation:
             self.cfg.les_model = s.les_model
             if s.les_model > 0:
                 self.cfg.dealias = 0  # every LES model runs with the 2/3 rule (m_parameters.f90:416-420)
-        self.ctx = Context(self.cfg.to_params(precision=s.precision, device=s.device, c_smag=s.c_smag))
+        c_t, c_mixed = self._les_constants()
+        self.ctx = Context(self.cfg.to_params(precision=s.precision, device=s.device, c_smag=s.c_smag, c_t=c_t,
+                                              c_mixed=c_mixed))
         if not s.pruning:
             self.ctx.set_pruning(False)
         if s.variant is not None:
@@ -81,6 +83,21 @@ class Simulation:
                 pass
         self.exit_reason = None
         self.log = []
+
+    def _les_constants(self):
+        """C_T of les_model 5 from c_t.in and C_mixed of les_models 6, 7 from
+        c_mixed.in, first value of the file, as m_les_init reads them
+        (m_les.f90:189-207, 213-290); a missing file stops the run."""
+        def first_value(name):
+            path = os.path.join(self.wd, name)
+            if not os.path.exists(path):
+                raise InputFileError(f"Cannot find the file '{name}' (les_model {self.cfg.les_model})")
+            try:
+                return float(open(path).read().replace(",", " ").split()[0].replace("d", "e").replace("D", "e"))
+            except (IndexError, ValueError) as e:
+                raise InputFileError(f"bad value in {name}") from e
+        m = self.cfg.les_model
+        return (first_value("c_t.in") if m == 5 else 1.0), (first_value("c_mixed.in") if m in (6, 7) else 0.0)
 
     def _load_closure(self):
         s = self.settings

@@ -26,9 +26,10 @@ N_VARIANTS = 11  # launch-shape variants of the fused x pass (HIT3D_FUSED_VARIAN
 
 
 def les_fields(les_model: int) -> int:
-    """LES-related transported fields (m_les.f90:111-137): k_sgs for the dynamic
-    localization model (2); k_sgs, (B T_B), (eps T_eps) with the lag model (3)."""
-    return {2: 1, 3: 3}.get(int(les_model), 0)
+    """LES-related transported fields (m_les.f90:111-300): k_sgs for the models with
+    an algebraic dissipation (2, 4, 6); k_sgs, (B T_B), (eps T_eps) with the lag
+    model (3, 5, 7)."""
+    return {2: 1, 3: 3, 4: 1, 5: 3, 6: 1, 7: 3}.get(int(les_model), 0)
 
 
 _lib = None
@@ -44,7 +45,7 @@ class _Params(C.Structure):
         ("kfmax", C.c_int32), ("n_scalars", C.c_int32), ("precision", C.c_int32), ("les_model", C.c_int32),
         ("scalar_type", C.c_int32 * MAX_SCALARS), ("device", C.c_int32), ("reserved", C.c_int32),
         ("nu", C.c_double), ("dt", C.c_double), ("famp", C.c_double), ("c_smag", C.c_double),
-        ("sc", C.c_double * MAX_SCALARS),
+        ("sc", C.c_double * MAX_SCALARS), ("c_t", C.c_double), ("c_mixed", C.c_double),
     ]
 
 
@@ -66,6 +67,8 @@ class Params:
     famp: float = 0.5
     c_smag: float = 0.18
     sc: Sequence[float] = field(default_factory=list)
+    c_t: float = 1.0        # lag-model C_T of les_model 5 (c_t.in)
+    c_mixed: float = 0.0    # C_mixed of les_models 6, 7 (c_mixed.in)
 
     @property
     def kmax(self) -> int:
@@ -80,7 +83,7 @@ class Params:
         for k in ("nx", "dealias", "flow_type", "force_type", "kfmax", "n_scalars", "precision", "les_model",
                   "device"):
             setattr(p, k, int(getattr(self, k)))
-        for k in ("nu", "dt", "famp", "c_smag"):
+        for k in ("nu", "dt", "famp", "c_smag", "c_t", "c_mixed"):
             setattr(p, k, float(getattr(self, k)))
         st = list(self.scalar_type) + [0] * MAX_SCALARS
         sc = list(self.sc) + [1.0] * MAX_SCALARS

@@ -79,11 +79,12 @@ class RunConfig:
     def pe(self) -> List[float]:
         return [self.nu / s for s in self.sc]
 
-    def to_params(self, precision: int = 0, device: int = 0, c_smag: float = 0.18) -> Params:
+    def to_params(self, precision: int = 0, device: int = 0, c_smag: float = 0.18, c_t: float = 1.0,
+                  c_mixed: float = 0.0) -> Params:
         return Params(nx=self.nx, dealias=self.dealias, flow_type=self.flow_type, force_type=self.force_type,
                       kfmax=self.kfmax, n_scalars=self.n_scalars, precision=precision, les_model=self.les_model,
                       scalar_type=list(self.scalar_type), device=device, nu=self.nu, dt=self.dt, famp=self.famp,
-                      c_smag=c_smag, sc=list(self.sc))
+                      c_smag=c_smag, sc=list(self.sc), c_t=c_t, c_mixed=c_mixed)
 
 
 class _ListDirected:

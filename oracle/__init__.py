@@ -71,6 +71,9 @@ def lib():
         L.oracle_fft1d.argtypes = [C.c_int, dp, C.c_int]
         L.oracle_stats.argtypes = [vp, dp]
         L.oracle_les_stats.argtypes = [vp, dp]
+        L.oracle_nwrk.argtypes = [vp]
+        L.oracle_nwrk.restype = C.c_int
+        L.oracle_set_les_constants.argtypes = [vp, C.c_double, C.c_double]
         L.oracle_scalar_stats.argtypes = [vp, dp]
         L.oracle_energy_spectrum.argtypes = [vp, C.c_int, C.c_int, dp]
         L.oracle_forcing_energy.restype = C.c_double
@@ -139,7 +142,8 @@ class Oracle:
         if not self._p:
             raise MemoryError("oracle_create failed")
         self.n, self.nscal = n, nscal
-        self.nles = {2: 1, 3: 3}.get(les_model, 0)   # LES fields of the dynamic localization models
+        # LES fields: k_sgs, and (B T_B), (eps T_eps) with the lag model
+        self.nles = {2: 1, 3: 3, 4: 1, 5: 3, 6: 1, 7: 3}.get(les_model, 0)
         self.nu = nu
         self.kmax = L.oracle_kmax(self._p)
         self.fsz = (n + 2) * n * n
@@ -148,7 +152,7 @@ class Oracle:
             nf, n, n, n + 2)
         self.rhs_old = np.ctypeslib.as_array(L.oracle_rhs_old(self._p), shape=(nf * self.fsz,)).reshape(
             nf, n, n, n + 2)
-        nw = max(7, 6 + nscal + self.nles)
+        nw = L.oracle_nwrk(self._p)
         self.wrk = np.ctypeslib.as_array(L.oracle_wrk(self._p), shape=(nw * self.fsz,)).reshape(
             nw, n, n, n + 2)
 
@@ -216,6 +220,10 @@ class Oracle:
         keys = ["energy", "eps_v", "eta", "etakmax", "uvar", "x_length", "lambda", "re_lambda",
                 "re_lambda1", "tau_e", "enstrophy", "skewness"]
         return out[: self.kmax].copy(), dict(zip(keys, out[self.kmax:].tolist()))
+
+    def set_les_constants(self, c_t=1.0, c_mixed=0.0):
+        """C_T of les_model 5 (c_t.in) and C_mixed of les_models 6 and 7 (c_mixed.in)."""
+        lib().oracle_set_les_constants(self._p, float(c_t), float(c_mixed))
 
     def les_stats(self):
         """les.gp quantities of the last RHS evaluation (dynamic localization model)."""

@@ -214,6 +214,9 @@ typedef struct {
     fftplan plan;
     double courant, time;
     double les_stat[4];       /* les.gp: mean k_sgs, production, B, dissipation */
+    double c_t, c_mixed;      /* lag-model scale (c_t.in) and mixed-model fraction (c_mixed.in) */
+    double *gfilt;            /* test filter transfer function (DSTM models) */
+    double *vsrc;             /* vel_source_les: 3 fields (DSTM models) */
     int fov, fos, int_scalars;
     double *scratch;          /* per-thread FFT scratch: nthreads * 4n doubles */
     int nthreads;
@@ -383,6 +386,9 @@ void oracle_fft3d(oracle_t *o, int flag, double *a) { xfft3d(o, flag, a); }
 /* ------------------------------------------------------------------------- */
 /*  create / destroy                                                          */
 /* ------------------------------------------------------------------------- */
+void oracle_filter_g(oracle_t *o, int kind, double delta, double *g);
+void oracle_apply_filter(oracle_t *o, const double *g, double *a);
+
 oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_type, int kfmax,
                         double nu, double dt, double famp, int les_model, double c_smag,
                         const double *sc, const int *scalar_type)
@@ -397,7 +403,10 @@ oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_
     /* LES-related transported quantities: k_sgs for the DLM (m_les.f90:111-123);
      * k_sgs, (B T_B), (eps T_eps) with the lag model (m_les.f90:124-137); all
      * with Schmidt number one (m_les.f90:372-391) */
-    o->nles = les_model == 2 ? 1 : les_model == 3 ? 3 : 0;
+    o->nles = (les_model == 2 || les_model == 4 || les_model == 6) ? 1
+            : (les_model == 3 || les_model == 5 || les_model == 7) ? 3 : 0;
+    o->c_t = 1.0;
+    o->c_mixed = 0.0;
     if (o->nles && nscal > 0) { free(o); return NULL; }
     /* kmax (m_parameters.f90:123-131) */
     if (dealias == 0) o->kmax = n / 3;
@@ -407,6 +416,8 @@ oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_
     o->fsz = (size_t)(n + 2) * n * n;
     o->nwrk = 7;
     if (6 + nscal + o->nles > o->nwrk) o->nwrk = 6 + nscal + o->nles;
+    /* the DSTM models use four work arrays past the LES fields (m_work.f90) */
+    if (les_model >= 4 && les_model <= 7 && 3 + nscal + o->nles + 5 > o->nwrk) o->nwrk = 3 + nscal + o->nles + 5;
     o->fields = (double *)calloc(o->fsz * (3 + nscal + o->nles), sizeof(double));
     o->rhs_old = (double *)calloc(o->fsz * (3 + nscal + o->nles), sizeof(double));
     o->wrk = (double *)calloc(o->fsz * o->nwrk, sizeof(double));
@@ -449,7 +460,18 @@ oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_
      * i.e. only the (0,0,0) mode, 0.1 N^3 after the unnormalised transform */
     if (o->nles) F(o, 3 + nscal)[0] = 0.1 * (double)n * (double)n * (double)n;
     /* lag model: (B T_B) = (eps T_eps) = 0.5 k_sgs (m_les.f90:474-479) */
-    if (o->nles == 3) F(o, 4 + nscal)[0] = F(o, 5 + nscal)[0] = 0.5 * F(o, 3 + nscal)[0];
+    if (les_model == 3) F(o, 4 + nscal)[0] = F(o, 5 + nscal)[0] = 0.5 * F(o, 3 + nscal)[0];
+    /* DSTM models (m_les_begin, m_les.f90:485-570): k_sgs = 0.2 (4) or 0.5
+     * (5-7); with the lag model (B T_B) = k_sgs and (eps T_eps) = 0; the test
+     * filter is the Gaussian of width 4 dx (m_filter_xfftw.f90:140-150) */
+    if (les_model >= 4 && les_model <= 7) {
+        const double n3 = (double)n * (double)n * (double)n;
+        F(o, 3 + nscal)[0] = (les_model == 4 ? 0.2 : 0.5) * n3;
+        if (o->nles == 3) { F(o, 4 + nscal)[0] = F(o, 3 + nscal)[0]; F(o, 5 + nscal)[0] = 0.0; }
+        o->gfilt = (double *)calloc(o->fsz, sizeof(double));
+        o->vsrc = (double *)calloc(3 * o->fsz, sizeof(double));
+        oracle_filter_g(o, 2, 4.0 * o->dx, o->gfilt);
+    }
     return o;
 }
 
@@ -459,6 +481,7 @@ void oracle_destroy(oracle_t *o)
     free(o->fields); free(o->rhs_old); free(o->wrk); free(o->turb_visc);
     free(o->akx); free(o->aky); free(o->akz); free(o->ialias);
     free(o->fn_i); free(o->fn_j); free(o->fn_k); free(o->scratch);
+    free(o->gfilt); free(o->vsrc);
     plan_free(&o->plan);
     free(o);
 }
@@ -466,6 +489,9 @@ void oracle_destroy(oracle_t *o)
 double *oracle_fields(oracle_t *o) { return o->fields; }
 double *oracle_rhs_old(oracle_t *o) { return o->rhs_old; }
 double *oracle_wrk(oracle_t *o) { return o->wrk; }
+int oracle_nwrk(oracle_t *o) { return o->nwrk; }
+/* C_T of les_model 5 (c_t.in) and C_mixed of les_models 6, 7 (c_mixed.in) */
+void oracle_set_les_constants(oracle_t *o, double c_t, double c_mixed) { o->c_t = c_t; o->c_mixed = c_mixed; }
 int oracle_kmax(oracle_t *o) { return o->kmax; }
 int oracle_nforced(oracle_t *o) { return o->nfn; }
 double oracle_courant(oracle_t *o) { return o->courant; }
@@ -562,7 +588,15 @@ static void les_rhs_velocity(oracle_t *o)
 {
     int n = o->n;
     double *tv = o->turb_visc;
-    for (int pass = 0; pass < 2; pass++) {
+    /* les_rhs_velocity (m_les.f90:635-676): the DSTM velocity sources (4-7),
+     * the eddy-viscosity stress (1-3, 6, 7) */
+    if (o->les_model >= 4 && o->les_model <= 7)
+        for (int m = 0; m < 3; m++) {
+            double *r = W(o, 1 + m), *vs = o->vsrc + (size_t)m * o->fsz;
+            for (size_t q = 0; q < o->fsz; q++) r[q] = r[q] + vs[q];
+        }
+    const int eddy = o->les_model <= 3 || o->les_model == 6 || o->les_model == 7;
+    for (int pass = 0; pass < (eddy ? 2 : 0); pass++) {
         strain_first(o, pass);
         for (int m = 4; m <= 6; m++) {
             double *a = W(o, m);
@@ -700,6 +734,8 @@ static void les_k_src_dlm(oracle_t *o)
         }
     }
     for (size_t q = 0; q < o->fsz; q++) w0[q] = 2.0 * w0[q];
+    /* with les_model 5 only |S|^2 in wrk0 is wanted (m_les.f90:1508-1510) */
+    if (o->les_model == 5) return;
     int n = o->n;
     for (size_t q = 0; q < o->fsz; q++) a1[q] = w0[q];
     for (int k = 0; k < n; k++)
@@ -710,13 +746,13 @@ static void les_k_src_dlm(oracle_t *o)
             }
     xfft3d(o, 1, a1);
     /* saved for les.gp (m_les.f90:1536): the zero mode over N^3 */
-    o->les_stat[1] = a1[0] / ((double)n * n * n);
+    o->les_stat[1] += a1[0] / ((double)n * n * n);
     double *r = W(o, kn);
     for (size_t q = 0; q < o->fsz; q++)
         if (o->ialias[q] == 0) r[q] = r[q] + a1[q];
     /* with the lag model the transfer term is also a source for (B T_B)
      * (m_les.f90:1547-1557) */
-    if (o->les_model == 3) {
+    if (o->les_model == 3 || o->les_model == 7) {
         double *rb = W(o, kn + 1);
         for (size_t q = 0; q < o->fsz; q++)
             if (o->ialias[q] == 0) rb[q] = rb[q] + a1[q];
@@ -729,7 +765,8 @@ static void les_k_src_dlm(oracle_t *o)
  * (B T_B) loses B and that of (eps T_eps) gains B - eps. */
 static void les_lag_model_sources(oracle_t *o)
 {
-    const double C_T = 1.0;   /* m_les.f90:43-44 */
+    /* C_T = 1 (m_les.f90:43-44) unless les_model 5 read c_t.in (m_les.f90:195-207) */
+    const double C_T = o->les_model == 5 ? o->c_t : 1.0;
     int n = o->n, nk = 3 + o->nscal + 1, n1 = 3 + o->nscal + o->nles + 1, n2 = n1 + 1;
     double *w0 = W(o, 0), *b = W(o, n1), *e = W(o, n2);
     copy_field(o, b, F(o, nk));            /* (B T_B): field nk+1 in the 1-based count */
@@ -743,8 +780,8 @@ static void les_lag_model_sources(oracle_t *o)
         e[q] = pow(v, 1.5) / (o->les_delta * pow(C_T, 1.5));
     }
     xfft3d(o, 1, e);
-    o->les_stat[2] = b[0] / ((double)n * n * n);
-    o->les_stat[3] = e[0] / ((double)n * n * n);
+    o->les_stat[2] += b[0] / ((double)n * n * n);
+    o->les_stat[3] += e[0] / ((double)n * n * n);
     double *rk = W(o, nk), *rb = W(o, nk + 1), *re = W(o, nk + 2);
     for (size_t q = 0; q < o->fsz; q++)
         if (o->ialias[q] == 0) {
@@ -769,7 +806,7 @@ static void les_k_diss_algebraic(oracle_t *o)
         w0[q] = pow(v, 1.5) / o->les_delta;
     }
     xfft3d(o, 1, w0);
-    o->les_stat[3] = w0[0] / ((double)n * n * n);    /* m_les.f90:1617 */
+    o->les_stat[3] += w0[0] / ((double)n * n * n);    /* m_les.f90:1617 */
     double *r = W(o, kn);
     for (int k = 0; k < n; k++)
         for (int j = 0; j < n; j++)
@@ -780,6 +817,78 @@ static void les_k_diss_algebraic(oracle_t *o)
 }
 
 static void derivative(oracle_t *o, const double *src, char axis, double *dst);
+
+/* m_les_dstm_vel_k_sources (m_les.f90:1697-1960), the Dynamic Structure Model:
+ * tau_ij = 2 k_sgs / L_kk * L_ij with L_ij = (u_i u_j)~ - u~_i u~_j (~: the test
+ * filter), max(k_sgs, 0) and max(L_kk, 1e-15); velocity sources -d tau_ij/dx_j
+ * and the k_sgs source -tau_ij du_i/dx_j (also a source for (B T_B) with
+ * les_models 5 and 7), all added where ialias == 0.  The reference's
+ * diagnostic outputs of this routine (units 698, 699 and the k., L., F.,
+ * tau.., pi. real*4 dumps) are left out. */
+static void les_dstm_vel_k_sources(oracle_t *o)
+{
+    const int n = o->n, ns = o->nscal, nl = o->nles;
+    const int nk = 3 + ns + 1;              /* 1-based field number of k_sgs */
+    const int n2 = 3 + ns + nl + 1, n3 = n2 + 1, n4 = n2 + 2, n5 = n2 + 3;
+    const double n3d = (double)n * n * n;
+    double *w1 = W(o, 0), *a2 = W(o, n2), *a3 = W(o, n3), *a4 = W(o, n4), *a5 = W(o, n5);
+    const size_t fsz = o->fsz;
+    const char dirs[3] = {'x', 'y', 'z'};
+    /* k_sgs in physical space */
+    copy_field(o, w1, F(o, nk - 1));
+    xfft3d(o, -1, w1);
+    /* L_kk = (u_k u_k)~ - u~_k u~_k */
+    copy_field(o, a3, F(o, 0)); copy_field(o, a4, F(o, 1)); copy_field(o, a5, F(o, 2));
+    xfft3d(o, -1, a3); xfft3d(o, -1, a4); xfft3d(o, -1, a5);
+    for (size_t q = 0; q < fsz; q++) a2[q] = a3[q] * a3[q] + a4[q] * a4[q] + a5[q] * a5[q];
+    xfft3d(o, 1, a2);
+    oracle_apply_filter(o, o->gfilt, a2);
+    xfft3d(o, -1, a2);
+    copy_field(o, a3, F(o, 0)); copy_field(o, a4, F(o, 1)); copy_field(o, a5, F(o, 2));
+    oracle_apply_filter(o, o->gfilt, a3); oracle_apply_filter(o, o->gfilt, a4); oracle_apply_filter(o, o->gfilt, a5);
+    xfft3d(o, -1, a3); xfft3d(o, -1, a4); xfft3d(o, -1, a5);
+    for (size_t q = 0; q < fsz; q++) a2[q] = a2[q] - a3[q] * a3[q] - a4[q] * a4[q] - a5[q] * a5[q];
+    /* the coefficient 2 k / L_kk */
+    for (size_t q = 0; q < fsz; q++) {
+        double kk = w1[q] > 0.0 ? w1[q] : 0.0, lk = a2[q] > 1.e-15 ? a2[q] : 1.e-15;
+        w1[q] = 2.0 * kk / lk;
+    }
+    memset(o->vsrc, 0, sizeof(double) * 3 * fsz);
+    double *rk = W(o, nk), *rb = W(o, nk + 1);
+    const int to_b = o->les_model == 5 || o->les_model == 7;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            copy_field(o, a2, F(o, i)); copy_field(o, a3, F(o, j));
+            copy_field(o, a4, F(o, i)); copy_field(o, a5, F(o, j));
+            xfft3d(o, -1, a2); xfft3d(o, -1, a3);
+            oracle_apply_filter(o, o->gfilt, a4); oracle_apply_filter(o, o->gfilt, a5);
+            xfft3d(o, -1, a4); xfft3d(o, -1, a5);
+            for (size_t q = 0; q < fsz; q++) a2[q] = a2[q] * a3[q];
+            xfft3d(o, 1, a2);
+            oracle_apply_filter(o, o->gfilt, a2);
+            xfft3d(o, -1, a2);
+            for (size_t q = 0; q < fsz; q++) {
+                double t = a2[q] - a4[q] * a5[q];
+                a2[q] = t * w1[q];                  /* tau_ij in physical space */
+            }
+            copy_field(o, a3, F(o, i));
+            derivative(o, a3, dirs[j], a3);
+            xfft3d(o, -1, a3);
+            for (size_t q = 0; q < fsz; q++) a5[q] = -a3[q] * a2[q];
+            xfft3d(o, 1, a2);
+            xfft3d(o, 1, a5);
+            for (size_t q = 0; q < fsz; q++) a3[q] = -a2[q];
+            derivative(o, a3, dirs[j], a3);
+            double *vs = o->vsrc + (size_t)i * fsz;
+            for (size_t q = 0; q < fsz; q++)
+                if (o->ialias[q] == 0) {
+                    vs[q] = vs[q] + a3[q];
+                    rk[q] = rk[q] + a5[q];
+                    if (to_b) rb[q] = rb[q] + a5[q];
+                }
+            o->les_stat[1] += a5[0] / n3d;
+        }
+}
 
 /* m_les_rhss_turb_visc1 (m_les.f90:1041-1091): sum_i d/dx_i (nu_t d phi/dx_i)
  * added to the RHS of field m where ialias == 0 */
@@ -835,11 +944,23 @@ static void mul3(oracle_t *o, double *dst, const double *a, const double *b)
     for (size_t q = 0; q < o->fsz; q++) dst[q] = a[q] * b[q];
 }
 
+static void les_dstm_vel_k_sources(oracle_t *o);
+static void les_get_turb_visc(oracle_t *o)
+{
+    /* les_get_turb_visc (m_les.f90:1096-1137) */
+    const int m = o->les_model;
+    if (m == 1 || m == 4 || m == 5) les_get_turb_visc_smag(o);
+    if (m == 2 || m == 3) les_get_turb_visc_dlm(o);
+    if (m == 6 || m == 7) {
+        les_get_turb_visc_smag(o);
+        for (size_t q = 0; q < o->fsz; q++) o->turb_visc[q] = o->c_mixed * o->turb_visc[q];
+    }
+}
+
 static void oracle_rhs_scalars(oracle_t *o)
 {
     int n = o->n, ns = o->nscal, nl = o->nles;
-    if (o->les_model == 1) les_get_turb_visc_smag(o);
-    if (o->les_model == 2 || o->les_model == 3) les_get_turb_visc_dlm(o);
+    if (o->les_model) les_get_turb_visc(o);
     if (!o->int_scalars && nl == 0) {
         for (int m = 0; m < 3; m++) { copy_field(o, W(o, 1 + m), F(o, m)); xfft3d(o, -1, W(o, 1 + m)); }
         return;
@@ -945,14 +1066,20 @@ static void oracle_rhs_scalars(oracle_t *o)
             for (size_t q = 0; q < o->fsz; q++) r[q] = r[q] - u[q];
         }
     /* les_rhs_scalars, DLM branch (m_les.f90:714-719) */
-    if (o->les_model == 2 || o->les_model == 3) {
-        /* les.gp energy (m_les.f90:880-885); B stays 0 without the lag model */
+    /* les_rhs_scalars (m_les.f90:700-858); les.gp sums restart every step */
+    if (nl > 0) {
         o->les_stat[0] = F(o, 3 + ns)[0] / ((double)o->n * o->n * o->n);
-        o->les_stat[2] = 0.0;
-        les_k_src_dlm(o);
-        if (o->les_model == 2) les_k_diss_algebraic(o);
-        else les_lag_model_sources(o);
+        o->les_stat[1] = o->les_stat[2] = o->les_stat[3] = 0.0;
+        switch (o->les_model) {
+        case 2: les_k_src_dlm(o); les_k_diss_algebraic(o); break;
+        case 3: les_k_src_dlm(o); les_lag_model_sources(o); break;
+        case 4: les_dstm_vel_k_sources(o); les_k_diss_algebraic(o); break;
+        case 5: les_dstm_vel_k_sources(o); les_k_src_dlm(o); les_lag_model_sources(o); break;
+        case 6: les_dstm_vel_k_sources(o); les_k_src_dlm(o); break;
+        case 7: les_dstm_vel_k_sources(o); les_k_src_dlm(o); les_lag_model_sources(o); break;
+        }
         for (int m = 4; m <= 3 + ns + nl; m++) les_rhss_turb_visc1(o, m);
+        if (o->les_model == 6) les_k_diss_algebraic(o);
     }
 }
 

@@ -20,7 +20,7 @@ def spectral_view(fields):
 
 def make_pair(n, *, dealias=0, flow_type=0, kfmax=2, nu=1.0 / 400.0, dt=0.005, famp=0.5, nscal=0, sc=(),
               scalar_type=(), les_model=0, c_smag=0.18, precision=0, isp_type=1, peak=4.0, ir_exp=2.0,
-              init="gpu"):
+              init="gpu", c_t=1.0, c_mixed=0.0):
     """Create an oracle and a GPU context holding the same initial state.
 
     init="gpu": velocity initialised by the GPU path, copied into the oracle.
@@ -30,8 +30,10 @@ def make_pair(n, *, dealias=0, flow_type=0, kfmax=2, nu=1.0 / 400.0, dt=0.005, f
 
     o = oracle.Oracle(n, nscal=nscal, dealias=dealias, flow_type=flow_type, kfmax=kfmax, nu=nu, dt=dt, famp=famp,
                       les_model=les_model, c_smag=c_smag, sc=sc, scalar_type=scalar_type)
+    o.set_les_constants(c_t, c_mixed)
     p = Params(nx=n, dealias=dealias, flow_type=flow_type, kfmax=kfmax, nu=nu, dt=dt, famp=famp, n_scalars=nscal,
-               sc=list(sc), scalar_type=list(scalar_type), les_model=les_model, c_smag=c_smag, precision=precision)
+               sc=list(sc), scalar_type=list(scalar_type), les_model=les_model, c_smag=c_smag, precision=precision,
+               c_t=c_t, c_mixed=c_mixed)
     g = Context(p)
     if init == "gpu":
         g.init_velocity(RN1, isp_type, peak, ir_exp)

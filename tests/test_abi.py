@@ -39,12 +39,13 @@ def test_params_struct_layout_matches_c(tmp_path):
         '#include <stdio.h>\n#include <stddef.h>\n#include "hit3d_gpu.h"\n'
         "int main(void){printf(\"%zu %zu %zu %zu %zu\\n\", sizeof(hit3d_params),"
         " offsetof(hit3d_params, scalar_type), offsetof(hit3d_params, device),"
-        " offsetof(hit3d_params, nu), offsetof(hit3d_params, sc)); return 0;}\n")
+        " offsetof(hit3d_params, nu), offsetof(hit3d_params, sc));"
+        " printf(\"%zu %zu\\n\", offsetof(hit3d_params, c_t), offsetof(hit3d_params, c_mixed)); return 0;}\n")
     exe = tmp_path / "probe"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
     got = [C.sizeof(_Params), _Params.scalar_type.offset, _Params.device.offset, _Params.nu.offset,
-           _Params.sc.offset]
+           _Params.sc.offset, _Params.c_t.offset, _Params.c_mixed.offset]
     assert [int(x) for x in out] == got
 
 
@@ -64,9 +65,9 @@ def test_unsupported_size_rejected_before_device_use():
 
 
 def test_reference_les_models_without_a_port_are_rejected():
-    """The reference's LES models 4-10 (DSTM, mixed) are not built: an input
-    asking for one fails at init instead of running another model."""
+    """The reference's LES model 10 (mixed model with Harlow scalar fluxes) is not
+    built: an input asking for it fails at init instead of running another model."""
     from hit3d_b200 import Hit3dError, Params, Context
-    for m in (4, 5, 6, 7, 10):
+    for m in (8, 9, 10):
         with pytest.raises(Hit3dError, match="les_model"):
             Context(Params(nx=32, les_model=m))

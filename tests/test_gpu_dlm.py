@@ -74,7 +74,7 @@ def test_lag_model_matches_oracle(n):
 def test_les_stats_only_for_the_dynamic_localization_model():
     from hit3d_b200 import Context, Hit3dError, Params
     with Context(Params(nx=32, les_model=1)) as c:
-        with pytest.raises(Hit3dError, match="les_model 2"):
+        with pytest.raises(Hit3dError, match="les_models 2-7"):
             c.les_stats()
 
 
@@ -84,3 +84,36 @@ def test_dlm_rejects_what_it_does_not_support():
         Context(Params(nx=32, les_model=2, precision=1))
     with pytest.raises(Hit3dError, match="scalars"):
         Context(Params(nx=32, les_model=2, n_scalars=1, sc=[1.0], scalar_type=[0]))
+
+
+@pytest.mark.parametrize("model,nles", [(4, 1), (5, 3), (6, 1), (7, 3)])
+def test_dynamic_structure_models_match_oracle(model, nles):
+    """les_models 4-7 (m_les.f90:138-300, 1697-1960): the Dynamic Structure Model
+    with the algebraic (4) or lag (5) dissipation, and the mixed models (6, 7)
+    with C_mixed times the Smagorinsky viscosity; test filter Gaussian of width
+    4 dx; parity of all fields and of the les.gp means."""
+    n = 32
+    o, g = make_pair(n, flow_type=1, les_model=model, nu=1.0 / 2000.0, dt=0.004, isp_type=2, c_t=0.8,
+                     c_mixed=0.3)
+    f0 = g.download_fields()
+    assert f0.shape[0] == 3 + nles
+    assert f0[3, 0, 0, 0] == pytest.approx((0.2 if model == 4 else 0.5) * n ** 3, rel=1e-15)
+    for _ in range(3):
+        o.step(3)
+        g.step(3)
+        f = g.download_fields()
+        for m in range(3 + nles):
+            assert relerr(f[m], o.fields[m]) < 1e-10, m
+        gs, os_ = g.les_stats(), o.les_stats()
+        for k in ("energy", "production", "B", "dissipation"):
+            assert gs[k] == pytest.approx(os_[k], rel=1e-10, abs=1e-14), k
+    assert relerr(g.download_rhs_old(), o.rhs_old) < 1e-9
+
+
+def test_les_constants_are_required():
+    from hit3d_b200 import Context, Hit3dError, Params
+    with pytest.raises(Hit3dError, match="C_T"):
+        Context(Params(nx=32, les_model=5, c_t=0.0))
+    for m in (6, 7):
+        with pytest.raises(Hit3dError, match="C_mixed"):
+            Context(Params(nx=32, les_model=m))

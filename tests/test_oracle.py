@@ -320,3 +320,70 @@ def test_lag_model_les_means_for_uniform_fields():
     assert st["production"] == pytest.approx(2 * nut * ss.mean(), rel=1e-12)
     assert st["B"] == pytest.approx(0.05 * np.sqrt(2 * ss).mean(), rel=1e-12)
     assert st["dissipation"] == pytest.approx(0.05 ** 1.5 / dx, rel=1e-13)
+
+
+def _gaussian_transfer(n, delta):
+    """The test filter of m_filter_xfftw.f90:197-220 (Gaussian, values below 1e-20
+    dropped) as the numpy rfftn of its kernel."""
+    dx = 2 * np.pi / n
+    d = np.minimum(np.arange(n), n - np.arange(n)) * dx
+    Z, Y, X = np.meshgrid(d, d, d, indexing="ij")
+    c1 = 6.0 / delta ** 2
+    g = (np.sqrt(c1 / np.pi) ** 3 * dx ** 3) * np.exp(-c1 * (X ** 2 + Y ** 2 + Z ** 2))
+    g[g < 1e-20] = 0.0
+    return np.fft.rfftn(g)
+
+
+@pytest.mark.parametrize("model,k0", [(4, 0.2), (6, 0.5)])
+def test_dynamic_structure_model_against_numpy(model, k0):
+    """m_les_dstm_vel_k_sources (m_les.f90:1697-1960) restated in numpy for the
+    initial uniform k_sgs: tau_ij = 2 k / L_kk L_ij with L_ij = (u_i u_j)~ -
+    u~_i u~_j; the velocity RHS gains -d tau_ij/dx_j on the 2/3-rule modes and
+    the production is <-tau_ij du_i/dx_j>.  The mixed model (6) adds the
+    eddy-viscosity stress with C_mixed nu_Smagorinsky and its transfer."""
+    n = 32
+    kw = dict(flow_type=0, nu=1.0 / 2000.0)
+    o = oracle.Oracle(n, les_model=model, **kw)
+    o.set_les_constants(c_mixed=0.25)
+    o0 = oracle.Oracle(n, les_model=0, **kw)
+    o0.init_velocity(RN1, isp_type=1, peak_wavenum=4.0)
+    o0.dealias_all()
+    o.fields[:3] = o0.fields[:3]
+    assert o.fields[3, 0, 0, 0] == k0 * n ** 3
+    o.rhs()
+    o0.rhs()
+    u_hat = _to_complex(o0.fields[:3]).transpose(0, 2, 1, 3)          # [c][kz][ky][kx]
+    kz = np.fft.fftfreq(n, 1.0 / n)[:, None, None]
+    ky = np.fft.fftfreq(n, 1.0 / n)[None, :, None]
+    kx = np.arange(n // 2 + 1)[None, None, :]
+    kk = (kx, ky, kz)
+    inv = lambda f: np.fft.irfftn(f, s=(n, n, n), axes=(0, 1, 2))
+    fwd = lambda f: np.fft.rfftn(f, axes=(0, 1, 2))
+    G = _gaussian_transfer(n, 4 * 2 * np.pi / n)
+    u = [inv(u_hat[i]) for i in range(3)]
+    uf = [inv(G * u_hat[i]) for i in range(3)]
+    L = [[inv(G * fwd(u[i] * u[j])) - uf[i] * uf[j] for j in range(3)] for i in range(3)]
+    Lkk = L[0][0] + L[1][1] + L[2][2]
+    F = 2 * k0 / np.maximum(Lkk, 1e-15)
+    tau = [[F * L[i][j] for j in range(3)] for i in range(3)]
+    grad = [[inv(1j * kk[j] * u_hat[i]) for j in range(3)] for i in range(3)]
+    prod = -sum(grad[i][j] * tau[i][j] for i in range(3) for j in range(3)).mean()
+    keep = (np.abs(kz) <= n // 3) & (np.abs(ky) <= n // 3) & (kx <= n // 3)
+    vsrc = [np.where(keep, -sum(1j * kk[j] * fwd(tau[i][j]) for j in range(3)), 0) for i in range(3)]
+    d = _to_complex(o.wrk[1:4] - o0.wrk[1:4]).transpose(0, 2, 1, 3)
+    st = o.les_stats()
+    if model == 4:
+        for i in range(3):
+            assert np.abs(d[i] - vsrc[i]).max() <= 1e-10 * np.abs(vsrc[i]).max()
+        assert st["production"] == pytest.approx(prod, rel=1e-10)
+        dx = 2 * np.pi / n
+        assert st["dissipation"] == pytest.approx(k0 ** 1.5 / dx, rel=1e-13)
+    else:
+        S = [[0.5 * (grad[i][j] + grad[j][i]) for j in range(3)] for i in range(3)]
+        ss = sum(S[i][j] ** 2 for i in range(3) for j in range(3))
+        nut = 0.25 * (0.18 * 2 * np.pi / n) ** 2 * np.sqrt(2 * ss)
+        eddy = [np.where(keep, sum(1j * kk[j] * fwd(2 * nut * S[i][j]) for j in range(3)), 0) for i in range(3)]
+        for i in range(3):
+            want = vsrc[i] + eddy[i]
+            assert np.abs(d[i] - want).max() <= 1e-10 * np.abs(want).max()
+        assert st["production"] == pytest.approx(prod + (2 * nut * ss).mean(), rel=1e-10)
