@@ -342,9 +342,12 @@ def configs_leg(torch, args, device):
 
     les = {}
     nparam = None
-    for name, model in (("smagorinsky", 1), ("dynamic_localization", 2), ("learned", 20)):
+    for name, model in (("smagorinsky", 1), ("dynamic_localization", 2), ("dynamic_localization_lag", 3),
+                        ("dynamic_structure", 4), ("dynamic_structure_lag", 5), ("mixed", 6), ("mixed_lag", 7),
+                        ("learned", 20)):
+        # C_T and C_mixed stand in for the values of c_t.in / c_mixed.in
         c = Context(Params(nx=128, dealias=0, flow_type=1, force_type=1, kfmax=2, famp=0.5, nu=1.0 / 6000.0,
-                           dt=0.002, les_model=model, device=device))
+                           dt=0.002, les_model=model, device=device, c_t=1.0, c_mixed=0.5))
         if model == 20:
             from hit3d_b200 import gpu
             nparam = int(gpu.lib().hit3d_mlp_nparam())
