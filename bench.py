@@ -344,7 +344,7 @@ def configs_leg(torch, args, device):
     nparam = None
     for name, model in (("smagorinsky", 1), ("dynamic_localization", 2), ("dynamic_localization_lag", 3),
                         ("dynamic_structure", 4), ("dynamic_structure_lag", 5), ("mixed", 6), ("mixed_lag", 7),
-                        ("learned", 20)):
+                        ("one_equation_mixed", 10), ("learned", 20)):
         # C_T and C_mixed stand in for the values of c_t.in / c_mixed.in
         c = Context(Params(nx=128, dealias=0, flow_type=1, force_type=1, kfmax=2, famp=0.5, nu=1.0 / 6000.0,
                            dt=0.002, les_model=model, device=device, c_t=1.0, c_mixed=0.5))

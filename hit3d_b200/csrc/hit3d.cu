@@ -475,12 +475,14 @@ struct Prof {
 // lag model (3, 5, 7)
 static int les_nles(int model)
 {
-    return (model == 2 || model == 4 || model == 6) ? 1 : (model == 3 || model == 5 || model == 7) ? 3 : 0;
+    return (model == 2 || model == 4 || model == 6) ? 1 : (model == 3 || model == 5 || model == 7) ? 3
+                                                                                                : model == 10 ? 2 : 0;
 }
 static bool les_dlm(int model) { return model == 2 || model == 3; }
 static bool les_dstm(int model) { return model >= 4 && model <= 7; }
 // work fields of the Dynamic Structure models past the products (k_dstm_phys layout)
 static int dstm_fields(int nles) { return (nles == 3 ? 21 : 20) + 3 * nles; }
+static constexpr int kM10Fields = 26;  // work fields of les_model 10 (k_m10_phys layout)
 static int filter_transfer(hit3d_ctx *c, int kind, double delta);
 
 // ---------------------------------------------------------------------------
@@ -525,7 +527,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     const int ns = c->int_scalars ? c->nsc : 0;
     const int nprod = 6 + 3 * ns;
     const bool les = p.les_model == 1, les_mlp = p.les_model == HIT3D_LES_LEARNED, dlm = les_dlm(p.les_model);
-    const bool lag = p.les_model == 3, dstm = les_dstm(p.les_model);
+    const bool lag = p.les_model == 3, dstm = les_dstm(p.les_model), m10 = p.les_model == 10;
 
     StepArgs a;
     memset(&a, 0, sizeof a);
@@ -688,6 +690,40 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 H3D_TRY(spass<T>(c, 1, true, Wf(t0 + g0), wfs, wp, 3 * nl));
                 H3D_TRY(spass<T>(c, 2, true, Wf(t0 + g0), wfs, wp, 3 * nl));
                 tau = Wf(t0);
+            } else if (m10) {
+                // les_model 10: the stress of the mixed model from (B T_B) + (eps T_eps),
+                // the lag-model sources without k_sgs, the turbulent fluxes
+                MARK(6);
+                const int t0 = nprod;
+                H3D_TRY(zinv<T>(c, 6, PRE_FILT, 0, reinterpret_cast<const double2 *>(Wf(0)), wfs, Wf(t0), wfs, wp));
+                H3D_TRY(zinv<T>(c, 3, PRE_FILT, 0, c->U, c->fs64, Wf(t0 + 6), wfs, wp));
+                for (int i = 0; i < 3; i++)
+                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, i, c->U, c->fs64, Wf(t0 + 9 + 3 * i), wfs, wp));
+                H3D_TRY(zinv<T>(c, 2, PRE_COPY, 0, c->U + 3 * c->fs64, c->fs64, Wf(t0 + 18), wfs, wp));
+                for (int j = 0; j < 2; j++)
+                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, 3 + j, c->U, c->fs64, Wf(t0 + 20 + 3 * j), wfs, wp));
+                H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, kM10Fields));
+                H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, kM10Fields));
+                DstmArgs da;
+                memset(&da, 0, sizeof da);
+                da.n = c->n; da.rp = 2 * (int64_t)wp; da.fs = 2 * wfs;
+                const double cd = p.c_smag * c->dx;
+                da.cs2 = cd * cd;
+                da.cmix = p.c_mixed;
+                da.delta = c->dx;
+                k_m10_phys<<<pw_grid(c), 256, 0, c->st>>>(da, reinterpret_cast<double *>(Wf(t0)), c->d_kmin + 8);
+                H3D_LAUNCH_CHECK();
+                k_dlm_stats<<<1, 32, 0, c->st>>>((int)pw_grid(c).x, 1.0 / ((double)c->n * c->n * c->n),
+                                                 c->U + 3 * c->fs64, c->d_kmin + 8, c->d_kmin + 4,
+                                                 c->U + 4 * c->fs64);
+                H3D_LAUNCH_CHECK();
+                H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, 8));
+                H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, 8));
+                H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, 8));
+                H3D_TRY(xr2c<T>(c, Wf(t0 + 20), wfs, wp, 6));
+                H3D_TRY(spass<T>(c, 1, true, Wf(t0 + 20), wfs, wp, 6));
+                H3D_TRY(spass<T>(c, 2, true, Wf(t0 + 20), wfs, wp, 6));
+                tau = Wf(t0);
             } else if (lag) {
                 // dynamic localization model with the lag model for the dissipation
                 // (les_model 3; m_les.f90:720-724, 1422-1561, 1629-1684, 1041-1091)
@@ -765,7 +801,10 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 // sources and turbulent fluxes of the LES fields (layout above)
                 const int j = s - p.n_scalars;
                 const cx<T> *src = nullptr, *flux = nullptr;
-                if (dstm && j >= 0) {
+                if (m10 && j >= 0) {
+                    src = Wf(nprod + 6 + j);
+                    flux = Wf(nprod + 20 + 3 * j);
+                } else if (dstm && j >= 0) {
                     src = Wf(nprod + 6 + j);
                     flux = Wf(nprod + (les_nles(p.les_model) == 3 ? 21 : 20) + 3 * j);
                 } else if (lag && j >= 0) {
@@ -863,12 +902,15 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     if (p->dealias != 0 && p->dealias != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: wrong dealias flag");
     if (p->flow_type == 1 && p->force_type != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: WRONG FORCE TYPE");
     if (p->flow_type == 1 && (p->kfmax < 1 || p->kfmax > 15)) return h3d_set_error_msg(-1, "hit3d_gpu_init: kfmax must be in 1..15");
-    if (!(p->les_model >= 0 && p->les_model <= 7) && p->les_model != HIT3D_LES_LEARNED)
+    if (!(p->les_model >= 0 && p->les_model <= 7) && p->les_model != 10 && p->les_model != HIT3D_LES_LEARNED)
         return h3d_set_error_msg(-1, "hit3d_gpu_init: les_model must be 0 (none), 1 (Smagorinsky), 2-3 (dynamic "
-                                     "localization), 4-7 (dynamic structure, mixed) or 20 (learned closure); the "
-                                     "reference's model 10 is not supported");
+                                     "localization), 4-7 (dynamic structure, mixed), 10 (one-equation mixed) or 20 "
+                                     "(learned closure)");
     if (les_nles(p->les_model) > 0 && p->precision != 0)
-        return h3d_set_error_msg(-1, "hit3d_gpu_init: the LES models with k_sgs (les_model 2-7) run with FP64 transforms");
+        return h3d_set_error_msg(-1, "hit3d_gpu_init: the LES models with transported fields (les_model 2-7, 10) run "
+                                     "with FP64 transforms");
+    if (p->les_model == 10 && !(p->c_mixed >= 0.0))
+        return h3d_set_error_msg(-1, "hit3d_gpu_init: les_model 10 needs C_mixed >= 0 (c_mixed.in, default 0.5)");
     if (p->les_model == 5 && !(p->c_t > 0.0))
         return h3d_set_error_msg(-1, "hit3d_gpu_init: les_model 5 needs C_T > 0 (the reference reads it from c_t.in)");
     if ((p->les_model == 6 || p->les_model == 7) && !(p->c_mixed > 0.0))
@@ -914,6 +956,7 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
                                                                                : c->p.les_model == 3 ? 20
                                                                                : les_dstm(c->p.les_model)
                                                                                    ? dstm_fields(les_nles(c->p.les_model))
+                                                                               : c->p.les_model == 10 ? kM10Fields
                                                                                    : 0);
     if (c->p.precision == 0) {
         c->wpitch = c->P64;
@@ -973,17 +1016,19 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
         // m_les_begin (m_les.f90:430-570): k_sgs = 0.2 for les_model 4, 0.5 for
         // 5-7; with the lag model (B T_B) = (eps T_eps) = 0.5 k_sgs (3), or
         // (B T_B) = k_sgs and (eps T_eps) = 0 (5, 7)
+        // les_model 10: (B T_B) = (eps T_eps) = 0.1, no k_sgs field (m_les.f90:592-608)
         const int m = c->p.les_model;
         const double n3 = (double)c->n * (double)c->n * (double)c->n;
-        const double2 k0 = make_double2((m <= 3 ? 0.1 : m == 4 ? 0.2 : 0.5) * n3, 0.0);
+        const double2 k0 = make_double2((m <= 3 || m == 10 ? 0.1 : m == 4 ? 0.2 : 0.5) * n3, 0.0);
         H3D_CHECK(cudaMemcpy(c->U + 3 * c->fs64, &k0, sizeof k0, cudaMemcpyHostToDevice));
+        if (m == 10) H3D_CHECK(cudaMemcpy(c->U + 4 * c->fs64, &k0, sizeof k0, cudaMemcpyHostToDevice));
         if (les_nles(m) == 3) {
             const double2 b0 = make_double2(m == 3 ? 0.5 * k0.x : k0.x, 0.0);
             const double2 e0 = make_double2(m == 3 ? 0.5 * k0.x : 0.0, 0.0);
             H3D_CHECK(cudaMemcpy(c->U + 4 * c->fs64, &b0, sizeof b0, cudaMemcpyHostToDevice));
             H3D_CHECK(cudaMemcpy(c->U + 5 * c->fs64, &e0, sizeof e0, cudaMemcpyHostToDevice));
         }
-        if (les_dstm(m)) {
+        if (les_dstm(m) || m == 10) {
             // the test filter: Gaussian of width 4 dx (m_filter_xfftw.f90:140-150, 197-220)
             if ((rc = ctx_alloc((void **)&c->gfilt, sizeof(double2) * (size_t)c->fs64))) {
                 hit3d_gpu_finalize(c);
@@ -1230,7 +1275,7 @@ extern "C" int hit3d_gpu_les_stats(hit3d_ctx *c, double *out4)
 {
     if (!c || !out4) return h3d_set_error_msg(-1, "hit3d_gpu_les_stats: null argument");
     if (les_nles(c->p.les_model) == 0)
-        return h3d_set_error_msg(-1, "hit3d_gpu_les_stats: les.gp quantities exist for les_models 2-7 only");
+        return h3d_set_error_msg(-1, "hit3d_gpu_les_stats: les.gp quantities exist for les_models 2-7 and 10 only");
     H3D_CHECK(cudaSetDevice(c->dev));
     H3D_CHECK(cudaMemcpyAsync(out4, c->d_kmin + 4, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
     H3D_CHECK(cudaStreamSynchronize(c->st));

@@ -775,11 +775,74 @@ __global__ void __launch_bounds__(256) k_dstm_phys(const DstmArgs a, double *__r
     block_sums3(psum, bsum, dsum, part);
 }
 
+// les_model 10 (m_les.f90:1223-1307, 2009-2392), per point of W laid out as
+// for k_dstm_phys but W[18] (B T_B), W[19] (eps T_eps), W[20..26) their
+// gradients: k = (B T_B) + (eps T_eps), c = 2 k / L_kk (0 where L_kk < 1e-10),
+// tau_ij = c L_ij - 2 C_mixed nu_t S_ij, Pi = -c L_ij S_ij + C_mixed nu_t^3 /
+// (c_s Delta)^4, B = (B T_B) nu_t / (c_s Delta)^2, eps = max(eps T_eps, 0)^1.5 /
+// Delta; sources (B T_B): Pi - B -> W[6], (eps T_eps): B - eps -> W[7];
+// fluxes nu_t grad -> W[20..26); nu_t = (c_s Delta)^2 sqrt(2 S:S).
+__global__ void __launch_bounds__(256) k_m10_phys(const DstmArgs a, double *__restrict__ W, double *__restrict__ part)
+{
+    const int64_t np = (int64_t)a.n * a.n * a.n;
+    const double cd2 = a.cs2, cd4 = a.cs2 * a.cs2;
+    double psum = 0.0, bsum = 0.0, dsum = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / a.n, o = row * a.rp + (t - row * a.n);
+        double g[9], fu[3], fp[6];
+#pragma unroll
+        for (int q = 0; q < 9; q++) g[q] = W[o + (9 + q) * a.fs];
+#pragma unroll
+        for (int q = 0; q < 3; q++) fu[q] = W[o + (6 + q) * a.fs];
+#pragma unroll
+        for (int q = 0; q < 6; q++) fp[q] = W[o + q * a.fs];
+        const double bt = W[o + 18 * a.fs], et = W[o + 19 * a.fs];
+        const int pi[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+        double lij[6], sv[6];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = i; j < 3; j++) {
+                lij[pi[i][j]] = fp[pi[i][j]] - fu[i] * fu[j];
+                sv[pi[i][j]] = 0.5 * (g[3 * i + j] + g[3 * j + i]);
+            }
+        const double lkk = (lij[0] + lij[3]) + lij[5];
+        const double cc = lkk < 1e-10 ? 0.0 : 2.0 * (bt + et) / lkk;
+        double ss = sv[0] * sv[0];
+        ss = ss + 2.0 * (sv[1] * sv[1]);
+        ss = ss + 2.0 * (sv[2] * sv[2]);
+        ss = ss + sv[3] * sv[3];
+        ss = ss + 2.0 * (sv[4] * sv[4]);
+        ss = ss + sv[5] * sv[5];
+        const double nut = sqrt(2.0 * ss) * cd2;
+        double ls = -lij[0] * sv[0];
+        ls = ls - lij[3] * sv[3];
+        ls = ls - lij[5] * sv[5];
+        ls = ls - 2.0 * lij[1] * sv[1];
+        ls = ls - 2.0 * lij[2] * sv[2];
+        ls = ls - 2.0 * lij[4] * sv[4];
+        const double prod = ls * cc + a.cmix * (nut * nut * nut) / cd4;
+        const double bb = bt * (nut / cd2);
+        const double eps = pow(et > 0.0 ? et : 0.0, 1.5) / a.delta;
+        W[o + 6 * a.fs] = prod - bb;
+        W[o + 7 * a.fs] = bb - eps;
+#pragma unroll
+        for (int q = 0; q < 6; q++) W[o + q * a.fs] = cc * lij[q] - a.cmix * 2.0 * nut * sv[q];
+#pragma unroll
+        for (int q = 0; q < 6; q++) W[o + (20 + q) * a.fs] = W[o + (20 + q) * a.fs] * nut;
+        psum += prod;
+        bsum += bb;
+        dsum += eps;
+    }
+    block_sums3(psum, bsum, dsum, part);
+}
+
 // out[0..3] = energy, production, B, dissipation of les.gp (m_les.f90:876-892):
-// the mean k_sgs from its zero mode K0 (unnormalised forward transform) and the
-// block sums divided by N^3; one warp, fixed summation order
+// the mean k_sgs from the zero mode K0 (plus K1: (B T_B) + (eps T_eps) for
+// les_model 10) of the unnormalised forward transform, and the block sums
+// divided by N^3; one warp, fixed summation order
 __global__ void k_dlm_stats(int nblk, double inv_n3, const double2 *__restrict__ K0, const double *__restrict__ part,
-                            double *__restrict__ out)
+                            double *__restrict__ out, const double2 *__restrict__ K1 = nullptr)
 {
     double p = 0.0, b = 0.0, d = 0.0;
     for (int q = threadIdx.x; q < nblk; q += 32) {
@@ -793,7 +856,7 @@ __global__ void k_dlm_stats(int nblk, double inv_n3, const double2 *__restrict__
         d += __shfl_xor_sync(0xffffffffu, d, off);
     }
     if (threadIdx.x == 0) {
-        out[0] = K0[0].x * inv_n3;
+        out[0] = (K1 != nullptr ? K0[0].x + K1[0].x : K0[0].x) * inv_n3;
         out[1] = p * inv_n3;
         out[2] = b * inv_n3;
         out[3] = d * inv_n3;

@@ -85,9 +85,10 @@ class Simulation:
         self.log = []
 
     def _les_constants(self):
-        """C_T of les_model 5 from c_t.in and C_mixed of les_models 6, 7 from
+        """C_T of les_model 5 from c_t.in and C_mixed of les_models 6, 7, 10 from
         c_mixed.in, first value of the file, as m_les_init reads them
-        (m_les.f90:189-207, 213-290); a missing file stops the run."""
+        (m_les.f90:189-207, 213-290, 314-335); a missing file stops the run,
+        except for les_model 10, which then takes C_mixed = 0.5."""
         def first_value(name):
             path = os.path.join(self.wd, name)
             if not os.path.exists(path):
@@ -97,7 +98,12 @@ class Simulation:
             except (IndexError, ValueError) as e:
                 raise InputFileError(f"bad value in {name}") from e
         m = self.cfg.les_model
-        return (first_value("c_t.in") if m == 5 else 1.0), (first_value("c_mixed.in") if m in (6, 7) else 0.0)
+        c_mixed = 0.0
+        if m in (6, 7):
+            c_mixed = first_value("c_mixed.in")
+        elif m == 10:
+            c_mixed = first_value("c_mixed.in") if os.path.exists(os.path.join(self.wd, "c_mixed.in")) else 0.5
+        return (first_value("c_t.in") if m == 5 else 1.0), c_mixed
 
     def _load_closure(self):
         s = self.settings

@@ -28,8 +28,8 @@ N_VARIANTS = 11  # launch-shape variants of the fused x pass (HIT3D_FUSED_VARIAN
 def les_fields(les_model: int) -> int:
     """LES-related transported fields (m_les.f90:111-300): k_sgs for the models with
     an algebraic dissipation (2, 4, 6); k_sgs, (B T_B), (eps T_eps) with the lag
-    model (3, 5, 7)."""
-    return {2: 1, 3: 3, 4: 1, 5: 3, 6: 1, 7: 3}.get(int(les_model), 0)
+    model (3, 5, 7); (B T_B), (eps T_eps) for the one-equation mixed model (10)."""
+    return {2: 1, 3: 3, 4: 1, 5: 3, 6: 1, 7: 3, 10: 2}.get(int(les_model), 0)
 
 
 _lib = None

@@ -83,8 +83,8 @@ def _variant(v: str) -> Optional[int]:
 
 def _les_model(v: str) -> int:
     x = int(v)
-    if x not in (0, 1, 2, 3, 4, 5, 6, 7, 20):
-        raise ValueError(f"les_model {x} is not supported (0-7 or 20)")
+    if x not in (0, 1, 2, 3, 4, 5, 6, 7, 10, 20):
+        raise ValueError(f"les_model {x} is not supported (0-7, 10 or 20)")
     return x
 
 

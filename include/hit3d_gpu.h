@@ -52,12 +52,14 @@ typedef struct hit3d_params {
                             the dissipation (m_les.f90:124-137); 4, 5: dynamic structure
                             model with the algebraic / lag dissipation (m_les.f90:138-190);
                             6, 7: mixed models, dynamic structure + C_mixed Smagorinsky
-                            (m_les.f90:208-300).  2, 4, 6 carry k_sgs as state field
-                            3+n_scalars; 3, 5, 7 k_sgs, (B T_B), (eps T_eps) as fields
-                            3+n_scalars .. 5+n_scalars; 2-7: FP64 only, no passive
-                            scalars; HIT3D_LES_LEARNED (20): learned closure
-                            (hit3d_gpu_les_set_mlp; no reference counterpart).
-                            The reference's model 10 is rejected.                          */
+                            (m_les.f90:208-300); 10: one-equation mixed model with the
+                            lag model and no k_sgs equation (m_les.f90:303-358).  2, 4, 6
+                            carry k_sgs as state field 3+n_scalars; 3, 5, 7 k_sgs,
+                            (B T_B), (eps T_eps) as fields 3+n_scalars .. 5+n_scalars;
+                            10 (B T_B), (eps T_eps) as 3+n_scalars, 4+n_scalars; 2-10:
+                            FP64 only, no passive scalars (so model 10's Harlow scalar
+                            fluxes are not built); HIT3D_LES_LEARNED (20): learned
+                            closure (hit3d_gpu_les_set_mlp; no reference counterpart). */
     int32_t scalar_type[HIT3D_MAX_SCALARS]; /* 0 = uniform mean gradient source            */
     int32_t device;      /* CUDA device ordinal                                            */
     int32_t reserved;
@@ -68,8 +70,8 @@ typedef struct hit3d_params {
     double sc[HIT3D_MAX_SCALARS]; /* Schmidt numbers; PE = nu/sc (m_parameters.f90:451)    */
     double c_t;          /* lag-model constant C_T of les_model 5 (the reference reads c_t.in,
                             m_les.f90:189-207); les_models 3 and 7 use C_T = 1             */
-    double c_mixed;      /* fraction C_mixed of the Smagorinsky viscosity in les_models 6, 7
-                            (the reference reads c_mixed.in, m_les.f90:213-290)            */
+    double c_mixed;      /* fraction C_mixed of the Smagorinsky viscosity in les_models 6, 7,
+                            10 (the reference reads c_mixed.in, m_les.f90:213-335)        */
 } hit3d_params;
 
 /* Allocate the device state, transform plans and wavenumber tables.
@@ -146,8 +148,9 @@ int hit3d_gpu_pruned(hit3d_ctx *ctx);
 int hit3d_gpu_check_finite(hit3d_ctx *ctx, int64_t *nonfinite);
 
 /* The les.gp quantities of the last step of a dynamic-localization run
- * (les_model 2-7; m_les.f90:876-892, the write of les_rhs_scalars):
- * out4 = {mean k_sgs, mean production (2 nu_t S:S, -tau_ij du_i/dx_j for
+ * (les_model 2-7, 10; m_les.f90:876-892, the write of les_rhs_scalars):
+ * out4 = {mean k_sgs ((B T_B) + (eps T_eps) for les_model 10), mean
+ * production (2 nu_t S:S, -tau_ij du_i/dx_j for
  * the dynamic structure models, their sum for the mixed ones), mean B (0
  * without the lag model), mean dissipation (k^(3/2)/Delta; with the lag
  * model (eps T_eps)^(3/2)/(Delta C_T^(3/2)))}, all from the state at the

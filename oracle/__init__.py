@@ -143,7 +143,7 @@ class Oracle:
             raise MemoryError("oracle_create failed")
         self.n, self.nscal = n, nscal
         # LES fields: k_sgs, and (B T_B), (eps T_eps) with the lag model
-        self.nles = {2: 1, 3: 3, 4: 1, 5: 3, 6: 1, 7: 3}.get(les_model, 0)
+        self.nles = {2: 1, 3: 3, 4: 1, 5: 3, 6: 1, 7: 3, 10: 2}.get(les_model, 0)
         self.nu = nu
         self.kmax = L.oracle_kmax(self._p)
         self.fsz = (n + 2) * n * n

@@ -217,6 +217,7 @@ typedef struct {
     double c_t, c_mixed;      /* lag-model scale (c_t.in) and mixed-model fraction (c_mixed.in) */
     double *gfilt;            /* test filter transfer function (DSTM models) */
     double *vsrc;             /* vel_source_les: 3 fields (DSTM models) */
+    double *tauij;            /* tauij: 6 fields, strain then stress (les_model 10) */
     int fov, fos, int_scalars;
     double *scratch;          /* per-thread FFT scratch: nthreads * 4n doubles */
     int nthreads;
@@ -404,7 +405,7 @@ oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_
      * k_sgs, (B T_B), (eps T_eps) with the lag model (m_les.f90:124-137); all
      * with Schmidt number one (m_les.f90:372-391) */
     o->nles = (les_model == 2 || les_model == 4 || les_model == 6) ? 1
-            : (les_model == 3 || les_model == 5 || les_model == 7) ? 3 : 0;
+            : (les_model == 3 || les_model == 5 || les_model == 7) ? 3 : les_model == 10 ? 2 : 0;
     o->c_t = 1.0;
     o->c_mixed = 0.0;
     if (o->nles && nscal > 0) { free(o); return NULL; }
@@ -417,7 +418,7 @@ oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_
     o->nwrk = 7;
     if (6 + nscal + o->nles > o->nwrk) o->nwrk = 6 + nscal + o->nles;
     /* the DSTM models use four work arrays past the LES fields (m_work.f90) */
-    if (les_model >= 4 && les_model <= 7 && 3 + nscal + o->nles + 5 > o->nwrk) o->nwrk = 3 + nscal + o->nles + 5;
+    if (les_model >= 4 && 3 + nscal + o->nles + 5 > o->nwrk) o->nwrk = 3 + nscal + o->nles + 5;
     o->fields = (double *)calloc(o->fsz * (3 + nscal + o->nles), sizeof(double));
     o->rhs_old = (double *)calloc(o->fsz * (3 + nscal + o->nles), sizeof(double));
     o->wrk = (double *)calloc(o->fsz * o->nwrk, sizeof(double));
@@ -472,6 +473,15 @@ oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_
         o->vsrc = (double *)calloc(3 * o->fsz, sizeof(double));
         oracle_filter_g(o, 2, 4.0 * o->dx, o->gfilt);
     }
+    /* les_model 10 (m_les.f90:592-608): (B T_B) = (eps T_eps) = 0.1, no k_sgs */
+    if (les_model == 10) {
+        const double n3 = (double)n * (double)n * (double)n;
+        F(o, 3 + nscal)[0] = 0.1 * n3;
+        F(o, 4 + nscal)[0] = 0.1 * n3;
+        o->gfilt = (double *)calloc(o->fsz, sizeof(double));
+        o->tauij = (double *)calloc(6 * o->fsz, sizeof(double));
+        oracle_filter_g(o, 2, 4.0 * o->dx, o->gfilt);
+    }
     return o;
 }
 
@@ -481,7 +491,7 @@ void oracle_destroy(oracle_t *o)
     free(o->fields); free(o->rhs_old); free(o->wrk); free(o->turb_visc);
     free(o->akx); free(o->aky); free(o->akz); free(o->ialias);
     free(o->fn_i); free(o->fn_j); free(o->fn_k); free(o->scratch);
-    free(o->gfilt); free(o->vsrc);
+    free(o->gfilt); free(o->vsrc); free(o->tauij);
     plan_free(&o->plan);
     free(o);
 }
@@ -584,6 +594,7 @@ static void les_get_turb_visc_smag(oracle_t *o)
 
 /* les_rhsv_turb_visc (m_les.f90:902-1018) followed by the ialias mask of
  * les_rhs_velocity (m_les.f90:682-690) */
+static void derivative(oracle_t *o, const double *src, char axis, double *dst);
 static void les_rhs_velocity(oracle_t *o)
 {
     int n = o->n;
@@ -595,6 +606,20 @@ static void les_rhs_velocity(oracle_t *o)
             double *r = W(o, 1 + m), *vs = o->vsrc + (size_t)m * o->fsz;
             for (size_t q = 0; q < o->fsz; q++) r[q] = r[q] + vs[q];
         }
+    if (o->les_model == 10) {
+        /* les_add_vel_source_from_tauij (m_les.f90:2344-2392) */
+        const size_t fsz = o->fsz;
+        const int comp[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+        const char dirs[3] = {'x', 'y', 'z'};
+        for (int q = 0; q < 6; q++) xfft3d(o, 1, o->tauij + (size_t)q * fsz);
+        double *d = W(o, 3 + o->nscal + o->nles + 1);
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) {
+                derivative(o, o->tauij + (size_t)comp[i][j] * fsz, dirs[j], d);
+                double *r = W(o, 1 + i);
+                for (size_t q = 0; q < fsz; q++) r[q] = r[q] - d[q];
+            }
+    }
     const int eddy = o->les_model <= 3 || o->les_model == 6 || o->les_model == 7;
     for (int pass = 0; pass < (eddy ? 2 : 0); pass++) {
         strain_first(o, pass);
@@ -955,6 +980,137 @@ static void les_get_turb_visc(oracle_t *o)
         les_get_turb_visc_smag(o);
         for (size_t q = 0; q < o->fsz; q++) o->turb_visc[q] = o->c_mixed * o->turb_visc[q];
     }
+    if (m == 10) {
+        /* les_get_turb_visc_smag_save_sij (m_les.f90:1223-1307): the same
+         * viscosity, the physical strain S11 S12 S13 S22 S23 S33 kept in tauij */
+        les_get_turb_visc_smag(o);
+        const size_t fsz = o->fsz;
+        for (int pass = 0; pass < 2; pass++) {
+            strain_first(o, pass);
+            for (int q = 0; q < 3; q++) {
+                xfft3d(o, -1, W(o, 4 + q));
+                memcpy(o->tauij + (size_t)(3 * pass + q) * fsz, W(o, 4 + q), sizeof(double) * fsz);
+            }
+        }
+    }
+}
+
+/* m_les_get_tauij_dstm_source_BT (m_les.f90:2009-2179), les_model 10: with
+ * k = (B T_B) + (eps T_eps), L_ij = (u_i u_j)~ - u~_i u~_j and c = 2 k / L_kk
+ * (0 where L_kk < 1e-10): tau_ij = c L_ij - 2 C_mixed nu_t S_ij, kept in tauij
+ * in physical space, and the (B T_B) source Pi = -c L_ij S_ij + C_mixed
+ * nu_t^3 / (c_s Delta)^4 (masked with the rest of the LES RHS afterwards). */
+static void les_tauij_dstm_source_bt(oracle_t *o)
+{
+    const int ns = o->nscal, nl = o->nles;
+    const int n2i = 3 + ns + nl + 1;
+    const size_t fsz = o->fsz;
+    double *w1 = W(o, 0), *a2 = W(o, n2i), *a3 = W(o, n2i + 1), *a4 = W(o, n2i + 2), *a5 = W(o, n2i + 3);
+    double *L[3] = {w1, a2, a3}, *tv = o->turb_visc, *ta = o->tauij;
+    for (int i = 0; i < 3; i++) {
+        copy_field(o, a4, F(o, i));
+        xfft3d(o, -1, a4);
+        for (size_t q = 0; q < fsz; q++) a4[q] = a4[q] * a4[q];
+        xfft3d(o, 1, a4);
+        oracle_apply_filter(o, o->gfilt, a4);
+        xfft3d(o, -1, a4);
+        copy_field(o, a5, F(o, i));
+        oracle_apply_filter(o, o->gfilt, a5);
+        xfft3d(o, -1, a5);
+        for (size_t q = 0; q < fsz; q++) L[i][q] = a4[q] - a5[q] * a5[q];
+    }
+    for (size_t q = 0; q < fsz; q++) a4[q] = w1[q] + a2[q] + a3[q];
+    for (size_t q = 0; q < fsz; q++) a5[q] = F(o, 3 + ns)[q] + F(o, 4 + ns)[q];
+    xfft3d(o, -1, a5);
+    for (int k = 0; k < o->n; k++)
+        for (int j = 0; j < o->n; j++)
+            for (int i = 0; i < o->n; i++) {
+                size_t q = IX(o, i, j, k);
+                a4[q] = a4[q] < 1e-10 ? 0.0 : 2.0 * a5[q] / a4[q];
+            }
+    for (size_t q = 0; q < fsz; q++)
+        a5[q] = -w1[q] * ta[q] - a2[q] * ta[3 * fsz + q] - a3[q] * ta[5 * fsz + q];
+    const int diag[3] = {0, 3, 5};
+    for (int d = 0; d < 3; d++)
+        for (int k = 0; k < o->n; k++)
+            for (int j = 0; j < o->n; j++)
+                for (int i = 0; i < o->n; i++) {
+                    size_t q = IX(o, i, j, k);
+                    double *t = ta + (size_t)diag[d] * fsz;
+                    t[q] = a4[q] * L[d][q] - o->c_mixed * 2.0 * tv[q] * t[q];
+                }
+    int nn = 0;
+    for (int i = 0; i < 3; i++)
+        for (int j = i; j < 3; j++, nn++) {
+            if (i == j) continue;
+            copy_field(o, w1, F(o, i)); copy_field(o, a2, F(o, j));
+            xfft3d(o, -1, w1); xfft3d(o, -1, a2);
+            for (size_t q = 0; q < fsz; q++) w1[q] = w1[q] * a2[q];
+            xfft3d(o, 1, w1);
+            oracle_apply_filter(o, o->gfilt, w1);
+            xfft3d(o, -1, w1);
+            copy_field(o, a2, F(o, i)); copy_field(o, a3, F(o, j));
+            oracle_apply_filter(o, o->gfilt, a2); oracle_apply_filter(o, o->gfilt, a3);
+            xfft3d(o, -1, a2); xfft3d(o, -1, a3);
+            double *t = ta + (size_t)nn * fsz;
+            for (size_t q = 0; q < fsz; q++) {
+                w1[q] = w1[q] - a2[q] * a3[q];
+                a5[q] = a5[q] - 2.0 * w1[q] * t[q];
+            }
+            for (int k = 0; k < o->n; k++)
+                for (int jj = 0; jj < o->n; jj++)
+                    for (int ii = 0; ii < o->n; ii++) {
+                        size_t q = IX(o, ii, jj, k);
+                        t[q] = a4[q] * w1[q] - o->c_mixed * 2.0 * tv[q] * t[q];
+                    }
+        }
+    const double cd = o->c_smag * o->les_delta, cd4 = cd * cd * cd * cd;
+    for (size_t q = 0; q < fsz; q++) a5[q] = a5[q] * a4[q];
+    for (int k = 0; k < o->n; k++)
+        for (int j = 0; j < o->n; j++)
+            for (int i = 0; i < o->n; i++) {
+                size_t q = IX(o, i, j, k);
+                a5[q] = a5[q] + o->c_mixed * (tv[q] * tv[q] * tv[q]) / cd4;
+            }
+    xfft3d(o, 1, a5);
+    double *rb = W(o, 3 + ns + 1);
+    for (size_t q = 0; q < fsz; q++) rb[q] = rb[q] + a5[q];
+    o->les_stat[1] = a5[0] / ((double)o->n * o->n * o->n);
+}
+
+/* m_les_lag_model_sources_no_k (m_les.f90:2282-2338): B = (B T_B) |S| with
+ * |S| = nu_t / (c_s Delta)^2, eps = max(eps T_eps, 0)^1.5 / (Delta C_T^1.5),
+ * C_T = 1; (B T_B) loses B, (eps T_eps) gains B - eps. */
+static void les_lag_model_sources_no_k(oracle_t *o)
+{
+    const int ns = o->nscal, nl = o->nles, n = o->n;
+    const size_t fsz = o->fsz;
+    double *w1 = W(o, 0), *a2 = W(o, 3 + ns + nl + 1), *a5 = W(o, 3 + ns + nl + 4), *tv = o->turb_visc;
+    const double cd = o->c_smag * o->les_delta, C_T = 1.0;
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                size_t q = IX(o, i, j, k);
+                a5[q] = tv[q] / (cd * cd);
+            }
+    copy_field(o, w1, F(o, 3 + ns));
+    xfft3d(o, -1, w1);
+    for (size_t q = 0; q < fsz; q++) w1[q] = w1[q] * a5[q];
+    xfft3d(o, 1, w1);
+    copy_field(o, a2, F(o, 4 + ns));
+    xfft3d(o, -1, a2);
+    for (size_t q = 0; q < fsz; q++) {
+        double v = a2[q] > 0.0 ? a2[q] : 0.0;
+        a2[q] = pow(v, 1.5) / (o->les_delta * pow(C_T, 1.5));
+    }
+    xfft3d(o, 1, a2);
+    double *rb = W(o, 3 + ns + 1), *re = W(o, 3 + ns + 2);
+    for (size_t q = 0; q < fsz; q++) {
+        rb[q] = rb[q] - w1[q];
+        re[q] = re[q] + w1[q] - a2[q];
+    }
+    o->les_stat[2] = w1[0] / ((double)n * n * n);
+    o->les_stat[3] = a2[0] / ((double)n * n * n);
 }
 
 static void oracle_rhs_scalars(oracle_t *o)
@@ -1068,7 +1224,9 @@ static void oracle_rhs_scalars(oracle_t *o)
     /* les_rhs_scalars, DLM branch (m_les.f90:714-719) */
     /* les_rhs_scalars (m_les.f90:700-858); les.gp sums restart every step */
     if (nl > 0) {
-        o->les_stat[0] = F(o, 3 + ns)[0] / ((double)o->n * o->n * o->n);
+        /* energy: k_sgs, or (B T_B) + (eps T_eps) for les_model 10 (m_les.f90:880-884) */
+        o->les_stat[0] = (F(o, 3 + ns)[0] + (o->les_model == 10 ? F(o, 4 + ns)[0] : 0.0)) /
+                         ((double)o->n * o->n * o->n);
         o->les_stat[1] = o->les_stat[2] = o->les_stat[3] = 0.0;
         switch (o->les_model) {
         case 2: les_k_src_dlm(o); les_k_diss_algebraic(o); break;
@@ -1077,9 +1235,22 @@ static void oracle_rhs_scalars(oracle_t *o)
         case 5: les_dstm_vel_k_sources(o); les_k_src_dlm(o); les_lag_model_sources(o); break;
         case 6: les_dstm_vel_k_sources(o); les_k_src_dlm(o); break;
         case 7: les_dstm_vel_k_sources(o); les_k_src_dlm(o); les_lag_model_sources(o); break;
+        case 10:
+            les_rhss_turb_visc1(o, 4 + ns);
+            les_rhss_turb_visc1(o, 5 + ns);
+            les_tauij_dstm_source_bt(o);
+            les_lag_model_sources_no_k(o);
+            break;
         }
-        for (int m = 4; m <= 3 + ns + nl; m++) les_rhss_turb_visc1(o, m);
+        if (o->les_model != 10)
+            for (int m = 4; m <= 3 + ns + nl; m++) les_rhss_turb_visc1(o, m);
         if (o->les_model == 6) les_k_diss_algebraic(o);
+        /* no aliasing in the scalar RHSs (m_les.f90:860-870) */
+        for (int m = 4; m <= 3 + ns + nl; m++) {
+            double *r = W(o, m);
+            for (size_t q = 0; q < o->fsz; q++)
+                if (o->ialias[q] != 0) r[q] = 0.0;
+        }
     }
 }
 

@@ -65,9 +65,9 @@ def test_unsupported_size_rejected_before_device_use():
 
 
 def test_reference_les_models_without_a_port_are_rejected():
-    """The reference's LES model 10 (mixed model with Harlow scalar fluxes) is not
-    built: an input asking for it fails at init instead of running another model."""
+    """The reference has no LES models 8 and 9 (m_les.f90:364-368 stops on them):
+    an input asking for one fails at init."""
     from hit3d_b200 import Hit3dError, Params, Context
-    for m in (8, 9, 10):
+    for m in (8, 9, 11):
         with pytest.raises(Hit3dError, match="les_model"):
             Context(Params(nx=32, les_model=m))

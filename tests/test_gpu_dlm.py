@@ -117,3 +117,24 @@ def test_les_constants_are_required():
     for m in (6, 7):
         with pytest.raises(Hit3dError, match="C_mixed"):
             Context(Params(nx=32, les_model=m))
+
+
+def test_one_equation_mixed_model_matches_oracle():
+    """les_model 10 (m_les.f90:303-358, 2009-2392): (B T_B) and (eps T_eps)
+    transported, k = their sum, tau from the DSTM with C_mixed times the
+    Smagorinsky stress; parity of the five fields and the les.gp means."""
+    n = 32
+    o, g = make_pair(n, flow_type=1, les_model=10, nu=1.0 / 2000.0, dt=0.004, isp_type=2, c_mixed=0.4)
+    f0 = g.download_fields()
+    assert f0.shape[0] == 5
+    assert f0[3, 0, 0, 0] == f0[4, 0, 0, 0] == pytest.approx(0.1 * n ** 3, rel=1e-15)
+    for _ in range(3):
+        o.step(3)
+        g.step(3)
+        f = g.download_fields()
+        for m in range(5):
+            assert relerr(f[m], o.fields[m]) < 1e-10, m
+        gs, os_ = g.les_stats(), o.les_stats()
+        for k in ("energy", "production", "B", "dissipation"):
+            assert gs[k] == pytest.approx(os_[k], rel=1e-10, abs=1e-14), k
+    assert relerr(g.download_rhs_old(), o.rhs_old) < 1e-9

@@ -154,7 +154,7 @@ def test_sidecar_keys_and_defaults(tmp_path):
     ("precision", "key = value"),
     ("precision = 1\nprecision = 0", "twice"),
     ("c_smag = -0.1", "positive"),
-    ("les_model = 10", "not supported"),
+    ("les_model = 8", "not supported"),
     ("les_model = 20", "les_mlp"),
     ("device =", "no value"),
 ])

@@ -387,3 +387,52 @@ def test_dynamic_structure_model_against_numpy(model, k0):
             want = vsrc[i] + eddy[i]
             assert np.abs(d[i] - want).max() <= 1e-10 * np.abs(want).max()
         assert st["production"] == pytest.approx(prod + (2 * nut * ss).mean(), rel=1e-10)
+
+
+def test_model_10_against_numpy():
+    """les_model 10 (m_les.f90:2009-2392) restated in numpy at its initial state
+    (B T_B) = (eps T_eps) = 0.1: k = 0.2, c = 2 k / L_kk, tau_ij = c L_ij -
+    2 C_mixed nu_t S_ij (nu_t Smagorinsky's), the velocity RHS gains -d
+    tau_ij/dx_j on the 2/3-rule modes; production <-c L:S + C_mixed nu_t^3 /
+    (c_s dx)^4>, B = 0.1 <|S|>, dissipation 0.1^1.5 / dx."""
+    n, cm = 32, 0.4
+    kw = dict(flow_type=0, nu=1.0 / 2000.0)
+    o = oracle.Oracle(n, les_model=10, **kw)
+    o.set_les_constants(c_mixed=cm)
+    o0 = oracle.Oracle(n, les_model=0, **kw)
+    o0.init_velocity(RN1, isp_type=1, peak_wavenum=4.0)
+    o0.dealias_all()
+    o.fields[:3] = o0.fields[:3]
+    o.rhs()
+    o0.rhs()
+    u_hat = _to_complex(o0.fields[:3]).transpose(0, 2, 1, 3)
+    kz = np.fft.fftfreq(n, 1.0 / n)[:, None, None]
+    ky = np.fft.fftfreq(n, 1.0 / n)[None, :, None]
+    kx = np.arange(n // 2 + 1)[None, None, :]
+    kk = (kx, ky, kz)
+    inv = lambda f: np.fft.irfftn(f, s=(n, n, n), axes=(0, 1, 2))
+    fwd = lambda f: np.fft.rfftn(f, axes=(0, 1, 2))
+    dx = 2 * np.pi / n
+    G = _gaussian_transfer(n, 4 * dx)
+    u = [inv(u_hat[i]) for i in range(3)]
+    uf = [inv(G * u_hat[i]) for i in range(3)]
+    L = [[inv(G * fwd(u[i] * u[j])) - uf[i] * uf[j] for j in range(3)] for i in range(3)]
+    Lkk = L[0][0] + L[1][1] + L[2][2]
+    c = np.where(Lkk < 1e-10, 0.0, 2 * 0.2 / np.where(Lkk < 1e-10, 1.0, Lkk))
+    grad = [[inv(1j * kk[j] * u_hat[i]) for j in range(3)] for i in range(3)]
+    S = [[0.5 * (grad[i][j] + grad[j][i]) for j in range(3)] for i in range(3)]
+    ss = sum(S[i][j] ** 2 for i in range(3) for j in range(3))
+    cs = 0.18 * dx
+    nut = cs ** 2 * np.sqrt(2 * ss)
+    tau = [[c * L[i][j] - cm * 2 * nut * S[i][j] for j in range(3)] for i in range(3)]
+    keep = (np.abs(kz) <= n // 3) & (np.abs(ky) <= n // 3) & (kx <= n // 3)
+    vsrc = [np.where(keep, -sum(1j * kk[j] * fwd(tau[i][j]) for j in range(3)), 0) for i in range(3)]
+    d = _to_complex(o.wrk[1:4] - o0.wrk[1:4]).transpose(0, 2, 1, 3)
+    for i in range(3):
+        assert np.abs(d[i] - vsrc[i]).max() <= 1e-10 * np.abs(vsrc[i]).max()
+    st = o.les_stats()
+    lds = sum(L[i][j] * S[i][j] for i in range(3) for j in range(3))
+    assert st["energy"] == pytest.approx(0.2, rel=1e-14)
+    assert st["production"] == pytest.approx((-c * lds + cm * nut ** 3 / cs ** 4).mean(), rel=1e-10)
+    assert st["B"] == pytest.approx(0.1 * np.sqrt(2 * ss).mean(), rel=1e-12)
+    assert st["dissipation"] == pytest.approx(0.1 ** 1.5 / dx, rel=1e-13)
