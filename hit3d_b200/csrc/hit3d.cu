@@ -541,12 +541,17 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
         a.pe[p.n_scalars + j] = p.nu / 1.0;
         a.stype[p.n_scalars + j] = -1;
     }
-    // work fields of the dynamic localization models after the nprod products:
-    // model 2: [0,6) strain -> tau, [6] k cube -> k source, [7,10) grad k -> fluxes
+    // work fields of the LES models after the nprod products (nps passive scalars):
+    // model 1 with scalars: [0,6) strain -> tau, [6, 6+3 nps) scalar gradients -> fluxes
+    // model 2: [0,6) strain -> tau, [6] k cube -> k source, [7,10) grad k and
+    //          [10, 10+3 nps) scalar gradients -> fluxes
     // model 3: [0,6) strain -> tau, [6] (B T_B) -> k source, [7] (eps T_eps) -> B T_B
-    //          source, [8,17) gradients of the three -> fluxes, [17] eps T_eps source
-    // then k_sgs truncated (kf) and nu_t (nutf)
-    const int kf = nprod + (lag ? 18 : 10), nutf = kf + 1;
+    //          source, [8,17) gradients of the three and [17, 17+3 nps) scalar
+    //          gradients -> fluxes, [17+3 nps] eps T_eps source
+    // then, for 2 and 3, k_sgs truncated (kf) and nu_t (nutf)
+    // model 10: as k_m10_phys lays out, scalar gradients at [26, 26+3 nps)
+    const int nps = p.n_scalars, kf0 = 3 + p.n_scalars;  // kf0: first LES field of the state
+    const int kf = nprod + (lag ? 18 : 10) + 3 * nps, nutf = kf + 1;
 
     MARK(7);
     if constexpr (std::is_same<T, double>::value) {
@@ -555,7 +560,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
             // field replaces the state when its minimum is negative
             // (les_get_turb_visc_dlm, m_les.f90:1313-1388)
             MARK(6);
-            double2 *K = c->U + 3 * c->fs64;
+            double2 *K = c->U + kf0 * c->fs64;
             c->k2max = (double)c->kmax * (double)c->kmax;
             H3D_TRY(zinv<T>(c, 1, PRE_TRUNC, 0, K, c->fs64, Wf(kf), wfs, wp));
             H3D_TRY(spass<T>(c, 1, false, Wf(kf), wfs, wp, 1));
@@ -630,7 +635,28 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
         H3D_TRY(spass<T>(c, 2, true, Wf(0), wfs, wp, nprod));
 
         const cx<T> *tau = nullptr;
-        if (les) {
+        if (les && ns > 0) {
+            MARK(6);
+            // Smagorinsky with passive scalars: stress and the scalars' turbulent
+            // fluxes nu_t grad(phi) from the physical fields (m_les.f90:1142-1215,
+            // 902-1018, 1028-1091)
+            const int t0 = nprod, nf = 6 + 3 * ns;
+            H3D_TRY(zinv<T>(c, 3, PRE_STRAIN_A, 0, c->U, c->fs64, Wf(t0), wfs, wp));
+            H3D_TRY(zinv<T>(c, 3, PRE_STRAIN_B, 0, c->U, c->fs64, Wf(t0 + 3), wfs, wp));
+            for (int s = 0; s < ns; s++)
+                H3D_TRY(zinv<T>(c, 3, PRE_GRAD, 3 + s, c->U, c->fs64, Wf(t0 + 6 + 3 * s), wfs, wp));
+            H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, nf));
+            H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, nf));
+            const double cd = p.c_smag * c->dx;
+            k_smag_phys<T><<<pw_grid(c), 256, 0, c->st>>>(c->n, 2 * (int64_t)wp, 2 * wfs, cd * cd,
+                                                           reinterpret_cast<T *>(Wf(t0)),
+                                                           reinterpret_cast<T *>(Wf(t0 + 6)), 3 * ns);
+            H3D_LAUNCH_CHECK();
+            H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, nf));
+            H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, nf));
+            H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, nf));
+            tau = Wf(t0);
+        } else if (les) {
             MARK(6);
             // Smagorinsky stress from the same state (m_les.f90:1142-1215, 902-1018)
             const int t0 = nprod;
@@ -663,11 +689,11 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 H3D_TRY(zinv<T>(c, 3, PRE_FILT, 0, c->U, c->fs64, Wf(t0 + 6), wfs, wp));
                 for (int i = 0; i < 3; i++)
                     H3D_TRY(zinv<T>(c, 3, PRE_GRAD, i, c->U, c->fs64, Wf(t0 + 9 + 3 * i), wfs, wp));
-                H3D_TRY(zinv<T>(c, 1, PRE_COPY, 0, c->U + 3 * c->fs64, c->fs64, Wf(t0 + 18), wfs, wp));
-                if (lagm) H3D_TRY(zinv<T>(c, 2, PRE_COPY, 0, c->U + 4 * c->fs64, c->fs64, Wf(t0 + 19), wfs, wp));
-                else H3D_TRY(zinv<T>(c, 1, PRE_CUBE, 0, c->U + 3 * c->fs64, c->fs64, Wf(t0 + 19), wfs, wp));
+                H3D_TRY(zinv<T>(c, 1, PRE_COPY, 0, c->U + kf0 * c->fs64, c->fs64, Wf(t0 + 18), wfs, wp));
+                if (lagm) H3D_TRY(zinv<T>(c, 2, PRE_COPY, 0, c->U + (kf0 + 1) * c->fs64, c->fs64, Wf(t0 + 19), wfs, wp));
+                else H3D_TRY(zinv<T>(c, 1, PRE_CUBE, 0, c->U + kf0 * c->fs64, c->fs64, Wf(t0 + 19), wfs, wp));
                 for (int j = 0; j < nl; j++)
-                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, 3 + j, c->U, c->fs64, Wf(t0 + g0 + 3 * j), wfs, wp));
+                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, kf0 + j, c->U, c->fs64, Wf(t0 + g0 + 3 * j), wfs, wp));
                 H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, nfld));
                 H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, nfld));
                 DstmArgs da;
@@ -681,7 +707,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 k_dstm_phys<<<pw_grid(c), 256, 0, c->st>>>(da, reinterpret_cast<double *>(Wf(t0)), c->d_kmin + 8);
                 H3D_LAUNCH_CHECK();
                 k_dlm_stats<<<1, 32, 0, c->st>>>((int)pw_grid(c).x, 1.0 / ((double)c->n * c->n * c->n),
-                                                 c->U + 3 * c->fs64, c->d_kmin + 8, c->d_kmin + 4);
+                                                 c->U + kf0 * c->fs64, c->d_kmin + 8, c->d_kmin + 4);
                 H3D_LAUNCH_CHECK();
                 H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, 6 + nl));
                 H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, 6 + nl));
@@ -699,11 +725,13 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 H3D_TRY(zinv<T>(c, 3, PRE_FILT, 0, c->U, c->fs64, Wf(t0 + 6), wfs, wp));
                 for (int i = 0; i < 3; i++)
                     H3D_TRY(zinv<T>(c, 3, PRE_GRAD, i, c->U, c->fs64, Wf(t0 + 9 + 3 * i), wfs, wp));
-                H3D_TRY(zinv<T>(c, 2, PRE_COPY, 0, c->U + 3 * c->fs64, c->fs64, Wf(t0 + 18), wfs, wp));
+                H3D_TRY(zinv<T>(c, 2, PRE_COPY, 0, c->U + kf0 * c->fs64, c->fs64, Wf(t0 + 18), wfs, wp));
                 for (int j = 0; j < 2; j++)
-                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, 3 + j, c->U, c->fs64, Wf(t0 + 20 + 3 * j), wfs, wp));
-                H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, kM10Fields));
-                H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, kM10Fields));
+                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, kf0 + j, c->U, c->fs64, Wf(t0 + 20 + 3 * j), wfs, wp));
+                for (int s = 0; s < nps; s++)
+                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, 3 + s, c->U, c->fs64, Wf(t0 + kM10Fields + 3 * s), wfs, wp));
+                H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, kM10Fields + 3 * nps));
+                H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, kM10Fields + 3 * nps));
                 DstmArgs da;
                 memset(&da, 0, sizeof da);
                 da.n = c->n; da.rp = 2 * (int64_t)wp; da.fs = 2 * wfs;
@@ -711,18 +739,19 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 da.cs2 = cd * cd;
                 da.cmix = p.c_mixed;
                 da.delta = c->dx;
+                da.nps = nps;
                 k_m10_phys<<<pw_grid(c), 256, 0, c->st>>>(da, reinterpret_cast<double *>(Wf(t0)), c->d_kmin + 8);
                 H3D_LAUNCH_CHECK();
                 k_dlm_stats<<<1, 32, 0, c->st>>>((int)pw_grid(c).x, 1.0 / ((double)c->n * c->n * c->n),
-                                                 c->U + 3 * c->fs64, c->d_kmin + 8, c->d_kmin + 4,
-                                                 c->U + 4 * c->fs64);
+                                                 c->U + kf0 * c->fs64, c->d_kmin + 8, c->d_kmin + 4,
+                                                 c->U + (kf0 + 1) * c->fs64);
                 H3D_LAUNCH_CHECK();
                 H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, 8));
                 H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, 8));
                 H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, 8));
-                H3D_TRY(xr2c<T>(c, Wf(t0 + 20), wfs, wp, 6));
-                H3D_TRY(spass<T>(c, 1, true, Wf(t0 + 20), wfs, wp, 6));
-                H3D_TRY(spass<T>(c, 2, true, Wf(t0 + 20), wfs, wp, 6));
+                H3D_TRY(xr2c<T>(c, Wf(t0 + 20), wfs, wp, 6 + 3 * nps));
+                H3D_TRY(spass<T>(c, 1, true, Wf(t0 + 20), wfs, wp, 6 + 3 * nps));
+                H3D_TRY(spass<T>(c, 2, true, Wf(t0 + 20), wfs, wp, 6 + 3 * nps));
                 tau = Wf(t0);
             } else if (lag) {
                 // dynamic localization model with the lag model for the dissipation
@@ -731,23 +760,26 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 const int t0 = nprod;
                 H3D_TRY(zinv<T>(c, 3, PRE_STRAIN_A, 0, c->U, c->fs64, Wf(t0), wfs, wp));
                 H3D_TRY(zinv<T>(c, 3, PRE_STRAIN_B, 0, c->U, c->fs64, Wf(t0 + 3), wfs, wp));
-                H3D_TRY(zinv<T>(c, 2, PRE_COPY, 0, c->U + 4 * c->fs64, c->fs64, Wf(t0 + 6), wfs, wp));
+                const int ninv = 17 + 3 * nps;
+                H3D_TRY(zinv<T>(c, 2, PRE_COPY, 0, c->U + (kf0 + 1) * c->fs64, c->fs64, Wf(t0 + 6), wfs, wp));
                 for (int j = 0; j < 3; j++)
-                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, 3 + j, c->U, c->fs64, Wf(t0 + 8 + 3 * j), wfs, wp));
-                H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, 17));
-                H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, 17));
+                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, kf0 + j, c->U, c->fs64, Wf(t0 + 8 + 3 * j), wfs, wp));
+                for (int s = 0; s < nps; s++)
+                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, 3 + s, c->U, c->fs64, Wf(t0 + 17 + 3 * s), wfs, wp));
+                H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, ninv));
+                H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, ninv));
                 k_dll_phys<<<pw_grid(c), 256, 0, c->st>>>(
                     c->n, 2 * (int64_t)wp, 2 * wfs, c->dx, 1.0, reinterpret_cast<const double *>(Wf(nutf)),
                     reinterpret_cast<double *>(Wf(t0)), reinterpret_cast<double *>(Wf(t0 + 6)),
-                    reinterpret_cast<double *>(Wf(t0 + 7)), reinterpret_cast<double *>(Wf(t0 + 8)),
-                    reinterpret_cast<double *>(Wf(t0 + 17)), c->d_kmin + 8);
+                    reinterpret_cast<double *>(Wf(t0 + 7)), reinterpret_cast<double *>(Wf(t0 + 8)), 9 + 3 * nps,
+                    reinterpret_cast<double *>(Wf(t0 + ninv)), c->d_kmin + 8);
                 H3D_LAUNCH_CHECK();
                 k_dlm_stats<<<1, 32, 0, c->st>>>((int)pw_grid(c).x, 1.0 / ((double)c->n * c->n * c->n),
-                                                 c->U + 3 * c->fs64, c->d_kmin + 8, c->d_kmin + 4);
+                                                 c->U + kf0 * c->fs64, c->d_kmin + 8, c->d_kmin + 4);
                 H3D_LAUNCH_CHECK();
-                H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, 18));
-                H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, 18));
-                H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, 18));
+                H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, ninv + 1));
+                H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, ninv + 1));
+                H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, ninv + 1));
                 tau = Wf(t0);
             } else if (dlm) {
                 // dynamic localization model: tau = -2 nu_t S for the velocities, and
@@ -758,21 +790,24 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 const int t0 = nprod;
                 H3D_TRY(zinv<T>(c, 3, PRE_STRAIN_A, 0, c->U, c->fs64, Wf(t0), wfs, wp));
                 H3D_TRY(zinv<T>(c, 3, PRE_STRAIN_B, 0, c->U, c->fs64, Wf(t0 + 3), wfs, wp));
-                H3D_TRY(zinv<T>(c, 1, PRE_CUBE, 0, c->U + 3 * c->fs64, c->fs64, Wf(t0 + 6), wfs, wp));
-                H3D_TRY(zinv<T>(c, 3, PRE_GRAD, 3, c->U, c->fs64, Wf(t0 + 7), wfs, wp));
-                H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, 10));
-                H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, 10));
+                const int nall = 10 + 3 * nps;
+                H3D_TRY(zinv<T>(c, 1, PRE_CUBE, 0, c->U + kf0 * c->fs64, c->fs64, Wf(t0 + 6), wfs, wp));
+                H3D_TRY(zinv<T>(c, 3, PRE_GRAD, kf0, c->U, c->fs64, Wf(t0 + 7), wfs, wp));
+                for (int s = 0; s < nps; s++)
+                    H3D_TRY(zinv<T>(c, 3, PRE_GRAD, 3 + s, c->U, c->fs64, Wf(t0 + 10 + 3 * s), wfs, wp));
+                H3D_TRY(spass<T>(c, 1, false, Wf(t0), wfs, wp, nall));
+                H3D_TRY(xc2r<T>(c, Wf(t0), wfs, wp, nall));
                 k_dlm_phys<<<pw_grid(c), 256, 0, c->st>>>(
                     c->n, 2 * (int64_t)wp, 2 * wfs, c->dx, reinterpret_cast<const double *>(Wf(nutf)),
                     reinterpret_cast<double *>(Wf(t0)), reinterpret_cast<double *>(Wf(t0 + 6)),
-                    reinterpret_cast<double *>(Wf(t0 + 7)), c->d_kmin + 8);
+                    reinterpret_cast<double *>(Wf(t0 + 7)), 3 + 3 * nps, c->d_kmin + 8);
                 H3D_LAUNCH_CHECK();
                 k_dlm_stats<<<1, 32, 0, c->st>>>((int)pw_grid(c).x, 1.0 / ((double)c->n * c->n * c->n),
-                                                 c->U + 3 * c->fs64, c->d_kmin + 8, c->d_kmin + 4);
+                                                 c->U + kf0 * c->fs64, c->d_kmin + 8, c->d_kmin + 4);
                 H3D_LAUNCH_CHECK();
-                H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, 10));
-                H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, 10));
-                H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, 10));
+                H3D_TRY(xr2c<T>(c, Wf(t0), wfs, wp, nall));
+                H3D_TRY(spass<T>(c, 1, true, Wf(t0), wfs, wp, nall));
+                H3D_TRY(spass<T>(c, 2, true, Wf(t0), wfs, wp, nall));
                 tau = Wf(t0);
                 les_src = Wf(t0 + 6);
                 les_flux = Wf(t0 + 7);
@@ -799,20 +834,23 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
         if (p.dealias == 0) {
             for (int s = 0; s < ns; s++) {
                 // sources and turbulent fluxes of the LES fields (layout above)
+                // (passive scalars: j < 0, their turbulent or Harlow fluxes only)
                 const int j = s - p.n_scalars;
                 const cx<T> *src = nullptr, *flux = nullptr;
-                if (m10 && j >= 0) {
-                    src = Wf(nprod + 6 + j);
-                    flux = Wf(nprod + 20 + 3 * j);
+                if (m10) {
+                    if (j >= 0) { src = Wf(nprod + 6 + j); flux = Wf(nprod + 20 + 3 * j); }
+                    else flux = Wf(nprod + kM10Fields + 3 * s);
                 } else if (dstm && j >= 0) {
                     src = Wf(nprod + 6 + j);
                     flux = Wf(nprod + (les_nles(p.les_model) == 3 ? 21 : 20) + 3 * j);
-                } else if (lag && j >= 0) {
-                    src = Wf(nprod + (j == 0 ? 6 : j == 1 ? 7 : 17));
-                    flux = Wf(nprod + 8 + 3 * j);
-                } else if (dlm && j == 0) {
-                    src = les_src;
-                    flux = les_flux;
+                } else if (lag) {
+                    if (j >= 0) { src = Wf(nprod + (j == 0 ? 6 : j == 1 ? 7 : 17 + 3 * nps)); flux = Wf(nprod + 8 + 3 * j); }
+                    else flux = Wf(nprod + 17 + 3 * s);
+                } else if (dlm) {
+                    if (j == 0) { src = les_src; flux = les_flux; }
+                    else flux = Wf(nprod + 10 + 3 * s);
+                } else if (les) {
+                    flux = Wf(nprod + 6 + 3 * s);
                 }
                 k_scalar<T><<<pw_grid(c), 256, 0, c->st>>>(a, 0, s, c->dx, Wf(6 + 3 * s), nullptr, c->U,
                                                             c->U + (3 + s) * c->fs64, c->RO + (3 + s) * c->fs64,
@@ -916,7 +954,12 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     if ((p->les_model == 6 || p->les_model == 7) && !(p->c_mixed > 0.0))
         return h3d_set_error_msg(-1, "hit3d_gpu_init: les_models 6 and 7 need C_mixed > 0 (the reference reads it "
                                      "from c_mixed.in)");
-    if (p->les_model != 0 && p->n_scalars > 0) return h3d_set_error_msg(-1, "hit3d_gpu_init: LES with scalars is not supported");
+    // passive scalars with LES: turbulent diffusion (les_models 1-3,
+    // m_les.f90:1028-1036) or Harlow fluxes (10); the reference stops on
+    // scalars with les_models 4-7 (m_les.f90:725-800)
+    if (p->n_scalars > 0 && ((p->les_model >= 4 && p->les_model <= 7) || p->les_model == HIT3D_LES_LEARNED))
+        return h3d_set_error_msg(-1, "hit3d_gpu_init: passive scalars are not transported with les_model 4-7 or "
+                                     "20 (the reference cannot transport scalars with the dynamic structure models)");
     if (p->precision != 0 && p->precision != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: precision must be 0 or 1");
     for (int s = 0; s < p->n_scalars; s++) {
         if (p->scalar_type[s] >= 100) return h3d_set_error_msg(-1, "hit3d_gpu_init: reacting scalars are not supported");
@@ -952,11 +995,13 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     const int nf = 3 + c->nsc;
     const size_t f64 = (size_t)c->fs64 * sizeof(double2);
     c->nw = 6 + 3 * c->nsc +
-            (c->p.les_model == 1 ? 6 : c->p.les_model == HIT3D_LES_LEARNED ? 9 : c->p.les_model == 2 ? 12
-                                                                               : c->p.les_model == 3 ? 20
+            (c->p.les_model == 1 ? 6 + 3 * p->n_scalars : c->p.les_model == HIT3D_LES_LEARNED ? 9
+                                                                               : c->p.les_model == 2 ? 12 + 3 * p->n_scalars
+                                                                               : c->p.les_model == 3 ? 20 + 3 * p->n_scalars
                                                                                : les_dstm(c->p.les_model)
                                                                                    ? dstm_fields(les_nles(c->p.les_model))
-                                                                               : c->p.les_model == 10 ? kM10Fields
+                                                                               : c->p.les_model == 10
+                                                                                   ? kM10Fields + 3 * p->n_scalars
                                                                                    : 0);
     if (c->p.precision == 0) {
         c->wpitch = c->P64;
@@ -1020,13 +1065,14 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
         const int m = c->p.les_model;
         const double n3 = (double)c->n * (double)c->n * (double)c->n;
         const double2 k0 = make_double2((m <= 3 || m == 10 ? 0.1 : m == 4 ? 0.2 : 0.5) * n3, 0.0);
-        H3D_CHECK(cudaMemcpy(c->U + 3 * c->fs64, &k0, sizeof k0, cudaMemcpyHostToDevice));
-        if (m == 10) H3D_CHECK(cudaMemcpy(c->U + 4 * c->fs64, &k0, sizeof k0, cudaMemcpyHostToDevice));
+        const int kf0 = 3 + c->p.n_scalars;  // first LES field of the state
+        H3D_CHECK(cudaMemcpy(c->U + kf0 * c->fs64, &k0, sizeof k0, cudaMemcpyHostToDevice));
+        if (m == 10) H3D_CHECK(cudaMemcpy(c->U + (kf0 + 1) * c->fs64, &k0, sizeof k0, cudaMemcpyHostToDevice));
         if (les_nles(m) == 3) {
             const double2 b0 = make_double2(m == 3 ? 0.5 * k0.x : k0.x, 0.0);
             const double2 e0 = make_double2(m == 3 ? 0.5 * k0.x : 0.0, 0.0);
-            H3D_CHECK(cudaMemcpy(c->U + 4 * c->fs64, &b0, sizeof b0, cudaMemcpyHostToDevice));
-            H3D_CHECK(cudaMemcpy(c->U + 5 * c->fs64, &e0, sizeof e0, cudaMemcpyHostToDevice));
+            H3D_CHECK(cudaMemcpy(c->U + (kf0 + 1) * c->fs64, &b0, sizeof b0, cudaMemcpyHostToDevice));
+            H3D_CHECK(cudaMemcpy(c->U + (kf0 + 2) * c->fs64, &e0, sizeof e0, cudaMemcpyHostToDevice));
         }
         if (les_dstm(m) || m == 10) {
             // the test filter: Gaussian of width 4 dx (m_filter_xfftw.f90:140-150, 197-220)
@@ -1317,7 +1363,12 @@ extern "C" int hit3d_gpu_set_dt(hit3d_ctx *c, double dt)
 extern "C" int hit3d_gpu_set_scalars_active(hit3d_ctx *c, int32_t on)
 {
     if (!c) return h3d_set_error_msg(-1, "null context");
-    // the LES fields are always transported (rhs_scalars.f90:72-74)
+    // the LES fields are always transported (rhs_scalars.f90:72-74).  While the
+    // passive scalars wait for TSCALAR, the reference still diffuses them with
+    // nu_t in that case; that mixed state is not supported
+    if (on == 0 && les_nles(c->p.les_model) > 0 && c->p.n_scalars > 0)
+        return h3d_set_error_msg(-1, "hit3d_gpu_set_scalars_active: with the LES fields of les_model 2, 3 or 10, "
+                                     "passive scalars move from the start (TSCALAR <= 0)");
     c->int_scalars = ((on != 0) && c->nsc > 0) || les_nles(c->p.les_model) > 0;
     return 0;
 }

@@ -311,9 +311,10 @@ __global__ void k_scalar(const StepArgs a, int mode, int s, double dx, const cx<
             r.x = r.x - u.x;
             r.y = r.y - u.y;
         }
-        if (LS != nullptr && m.ialias == 0) {
-            const double2 sv = ld2<TP>(LS, po), f1 = ld2<TP>(LF, po), f2 = ld2<TP>(LF, po + a.pfs),
-                          f3 = ld2<TP>(LF, po + 2 * a.pfs);
+        // LES: the source LS (LES fields only) and the divergence of the fluxes LF
+        if (LF != nullptr && m.ialias == 0) {
+            const double2 sv = LS != nullptr ? ld2<TP>(LS, po) : make_double2(0.0, 0.0), f1 = ld2<TP>(LF, po),
+                          f2 = ld2<TP>(LF, po + a.pfs), f3 = ld2<TP>(LF, po + 2 * a.pfs);
             r.x = r.x + sv.x - (kx * f1.y + ky * f2.y + kz * f3.y);
             r.y = r.y + sv.y + (kx * f1.x + ky * f2.x + kz * f3.x);
         }
@@ -601,7 +602,7 @@ H3D_D void block_sums3(double a, double b, double d, double *__restrict__ part)
 // (m_les.f90:1536,1617)
 __global__ void __launch_bounds__(256) k_dlm_phys(int n, int64_t rp, int64_t fs, double delta,
                                                   const double *__restrict__ NUT, double *__restrict__ S,
-                                                  double *__restrict__ KC, double *__restrict__ G,
+                                                  double *__restrict__ KC, double *__restrict__ G, int ng,
                                                   double *__restrict__ part)
 {
     const int64_t np = (int64_t)n * n * n;
@@ -625,8 +626,7 @@ __global__ void __launch_bounds__(256) k_dlm_phys(int n, int64_t rp, int64_t fs,
         dsum += diss;
 #pragma unroll
         for (int c = 0; c < 6; c++) S[o + c * fs] = (-2.0 * nut) * sv[c];
-#pragma unroll
-        for (int d = 0; d < 3; d++) G[o + d * fs] = G[o + d * fs] * nut;
+        for (int d = 0; d < ng; d++) G[o + d * fs] = G[o + d * fs] * nut;
     }
     block_sums3(psum, 0.0, dsum, part);
 }
@@ -643,7 +643,7 @@ __global__ void __launch_bounds__(256) k_dlm_phys(int n, int64_t rp, int64_t fs,
 __global__ void __launch_bounds__(256) k_dll_phys(int n, int64_t rp, int64_t fs, double delta, double c_t,
                                                   const double *__restrict__ NUT, double *__restrict__ S,
                                                   double *__restrict__ BT, double *__restrict__ ET,
-                                                  double *__restrict__ G, double *__restrict__ S3,
+                                                  double *__restrict__ G, int ng, double *__restrict__ S3,
                                                   double *__restrict__ part)
 {
     const int64_t np = (int64_t)n * n * n;
@@ -674,8 +674,7 @@ __global__ void __launch_bounds__(256) k_dll_phys(int n, int64_t rp, int64_t fs,
         dsum += eps;
 #pragma unroll
         for (int c = 0; c < 6; c++) S[o + c * fs] = (-2.0 * nut) * sv[c];
-#pragma unroll
-        for (int d = 0; d < 9; d++) G[o + d * fs] = G[o + d * fs] * nut;
+        for (int d = 0; d < ng; d++) G[o + d * fs] = G[o + d * fs] * nut;
     }
     block_sums3(psum, bsum, dsum, part);
 }
@@ -700,6 +699,7 @@ struct DstmArgs {
     int64_t rp, fs;
     int lag, mixed, g0;
     double cs2, cmix, delta, c_t;
+    int nps;  // les_model 10: passive scalars, their gradients at W[26 + 3 s] -> Harlow fluxes
 };
 __global__ void __launch_bounds__(256) k_dstm_phys(const DstmArgs a, double *__restrict__ W, double *__restrict__ part)
 {
@@ -826,15 +826,57 @@ __global__ void __launch_bounds__(256) k_m10_phys(const DstmArgs a, double *__re
         const double eps = pow(et > 0.0 ? et : 0.0, 1.5) / a.delta;
         W[o + 6 * a.fs] = prod - bb;
         W[o + 7 * a.fs] = bb - eps;
+        double tau[6];
 #pragma unroll
-        for (int q = 0; q < 6; q++) W[o + q * a.fs] = cc * lij[q] - a.cmix * 2.0 * nut * sv[q];
+        for (int q = 0; q < 6; q++) {
+            tau[q] = cc * lij[q] - a.cmix * 2.0 * nut * sv[q];
+            W[o + q * a.fs] = tau[q];
+        }
 #pragma unroll
         for (int q = 0; q < 6; q++) W[o + (20 + q) * a.fs] = W[o + (20 + q) * a.fs] * nut;
+        // Harlow fluxes of the passive scalars (m_les.f90:2191-2270): T tau_ij dphi/dx_j
+        // with the time scale T = 1/|S|, |S| = nu_t / (c_s Delta)^2 (T = 0 where |S| < 1e-10)
+        const double sm = nut / cd2;
+        const double tt = fabs(sm) < 1e-10 ? 0.0 : 1.0 / sm;
+        for (int s = 0; s < a.nps; s++) {
+            double *gp = W + o + (26 + 3 * s) * a.fs;
+            const double g0 = gp[0], g1 = gp[a.fs], g2 = gp[2 * a.fs];
+            gp[0] = (tau[0] * g0 + tau[1] * g1 + tau[2] * g2) * tt;
+            gp[a.fs] = (tau[1] * g0 + tau[3] * g1 + tau[4] * g2) * tt;
+            gp[2 * a.fs] = (tau[2] * g0 + tau[4] * g1 + tau[5] * g2) * tt;
+        }
         psum += prod;
         bsum += bb;
         dsum += eps;
     }
     block_sums3(psum, bsum, dsum, part);
+}
+
+// Smagorinsky model with passive scalars (les_model 1; m_les.f90:1142-1215,
+// 902-1018, 1041-1091): from the six strain components S (physical, in place),
+// nu_t = (c_s Delta)^2 sqrt(2 S:S), tau = -2 nu_t S, and the ng scalar gradient
+// fields G times nu_t (the turbulent fluxes)
+template <typename T>
+__global__ void __launch_bounds__(256) k_smag_phys(int n, int64_t rp, int64_t fs, double cs2, T *__restrict__ S,
+                                                   T *__restrict__ G, int ng)
+{
+    const int64_t np = (int64_t)n * n * n;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / n, o = row * rp + (t - row * n);
+        double sv[6];
+#pragma unroll
+        for (int c = 0; c < 6; c++) sv[c] = (double)S[o + c * fs];
+        double ss = sv[0] * sv[0];
+        ss = ss + 2.0 * (sv[1] * sv[1]);
+        ss = ss + 2.0 * (sv[2] * sv[2]);
+        ss = ss + sv[3] * sv[3];
+        ss = ss + 2.0 * (sv[4] * sv[4]);
+        ss = ss + sv[5] * sv[5];
+        const double nut = sqrt(2.0 * ss) * cs2;
+#pragma unroll
+        for (int c = 0; c < 6; c++) S[o + c * fs] = (T)((-2.0 * nut) * sv[c]);
+        for (int d = 0; d < ng; d++) G[o + d * fs] = (T)((double)G[o + d * fs] * nut);
+    }
 }
 
 // out[0..3] = energy, production, B, dissipation of les.gp (m_les.f90:876-892):

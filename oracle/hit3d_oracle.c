@@ -408,7 +408,8 @@ oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_
             : (les_model == 3 || les_model == 5 || les_model == 7) ? 3 : les_model == 10 ? 2 : 0;
     o->c_t = 1.0;
     o->c_mixed = 0.0;
-    if (o->nles && nscal > 0) { free(o); return NULL; }
+    /* passive scalars go with les_models 0-3 and 10 (m_les.f90:725-800 stops on 4-7) */
+    if (nscal > 0 && les_model >= 4 && les_model <= 7) { free(o); return NULL; }
     /* kmax (m_parameters.f90:123-131) */
     if (dealias == 0) o->kmax = n / 3;
     else o->kmax = (int)floor((double)n / 3.0 * sqrt(2.0));
@@ -1078,6 +1079,44 @@ static void les_tauij_dstm_source_bt(oracle_t *o)
     o->les_stat[1] = a5[0] / ((double)o->n * o->n * o->n);
 }
 
+/* m_les_rhss_sgs_flux_harlow (m_les.f90:2191-2270): for each passive scalar
+ * the RHS gains d/dx_i (T tau_ij dphi/dx_j), tau_ij the physical stress left in
+ * tauij, T = (c_s Delta)^2 / nu_t (0 where nu_t / (c_s Delta)^2 < 1e-10). */
+static void les_rhss_sgs_flux_harlow(oracle_t *o)
+{
+    const int ns = o->nscal, nl = o->nles, n = o->n;
+    const size_t fsz = o->fsz;
+    double *w1 = W(o, 0), *a2 = W(o, 3 + ns + nl + 1), *a3 = W(o, 3 + ns + nl + 2), *a4 = W(o, 3 + ns + nl + 3),
+           *a5 = W(o, 3 + ns + nl + 4), *tv = o->turb_visc, *ta = o->tauij;
+    const double cd = o->c_smag * o->les_delta;
+    for (int k = 0; k < n; k++)
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                size_t q = IX(o, i, j, k);
+                double v = tv[q] / (cd * cd);
+                a5[q] = fabs(v) < 1e-10 ? 0.0 : 1.0 / v;
+            }
+    const int row[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    const char dirs[3] = {'x', 'y', 'z'};
+    for (int s = 1; s <= ns; s++) {
+        copy_field(o, w1, F(o, 2 + s));
+        derivative(o, w1, 'z', a3);
+        derivative(o, w1, 'y', a2);
+        derivative(o, w1, 'x', w1);
+        xfft3d(o, -1, w1); xfft3d(o, -1, a2); xfft3d(o, -1, a3);
+        double *r = W(o, 3 + s);
+        for (int c = 0; c < 3; c++) {
+            const double *t0 = ta + (size_t)row[c][0] * fsz, *t1 = ta + (size_t)row[c][1] * fsz,
+                         *t2 = ta + (size_t)row[c][2] * fsz;
+            for (size_t q = 0; q < fsz; q++) a4[q] = t0[q] * w1[q] + t1[q] * a2[q] + t2[q] * a3[q];
+            for (size_t q = 0; q < fsz; q++) a4[q] = a4[q] * a5[q];
+            xfft3d(o, 1, a4);
+            derivative(o, a4, dirs[c], a4);
+            for (size_t q = 0; q < fsz; q++) r[q] = r[q] + a4[q];
+        }
+    }
+}
+
 /* m_les_lag_model_sources_no_k (m_les.f90:2282-2338): B = (B T_B) |S| with
  * |S| = nu_t / (c_s Delta)^2, eps = max(eps T_eps, 0)^1.5 / (Delta C_T^1.5),
  * C_T = 1; (B T_B) loses B, (eps T_eps) gains B - eps. */
@@ -1223,10 +1262,11 @@ static void oracle_rhs_scalars(oracle_t *o)
         }
     /* les_rhs_scalars, DLM branch (m_les.f90:714-719) */
     /* les_rhs_scalars (m_les.f90:700-858); les.gp sums restart every step */
-    if (nl > 0) {
+    if (o->les_model) {
         /* energy: k_sgs, or (B T_B) + (eps T_eps) for les_model 10 (m_les.f90:880-884) */
-        o->les_stat[0] = (F(o, 3 + ns)[0] + (o->les_model == 10 ? F(o, 4 + ns)[0] : 0.0)) /
-                         ((double)o->n * o->n * o->n);
+        if (nl > 0)
+            o->les_stat[0] = (F(o, 3 + ns)[0] + (o->les_model == 10 ? F(o, 4 + ns)[0] : 0.0)) /
+                             ((double)o->n * o->n * o->n);
         o->les_stat[1] = o->les_stat[2] = o->les_stat[3] = 0.0;
         switch (o->les_model) {
         case 2: les_k_src_dlm(o); les_k_diss_algebraic(o); break;
@@ -1239,6 +1279,7 @@ static void oracle_rhs_scalars(oracle_t *o)
             les_rhss_turb_visc1(o, 4 + ns);
             les_rhss_turb_visc1(o, 5 + ns);
             les_tauij_dstm_source_bt(o);
+            if (ns > 0) les_rhss_sgs_flux_harlow(o);
             les_lag_model_sources_no_k(o);
             break;
         }

@@ -83,7 +83,7 @@ def test_dlm_rejects_what_it_does_not_support():
     with pytest.raises(Hit3dError, match="FP64"):
         Context(Params(nx=32, les_model=2, precision=1))
     with pytest.raises(Hit3dError, match="scalars"):
-        Context(Params(nx=32, les_model=2, n_scalars=1, sc=[1.0], scalar_type=[0]))
+        Context(Params(nx=32, les_model=5, n_scalars=1, sc=[1.0], scalar_type=[0], c_t=1.0))
 
 
 @pytest.mark.parametrize("model,nles", [(4, 1), (5, 3), (6, 1), (7, 3)])
@@ -138,3 +138,47 @@ def test_one_equation_mixed_model_matches_oracle():
         for k in ("energy", "production", "B", "dissipation"):
             assert gs[k] == pytest.approx(os_[k], rel=1e-10, abs=1e-14), k
     assert relerr(g.download_rhs_old(), o.rhs_old) < 1e-9
+
+
+@pytest.mark.parametrize("model", [1, 2, 3, 10])
+def test_les_with_passive_scalars_matches_oracle(model):
+    """Passive scalars under LES: turbulent diffusion with nu_t (les_models 1-3,
+    m_les.f90:1028-1091) or Harlow fluxes (10, m_les.f90:2191-2270), next to the
+    LES fields, which follow the scalars in the state."""
+    n = 32
+    kw = dict(flow_type=1, les_model=model, nu=1.0 / 2000.0, dt=0.004, isp_type=2, nscal=2, sc=(0.7, 1.0),
+              scalar_type=(0, 1), c_mixed=0.4)
+    o, g = make_pair(n, **kw)
+    f = g.download_fields()
+    rng = np.random.default_rng(model)
+    for s in (3, 4):   # smooth scalar fields inside the 2/3-rule cube
+        f[s] = 0.0
+        for _ in range(8):
+            # kx >= 1: no Hermitian constraint to respect on the kx = 0 plane
+            ky, kz, kx = rng.integers(-5, 6), rng.integers(-5, 6), rng.integers(1, 6)
+            f[s, ky % n, kz % n, 2 * kx:2 * kx + 2] = rng.standard_normal(2) * n ** 3 * 0.01
+    g.upload_fields(f)
+    g.dealias_all()
+    f = g.download_fields()
+    o.fields[:] = f
+    g.set_scalars_active(True)
+    o.set_flags(1, 1, 1)
+    for _ in range(3):
+        o.step(3)
+        g.step(3)
+        got = g.download_fields()
+        for m in range(got.shape[0]):
+            assert relerr(got[m], o.fields[m]) < 1e-10, m
+    if model != 1:
+        gs, os_ = g.les_stats(), o.les_stats()
+        for k in ("energy", "production", "B", "dissipation"):
+            assert gs[k] == pytest.approx(os_[k], rel=1e-10, abs=1e-14), k
+
+
+def test_les_fields_need_active_passive_scalars():
+    from hit3d_b200 import Context, Hit3dError, Params
+    with Context(Params(nx=32, les_model=2, n_scalars=1, sc=[1.0], scalar_type=[0])) as c:
+        with pytest.raises(Hit3dError, match="TSCALAR"):
+            c.set_scalars_active(False)
+    with pytest.raises(Hit3dError, match="scalars"):
+        Context(Params(nx=32, les_model=4, n_scalars=1, sc=[1.0], scalar_type=[0]))

@@ -436,3 +436,65 @@ def test_model_10_against_numpy():
     assert st["production"] == pytest.approx((-c * lds + cm * nut ** 3 / cs ** 4).mean(), rel=1e-10)
     assert st["B"] == pytest.approx(0.1 * np.sqrt(2 * ss).mean(), rel=1e-12)
     assert st["dissipation"] == pytest.approx(0.1 ** 1.5 / dx, rel=1e-13)
+
+
+def _scalar_field(n, seed):
+    """A smooth scalar field inside the 2/3-rule cube, in the reference layout."""
+    rng = np.random.default_rng(seed)
+    X, Y, Z = _grid(n)
+    f = sum(rng.standard_normal() * np.cos(a * X + b * Y + c * Z + rng.uniform(0, 6.28))
+            for a, b, c in rng.integers(-4, 5, size=(10, 3)))
+    a = _phys(n, f)
+    return a
+
+
+@pytest.mark.parametrize("model", [1, 10])
+def test_les_scalar_fluxes_against_numpy(model):
+    """Passive scalars under LES: les_model 1 adds d/dx_i (nu_t dphi/dx_i)
+    (m_les.f90:1028-1091); les_model 10 adds d/dx_i (T tau_ij dphi/dx_j) with
+    T = (c_s dx)^2 / nu_t (Harlow, m_les.f90:2191-2270); both on the 2/3-rule
+    modes, restated in numpy against a run without LES."""
+    n, cm = 32, 0.4
+    kw = dict(flow_type=0, nu=1.0 / 2000.0, nscal=1, sc=(0.7,), scalar_type=(1,))
+    o = oracle.Oracle(n, les_model=model, **kw)
+    o.set_les_constants(c_mixed=cm)
+    o0 = oracle.Oracle(n, les_model=0, **kw)
+    o0.init_velocity(RN1, isp_type=1, peak_wavenum=4.0)
+    a = _scalar_field(n, 3)
+    o0.fft3d(1, a)
+    o0.fields[3] = a
+    o0.dealias_all()
+    o.fields[:4] = o0.fields[:4]
+    for x in (o, o0):
+        x.set_flags(1, 1, 1)
+        x.rhs()
+    u_hat = _to_complex(o0.fields[:4]).transpose(0, 2, 1, 3)
+    kz = np.fft.fftfreq(n, 1.0 / n)[:, None, None]
+    ky = np.fft.fftfreq(n, 1.0 / n)[None, :, None]
+    kx = np.arange(n // 2 + 1)[None, None, :]
+    kk = (kx, ky, kz)
+    inv = lambda f: np.fft.irfftn(f, s=(n, n, n), axes=(0, 1, 2))
+    fwd = lambda f: np.fft.rfftn(f, axes=(0, 1, 2))
+    dx = 2 * np.pi / n
+    grad = [[inv(1j * kk[j] * u_hat[i]) for j in range(3)] for i in range(3)]
+    S = [[0.5 * (grad[i][j] + grad[j][i]) for j in range(3)] for i in range(3)]
+    cs = 0.18 * dx
+    nut = cs ** 2 * np.sqrt(2 * sum(S[i][j] ** 2 for i in range(3) for j in range(3)))
+    gphi = [inv(1j * kk[j] * u_hat[3]) for j in range(3)]
+    if model == 1:
+        flux = [nut * gphi[i] for i in range(3)]
+    else:
+        G = _gaussian_transfer(n, 4 * dx)
+        u = [inv(u_hat[i]) for i in range(3)]
+        uf = [inv(G * u_hat[i]) for i in range(3)]
+        L = [[inv(G * fwd(u[i] * u[j])) - uf[i] * uf[j] for j in range(3)] for i in range(3)]
+        Lkk = L[0][0] + L[1][1] + L[2][2]
+        c = np.where(Lkk < 1e-10, 0.0, 2 * 0.2 / np.where(Lkk < 1e-10, 1.0, Lkk))
+        tau = [[c * L[i][j] - cm * 2 * nut * S[i][j] for j in range(3)] for i in range(3)]
+        smag = nut / cs ** 2
+        T = np.where(np.abs(smag) < 1e-10, 0.0, 1.0 / np.where(np.abs(smag) < 1e-10, 1.0, smag))
+        flux = [T * sum(tau[i][j] * gphi[j] for j in range(3)) for i in range(3)]
+    keep = (np.abs(kz) <= n // 3) & (np.abs(ky) <= n // 3) & (kx <= n // 3)
+    want = np.where(keep, sum(1j * kk[i] * fwd(flux[i]) for i in range(3)), 0)
+    d = _to_complex(o.wrk[4] - o0.wrk[4]).transpose(1, 0, 2)
+    assert np.abs(d - want).max() <= 1e-10 * np.abs(want).max()
