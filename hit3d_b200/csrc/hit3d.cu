@@ -16,6 +16,7 @@
 #include "particles.cuh"
 #include "passes.cuh"
 #include "spectral.cuh"
+#include "fused_update.cuh"
 
 // ---------------------------------------------------------------------------
 // errors
@@ -151,6 +152,7 @@ struct hit3d_ctx {
     int pblocks;
     int64_t nlaunch;
     int xcfg;            // launch-shape variant of the fused x pass
+    int fuse_update;     // 1: z forward pass of the velocity products fused with the update
     double k2max;        // truncation radius squared of PRE_TRUNC
     void *mlp_wb;        // bf16 weights of the learned closure (les_model HIT3D_LES_LEARNED)
     double mlp_delta;    // filter width the closure was trained for
@@ -421,6 +423,26 @@ template <typename T, template <class> class OP> static int xfused(hit3d_ctx *c,
 
 static dim3 pw_grid(const hit3d_ctx *c) { return dim3(c->nsm * 4); }
 
+// z forward pass of the six velocity products (after their y pass, in P) fused
+// with the 2/3-rule update of U and RO
+template <typename T, int L> static int zfwd_update_L(hit3d_ctx *c, const StepArgs &a, const cx<T> *P)
+{
+    using CF = ZUpdCfg<T, L>;
+    auto k = k_zfwd_update<T, L, CF::TC, CF::NT, CF::MINB>;
+    H3D_TRY(set_smem(k, CF::SMEM));
+    const int ncol = c->kc_active >= 0 ? c->kc_active + 1 : c->nh;
+    const int rows = c->kc_active >= 0 ? 2 * c->kc_active + 1 : c->n;
+    k<<<dim3((ncol + CF::TC - 1) / CF::TC, rows), CF::NT, CF::SMEM, c->st>>>(a, P, ncol, c->U, c->RO, twid<T>(c));
+    H3D_LAUNCH_CHECK();
+    return 0;
+}
+template <typename T> static int zfwd_update(hit3d_ctx *c, const StepArgs &a, const cx<T> *P)
+{
+#define CALL(L) zfwd_update_L<T, L>(c, a, P)
+    H3D_DISPATCH(c->n, CALL)
+#undef CALL
+}
+
 // full forward 3-D transform of nf FP64 scratch fields holding physical rows
 static int fwd3d64(hit3d_ctx *c, double2 *base, int nf)
 {
@@ -632,7 +654,14 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
         MARK(3);
         H3D_TRY(spass<T>(c, 1, true, Wf(0), wfs, wp, nprod));
         MARK(4);
-        H3D_TRY(spass<T>(c, 2, true, Wf(0), wfs, wp, nprod));
+        // without LES, the velocity products' z pass runs inside the update
+        // kernel (k_zfwd_update); the scalars' products take the plain z pass
+        const bool fuse = c->fuse_update && p.dealias == 0 && p.les_model == 0;
+        if (fuse) {
+            if (nprod > 6) H3D_TRY(spass<T>(c, 2, true, Wf(6), wfs, wp, nprod - 6));
+        } else {
+            H3D_TRY(spass<T>(c, 2, true, Wf(0), wfs, wp, nprod));
+        }
 
         const cx<T> *tau = nullptr;
         if (les && ns > 0) {
@@ -857,8 +886,12 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                                                             src, flux);
                 H3D_LAUNCH_CHECK();
             }
-            k_update_vel_23<T><<<pw_grid(c), 256, 0, c->st>>>(a, Wf(0), tau, c->U, c->RO);
-            H3D_LAUNCH_CHECK();
+            if (fuse) {
+                H3D_TRY(zfwd_update<T>(c, a, Wf(0)));
+            } else {
+                k_update_vel_23<T><<<pw_grid(c), 256, 0, c->st>>>(a, Wf(0), tau, c->U, c->RO);
+                H3D_LAUNCH_CHECK();
+            }
         } else if (pass == 0) {
             for (int s = 0; s < ns; s++) {
                 k_scalar<T><<<pw_grid(c), 256, 0, c->st>>>(a, 1, s, c->dx, Wf(6 + 3 * s), c->SP + s * c->fs64, c->U,
@@ -983,6 +1016,7 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     c->dx = 2.0 * (4.0 * atan(1.0)) / (double)c->n;
     c->int_scalars = c->nsc > 0;
     c->xcfg = 4;  // register-resident fused x pass, the tuner's usual pick
+    c->fuse_update = 0;  // the separate z pass + update measured faster so far
     // a clipped k_sgs brings modes beyond N/3 into the state; the LES fields keep
     // the unpruned transforms throughout
     c->prune_on = les_nles(p->les_model) == 0;
@@ -1325,6 +1359,13 @@ extern "C" int hit3d_gpu_les_stats(hit3d_ctx *c, double *out4)
     H3D_CHECK(cudaSetDevice(c->dev));
     H3D_CHECK(cudaMemcpyAsync(out4, c->d_kmin + 4, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
     H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+extern "C" int hit3d_gpu_set_update_fusion(hit3d_ctx *c, int32_t on)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    c->fuse_update = on != 0;
     return 0;
 }
 

@@ -110,6 +110,7 @@ SIGNATURES = [
     ("hit3d_gpu_autotune", C.c_int, [_vp, C.POINTER(_i32), _dp]),
     ("hit3d_gpu_set_variant", C.c_int, [_vp, _i32]),
     ("hit3d_gpu_set_pruning", C.c_int, [_vp, _i32]),
+    ("hit3d_gpu_set_update_fusion", C.c_int, [_vp, _i32]),
     ("hit3d_gpu_check_finite", C.c_int, [_vp, C.POINTER(_i64)]),
     ("hit3d_gpu_les_stats", C.c_int, [_vp, _dp]),
     ("hit3d_gpu_pruned", C.c_int, [_vp]),
@@ -286,6 +287,10 @@ class Context:
         out = np.zeros(4)
         _check(lib().hit3d_gpu_les_stats(self._h, _ptr(out)), "les_stats")
         return dict(zip(("energy", "production", "B", "dissipation"), out.tolist()))
+
+    def set_update_fusion(self, on: bool):
+        """Fuse the velocity products' z pass with the update (the default) or not."""
+        _check(lib().hit3d_gpu_set_update_fusion(self._h, int(bool(on))), "set_update_fusion")
 
     def set_pruning(self, on: bool):
         """Allow (default) or forbid 2/3-rule pruning of the step's transforms."""

@@ -141,6 +141,12 @@ int hit3d_gpu_set_variant(hit3d_ctx *ctx, int32_t variant);
 int hit3d_gpu_set_pruning(hit3d_ctx *ctx, int32_t on);
 int hit3d_gpu_pruned(hit3d_ctx *ctx);
 
+/* Without LES and with the 2/3 rule, the z forward pass of the six velocity
+ * products runs inside the update kernel, so that the product spectra never
+ * reach HBM (the same arithmetic per mode either way; off by default, as the
+ * separate z pass + update measured faster). */
+int hit3d_gpu_set_update_fusion(hit3d_ctx *ctx, int32_t on);
+
 /* Failure detection (no reference counterpart: a diverged run of the
  * reference carries NaN into its files).  Counts, on the device, the
  * non-finite components of the state and the AB2 history; the host loop
