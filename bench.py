@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--cmp-points", type=int, default=4)
     ap.add_argument("--variant", type=int, default=-1,
                     help="fix the fused x-pass launch shape instead of tuning (profiling runs)")
+    ap.add_argument("--update-fusion", type=int, default=-1, choices=(-1, 0, 1),
+                    help="fuse the products' z pass with the update (1) or not (0); -1: the library default")
     return ap.parse_args()
 
 
@@ -400,6 +402,8 @@ def main():
     peak, peak_kind = peaks()
 
     ctx = make_context(n, 0, local)
+    if args.update_fusion >= 0:
+        ctx.set_update_fusion(bool(args.update_fusion))
     ctx.init_velocity(RN1, 2, 4.0, 2.0)
     ctx.dealias_all()
     fields0 = ctx.download_fields()
@@ -483,6 +487,8 @@ def main():
     fp32 = None
     if not args.no_fp32:
         c32 = make_context(n, 1, local)
+        if args.update_fusion >= 0:
+            c32.set_update_fusion(bool(args.update_fusion))
         c32.upload_fields(fields0)
         if args.variant >= 0:
             c32.set_variant(args.variant)
