@@ -22,6 +22,7 @@ import numpy as np
 from .gpu import Context, les_fields
 from .params import InputFileError, RunConfig, read_input_file
 from .restart import read_restart, restart_name, write_real4, write_restart
+from . import particles as _pt
 from .sidecar import GpuSettings, SidecarError, read_sidecar
 
 
@@ -83,6 +84,11 @@ class Simulation:
                 pass
         self.exit_reason = None
         self.log = []
+        # Lagrangian particles (the reference's 'parts' task)
+        self.int_particles = False
+        self.ipart = None
+        if self.cfg.nptot > 0 and self.cfg.particles_filter_size > 0.0:
+            raise NotImplementedError("particles_filter_size > 0 (filtered particle velocity) is not built")
 
     def _les_constants(self):
         """C_T of les_model 5 from c_t.in and C_mixed of les_models 6, 7, 10 from
@@ -152,6 +158,31 @@ class Simulation:
         f = self.ctx.download_fields()
         f[3:] = 0.0
         self.ctx.upload_fields(f)
+
+    # -- particles (m_particles.f90) -------------------------------------------
+    def _particles_start(self):
+        """particles_init: pt.<ext> of the restart step, else <run_name>.pt, else the lattice;
+        uploaded once TIME reaches starttime_particles (m_fields.f90:239-247)."""
+        c = self.cfg
+        n = c.nx
+        pt = os.path.join(self.wd, f"pt.{c.itmin:06d}")
+        if c.itmin > 0 and os.path.exists(pt):
+            self.ipart, grid, _ = _pt.read_pt(pt, n)
+        else:
+            own = os.path.join(self.wd, self.run_name + ".pt")
+            if os.path.exists(own):
+                phys = _pt.read_run_pt(own, c.nptot)
+                self.ipart = np.arange(1, c.nptot + 1, dtype=np.int32)
+            else:
+                self.ipart, phys = _pt.lattice(c.nptot, n)
+            grid = _pt.to_grid(phys, n)
+        self.ctx.particles_upload(grid, None, c.particles_tracking_scheme)
+        self.int_particles = True
+
+    def write_particles(self):
+        """particles_restart_write_binary: pt.<ext>."""
+        grid, _ = self.ctx.particles_download()
+        _pt.write_pt(os.path.join(self.wd, f"pt.{self.file_ext()}"), self.ipart, grid, self.cfg.nx, self.time)
 
     # -- outputs ---------------------------------------------------------------
     def file_ext(self):
@@ -250,7 +281,14 @@ class Simulation:
                     self.ctx.fov = self.ctx.fos = 1
                     if it % c.iprint1 == 0:
                         self.stat_main()
+            if c.nptot > 0 and not self.int_particles and t >= c.starttime_particles:
+                self._particles_start()
             courant = self.ctx.step(1)
+            if self.int_particles and len(self.ipart) < 1000:
+                grid, uvw = self.ctx.particles_download()
+                _pt.append_trajectories(self.wd, it, t, self.ipart, grid, uvw, c.nx)
+            if self.int_particles and it % c.iwrite4 == 0:
+                self.write_particles()
             if self.n_les > 0 and it % c.iprint1 == 0:
                 self._les_gp(it, t)
             self.time += c.dt
@@ -291,6 +329,8 @@ class Simulation:
         self.exit_reason = reason
         if reason >= 0:
             self.write_restart()
+            if self.int_particles:
+                self.write_particles()
         return reason
 
 

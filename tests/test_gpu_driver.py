@@ -185,3 +185,35 @@ def test_sidecar_runs_the_learned_closure_with_fixed_settings(tmp_path):
     c.step(4)
     assert np.array_equal(c.download_fields(), got)
     c.close()
+
+
+def test_particles_through_the_host_loop(tmp_path):
+    """The 'parts' task of the reference through the host loop: 27 lattice
+    particles from time_p = 0, trajectories p.NNNN every step (nptot < 1000)
+    and pt.<ext> every IWRITE4 steps and at the end."""
+    from hit3d_b200 import particles as pt
+    from hit3d_b200.driver import Simulation
+    wd = str(tmp_path)
+    text = open(os.path.join(GOLDEN, "decay64_.in")).read()
+    text = text.replace("0\t\tnp, number of Largangian particles", "27\t\tnp, number of Largangian particles")
+    text = text.replace("0.1\t\ttime_p, when to release the particles into the flow",
+                        "0.0\t\ttime_p, when to release the particles into the flow")
+    text = text.replace("20\t\tIWRITE4", "2\t\tIWRITE4")
+    with open(os.path.join(wd, "decay64_.in"), "w") as fh:
+        fh.write(text)
+    sim = Simulation("decay64_", wd)
+    assert sim.cfg.nptot == 27 and sim.cfg.starttime_particles == 0.0
+    sim.begin()
+    assert sim.run(max_steps=4) is None
+    grid, uvw = sim.ctx.particles_download()
+    assert grid.shape == (27, 3) and np.isfinite(uvw).all() and np.abs(uvw).max() > 0
+    rows = open(os.path.join(wd, "p.0001")).read().splitlines()
+    assert [int(r[:6]) for r in rows] == [1, 2, 3, 4]
+    last = [float(rows[-1][11 + 16 * k: 11 + 16 * (k + 1)]) for k in range(7)]
+    dx = 2 * np.pi / 64
+    assert np.allclose(last[1:4], (grid[0] - 1.0) * dx, rtol=1e-7)
+    assert np.allclose(last[4:7], uvw[0], rtol=1e-7, atol=1e-12)
+    ip, g4, t4 = pt.read_pt(os.path.join(wd, "pt.000004"), 64)
+    assert np.array_equal(ip, np.arange(1, 28)) and abs(t4 - 4 * 0.005) < 1e-12
+    assert np.allclose(g4, grid, rtol=0, atol=1e-10)
+    assert os.path.exists(os.path.join(wd, "pt.000002"))

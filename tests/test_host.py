@@ -162,3 +162,39 @@ def test_sidecar_errors_name_the_line(text, msg):
     from hit3d_b200.sidecar import SidecarError, parse_sidecar
     with pytest.raises(SidecarError, match=msg):
         parse_sidecar(text, "run.gpu.in")
+
+
+def test_particle_lattice_and_restart_file(tmp_path):
+    """particles_init's lattice (m_particles.f90:195-226) and the pt.<ext> binary
+    layout (m_particles.f90:620-640): int64 nptot, (int32 id, 3 x float64) per
+    particle in physical units, float64 TIME."""
+    from hit3d_b200 import particles as pt
+    ip, phys = pt.lattice(30, 32)                 # nearer cube: 27
+    assert len(ip) == 27 and ip[0] == 1 and ip[-1] == 27
+    step = 2 * np.pi / 3
+    assert np.allclose(phys[0], [0.5 * step] * 3) and np.allclose(phys[1], [1.5 * step, 0.5 * step, 0.5 * step])
+    assert len(pt.lattice(35, 32)[0]) == 27 and len(pt.lattice(50, 32)[0]) == 64
+    grid = pt.to_grid(phys, 32)
+    assert np.allclose(grid, phys / (2 * np.pi / 32) + 1.0)
+    assert np.allclose(pt.to_grid(np.array([[-0.5, 2 * np.pi + 0.25, 1.0]]), 32),
+                       np.array([[2 * np.pi - 0.5, 0.25, 1.0]]) / (2 * np.pi / 32) + 1.0)
+    path = str(tmp_path / "pt.000010")
+    pt.write_pt(path, ip, grid, 32, 0.125)
+    raw = open(path, "rb").read()
+    assert len(raw) == 8 + 27 * 28 + 8 and struct.unpack_from("<q", raw)[0] == 27
+    ip2, grid2, t = pt.read_pt(path, 32)
+    assert np.array_equal(ip2, ip) and np.allclose(grid2, grid, rtol=0, atol=1e-12) and t == 0.125
+    open(path, "r+b").truncate(100)
+    with pytest.raises(pt.ParticleFileError, match="truncated"):
+        pt.read_pt(path, 32)
+
+
+def test_particle_trajectory_line_format(tmp_path):
+    from hit3d_b200 import particles as pt
+    pt.append_trajectories(str(tmp_path), 12, 0.06, np.array([7], dtype=np.int32),
+                           np.array([[1.0, 2.0, 3.0]]), np.array([[0.5, -0.25, 1e-3]]), 32)
+    line = open(tmp_path / "p.0007").read().rstrip("\n")
+    assert line.startswith("000012    0")
+    vals = [float(line[11 + 16 * k: 11 + 16 * (k + 1)]) for k in range(7)]
+    dx = 2 * np.pi / 32
+    assert np.allclose(vals, [0.06, 0.0, dx, 2 * dx, 0.5, -0.25, 1e-3], rtol=1e-7)
