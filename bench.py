@@ -145,7 +145,7 @@ def make_context(n, precision, device):
     return Context(p)
 
 
-def stage_units(n, precision, pruned):
+def stage_units(n, precision, pruned, fused=False):
     """Algorithmic bytes per step of each stage, in units of one unpadded complex
     half-spectrum field B1 = N^2 (N/2+1) * 16 bytes, velocity only, 2/3 rule.
 
@@ -167,6 +167,15 @@ def stage_units(n, precision, pruned):
         "z_forward": w * (6 * a * b + 6 * a * b * b),
         # U, RO read and written, products read: at the kept modes only when pruned
         "update": (12 if not pruned else 12 * a0 * b0 * b0) + w * 6 * a0 * b0 * b0,
+    } if not fused else {
+        "z_inverse": 3 * a * b * b + w * 3 * a * b,
+        "y_inverse": w * (3 * a * b + 3 * a),
+        "x_fused": w * (3 * a + 6 * a),
+        "y_forward": w * (6 * a + 6 * a * b),
+        # the products' z pass inside the update kernel: products read along all z
+        # (kept kx and ky), U and RO read and written at the kept modes
+        "z_forward": 0.0,
+        "update": w * 6 * a * b + (12 if not pruned else 12 * a0 * b0 * b0),
     }
 
 
@@ -434,7 +443,7 @@ def main():
     pruned = ctx.pruned
     prof = ctx.step_profile(3)
     prof = {k: v / 3 for k, v in prof.items()}
-    units = stage_units(n, 0, pruned)
+    units = stage_units(n, 0, pruned, fused=args.update_fusion == 1)
     top = max(units, key=lambda k: prof.get(k, 0.0))
     ach = units[top] * B1 / (prof[top] / 1000.0) / 1e9
     traffic = load_traffic().get(f"{n}:{top}")
