@@ -87,6 +87,7 @@ class Simulation:
         # Lagrangian particles (the reference's 'parts' task)
         self.int_particles = False
         self.ipart = None
+        self.particles_time = 0.0
         if self.cfg.nptot > 0 and self.cfg.particles_filter_size > 0.0:
             raise NotImplementedError("particles_filter_size > 0 (filtered particle velocity) is not built")
 
@@ -180,9 +181,12 @@ class Simulation:
         self.int_particles = True
 
     def write_particles(self):
-        """particles_restart_write_binary: pt.<ext>."""
+        """particles_restart_write_binary: pt.<ext>, with the 'parts' task's TIME, the
+        time at the start of the step that moved the particles last (the hydro
+        task hands it over before advancing, main.f90:124-128, 166-167)."""
         grid, _ = self.ctx.particles_download()
-        _pt.write_pt(os.path.join(self.wd, f"pt.{self.file_ext()}"), self.ipart, grid, self.cfg.nx, self.time)
+        _pt.write_pt(os.path.join(self.wd, f"pt.{self.file_ext()}"), self.ipart, grid, self.cfg.nx,
+                     self.particles_time)
 
     # -- outputs ---------------------------------------------------------------
     def file_ext(self):
@@ -284,6 +288,7 @@ class Simulation:
             if c.nptot > 0 and not self.int_particles and t >= c.starttime_particles:
                 self._particles_start()
             courant = self.ctx.step(1)
+            self.particles_time = t
             if self.int_particles and len(self.ipart) < 1000:
                 grid, uvw = self.ctx.particles_download()
                 _pt.append_trajectories(self.wd, it, t, self.ipart, grid, uvw, c.nx)

@@ -214,6 +214,7 @@ def test_particles_through_the_host_loop(tmp_path):
     assert np.allclose(last[1:4], (grid[0] - 1.0) * dx, rtol=1e-7)
     assert np.allclose(last[4:7], uvw[0], rtol=1e-7, atol=1e-12)
     ip, g4, t4 = pt.read_pt(os.path.join(wd, "pt.000004"), 64)
-    assert np.array_equal(ip, np.arange(1, 28)) and abs(t4 - 4 * 0.005) < 1e-12
+    # the 'parts' task's TIME: the start of step 4
+    assert np.array_equal(ip, np.arange(1, 28)) and abs(t4 - 3 * 0.005) < 1e-12
     assert np.allclose(g4, grid, rtol=0, atol=1e-10)
     assert os.path.exists(os.path.join(wd, "pt.000002"))
