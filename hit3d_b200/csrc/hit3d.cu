@@ -161,6 +161,9 @@ struct hit3d_ctx {
     int *d_mlp_err;      // set by the tensor-core kernel when a completion wait runs out
     double *d_kmin;      // LES with k_sgs: minimum of k_sgs (slot 2), les.gp means, block sums
     double2 *gfilt;      // test filter transfer function of the Dynamic Structure models
+    double2 *pfilt;      // particle filter transfer function (particles_filter_size > 0)
+    double2 *pbuf;       // 3 FP64 fields: the filtered velocity the particles see
+    const double2 *zfilt;  // filter of PRE_FILT when set (else gfilt)
     int prune_on;        // allow 2/3-rule pruning of the step's transforms
     int pruned;          // the state is zero beyond N/3 (checked), so pruning is exact
     int alias_known;     // `pruned` is up to date with the state
@@ -191,7 +194,7 @@ static int zinv_LM(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_t
     io.n = c->n; io.psrc = c->P64; io.pdst = dpitch; io.ncol = c->nh; io.sfield = sfield;
     io.dx = c->dx;
     io.k2max = c->k2max;
-    io.g = c->gfilt;
+    io.g = c->zfilt ? c->zfilt : c->gfilt;
     int rows = c->n;
     if (c->kc_active >= 0) {
         io.kl = io.ko = c->kc_active;
@@ -647,7 +650,20 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
             MARK(7);
             PartArgs pa;
             pa.n = c->n; pa.scheme = c->pscheme; pa.np = c->np; pa.dt = p.dt; pa.dx = c->dx;
-            pa.U = c->phys; pa.fs = (int64_t)c->n * c->n * c->n; pa.xyz = c->d_xyz; pa.uvw = c->d_uvw;
+            pa.U = c->phys; pa.fs = (int64_t)c->n * c->n * c->n; pa.rp = c->n; pa.xyz = c->d_xyz; pa.uvw = c->d_uvw;
+            if (c->pfilt) {
+                // the velocity filtered with the particle filter, in physical space
+                // (particles_move, m_particles.f90:759-766), in FP64
+                c->zfilt = c->pfilt;
+                const int rc = zinv<double>(c, 3, PRE_FILT, 0, c->U, c->fs64, c->pbuf, c->fs64, c->P64);
+                c->zfilt = nullptr;
+                H3D_TRY(rc);
+                H3D_TRY(spass<double>(c, 1, false, c->pbuf, c->fs64, c->P64, 3));
+                H3D_TRY(xc2r<double>(c, c->pbuf, c->fs64, c->P64, 3));
+                pa.U = reinterpret_cast<const double *>(c->pbuf);
+                pa.fs = 2 * c->fs64;
+                pa.rp = 2 * (int64_t)c->P64;
+            }
             k_particles<<<(unsigned)((c->np + 255) / 256), 256, 0, c->st>>>(pa);
             H3D_LAUNCH_CHECK();
         }
@@ -1135,7 +1151,7 @@ extern "C" void hit3d_gpu_finalize(hit3d_ctx *c)
     if (c->W64 && c->W64 != c->W) cudaFree(c->W64);
     void *ptrs[] = {c->U, c->RO, c->RP, c->SP, c->W, c->phys, c->tw64, c->tw32, c->d_fen, c->d_part,
                     c->d_red, c->d_ratio, c->d_cmax, c->stage, c->d_xyz, c->d_uvw, c->sgs, c->mlp_wb,
-                    c->d_mlp_err, c->d_kmin, c->gfilt};
+                    c->d_mlp_err, c->d_kmin, c->gfilt, c->pfilt, c->pbuf};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->st) cudaStreamDestroy(c->st);
@@ -1584,6 +1600,27 @@ extern "C" int hit3d_gpu_init_velocity(hit3d_ctx *c, double rn1, int32_t isp, do
     c->alias_known = 0;
     k_shell_scale<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, c->fs64, 3, kmax, c->d_ratio, c->U);
     H3D_LAUNCH_CHECK();
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+extern "C" int hit3d_gpu_particles_filter(hit3d_ctx *c, double delta)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    if (!(delta > 0.0)) {
+        if (c->pfilt) { cudaFree(c->pfilt); c->pfilt = nullptr; }
+        if (c->pbuf) { cudaFree(c->pbuf); c->pbuf = nullptr; }
+        return 0;
+    }
+    if (delta < 3.0 * c->dx)
+        return h3d_set_error_msg(-1, "hit3d_gpu_particles_filter: particles_filter_size is too small (less than 3*dx)");
+    if (!c->pfilt) H3D_TRY(ctx_alloc((void **)&c->pfilt, sizeof(double2) * (size_t)c->fs64));
+    if (!c->pbuf) H3D_TRY(ctx_alloc((void **)&c->pbuf, sizeof(double2) * 3 * (size_t)c->fs64));
+    // the Gaussian of m_filter_xfftw.f90:197-220 with the particle filter width,
+    // made in the FP64 work field and kept
+    H3D_TRY(filter_transfer(c, 2, delta));
+    H3D_CHECK(cudaMemcpyAsync(c->pfilt, c->W64, sizeof(double2) * (size_t)c->fs64, cudaMemcpyDeviceToDevice, c->st));
     H3D_CHECK(cudaStreamSynchronize(c->st));
     return 0;
 }

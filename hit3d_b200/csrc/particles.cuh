@@ -10,8 +10,8 @@ struct PartArgs {
     int scheme;               // 0 trilinear, 1 CINT
     int64_t np;
     double dt, dx;
-    const double *U;          // physical u,v,w: [f][z][y][x], row pitch n, field stride fs
-    int64_t fs;
+    const double *U;          // physical u,v,w: [f][z][y][x], row pitch rp, field stride fs
+    int64_t fs, rp;
     double *xyz, *uvw;        // (np, 3) each, particle-major as xyzp(3,np)
 };
 
@@ -44,8 +44,9 @@ __global__ void k_particles(const PartArgs a)
     j = ((j - 1) % n + n) % n + 1;
     k = ((k - 1) % n + n) % n + 1;
     // 1-based indices of the reference -> 0-based offsets, periodic
-    auto idx = [n](int ii, int jj, int kk) -> int64_t {
-        return (int64_t)(ii - 1) + (int64_t)n * ((int64_t)(jj - 1) + (int64_t)n * (int64_t)(kk - 1));
+    const int64_t rp = a.rp;
+    auto idx = [n, rp](int ii, int jj, int kk) -> int64_t {
+        return (int64_t)(ii - 1) + rp * ((int64_t)(jj - 1) + (int64_t)n * (int64_t)(kk - 1));
     };
     double up[3];
     if (a.scheme == 0) {

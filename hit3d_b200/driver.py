@@ -88,8 +88,6 @@ class Simulation:
         self.int_particles = False
         self.ipart = None
         self.particles_time = 0.0
-        if self.cfg.nptot > 0 and self.cfg.particles_filter_size > 0.0:
-            raise NotImplementedError("particles_filter_size > 0 (filtered particle velocity) is not built")
 
     def _les_constants(self):
         """C_T of les_model 5 from c_t.in and C_mixed of les_models 6, 7, 10 from
@@ -178,6 +176,8 @@ class Simulation:
                 self.ipart, phys = _pt.lattice(c.nptot, n)
             grid = _pt.to_grid(phys, n)
         self.ctx.particles_upload(grid, None, c.particles_tracking_scheme)
+        if c.particles_filter_size > 0.0:
+            self.ctx.particles_filter(c.particles_filter_size)
         self.int_particles = True
 
     def write_particles(self):

@@ -192,6 +192,12 @@ int hit3d_gpu_stats(hit3d_ctx *ctx, double *e_spec, int32_t kmax, double *out12)
  * min, max. */
 int hit3d_gpu_scalar_stats(hit3d_ctx *ctx, int32_t s, double *spectrum, int32_t kmax, double *out5);
 
+/* particles_move with particles_filter_size > 0 (m_particles.f90:759-766): the
+ * particles see the velocity filtered with the Gaussian of width delta
+ * (m_filter_xfftw.f90:197-220).  delta <= 0 switches the filter off;
+ * delta < 3 dx is an error, as in the reference. */
+int hit3d_gpu_particles_filter(hit3d_ctx *ctx, double delta);
+
 /* Lagrangian particles (m_particles.f90:157-337, 815-1230).  xyzp(3, np) in the
  * reference's grid units (x/dx + 1); uvwp(3, np) starts at -999 (Euler first
  * step).  scheme 0 = trilinear, 1 = 4-point cubic (CINT).  The whole field is
