@@ -153,6 +153,7 @@ struct hit3d_ctx {
     int64_t nlaunch;
     int xcfg;            // launch-shape variant of the fused x pass
     int fuse_update;     // 1: z forward pass of the velocity products fused with the update
+    int idle_passive;    // passive scalars waiting for TSCALAR while LES fields move
     double k2max;        // truncation radius squared of PRE_TRUNC
     void *mlp_wb;        // bf16 weights of the learned closure (les_model HIT3D_LES_LEARNED)
     double mlp_delta;    // filter width the closure was trained for
@@ -560,6 +561,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     a.nu = p.nu; a.dt = p.dt; a.euler_v = euler_v; a.euler_s = euler_s;
     a.flow_type = p.flow_type; a.kfmax = p.kfmax; a.famp = p.famp; a.fenergy = c->d_fen; a.nscal = ns;
     a.kc = c->kc_active;  // pruned state: the updates visit only the kept modes
+    a.idle = c->idle_passive;
     for (int s = 0; s < p.n_scalars; s++) { a.pe[s] = p.nu / p.sc[s]; a.stype[s] = p.scalar_type[s]; }
     for (int j = 0; j < les_nles(p.les_model); j++) {
         // LES fields: Schmidt number one (m_les.f90:372-391), no mean-gradient source
@@ -1421,12 +1423,11 @@ extern "C" int hit3d_gpu_set_scalars_active(hit3d_ctx *c, int32_t on)
 {
     if (!c) return h3d_set_error_msg(-1, "null context");
     // the LES fields are always transported (rhs_scalars.f90:72-74).  While the
-    // passive scalars wait for TSCALAR, the reference still diffuses them with
-    // nu_t in that case; that mixed state is not supported
-    if (on == 0 && les_nles(c->p.les_model) > 0 && c->p.n_scalars > 0)
-        return h3d_set_error_msg(-1, "hit3d_gpu_set_scalars_active: with the LES fields of les_model 2, 3 or 10, "
-                                     "passive scalars move from the start (TSCALAR <= 0)");
+    // passive scalars wait for TSCALAR next to LES fields, the reference still
+    // advances them, with a RHS of only the mean-gradient source and the LES
+    // fluxes (rhs_scalars.f90:28-36, 384-395, main.f90:132-146)
     c->int_scalars = ((on != 0) && c->nsc > 0) || les_nles(c->p.les_model) > 0;
+    c->idle_passive = (on == 0 && les_nles(c->p.les_model) > 0) ? c->p.n_scalars : 0;
     return 0;
 }
 

@@ -105,6 +105,8 @@ struct StepArgs {
     double pe[8];
     int stype[8];
     int kc;                    // >= 0: visit only the modes the 2/3 rule keeps (pruned state)
+    int idle;                  // passive scalars 0..idle-1 wait for TSCALAR while LES fields move:
+                               // no advection or molecular diffusion, only sources and LES fluxes
 };
 
 // 2/3 rule (rhs_velocity.f90:85-142) + forcing + AB2 + pressure.
@@ -289,7 +291,7 @@ __global__ void k_scalar(const StepArgs a, int mode, int s, double dx, const cx<
         double2 r;
         double wn2 = kx * kx + ky * ky + kz * kz;
         if (mode == 0) {
-            if (m.ialias > 0) r = make_double2(0.0, 0.0);
+            if (m.ialias > 0 || s < a.idle) r = make_double2(0.0, 0.0);
             else {
                 double rt1 = kx * pu.y + ky * pv.y + kz * pw.y;
                 double rt2 = kx * pu.x + ky * pv.x + kz * pw.x;

@@ -155,7 +155,7 @@ class Simulation:
             if t % 100 != 0:
                 raise NotImplementedError("only scalars of initial type 0 are generated on this path")
         f = self.ctx.download_fields()
-        f[3:] = 0.0
+        f[3:3 + self.cfg.n_scalars] = 0.0   # the LES fields that follow keep their values
         self.ctx.upload_fields(f)
 
     # -- particles (m_particles.f90) -------------------------------------------

@@ -175,10 +175,44 @@ def test_les_with_passive_scalars_matches_oracle(model):
             assert gs[k] == pytest.approx(os_[k], rel=1e-10, abs=1e-14), k
 
 
-def test_les_fields_need_active_passive_scalars():
+@pytest.mark.parametrize("model", [2, 10])
+def test_idle_passive_scalars_next_to_les_fields(model):
+    """Before TSCALAR the reference still advances the passive scalars when LES
+    fields move, with a RHS of only the mean-gradient source and the LES fluxes
+    (rhs_scalars.f90:28-36, 384-395, main.f90:132-146); then they start moving."""
+    n = 32
+    kw = dict(flow_type=1, les_model=model, nu=1.0 / 2000.0, dt=0.004, isp_type=2, nscal=2, sc=(0.7, 1.0),
+              scalar_type=(0, 1), c_mixed=0.4)
+    o, g = make_pair(n, **kw)
+    f = g.download_fields()
+    rng = np.random.default_rng(7)
+    for s in (3, 4):
+        f[s] = 0.0
+        for _ in range(6):
+            ky, kz, kx = rng.integers(-5, 6), rng.integers(-5, 6), rng.integers(1, 6)
+            f[s, ky % n, kz % n, 2 * kx:2 * kx + 2] = rng.standard_normal(2) * n ** 3 * 0.01
+    g.upload_fields(f)
+    g.dealias_all()
+    o.fields[:] = g.download_fields()
+    g.set_scalars_active(False)
+    o.set_flags(1, 1, 0)
+    o.step(3)
+    g.step(3)
+    got = g.download_fields()
+    for m in range(got.shape[0]):
+        assert relerr(got[m], o.fields[m]) < 1e-10, m
+    # the scalars start moving
+    g.set_scalars_active(True)
+    fl = list(o.flags())
+    o.set_flags(fl[0], fl[1], 1)
+    o.step(3)
+    g.step(3)
+    got = g.download_fields()
+    for m in range(got.shape[0]):
+        assert relerr(got[m], o.fields[m]) < 1e-10, m
+
+
+def test_dynamic_structure_models_refuse_passive_scalars():
     from hit3d_b200 import Context, Hit3dError, Params
-    with Context(Params(nx=32, les_model=2, n_scalars=1, sc=[1.0], scalar_type=[0])) as c:
-        with pytest.raises(Hit3dError, match="TSCALAR"):
-            c.set_scalars_active(False)
     with pytest.raises(Hit3dError, match="scalars"):
         Context(Params(nx=32, les_model=4, n_scalars=1, sc=[1.0], scalar_type=[0]))
