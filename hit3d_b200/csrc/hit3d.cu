@@ -126,6 +126,46 @@ static bool size_supported(int n)
 // ---------------------------------------------------------------------------
 // context
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// RANDu on the host (RANDu.f:12-52), bit-exact with the reference: the
+// initial-condition stream stays on the host as the reference generates it.
+// ---------------------------------------------------------------------------
+namespace {
+struct Randu {
+    int64_t idum2 = 123456789, iy = 0, iv[32] = {0};
+    double next(double idum3)
+    {
+        const int64_t im1 = 2147483563, im2 = 2147483399, imm1 = im1 - 1;
+        const int64_t ia1 = 40014, ia2 = 40692, iq1 = 53668, iq2 = 52774;
+        const int64_t ir1 = 12211, ir2 = 3791, ntab = 32, ndiv = 1 + imm1 / ntab;
+        const double am = 1.0 / (double)im1, eps = 1.2e-7, rnmx = 1.0 - eps;
+        int64_t idum = (int64_t)llround(idum3 / 987.0), k, j;
+        if (idum <= 0) {
+            idum = (-idum > 1) ? -idum : 1;
+            idum2 = idum;
+            for (j = ntab + 8; j >= 1; j--) {
+                k = idum / iq1;
+                idum = ia1 * (idum - k * iq1) - k * ir1;
+                if (idum < 0) idum += im1;
+                if (j <= ntab) iv[j - 1] = idum;
+            }
+        }
+        k = idum / iq1;
+        idum = ia1 * (idum - k * iq1) - k * ir1;
+        if (idum < 0) idum += im1;
+        k = idum2 / iq2;
+        idum2 = ia2 * (idum2 - k * iq2) - k * ir2;
+        if (idum2 < 0) idum2 += im2;
+        j = 1 + iy / ndiv;
+        iy = iv[j - 1] - idum2;
+        iv[j - 1] = idum;
+        if (iy < 1) iy += imm1;
+        double r = am * (double)iy;
+        return r < rnmx ? r : rnmx;
+    }
+};
+}  // namespace
+
 struct hit3d_ctx {
     hit3d_params p;
     int n, nh, P64, P32, nsc, dev, kmax, nsm;
@@ -154,6 +194,8 @@ struct hit3d_ctx {
     int xcfg;            // launch-shape variant of the fused x pass
     int fuse_update;     // 1: z forward pass of the velocity products fused with the update
     int idle_passive;    // passive scalars waiting for TSCALAR while LES fields move
+    Randu rng;           // RANDu state, carried from the velocity to the scalar initial
+                         // conditions as the reference's module state is (RANDu.f:20-22)
     double k2max;        // truncation radius squared of PRE_TRUNC
     void *mlp_wb;        // bf16 weights of the learned closure (les_model HIT3D_LES_LEARNED)
     double mlp_delta;    // filter width the closure was trained for
@@ -932,45 +974,6 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     return 0;
 }
 
-// ---------------------------------------------------------------------------
-// RANDu on the host (RANDu.f:12-52), bit-exact with the reference: the
-// initial-condition stream stays on the host as the reference generates it.
-// ---------------------------------------------------------------------------
-namespace {
-struct Randu {
-    int64_t idum2 = 123456789, iy = 0, iv[32] = {0};
-    double next(double idum3)
-    {
-        const int64_t im1 = 2147483563, im2 = 2147483399, imm1 = im1 - 1;
-        const int64_t ia1 = 40014, ia2 = 40692, iq1 = 53668, iq2 = 52774;
-        const int64_t ir1 = 12211, ir2 = 3791, ntab = 32, ndiv = 1 + imm1 / ntab;
-        const double am = 1.0 / (double)im1, eps = 1.2e-7, rnmx = 1.0 - eps;
-        int64_t idum = (int64_t)llround(idum3 / 987.0), k, j;
-        if (idum <= 0) {
-            idum = (-idum > 1) ? -idum : 1;
-            idum2 = idum;
-            for (j = ntab + 8; j >= 1; j--) {
-                k = idum / iq1;
-                idum = ia1 * (idum - k * iq1) - k * ir1;
-                if (idum < 0) idum += im1;
-                if (j <= ntab) iv[j - 1] = idum;
-            }
-        }
-        k = idum / iq1;
-        idum = ia1 * (idum - k * iq1) - k * ir1;
-        if (idum < 0) idum += im1;
-        k = idum2 / iq2;
-        idum2 = ia2 * (idum2 - k * iq2) - k * ir2;
-        if (idum2 < 0) idum2 += im2;
-        j = 1 + iy / ndiv;
-        iy = iv[j - 1] - idum2;
-        iv[j - 1] = idum;
-        if (iy < 1) iy += imm1;
-        double r = am * (double)iy;
-        return r < rnmx ? r : rnmx;
-    }
-};
-}  // namespace
 
 // ---------------------------------------------------------------------------
 // C-ABI
@@ -1019,6 +1022,7 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     H3D_CHECK(cudaSetDevice(p->device));
     hit3d_ctx *c = new hit3d_ctx();
     memset(c, 0, sizeof *c);
+    c->rng = Randu();
     c->p = *p;
     if (c->p.dealias == 1 && c->p.les_model) c->p.dealias = 0;  // LES forces the 2/3 rule (m_parameters.f90:416-420)
     c->dev = p->device;
@@ -1579,7 +1583,7 @@ extern "C" int hit3d_gpu_init_velocity(hit3d_ctx *c, double rn1, int32_t isp, do
     }
     // RANDu over six full padded arrays in the reference's order, then Box-Muller
     // (init_velocity.f90:67-113)
-    Randu r;
+    Randu &r = c->rng;
     (void)r.next(-rn1);
     for (size_t q = 0; q < 3 * fsz; q++) g[q] = r.next(rn1);
     for (int f = 0; f < 3; f++)
@@ -1600,6 +1604,95 @@ extern "C" int hit3d_gpu_init_velocity(hit3d_ctx *c, double rn1, int32_t isp, do
     H3D_CHECK(cudaMemcpyAsync(c->d_ratio, ratio.data(), sizeof(double) * kmax, cudaMemcpyHostToDevice, c->st));
     c->alias_known = 0;
     k_shell_scale<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, c->fs64, 3, kmax, c->d_ratio, c->U);
+    H3D_LAUNCH_CHECK();
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+extern "C" int hit3d_gpu_init_scalar(hit3d_ctx *c, int32_t s, double rn2, double peak)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    if (s < 0 || s >= c->p.n_scalars) return h3d_set_error_msg(-1, "hit3d_gpu_init_scalar: no such passive scalar");
+    const int type = c->p.scalar_type[s], ic = type - (type / 100) * 100;
+    H3D_CHECK(cudaSetDevice(c->dev));
+    const int n = c->n, kmax = c->kmax;
+    const size_t ld = (size_t)n + 2, fsz = ld * n * n;
+    const double PI = 4.0 * atan(1.0), TWO_PI = 2.0 * PI, dx = 2.0 * PI / (double)n;
+    double2 *F = c->U + (3 + s) * c->fs64;
+    double2 *G = c->W64;
+    c->alias_known = 0;
+    if (ic == 0) {
+        // init_scalar (init_scalars.f90:60-62): zero
+        H3D_CHECK(cudaMemsetAsync(F, 0, sizeof(double2) * (size_t)c->fs64, c->st));
+    } else if (ic < 10) {
+        // init_scalar_spectrum (init_scalars.f90:84-269): Box-Muller noise from the
+        // RANDu stream of RN2 over two full padded arrays, forward transform,
+        // shells 1..kmax rescaled to the normalised target spectrum
+        if (type != 1 && type != 2 && type != 3)
+            return h3d_set_error_msg(-1, "INIT_SCALARS: WRONG INITIAL SPECTRUM TYPE");
+        if (!(peak > 0.0)) return h3d_set_error_msg(-1, "hit3d_gpu_init_scalar: peak wavenumber must be > 0");
+        std::vector<double> g(2 * fsz);
+        Randu &r = c->rng;
+        (void)r.next(-rn2);
+        for (size_t q = 0; q < 2 * fsz; q++) g[q] = r.next(rn2);
+        for (size_t q = 0; q < fsz; q++) g[q] = sqrt(-2.0 * log(g[q])) * sin(TWO_PI * g[fsz + q]);
+        H3D_TRY(upload_phys(c, g.data(), (int64_t)ld, 1));
+        H3D_TRY(fwd3d64(c, G, 1));
+        std::vector<double> es(kmax), et, ratio(kmax);
+        H3D_TRY(shell_spectrum(c, G, 1, es.data()));
+        // types 1 and 3: the velocity's spectrum 1; type 2: its spectrum 3
+        target_spectrum(type == 2 ? 3 : 1, peak, 0.0, kmax, et);
+        for (int k = 0; k < kmax; k++) ratio[k] = es[k] > 0.0 ? sqrt(et[k] / es[k]) : -1.0;
+        H3D_CHECK(cudaMemcpyAsync(c->d_ratio, ratio.data(), sizeof(double) * kmax, cudaMemcpyHostToDevice, c->st));
+        k_shell_scale<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, c->fs64, 1, kmax, c->d_ratio, G);
+        H3D_LAUNCH_CHECK();
+        if (type == 3) {
+            // sign(phi) * 0.9 in physical space, then shells 0 and >= 2 kmax / 3 removed
+            H3D_TRY(inv3d64(c, G, 1));
+            k_sign09<<<pw_grid(c), 256, 0, c->st>>>(n, 2 * (int64_t)c->P64, reinterpret_cast<double *>(G));
+            H3D_LAUNCH_CHECK();
+            H3D_TRY(fwd3d64(c, G, 1));
+            const int kcut = kmax * 2 / 3;
+            for (int k = 0; k < kmax; k++) ratio[k] = (k + 1) < kcut ? 1.0 : -1.0;
+            H3D_CHECK(cudaMemcpyAsync(c->d_ratio, ratio.data(), sizeof(double) * kmax, cudaMemcpyHostToDevice, c->st));
+            k_shell_scale<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, c->fs64, 1, kmax, c->d_ratio, G);
+            H3D_LAUNCH_CHECK();
+        }
+        H3D_CHECK(cudaMemcpyAsync(F, G, sizeof(double2) * (size_t)c->fs64, cudaMemcpyDeviceToDevice, c->st));
+    } else {
+        // init_scalar_space (init_scalars.f90:280-345): profiles in physical space
+        if (ic != 11 && ic != 12 && ic != 13) return h3d_set_error_msg(-1, "INIT_SCALARS: UNEXPECTED SCALAR TYPE");
+        std::vector<double> g(fsz, 0.0);
+        if (ic == 11) {
+            const double h = std::max(2.0 * dx, TWO_PI / peak);
+            for (int k = 0; k < n; k++) {
+                const double z = (double)k * dx;
+                const double v = tanh((z - PI * 0.5) / h) - tanh((z - PI * 1.5) / h) - 1.0;
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) g[i + ld * (j + (size_t)n * k)] = v;
+            }
+        } else if (ic == 12) {
+            const double h = std::max(8.0 * dx, PI / 8.0);
+            for (int i = 0; i < n; i++) {
+                const double x = (double)i * dx;
+                const double v = tanh((x - PI * 0.25) / h) - tanh((x - PI * 0.75) / h) + tanh((x - PI * 1.25) / h) -
+                                 tanh((x - PI * 1.75) / h) - 1.0;
+                for (size_t r = 0; r < (size_t)n * n; r++) g[i + ld * r] = v;
+            }
+        } else {
+            const double pk = std::min(peak, (double)(n / 8));
+            for (int i = 0; i < n; i++) {
+                const double v = sin(pk * dx * (double)i);
+                for (size_t r = 0; r < (size_t)n * n; r++) g[i + ld * r] = v;
+            }
+        }
+        H3D_TRY(upload_phys(c, g.data(), (int64_t)ld, 1));
+        H3D_TRY(fwd3d64(c, G, 1));
+        H3D_CHECK(cudaMemcpyAsync(F, G, sizeof(double2) * (size_t)c->fs64, cudaMemcpyDeviceToDevice, c->st));
+        if (ic != 13) H3D_CHECK(cudaMemsetAsync(F, 0, sizeof(double2), c->st));  // the mean mode
+    }
+    // no modes beyond N/3 in any direction (init_scalars.f90:26-33)
+    k_dealias_all<<<pw_grid(c), 256, 0, c->st>>>(n, c->nh, c->P64, c->fs64, 1, n / 3, F);
     H3D_LAUNCH_CHECK();
     H3D_CHECK(cudaStreamSynchronize(c->st));
     return 0;

@@ -929,6 +929,17 @@ __global__ void k_init_curl(int n, int nh, int pitch, int64_t fs, int kmax, cons
     }
 }
 
+// physical values of one field (row pitch rp, n per row) -> sign(x) * 0.9
+// (init_scalars.f90:242-247; Fortran's sign(1, x) is +1 at x = 0)
+__global__ void k_sign09(int n, int64_t rp, double *__restrict__ X)
+{
+    const int64_t np = (int64_t)n * n * n;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / n, o = row * rp + (t - row * n);
+        X[o] = X[o] < 0.0 ? -0.9 : 0.9;
+    }
+}
+
 // multiply modes of shells 1..kmax by ratio[shell] and zero the rest
 // (init_velocity.f90:224-237); ratio[s] < 0 marks an empty shell
 __global__ void k_shell_scale(int n, int nh, int pitch, int64_t fs, int nf, int kmax, const double *__restrict__ ratio,

@@ -150,13 +150,9 @@ class Simulation:
             self.ctx.autotune()
 
     def _init_scalars(self):
-        """init_scalars.f90: only type-0 (uniform mean gradient, zero initial field) is generated."""
-        for t in self.cfg.scalar_type:
-            if t % 100 != 0:
-                raise NotImplementedError("only scalars of initial type 0 are generated on this path")
-        f = self.ctx.download_fields()
-        f[3:3 + self.cfg.n_scalars] = 0.0   # the LES fields that follow keep their values
-        self.ctx.upload_fields(f)
+        """init_scalars (init_scalars.f90:1-35): every passive scalar from RN2 by its type."""
+        for s in range(self.cfg.n_scalars):
+            self.ctx.init_scalar(s, self.cfg.rn2, self.cfg.peak_wavenum_sc[s])
 
     # -- particles (m_particles.f90) -------------------------------------------
     def _particles_start(self):

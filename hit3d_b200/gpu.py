@@ -124,6 +124,7 @@ SIGNATURES = [
     ("hit3d_gpu_particles_upload", C.c_int, [_vp, _dp, _dp, _i64, _i32]),
     ("hit3d_gpu_particles_download", C.c_int, [_vp, _dp, _dp]),
     ("hit3d_gpu_particles_filter", C.c_int, [_vp, _d]),
+    ("hit3d_gpu_init_scalar", C.c_int, [_vp, _i32, _d, _d]),
     ("hit3d_gpu_xfft3d", C.c_int, [_vp, _i32, _dp, _dp, _i64]),
     ("hit3d_gpu_filter_field", C.c_int, [_vp, _i32, _d, _i32]),
     ("hit3d_gpu_xfft3d_static", C.c_int, [_i32, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -347,6 +348,10 @@ class Context:
         _check(lib().hit3d_gpu_particles_upload(self._h, _ptr(xyzp), None if u is None else _ptr(u),
                                                 xyzp.shape[0], int(scheme)), "particles_upload")
         self._np = xyzp.shape[0]
+
+    def init_scalar(self, s: int, rn2: float, peak_wavenum: float = 4.0):
+        """init_scalar for passive scalar s (its scalar_type decides the form)."""
+        _check(lib().hit3d_gpu_init_scalar(self._h, int(s), float(rn2), float(peak_wavenum)), "init_scalar")
 
     def particles_filter(self, delta: float):
         """Particles see the velocity filtered with a Gaussian of width delta (0: off)."""

@@ -192,6 +192,14 @@ int hit3d_gpu_stats(hit3d_ctx *ctx, double *e_spec, int32_t kmax, double *out12)
  * min, max. */
 int hit3d_gpu_scalar_stats(hit3d_ctx *ctx, int32_t s, double *spectrum, int32_t kmax, double *out5);
 
+/* init_scalar (init_scalars.f90:41-345) for passive scalar s, by its
+ * scalar_type: 0 zero; 1, 2, 3 a random field with the normalised spectrum
+ * of peak wavenumber `peak` (the RANDu stream of rn2 = RN2, continuing the
+ * generator state the velocity's initial condition left, as the reference's
+ * module state does; 3 then clipped to +-0.9); 11, 12, 13 the reference's
+ * tanh and sine profiles.  Modes with some |k_i| > N/3 are zeroed. */
+int hit3d_gpu_init_scalar(hit3d_ctx *ctx, int32_t s, double rn2, double peak);
+
 /* particles_move with particles_filter_size > 0 (m_particles.f90:759-766): the
  * particles see the velocity filtered with the Gaussian of width delta
  * (m_filter_xfftw.f90:197-220).  delta <= 0 switches the filter off;

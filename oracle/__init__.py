@@ -80,6 +80,7 @@ def lib():
         L.oracle_forcing_energy.argtypes = [vp]
         L.oracle_init_velocity.restype = C.c_int
         L.oracle_init_velocity.argtypes = [vp, C.c_double, C.c_int, C.c_double, C.c_double]
+        L.oracle_init_scalar.argtypes = [vp, C.c_int, C.c_double, C.c_double]
         L.oracle_randu_stream.argtypes = [C.c_double, C.c_int64, dp]
         L.oracle_velocity_rescale.restype = C.c_int
         L.oracle_velocity_rescale.argtypes = [vp, C.c_int, C.c_double, C.c_double]
@@ -167,6 +168,10 @@ class Oracle:
         rc = lib().oracle_init_velocity(self._p, float(rn1), int(isp_type), float(peak_wavenum), float(ir_exp))
         if rc != 0:
             raise ValueError(f"unsupported isp_type {isp_type}")
+
+    def init_scalar(self, s, rn2, peak_wavenum=4.0):
+        if lib().oracle_init_scalar(self._p, int(s), float(rn2), float(peak_wavenum)) != 0:
+            raise ValueError("unsupported scalar type")
 
     def dealias_all(self):
         lib().oracle_dealias_all(self._p)

@@ -214,6 +214,7 @@ typedef struct {
     fftplan plan;
     double courant, time;
     double les_stat[4];       /* les.gp: mean k_sgs, production, B, dissipation */
+    randu_state rs;           /* RANDu module state (RANDu.f:20-22), kept between initial conditions */
     double c_t, c_mixed;      /* lag-model scale (c_t.in) and mixed-model fraction (c_mixed.in) */
     double *gfilt;            /* test filter transfer function (DSTM models) */
     double *vsrc;             /* vel_source_les: 3 fields (DSTM models) */
@@ -408,6 +409,7 @@ oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_
             : (les_model == 3 || les_model == 5 || les_model == 7) ? 3 : les_model == 10 ? 2 : 0;
     o->c_t = 1.0;
     o->c_mixed = 0.0;
+    oracle_randu_reset(&o->rs);
     /* passive scalars go with les_models 0-3 and 10 (m_les.f90:725-800 stops on 4-7) */
     if (nscal > 0 && les_model >= 4 && les_model <= 7) { free(o); return NULL; }
     /* kmax (m_parameters.f90:123-131) */
@@ -1783,12 +1785,11 @@ int oracle_init_velocity(oracle_t *o, double rn1, int isp_type, double peak_wave
         return 0;
     }
     /* random numbers over the full padded arrays, wrk1..6 in order */
-    randu_state st;
-    oracle_randu_reset(&st);
-    (void)oracle_randu(&st, -rn1);
+    randu_state *st = &o->rs;
+    (void)oracle_randu(st, -rn1);
     for (int m = 1; m <= 6; m++) {
         double *w = W(o, m);
-        for (size_t q = 0; q < o->fsz; q++) w[q] = oracle_randu(&st, rn1);
+        for (size_t q = 0; q < o->fsz; q++) w[q] = oracle_randu(st, rn1);
     }
     for (int m = 1; m <= 3; m++) {
         double *a = W(o, m), *b = W(o, m + 3);
@@ -1845,6 +1846,87 @@ int oracle_init_velocity(oracle_t *o, double rn1, int isp_type, double peak_wave
                 }
             }
     free(es); free(et);
+    return 0;
+}
+
+/* init_scalar (init_scalars.f90:41-345) for passive scalar s (0-based):
+ * type 0 zero; 1, 2, 3 Box-Muller noise from the RANDu stream of RN2 over
+ * wrk1, wrk2, shaped to the normalised spectrum (3: then sign * 0.9 with
+ * shells 0 and >= 2 kmax / 3 removed); 11, 12, 13 physical profiles.  The
+ * modes with ialias > 0 are zeroed afterwards, as init_scalars does. */
+int oracle_init_scalar(oracle_t *o, int s, double rn2, double peak)
+{
+    int n = o->n, kmax = o->kmax, type = o->scalar_type[s], ic = type - (type / 100) * 100;
+    double PI = 4.0 * atan(1.0), TWO_PI = 2.0 * PI, dx = 2.0 * PI / (double)n;
+    double *f = F(o, 3 + s), *w0 = W(o, 0), *w1 = W(o, 1), *w2 = W(o, 2), *w3 = W(o, 3);
+    if (ic == 0) {
+        memset(f, 0, sizeof(double) * o->fsz);
+    } else if (ic < 10) {
+        if (type != 1 && type != 2 && type != 3) return -1;
+        (void)oracle_randu(&o->rs, -rn2);
+        for (size_t q = 0; q < o->fsz; q++) w1[q] = oracle_randu(&o->rs, rn2);
+        for (size_t q = 0; q < o->fsz; q++) w2[q] = oracle_randu(&o->rs, rn2);
+        for (size_t q = 0; q < o->fsz; q++) w3[q] = sqrt(-2.0 * log(w1[q])) * sin(TWO_PI * w2[q]);
+        xfft3d(o, 1, w3);
+        copy_field(o, f, w3);
+        double *es = (double *)calloc(kmax + 1, sizeof(double)), *et = (double *)calloc(kmax + 1, sizeof(double));
+        oracle_energy_spectrum(o, 3 + s, 1, es);
+        for (int k = 1; k <= kmax; k++) {
+            double wmag = (double)k, ratio = wmag / peak;
+            if (type == 1 || type == 3) et[k - 1] = ratio * ratio * ratio / peak * exp(-3.0 * ratio);
+            else {
+                double ff = 2.0 * PI * ratio, f2 = ff * ff, d = 1.0 + f2;
+                et[k - 1] = (f2 * f2) / (d * d * d);
+            }
+        }
+        double tot = 0.0;
+        for (int k = 0; k < kmax; k++) tot = tot + et[k];
+        for (int k = 0; k < kmax; k++) et[k] = et[k] / tot;
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n + 2; i++) {
+                    double k2 = o->akx[i] * o->akx[i] + o->aky[k] * o->aky[k] + o->akz[j] * o->akz[j];
+                    int sh = nint_shell32(k2);
+                    size_t a = IX(o, i, j, k);
+                    f[a] = (sh > 0 && sh <= kmax && es[sh - 1] > 0.0) ? w3[a] * sqrt(et[sh - 1] / es[sh - 1]) : 0.0;
+                }
+        free(es); free(et);
+        if (type == 3) {
+            copy_field(o, w0, f);
+            xfft3d(o, -1, w0);
+            for (size_t q = 0; q < o->fsz; q++) w0[q] = w0[q] < 0.0 ? -0.9 : 0.9;
+            xfft3d(o, 1, w0);
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n + 2; i++) {
+                        double k2 = o->akx[i] * o->akx[i] + o->aky[k] * o->aky[k] + o->akz[j] * o->akz[j];
+                        int sh = nint_shell32(k2);
+                        if (sh == 0 || sh >= kmax * 2 / 3) w0[IX(o, i, j, k)] = 0.0;
+                    }
+            copy_field(o, f, w0);
+        }
+    } else {
+        if (ic != 11 && ic != 12 && ic != 13) return -1;
+        memset(w0, 0, sizeof(double) * o->fsz);
+        double h11 = fmax(2.0 * dx, TWO_PI / peak), h12 = fmax(8.0 * dx, PI / 8.0);
+        double pk = fmin(peak, (double)(n / 8));
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n; i++) {
+                    double z = (double)k * dx, x = (double)i * dx, v;
+                    if (ic == 11) v = tanh((z - PI * 0.5) / h11) - tanh((z - PI * 1.5) / h11) - 1.0;
+                    else if (ic == 12)
+                        v = tanh((x - PI * 0.25) / h12) - tanh((x - PI * 0.75) / h12) + tanh((x - PI * 1.25) / h12) -
+                            tanh((x - PI * 1.75) / h12) - 1.0;
+                    else v = sin(pk * dx * (double)i);
+                    w0[IX(o, i, j, k)] = v;
+                }
+        xfft3d(o, 1, w0);
+        copy_field(o, f, w0);
+        if (ic != 13) f[0] = 0.0;
+    }
+    for (size_t q = 0; q < o->fsz; q++)
+        if (o->ialias[q] > 0) f[q] = 0.0;
     return 0;
 }
 

@@ -148,3 +148,31 @@ def test_filter_gaussian_matches_oracle():
     o.apply_filter(gf, a)
     g.filter_field(2, delta, 0)
     assert relerr(g.download_fields()[0], a) < 1e-12
+
+
+@pytest.mark.parametrize("dealias", [0, 1])
+def test_init_scalars_match_oracle(dealias):
+    """init_scalar (init_scalars.f90:41-345) for every type the reference has:
+    zero (0), random fields with spectra (1, 2, 3) from the RANDu stream of RN2
+    continuing the velocity's generator state, and the profiles 11, 12, 13."""
+    import oracle
+    from hit3d_b200 import Context, Params
+    n = 32
+    types = [0, 1, 2, 3, 11, 12, 13]
+    peaks = [4.0, 4.0, 3.0, 5.0, 2.0, 4.0, 3.0]
+    o = oracle.Oracle(n, nscal=7, dealias=dealias, sc=(1.0,) * 7, scalar_type=types)
+    g = Context(Params(nx=n, dealias=dealias, n_scalars=7, sc=[1.0] * 7, scalar_type=types))
+    o.init_velocity(RN1, isp_type=1, peak_wavenum=4.0)
+    g.init_velocity(RN1, 1, 4.0, 2.0)
+    for s in range(7):
+        o.init_scalar(s, 93712139.0, peaks[s])
+        g.init_scalar(s, 93712139.0, peaks[s])
+    f = g.download_fields()
+    assert relerr(f[:3], o.fields[:3]) < 1e-12
+    for s in range(7):
+        a, b = f[3 + s], o.fields[3 + s]
+        if types[s] == 0:
+            assert np.abs(a).max() == 0.0
+        else:
+            assert np.abs(b).max() > 0 and relerr(a, b) < 1e-12, types[s]
+    g.close()

@@ -498,3 +498,59 @@ def test_les_scalar_fluxes_against_numpy(model):
     want = np.where(keep, sum(1j * kk[i] * fwd(flux[i]) for i in range(3)), 0)
     d = _to_complex(o.wrk[4] - o0.wrk[4]).transpose(1, 0, 2)
     assert np.abs(d - want).max() <= 1e-10 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("stype,peak", [(1, 4.0), (2, 3.0), (101, 4.0)])
+def test_init_scalar_imposes_the_target_spectrum(stype, peak):
+    """init_scalar_spectrum (init_scalars.f90:84-240): the scalar's shells carry
+    the normalised spectrum (types 1 and 3: k^3 e^{-3k/kp}; 2: (2 pi k/kp)^4 /
+    (1 + (2 pi k/kp)^2)^3), binned as the reference bins; modes beyond N/3 zero."""
+    n = 32
+    o = oracle.Oracle(n, nscal=1, sc=(1.0,), scalar_type=(stype,))
+    if stype == 101:             # a reaction-type scalar has no spectrum of its own
+        with pytest.raises(ValueError):
+            o.init_scalar(0, 93712139.0, peak)
+        return
+    o.init_scalar(0, 93712139.0, peak)
+    akx, aky, akz = _wavenumbers(n)
+    k2 = akx[None, None, :] ** 2 + aky[:, None, None] ** 2 + akz[None, :, None] ** 2
+    sh = _shell32(k2)[..., :n]
+    w = np.where(akx[:n] == 0, 0.5, 1.0)[None, None, :]
+    e = o.fields[3, ..., :n] ** 2 * w / float(n) ** 6
+    kmax = o.kmax
+    got = np.bincount(sh.ravel(), weights=e.ravel(), minlength=kmax + 2)[1:kmax + 1]
+    r = np.arange(1, kmax + 1) / peak
+    tgt = r ** 3 / peak * np.exp(-3 * r) if stype == 1 else (2 * np.pi * r) ** 4 / (1 + (2 * np.pi * r) ** 2) ** 3
+    assert np.abs(got - tgt / tgt.sum()).max() <= 1e-13
+    keep = ((np.abs(aky) <= n // 3)[:, None, None] & (np.abs(akz) <= n // 3)[None, :, None]
+            & (akx <= n // 3)[None, None, :])
+    assert np.abs(o.fields[3][~keep]).max() == 0.0
+
+
+def test_init_scalar_randu_continues_the_velocity_stream():
+    """The RANDu state is module state (RANDu.f:20-22): a scalar made after the
+    velocity differs from one made by a fresh generator (iy carries over)."""
+    n = 16
+    a = oracle.Oracle(n, nscal=1, sc=(1.0,), scalar_type=(1,))
+    b = oracle.Oracle(n, nscal=1, sc=(1.0,), scalar_type=(1,))
+    a.init_velocity(RN1, isp_type=1)
+    a.init_scalar(0, 93712139.0)
+    b.init_scalar(0, 93712139.0)
+    assert not np.array_equal(a.fields[3], b.fields[3])
+
+
+def test_init_scalar_profiles():
+    """init_scalar_space (init_scalars.f90:280-345): type 13 is sin(k_p x) with
+    k_p = min(peak, N/8); type 11 a tanh slab in z with zero mean."""
+    n = 32
+    o = oracle.Oracle(n, nscal=2, sc=(1.0, 1.0), scalar_type=(13, 11))
+    o.init_scalar(0, 1.0, 6.0)
+    o.init_scalar(1, 1.0, 2.0)
+    X, Y, Z = _grid(n)
+    a = o.fields[3].copy()
+    o.fft3d(-1, a)
+    assert np.abs(a[..., :n] - np.sin(4.0 * X)).max() <= 1e-13
+    b = o.fields[4].copy()
+    o.fft3d(-1, b)
+    assert abs(b[..., :n].mean()) <= 1e-14
+    assert np.abs(b[..., :n] - b[:, :1, :1][..., :1]).max() <= 1e-13   # depends on z only
