@@ -261,6 +261,7 @@ static int zinv_L(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src
     case PRE_STRAIN_A: return zinv_LM<T, L, PRE_STRAIN_A>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
     case PRE_STRAIN_B: return zinv_LM<T, L, PRE_STRAIN_B>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
     case PRE_GRAD: return zinv_LM<T, L, PRE_GRAD>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+    case PRE_QUART: return zinv_LM<T, L, PRE_QUART>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
     default: break;
     }
     if constexpr (std::is_same<T, double>::value) {
@@ -656,6 +657,27 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
         k_forcing_energy<<<1, 32, 0, c->st>>>(c->n, c->P64, c->fs64, p.kfmax, c->U, c->d_fen);
         H3D_LAUNCH_CHECK();
     }
+    // reaction sources of type-311 scalars, from this state (phase shift only,
+    // rhs_scalars.f90:281-303), in the work fields after the products
+    int reac_slot[HIT3D_MAX_SCALARS];
+    for (int s = 0; s < HIT3D_MAX_SCALARS; s++) reac_slot[s] = -1;
+    if (p.dealias == 1 && ns > 0) {
+        int j = 0;
+        for (int s = 0; s < p.n_scalars; s++) {
+            if (p.scalar_type[s] != 311) continue;
+            const int slot = nprod + j++;
+            reac_slot[s] = slot;
+            H3D_TRY(zinv<T>(c, 1, PRE_QUART, 0, c->U + (3 + s) * c->fs64, c->fs64, Wf(slot), wfs, wp));
+            H3D_TRY(spass<T>(c, 1, false, Wf(slot), wfs, wp, 1));
+            H3D_TRY(xc2r<T>(c, Wf(slot), wfs, wp, 1));
+            k_reaction<T><<<pw_grid(c), 256, 0, c->st>>>(c->n, 2 * (int64_t)wp, p.reac_sc[s], c->U + (3 + s) * c->fs64,
+                                                          reinterpret_cast<T *>(Wf(slot)));
+            H3D_LAUNCH_CHECK();
+            H3D_TRY(xr2c<T>(c, Wf(slot), wfs, wp, 1));
+            H3D_TRY(spass<T>(c, 1, true, Wf(slot), wfs, wp, 1));
+            H3D_TRY(spass<T>(c, 2, true, Wf(slot), wfs, wp, 1));
+        }
+    }
     const int npass = p.dealias == 1 ? 2 : 1;
     for (int pass = 0; pass < npass; pass++) {
         const int mode = pass == 0 ? PRE_COPY : PRE_SHIFT;
@@ -962,8 +984,10 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
             H3D_LAUNCH_CHECK();
         } else {
             for (int s = 0; s < ns; s++) {
+                const cx<T> *rs = (s < p.n_scalars && reac_slot[s] >= 0) ? Wf(reac_slot[s]) : nullptr;
                 k_scalar<T><<<pw_grid(c), 256, 0, c->st>>>(a, 2, s, c->dx, Wf(6 + 3 * s), c->SP + s * c->fs64, c->U,
-                                                            c->U + (3 + s) * c->fs64, c->RO + (3 + s) * c->fs64);
+                                                            c->U + (3 + s) * c->fs64, c->RO + (3 + s) * c->fs64,
+                                                            nullptr, nullptr, rs);
                 H3D_LAUNCH_CHECK();
             }
             k_update_vel_ps2<T><<<pw_grid(c), 256, 0, c->st>>>(a, c->dx, Wf(0), c->RP, c->U, c->RO);
@@ -1016,7 +1040,9 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
                                      "20 (the reference cannot transport scalars with the dynamic structure models)");
     if (p->precision != 0 && p->precision != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: precision must be 0 or 1");
     for (int s = 0; s < p->n_scalars; s++) {
-        if (p->scalar_type[s] >= 100) return h3d_set_error_msg(-1, "hit3d_gpu_init: reacting scalars are not supported");
+        // types above 300 carry a reaction; only 311 has one (rhs_scalars.f90:281-303)
+        if (p->scalar_type[s] > 300 && p->scalar_type[s] != 311)
+            return h3d_set_error_msg(-1, "hit3d_gpu_init: The scalar type has a reaction rate that is not supported yet");
         if (!(p->sc[s] > 0.0)) return h3d_set_error_msg(-1, "hit3d_gpu_init: Schmidt numbers must be > 0");
     }
     H3D_CHECK(cudaSetDevice(p->device));
@@ -1050,7 +1076,9 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     int rc = 0;
     const int nf = 3 + c->nsc;
     const size_t f64 = (size_t)c->fs64 * sizeof(double2);
-    c->nw = 6 + 3 * c->nsc +
+    int nreac = 0;  // type-311 scalars: one work field each for the reaction source (phase shift)
+    for (int s = 0; s < p->n_scalars; s++) nreac += (c->p.dealias == 1 && p->scalar_type[s] == 311) ? 1 : 0;
+    c->nw = 6 + 3 * c->nsc + nreac +
             (c->p.les_model == 1 ? 6 + 3 * p->n_scalars : c->p.les_model == HIT3D_LES_LEARNED ? 9
                                                                                : c->p.les_model == 2 ? 12 + 3 * p->n_scalars
                                                                                : c->p.les_model == 3 ? 20 + 3 * p->n_scalars

@@ -62,6 +62,7 @@ enum PreMode : int {
     PRE_TRUNC = 7,     // field f with |k|^2 > k2max zeroed       (io_write_4.f90:21-42)
     PRE_CUBE = 8,      // field f with some |k_i| > N/3 zeroed    (m_les.f90:1579-1586)
     PRE_FILT = 9,      // field f times the test filter g         (m_filter_xfftw.f90:81-100)
+    PRE_QUART = 10,    // field f with some |k_i| > N/4 zeroed    (rhs_scalars.f90:284-292)
 };
 
 // MODE is a compile-time PreMode so that the plain copy carries no per-element
@@ -134,6 +135,11 @@ template <typename T, typename TO, int MODE> struct IOSpec {
         case PRE_CUBE: {
             const double k3 = (double)(n / 3);
             r = (fabs(kx) > k3 || fabs(ky) > k3 || fabs(kz) > k3) ? make_double2(0.0, 0.0) : U(f, o, c, p);
+            break;
+        }
+        case PRE_QUART: {
+            const double k4 = (double)(n / 4);
+            r = (fabs(kx) > k4 || fabs(ky) > k4 || fabs(kz) > k4) ? make_double2(0.0, 0.0) : U(f, o, c, p);
             break;
         }
         case PRE_FILT: {

@@ -261,7 +261,7 @@ template <typename TP>
 __global__ void k_scalar(const StepArgs a, int mode, int s, double dx, const cx<TP> *__restrict__ P,
                          double2 *__restrict__ SP, const double2 *__restrict__ Uvel, double2 *__restrict__ PHI,
                          double2 *__restrict__ RO, const cx<TP> *__restrict__ LS = nullptr,
-                         const cx<TP> *__restrict__ LF = nullptr)
+                         const cx<TP> *__restrict__ LF = nullptr, const cx<TP> *__restrict__ RS = nullptr)
 {
     const int kc = mode == 0 ? a.kc : -1;
     const int64_t nm = mode_count(a.n, a.nh, kc);
@@ -307,6 +307,11 @@ __global__ void k_scalar(const StepArgs a, int mode, int s, double dx, const cx<
                 r.x = r.x + sp.x - pe * wn2 * phi.x;
                 r.y = r.y + sp.y - pe * wn2 * phi.y;
             }
+        }
+        if (RS != nullptr) {  // reaction source, every mode (phase shift, rhs_scalars.f90:300)
+            const double2 rs = ld2<TP>(RS, po);
+            r.x = r.x + rs.x;
+            r.y = r.y + rs.y;
         }
         if (a.stype[s] == 0) {
             double2 u = Uvel[o];
@@ -926,6 +931,21 @@ __global__ void k_init_curl(int n, int nh, int pitch, int64_t fs, int kmax, cons
             r6 = make_double2(-(kx * g2.y - ky * g1.y), kx * g2.x - ky * g1.x);
         }
         U[o] = r4; U[o + fs] = r5; U[o + 2 * fs] = r6;
+    }
+}
+
+// reaction source of a type-311 scalar (rhs_scalars.f90:281-303), in place on
+// the physical band-limited scalar X (row pitch rp): reac (1 - X^2)(X - mean),
+// mean the scalar's zero mode K0 over N^3
+template <typename T>
+__global__ void k_reaction(int n, int64_t rp, double reac, const double2 *__restrict__ K0, T *__restrict__ X)
+{
+    const int64_t np = (int64_t)n * n * n;
+    const double mean = K0[0].x / ((double)n * n * n);
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < np; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / n, o = row * rp + (t - row * n);
+        const double x = (double)X[o];
+        X[o] = (T)(reac * (1.0 - x * x) * (x - mean));
     }
 }
 

@@ -46,6 +46,7 @@ class _Params(C.Structure):
         ("scalar_type", C.c_int32 * MAX_SCALARS), ("device", C.c_int32), ("reserved", C.c_int32),
         ("nu", C.c_double), ("dt", C.c_double), ("famp", C.c_double), ("c_smag", C.c_double),
         ("sc", C.c_double * MAX_SCALARS), ("c_t", C.c_double), ("c_mixed", C.c_double),
+        ("reac_sc", C.c_double * MAX_SCALARS),
     ]
 
 
@@ -69,6 +70,7 @@ class Params:
     sc: Sequence[float] = field(default_factory=list)
     c_t: float = 1.0        # lag-model C_T of les_model 5 (c_t.in)
     c_mixed: float = 0.0    # C_mixed of les_models 6, 7 (c_mixed.in)
+    reac_sc: Sequence[float] = field(default_factory=list)  # reaction rates (scalar_type 311)
 
     @property
     def kmax(self) -> int:
@@ -87,9 +89,11 @@ class Params:
             setattr(p, k, float(getattr(self, k)))
         st = list(self.scalar_type) + [0] * MAX_SCALARS
         sc = list(self.sc) + [1.0] * MAX_SCALARS
+        rc = list(self.reac_sc) + [0.0] * MAX_SCALARS
         for i in range(MAX_SCALARS):
             p.scalar_type[i] = int(st[i])
             p.sc[i] = float(sc[i])
+            p.reac_sc[i] = float(rc[i])
         return p
 
 

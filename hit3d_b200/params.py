@@ -84,7 +84,7 @@ class RunConfig:
         return Params(nx=self.nx, dealias=self.dealias, flow_type=self.flow_type, force_type=self.force_type,
                       kfmax=self.kfmax, n_scalars=self.n_scalars, precision=precision, les_model=self.les_model,
                       scalar_type=list(self.scalar_type), device=device, nu=self.nu, dt=self.dt, famp=self.famp,
-                      c_smag=c_smag, sc=list(self.sc), c_t=c_t, c_mixed=c_mixed)
+                      c_smag=c_smag, sc=list(self.sc), c_t=c_t, c_mixed=c_mixed, reac_sc=list(self.reac_sc))
 
 
 class _ListDirected:

@@ -72,6 +72,8 @@ typedef struct hit3d_params {
                             m_les.f90:189-207); les_models 3 and 7 use C_T = 1             */
     double c_mixed;      /* fraction C_mixed of the Smagorinsky viscosity in les_models 6, 7,
                             10 (the reference reads c_mixed.in, m_les.f90:213-335)        */
+    double reac_sc[HIT3D_MAX_SCALARS]; /* reaction rates; used by scalar_type 311 with
+                            phase-shift dealiasing (rhs_scalars.f90:281-303)               */
 } hit3d_params;
 
 /* Allocate the device state, transform plans and wavenumber tables.

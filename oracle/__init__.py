@@ -74,6 +74,7 @@ def lib():
         L.oracle_nwrk.argtypes = [vp]
         L.oracle_nwrk.restype = C.c_int
         L.oracle_set_les_constants.argtypes = [vp, C.c_double, C.c_double]
+        L.oracle_set_reaction.argtypes = [vp, C.c_int, C.c_double]
         L.oracle_scalar_stats.argtypes = [vp, dp]
         L.oracle_energy_spectrum.argtypes = [vp, C.c_int, C.c_int, dp]
         L.oracle_forcing_energy.restype = C.c_double
@@ -225,6 +226,10 @@ class Oracle:
         keys = ["energy", "eps_v", "eta", "etakmax", "uvar", "x_length", "lambda", "re_lambda",
                 "re_lambda1", "tau_e", "enstrophy", "skewness"]
         return out[: self.kmax].copy(), dict(zip(keys, out[self.kmax:].tolist()))
+
+    def set_reaction(self, s, rate):
+        """reac_sc of scalar s (used by scalar type 311 with phase-shift dealiasing)."""
+        lib().oracle_set_reaction(self._p, int(s), float(rate))
 
     def set_les_constants(self, c_t=1.0, c_mixed=0.0):
         """C_T of les_model 5 (c_t.in) and C_mixed of les_models 6 and 7 (c_mixed.in)."""

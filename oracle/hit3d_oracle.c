@@ -215,6 +215,7 @@ typedef struct {
     double courant, time;
     double les_stat[4];       /* les.gp: mean k_sgs, production, B, dissipation */
     randu_state rs;           /* RANDu module state (RANDu.f:20-22), kept between initial conditions */
+    double reac[MAXS];        /* reaction rates reac_sc of the scalars (rhs_scalars.f90:281-303) */
     double c_t, c_mixed;      /* lag-model scale (c_t.in) and mixed-model fraction (c_mixed.in) */
     double *gfilt;            /* test filter transfer function (DSTM models) */
     double *vsrc;             /* vel_source_les: 3 fields (DSTM models) */
@@ -420,6 +421,7 @@ oracle_t *oracle_create(int n, int nscal, int dealias, int flow_type, int force_
     o->fsz = (size_t)(n + 2) * n * n;
     o->nwrk = 7;
     if (6 + nscal + o->nles > o->nwrk) o->nwrk = 6 + nscal + o->nles;
+    if (dealias == 1 && 3 + nscal + o->nles + 6 > o->nwrk) o->nwrk = 3 + nscal + o->nles + 6;
     /* the DSTM models use four work arrays past the LES fields (m_work.f90) */
     if (les_model >= 4 && 3 + nscal + o->nles + 5 > o->nwrk) o->nwrk = 3 + nscal + o->nles + 5;
     o->fields = (double *)calloc(o->fsz * (3 + nscal + o->nles), sizeof(double));
@@ -503,6 +505,7 @@ double *oracle_fields(oracle_t *o) { return o->fields; }
 double *oracle_rhs_old(oracle_t *o) { return o->rhs_old; }
 double *oracle_wrk(oracle_t *o) { return o->wrk; }
 int oracle_nwrk(oracle_t *o) { return o->nwrk; }
+void oracle_set_reaction(oracle_t *o, int s, double rate) { o->reac[s] = rate; }
 /* C_T of les_model 5 (c_t.in) and C_mixed of les_models 6, 7 (c_mixed.in) */
 void oracle_set_les_constants(oracle_t *o, double c_t, double c_mixed) { o->c_t = c_t; o->c_mixed = c_mixed; }
 int oracle_kmax(oracle_t *o) { return o->kmax; }
@@ -1254,6 +1257,27 @@ static void oracle_rhs_scalars(oracle_t *o)
                             r[b] = r[b] - 0.5 * rt2 - pe * wn2 * phi[b];
                         }
                     }
+        }
+        /* reaction rates (rhs_scalars.f90:281-303), phase shift only: type 311 gains
+         * reac (1 - phi~^2)(phi~ - <phi>), phi~ the scalar without the modes of
+         * some |k_i| > N/4, <phi> its mean; other types above 300 stop the run */
+        for (int s = 1; s <= o->nscal; s++) {
+            if (o->scalar_type[s - 1] <= 300) continue;
+            double *w1 = W(o, 3 + ns + nl + 4), *w2 = W(o, 3 + ns + nl + 5);
+            copy_field(o, w1, F(o, 2 + s));
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n + 1; i += 2) {
+                        size_t a = IX(o, i, j, k);
+                        if (fabs(o->akx[i]) > n / 4 || fabs(o->aky[k]) > n / 4 || fabs(o->akz[j]) > n / 4)
+                            w1[a] = w1[a + 1] = 0.0;
+                    }
+            xfft3d(o, -1, w1);
+            const double mean = F(o, 2 + s)[0] / ((double)n * n * n);
+            for (size_t q = 0; q < o->fsz; q++) w2[q] = o->reac[s - 1] * (1.0 - w1[q] * w1[q]) * (w1[q] - mean);
+            xfft3d(o, 1, w2);
+            double *r = W(o, 3 + s);
+            for (size_t q = 0; q < o->fsz; q++) r[q] = r[q] + w2[q];
         }
     }
     /* uniform mean-gradient source for type-0 scalars (rhs_scalars.f90:387-389) */

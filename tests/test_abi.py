@@ -40,12 +40,13 @@ def test_params_struct_layout_matches_c(tmp_path):
         "int main(void){printf(\"%zu %zu %zu %zu %zu\\n\", sizeof(hit3d_params),"
         " offsetof(hit3d_params, scalar_type), offsetof(hit3d_params, device),"
         " offsetof(hit3d_params, nu), offsetof(hit3d_params, sc));"
-        " printf(\"%zu %zu\\n\", offsetof(hit3d_params, c_t), offsetof(hit3d_params, c_mixed)); return 0;}\n")
+        " printf(\"%zu %zu %zu\\n\", offsetof(hit3d_params, c_t), offsetof(hit3d_params, c_mixed),"
+        " offsetof(hit3d_params, reac_sc)); return 0;}\n")
     exe = tmp_path / "probe"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
     got = [C.sizeof(_Params), _Params.scalar_type.offset, _Params.device.offset, _Params.nu.offset,
-           _Params.sc.offset, _Params.c_t.offset, _Params.c_mixed.offset]
+           _Params.sc.offset, _Params.c_t.offset, _Params.c_mixed.offset, _Params.reac_sc.offset]
     assert [int(x) for x in out] == got
 
 

@@ -176,3 +176,47 @@ def test_init_scalars_match_oracle(dealias):
         else:
             assert np.abs(b).max() > 0 and relerr(a, b) < 1e-12, types[s]
     g.close()
+
+
+def test_reacting_scalar_matches_oracle():
+    """scalar_type 311 with phase-shift dealiasing (rhs_scalars.f90:281-303): the
+    RHS gains reac (1 - phi~^2)(phi~ - <phi>), phi~ the scalar without the
+    modes of some |k_i| > N/4; the initial field is the tanh slab of type 11."""
+    import oracle
+    from hit3d_b200 import Context, Params
+    n = 32
+    types, sc, reac = [311, 0], [0.7, 1.0], [2.0, 0.0]
+    o = oracle.Oracle(n, nscal=2, dealias=1, flow_type=1, nu=1.0 / 400.0, dt=0.004, sc=sc, scalar_type=types)
+    o.set_reaction(0, reac[0])
+    g = Context(Params(nx=n, dealias=1, flow_type=1, nu=1.0 / 400.0, dt=0.004, n_scalars=2, sc=sc,
+                       scalar_type=types, reac_sc=reac))
+    g.init_velocity(RN1, 1, 4.0, 2.0)
+    for s in range(2):
+        g.init_scalar(s, 93712139.0, 2.0)
+    o.fields[:] = g.download_fields()
+    o.set_flags(1, 1, 1)
+    g.set_scalars_active(True)
+    for _ in range(3):
+        o.step(3)
+        g.step(3)
+        f = g.download_fields()
+        for m in range(5):
+            assert relerr(f[m], o.fields[m]) < 1e-10, m
+    # the reaction acts: the oracle without it ends elsewhere
+    o0 = oracle.Oracle(n, nscal=2, dealias=1, flow_type=1, nu=1.0 / 400.0, dt=0.004, sc=sc, scalar_type=types)
+    g0 = Context(Params(nx=n, dealias=1, n_scalars=2, sc=sc, scalar_type=types))
+    g0.init_velocity(RN1, 1, 4.0, 2.0)
+    for s in range(2):
+        g0.init_scalar(s, 93712139.0, 2.0)
+    o0.fields[:] = g0.download_fields()
+    o0.set_flags(1, 1, 1)
+    o0.step(9)
+    assert relerr(o0.fields[3], o.fields[3]) > 1e-3
+    g0.close()
+    g.close()
+
+
+def test_unsupported_reaction_type_is_rejected():
+    from hit3d_b200 import Context, Hit3dError, Params
+    with pytest.raises(Hit3dError, match="reaction rate"):
+        Context(Params(nx=32, dealias=1, n_scalars=1, sc=[1.0], scalar_type=[312]))
