@@ -138,6 +138,10 @@ class Simulation:
             f, self.time, dt, nums1, _ = read_restart(
                 os.path.join(self.wd, restart_name(self.run_name, c.itmin)), c.nx, c.n_scalars, self.n_les)
             self.ctx.upload_fields(f)
+            # scalars the .in file has beyond the file's count start from their
+            # initial condition (restart_io.f90:419-432)
+            for s in range(min(nums1, c.n_scalars), c.n_scalars):
+                self.ctx.init_scalar(s, c.rn2, c.peak_wavenum_sc[s])
             if nums1 > 0 or c.tscalar <= self.time:
                 self.int_scalars = c.n_scalars > 0
             if c.variable_dt:

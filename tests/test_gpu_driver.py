@@ -218,3 +218,25 @@ def test_particles_through_the_host_loop(tmp_path):
     assert np.array_equal(ip, np.arange(1, 28)) and abs(t4 - 3 * 0.005) < 1e-12
     assert np.allclose(g4, grid, rtol=0, atol=1e-10)
     assert os.path.exists(os.path.join(wd, "pt.000002"))
+
+
+def test_restart_with_an_added_scalar_initialises_it(tmp_path):
+    """restart_io.f90:419-432: a scalar the .in file adds to a restart file
+    without it starts from its initial condition (type 1: a random field)."""
+    from dataclasses import replace
+    from hit3d_b200.driver import Simulation
+    from hit3d_b200.params import read_input_file
+    wd = str(tmp_path)
+    cfg = read_input_file(os.path.join(GOLDEN, "decay64_.in"))
+    cfg0 = replace(cfg, n_scalars=0, scalar_type=[], sc=[], ir_exp_sc=[], peak_wavenum_sc=[], reac_sc=[],
+                   itmax=2, iprint1=2, iprint2=2, iwrite4=100)
+    sim = Simulation("add64", wd, cfg=cfg0)
+    sim.begin()
+    assert sim.run() == 0
+    cfg1 = replace(cfg, n_scalars=1, scalar_type=[1], sc=[0.7], ir_exp_sc=[4.0], peak_wavenum_sc=[3.0],
+                   reac_sc=[0.0], itmin=2, itmax=4, iprint1=2, iprint2=2, iwrite4=100)
+    sim2 = Simulation("add64", wd, cfg=cfg1)
+    sim2.begin()
+    f = sim2.ctx.download_fields()
+    assert f.shape[0] == 4 and np.abs(f[3]).max() > 0
+    assert np.array_equal(f[:3, ..., :64], sim.ctx.download_fields()[:3, ..., :64])
