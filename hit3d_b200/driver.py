@@ -40,6 +40,10 @@ def _fmt_e(x: float, w: int = 15, d: int = 6) -> str:
     return s.rjust(w)
 
 
+# les_model_name of m_les.f90:56-352, the last column of the progress line
+LES_MODEL_NAME = {1: " SM", 2: "DLM", 3: "DLL", 4: "DST", 5: "STL", 6: "MMA", 7: "MML", 10: "#10", 20: "MLP"}
+
+
 class Simulation:
     """One run: the reference's hydro task with the state resident on the GPU."""
 
@@ -88,6 +92,13 @@ class Simulation:
         self.int_particles = False
         self.ipart = None
         self.particles_time = 0.0
+
+    def _out(self, line: str):
+        """A line of the run log d0000.txt (the reference's unit `out`, m_io.f90:27);
+        the progress line has format 9000 of main.f90:301-302."""
+        self.log.append(line)
+        with open(os.path.join(self.wd, "d0000.txt"), "a") as fh:
+            fh.write(line + "\n")
 
     def _les_constants(self):
         """C_T of les_model 5 from c_t.in and C_mixed of les_models 6, 7, 10 from
@@ -299,7 +310,7 @@ class Simulation:
             self.time += c.dt
             if not math.isfinite(courant) or \
                     (self.settings.nonfinite_check and it % c.iprint1 == 0 and self.ctx.nonfinite() > 0):
-                self.log.append(f"ITIME={it:6d}   non-finite state")
+                self._out(f"ITIME={it:6d}   non-finite state")
                 return self.exit(-2)
             if it % c.iprint2 == 0:
                 self.write_restart()
@@ -307,8 +318,10 @@ class Simulation:
                 self.my_dt(courant)
             if it % c.iprint1 == 0:
                 el = int(_time.time() - self.t0)
-                self.log.append(f"ITIME={it:6d}   TIME={self.time:8.4f}    DT={c.dt:8.5f}   Courn= {courant:6.4f}  "
-                                f"CPU:({el // 3600:04d}:{el // 60 % 60:02d}:{el % 60:02d})")
+                sym = "*" if it % c.iwrite4 == 0 else " "
+                self._out(f"ITIME={it:6d}   TIME={self.time:8.4f}    DT={c.dt:8.5f}   Courn= {courant:6.4f}  "
+                          f"CPU:({el // 3600:04d}:{el // 60 % 60:02d}:{el % 60:02d}) {sym} "
+                          f"{LES_MODEL_NAME.get(c.les_model, '   ')}")
             if it % c.iprint1 == 0 or it % c.iwrite4 == 0:
                 if self.time > c.tmax:
                     return self.exit(1)
@@ -332,6 +345,7 @@ class Simulation:
     def exit(self, reason: int):
         """my_exit: a restart file is written for every reason >= 0."""
         self.exit_reason = reason
+        self._out(f"my_exit with reason {reason:4d}")
         if reason >= 0:
             self.write_restart()
             if self.int_particles:

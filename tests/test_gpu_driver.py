@@ -53,6 +53,11 @@ def test_driver_run_writes_reference_files(tmp_path):
     assert len(lines) == 2 and lines[0].split()[0] == "10"
     es_blocks = open(os.path.join(wd, "es.gp")).read().count("# ITIME=")
     assert es_blocks == 2
+    # the run log: format 9000 of main.f90 at every statistics step, then my_exit
+    log = open(os.path.join(wd, "d0000.txt")).read().splitlines()
+    assert [ln[:12] for ln in log[:2]] == ["ITIME=    10", "ITIME=    20"]
+    assert log[1].rstrip().endswith("*") and "TIME=  0.1000" in log[1]
+    assert log[-1] == "my_exit with reason    0"
     assert os.path.exists(os.path.join(wd, "sc01.gp")) and os.path.exists(os.path.join(wd, "es_02.gp"))
     u0 = read_real4(os.path.join(wd, "u.000000"))
     assert u0.shape == (64, 64, 64) and np.isfinite(u0).all()
