@@ -87,6 +87,14 @@ template <typename T, int L, int V> struct RowCfgV {
 //            the last with registers capped for 3 (FP64) or 4 (FP32) CTAs per SM
 //   8, 9, 10: staged lockstep kernel (k_xfused_st), the same three groupings,
 //            each CTA walking tiles with the next tile's input prefetched
+//   11: staged lockstep kernel, groups of 3, with 512/L row pairs (at least one)
+//       on 64 threads (128 from L = 1024), so that the CTAs of an SM pass their
+//       barriers independently
+template <typename T, int L> struct RowCfgSmall {
+    static constexpr int TC = L >= 512 ? 1 : 512 / L;
+    static constexpr int NT = L >= 1024 ? 128 : 64;
+    static constexpr size_t SMEM = (size_t)Lay<L, TC, true>::elems * sizeof(cx<T>);
+};
 constexpr int kFusedVariants = HIT3D_FUSED_VARIANTS;
 
 // Raise a kernel's dynamic shared-memory limit once per kernel and device, so
@@ -405,10 +413,9 @@ static int xfused_ms_L(hit3d_ctx *c, FusedArgs a)
 }
 // staged lockstep kernel: a grid of the CTAs that fit at once, each walking tiles
 // with the next tile's input rows prefetched into shared memory
-template <typename T, template <class> class OP, int L, int GF, int MINB>
+template <typename T, template <class> class OP, int L, int GF, int MINB, class RC = RowCfg<T, L>>
 static int xfused_st_L(hit3d_ctx *c, FusedArgs a)
 {
-    using RC = RowCfg<T, L>;
     constexpr int NIN = OP<T>::NIN;
     constexpr int NB = NIN > GF ? NIN : GF;
     auto k = k_xfused_st<T, L, RC::TC, RC::NT, T, OP<T>, GF, MINB>;
@@ -442,6 +449,10 @@ template <typename T, template <class> class OP, int L> static int xfused_L(hit3
         if (c->xcfg == 8) return xfused_st_L<T, OP, L, 3, 2>(c, a);
         if (c->xcfg == 9) return xfused_st_L<T, OP, L, 2, 2>(c, a);
         if (c->xcfg == 10) return xfused_st_L<T, OP, L, 1, sizeof(T) == 4 ? 4 : 3>(c, a);
+        if (c->xcfg == 11) {
+            using RS = RowCfgSmall<T, L>;  // 256 threads per SM at the full register file
+            return xfused_st_L<T, OP, L, 3, 256 / RS::NT, RS>(c, a);
+        }
         if (c->xcfg == 5) return xfused_ms_L<T, OP, L, 3>(c, a);
         if (c->xcfg == 6) return xfused_ms_L<T, OP, L, 2>(c, a);
         if (c->xcfg == 7) return xfused_ms_L<T, OP, L, 1, sizeof(T) == 4 ? 4 : 3>(c, a);
