@@ -216,9 +216,7 @@ H3D_D void store_split(const cx<T> *sm, cx<TS> *__restrict__ base, int64_t pitch
 {
     using LY = Lay<L, TC, true>;
     const int NH = lim < L / 2 + 1 ? lim : L / 2 + 1;
-    for (int t = threadIdx.x; t < TC * NH; t += NT) {
-        int c = t / NH, k = t - c * NH;
-        if (pair0 + c >= npairs) continue;
+    auto one = [&](int c, int k) {
         cx<T> zk = sm[LY::idx(c, k)], zm = sm[LY::idx(c, k == 0 ? 0 : L - k)];
         cx<TS> xa, xb;
         xa.x = (TS)((T)0.5 * (zk.x + zm.x));
@@ -228,6 +226,15 @@ H3D_D void store_split(const cx<T> *sm, cx<TS> *__restrict__ base, int64_t pitch
         cx<TS> *A = base + (int64_t)(2 * (pair0 + c)) * pitch;
         A[k] = xa;
         A[pitch + k] = xb;
+    };
+    if constexpr (TC == 1) {  // one pair: no division by the runtime NH
+        if (pair0 >= npairs) return;
+        for (int k = threadIdx.x; k < NH; k += NT) one(0, k);
+    } else {
+        for (int t = threadIdx.x; t < TC * NH; t += NT) {
+            int c = t / NH, k = t - c * NH;
+            if (pair0 + c < npairs) one(c, k);
+        }
     }
 }
 
@@ -699,13 +706,23 @@ H3D_D void stage_issue(const FusedArgs &a, cx<TS> *st, int pair0, int nch)
 {
     constexpr int PER = StageRow<TS>::PER;
     const int rs = nch * PER;
-    const int total = NIN * 2 * TC * nch;
-    for (int q = threadIdx.x; q < total; q += NT) {
-        const int ch = q % nch, rr = q / nch;
-        const int r = rr % (2 * TC), f = rr / (2 * TC);
-        if (pair0 + r / 2 >= a.npairs) continue;
-        const cx<TS> *src = reinterpret_cast<const cx<TS> *>(a.in[f]) + (int64_t)(2 * pair0 + r) * a.pitch + ch * PER;
-        cp_async16(st + (f * 2 * TC + r) * rs + ch * PER, src);
+    if constexpr (TC == 1) {  // one pair: row by row, no division by the runtime nch
+        if (pair0 < a.npairs) {
+#pragma unroll
+            for (int rr = 0; rr < NIN * 2; rr++) {
+                const cx<TS> *src = reinterpret_cast<const cx<TS> *>(a.in[rr >> 1]) + (int64_t)(2 * pair0 + (rr & 1)) * a.pitch;
+                for (int ch = threadIdx.x; ch < nch; ch += NT) cp_async16(st + rr * rs + ch * PER, src + ch * PER);
+            }
+        }
+    } else {
+        const int total = NIN * 2 * TC * nch;
+        for (int q = threadIdx.x; q < total; q += NT) {
+            const int ch = q % nch, rr = q / nch;
+            const int r = rr % (2 * TC), f = rr / (2 * TC);
+            if (pair0 + r / 2 >= a.npairs) continue;
+            const cx<TS> *src = reinterpret_cast<const cx<TS> *>(a.in[f]) + (int64_t)(2 * pair0 + r) * a.pitch + ch * PER;
+            cp_async16(st + (f * 2 * TC + r) * rs + ch * PER, src);
+        }
     }
     cp_async_commit();
 }
