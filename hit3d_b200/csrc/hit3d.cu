@@ -480,6 +480,31 @@ template <typename T, template <class> class OP> static int xfused(hit3d_ctx *c,
 }
 
 static dim3 pw_grid(const hit3d_ctx *c) { return dim3(c->nsm * 4); }
+// grid of a grid-stride kernel of 256-thread CTAs that may fit fewer than four
+// CTAs per SM: as many CTAs as are resident at once (at most four per SM), so
+// that no partial second wave leaves most SMs idle at the end of the pass
+static std::mutex g_occ_mu;
+static std::vector<std::pair<const void *, int>> g_occ;
+template <typename KF> static dim3 pw_grid(const hit3d_ctx *c, KF kernel)
+{
+    const void *key = reinterpret_cast<const void *>(kernel);
+    int per = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_occ_mu);
+        for (auto &e : g_occ)
+            if (e.first == key) per = e.second;
+        if (per == 0) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 256, 0) != cudaSuccess) {
+                (void)cudaGetLastError();  // not a launch error: fall back to one CTA per SM
+                per = 1;
+            }
+            if (per < 1) per = 1;
+            if (per > 4) per = 4;
+            g_occ.emplace_back(key, per);
+        }
+    }
+    return dim3(c->nsm * per);
+}
 
 // z forward pass of the six velocity products (after their y pass, in P) fused
 // with the 2/3-rule update of U and RO
@@ -974,7 +999,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 } else if (les) {
                     flux = Wf(nprod + 6 + 3 * s);
                 }
-                k_scalar<T><<<pw_grid(c), 256, 0, c->st>>>(a, 0, s, c->dx, Wf(6 + 3 * s), nullptr, c->U,
+                k_scalar<T><<<pw_grid(c, k_scalar<T>), 256, 0, c->st>>>(a, 0, s, c->dx, Wf(6 + 3 * s), nullptr, c->U,
                                                             c->U + (3 + s) * c->fs64, c->RO + (3 + s) * c->fs64,
                                                             src, flux);
                 H3D_LAUNCH_CHECK();
@@ -982,26 +1007,26 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
             if (fuse) {
                 H3D_TRY(zfwd_update<T>(c, a, Wf(0)));
             } else {
-                k_update_vel_23<T><<<pw_grid(c), 256, 0, c->st>>>(a, Wf(0), tau, c->U, c->RO);
+                k_update_vel_23<T><<<pw_grid(c, k_update_vel_23<T>), 256, 0, c->st>>>(a, Wf(0), tau, c->U, c->RO);
                 H3D_LAUNCH_CHECK();
             }
         } else if (pass == 0) {
             for (int s = 0; s < ns; s++) {
-                k_scalar<T><<<pw_grid(c), 256, 0, c->st>>>(a, 1, s, c->dx, Wf(6 + 3 * s), c->SP + s * c->fs64, c->U,
+                k_scalar<T><<<pw_grid(c, k_scalar<T>), 256, 0, c->st>>>(a, 1, s, c->dx, Wf(6 + 3 * s), c->SP + s * c->fs64, c->U,
                                                             c->U + (3 + s) * c->fs64, c->RO + (3 + s) * c->fs64);
                 H3D_LAUNCH_CHECK();
             }
-            k_rhs_vel_ps1<T><<<pw_grid(c), 256, 0, c->st>>>(a, Wf(0), c->U, c->RP);
+            k_rhs_vel_ps1<T><<<pw_grid(c, k_rhs_vel_ps1<T>), 256, 0, c->st>>>(a, Wf(0), c->U, c->RP);
             H3D_LAUNCH_CHECK();
         } else {
             for (int s = 0; s < ns; s++) {
                 const cx<T> *rs = (s < p.n_scalars && reac_slot[s] >= 0) ? Wf(reac_slot[s]) : nullptr;
-                k_scalar<T><<<pw_grid(c), 256, 0, c->st>>>(a, 2, s, c->dx, Wf(6 + 3 * s), c->SP + s * c->fs64, c->U,
+                k_scalar<T><<<pw_grid(c, k_scalar<T>), 256, 0, c->st>>>(a, 2, s, c->dx, Wf(6 + 3 * s), c->SP + s * c->fs64, c->U,
                                                             c->U + (3 + s) * c->fs64, c->RO + (3 + s) * c->fs64,
                                                             nullptr, nullptr, rs);
                 H3D_LAUNCH_CHECK();
             }
-            k_update_vel_ps2<T><<<pw_grid(c), 256, 0, c->st>>>(a, c->dx, Wf(0), c->RP, c->U, c->RO);
+            k_update_vel_ps2<T><<<pw_grid(c, k_update_vel_ps2<T>), 256, 0, c->st>>>(a, c->dx, Wf(0), c->RP, c->U, c->RO);
             H3D_LAUNCH_CHECK();
         }
     }

@@ -11,19 +11,23 @@ struct ModeIdx {
     int ialias;             // number of |k_i| > N/3 (x_fftw.f90:298-310)
 };
 
-H3D_D ModeIdx mode_of(int64_t t, int n, int nh)
+H3D_D ModeIdx mode_from(int kx, int kyi, int kzi, int n)
 {
     ModeIdx m;
-    m.kx = (int)(t % nh);
-    int64_t r = t / nh;
-    m.kyi = (int)(r % n);
-    m.kzi = (int)(r / n);
+    m.kx = kx;
+    m.kyi = kyi;
+    m.kzi = kzi;
     m.ax = m.kx;
     m.ay = kwave(m.kyi, n);
     m.az = kwave(m.kzi, n);
     const double rn3 = (double)(n / 3);
     m.ialias = (fabs(m.ay) > rn3) + (fabs(m.az) > rn3) + (fabs(m.ax) > rn3);
     return m;
+}
+H3D_D ModeIdx mode_of(int64_t t, int n, int nh)
+{
+    const int64_t r = t / nh;
+    return mode_from((int)(t % nh), (int)(r % n), (int)(r / n), n);
 }
 H3D_D int64_t soff(const ModeIdx &m, int n, int pitch) { return ((int64_t)m.kzi * n + m.kyi) * pitch + m.kx; }
 
@@ -46,6 +50,37 @@ H3D_D ModeIdx mode_at(int64_t t, int n, int nh, int kc)
     const int kyi = yc <= kc ? yc : n - (nk - yc), kzi = zc <= kc ? zc : n - (nk - zc);
     return mode_of(((int64_t)kzi * n + kyi) * nh + kx, n, nh);
 }
+
+// t / d for 0 <= t by a multiply-high with m = ceil(2^64 / d), exact while
+// t * d < 2^64 (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994): the per-step mode loops prepare their divisors
+// once per thread instead of dividing 64-bit integers at every mode.
+struct DivU64 {
+    uint64_t m;
+    int64_t d;
+    H3D_D explicit DivU64(int64_t d_) : m(~0ull / (uint64_t)d_ + 1ull), d(d_) {}  // d = 1 wraps m to 0
+    H3D_D int64_t operator()(int64_t t) const { return m ? (int64_t)__umul64hi((uint64_t)t, m) : t; }
+};
+
+// mode_at with the divisors prepared: index t of the loop over every mode
+// (kc < 0) or over the kept modes (kc >= 0) -> the mode
+struct ModeLoop {
+    DivU64 dx, dy;
+    int n, kc;
+    H3D_D ModeLoop(int n_, int nh, int kc_) : dx(kc_ < 0 ? nh : kc_ + 1), dy(kc_ < 0 ? n_ : 2 * kc_ + 1), n(n_), kc(kc_) {}
+    H3D_D ModeIdx at(int64_t t) const
+    {
+        const int64_t r = dx(t), zc = dy(r);
+        const int kx = (int)(t - r * dx.d), yc = (int)(r - zc * dy.d);
+        int kyi = yc, kzi = (int)zc;
+        if (kc >= 0) {
+            const int nk = 2 * kc + 1;
+            kyi = kyi <= kc ? kyi : n - (nk - kyi);
+            kzi = kzi <= kc ? kzi : n - (nk - kzi);
+        }
+        return mode_from(kx, kyi, kzi, n);
+    }
+};
 
 // Machiels band forcing: a mode takes part when kx < N/2 (the reference loops
 // over real indices 1..nx) and its float32 shell index is in [1, kfmax]
@@ -119,8 +154,9 @@ __global__ void k_update_vel_23(const StepArgs a, const cx<TP> *__restrict__ P, 
 {
     const int64_t nm = mode_count(a.n, a.nh, a.kc);
     const double fac = (a.flow_type == 1) ? a.famp / *a.fenergy : 0.0;
+    const ModeLoop ml(a.n, a.nh, a.kc);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
-        ModeIdx m = mode_at(t, a.n, a.nh, a.kc);
+        ModeIdx m = ml.at(t);
         int64_t o = soff(m, a.n, a.pitch), po = soff(m, a.n, a.ppitch);
         double2 u[3] = {U[o], U[o + a.fs], U[o + 2 * a.fs]};
         double2 r[3];
@@ -171,8 +207,9 @@ __global__ void k_rhs_vel_ps1(const StepArgs a, const cx<TP> *__restrict__ P, co
                               double2 *__restrict__ RP)
 {
     const int64_t nm = (int64_t)a.n * a.n * a.nh;
+    const ModeLoop ml(a.n, a.nh, -1);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
-        ModeIdx m = mode_of(t, a.n, a.nh);
+        ModeIdx m = ml.at(t);
         int64_t o = soff(m, a.n, a.pitch), po = soff(m, a.n, a.ppitch);
         double2 r[3];
         if (m.ialias > 1) {
@@ -209,8 +246,9 @@ __global__ void k_update_vel_ps2(const StepArgs a, double dx, const cx<TP> *__re
 {
     const int64_t nm = (int64_t)a.n * a.n * a.nh;
     const double fac = (a.flow_type == 1) ? a.famp / *a.fenergy : 0.0;
+    const ModeLoop ml(a.n, a.nh, -1);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
-        ModeIdx m = mode_of(t, a.n, a.nh);
+        ModeIdx m = ml.at(t);
         int64_t o = soff(m, a.n, a.pitch), po = soff(m, a.n, a.ppitch);
         double2 u[3] = {U[o], U[o + a.fs], U[o + 2 * a.fs]};
         double2 r[3];
@@ -266,8 +304,9 @@ __global__ void k_scalar(const StepArgs a, int mode, int s, double dx, const cx<
     const int kc = mode == 0 ? a.kc : -1;
     const int64_t nm = mode_count(a.n, a.nh, kc);
     const double pe = a.pe[s];
+    const ModeLoop ml(a.n, a.nh, kc);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
-        ModeIdx m = mode_at(t, a.n, a.nh, kc);
+        ModeIdx m = ml.at(t);
         int64_t o = soff(m, a.n, a.pitch), po = soff(m, a.n, a.ppitch);
         double kx = m.ax, ky = m.ay, kz = m.az;
         // the products are read only where they are used (the 2/3 rule masks the rest)
