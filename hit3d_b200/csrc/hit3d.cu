@@ -64,7 +64,7 @@ template <typename T, int L, bool YPASS = false> struct ColCfg {
     // CTAs per SM (measured faster there, slower for the z passes and FP32)
     static constexpr int TC = sizeof(T) == 8 ? ((L >= 1024 && YPASS) ? 4 : 8) : 16;
     static constexpr int NT0 = TC * L / plan_rmax(L);
-    static constexpr int NTMAX = sizeof(T) == 8 ? 256 : 512;
+    static constexpr int NTMAX = 512;
     static constexpr int NT = NT0 > NTMAX ? NTMAX : NT0;
     static constexpr size_t SMEM = (size_t)Lay<L, TC, false>::elems * sizeof(cx<T>);
 };
