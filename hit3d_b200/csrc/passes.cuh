@@ -746,6 +746,10 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_st(const FusedArgs a, const
     const int rs = nch * StageRow<TS>::PER;
     const int ntiles = (a.npairs + TC - 1) / TC;
     OP op{(T)a.p0, (T)a.p1};
+    // each warp's Courant maximum over its tiles, kept in shared memory rather
+    // than in a register live across the tile loop; one atomic per warp at the end
+    __shared__ double cwarp[NT / 32];
+    if ((threadIdx.x & 31) == 0) cwarp[threadIdx.x >> 5] = 0.0;
     if ((int)blockIdx.x < ntiles) stage_issue<TS, OP::NIN, TC, NT>(a, st, blockIdx.x * TC, nch);
 
 #pragma unroll 1
@@ -809,7 +813,7 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_st(const FusedArgs a, const
             }
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, off));
-            if ((threadIdx.x & 31) == 0) atomicMax(a.cmax, (unsigned long long)__double_as_longlong(cm));
+            if ((threadIdx.x & 31) == 0) cwarp[threadIdx.x >> 5] = fmax(cwarp[threadIdx.x >> 5], cm);
         }
         cx<T> aux[NP];
 #pragma unroll
@@ -861,6 +865,8 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_st(const FusedArgs a, const
         }
     }
     cp_async_wait_all();
+    if (a.cmax != nullptr && (threadIdx.x & 31) == 0)
+        atomicMax(a.cmax, (unsigned long long)__double_as_longlong(cwarp[threadIdx.x >> 5]));
 }
 
 // velocity products (rhs_velocity.f90:56-72): uu uv uw vv vw ww; Courant |u|+|v|+|w|
