@@ -64,7 +64,9 @@ template <typename T, int L, bool YPASS = false> struct ColCfg {
     // CTAs per SM (measured faster there, slower for the z passes and FP32)
     static constexpr int TC = sizeof(T) == 8 ? ((L >= 1024 && YPASS) ? 4 : 8) : 16;
     static constexpr int NT0 = TC * L / plan_rmax(L);
-    static constexpr int NTMAX = 512;
+    // one 8-element butterfly set per thread where 512 threads allow it; the
+    // FP64 y passes at L = 1024 keep 256 threads (measured faster there)
+    static constexpr int NTMAX = (sizeof(T) == 8 && L >= 1024 && YPASS) ? 256 : 512;
     static constexpr int NT = NT0 > NTMAX ? NTMAX : NT0;
     static constexpr size_t SMEM = (size_t)Lay<L, TC, false>::elems * sizeof(cx<T>);
 };

@@ -191,6 +191,18 @@ __global__ void __launch_bounds__(NT, (ColMinBlocks<T, L, TC, NT>::value)) k_col
 template <typename T, int L, int TC, int NT, bool REV>
 using RowFFT = ColFFT<T, L, TC, NT, true, REV ? false : true, REV>;
 
+// t / d for 0 <= t with t * d < 2^32, by a multiply-high with m = ceil(2^32 / d)
+// (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994): the row passes split their flat loop indices
+// with a divisor prepared once instead of dividing by a runtime count at every
+// iteration
+struct DivU32 {
+    unsigned m;
+    int d;
+    H3D_D explicit DivU32(int d_) : m(0xffffffffu / (unsigned)d_ + 1u), d(d_) {}  // d = 1 wraps m to 0
+    H3D_D int operator()(int t) const { return m ? (int)__umulhi((unsigned)t, m) : t; }
+};
+
 // Hermitian-extended packed spectrum Z[k] = Xa[k] + i Xb[k] of rows A, B at
 // k in [0, L); the imaginary parts of kx = 0 and kx = N/2 are ignored, as
 // FFTW's c2r does.  Only kx < lim is read (2/3-rule pruning; the rest is zero).
@@ -231,8 +243,9 @@ H3D_D void store_split(const cx<T> *sm, cx<TS> *__restrict__ base, int64_t pitch
         if (pair0 >= npairs) return;
         for (int k = threadIdx.x; k < NH; k += NT) one(0, k);
     } else {
+        const DivU32 dnh(NH);  // t < TC * NH <= 2^15, NH <= 513
         for (int t = threadIdx.x; t < TC * NH; t += NT) {
-            int c = t / NH, k = t - c * NH;
+            int c = dnh(t), k = t - c * NH;
             if (pair0 + c < npairs) one(c, k);
         }
     }
@@ -716,8 +729,9 @@ H3D_D void stage_issue(const FusedArgs &a, cx<TS> *st, int pair0, int nch)
         }
     } else {
         const int total = NIN * 2 * TC * nch;
+        const DivU32 dch(nch);  // q < total <= 2^18, nch <= 513
         for (int q = threadIdx.x; q < total; q += NT) {
-            const int ch = q % nch, rr = q / nch;
+            const int rr = dch(q), ch = q - rr * nch;
             const int r = rr % (2 * TC), f = rr / (2 * TC);
             if (pair0 + r / 2 >= a.npairs) continue;
             const cx<TS> *src = reinterpret_cast<const cx<TS> *>(a.in[f]) + (int64_t)(2 * pair0 + r) * a.pitch + ch * PER;
