@@ -92,6 +92,8 @@ template <typename T, int L, int V> struct RowCfgV {
 //   11: staged lockstep kernel, groups of 3, with 512/L row pairs (at least one)
 //       on 64 threads (128 from L = 1024), so that the CTAs of an SM pass their
 //       barriers independently
+//   12: as 11 with six CTAs per SM for FP32 (the register file holds 384
+//       threads at 168 registers), groups of 2 for FP64
 template <typename T, int L> struct RowCfgSmall {
     static constexpr int TC = L >= 512 ? 1 : 512 / L;
     static constexpr int NT = L >= 1024 ? 128 : 64;
@@ -454,6 +456,11 @@ template <typename T, template <class> class OP, int L> static int xfused_L(hit3
         if (c->xcfg == 11) {
             using RS = RowCfgSmall<T, L>;  // 256 threads per SM at the full register file
             return xfused_st_L<T, OP, L, 3, 256 / RS::NT, RS>(c, a);
+        }
+        if (c->xcfg == 12) {
+            using RS = RowCfgSmall<T, L>;
+            if constexpr (sizeof(T) == 4) return xfused_st_L<T, OP, L, 3, 384 / RS::NT, RS>(c, a);  // 168 registers
+            else return xfused_st_L<T, OP, L, 2, 256 / RS::NT, RS>(c, a);
         }
         if (c->xcfg == 5) return xfused_ms_L<T, OP, L, 3>(c, a);
         if (c->xcfg == 6) return xfused_ms_L<T, OP, L, 2>(c, a);

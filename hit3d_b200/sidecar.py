@@ -12,7 +12,7 @@ error that names the line, as a bad `.in` line is in the reference.
 
   precision       0 | 1        FP64 transforms | FP32 transforms (FP64 state)
   pruning         on | off     skip work on the modes the 2/3 rule discards
-  variant         auto | 0..11 launch shape of the fused row pass; auto tunes
+  variant         auto | 0..12 launch shape of the fused row pass; auto tunes
   device          int          CUDA device ordinal
   c_smag          float        Smagorinsky constant (the reference fixes 0.18)
   les_model       int          overrides the `.in` LES model; 20 is the learned
