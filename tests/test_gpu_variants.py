@@ -29,8 +29,29 @@ def test_variants_agree(n, precision, case):
         outs.append(c.download_fields())
         c.close()
     tol = 1e-13 if precision == 0 else 1e-6
-    for v in range(1, 8):
+    for v in range(1, N_VARIANTS):
         assert relerr(outs[v], outs[0]) < tol, (v, relerr(outs[v], outs[0]))
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_one_pair_variants_at_512(precision):
+    """At L = 512 variants 11 and 12 take one row pair per CTA (the stage and
+    split loops without index division); they agree with variant 8 (two pairs
+    per CTA) over two forced steps."""
+    from hit3d_b200 import Context, Params
+    kw = dict(nx=512, flow_type=1, kfmax=2, nu=1.0 / 3000.0, dt=2e-4, precision=precision)
+    outs = {}
+    for v in (8, 11, 12):
+        c = Context(Params(**kw))
+        c.set_variant(v)
+        c.init_velocity(RN1, 2, 4.0, 2.0)
+        c.dealias_all()
+        c.step(2)
+        outs[v] = c.download_fields()
+        c.close()
+    tol = 1e-13 if precision == 0 else 1e-6
+    for v in (11, 12):
+        assert relerr(outs[v], outs[8]) < tol, (v, relerr(outs[v], outs[8]))
 
 
 def test_tuner_picks_a_valid_variant():
