@@ -224,17 +224,17 @@ H3D_D cx<T> load_packed(const cx<TS> *__restrict__ A, const cx<TS> *__restrict__
 // into the half spectra of the two packed rows and store kx < lim of them.
 template <typename T, int L, int TC, int NT, typename TS>
 H3D_D void store_split(const cx<T> *sm, cx<TS> *__restrict__ base, int64_t pitch, int pair0, int npairs,
-                       int lim = L / 2 + 1)
+                       int lim = L / 2 + 1, T half = (T)0.5)
 {
     using LY = Lay<L, TC, true>;
     const int NH = lim < L / 2 + 1 ? lim : L / 2 + 1;
     auto one = [&](int c, int k) {
         cx<T> zk = sm[LY::idx(c, k)], zm = sm[LY::idx(c, k == 0 ? 0 : L - k)];
         cx<TS> xa, xb;
-        xa.x = (TS)((T)0.5 * (zk.x + zm.x));
-        xa.y = (TS)((T)0.5 * (zk.y - zm.y));
-        xb.x = (TS)((T)0.5 * (zk.y + zm.y));
-        xb.y = (TS)((T)-0.5 * (zk.x - zm.x));
+        xa.x = (TS)(half * (zk.x + zm.x));
+        xa.y = (TS)(half * (zk.y - zm.y));
+        xb.x = (TS)(half * (zk.y + zm.y));
+        xb.y = (TS)(-half * (zk.x - zm.x));
         cx<TS> *A = base + (int64_t)(2 * (pair0 + c)) * pitch;
         A[k] = xa;
         A[pitch + k] = xb;
@@ -793,10 +793,15 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_st(const FusedArgs a, const
             if (tile + (int)gridDim.x < ntiles) stage_issue<TS, OP::NIN, TC, NT>(a, st, pair0 + gridDim.x * TC, nch);
             FI::template run_multi<OP::NIN>(in, sm, phys, tw);
         }
+        // quadratic products: the 1/N^3 of the inverse transforms is applied
+        // once, as norm^2 in the split of the forward outputs (and norm to the
+        // Courant maximum and the physical fields written out)
+        if constexpr (!OP::QUAD) {
 #pragma unroll
-        for (int f = 0; f < OP::NIN; f++)
+            for (int f = 0; f < OP::NIN; f++)
 #pragma unroll
-            for (int q = 0; q < NP; q++) phys[f][q] = mk<T>(phys[f][q].x * norm, phys[f][q].y * norm);
+                for (int q = 0; q < NP; q++) phys[f][q] = mk<T>(phys[f][q].x * norm, phys[f][q].y * norm);
+        }
         __syncthreads();
         if (a.phys != nullptr) {
             double *pb = a.phys;
@@ -809,8 +814,8 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_st(const FusedArgs a, const
                         int64_t r = 2 * (pair0 + c);
 #pragma unroll
                         for (int f = 0; f < OP::NPHYS; f++) {
-                            pb[f * a.phys_fs + r * a.phys_pitch + p] = (double)phys[f][i * FI::RL + m].x;
-                            pb[f * a.phys_fs + (r + 1) * a.phys_pitch + p] = (double)phys[f][i * FI::RL + m].y;
+                            pb[f * a.phys_fs + r * a.phys_pitch + p] = (double)(phys[f][i * FI::RL + m].x * (OP::QUAD ? (T)a.norm : (T)1));
+                            pb[f * a.phys_fs + (r + 1) * a.phys_pitch + p] = (double)(phys[f][i * FI::RL + m].y * (OP::QUAD ? (T)a.norm : (T)1));
                         }
                     }
                 }
@@ -873,19 +878,20 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_st(const FusedArgs a, const
                 const int o = g * GF + gf;
                 if (o < OP::NOUT)
                     store_split<T, L, TC, NT, TS>(sm + gf * E, reinterpret_cast<cx<TS> *>(a.out[o]), a.pitch, pair0,
-                                                  a.npairs, lim);
+                                                  a.npairs, lim, OP::QUAD ? (T)0.5 * (T)a.norm * (T)a.norm : (T)0.5);
             }
             __syncthreads();
         }
     }
     cp_async_wait_all();
     if (a.cmax != nullptr && (threadIdx.x & 31) == 0)
-        atomicMax(a.cmax, (unsigned long long)__double_as_longlong(cwarp[threadIdx.x >> 5]));
+        atomicMax(a.cmax, (unsigned long long)__double_as_longlong(cwarp[threadIdx.x >> 5] * (OP::QUAD ? (double)(T)a.norm : 1.0)));
 }
 
 // velocity products (rhs_velocity.f90:56-72): uu uv uw vv vw ww; Courant |u|+|v|+|w|
 template <typename T> struct OpVel {
     static constexpr int NIN = 3, NOUT = 6, NPHYS = 3;
+    static constexpr bool QUAD = true;  // products of degree 2, Courant of degree 1 in the fields
     static constexpr bool NEED_AUX = false;
     static H3D_HD constexpr bool uses(int o, int f)
     {
@@ -910,6 +916,7 @@ template <typename T> struct OpVel {
 // scalar fluxes (rhs_scalars.f90:82-85): phi*u, phi*v, phi*w from (u, v, w, phi)
 template <typename T> struct OpScal {
     static constexpr int NIN = 4, NOUT = 3, NPHYS = 0;
+    static constexpr bool QUAD = false;
     static constexpr bool NEED_AUX = false;
     static H3D_HD constexpr bool uses(int o, int f) { return f == o || f == 3; }
     T p0, p1;
@@ -923,6 +930,7 @@ template <typename T> struct OpScal {
 // p0 = (Cs Delta)^2
 template <typename T> struct OpSmag {
     static constexpr int NIN = 6, NOUT = 6, NPHYS = 0;
+    static constexpr bool QUAD = false;
     static constexpr bool NEED_AUX = true;
     static H3D_HD constexpr bool uses(int o, int f) { return f == o; }
     T p0, p1;
