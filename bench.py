@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--les-only", action="store_true", help="only the learned-LES step rates (profiling runs)")
     ap.add_argument("--no-configs", action="store_true", help="skip the step rates of the other configurations")
     ap.add_argument("--configs-only", action="store_true", help="only the step rates of the other configurations")
+    ap.add_argument("--config", default=None, choices=CONFIG_NAMES, help="with --configs-only: just this configuration")
+    ap.add_argument("--config-steps", type=int, default=0, help="timed steps of --config forced_256 (default 20)")
     ap.add_argument("--cmp-every", type=int, default=50, help="FP32 vs FP64 statistics every this many steps")
     ap.add_argument("--cmp-points", type=int, default=4)
     ap.add_argument("--variant", type=int, default=-1,
@@ -214,29 +216,64 @@ def timed_steps(torch, ctx, steps):
     return e0.elapsed_time(e1) / 1000.0
 
 
-def cpu_sample(n_gpu, fields0):
-    """Oracle (C/OpenMP FP64 restatement) on the host cores: one step at 256^3 if
-    the workload is 512^3, scaled by the N^3 log N work ratio to the 512^3 unit."""
+def host_cpu():
+    """CPU model, physical cores and the threads this process may use."""
+    model, cores = None, set()
+    phys = core = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                k, _, v = line.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "model name" and model is None:
+                    model = v
+                elif k == "physical id":
+                    phys = v
+                elif k == "core id":
+                    core = v
+                elif not k and phys is not None and core is not None:
+                    cores.add((phys, core))
+                    phys = core = None
+        if phys is not None and core is not None:
+            cores.add((phys, core))
+    except OSError:
+        pass
+    try:
+        threads = len(os.sched_getaffinity(0))
+    except AttributeError:
+        threads = os.cpu_count() or 1
+    return {"cpu_model": model, "physical_cores": len(cores) or None, "threads": threads}
+
+
+def oracle_run(n):
+    """The oracle (C/OpenMP FP64 restatement of the reference step) on the host,
+    initialised as the GPU run is: RANDu/Box-Muller from RN1, E(k) ~ k^2 exp(-2(k/4)^2)."""
     import oracle
-    cores = os.cpu_count() or 1
-    n_s = 256 if n_gpu >= 256 else n_gpu
-    o = oracle.Oracle(n_s, nscal=0, dealias=0, flow_type=1, kfmax=2, nu=1.0 / RE, dt=DT, famp=0.5)
+    o = oracle.Oracle(n, nscal=0, dealias=0, flow_type=1, kfmax=2, nu=1.0 / RE, dt=DT, famp=0.5)
     o.init_velocity(RN1, isp_type=2, peak_wavenum=4.0, ir_exp=2.0)
     o.dealias_all()
-    o.step(1)  # warm-up: page in and first-order step
+    return o
+
+
+def cpu_sample(n, warm=1, timed=2, budget_s=240.0):
+    """Time the oracle at the workload's own grid: `warm` untimed steps (the first
+    one is the first-order step), then up to `timed` steps, fewer only if the
+    warm-up step says they would take longer than budget_s."""
+    hc = host_cpu()
+    o = oracle_run(n)
     t0 = time.perf_counter()
-    nst = 0
-    while True:
-        o.step(1)
-        nst += 1
-        el = time.perf_counter() - t0
-        if el > 10.0 or nst >= 5:
-            break
-    rate = nst / el
-    scale = (n_gpu ** 3 * np.log2(n_gpu ** 3)) / (n_s ** 3 * np.log2(n_s ** 3))
-    return {"value": rate / scale, "unit": "timesteps/s", "cores": cores, "kind": "port",
-            "sample": f"{nst} oracle steps at {n_s}^3 ({el:.1f} s, OpenMP on {cores} threads), scaled by the "
-                      f"N^3 log2 N^3 work ratio {scale:.2f} to {n_gpu}^3"}
+    o.step(max(1, warm))
+    t_warm = (time.perf_counter() - t0) / max(1, warm)
+    k = max(1, min(timed, int(budget_s / max(t_warm, 1e-9))))
+    t0 = time.perf_counter()
+    o.step(k)
+    el = time.perf_counter() - t0
+    del o
+    return {"value": k / el, "unit": "timesteps/s", "cores": hc["threads"], "kind": "port",
+            "cpu_model": hc["cpu_model"], "physical_cores": hc["physical_cores"], "steps_timed": k,
+            "seconds": round(el, 2),
+            "sample": f"{k} oracle steps at {n}^3 after {max(1, warm)} warm-up (OpenMP on {hc['threads']} threads of "
+                      f"{hc['physical_cores']} physical cores, {hc['cpu_model']})"}
 
 
 def les_leg(torch, args, dns_rate, dns32_rate, device):
@@ -300,11 +337,14 @@ def les_leg(torch, args, dns_rate, dns32_rate, device):
     return out
 
 
-def configs_leg(torch, args, device):
+CONFIG_NAMES = ("decaying_64", "forced_256", "batched_96", "les_128")
+
+
+def configs_leg(torch, args, device, only=None):
     """Step rates of the other configurations of the path (the per-configuration
     parity lives in tests/): 64^3 decaying; 256^3 forced with phase-shift
     dealiasing, two scalars and 10^6 CINT particles; the batched 96-run set;
-    128^3 LES with each closure."""
+    128^3 LES with each closure.  `only` runs one of CONFIG_NAMES."""
     from hit3d_b200 import Context, Params
     from hit3d_b200.batch import Batch, batched_runs
     out = {}
@@ -320,76 +360,139 @@ def configs_leg(torch, args, device):
         t = timed_steps(torch, c, steps)
         return steps / t
 
-    c = Context(Params(nx=64, dealias=0, flow_type=0, nu=1.0 / 400.0, dt=0.005, device=device))
-    r = rate(c, 100)
-    out["decaying_64"] = {"workload": "decaying DNS 64^3, Re=400, dt=0.005, 2/3 rule", "steps_per_s": r,
-                          "grid_points_steps_per_s": r * 64 ** 3}
-    c.close()
-
-    n = 256
-    c = Context(Params(nx=n, dealias=1, flow_type=1, force_type=1, kfmax=2, famp=0.5, nu=1.0 / 1000.0, dt=0.001,
-                       n_scalars=2, sc=[0.7, 1.0], scalar_type=[0, 0], device=device))
-    c.set_scalars_active(True)
-    # 100^3 = 10^6 particles on the reference's lattice of cell centres, in its
-    # 1-based grid units (m_particles.f90:220-262, 314-319)
-    g = (np.arange(100) + 0.5) * n / 100.0 + 1.0
-    Z, Y, X = np.meshgrid(g, g, g, indexing="ij")
-    c.particles_upload(np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1), None, scheme=1)
-    r = rate(c, 20)
-    out["forced_256_phase_shift_2_scalars_1e6_particles"] = {
-        "workload": "forced DNS 256^3, Re=1000, dt=0.001, phase shift, 2 scalars (Sc 0.7, 1.0), 10^6 CINT particles",
-        "steps_per_s": r, "grid_points_steps_per_s": r * n ** 3}
-    c.close()
-
-    ps = batched_runs()
-    b = Batch(ps)
-    b.init()
-    b.step(args.warmup + 1, graph_steps=10)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    b.step(50, graph_steps=10)
-    torch.cuda.synchronize()
-    t = time.perf_counter() - t0
-    pts = sum(p.nx ** 3 for p in ps)
-    out["batched_96_runs"] = {"workload": "96 forced runs: 32 x 32^3, 32 x 48^3, 28 x 64^3, 4 x 128^3, one recorded graph",
-                              "run_steps_per_s": len(ps) * 50 / t, "grid_points_steps_per_s": pts * 50 / t,
-                              "graph_launches": b.graph_launches, "timing": "host clock around 50 steps (5 graph launches)"}
-    b.close()
-
-    les = {}
-    nparam = None
-    for name, model in (("smagorinsky", 1), ("dynamic_localization", 2), ("dynamic_localization_lag", 3),
-                        ("dynamic_structure", 4), ("dynamic_structure_lag", 5), ("mixed", 6), ("mixed_lag", 7),
-                        ("one_equation_mixed", 10), ("learned", 20)):
-        # C_T and C_mixed stand in for the values of c_t.in / c_mixed.in
-        c = Context(Params(nx=128, dealias=0, flow_type=1, force_type=1, kfmax=2, famp=0.5, nu=1.0 / 6000.0,
-                           dt=0.002, les_model=model, device=device, c_t=1.0, c_mixed=0.5))
-        if model == 20:
-            from hit3d_b200 import gpu
-            nparam = int(gpu.lib().hit3d_mlp_nparam())
-            w = np.zeros(nparam, dtype=np.float32)
-            w[nparam - 5] = -2.0 * 0.18 ** 2 / 4.0
-            bits = ((w.view(np.uint32).astype(np.uint64) + 0x7FFF + ((w.view(np.uint32) >> 16) & 1)) >> 16).astype(np.uint16)
-            c.les_set_mlp(bits, 2 * 2.0 * np.pi / 128, clip=True, kernel=1)
-        les[name] = rate(c, 50)
+    if only in (None, "decaying_64"):
+        c = Context(Params(nx=64, dealias=0, flow_type=0, nu=1.0 / 400.0, dt=0.005, device=device))
+        r = rate(c, 100)
+        out["decaying_64"] = {"workload": "decaying DNS 64^3, Re=400, dt=0.005, 2/3 rule", "steps_per_s": r,
+                              "grid_points_steps_per_s": r * 64 ** 3}
         c.close()
-    out["les_128"] = {"workload": "LES 128^3, Re=6000, 2/3 rule", "steps_per_s": les}
+
+    if only in (None, "forced_256"):
+        n = 256
+        c = Context(Params(nx=n, dealias=1, flow_type=1, force_type=1, kfmax=2, famp=0.5, nu=1.0 / 1000.0, dt=0.001,
+                           n_scalars=2, sc=[0.7, 1.0], scalar_type=[0, 0], device=device))
+        c.set_scalars_active(True)
+        # 100^3 = 10^6 particles on the reference's lattice of cell centres, in its
+        # 1-based grid units (m_particles.f90:220-262, 314-319)
+        g = (np.arange(100) + 0.5) * n / 100.0 + 1.0
+        Z, Y, X = np.meshgrid(g, g, g, indexing="ij")
+        c.particles_upload(np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1), None, scheme=1)
+        r = rate(c, args.config_steps or 20)
+        prof = c.step_profile(2)
+        out["forced_256"] = {
+            "workload": "forced DNS 256^3, Re=1000, dt=0.001, phase shift, 2 scalars (Sc 0.7, 1.0), 10^6 CINT particles",
+            "steps_per_s": r, "grid_points_steps_per_s": r * n ** 3,
+            "stage_ms": {k: round(v / 2, 4) for k, v in prof.items() if v > 0}}
+        c.close()
+
+    if only in (None, "batched_96"):
+        ps = batched_runs()
+        b = Batch(ps)
+        b.init()
+        # first-order step, then one chunk through the graph, so that the timed
+        # region replays a graph recorded beforehand
+        b.step(1 + 10, graph_steps=10)
+        b.step(args.warmup, graph_steps=10)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.step(50, graph_steps=10)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        pts = sum(p.nx ** 3 for p in ps)
+        out["batched_96"] = {"workload": "96 forced runs: 32 x 32^3, 32 x 48^3, 28 x 64^3, 4 x 128^3, one recorded graph",
+                             "run_steps_per_s": len(ps) * 50 / t, "grid_points_steps_per_s": pts * 50 / t,
+                             "graph_launches": b.graph_launches, "timing": "host clock around 50 steps (5 graph launches)"}
+        b.close()
+
+    if only in (None, "les_128"):
+        les = {}
+        for name, model in (("smagorinsky", 1), ("dynamic_localization", 2), ("dynamic_localization_lag", 3),
+                            ("dynamic_structure", 4), ("dynamic_structure_lag", 5), ("mixed", 6), ("mixed_lag", 7),
+                            ("one_equation_mixed", 10), ("learned", 20)):
+            # C_T and C_mixed stand in for the values of c_t.in / c_mixed.in
+            c = Context(Params(nx=128, dealias=0, flow_type=1, force_type=1, kfmax=2, famp=0.5, nu=1.0 / 6000.0,
+                               dt=0.002, les_model=model, device=device, c_t=1.0, c_mixed=0.5))
+            if model == 20:
+                from hit3d_b200 import gpu
+                nparam = int(gpu.lib().hit3d_mlp_nparam())
+                w = np.zeros(nparam, dtype=np.float32)
+                w[nparam - 5] = -2.0 * 0.18 ** 2 / 4.0
+                bits = ((w.view(np.uint32).astype(np.uint64) + 0x7FFF + ((w.view(np.uint32) >> 16) & 1)) >> 16).astype(np.uint16)
+                c.les_set_mlp(bits, 2 * 2.0 * np.pi / 128, clip=True, kernel=1)
+            les[name] = rate(c, 50)
+            c.close()
+        out["les_128"] = {"workload": "LES 128^3, Re=6000, 2/3 rule", "steps_per_s": les}
     return out
 
 
+def workload_name(n):
+    return (f"forced DNS {n}^3, Re={RE:g}, dt={DT}, 2/3 rule, KFMAX=2, FAMP=0.5, "
+            "E(k)~k^2 exp(-2(k/4)^2) RANDu init")
+
+
 def run_reference(args):
+    """The CPU implementation of the step (the oracle port: the reference itself
+    needs a Fortran/MPI/FFTW toolchain that these machines lack) on this host's
+    cores, on the same workload; one step of the arm is one oracle step."""
     rank, world, _ = dist_info()
     if rank != 0:
         return
-    cs = cpu_sample(args.n, None)
-    line = {"impl": "reference", "metric": metric_name(args.n), "value": cs["value"], "unit": "timesteps/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"forced DNS {args.n}^3, Re={RE:g}, dt={DT}, 2/3 rule, KFMAX=2, FAMP=0.5",
-                       "grid": args.n},
+    cs = cpu_sample(args.n, warm=args.warmup, timed=args.steps, budget_s=300.0)
+    line = {"impl": "reference", "metric": metric_name(args.n), "value": cs["value"], "unit": "timesteps/s",
+            "n_gpus": args.gpus, "steps": cs["steps_timed"], "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_name(args.n), "grid": args.n},
             "cpu_baseline": cs,
             "e2e": {"value": cs["value"], "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def _sig(x, d=4):
+    """Round floats to d significant digits, recursively."""
+    if isinstance(x, float):
+        return float(f"{x:.{d}g}")
+    if isinstance(x, dict):
+        return {k: _sig(v, d) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [_sig(v, d) for v in x]
+    return x
+
+
+def summarize(line):
+    """Compact summary of the bench line: the headline, the FP32 form, the
+    other configurations, the learned LES and the CPU baseline."""
+    s = {"fp64_steps_per_s": line["value"], "ms_per_step": line["ms_per_step"],
+         "roofline_frac": line["roofline"]["frac"], "roofline_kernel": line["roofline"]["kernel"],
+         "e2e_steps_per_s": (line.get("e2e") or {}).get("value")}
+    f = line.get("fp32_fft")
+    if f:
+        s["fp32"] = {"steps_per_s": f["value"], "speedup_vs_fp64": f["speedup_vs_fp64"],
+                     "ek_max_rel_err_over_run": f.get("ek_max_rel_err_over_run"),
+                     "per_step": [[c["step"], c["ek_max_rel_err"], c["eps_rel_err"], c["skew_abs_err"]]
+                                  for c in f.get("vs_fp64_every_%d_steps" % 50, [])]}
+    oc = line.get("other_configs") or {}
+    if "error" in oc:
+        s["configs_error"] = oc["error"]
+    for k, v in oc.items():
+        if isinstance(v, dict) and "steps_per_s" in v and not isinstance(v["steps_per_s"], dict):
+            s[k] = v["steps_per_s"]
+    if "batched_96" in oc:
+        b = oc["batched_96"]
+        s["batched_96"] = {"run_steps_per_s": b["run_steps_per_s"],
+                                "grid_points_steps_per_s": b["grid_points_steps_per_s"]}
+    if "les_128" in oc:
+        s["les_128_steps_per_s"] = oc["les_128"]["steps_per_s"]
+    le = line.get("learned_les")
+    if le:
+        s["learned_les"] = {"steps_per_s": le.get("steps_per_s"),
+                            "closure_ms": (le.get("learned_stage_ms") or {}).get("closure"),
+                            "speedup_vs_dns_fp64": le.get("speedup_vs_dns_fp64")}
+        ap = le.get("aposteriori") or {}
+        if "mean_abs_log_spectrum_error" in ap:
+            s["learned_les"]["aposteriori"] = {"case": ap["dns_to_les"], "error": ap["mean_abs_log_spectrum_error"]}
+    c = line.get("cpu_baseline") or {}
+    s["cpu_baseline_steps_per_s"] = c.get("value")
+    return _sig(s)
 
 
 def main():
@@ -404,7 +507,7 @@ def main():
         print(json.dumps({"learned_les": les_leg(torch, args, None, None, local)}), flush=True)
         return
     if args.configs_only:
-        print(json.dumps({"other_configs": configs_leg(torch, args, local)}), flush=True)
+        print(json.dumps({"other_configs": configs_leg(torch, args, local, only=args.config)}), flush=True)
         return
     dist = None
     if world > 1:
@@ -557,7 +660,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu = cpu_sample(n, fields0)
+            cpu = cpu_sample(n)
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "error": str(e)}
 
@@ -566,8 +669,7 @@ def main():
             "metric": metric_name(n), "value": value, "unit": "timesteps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"forced DNS {n}^3, Re={RE:g}, dt={DT}, 2/3 rule, KFMAX=2, FAMP=0.5, "
-                                   "E(k)~k^2 exp(-2(k/4)^2) RANDu init",
+            "config": {"workload": workload_name(n),
                        "grid": n, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs > L2 (1.1 GB per field), no flush"},
             "grid_points_steps_per_s": value * n ** 3,
@@ -590,6 +692,8 @@ def main():
             "other_configs": configs,
             "cpu_baseline": cpu,
         }
+        # the figures a reader needs first, last on the line (a log tail keeps them)
+        line["summary"] = summarize(line)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

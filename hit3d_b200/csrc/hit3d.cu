@@ -14,7 +14,9 @@
 
 #include "../../include/hit3d_gpu.h"
 #include "particles.cuh"
+#include "ctx.cuh"
 #include "passes.cuh"
+#include "launch_cfg.cuh"
 #include "spectral.cuh"
 #include "fused_update.cuh"
 
@@ -36,206 +38,6 @@ int h3d_set_error_msg(int code, const char *msg)
     return code;
 }
 extern "C" const char *hit3d_gpu_last_error(void) { return g_err.c_str(); }
-
-// every launch site has the context `c` in scope and counts its kernels
-#define H3D_LAUNCH_CHECK()                 \
-    do {                                   \
-        c->nlaunch++;                      \
-        H3D_CHECK(cudaGetLastError());     \
-    } while (0)
-#define H3D_TRY(x)            \
-    do {                      \
-        int rc__ = (x);       \
-        if (rc__ != 0) return rc__; \
-    } while (0)
-
-// ---------------------------------------------------------------------------
-// launch configurations per transform length
-// ---------------------------------------------------------------------------
-H3D_HD constexpr int plan_rmax(int L)
-{
-    int r = 0;
-    for (int s = 0; s < plan_stages(L); s++) r = plan_radix_fwd(L, s) > r ? plan_radix_fwd(L, s) : r;
-    return r;
-}
-template <typename T, int L, bool YPASS = false> struct ColCfg {
-    // 128-byte rows of kx columns; the FP64 y passes at L = 1024 take 64-byte
-    // rows, so that a CTA's shared memory (TC x L elements) leaves room for two
-    // CTAs per SM (measured faster there, slower for the z passes and FP32)
-    static constexpr int TC = sizeof(T) == 8 ? ((L >= 1024 && YPASS) ? 4 : 8) : 16;
-    static constexpr int NT0 = TC * L / plan_rmax(L);
-    // one 8-element butterfly set per thread where 512 threads allow it; the
-    // FP64 y passes at L = 1024 keep 256 threads (measured faster there)
-    static constexpr int NTMAX = (sizeof(T) == 8 && L >= 1024 && YPASS) ? 256 : 512;
-    static constexpr int NT = NT0 > NTMAX ? NTMAX : NT0;
-    static constexpr size_t SMEM = (size_t)Lay<L, TC, false>::elems * sizeof(cx<T>);
-};
-template <typename T, int L> struct RowCfg {
-    static constexpr int TC = L >= 1024 ? 1 : 1024 / L;  // row pairs per CTA
-    static constexpr int NT = 128;
-    static constexpr size_t SMEM = (size_t)Lay<L, TC, true>::elems * sizeof(cx<T>);
-};
-// launch-shape variants of the fused x pass (picked by the tuner):
-//   0: 1024/L pairs x 128 threads   1: 2048/L pairs x 128 threads
-//   2: 1024/L pairs x  64 threads   3: 512/L pairs x 64 threads
-template <typename T, int L, int V> struct RowCfgV {
-    static constexpr int W = V == 1 ? 2048 : V == 3 ? 512 : 1024;
-    static constexpr int TC = L >= W ? 1 : W / L;
-    static constexpr int NT = (V >= 2) ? 64 : 128;
-    static constexpr size_t SMEM = (size_t)Lay<L, TC, true>::elems * sizeof(cx<T>);
-};
-//   4: register-resident kernel (k_xfused_reg), 1024/L pairs x 128 threads
-//   5, 6, 7: lockstep kernel (k_xfused_ms), forward transforms in groups of 3 / 2 / 1,
-//            the last with registers capped for 3 (FP64) or 4 (FP32) CTAs per SM
-//   8, 9, 10: staged lockstep kernel (k_xfused_st), the same three groupings,
-//            each CTA walking tiles with the next tile's input prefetched
-//   11: staged lockstep kernel, groups of 3, with 512/L row pairs (at least one)
-//       on 64 threads (128 from L = 1024), so that the CTAs of an SM pass their
-//       barriers independently
-//   12: as 11 with six CTAs per SM for FP32 (the register file holds 384
-//       threads at 168 registers), groups of 2 for FP64
-template <typename T, int L> struct RowCfgSmall {
-    static constexpr int TC = L >= 512 ? 1 : 512 / L;
-    static constexpr int NT = L >= 1024 ? 128 : 64;
-    static constexpr size_t SMEM = (size_t)Lay<L, TC, true>::elems * sizeof(cx<T>);
-};
-constexpr int kFusedVariants = HIT3D_FUSED_VARIANTS;
-
-// Raise a kernel's dynamic shared-memory limit once per kernel and device, so
-// that steps recorded into a CUDA graph later make no attribute calls.
-template <class K> static int set_smem(K kernel, size_t bytes)
-{
-    if (bytes <= 48 * 1024) return 0;
-    static std::mutex mu;
-    static std::set<std::pair<const void *, int>> done;
-    int dev = 0;
-    H3D_CHECK(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lk(mu);
-    auto key = std::make_pair((const void *)kernel, dev);
-    if (done.count(key)) return 0;
-    H3D_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    done.insert(key);
-    return 0;
-}
-
-#define H3D_DISPATCH(n, CALL)                          \
-    switch (n) {                                       \
-    case 32: return CALL(32);                          \
-    case 48: return CALL(48);                          \
-    case 64: return CALL(64);                          \
-    case 128: return CALL(128);                        \
-    case 256: return CALL(256);                        \
-    case 512: return CALL(512);                        \
-    case 1024: return CALL(1024);                      \
-    default: return h3d_set_error_msg(-3, "unsupported grid size"); \
-    }
-
-static bool size_supported(int n)
-{
-    return n == 32 || n == 48 || n == 64 || n == 128 || n == 256 || n == 512 || n == 1024;
-}
-
-// ---------------------------------------------------------------------------
-// context
-// ---------------------------------------------------------------------------
-// ---------------------------------------------------------------------------
-// RANDu on the host (RANDu.f:12-52), bit-exact with the reference: the
-// initial-condition stream stays on the host as the reference generates it.
-// ---------------------------------------------------------------------------
-namespace {
-struct Randu {
-    int64_t idum2 = 123456789, iy = 0, iv[32] = {0};
-    double next(double idum3)
-    {
-        const int64_t im1 = 2147483563, im2 = 2147483399, imm1 = im1 - 1;
-        const int64_t ia1 = 40014, ia2 = 40692, iq1 = 53668, iq2 = 52774;
-        const int64_t ir1 = 12211, ir2 = 3791, ntab = 32, ndiv = 1 + imm1 / ntab;
-        const double am = 1.0 / (double)im1, eps = 1.2e-7, rnmx = 1.0 - eps;
-        int64_t idum = (int64_t)llround(idum3 / 987.0), k, j;
-        if (idum <= 0) {
-            idum = (-idum > 1) ? -idum : 1;
-            idum2 = idum;
-            for (j = ntab + 8; j >= 1; j--) {
-                k = idum / iq1;
-                idum = ia1 * (idum - k * iq1) - k * ir1;
-                if (idum < 0) idum += im1;
-                if (j <= ntab) iv[j - 1] = idum;
-            }
-        }
-        k = idum / iq1;
-        idum = ia1 * (idum - k * iq1) - k * ir1;
-        if (idum < 0) idum += im1;
-        k = idum2 / iq2;
-        idum2 = ia2 * (idum2 - k * iq2) - k * ir2;
-        if (idum2 < 0) idum2 += im2;
-        j = 1 + iy / ndiv;
-        iy = iv[j - 1] - idum2;
-        iv[j - 1] = idum;
-        if (iy < 1) iy += imm1;
-        double r = am * (double)iy;
-        return r < rnmx ? r : rnmx;
-    }
-};
-}  // namespace
-
-struct hit3d_ctx {
-    hit3d_params p;
-    int n, nh, P64, P32, nsc, dev, kmax, nsm;
-    int64_t fs64, fs32;
-    cudaStream_t st;
-    double2 *U, *RO, *RP, *SP;
-    void *W;             // work fields in the transform precision
-    int nw;
-    int64_t wfs;         // complex elements per work field
-    int wpitch;
-    double2 *W64;        // FP64 scratch (3 fields) for statistics and the transform API
-    double2 *sgs;        // FP64 scratch (9 fields) of the subgrid-stress data path, on first use
-    double *phys;        // physical u,v,w [3][z][y][x] for particles
-    double2 *tw64;
-    float2 *tw32;
-    double *d_fen, *d_part, *d_red, *d_ratio;
-    unsigned long long *d_cmax;
-    double2 *stage;      // one field in the reference layout
-    double *d_xyz, *d_uvw;
-    int64_t np;
-    int pscheme;
-    int int_scalars;
-    double dx;
-    int pblocks;
-    int64_t nlaunch;
-    int xcfg;            // launch-shape variant of the fused x pass
-    int fuse_update;     // 1: z forward pass of the velocity products fused with the update
-    int idle_passive;    // passive scalars waiting for TSCALAR while LES fields move
-    Randu rng;           // RANDu state, carried from the velocity to the scalar initial
-                         // conditions as the reference's module state is (RANDu.f:20-22)
-    double k2max;        // truncation radius squared of PRE_TRUNC
-    void *mlp_wb;        // bf16 weights of the learned closure (les_model HIT3D_LES_LEARNED)
-    double mlp_delta;    // filter width the closure was trained for
-    int mlp_clip;        // zero the stress where its dissipation is negative
-    int mlp_kernel;      // 0: CUDA cores, 1: tensor cores for the hidden layers
-    int *d_mlp_err;      // set by the tensor-core kernel when a completion wait runs out
-    double *d_kmin;      // LES with k_sgs: minimum of k_sgs (slot 2), les.gp means, block sums
-    double2 *gfilt;      // test filter transfer function of the Dynamic Structure models
-    double2 *pfilt;      // particle filter transfer function (particles_filter_size > 0)
-    double2 *pbuf;       // 3 FP64 fields: the filtered velocity the particles see
-    const double2 *zfilt;  // filter of PRE_FILT when set (else gfilt)
-    int prune_on;        // allow 2/3-rule pruning of the step's transforms
-    int pruned;          // the state is zero beyond N/3 (checked), so pruning is exact
-    int alias_known;     // `pruned` is up to date with the state
-    int kc_active;       // >= 0 while a pruned step is being issued: the cutoff N/3
-};
-
-int h3d_mlp_apply(cudaStream_t st, int fp64, int64_t np, int64_t n, int64_t rp, int64_t fs, double delta, int clip,
-                  int kernel, const void *wb, void *G, int *err);
-
-static int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
-
-// ---------------------------------------------------------------------------
-// transform passes (templated on the compute precision T)
-// ---------------------------------------------------------------------------
-template <typename T> static const cx<T> *twid(const hit3d_ctx *c);
-template <> const double2 *twid<double>(const hit3d_ctx *c) { return c->tw64; }
-template <> const float2 *twid<float>(const hit3d_ctx *c) { return c->tw32; }
 
 // z pass reading the FP64 state with a spectral pre-operation, writing [z][ky][kx]
 template <typename T, int L, int MODE>
@@ -383,110 +185,9 @@ template <typename T> static int xr2c(hit3d_ctx *c, cx<T> *base, int64_t fs, int
 #undef CALL
 }
 
-template <typename T, template <class> class OP, int L, int V> static int xfused_LV(hit3d_ctx *c, FusedArgs a)
-{
-    using RC = RowCfgV<T, L, V>;
-    auto k = k_xfused<T, L, RC::TC, RC::NT, T, OP<T>>;
-    // transform buffer + the CTA's physical field; one cluster of NIN CTAs per tile
-    const size_t smem = 2 * RC::SMEM;
-    H3D_TRY(set_smem(k, smem));
-    const int tiles = (a.npairs + RC::TC - 1) / RC::TC;
-    k<<<dim3(tiles * OP<T>::NIN), RC::NT, smem, c->st>>>(a, twid<T>(c));
-    H3D_LAUNCH_CHECK();
-    return 0;
-}
-template <typename T, template <class> class OP, int L> static int xfused_reg_L(hit3d_ctx *c, FusedArgs a)
-{
-    using RC = RowCfg<T, L>;
-    auto k = k_xfused_reg<T, L, RC::TC, RC::NT, T, OP<T>>;
-    H3D_TRY(set_smem(k, RC::SMEM));
-    k<<<dim3((a.npairs + RC::TC - 1) / RC::TC), RC::NT, RC::SMEM, c->st>>>(a, twid<T>(c));
-    H3D_LAUNCH_CHECK();
-    return 0;
-}
-template <typename T, template <class> class OP, int L, int GF, int MINB = 1>
-static int xfused_ms_L(hit3d_ctx *c, FusedArgs a)
-{
-    using RC = RowCfg<T, L>;
-    constexpr int NB = OP<T>::NIN > GF ? OP<T>::NIN : GF;  // shared-memory buffers
-    auto k = k_xfused_ms<T, L, RC::TC, RC::NT, T, OP<T>, GF, MINB>;
-    H3D_TRY(set_smem(k, NB * RC::SMEM));
-    k<<<dim3((a.npairs + RC::TC - 1) / RC::TC), RC::NT, NB * RC::SMEM, c->st>>>(a, twid<T>(c));
-    H3D_LAUNCH_CHECK();
-    return 0;
-}
-// staged lockstep kernel: a grid of the CTAs that fit at once, each walking tiles
-// with the next tile's input rows prefetched into shared memory
-template <typename T, template <class> class OP, int L, int GF, int MINB, class RC = RowCfg<T, L>>
-static int xfused_st_L(hit3d_ctx *c, FusedArgs a)
-{
-    constexpr int NIN = OP<T>::NIN;
-    constexpr int NB = NIN > GF ? NIN : GF;
-    auto k = k_xfused_st<T, L, RC::TC, RC::NT, T, OP<T>, GF, MINB>;
-    for (int f = 0; f < NIN; f++)
-        if (reinterpret_cast<uintptr_t>(a.in[f]) % 16 != 0)
-            return h3d_set_error_msg(-1, "fused x pass: input field not 16-byte aligned");
-    if ((a.pitch * (int64_t)sizeof(cx<T>)) % 16 != 0)
-        return h3d_set_error_msg(-1, "fused x pass: row pitch not a multiple of 16 bytes");
-    auto stage_bytes = [&](int lim) {
-        return (size_t)NIN * 2 * RC::TC * StageRow<T>::chunks(lim) * StageRow<T>::PER * sizeof(cx<T>);
-    };
-    const int lim = a.kx_lim > 0 ? a.kx_lim : L / 2 + 1;
-    const size_t soff = (NB * RC::SMEM + 15) / 16 * 16;  // the stage starts on a 16-byte boundary
-    const size_t smax = soff + stage_bytes(L / 2 + 1), smem = soff + stage_bytes(lim);
-    H3D_TRY(set_smem(k, smax));
-    // CTAs per SM: the register cap of the kernel, or fewer if shared memory says so
-    // (233472 bytes per SM, 1 KB reserved per CTA)
-    int per_sm = (int)(233472 / (smem + 1024));
-    per_sm = per_sm < MINB ? per_sm : MINB;
-    if (per_sm < 1) return h3d_set_error_msg(-1, "fused x pass: stage does not fit in shared memory");
-    const int tiles = (a.npairs + RC::TC - 1) / RC::TC;
-    int grid = c->nsm * per_sm;
-    grid = grid < tiles ? grid : tiles;
-    k<<<dim3(grid), RC::NT, smem, c->st>>>(a, twid<T>(c));
-    H3D_LAUNCH_CHECK();
-    return 0;
-}
-template <typename T, template <class> class OP, int L> static int xfused_L(hit3d_ctx *c, FusedArgs a)
-{
-    if constexpr (OP<T>::NIN <= 3) {
-        if (c->xcfg == 8) return xfused_st_L<T, OP, L, 3, 2>(c, a);
-        if (c->xcfg == 9) return xfused_st_L<T, OP, L, 2, 2>(c, a);
-        if (c->xcfg == 10) return xfused_st_L<T, OP, L, 1, sizeof(T) == 4 ? 4 : 3>(c, a);
-        if (c->xcfg == 11) {
-            using RS = RowCfgSmall<T, L>;  // 256 threads per SM at the full register file
-            return xfused_st_L<T, OP, L, 3, 256 / RS::NT, RS>(c, a);
-        }
-        if (c->xcfg == 12) {
-            using RS = RowCfgSmall<T, L>;
-            if constexpr (sizeof(T) == 4) return xfused_st_L<T, OP, L, 3, 384 / RS::NT, RS>(c, a);  // 168 registers
-            else return xfused_st_L<T, OP, L, 2, 256 / RS::NT, RS>(c, a);
-        }
-        if (c->xcfg == 5) return xfused_ms_L<T, OP, L, 3>(c, a);
-        if (c->xcfg == 6) return xfused_ms_L<T, OP, L, 2>(c, a);
-        if (c->xcfg == 7) return xfused_ms_L<T, OP, L, 1, sizeof(T) == 4 ? 4 : 3>(c, a);
-    }
-    if (c->xcfg >= 4) return xfused_reg_L<T, OP, L>(c, a);
-    if constexpr (L >= 128) {
-        switch (c->xcfg) {
-        case 1: return xfused_LV<T, OP, L, 1>(c, a);
-        case 2: return xfused_LV<T, OP, L, 2>(c, a);
-        case 3: return xfused_LV<T, OP, L, 3>(c, a);
-        default: break;
-        }
-    }
-    return xfused_LV<T, OP, L, 0>(c, a);
-}
-template <typename T, template <class> class OP> static int xfused(hit3d_ctx *c, FusedArgs a)
-{
-    a.npairs = c->n * c->n / 2;
-    const double n3 = (double)c->n * c->n * c->n;
-    a.norm = 1.0 / n3;
-    a.kx_lim = c->kc_active >= 0 ? c->kc_active + 1 : 0;
-#define CALL(L) xfused_L<T, OP, L>(c, a)
-    H3D_DISPATCH(c->n, CALL)
-#undef CALL
-}
+// the fused x pass (xpass.cuh), instantiated in xpass_f64.cu and xpass_f32.cu
+template <typename T, template <class> class OP> int xfused(hit3d_ctx *c, FusedArgs a);
+constexpr int kFusedVariants = HIT3D_FUSED_VARIANTS;
 
 static dim3 pw_grid(const hit3d_ctx *c) { return dim3(c->nsm * 4); }
 // grid of a grid-stride kernel of 256-thread CTAs that may fit fewer than four
@@ -1384,6 +1085,21 @@ extern "C" int hit3d_gpu_step_profile(hit3d_ctx *c, int32_t nsteps, int32_t *fov
     return 0;
 }
 
+// a pair of timing events, destroyed on every exit path
+struct EventPair {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t create()
+    {
+        cudaError_t e = cudaEventCreate(&e0);
+        return e != cudaSuccess ? e : cudaEventCreate(&e1);
+    }
+    ~EventPair()
+    {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+};
+
 // time one fused x pass (velocity products) in the current variant; W is scratch
 template <typename T> static int time_fused(hit3d_ctx *c, float *ms)
 {
@@ -1394,17 +1110,14 @@ template <typename T> static int time_fused(hit3d_ctx *c, float *ms)
     for (int f = 0; f < 3; f++) fa.in[f] = W + f * c->wfs;
     for (int o = 0; o < 6; o++) fa.out[o] = W + o * c->wfs;
     fa.pitch = c->wpitch;
-    cudaEvent_t e0, e1;
-    H3D_CHECK(cudaEventCreate(&e0));
-    H3D_CHECK(cudaEventCreate(&e1));
+    EventPair ev;
+    H3D_CHECK(ev.create());
     H3D_TRY((xfused<T, OpVel>(c, fa)));  // warm-up
-    H3D_CHECK(cudaEventRecord(e0, c->st));
+    H3D_CHECK(cudaEventRecord(ev.e0, c->st));
     for (int r = 0; r < 3; r++) H3D_TRY((xfused<T, OpVel>(c, fa)));
-    H3D_CHECK(cudaEventRecord(e1, c->st));
-    H3D_CHECK(cudaEventSynchronize(e1));
-    H3D_CHECK(cudaEventElapsedTime(ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    H3D_CHECK(cudaEventRecord(ev.e1, c->st));
+    H3D_CHECK(cudaEventSynchronize(ev.e1));
+    H3D_CHECK(cudaEventElapsedTime(ms, ev.e0, ev.e1));
     return 0;
 }
 

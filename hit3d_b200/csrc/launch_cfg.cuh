@@ -1,0 +1,29 @@
+// Launch shapes of the transform passes per transform length, shared by every
+// translation unit that launches them (the context path and the allocation-free
+// entry point), so that both run the configurations the tests cover.
+#pragma once
+#include "fft.cuh"
+
+H3D_HD constexpr int plan_rmax(int L)
+{
+    int r = 0;
+    for (int s = 0; s < plan_stages(L); s++) r = plan_radix_fwd(L, s) > r ? plan_radix_fwd(L, s) : r;
+    return r;
+}
+template <typename T, int L, bool YPASS = false> struct ColCfg {
+    // 128-byte rows of kx columns; the FP64 y passes at L = 1024 take 64-byte
+    // rows, so that a CTA's shared memory (TC x L elements) leaves room for two
+    // CTAs per SM (measured faster there, slower for the z passes and FP32)
+    static constexpr int TC = sizeof(T) == 8 ? ((L >= 1024 && YPASS) ? 4 : 8) : 16;
+    static constexpr int NT0 = TC * L / plan_rmax(L);
+    // one 8-element butterfly set per thread where 512 threads allow it; the
+    // FP64 y passes at L = 1024 keep 256 threads (measured faster there)
+    static constexpr int NTMAX = (sizeof(T) == 8 && L >= 1024 && YPASS) ? 256 : 512;
+    static constexpr int NT = NT0 > NTMAX ? NTMAX : NT0;
+    static constexpr size_t SMEM = (size_t)Lay<L, TC, false>::elems * sizeof(cx<T>);
+};
+template <typename T, int L> struct RowCfg {
+    static constexpr int TC = L >= 1024 ? 1 : 1024 / L;  // row pairs per CTA
+    static constexpr int NT = 128;
+    static constexpr size_t SMEM = (size_t)Lay<L, TC, true>::elems * sizeof(cx<T>);
+};

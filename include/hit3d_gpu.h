@@ -227,15 +227,17 @@ int hit3d_gpu_xfft3d(hit3d_ctx *ctx, int32_t flag, const double *in, double *out
  * device memory is all handed out by its own pool allocator, or a loop that must
  * not risk the device-wide synchronisation of cudaMalloc/cudaFree).  No
  * counterpart in the reference.  `in` is a physical (nx+2, ny, nz) device array,
- * `out` receives the Fourier (nx+2, ny, nz) array; both belong to the caller,
- * must be 16-byte aligned and must not alias.  Work is queued on `stream`
- * (a cudaStream_t, NULL = default stream) and the caller synchronises.  Grid
- * sizes 32, 48, 64 and 128 only: the one scratch field lives in a file-scope
- * __device__ array (17 MB, held on every GPU that loads the library until the
- * process exits).  The first call on a device resolves that array's address and
- * uploads twiddle tables, so make it before any stream capture.  All calls share
- * the array: calls that overlap on the GPU race and must be serialised by the
- * caller. */
+ * `out` receives the Fourier (nx+2, ny, nz) array; both belong to the caller
+ * and must be 16-byte aligned.  They may be the same buffer (an in-place
+ * transform) or overlap: the whole input is copied into the scratch array before
+ * anything is written to `out`.  Work is queued on `stream` (a cudaStream_t,
+ * NULL = default stream) and the caller synchronises.  Grid sizes 32, 48, 64 and
+ * 128 only: the one scratch field lives in a file-scope __device__ array (17 MB,
+ * held on every GPU that loads the library until the process exits).  The first
+ * call in each CUDA context of a device (again after a device reset) resolves
+ * that array's address and uploads twiddle tables, so make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race and
+ * must be serialised by the caller. */
 int hit3d_gpu_xfft3d_static(int32_t n, const double *in, double *out, void *stream);
 
 /* Filter Fourier-space field `field` of the state in place

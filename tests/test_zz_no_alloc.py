@@ -45,6 +45,27 @@ def test_static_matches_context_transform_twice(n):
     g.close()
 
 
+@pytest.mark.parametrize("n", [32, 128])
+def test_static_in_place(n):
+    """Input and output the same device buffer: the whole input reaches the
+    scratch array before anything is written back."""
+    import torch
+    from hit3d_b200 import Context, Params, gpu
+    rng = np.random.default_rng(77 + n)
+    a = np.zeros((n, n, n + 2))
+    a[:, :, :n] = rng.standard_normal((n, n, n))
+    g = Context(Params(nx=n))
+    ref = g.xfft3d(1, a)
+    g.close()
+    d = torch.from_numpy(a).cuda()
+    torch.cuda.synchronize()
+    L = gpu.lib()
+    rc = L.hit3d_gpu_xfft3d_static(n, C.c_void_p(d.data_ptr()), C.c_void_p(d.data_ptr()), None)
+    assert rc == 0, L.hit3d_gpu_last_error().decode()
+    torch.cuda.synchronize()
+    assert relerr(d.cpu().numpy(), ref) < 1e-13
+
+
 def test_static_rejects_sizes_beyond_the_limit():
     from hit3d_b200 import gpu
     L = gpu.lib()
