@@ -117,7 +117,8 @@ struct hit3d_ctx {
     double2 *tw64;
     float2 *tw32;
     double *d_fen, *d_part, *d_red, *d_ratio;
-    unsigned long long *d_cmax;
+    unsigned long long *d_cmax;  // [0]: Courant maximum (bits of a double >= 0); [1]: the error word d_err
+    int *d_err;          // device error word: bit 1 = a fused x pass gave up waiting for its input stage
     double2 *stage;      // one field in the reference layout
     double *d_xyz, *d_uvw;
     int64_t np;

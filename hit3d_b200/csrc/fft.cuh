@@ -364,8 +364,10 @@ struct ColFFT {
     // buffer sm + f * LY::elems, all fields share one barrier per stage and one
     // twiddle load per butterfly.  Last-stage outputs are left in out[f][...].
     // The caller must __syncthreads() before reusing sm after this returns.
+    // stage 0 and the middle stages of NF transforms in lockstep; afterwards
+    // buffer f (sm + f * LY::elems) holds the input of transform f's last stage
     template <int NF>
-    static H3D_D void run_multi(cx<T> (&in)[NF][NIN], cx<T> *sm, cx<T> (&out)[NF][NOUT], const cx<T> *__restrict__ tw)
+    static H3D_D void run_multi_front(cx<T> (&in)[NF][NIN], cx<T> *sm, const cx<T> *__restrict__ tw)
     {
         constexpr int E = LY::elems;
         const int tid = threadIdx.x;
@@ -386,6 +388,14 @@ struct ColFFT {
         __syncthreads();
         if constexpr (S > 2) mid_multi<NF, 1>(sm, tw);
         if constexpr (S > 3) mid_multi<NF, 2>(sm, tw);
+    }
+
+    template <int NF>
+    static H3D_D void run_multi(cx<T> (&in)[NF][NIN], cx<T> *sm, cx<T> (&out)[NF][NOUT], const cx<T> *__restrict__ tw)
+    {
+        constexpr int E = LY::elems;
+        const int tid = threadIdx.x;
+        run_multi_front<NF>(in, sm, tw);
         constexpr int NsL = P::Ns(S - 1), nbpc = L / RL;
 #pragma unroll
         for (int i = 0; i < NBL; i++) {

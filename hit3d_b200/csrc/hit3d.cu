@@ -442,6 +442,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
             fa.in[0] = Wf(0); fa.in[1] = Wf(1); fa.in[2] = Wf(2); fa.in[3] = Wf(6 + 3 * s);
             fa.out[0] = Wf(6 + 3 * s); fa.out[1] = Wf(7 + 3 * s); fa.out[2] = Wf(8 + 3 * s);
             fa.pitch = wp;
+            fa.err = c->d_err;
             H3D_TRY((xfused<T, OpScal>(c, fa)));
         }
         {
@@ -450,6 +451,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
             for (int f = 0; f < 3; f++) fa.in[f] = Wf(f);
             for (int o = 0; o < 6; o++) fa.out[o] = Wf(o);
             fa.pitch = wp;
+            fa.err = c->d_err;
             if (pass == 0) fa.cmax = c->d_cmax;
             if (pass == 0 && c->np > 0) {
                 fa.phys = c->phys;
@@ -476,7 +478,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 pa.fs = 2 * c->fs64;
                 pa.rp = 2 * (int64_t)c->P64;
             }
-            k_particles<<<(unsigned)((c->np + 255) / 256), 256, 0, c->st>>>(pa);
+            k_particles<<<particle_blocks(c->np), 256, 0, c->st>>>(pa);
             H3D_LAUNCH_CHECK();
         }
         MARK(3);
@@ -857,7 +859,7 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
     c->pblocks = c->nsm * 2;
     const int kpart = c->kmax > 4 ? c->kmax : 4;
     if ((rc = ctx_alloc((void **)&c->tw64, sizeof(double2) * c->n)) || (rc = ctx_alloc((void **)&c->tw32, sizeof(float2) * c->n)) ||
-        (rc = ctx_alloc((void **)&c->d_fen, sizeof(double))) || (rc = ctx_alloc((void **)&c->d_cmax, sizeof(unsigned long long))) ||
+        (rc = ctx_alloc((void **)&c->d_fen, sizeof(double))) || (rc = ctx_alloc((void **)&c->d_cmax, 2 * sizeof(unsigned long long))) ||
         (rc = ctx_alloc((void **)&c->d_part, sizeof(double) * (size_t)c->pblocks * kpart)) ||
         (rc = ctx_alloc((void **)&c->d_red, sizeof(double) * (size_t)(kpart + 8))) ||
         (rc = ctx_alloc((void **)&c->d_ratio, sizeof(double) * (size_t)kpart)) ||
@@ -865,6 +867,8 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
         hit3d_gpu_finalize(c);
         return rc;
     }
+    c->d_err = reinterpret_cast<int *>(c->d_cmax + 1);
+    H3D_CHECK(cudaMemset(c->d_cmax, 0, 2 * sizeof(unsigned long long)));
     // twiddles exp(-2 pi i t/N), computed in long double and rounded once
     std::vector<double2> t64(c->n);
     std::vector<float2> t32(c->n);
@@ -1018,13 +1022,19 @@ extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_
         H3D_CHECK(cudaStreamSynchronize(c->st));
         if (herr) return h3d_set_error_msg(-5, "hit3d_gpu_step: a tensor-core completion wait of the closure ran out");
     }
-    if (courant && nsteps > 0) {
-        unsigned long long bits = 0;
-        H3D_CHECK(cudaMemcpyAsync(&bits, c->d_cmax, sizeof bits, cudaMemcpyDeviceToHost, c->st));
+    if (nsteps > 0) {
+        // the Courant maximum and the error word in one read
+        unsigned long long words[2] = {0, 0};
+        H3D_CHECK(cudaMemcpyAsync(words, c->d_cmax, sizeof words, cudaMemcpyDeviceToHost, c->st));
         H3D_CHECK(cudaStreamSynchronize(c->st));
-        double cm;
-        memcpy(&cm, &bits, sizeof cm);
-        *courant = cm * c->p.dt / c->dx;
+        int derr = 0;
+        memcpy(&derr, &words[1], sizeof derr);
+        if (derr) return h3d_set_error_msg(-5, "hit3d_gpu_step: a fused x pass gave up waiting for its input rows");
+        if (courant) {
+            double cm;
+            memcpy(&cm, &words[0], sizeof cm);
+            *courant = cm * c->p.dt / c->dx;
+        }
     }
     H3D_CHECK(cudaGetLastError());
     return 0;

@@ -345,6 +345,7 @@ struct FusedArgs {
     int64_t phys_fs, phys_pitch;
     double p0, p1;       // operator parameters
     int kx_lim;          // > 0: only kx < kx_lim is read and stored (2/3-rule pruning)
+    int *err;            // optional: set (bit 1) when a bounded wait on the input stage ran out
 };
 
 template <typename T, int L, int TC, int NT, typename TS, class OP>

@@ -5,6 +5,7 @@
 #include "ctx.cuh"
 #include "launch_cfg.cuh"
 #include "passes.cuh"
+#include "xfused2.cuh"
 
 // launch-shape variants of the fused x pass (picked by the tuner):
 //   0: 1024/L pairs x 128 threads   1: 2048/L pairs x 128 threads
@@ -25,6 +26,9 @@ template <typename T, int L, int V> struct RowCfgV {
 //       barriers independently
 //   12: as 11 with six CTAs per SM for FP32 (the register file holds 384
 //       threads at 168 registers), groups of 2 for FP64
+//   13: the launch shape of 12, forward transforms in groups of 2, input rows
+//       staged by bulk copies and the Hermitian split done in registers
+//       (k_xfused_v2)
 template <typename T, int L> struct RowCfgSmall {
     static constexpr int TC = L >= 512 ? 1 : 512 / L;
     static constexpr int NT = L >= 1024 ? 128 : 64;
@@ -97,9 +101,47 @@ static int xfused_st_L(hit3d_ctx *c, FusedArgs a)
     H3D_LAUNCH_CHECK();
     return 0;
 }
+// bulk-copy staged form with the split in registers (k_xfused_v2)
+template <typename T, template <class> class OP, int L, int MINB, class RC>
+static int xfused_v2_L(hit3d_ctx *c, FusedArgs a)
+{
+    constexpr int NIN = OP<T>::NIN;
+    constexpr int NB = NIN > 2 ? NIN : 2;
+    auto k = k_xfused_v2<T, L, RC::TC, RC::NT, T, OP<T>, MINB>;
+    for (int f = 0; f < NIN; f++)
+        if (reinterpret_cast<uintptr_t>(a.in[f]) % 16 != 0)
+            return h3d_set_error_msg(-1, "fused x pass: input field not 16-byte aligned");
+    if ((a.pitch * (int64_t)sizeof(cx<T>)) % 16 != 0)
+        return h3d_set_error_msg(-1, "fused x pass: row pitch not a multiple of 16 bytes");
+    const int lim = a.kx_lim > 0 ? a.kx_lim : L / 2 + 1;
+    // the copied rows are rounded up to 16 bytes and must stay inside the pitch
+    if ((int64_t)StageRow<T>::chunks(L / 2 + 1) * StageRow<T>::PER > a.pitch)
+        return h3d_set_error_msg(-1, "fused x pass: row pitch too small for the staged rows");
+    auto stage_bytes = [&](int l) {
+        return (size_t)NIN * 2 * RC::TC * StageRow<T>::chunks(l) * StageRow<T>::PER * sizeof(cx<T>);
+    };
+    const size_t soff = (NB * RC::SMEM + 15) / 16 * 16;
+    const size_t smax = soff + stage_bytes(L / 2 + 1) + 8, smem = soff + stage_bytes(lim) + 8;
+    H3D_TRY(set_smem(k, smax));
+    int per_sm = (int)(233472 / (smem + 1024));
+    per_sm = per_sm < MINB ? per_sm : MINB;
+    if (per_sm < 1) return h3d_set_error_msg(-1, "fused x pass: stage does not fit in shared memory");
+    const int tiles = (a.npairs + RC::TC - 1) / RC::TC;
+    int grid = c->nsm * per_sm;
+    grid = grid < tiles ? grid : tiles;
+    k<<<dim3(grid), RC::NT, smem, c->st>>>(a, twid<T>(c));
+    H3D_LAUNCH_CHECK();
+    return 0;
+}
+
 template <typename T, template <class> class OP, int L> static int xfused_L(hit3d_ctx *c, FusedArgs a)
 {
     if constexpr (OP<T>::NIN <= 3) {
+        if (c->xcfg == 13) {
+            using RS = RowCfgSmall<T, L>;
+            if constexpr (sizeof(T) == 4) return xfused_v2_L<T, OP, L, 384 / RS::NT, RS>(c, a);
+            else return xfused_v2_L<T, OP, L, 256 / RS::NT, RS>(c, a);
+        }
         if (c->xcfg == 8) return xfused_st_L<T, OP, L, 3, 2>(c, a);
         if (c->xcfg == 9) return xfused_st_L<T, OP, L, 2, 2>(c, a);
         if (c->xcfg == 10) return xfused_st_L<T, OP, L, 1, sizeof(T) == 4 ? 4 : 3>(c, a);

@@ -22,7 +22,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libhit3d_gpu.so")
 MAX_SCALARS = 8
 LES_LEARNED = 20  # les_model of the learned closure (HIT3D_LES_LEARNED)
-N_VARIANTS = 13  # launch-shape variants of the fused x pass (HIT3D_FUSED_VARIANTS)
+N_VARIANTS = 14  # launch-shape variants of the fused x pass (HIT3D_FUSED_VARIANTS)
 
 
 def les_fields(les_model: int) -> int:

@@ -128,7 +128,7 @@ int hit3d_gpu_step_profile(hit3d_ctx *ctx, int32_t nsteps, int32_t *fov, int32_t
  * *variant receives the choice, ms[0..HIT3D_FUSED_VARIANTS) the time of each
  * variant (unused entries are left untouched).
  * hit3d_gpu_set_variant fixes a variant by hand. */
-#define HIT3D_FUSED_VARIANTS 13
+#define HIT3D_FUSED_VARIANTS 14
 int hit3d_gpu_autotune(hit3d_ctx *ctx, int32_t *variant, double *ms);
 int hit3d_gpu_set_variant(hit3d_ctx *ctx, int32_t variant);
 

@@ -35,13 +35,14 @@ def test_variants_agree(n, precision, case):
 
 @pytest.mark.parametrize("precision", [0, 1])
 def test_one_pair_variants_at_512(precision):
-    """At L = 512 variants 11 and 12 take one row pair per CTA (the stage and
-    split loops without index division); they agree with variant 8 (two pairs
-    per CTA) over two forced steps."""
+    """At L = 512 variants 11, 12 and 13 take one row pair per CTA (the stage
+    and split loops without index division; 13 with bulk-copy staging and the
+    split in registers); they agree with variant 8 (two pairs per CTA) over two
+    forced steps."""
     from hit3d_b200 import Context, Params
     kw = dict(nx=512, flow_type=1, kfmax=2, nu=1.0 / 3000.0, dt=2e-4, precision=precision)
     outs = {}
-    for v in (8, 11, 12):
+    for v in (8, 11, 12, 13):
         c = Context(Params(**kw))
         c.set_variant(v)
         c.init_velocity(RN1, 2, 4.0, 2.0)
@@ -50,7 +51,7 @@ def test_one_pair_variants_at_512(precision):
         outs[v] = c.download_fields()
         c.close()
     tol = 1e-13 if precision == 0 else 1e-6
-    for v in (11, 12):
+    for v in (11, 12, 13):
         assert relerr(outs[v], outs[8]) < tol, (v, relerr(outs[v], outs[8]))
 
 
