@@ -389,6 +389,7 @@ def configs_leg(torch, args, device, only=None):
         ps = batched_runs()
         b = Batch(ps)
         b.init()
+        picks = b.autotune()
         # first-order step, then one chunk through the graph, so that the timed
         # region replays a graph recorded beforehand
         b.step(1 + 10, graph_steps=10)
@@ -401,6 +402,9 @@ def configs_leg(torch, args, device, only=None):
         pts = sum(p.nx ** 3 for p in ps)
         out["batched_96"] = {"workload": "96 forced runs: 32 x 32^3, 32 x 48^3, 28 x 64^3, 4 x 128^3, one recorded graph",
                              "run_steps_per_s": len(ps) * 50 / t, "grid_points_steps_per_s": pts * 50 / t,
+                             "size_classes": b.nclasses,
+                             "tuned": [{"variant": v, "tile": tl, "x_ms": [round(x, 4) for x in mv],
+                                        "columns_ms": [round(x, 4) for x in mt]} for v, tl, mv, mt in picks],
                              "graph_launches": b.graph_launches, "timing": "host clock around 50 steps (5 graph launches)"}
         b.close()
 

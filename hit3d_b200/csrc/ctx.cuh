@@ -147,6 +147,13 @@ struct hit3d_ctx {
     int pruned;          // the state is zero beyond N/3 (checked), so pruning is exact
     int alias_known;     // `pruned` is up to date with the state
     int kc_active;       // >= 0 while a pruned step is being issued: the cutoff N/3
+    int ext_bufs;        // U, RO and W belong to a batch's slab
+    int ctile;           // column-tile shape of the plain strided passes (ColCfgT), grids up to 128
+    // while a batch class is being stepped through this context (its first
+    // run): the number of runs, and the run strides of the state (complex FP64
+    // elements) and of the work fields (elements of the transform precision)
+    int bruns;
+    int64_t bru, brw;
 };
 
 int h3d_mlp_apply(cudaStream_t st, int fp64, int64_t np, int64_t n, int64_t rp, int64_t fs, double delta, int clip,

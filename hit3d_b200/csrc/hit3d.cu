@@ -40,11 +40,11 @@ int h3d_set_error_msg(int code, const char *msg)
 extern "C" const char *hit3d_gpu_last_error(void) { return g_err.c_str(); }
 
 // z pass reading the FP64 state with a spectral pre-operation, writing [z][ky][kx]
-template <typename T, int L, int MODE>
-static int zinv_LM(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_t src_fs, cx<T> *dst,
-                   int64_t dst_fs, int dpitch)
+template <typename T, int L, int MODE, int CT>
+static int zinv_LMC(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_t src_fs, cx<T> *dst,
+                    int64_t dst_fs, int dpitch)
 {
-    using CF = ColCfg<T, L>;
+    using CF = ColCfgT<T, L, false, CT>;
     using IO = IOSpec<T, T, MODE>;
     IO io;
     io.src = src; io.dst = dst; io.fs_src = src_fs; io.fs_dst = dst_fs;
@@ -58,12 +58,30 @@ static int zinv_LM(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_t
         io.ncol = c->kc_active + 1;
         rows = 2 * c->kc_active + 1;
     }
+    int nz = nf;
+    if (c->bruns > 1) {  // every run of a batch class: state run stride bru, work run stride brw
+        io.nfr = nf;
+        io.rs_src = c->bru;
+        io.rs_dst = c->brw;
+        nz = nf * c->bruns;
+    }
     auto k = k_colfft<T, L, CF::TC, CF::NT, false, IO>;
     H3D_TRY(set_smem(k, CF::SMEM));
-    dim3 g((io.ncol + CF::TC - 1) / CF::TC, rows, nf);
+    dim3 g((io.ncol + CF::TC - 1) / CF::TC, rows, nz);
     k<<<g, CF::NT, CF::SMEM, c->st>>>(io, twid<T>(c));
     H3D_LAUNCH_CHECK();
     return 0;
+}
+// the tuned column tile (ctile) applies to the plain copy of grids up to 128
+template <typename T, int L, int MODE>
+static int zinv_LM(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_t src_fs, cx<T> *dst,
+                   int64_t dst_fs, int dpitch)
+{
+    if constexpr (L <= 128 && MODE == PRE_COPY) {
+        if (c->ctile == 1) return zinv_LMC<T, L, MODE, 1>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+        if (c->ctile == 2) return zinv_LMC<T, L, MODE, 2>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
+    }
+    return zinv_LMC<T, L, MODE, 0>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
 }
 template <typename T, int L>
 static int zinv_L(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src, int64_t src_fs, cx<T> *dst,
@@ -101,10 +119,10 @@ static int zinv(hit3d_ctx *c, int nf, int mode, int sfield, const double2 *src, 
 }
 
 // in-place strided pass: axis 1 = y (stride pitch, outer z), axis 2 = z (stride n*pitch, outer ky)
-template <typename T, int L, bool YPASS>
-static int spass_LA(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, int pitch, int nf)
+template <typename T, int L, bool YPASS, int CT>
+static int spass_LAC(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, int pitch, int nf)
 {
-    using CF = ColCfg<T, L, YPASS>;
+    using CF = ColCfgT<T, L, YPASS, CT>;
     IOPlain<T, T, T> io;
     io.src = base; io.dst = base; io.fs_src = fs; io.fs_dst = fs; io.ncol = c->nh;
     if (axis == 1) { io.sa_src = io.sa_dst = pitch; io.so_src = io.so_dst = (int64_t)c->n * pitch; }
@@ -122,7 +140,13 @@ static int spass_LA(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, i
             rows = 2 * c->kc_active + 1;
         }
     }
-    dim3 g((io.ncol + CF::TC - 1) / CF::TC, rows, nf);
+    int nz = nf;
+    if (c->bruns > 1) {  // every run of a batch class (work fields, run stride brw)
+        io.nfr = nf;
+        io.rs_src = io.rs_dst = c->brw;
+        nz = nf * c->bruns;
+    }
+    dim3 g((io.ncol + CF::TC - 1) / CF::TC, rows, nz);
     if (fwd) {
         auto k = k_colfft<T, L, CF::TC, CF::NT, true, IOPlain<T, T, T>>;
         H3D_TRY(set_smem(k, CF::SMEM));
@@ -134,6 +158,15 @@ static int spass_LA(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, i
     }
     H3D_LAUNCH_CHECK();
     return 0;
+}
+template <typename T, int L, bool YPASS>
+static int spass_LA(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, int pitch, int nf)
+{
+    if constexpr (L <= 128) {
+        if (c->ctile == 1) return spass_LAC<T, L, YPASS, 1>(c, axis, fwd, base, fs, pitch, nf);
+        if (c->ctile == 2) return spass_LAC<T, L, YPASS, 2>(c, axis, fwd, base, fs, pitch, nf);
+    }
+    return spass_LAC<T, L, YPASS, 0>(c, axis, fwd, base, fs, pitch, nf);
 }
 template <typename T, int L>
 static int spass_L(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, int pitch, int nf)
@@ -757,7 +790,17 @@ static int ctx_alloc(void **p, size_t bytes)
     return 0;
 }
 
+// Context set-up.  ext_U/ext_RO/ext_W (all three or none): state, AB2 history
+// and work fields borrowed from a batch's slab instead of allocated here (the
+// context does not free them).
+static int ctx_init(const hit3d_params *p, hit3d_ctx **out, double2 *ext_U, double2 *ext_RO, void *ext_W);
+
 extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
+{
+    return ctx_init(p, out, nullptr, nullptr, nullptr);
+}
+
+static int ctx_init(const hit3d_params *p, hit3d_ctx **out, double2 *ext_U, double2 *ext_RO, void *ext_W)
 {
     if (!p || !out) return h3d_set_error_msg(-1, "hit3d_gpu_init: null argument");
     *out = nullptr;
@@ -843,8 +886,13 @@ extern "C" int hit3d_gpu_init(const hit3d_params *p, hit3d_ctx **out)
         c->wfs = c->fs32;
     }
     const size_t wbytes = (size_t)c->nw * c->wfs * (c->p.precision == 0 ? sizeof(double2) : sizeof(float2));
-    if ((rc = ctx_alloc((void **)&c->U, f64 * nf)) || (rc = ctx_alloc((void **)&c->RO, f64 * nf)) ||
-        (rc = ctx_alloc(&c->W, wbytes))) {
+    if (ext_U) {
+        c->U = ext_U;
+        c->RO = ext_RO;
+        c->W = ext_W;
+        c->ext_bufs = 1;
+    } else if ((rc = ctx_alloc((void **)&c->U, f64 * nf)) || (rc = ctx_alloc((void **)&c->RO, f64 * nf)) ||
+               (rc = ctx_alloc(&c->W, wbytes))) {
         hit3d_gpu_finalize(c);
         return rc;
     }
@@ -933,6 +981,7 @@ extern "C" void hit3d_gpu_finalize(hit3d_ctx *c)
     cudaSetDevice(c->dev);
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->W64 && c->W64 != c->W) cudaFree(c->W64);
+    if (c->ext_bufs) c->U = c->RO = nullptr, c->W = nullptr;  // a batch's slab
     void *ptrs[] = {c->U, c->RO, c->RP, c->SP, c->W, c->phys, c->tw64, c->tw32, c->d_fen, c->d_part,
                     c->d_red, c->d_ratio, c->d_cmax, c->stage, c->d_xyz, c->d_uvw, c->sgs, c->mlp_wb,
                     c->d_mlp_err, c->d_kmin, c->gfilt, c->pfilt, c->pbuf};
@@ -1819,9 +1868,28 @@ extern "C" int hit3d_gpu_physical_velocity(hit3d_ctx *c, double *out, int64_t ld
 // branch per run on its own stream, forked from and joined back into a root
 // stream -- and replayed with a single launch per chunk.
 // ---------------------------------------------------------------------------
+// Runs of a batch that share a grid size, precision and forcing (velocity only,
+// 2/3 rule, no LES) form a class: their state, AB2 history and work fields sit
+// in one slab (run r at a fixed run stride), and every pass of a step is ONE
+// launch over all the class's runs (the run index folded into the grid), with
+// each run's viscosity, time step and forcing-band energy in small device
+// tables.  Other runs step on their own.
+constexpr int kBatchVariants = 7;  // fused x-pass variants 8-14 walk the tiles of several runs
+
+struct BatchClass {
+    std::vector<int> runs;
+    double2 *U = nullptr, *RO = nullptr;
+    void *W = nullptr;
+    int64_t ru = 0, rw = 0;  // run strides: state (complex FP64 elements), work fields (transform precision)
+    double *tab = nullptr;   // [nu | dt | forcing energy] x runs
+    std::vector<double> tab_nu, tab_dt;  // the values uploaded
+};
+
 struct hit3d_batch {
     std::vector<hit3d_ctx *> runs;
     std::vector<int> fov, fos;
+    std::vector<int> run_class;  // class of each run, -1: stepped on its own
+    std::vector<BatchClass> classes;
     int dev = 0;
     cudaStream_t root = nullptr;
     cudaEvent_t fork = nullptr;
@@ -1839,6 +1907,201 @@ static int run_step(hit3d_ctx *c, int ev, int es)
     return c->p.precision == 0 ? step_once<double>(c, ev, es) : step_once<float>(c, ev, es);
 }
 
+// runs that can join a class, and the key of the class
+static bool class_eligible(const hit3d_params &p)
+{
+    return p.les_model == 0 && p.n_scalars == 0 && p.dealias == 0;
+}
+static bool same_class(const hit3d_params &a, const hit3d_params &b)
+{
+    return a.nx == b.nx && a.precision == b.precision && a.flow_type == b.flow_type &&
+           (a.flow_type == 0 || (a.kfmax == b.kfmax && a.famp == b.famp));
+}
+
+// upload the class's per-run viscosity and time step when they changed
+static int class_tables(hit3d_batch *b, BatchClass &k)
+{
+    const size_t nr = k.runs.size();
+    std::vector<double> nu(nr), dt(nr);
+    for (size_t i = 0; i < nr; i++) {
+        nu[i] = b->runs[k.runs[i]]->p.nu;
+        dt[i] = b->runs[k.runs[i]]->p.dt;
+    }
+    if (nu == k.tab_nu && dt == k.tab_dt) return 0;
+    hit3d_ctx *c = b->runs[k.runs[0]];
+    H3D_CHECK(cudaMemcpyAsync(k.tab, nu.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, c->st));
+    H3D_CHECK(cudaMemcpyAsync(k.tab + nr, dt.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, c->st));
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    k.tab_nu = nu;
+    k.tab_dt = dt;
+    return 0;
+}
+
+// every run of the class pruned (state zero beyond N/3): the pruned transforms
+static bool class_pruned(hit3d_batch *b, const BatchClass &k)
+{
+    for (int r : k.runs)
+        if (!(b->runs[r]->prune_on && b->runs[r]->pruned)) return false;
+    return true;
+}
+
+// one step of every run of a class, issued on its first run's stream: forcing
+// energy, z and y inverse, fused x pass, y and z forward and the update, each
+// one launch over the class (main.f90:124-167 for every run)
+// the class fields of the first run's context while a class is issued, reset
+// on every exit path
+struct ClassScope {
+    hit3d_ctx *c;
+    ClassScope(hit3d_batch *b, BatchClass &k) : c(b->runs[k.runs[0]])
+    {
+        c->bruns = (int)k.runs.size();
+        c->bru = k.ru;
+        c->brw = k.rw;
+        c->kc_active = (c->prune_on && class_pruned(b, k)) ? c->n / 3 : -1;
+    }
+    ~ClassScope()
+    {
+        c->bruns = 0;
+        c->bru = c->brw = 0;
+        c->kc_active = -1;
+    }
+};
+
+template <typename T> static int class_step(hit3d_batch *b, BatchClass &k, int euler)
+{
+    hit3d_ctx *c = b->runs[k.runs[0]];
+    const int nr = (int)k.runs.size();
+    const hit3d_params &p = c->p;
+    ClassScope scope(b, k);
+    cx<T> *W = reinterpret_cast<cx<T> *>(c->W);
+    const int64_t wfs = c->wfs;
+    const int wp = c->wpitch;
+    auto Wf = [&](int i) { return W + i * wfs; };
+    double *fen = k.tab + 2 * nr;
+    if (p.flow_type == 1) {
+        k_forcing_energy<<<nr, 32, 0, c->st>>>(c->n, c->P64, c->fs64, p.kfmax, c->U, fen, k.ru);
+        H3D_LAUNCH_CHECK();
+    }
+    H3D_TRY(zinv<T>(c, 3, PRE_COPY, 0, c->U, c->fs64, Wf(0), wfs, wp));
+    H3D_TRY(spass<T>(c, 1, false, Wf(0), wfs, wp, 3));
+    {
+        FusedArgs fa;
+        memset(&fa, 0, sizeof fa);
+        for (int f = 0; f < 3; f++) fa.in[f] = Wf(f);
+        for (int o = 0; o < 6; o++) fa.out[o] = Wf(o);
+        fa.pitch = wp;
+        fa.err = c->d_err;
+        H3D_TRY((xfused<T, OpVel>(c, fa)));
+    }
+    H3D_TRY(spass<T>(c, 1, true, Wf(0), wfs, wp, 6));
+    H3D_TRY(spass<T>(c, 2, true, Wf(0), wfs, wp, 6));
+    StepArgs a;
+    memset(&a, 0, sizeof a);
+    a.n = c->n; a.nh = c->nh; a.pitch = c->P64; a.ppitch = wp; a.fs = c->fs64; a.pfs = wfs;
+    a.nu = p.nu; a.dt = p.dt; a.euler_v = euler; a.euler_s = euler;
+    a.flow_type = p.flow_type; a.kfmax = p.kfmax; a.famp = p.famp; a.fenergy = fen;
+    a.kc = c->kc_active;
+    a.ru = k.ru; a.rp = k.rw; a.nu_r = k.tab; a.dt_r = k.tab + nr;
+    // CTAs per run: enough for the run's modes, at most one resident wave in all
+    const int64_t nm = (int64_t)(c->kc_active >= 0 ? (int64_t)(c->kc_active + 1) * (2 * c->kc_active + 1) *
+                                                         (2 * c->kc_active + 1)
+                                                   : (int64_t)c->n * c->n * c->nh);
+    int64_t gx = (nm + 255) / 256;
+    const int64_t wave = (int64_t)pw_grid(c, k_update_vel_23<T>).x;
+    const int64_t cap = wave / nr > 1 ? wave / nr : 1;
+    gx = gx < cap ? gx : cap;
+    k_update_vel_23<T><<<dim3((unsigned)gx, (unsigned)nr), 256, 0, c->st>>>(a, Wf(0), nullptr, c->U, c->RO);
+    H3D_LAUNCH_CHECK();
+    return 0;
+}
+static int class_step_any(hit3d_batch *b, BatchClass &k, int euler)
+{
+    return b->runs[k.runs[0]]->p.precision == 0 ? class_step<double>(b, k, euler) : class_step<float>(b, k, euler);
+}
+
+// the passes of a class step that the tuner's choices affect, on scratch work
+// fields only (the state is read, never written): what 0 = the fused x pass,
+// 1 = the strided passes (z and y inverse, y and z forward)
+template <typename T> static int class_passes(hit3d_batch *b, BatchClass &k, int what)
+{
+    hit3d_ctx *c = b->runs[k.runs[0]];
+    ClassScope scope(b, k);
+    cx<T> *W = reinterpret_cast<cx<T> *>(c->W);
+    const int64_t wfs = c->wfs;
+    const int wp = c->wpitch;
+    if (what == 0) {
+        FusedArgs fa;
+        memset(&fa, 0, sizeof fa);
+        for (int f = 0; f < 3; f++) fa.in[f] = W + f * wfs;
+        for (int o = 0; o < 6; o++) fa.out[o] = W + o * wfs;
+        fa.pitch = wp;
+        fa.err = c->d_err;
+        return xfused<T, OpVel>(c, fa);
+    }
+    H3D_TRY(zinv<T>(c, 3, PRE_COPY, 0, c->U, c->fs64, W, wfs, wp));
+    H3D_TRY(spass<T>(c, 1, false, W, wfs, wp, 3));
+    H3D_TRY(spass<T>(c, 1, true, W, wfs, wp, 6));
+    H3D_TRY(spass<T>(c, 2, true, W, wfs, wp, 6));
+    return 0;
+}
+static int class_time(hit3d_batch *b, BatchClass &k, int what, float *ms)
+{
+    hit3d_ctx *c = b->runs[k.runs[0]];
+    auto go = [&]() { return c->p.precision == 0 ? class_passes<double>(b, k, what) : class_passes<float>(b, k, what); };
+    EventPair ev;
+    H3D_CHECK(ev.create());
+    H3D_TRY(go());  // warm-up
+    H3D_CHECK(cudaEventRecord(ev.e0, c->st));
+    for (int r = 0; r < 3; r++) H3D_TRY(go());
+    H3D_CHECK(cudaEventRecord(ev.e1, c->st));
+    H3D_CHECK(cudaEventSynchronize(ev.e1));
+    H3D_CHECK(cudaEventElapsedTime(ms, ev.e0, ev.e1));
+    *ms /= 3.0f;
+    return 0;
+}
+
+extern "C" int hit3d_batch_nclasses(hit3d_batch *b) { return b ? (int)b->classes.size() : -1; }
+
+extern "C" int hit3d_batch_autotune(hit3d_batch *b, int32_t *choice, double *ms)
+{
+    if (!b) return h3d_set_error_msg(-1, "hit3d_batch_autotune: null batch");
+    H3D_CHECK(cudaSetDevice(b->dev));
+    for (hit3d_ctx *cr : b->runs) H3D_TRY(ensure_alias_state(cr));
+    for (size_t q = 0; q < b->classes.size(); q++) {
+        BatchClass &k = b->classes[q];
+        hit3d_ctx *c = b->runs[k.runs[0]];
+        double *mq = ms ? ms + q * (kBatchVariants + kColTiles) : nullptr;
+        int bv = 13;
+        float bt = 1e30f;
+        for (int v = 0; v < kBatchVariants; v++) {
+            c->xcfg = 8 + v;
+            float t = 0.f;
+            H3D_TRY(class_time(b, k, 0, &t));
+            if (mq) mq[v] = t;
+            if (t < bt) { bt = t; bv = 8 + v; }
+        }
+        c->xcfg = bv;
+        int bc = 0;
+        bt = 1e30f;
+        if (mq)
+            for (int ct = 0; ct < kColTiles; ct++) mq[kBatchVariants + ct] = 0.0;
+        for (int ct = 0; ct < (c->n <= 128 ? kColTiles : 1); ct++) {
+            c->ctile = ct;
+            float t = 0.f;
+            H3D_TRY(class_time(b, k, 1, &t));
+            if (mq) mq[kBatchVariants + ct] = t;
+            if (t < bt) { bt = t; bc = ct; }
+        }
+        c->ctile = bc;
+        if (choice) { choice[2 * q] = bv; choice[2 * q + 1] = bc; }
+    }
+    // the recorded graph holds the old launch shapes
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    for (hit3d_ctx *cr : b->runs) H3D_CHECK(cudaStreamSynchronize(cr->st));
+    return 0;
+}
+
 extern "C" void hit3d_batch_destroy(hit3d_batch *b)
 {
     if (!b) return;
@@ -1850,6 +2113,12 @@ extern "C" void hit3d_batch_destroy(hit3d_batch *b)
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->root) cudaStreamDestroy(b->root);
     for (hit3d_ctx *c : b->runs) hit3d_gpu_finalize(c);
+    for (BatchClass &k : b->classes) {
+        if (k.U) cudaFree(k.U);
+        if (k.RO) cudaFree(k.RO);
+        if (k.W) cudaFree(k.W);
+        if (k.tab) cudaFree(k.tab);
+    }
     delete b;
 }
 
@@ -1859,24 +2128,63 @@ extern "C" int hit3d_batch_create(const hit3d_params *p, int32_t nruns, hit3d_ba
     *out = nullptr;
     for (int r = 1; r < nruns; r++)
         if (p[r].device != p[0].device) return h3d_set_error_msg(-1, "hit3d_batch_create: all runs must share one device");
+    H3D_CHECK(cudaSetDevice(p[0].device));
     hit3d_batch *b = new hit3d_batch();
     b->dev = p[0].device;
+    b->run_class.assign(nruns, -1);
+    // classes, in order of their first run
     for (int r = 0; r < nruns; r++) {
+        if (!class_eligible(p[r]) || b->run_class[r] >= 0) continue;
+        BatchClass k;
+        for (int q = r; q < nruns; q++)
+            if (b->run_class[q] < 0 && class_eligible(p[q]) && same_class(p[r], p[q])) {
+                b->run_class[q] = (int)b->classes.size();
+                k.runs.push_back(q);
+            }
+        b->classes.push_back(k);
+    }
+    b->runs.assign(nruns, nullptr);
+    auto fail = [&](int rc) {
+        hit3d_batch_destroy(b);
+        return rc;
+    };
+    for (BatchClass &k : b->classes) {
+        const hit3d_params &q = p[k.runs[0]];
+        const int64_t nh = q.nx / 2 + 1, fs64 = (int64_t)q.nx * q.nx * round_up(nh, 8);
+        const int64_t wfs = q.precision == 0 ? fs64 : (int64_t)q.nx * q.nx * round_up(nh, 16);
+        const size_t welem = q.precision == 0 ? sizeof(double2) : sizeof(float2);
+        const int nr = (int)k.runs.size();
+        k.ru = 3 * fs64;
+        k.rw = 6 * wfs;
+        int rc = 0;
+        if ((rc = ctx_alloc((void **)&k.U, sizeof(double2) * (size_t)(k.ru * nr))) ||
+            (rc = ctx_alloc((void **)&k.RO, sizeof(double2) * (size_t)(k.ru * nr))) ||
+            (rc = ctx_alloc(&k.W, welem * (size_t)(k.rw * nr))) ||
+            (rc = ctx_alloc((void **)&k.tab, sizeof(double) * 3 * (size_t)nr)))
+            return fail(rc);
+        for (int i = 0; i < nr; i++) {
+            hit3d_ctx *c = nullptr;
+            rc = ctx_init(&p[k.runs[i]], &c, k.U + i * k.ru, k.RO + i * k.ru,
+                          static_cast<unsigned char *>(k.W) + welem * (size_t)(i * k.rw));
+            if (rc) return fail(rc);
+            b->runs[k.runs[i]] = c;
+            if (c->nw != 6) return fail(h3d_set_error_msg(-1, "hit3d_batch_create: class work fields mismatch"));
+        }
+    }
+    for (int r = 0; r < nruns; r++) {
+        if (b->runs[r]) continue;
         hit3d_ctx *c = nullptr;
         int rc = hit3d_gpu_init(&p[r], &c);
-        if (rc) { hit3d_batch_destroy(b); return rc; }
-        b->runs.push_back(c);
-        b->fov.push_back(1);
-        b->fos.push_back(1);
+        if (rc) return fail(rc);
+        b->runs[r] = c;
     }
+    b->fov.assign(nruns, 1);
+    b->fos.assign(nruns, 1);
     cudaError_t e = cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     b->join.resize(nruns, nullptr);
     for (int r = 0; r < nruns && e == cudaSuccess; r++) e = cudaEventCreateWithFlags(&b->join[r], cudaEventDisableTiming);
-    if (e != cudaSuccess) {
-        hit3d_batch_destroy(b);
-        return h3d_set_error(e, "hit3d_batch_create", __FILE__, __LINE__);
-    }
+    if (e != cudaSuccess) return fail(h3d_set_error(e, "hit3d_batch_create", __FILE__, __LINE__));
     *out = b;
     return 0;
 }
@@ -1888,21 +2196,39 @@ extern "C" int hit3d_batch_context(hit3d_batch *b, int32_t r, hit3d_ctx **ctx)
     return 0;
 }
 
+// the issuing stream of each unit of work: a class's first run, or a lone run
+static std::vector<int> batch_units(hit3d_batch *b)
+{
+    std::vector<int> u;
+    for (BatchClass &k : b->classes) u.push_back(k.runs[0]);
+    for (size_t r = 0; r < b->runs.size(); r++)
+        if (b->run_class[r] < 0) u.push_back((int)r);
+    return u;
+}
+
+// one Adams-Bashforth step of every run (classes batched), on the units' streams
+static int batch_issue(hit3d_batch *b)
+{
+    for (BatchClass &k : b->classes) H3D_TRY(class_step_any(b, k, 0));
+    for (size_t r = 0; r < b->runs.size(); r++)
+        if (b->run_class[r] < 0) H3D_TRY(run_step(b->runs[r], 0, 0));
+    return 0;
+}
+
 // record `steps` Adams-Bashforth steps of every run into one graph
 static int batch_capture(hit3d_batch *b, int steps)
 {
     if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
     if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
-    hit3d_ctx *c = b->runs[0];  // for the error macros
+    const std::vector<int> units = batch_units(b);
     H3D_CHECK(cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal));
     int rc = 0;
     for (int s = 0; s < steps && rc == 0; s++) {
         cudaEventRecord(b->fork, b->root);
-        for (size_t r = 0; r < b->runs.size() && rc == 0; r++) {
-            hit3d_ctx *cr = b->runs[r];
-            cudaStreamWaitEvent(cr->st, b->fork, 0);
-            rc = run_step(cr, 0, 0);
-            cudaEventRecord(b->join[r], cr->st);
+        for (int r : units) cudaStreamWaitEvent(b->runs[r]->st, b->fork, 0);
+        rc = batch_issue(b);
+        for (int r : units) {
+            cudaEventRecord(b->join[r], b->runs[r]->st);
             cudaStreamWaitEvent(b->root, b->join[r], 0);
         }
     }
@@ -1921,7 +2247,6 @@ static int batch_capture(hit3d_batch *b, int steps)
         b->cap_scal.push_back(cr->int_scalars);
         b->cap_prune.push_back(cr->prune_on && cr->pruned);
     }
-    (void)c;
     return 0;
 }
 
@@ -1933,15 +2258,30 @@ extern "C" int hit3d_batch_step(hit3d_batch *b, int32_t nsteps, int32_t graph_st
             return h3d_set_error_msg(-1, "hit3d_batch_step: a run with the learned closure (les_model 20) needs weights "
                                          "(hit3d_gpu_les_set_mlp)");
     if (graph_steps < 1) graph_steps = 1;
-    hit3d_ctx *c = b->runs[0];
     H3D_CHECK(cudaSetDevice(b->dev));
     for (hit3d_ctx *cr : b->runs) H3D_TRY(ensure_alias_state(cr));
+    for (BatchClass &k : b->classes) H3D_TRY(class_tables(b, k));
     int left = nsteps;
-    // first-order step of runs that need one, outside the graph
+    // first-order step of runs that need one, outside the graph: a whole class
+    // together when all its runs need it, else run by run
     bool any_first = false;
     for (size_t r = 0; r < b->runs.size(); r++) any_first |= b->fov[r] || (b->fos[r] && b->runs[r]->int_scalars);
     if (any_first && left > 0) {
+        for (BatchClass &k : b->classes) {
+            bool all = true, none = true;
+            for (int r : k.runs) {
+                all &= b->fov[r] != 0;
+                none &= b->fov[r] == 0;
+            }
+            if (all || none) {
+                H3D_TRY(class_step_any(b, k, all ? 1 : 0));
+            } else {
+                for (int r : k.runs) H3D_TRY(run_step(b->runs[r], b->fov[r], b->fos[r]));
+            }
+            for (int r : k.runs) b->fov[r] = 0;
+        }
         for (size_t r = 0; r < b->runs.size(); r++) {
+            if (b->run_class[r] >= 0) continue;
             H3D_TRY(run_step(b->runs[r], b->fov[r], b->fos[r]));
             b->fov[r] = 0;
             if (b->runs[r]->int_scalars) b->fos[r] = 0;
@@ -1969,18 +2309,21 @@ extern "C" int hit3d_batch_step(hit3d_batch *b, int32_t nsteps, int32_t graph_st
         }
         H3D_CHECK(cudaStreamSynchronize(b->root));
     }
-    for (; left > 0; left--)
-        for (hit3d_ctx *cr : b->runs) H3D_TRY(run_step(cr, 0, 0));
+    for (; left > 0; left--) H3D_TRY(batch_issue(b));
     for (hit3d_ctx *cr : b->runs) H3D_CHECK(cudaStreamSynchronize(cr->st));
     // a run with the learned closure on the tensor cores reports a completion
-    // wait that ran out, as hit3d_gpu_step does
-    for (hit3d_ctx *cr : b->runs)
+    // wait that ran out, as hit3d_gpu_step does; the fused x passes report a
+    // stage wait that ran out in the first run of their class
+    for (hit3d_ctx *cr : b->runs) {
         if (cr->p.les_model == HIT3D_LES_LEARNED && cr->mlp_kernel == 1 && nsteps > 0) {
             int herr = 0;
             H3D_CHECK(cudaMemcpy(&herr, cr->d_mlp_err, sizeof herr, cudaMemcpyDeviceToHost));
             if (herr) return h3d_set_error_msg(-5, "hit3d_batch_step: a tensor-core completion wait of the closure ran out");
         }
-    (void)c;
+        int derr = 0;
+        H3D_CHECK(cudaMemcpy(&derr, cr->d_err, sizeof derr, cudaMemcpyDeviceToHost));
+        if (derr) return h3d_set_error_msg(-5, "hit3d_batch_step: a fused x pass gave up waiting for its input rows");
+    }
     return 0;
 }
 

@@ -27,3 +27,15 @@ template <typename T, int L> struct RowCfg {
     static constexpr int NT = 128;
     static constexpr size_t SMEM = (size_t)Lay<L, TC, true>::elems * sizeof(cx<T>);
 };
+
+// Column-tile shapes the batch tuner picks from for grids up to 128 (ct = the
+// context's `ctile`): 0 the default ColCfg, 1 half as many kx columns per CTA,
+// 2 twice as many; at least one warp per CTA
+constexpr int kColTiles = 3;
+template <typename T, int L, bool YPASS, int CT> struct ColCfgT {
+    using B = ColCfg<T, L, YPASS>;
+    static constexpr int TC = CT == 0 ? B::TC : CT == 1 ? B::TC / 2 : B::TC * 2;
+    static constexpr int NT0 = TC * L / plan_rmax(L);
+    static constexpr int NT = CT == 0 ? B::NT : NT0 < 32 ? 32 : NT0 > 512 ? 512 : NT0;
+    static constexpr size_t SMEM = (size_t)Lay<L, TC, false>::elems * sizeof(cx<T>);
+};

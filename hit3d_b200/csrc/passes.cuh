@@ -37,6 +37,22 @@ template <typename T, typename TI, typename TO> struct IOPlain {
     int64_t sa_src, so_src, sa_dst, so_dst;
     int ncol;
     int n = 0, kl = -1, ks = -1, ko = -1;
+    // runs of a batch: nfr > 0 fields per run, run r's fields start rs_src /
+    // rs_dst elements after run r-1's; grid index z = r * nfr + f
+    int nfr = 0;
+    int64_t rs_src = 0, rs_dst = 0;
+    H3D_D IOPlain at(int z, int &f) const
+    {
+        IOPlain b = *this;
+        f = z;
+        if (nfr > 0) {
+            const int r = z / nfr;
+            f = z - r * nfr;
+            b.src += r * rs_src;
+            b.dst += r * rs_dst;
+        }
+        return b;
+    }
     H3D_D int outer(int y) const { return ko >= 0 ? kept_index(y, n, ko) : y; }
     H3D_D cx<T> load(int f, int o, int c, int p) const
     {
@@ -76,6 +92,20 @@ template <typename T, typename TO, int MODE> struct IOSpec {
     double k2max;  // truncation radius squared, for PRE_TRUNC
     const double2 *g = nullptr;  // test filter transfer function, for PRE_FILT (pitch psrc)
     int kl = -1, ko = -1;  // 2/3-rule pruning of the kz loads and the ky rows
+    int nfr = 0;           // runs of a batch, as IOPlain::at
+    int64_t rs_src = 0, rs_dst = 0;
+    H3D_D IOSpec at(int z, int &f) const
+    {
+        IOSpec b = *this;
+        f = z;
+        if (nfr > 0) {
+            const int r = z / nfr;
+            f = z - r * nfr;
+            b.src += r * rs_src;
+            b.dst += r * rs_dst;
+        }
+        return b;
+    }
     H3D_D int outer(int y) const { return ko >= 0 ? kept_index(y, n, ko) : y; }
 
     H3D_D double2 U(int f, int o, int c, int p) const { return src[f * fs_src + ((int64_t)p * n + o) * psrc + c]; }
@@ -170,16 +200,18 @@ __global__ void __launch_bounds__(NT, (ColMinBlocks<T, L, TC, NT>::value)) k_col
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
     using F = ColFFT<T, L, TC, NT, false, FWD, false>;
-    const int col0 = blockIdx.x * TC, outer = io.outer(blockIdx.y), f = blockIdx.z;
+    int f;
+    const IO iob = io.at(blockIdx.z, f);
+    const int col0 = blockIdx.x * TC, outer = iob.outer(blockIdx.y);
     cx<T> in[F::NIN];
 #pragma unroll
     for (int i = 0; i < F::NB0; i++)
 #pragma unroll
         for (int m = 0; m < F::R0; m++) {
             int c, p;
-            if (F::in_slot(i, m, c, p)) in[i * F::R0 + m] = io.load(f, outer, col0 + c, p);
+            if (F::in_slot(i, m, c, p)) in[i * F::R0 + m] = iob.load(f, outer, col0 + c, p);
         }
-    F::run_store(in, sm, tw, [&](int c, int p, cx<T> v) { io.store(f, outer, col0 + c, p, v); });
+    F::run_store(in, sm, tw, [&](int c, int p, cx<T> v) { iob.store(f, outer, col0 + c, p, v); });
 }
 
 // ---------------------------------------------------------------------------
@@ -346,6 +378,20 @@ struct FusedArgs {
     double p0, p1;       // operator parameters
     int kx_lim;          // > 0: only kx < kx_lim is read and stored (2/3-rule pruning)
     int *err;            // optional: set (bit 1) when a bounded wait on the input stage ran out
+    int nruns;           // runs of a batch (0 or 1: one run); npairs is per run
+    int64_t rstride;     // elements of cx<TS> from one run's work fields to the next run's
+};
+
+// tile -> (run, first row pair of the tile) for the staged kernels: the tiles of
+// a batch enumerate every run's row pairs, ntr = ceil(npairs / TC) tiles per run
+struct TileMap {
+    int ntr, nruns;
+    H3D_D int total() const { return ntr * nruns; }
+    H3D_D void at(int tile, int tc, int &run, int &pair0) const
+    {
+        run = nruns > 1 ? tile / ntr : 0;
+        pair0 = (tile - run * ntr) * tc;
+    }
 };
 
 template <typename T, int L, int TC, int NT, typename TS, class OP>
@@ -716,7 +762,7 @@ template <typename TS> struct StageRow {
 };
 
 template <typename TS, int NIN, int TC, int NT>
-H3D_D void stage_issue(const FusedArgs &a, cx<TS> *st, int pair0, int nch)
+H3D_D void stage_issue(const FusedArgs &a, cx<TS> *st, int pair0, int nch, int64_t roff = 0)
 {
     constexpr int PER = StageRow<TS>::PER;
     const int rs = nch * PER;
@@ -724,7 +770,7 @@ H3D_D void stage_issue(const FusedArgs &a, cx<TS> *st, int pair0, int nch)
         if (pair0 < a.npairs) {
 #pragma unroll
             for (int rr = 0; rr < NIN * 2; rr++) {
-                const cx<TS> *src = reinterpret_cast<const cx<TS> *>(a.in[rr >> 1]) + (int64_t)(2 * pair0 + (rr & 1)) * a.pitch;
+                const cx<TS> *src = reinterpret_cast<const cx<TS> *>(a.in[rr >> 1]) + roff + (int64_t)(2 * pair0 + (rr & 1)) * a.pitch;
                 for (int ch = threadIdx.x; ch < nch; ch += NT) cp_async16(st + rr * rs + ch * PER, src + ch * PER);
             }
         }
@@ -735,7 +781,7 @@ H3D_D void stage_issue(const FusedArgs &a, cx<TS> *st, int pair0, int nch)
             const int rr = dch(q), ch = q - rr * nch;
             const int r = rr % (2 * TC), f = rr / (2 * TC);
             if (pair0 + r / 2 >= a.npairs) continue;
-            const cx<TS> *src = reinterpret_cast<const cx<TS> *>(a.in[f]) + (int64_t)(2 * pair0 + r) * a.pitch + ch * PER;
+            const cx<TS> *src = reinterpret_cast<const cx<TS> *>(a.in[f]) + roff + (int64_t)(2 * pair0 + r) * a.pitch + ch * PER;
             cp_async16(st + (f * 2 * TC + r) * rs + ch * PER, src);
         }
     }
@@ -759,17 +805,24 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_st(const FusedArgs a, const
     const int lim = a.kx_lim > 0 ? a.kx_lim : L / 2 + 1;
     const int nch = StageRow<TS>::chunks(lim);
     const int rs = nch * StageRow<TS>::PER;
-    const int ntiles = (a.npairs + TC - 1) / TC;
+    const TileMap tm{(a.npairs + TC - 1) / TC, a.nruns > 1 ? a.nruns : 1};
+    const int ntiles = tm.total();
     OP op{(T)a.p0, (T)a.p1};
     // each warp's Courant maximum over its tiles, kept in shared memory rather
     // than in a register live across the tile loop; one atomic per warp at the end
     __shared__ double cwarp[NT / 32];
     if ((threadIdx.x & 31) == 0) cwarp[threadIdx.x >> 5] = 0.0;
-    if ((int)blockIdx.x < ntiles) stage_issue<TS, OP::NIN, TC, NT>(a, st, blockIdx.x * TC, nch);
+    if ((int)blockIdx.x < ntiles) {
+        int r0, p0;
+        tm.at(blockIdx.x, TC, r0, p0);
+        stage_issue<TS, OP::NIN, TC, NT>(a, st, p0, nch, r0 * a.rstride);
+    }
 
 #pragma unroll 1
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int pair0 = tile * TC;
+        int run, pair0;
+        tm.at(tile, TC, run, pair0);
+        const int64_t roff = run * a.rstride;
         cx<T> phys[OP::NIN][NP];
         {
             cp_async_wait_all();
@@ -791,7 +844,11 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_st(const FusedArgs a, const
                 for (int q = 0; q < NP; q++) phys[f][q] = mk<T>(0, 0);
             }
             __syncthreads();  // the stage is free: prefetch the next tile
-            if (tile + (int)gridDim.x < ntiles) stage_issue<TS, OP::NIN, TC, NT>(a, st, pair0 + gridDim.x * TC, nch);
+            if (tile + (int)gridDim.x < ntiles) {
+                int rn, pn;
+                tm.at(tile + gridDim.x, TC, rn, pn);
+                stage_issue<TS, OP::NIN, TC, NT>(a, st, pn, nch, rn * a.rstride);
+            }
             FI::template run_multi<OP::NIN>(in, sm, phys, tw);
         }
         // quadratic products: the 1/N^3 of the inverse transforms is applied
@@ -878,8 +935,8 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_st(const FusedArgs a, const
             for (int gf = 0; gf < GF; gf++) {
                 const int o = g * GF + gf;
                 if (o < OP::NOUT)
-                    store_split<T, L, TC, NT, TS>(sm + gf * E, reinterpret_cast<cx<TS> *>(a.out[o]), a.pitch, pair0,
-                                                  a.npairs, lim, OP::QUAD ? (T)0.5 * (T)a.norm * (T)a.norm : (T)0.5);
+                    store_split<T, L, TC, NT, TS>(sm + gf * E, reinterpret_cast<cx<TS> *>(a.out[o]) + roff, a.pitch, pair0,
+                                              a.npairs, lim, OP::QUAD ? (T)0.5 * (T)a.norm * (T)a.norm : (T)0.5);
             }
             __syncthreads();
         }

@@ -142,6 +142,12 @@ struct StepArgs {
     int kc;                    // >= 0: visit only the modes the 2/3 rule keeps (pruned state)
     int idle;                  // passive scalars 0..idle-1 wait for TSCALAR while LES fields move:
                                // no advection or molecular diffusion, only sources and LES fluxes
+    // runs of a batch (k_update_vel_23 over gridDim.y runs): run r's state starts
+    // r * ru elements after run 0's and its product fields r * rp after; nu_r
+    // and dt_r (when set) hold each run's viscosity and time step, and fenergy
+    // each run's forcing-band energy
+    int64_t ru, rp;
+    const double *nu_r, *dt_r;
 };
 
 // 2/3 rule (rhs_velocity.f90:85-142) + forcing + AB2 + pressure.
@@ -153,7 +159,12 @@ __global__ void k_update_vel_23(const StepArgs a, const cx<TP> *__restrict__ P, 
                                 double2 *__restrict__ U, double2 *__restrict__ RO)
 {
     const int64_t nm = mode_count(a.n, a.nh, a.kc);
-    const double fac = (a.flow_type == 1) ? a.famp / *a.fenergy : 0.0;
+    const int run = blockIdx.y;
+    U += run * a.ru;
+    RO += run * a.ru;
+    P += run * a.rp;
+    const double nu = a.nu_r != nullptr ? a.nu_r[run] : a.nu, dt = a.dt_r != nullptr ? a.dt_r[run] : a.dt;
+    const double fac = (a.flow_type == 1) ? a.famp / a.fenergy[run] : 0.0;
     const ModeLoop ml(a.n, a.nh, a.kc);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
         ModeIdx m = ml.at(t);
@@ -169,7 +180,7 @@ __global__ void k_update_vel_23(const StepArgs a, const cx<TP> *__restrict__ P, 
             double2 t1 = make_double2(-(kx * p11.x + ky * p12.x + kz * p13.x), -(kx * p11.y + ky * p12.y + kz * p13.y));
             double2 t2 = make_double2(-(kx * p12.x + ky * p22.x + kz * p23.x), -(kx * p12.y + ky * p22.y + kz * p23.y));
             double2 t3 = make_double2(-(kx * p13.x + ky * p23.x + kz * p33.x), -(kx * p13.y + ky * p23.y + kz * p33.y));
-            double t4 = -a.nu * (kx * kx + ky * ky + kz * kz);
+            double t4 = -nu * (kx * kx + ky * ky + kz * kz);
             double2 tt[3] = {t1, t2, t3};
 #pragma unroll
             for (int c = 0; c < 3; c++) r[c] = make_double2(-tt[c].y + t4 * u[c].x, tt[c].x + t4 * u[c].y);
@@ -194,7 +205,7 @@ __global__ void k_update_vel_23(const StepArgs a, const cx<TP> *__restrict__ P, 
         }
         double2 ro[3] = {RO[o], RO[o + a.fs], RO[o + 2 * a.fs]};
 #pragma unroll
-        for (int c = 0; c < 3; c++) ab2(u[c], ro[c], r[c], a.dt, a.euler_v);
+        for (int c = 0; c < 3; c++) ab2(u[c], ro[c], r[c], dt, a.euler_v);
         project(m, u[0], u[1], u[2]);
 #pragma unroll
         for (int c = 0; c < 3; c++) { U[o + c * a.fs] = u[c]; RO[o + c * a.fs] = ro[c]; }
@@ -373,10 +384,14 @@ __global__ void k_scalar(const StepArgs a, int mode, int s, double dx, const cx<
 
 // Energy in the forcing band, summed by one thread in the reference's loop
 // order (m_force.f90:266-284) so that the result is reproducible to the bit.
+// Batches launch one CTA per run (run r's state ru elements after run r-1's,
+// its energy in out[r]); one run launches one CTA with ru = 0.
 __global__ void k_forcing_energy(int n, int pitch, int64_t fs, int kfmax, const double2 *__restrict__ U,
-                                 double *out)
+                                 double *out, int64_t ru = 0)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (threadIdx.x != 0) return;
+    U += blockIdx.x * ru;
+    out += blockIdx.x;
     double es[16];
     for (int s = 0; s < 16; s++) es[s] = 0.0;
     const double n3 = (double)n * n * n;

@@ -54,7 +54,7 @@ H3D_D bool xf_mbar_wait(uint64_t *bar, unsigned parity)
 // Sources: 16-byte aligned fields and a row pitch of a multiple of 16 bytes
 // (checked by the host), and the rounded row stays inside the pitch.
 template <typename TS, int NIN, int TC>
-H3D_D void xf_stage_issue(const FusedArgs &a, cx<TS> *st, uint64_t *bar, int pair0, int rs)
+H3D_D void xf_stage_issue(const FusedArgs &a, cx<TS> *st, uint64_t *bar, int pair0, int rs, int64_t roff)
 {
     const int np = a.npairs - pair0 < TC ? a.npairs - pair0 : TC;
     const unsigned row_bytes = (unsigned)rs * (unsigned)sizeof(cx<TS>);
@@ -67,7 +67,7 @@ H3D_D void xf_stage_issue(const FusedArgs &a, cx<TS> *st, uint64_t *bar, int pai
 #pragma unroll
     for (int f = 0; f < NIN; f++)
         for (int r = 0; r < 2 * np; r++) {
-            const cx<TS> *src = reinterpret_cast<const cx<TS> *>(a.in[f]) + (int64_t)(2 * pair0 + r) * a.pitch;
+            const cx<TS> *src = reinterpret_cast<const cx<TS> *>(a.in[f]) + roff + (int64_t)(2 * pair0 + r) * a.pitch;
             asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                              xf_smem(st + (f * 2 * TC + r) * rs)),
                          "l"(src), "r"(row_bytes), "r"(xf_smem(bar))
@@ -173,7 +173,11 @@ H3D_D void xf_last_split(const cx<T> *sm, const cx<T> *__restrict__ tw, void *co
     }
 }
 
-template <typename T, int L, int TC, int NT, typename TS, class OP, int MINB>
+// NSMF: the last NSMF input fields wait in shared memory between the inverse
+// and the forward transforms (in the exchange buffers the forward groups of
+// two leave free), each thread at its own slots, which frees their registers
+// for the forward transforms (FP64 at L >= 512 otherwise spills)
+template <typename T, int L, int TC, int NT, typename TS, class OP, int MINB, int NSMF = 0>
 __global__ void __launch_bounds__(NT, MINB) k_xfused_v2(const FusedArgs a, const cx<T> *__restrict__ tw)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -183,7 +187,8 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_v2(const FusedArgs a, const
     constexpr int GF = 2;
     constexpr int NP = FI::NOUT;
     constexpr int E = Lay<L, TC, true>::elems;
-    constexpr int NB = OP::NIN > GF ? OP::NIN : GF;
+    constexpr int NB = (OP::NIN > GF ? OP::NIN : GF) > GF + NSMF ? (OP::NIN > GF ? OP::NIN : GF) : GF + NSMF;
+    static_assert(NSMF >= 0 && NSMF < OP::NIN, "fields kept in shared memory");
     constexpr size_t SOFF = ((size_t)NB * E * sizeof(cx<T>) + 15) / 16 * 16;
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
     cx<TS> *st = reinterpret_cast<cx<TS> *>(smraw + SOFF);
@@ -193,18 +198,25 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_v2(const FusedArgs a, const
     const int rs = nch * StageRow<TS>::PER;
     // the stage barrier follows the stage (rs * sizeof(cx<TS>) is a multiple of 16)
     uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + SOFF + (size_t)OP::NIN * 2 * TC * rs * sizeof(cx<TS>));
-    const int ntiles = (a.npairs + TC - 1) / TC;
+    const TileMap tm{(a.npairs + TC - 1) / TC, a.nruns > 1 ? a.nruns : 1};
+    const int ntiles = tm.total();
     OP op{(T)a.p0, (T)a.p1};
     __shared__ double cwarp[NT / 32];
     if ((threadIdx.x & 31) == 0) cwarp[threadIdx.x >> 5] = 0.0;
     if (threadIdx.x == 0) xf_mbar_init(bar);
     __syncthreads();
-    if (threadIdx.x == 0 && (int)blockIdx.x < ntiles) xf_stage_issue<TS, OP::NIN, TC>(a, st, bar, blockIdx.x * TC, rs);
+    if (threadIdx.x == 0 && (int)blockIdx.x < ntiles) {
+        int r0, p0;
+        tm.at(blockIdx.x, TC, r0, p0);
+        xf_stage_issue<TS, OP::NIN, TC>(a, st, bar, p0, rs, r0 * a.rstride);
+    }
     unsigned parity = 0;
 
 #pragma unroll 1
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int pair0 = tile * TC;
+        int run, pair0;
+        tm.at(tile, TC, run, pair0);
+        const int64_t roff = run * a.rstride;
         const bool ok = xf_mbar_wait(bar, parity);
         if (__syncthreads_or(!ok)) {
             // the copies never completed: report, and leave without touching the stage
@@ -231,8 +243,11 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_v2(const FusedArgs a, const
                 for (int q = 0; q < NP; q++) phys[f][q] = mk<T>(0, 0);
             }
             __syncthreads();  // the stage is free: bring in the next tile
-            if (threadIdx.x == 0 && tile + (int)gridDim.x < ntiles)
-                xf_stage_issue<TS, OP::NIN, TC>(a, st, bar, pair0 + gridDim.x * TC, rs);
+            if (threadIdx.x == 0 && tile + (int)gridDim.x < ntiles) {
+                int rn, pn;
+                tm.at(tile + gridDim.x, TC, rn, pn);
+                xf_stage_issue<TS, OP::NIN, TC>(a, st, bar, pn, rs, rn * a.rstride);
+            }
             FI::template run_multi<OP::NIN>(in, sm, phys, tw);
         }
         // quadratic products: the 1/N^3 of the inverse transforms is applied
@@ -286,6 +301,21 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_v2(const FusedArgs a, const
         }
         constexpr int NG = (OP::NOUT + GF - 1) / GF;
         const T half = OP::QUAD ? (T)0.5 * (T)a.norm * (T)a.norm : (T)0.5;
+        // fields NIN-NSMF..NIN-1 to buffers GF.., at this thread's own slots (the
+        // barrier above ended the inverse's reads of every buffer)
+        cx<T> *pw = sm + GF * E;
+        if constexpr (NSMF > 0) {
+#pragma unroll
+            for (int i = 0; i < FI::NBL; i++)
+#pragma unroll
+                for (int m = 0; m < FI::RL; m++) {
+                    int c, p;
+                    if (FI::out_slot(i, m, c, p))
+#pragma unroll
+                        for (int f = OP::NIN - NSMF; f < OP::NIN; f++)
+                            pw[(f - (OP::NIN - NSMF)) * E + Lay<L, TC, true>::idx(c, p)] = phys[f][i * FI::RL + m];
+                }
+        }
 #pragma unroll
         for (int g = 0; g < NG; g++) {
             cx<T> in[GF][FF::NIN];
@@ -297,12 +327,25 @@ __global__ void __launch_bounds__(NT, MINB) k_xfused_v2(const FusedArgs a, const
                     T va[OP::NIN], vb[OP::NIN];
 #pragma unroll
                     for (int f = 0; f < OP::NIN; f++) { va[f] = phys[f][q].x; vb[f] = phys[f][q].y; }
+                    if constexpr (NSMF > 0) {
+                        // the same slot the inverse left this thread (FI::NOUT == FF::NIN)
+                        int c, p;
+                        FF::in_slot(q / FF::R0, q % FF::R0, c, p);
+#pragma unroll
+                        for (int f = OP::NIN - NSMF; f < OP::NIN; f++)
+                            if (o < OP::NOUT && OP::uses(o, f)) {
+                                const cx<T> v = pw[(f - (OP::NIN - NSMF)) * E + Lay<L, TC, true>::idx(c, p)];
+                                va[f] = v.x;
+                                vb[f] = v.y;
+                            }
+                    }
                     in[gf][q] = o < OP::NOUT ? mk<T>(op.out(o, va, aux[q].x), op.out(o, vb, aux[q].y)) : mk<T>(0, 0);
                 }
             }
             FF::template run_multi_front<GF>(in, sm, tw);
-            void *const outs[GF] = {g * GF < OP::NOUT ? a.out[g * GF] : nullptr,
-                                    g * GF + 1 < OP::NOUT ? a.out[g * GF + 1] : nullptr};
+            void *const outs[GF] = {g * GF < OP::NOUT ? (void *)(reinterpret_cast<cx<TS> *>(a.out[g * GF]) + roff) : nullptr,
+                                    g * GF + 1 < OP::NOUT ? (void *)(reinterpret_cast<cx<TS> *>(a.out[g * GF + 1]) + roff)
+                                                          : nullptr};
             xf_last_split<T, L, TC, NT, GF, TS>(sm, tw, outs, a.pitch, pair0, a.npairs, lim, half);
             __syncthreads();  // the buffers are read: the next group may overwrite them
         }

@@ -28,7 +28,9 @@ template <typename T, int L, int V> struct RowCfgV {
 //       threads at 168 registers), groups of 2 for FP64
 //   13: the launch shape of 12, forward transforms in groups of 2, input rows
 //       staged by bulk copies and the Hermitian split done in registers
-//       (k_xfused_v2)
+//       (k_xfused_v2); FP64 at L >= 512 keeps the last physical field in
+//       shared memory between the inverse and forward transforms
+//   14: as 13 with two physical fields in shared memory (FP64), one (FP32)
 template <typename T, int L> struct RowCfgSmall {
     static constexpr int TC = L >= 512 ? 1 : 512 / L;
     static constexpr int NT = L >= 1024 ? 128 : 64;
@@ -102,12 +104,12 @@ static int xfused_st_L(hit3d_ctx *c, FusedArgs a)
     return 0;
 }
 // bulk-copy staged form with the split in registers (k_xfused_v2)
-template <typename T, template <class> class OP, int L, int MINB, class RC>
+template <typename T, template <class> class OP, int L, int MINB, class RC, int NSMF>
 static int xfused_v2_L(hit3d_ctx *c, FusedArgs a)
 {
     constexpr int NIN = OP<T>::NIN;
-    constexpr int NB = NIN > 2 ? NIN : 2;
-    auto k = k_xfused_v2<T, L, RC::TC, RC::NT, T, OP<T>, MINB>;
+    constexpr int NB = (NIN > 2 ? NIN : 2) > 2 + NSMF ? (NIN > 2 ? NIN : 2) : 2 + NSMF;
+    auto k = k_xfused_v2<T, L, RC::TC, RC::NT, T, OP<T>, MINB, NSMF>;
     for (int f = 0; f < NIN; f++)
         if (reinterpret_cast<uintptr_t>(a.in[f]) % 16 != 0)
             return h3d_set_error_msg(-1, "fused x pass: input field not 16-byte aligned");
@@ -137,10 +139,19 @@ static int xfused_v2_L(hit3d_ctx *c, FusedArgs a)
 template <typename T, template <class> class OP, int L> static int xfused_L(hit3d_ctx *c, FusedArgs a)
 {
     if constexpr (OP<T>::NIN <= 3) {
-        if (c->xcfg == 13) {
+        if (c->xcfg == 13 || c->xcfg == 14) {
+            // 13: FP64 at L >= 512 keeps one physical field in shared memory
+            // (registers), the rest none; 14: two (FP64) or one (FP32)
             using RS = RowCfgSmall<T, L>;
-            if constexpr (sizeof(T) == 4) return xfused_v2_L<T, OP, L, 384 / RS::NT, RS>(c, a);
-            else return xfused_v2_L<T, OP, L, 256 / RS::NT, RS>(c, a);
+            constexpr int N13 = (sizeof(T) == 8 && L >= 512 && OP<T>::NIN == 3) ? 1 : 0;
+            constexpr int N14 = OP<T>::NIN < 3 ? 0 : sizeof(T) == 8 ? 2 : 1;
+            if constexpr (sizeof(T) == 4) {
+                if (c->xcfg == 13) return xfused_v2_L<T, OP, L, 384 / RS::NT, RS, N13>(c, a);
+                return xfused_v2_L<T, OP, L, 384 / RS::NT, RS, N14>(c, a);
+            } else {
+                if (c->xcfg == 13) return xfused_v2_L<T, OP, L, 256 / RS::NT, RS, N13>(c, a);
+                return xfused_v2_L<T, OP, L, 256 / RS::NT, RS, N14>(c, a);
+            }
         }
         if (c->xcfg == 8) return xfused_st_L<T, OP, L, 3, 2>(c, a);
         if (c->xcfg == 9) return xfused_st_L<T, OP, L, 2, 2>(c, a);
@@ -172,6 +183,36 @@ template <typename T, template <class> class OP, int L> static int xfused_L(hit3
 template <typename T, template <class> class OP> int xfused(hit3d_ctx *c, FusedArgs a)
 {
     a.npairs = c->n * c->n / 2;
+    if (c->bruns > 1) {
+        // every run of a batch class: only the staged kernels walk the tiles of
+        // several runs (variants 8-13); others take variant 13's
+        if constexpr (OP<T>::NIN > 3) return h3d_set_error_msg(-1, "fused x pass: batch classes carry the velocity only");
+        a.nruns = c->bruns;
+        a.rstride = c->brw;
+        a.cmax = nullptr;
+        a.phys = nullptr;
+        if (c->xcfg < 8) {
+            const int saved = c->xcfg;
+            c->xcfg = 13;
+            a.norm = 1.0 / ((double)c->n * c->n * c->n);
+            a.kx_lim = c->kc_active >= 0 ? c->kc_active + 1 : 0;
+#define CALL(L) xfused_L<T, OP, L>(c, a)
+            int rc = 0;
+            switch (c->n) {
+            case 32: rc = CALL(32); break;
+            case 48: rc = CALL(48); break;
+            case 64: rc = CALL(64); break;
+            case 128: rc = CALL(128); break;
+            case 256: rc = CALL(256); break;
+            case 512: rc = CALL(512); break;
+            case 1024: rc = CALL(1024); break;
+            default: rc = h3d_set_error_msg(-3, "unsupported grid size");
+            }
+#undef CALL
+            c->xcfg = saved;
+            return rc;
+        }
+    }
     const double n3 = (double)c->n * c->n * c->n;
     a.norm = 1.0 / n3;
     a.kx_lim = c->kc_active >= 0 ? c->kc_active + 1 : 0;

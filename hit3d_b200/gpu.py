@@ -22,7 +22,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libhit3d_gpu.so")
 MAX_SCALARS = 8
 LES_LEARNED = 20  # les_model of the learned closure (HIT3D_LES_LEARNED)
-N_VARIANTS = 14  # launch-shape variants of the fused x pass (HIT3D_FUSED_VARIANTS)
+N_VARIANTS = 15  # launch-shape variants of the fused x pass (HIT3D_FUSED_VARIANTS)
 
 
 def les_fields(les_model: int) -> int:
@@ -141,6 +141,8 @@ SIGNATURES = [
     ("hit3d_batch_context", C.c_int, [_vp, _i32, C.POINTER(C.c_void_p)]),
     ("hit3d_batch_step", C.c_int, [_vp, _i32, _i32]),
     ("hit3d_batch_graph_launches", C.c_int64, [_vp]),
+    ("hit3d_batch_nclasses", C.c_int, [_vp]),
+    ("hit3d_batch_autotune", C.c_int, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     ("hit3d_batch_destroy", None, [_vp]),
     ("hit3d_mlp_nparam", C.c_int, []),
     ("hit3d_mlp_create", C.c_int, [_i32, C.c_uint64, C.POINTER(C.c_void_p)]),

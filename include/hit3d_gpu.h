@@ -128,7 +128,7 @@ int hit3d_gpu_step_profile(hit3d_ctx *ctx, int32_t nsteps, int32_t *fov, int32_t
  * *variant receives the choice, ms[0..HIT3D_FUSED_VARIANTS) the time of each
  * variant (unused entries are left untouched).
  * hit3d_gpu_set_variant fixes a variant by hand. */
-#define HIT3D_FUSED_VARIANTS 14
+#define HIT3D_FUSED_VARIANTS 15
 int hit3d_gpu_autotune(hit3d_ctx *ctx, int32_t *variant, double *ms);
 int hit3d_gpu_set_variant(hit3d_ctx *ctx, int32_t variant);
 
@@ -279,13 +279,17 @@ int hit3d_gpu_physical_velocity(hit3d_ctx *ctx, double *out, int64_t ld1);
 /* ---------------------------------------------------------------------------
  * Batched form (no reference counterpart: the reference runs one simulation per
  * MPI job).  Many independent runs of uneven sizes, each with its own
- * parameters (Re, seeds), on one GPU.  hit3d_batch_step takes the first-order
- * step of new runs eagerly, then records `graph_steps` Adams-Bashforth steps of
- * all runs into one CUDA graph (a branch per run) and replays it, one launch per
- * chunk.  dt and the scalar switch are baked into the recording: change them
- * (hit3d_gpu_set_dt, hit3d_gpu_set_scalars_active on a run's context) only
- * between calls; the next call re-records the graph when either, or
- * graph_steps, has changed.
+ * parameters (Re, seeds), on one GPU.  Runs that share a grid size, precision
+ * and forcing and carry the velocity only with the 2/3 rule form a size class:
+ * their state and work fields sit in one slab, and every pass of a step is one
+ * launch over all the class's runs (per-run viscosity, time step and forcing
+ * energy in device tables).  Other runs step on their own.  hit3d_batch_step
+ * takes the first-order step of new runs eagerly, then records `graph_steps`
+ * Adams-Bashforth steps of all classes and runs into one CUDA graph (a branch
+ * per class or lone run) and replays it, one launch per chunk.  dt and the
+ * scalar switch are baked into the recording: change them (hit3d_gpu_set_dt,
+ * hit3d_gpu_set_scalars_active on a run's context) only between calls; the next
+ * call re-records the graph when either, or graph_steps, has changed.
  * ------------------------------------------------------------------------- */
 typedef struct hit3d_batch hit3d_batch;
 int hit3d_batch_create(const hit3d_params *p /* [nruns] */, int32_t nruns, hit3d_batch **out);
@@ -294,6 +298,16 @@ int hit3d_batch_context(hit3d_batch *b, int32_t r, hit3d_ctx **ctx);
 int hit3d_batch_step(hit3d_batch *b, int32_t nsteps, int32_t graph_steps);
 /* Number of graph launches so far. */
 int64_t hit3d_batch_graph_launches(hit3d_batch *b);
+/* Number of size classes (ordered by their first run). */
+int hit3d_batch_nclasses(hit3d_batch *b);
+/* Per size class, time the fused x-pass launch shapes that walk several runs
+ * (variants 8-14) and the column-tile shapes of the strided passes (0: the
+ * default, 1: half, 2: twice the kx columns per CTA; grids up to 128) on the
+ * class's own buffers, reading the state without changing it, and keep the
+ * fastest of each.  choice[2k], choice[2k+1] receive class k's picks; ms (may
+ * be NULL) receives 10 times in ms per class (7 x-pass variants, then 3 tiles,
+ * NaN-free: tiles not tried report 0).  The next step re-records the graph. */
+int hit3d_batch_autotune(hit3d_batch *b, int32_t *choice, double *ms);
 void hit3d_batch_destroy(hit3d_batch *b);
 
 /* ---------------------------------------------------------------------------

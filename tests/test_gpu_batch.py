@@ -1,6 +1,11 @@
 """Batched form: runs advanced together through one recorded CUDA graph give
 the same fields as the same runs stepped one by one; subgrid-stress training
-data agree with the oracle."""
+data agree with the oracle.
+
+Runs of one size class step through batched launches (one launch per pass over
+all the class's runs) with the fused x pass of variant 13; stepped one by one
+with that variant they give bit-identical fields, and with any other variant
+fields equal to rounding."""
 import numpy as np
 import pytest
 
@@ -17,18 +22,47 @@ def test_batch_graph_matches_independent_runs():
     ps = [Params(nx=n, flow_type=1, kfmax=2, nu=nu, dt=0.004) for n, nu in zip(sizes, res)]
     b = Batch(ps)
     b.init()
-    ref = []
+    ref, ref_any = [], []
     for r, p in enumerate(ps):
-        c = Context(p)
-        c.init_velocity(run_seed(r), 2, 4.0, 2.0)
-        c.dealias_all()
-        c.step(12)
-        ref.append(c.download_fields())
-        c.close()
+        for variant, out in ((13, ref), (4, ref_any)):
+            c = Context(p)
+            c.set_variant(variant)
+            c.init_velocity(run_seed(r), 2, 4.0, 2.0)
+            c.dealias_all()
+            c.step(12)
+            out.append(c.download_fields())
+            c.close()
     b.step(12, graph_steps=5)
     assert b.graph_launches == 2  # 1 eager Euler step, 2 x 5 in the graph, 1 eager
     for r in range(len(ps)):
-        assert np.array_equal(b.contexts[r].download_fields(), ref[r])
+        f = b.contexts[r].download_fields()
+        assert np.array_equal(f, ref[r]), r
+        assert relerr(f, ref_any[r]) < 1e-13, r
+    b.close()
+
+
+def test_batch_classes_of_uneven_sizes_with_lone_runs():
+    """Classes of 3 x 32^3 (FP64), 2 x 48^3 (FP32) and lone runs that cannot join
+    a class (phase shift, a passive scalar) in one batch: every run equals the
+    same run stepped on its own."""
+    from hit3d_b200 import Context, Params
+    from hit3d_b200.batch import Batch, run_seed
+    ps = [Params(nx=32, flow_type=1, kfmax=2, nu=1.0 / (300 + 50 * r), dt=0.004) for r in range(3)]
+    ps += [Params(nx=48, flow_type=1, kfmax=2, nu=1.0 / (400 + 50 * r), dt=0.003, precision=1) for r in range(2)]
+    ps += [Params(nx=32, dealias=1, flow_type=1, kfmax=2, nu=1.0 / 300, dt=0.004),
+           Params(nx=32, flow_type=0, nu=1.0 / 300, dt=0.004, n_scalars=1, sc=[0.7], scalar_type=[0])]
+    b = Batch(ps)
+    b.init()
+    b.step(9, graph_steps=4)
+    for r, p in enumerate(ps):
+        c = Context(p)
+        if r < 5:  # class runs use variant 13; lone runs keep their own (the default)
+            c.set_variant(13)
+        c.init_velocity(run_seed(r), 2, 4.0, 2.0)
+        c.dealias_all()
+        c.step(9)
+        assert np.array_equal(b.contexts[r].download_fields(), c.download_fields()), r
+        c.close()
     b.close()
 
 
@@ -86,6 +120,7 @@ def test_batch_rerecords_graph_after_dt_change():
     assert b.graph_launches == 3
     for r, p in enumerate(ps):
         c = Context(Params(nx=32, flow_type=1, kfmax=2, nu=1.0 / 300, dt=0.004))
+        c.set_variant(13)
         c.init_velocity(run_seed(r), 2, 4.0, 2.0)
         c.dealias_all()
         c.step(6)
@@ -104,4 +139,36 @@ def test_batch_refuses_a_learned_closure_run_without_weights():
     b.init()
     with pytest.raises(Hit3dError, match="weights"):
         b.step(3, graph_steps=2)
+    b.close()
+
+
+def test_batch_autotune_picks_shapes_and_keeps_results():
+    """The per-class tuner picks a staged x-pass variant (8-14) and a column
+    tile (0-2) per size class without changing the state; afterwards every run
+    equals the same run stepped on its own with that variant (the column tile
+    does not change any run's arithmetic)."""
+    from hit3d_b200 import Context, Params
+    from hit3d_b200.batch import Batch, run_seed
+    ps = [Params(nx=32, flow_type=1, kfmax=2, nu=1.0 / (300 + 100 * r), dt=0.004) for r in range(2)]
+    ps.append(Params(nx=64, flow_type=1, kfmax=2, nu=1.0 / 600, dt=0.003))
+    b = Batch(ps)
+    b.init()
+    f0 = [c.download_fields() for c in b.contexts]
+    picks = b.autotune()
+    assert b.nclasses == 2 and len(picks) == 2
+    for v, tile, ms_v, ms_t in picks:
+        assert 8 <= v <= 14 and 0 <= tile <= 2
+        assert all(x > 0 for x in ms_v) and all(x > 0 for x in ms_t)
+    for r, c in enumerate(b.contexts):
+        assert np.array_equal(c.download_fields(), f0[r])
+    b.step(7, graph_steps=3)
+    cls = [0, 0, 1]
+    for r, p in enumerate(ps):
+        c = Context(p)
+        c.set_variant(picks[cls[r]][0])
+        c.init_velocity(run_seed(r), 2, 4.0, 2.0)
+        c.dealias_all()
+        c.step(7)
+        assert np.array_equal(b.contexts[r].download_fields(), c.download_fields()), r
+        c.close()
     b.close()

@@ -42,7 +42,7 @@ def test_one_pair_variants_at_512(precision):
     from hit3d_b200 import Context, Params
     kw = dict(nx=512, flow_type=1, kfmax=2, nu=1.0 / 3000.0, dt=2e-4, precision=precision)
     outs = {}
-    for v in (8, 11, 12, 13):
+    for v in (8, 11, 12, 13, 14):
         c = Context(Params(**kw))
         c.set_variant(v)
         c.init_velocity(RN1, 2, 4.0, 2.0)
@@ -51,7 +51,7 @@ def test_one_pair_variants_at_512(precision):
         outs[v] = c.download_fields()
         c.close()
     tol = 1e-13 if precision == 0 else 1e-6
-    for v in (11, 12, 13):
+    for v in (11, 12, 13, 14):
         assert relerr(outs[v], outs[8]) < tol, (v, relerr(outs[v], outs[8]))
 
 

@@ -149,7 +149,7 @@ def test_sidecar_keys_and_defaults(tmp_path):
 @pytest.mark.parametrize("text,msg", [
     ("precision = 2", "precision"),
     ("speed = 11", "unknown key"),
-    ("variant = 14", "variant"),
+    ("variant = 15", "variant"),
     ("pruning = maybe", "on/off"),
     ("precision", "key = value"),
     ("precision = 1\nprecision = 0", "twice"),
