@@ -147,6 +147,12 @@ struct hit3d_ctx {
     int pruned;          // the state is zero beyond N/3 (checked), so pruning is exact
     int alias_known;     // `pruned` is up to date with the state
     int kc_active;       // >= 0 while a pruned step is being issued: the cutoff N/3
+    // pipelined host transfers (hit3d_gpu_step_host), created on first use: copy
+    // streams, staging fields in the reference layout and their events
+    cudaStream_t cs_h2d, cs_d2h;
+    double2 *sin, *sout;
+    int nstage_io;       // fields each staging buffer holds
+    cudaEvent_t ev_in_ready, ev_in_free, ev_out_ready, ev_out_free;
     int ext_bufs;        // U, RO and W belong to a batch's slab
     int ctile;           // column-tile shape of the plain strided passes (ColCfgT), grids up to 128
     // while a batch class is being stepped through this context (its first

@@ -59,7 +59,7 @@ static int zinv_LMC(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_
         rows = 2 * c->kc_active + 1;
     }
     int nz = nf;
-    if (c->bruns > 1) {  // every run of a batch class: state run stride bru, work run stride brw
+    if (c->bruns > 0) {  // every run of a batch class: state run stride bru, work run stride brw
         io.nfr = nf;
         io.rs_src = c->bru;
         io.rs_dst = c->brw;
@@ -141,7 +141,7 @@ static int spass_LAC(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, 
         }
     }
     int nz = nf;
-    if (c->bruns > 1) {  // every run of a batch class (work fields, run stride brw)
+    if (c->bruns > 0) {  // every run of a batch class (work fields, run stride brw)
         io.nfr = nf;
         io.rs_src = io.rs_dst = c->brw;
         nz = nf * c->bruns;
@@ -982,6 +982,18 @@ extern "C" void hit3d_gpu_finalize(hit3d_ctx *c)
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->W64 && c->W64 != c->W) cudaFree(c->W64);
     if (c->ext_bufs) c->U = c->RO = nullptr, c->W = nullptr;  // a batch's slab
+    if (c->cs_h2d) {
+        cudaStreamSynchronize(c->cs_h2d);
+        cudaStreamSynchronize(c->cs_d2h);
+        cudaStreamDestroy(c->cs_h2d);
+        cudaStreamDestroy(c->cs_d2h);
+        cudaEventDestroy(c->ev_in_ready);
+        cudaEventDestroy(c->ev_in_free);
+        cudaEventDestroy(c->ev_out_ready);
+        cudaEventDestroy(c->ev_out_free);
+    }
+    if (c->sin) cudaFree(c->sin);
+    if (c->sout) cudaFree(c->sout);
     void *ptrs[] = {c->U, c->RO, c->RP, c->SP, c->W, c->phys, c->tw64, c->tw32, c->d_fen, c->d_part,
                     c->d_red, c->d_ratio, c->d_cmax, c->stage, c->d_xyz, c->d_uvw, c->sgs, c->mlp_wb,
                     c->d_mlp_err, c->d_kmin, c->gfilt, c->pfilt, c->pbuf};
@@ -1046,6 +1058,95 @@ extern "C" int hit3d_gpu_download_rhs_old(hit3d_ctx *c, double *r, int64_t ld1, 
 {
     if (!r) return h3d_set_error_msg(-1, "null rhs_old");
     return transfer_fields(c, c ? c->RO : nullptr, nullptr, r, ld1, nf);
+}
+
+// streams, staging fields and events of hit3d_gpu_step_host, on first use
+static int io_setup(hit3d_ctx *c, int nf)
+{
+    if (!c->cs_h2d) {
+        H3D_CHECK(cudaStreamCreateWithFlags(&c->cs_h2d, cudaStreamNonBlocking));
+        H3D_CHECK(cudaStreamCreateWithFlags(&c->cs_d2h, cudaStreamNonBlocking));
+        H3D_CHECK(cudaEventCreateWithFlags(&c->ev_in_ready, cudaEventDisableTiming));
+        H3D_CHECK(cudaEventCreateWithFlags(&c->ev_in_free, cudaEventDisableTiming));
+        H3D_CHECK(cudaEventCreateWithFlags(&c->ev_out_ready, cudaEventDisableTiming));
+        H3D_CHECK(cudaEventCreateWithFlags(&c->ev_out_free, cudaEventDisableTiming));
+    }
+    if (c->nstage_io < nf) {
+        H3D_CHECK(cudaStreamSynchronize(c->st));
+        if (c->sin) cudaFree(c->sin);
+        if (c->sout) cudaFree(c->sout);
+        c->sin = c->sout = nullptr;
+        c->nstage_io = 0;
+        const size_t fe = (size_t)c->n * c->n * c->nh;
+        H3D_TRY(ctx_alloc((void **)&c->sin, sizeof(double2) * fe * nf));
+        H3D_TRY(ctx_alloc((void **)&c->sout, sizeof(double2) * fe * nf));
+        c->nstage_io = nf;
+    }
+    return 0;
+}
+
+extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_t *fos, double *courant);
+
+extern "C" int hit3d_gpu_step_host(hit3d_ctx *c, int32_t nio, const double *const *in, double *const *out, int64_t ld1,
+                                   int32_t nf, int32_t nsteps, int32_t *fov, int32_t *fos)
+{
+    if (!c || !in || !out || nio < 1 || nsteps < 0) return h3d_set_error_msg(-1, "hit3d_gpu_step_host: bad arguments");
+    if (ld1 < c->n + 2) return h3d_set_error_msg(-1, "ld1 must be >= nx+2");
+    if (nf < 1 || nf > 3 + c->nsc) return h3d_set_error_msg(-1, "nfields out of range");
+    for (int i = 0; i < nio; i++)
+        if (!in[i] || !out[i]) return h3d_set_error_msg(-1, "hit3d_gpu_step_host: null field array");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    H3D_TRY(io_setup(c, nf));
+    const size_t fe = (size_t)c->n * c->n * c->nh;  // complex elements of one reference-layout field
+    const size_t width = (size_t)c->nh * sizeof(double2), hp = (size_t)ld1 * sizeof(double);
+    const size_t rows = (size_t)c->n * c->n;
+    auto copy = [&](void *dst, size_t dp, const void *src, size_t sp, cudaMemcpyKind kind, cudaStream_t s) {
+        return dp == sp && sp == width ? cudaMemcpyAsync(dst, src, width * rows, kind, s)
+                                       : cudaMemcpy2DAsync(dst, dp, src, sp, width, rows, kind, s);
+    };
+    auto upload = [&](int i) -> int {  // host in[i] -> sin, on the copy-in stream
+        H3D_CHECK(cudaStreamWaitEvent(c->cs_h2d, c->ev_in_free, 0));
+        for (int f = 0; f < nf; f++)
+            H3D_CHECK(copy(c->sin + f * fe, width, in[i] + (size_t)f * ld1 * rows, hp, cudaMemcpyHostToDevice, c->cs_h2d));
+        H3D_CHECK(cudaEventRecord(c->ev_in_ready, c->cs_h2d));
+        return 0;
+    };
+    // the staging buffers start free
+    H3D_CHECK(cudaEventRecord(c->ev_in_free, c->st));
+    H3D_CHECK(cudaEventRecord(c->ev_out_free, c->st));
+    H3D_TRY(upload(0));
+    int32_t ev = fov ? *fov : 0, es = fos ? *fos : 0;
+    for (int i = 0; i < nio; i++) {
+        // sin -> the state; then sin is free for the next upload, which runs
+        // while this state steps and downloads
+        H3D_CHECK(cudaStreamWaitEvent(c->st, c->ev_in_ready, 0));
+        for (int f = 0; f < nf; f++) {
+            k_ref_to_dev<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->sin + f * fe, c->U + f * c->fs64);
+            H3D_LAUNCH_CHECK();
+        }
+        H3D_CHECK(cudaEventRecord(c->ev_in_free, c->st));
+        if (i + 1 < nio) H3D_TRY(upload(i + 1));
+        c->alias_known = 0;
+        H3D_TRY(hit3d_gpu_step(c, nsteps, &ev, &es, nullptr));
+        // the state -> sout once the previous download has left it, then to the host
+        H3D_CHECK(cudaStreamWaitEvent(c->st, c->ev_out_free, 0));
+        for (int f = 0; f < nf; f++) {
+            k_dev_to_ref<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->U + f * c->fs64, c->sout + f * fe);
+            H3D_LAUNCH_CHECK();
+        }
+        H3D_CHECK(cudaEventRecord(c->ev_out_ready, c->st));
+        H3D_CHECK(cudaStreamWaitEvent(c->cs_d2h, c->ev_out_ready, 0));
+        for (int f = 0; f < nf; f++)
+            H3D_CHECK(copy(out[i] + (size_t)f * ld1 * rows, hp, c->sout + f * fe, width, cudaMemcpyDeviceToHost, c->cs_d2h));
+        H3D_CHECK(cudaEventRecord(c->ev_out_free, c->cs_d2h));
+    }
+    // the compute stream ends after the last download, so that events recorded
+    // on it afterwards time the whole call
+    H3D_CHECK(cudaStreamWaitEvent(c->st, c->ev_out_free, 0));
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    if (fov) *fov = ev;
+    if (fos) *fos = es;
+    return 0;
 }
 
 extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_t *fos, double *courant)

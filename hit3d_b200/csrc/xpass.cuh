@@ -183,7 +183,7 @@ template <typename T, template <class> class OP, int L> static int xfused_L(hit3
 template <typename T, template <class> class OP> int xfused(hit3d_ctx *c, FusedArgs a)
 {
     a.npairs = c->n * c->n / 2;
-    if (c->bruns > 1) {
+    if (c->bruns > 0) {
         // every run of a batch class: only the staged kernels walk the tiles of
         // several runs (variants 8-13); others take variant 13's
         if constexpr (OP<T>::NIN > 3) return h3d_set_error_msg(-1, "fused x pass: batch classes carry the velocity only");

@@ -109,6 +109,8 @@ SIGNATURES = [
     ("hit3d_gpu_upload_rhs_old", C.c_int, [_vp, _dp, _i64, _i32]),
     ("hit3d_gpu_download_rhs_old", C.c_int, [_vp, _dp, _i64, _i32]),
     ("hit3d_gpu_step", C.c_int, [_vp, _i32, C.POINTER(_i32), C.POINTER(_i32), _dp]),
+    ("hit3d_gpu_step_host", C.c_int, [_vp, _i32, C.POINTER(_dp), C.POINTER(_dp), _i64, _i32, _i32, C.POINTER(_i32),
+                                      C.POINTER(_i32)]),
     ("hit3d_gpu_stream", C.c_void_p, [_vp]),
     ("hit3d_gpu_launch_count", C.c_int64, [_vp]),
     ("hit3d_gpu_autotune", C.c_int, [_vp, C.POINTER(_i32), _dp]),
@@ -262,6 +264,24 @@ class Context:
         _check(lib().hit3d_gpu_step(self._h, int(nsteps), C.byref(fov), C.byref(fos), C.byref(cour)), "step")
         self.fov, self.fos, self.courant = fov.value, fos.value, cour.value
         return self.courant
+
+    def step_host(self, ins, outs, nsteps: int = 1):
+        """For each (in, out) pair of host arrays (field_shape()), upload `in`,
+        advance nsteps and download into `out`, the next upload overlapping this
+        step and download (hit3d_gpu_step_host).  Use pinned arrays for full rate."""
+        n = len(ins)
+        if n < 1 or len(outs) != n:
+            raise ValueError("step_host: ins and outs must be non-empty and of equal length")
+        nf = ins[0].shape[0]
+        for a in list(ins) + list(outs):
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.shape != ins[0].shape:
+                raise ValueError("step_host: C-contiguous float64 arrays of one shape")
+        pin = (_dp * n)(*[_ptr(a) for a in ins])
+        pout = (_dp * n)(*[_ptr(a) for a in outs])
+        fov, fos = C.c_int32(self.fov), C.c_int32(self.fos)
+        _check(lib().hit3d_gpu_step_host(self._h, n, pin, pout, self.n + 2, nf, int(nsteps), C.byref(fov),
+                                         C.byref(fos)), "step_host")
+        self.fov, self.fos = fov.value, fos.value
 
     STAGES = ["z_inverse", "y_inverse", "x_fused", "y_forward", "z_forward", "update", "smagorinsky", "other"]
 

@@ -108,6 +108,19 @@ int hit3d_gpu_download_rhs_old(hit3d_ctx *ctx, double *rhs_old, int64_t ld1, int
  * uploaded, move with the level-n velocity of every step (main.f90:235-247). */
 int hit3d_gpu_step(hit3d_ctx *ctx, int32_t nsteps, int32_t *fov, int32_t *fos, double *courant);
 
+/* Steps with host-owned fields, pipelined over PCIe (no counterpart in the
+ * reference, whose host owns `fields` and calls the step between copies,
+ * main.f90:124-167).  For i = 0..nio-1: upload in[i] (nf fields in the reference
+ * layout (ld1, ny, nz)), advance nsteps steps (flags as hit3d_gpu_step: the
+ * first step of the call takes *fov/*fos), download the state into out[i].  The
+ * upload of in[i+1] runs while step i and the download of out[i] run, on copy
+ * streams of their own, so the host-to-device and device-to-host copies overlap.
+ * in[i+1] must not share memory with out[i]; every array stays valid until the
+ * call returns, and pinned host memory gives the full PCIe rate.  The staging
+ * fields (2 nf fields in the reference layout) are allocated on first use. */
+int hit3d_gpu_step_host(hit3d_ctx *ctx, int32_t nio, const double *const *in, double *const *out, int64_t ld1,
+                        int32_t nf, int32_t nsteps, int32_t *fov, int32_t *fos);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, for
  * callers that time or order work around the library (the reference's
  * system_clock stage timers, m_timing.f90:48-73, x_fftw.f90:871-889). */
