@@ -150,9 +150,9 @@ struct hit3d_ctx {
     // pipelined host transfers (hit3d_gpu_step_host), created on first use: copy
     // streams, staging fields in the reference layout and their events
     cudaStream_t cs_h2d, cs_d2h;
-    double2 *sin, *sout;
-    int nstage_io;       // fields each staging buffer holds
-    cudaEvent_t ev_in_ready, ev_in_free, ev_out_ready, ev_out_free;
+    double2 *sin, *sout[2];  // one input staging set, two output sets used in turn
+    int nstage_io;           // fields each staging set holds
+    cudaEvent_t ev_in_ready, ev_in_free, ev_out_ready, ev_out_free[2];
     int ext_bufs;        // U, RO and W belong to a batch's slab
     int ctile;           // column-tile shape of the plain strided passes (ColCfgT), grids up to 128
     // while a batch class is being stepped through this context (its first

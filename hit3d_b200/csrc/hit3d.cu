@@ -990,10 +990,12 @@ extern "C" void hit3d_gpu_finalize(hit3d_ctx *c)
         cudaEventDestroy(c->ev_in_ready);
         cudaEventDestroy(c->ev_in_free);
         cudaEventDestroy(c->ev_out_ready);
-        cudaEventDestroy(c->ev_out_free);
+        cudaEventDestroy(c->ev_out_free[0]);
+        cudaEventDestroy(c->ev_out_free[1]);
     }
     if (c->sin) cudaFree(c->sin);
-    if (c->sout) cudaFree(c->sout);
+    if (c->sout[0]) cudaFree(c->sout[0]);
+    if (c->sout[1]) cudaFree(c->sout[1]);
     void *ptrs[] = {c->U, c->RO, c->RP, c->SP, c->W, c->phys, c->tw64, c->tw32, c->d_fen, c->d_part,
                     c->d_red, c->d_ratio, c->d_cmax, c->stage, c->d_xyz, c->d_uvw, c->sgs, c->mlp_wb,
                     c->d_mlp_err, c->d_kmin, c->gfilt, c->pfilt, c->pbuf};
@@ -1069,19 +1071,112 @@ static int io_setup(hit3d_ctx *c, int nf)
         H3D_CHECK(cudaEventCreateWithFlags(&c->ev_in_ready, cudaEventDisableTiming));
         H3D_CHECK(cudaEventCreateWithFlags(&c->ev_in_free, cudaEventDisableTiming));
         H3D_CHECK(cudaEventCreateWithFlags(&c->ev_out_ready, cudaEventDisableTiming));
-        H3D_CHECK(cudaEventCreateWithFlags(&c->ev_out_free, cudaEventDisableTiming));
+        H3D_CHECK(cudaEventCreateWithFlags(&c->ev_out_free[0], cudaEventDisableTiming));
+        H3D_CHECK(cudaEventCreateWithFlags(&c->ev_out_free[1], cudaEventDisableTiming));
     }
     if (c->nstage_io < nf) {
         H3D_CHECK(cudaStreamSynchronize(c->st));
-        if (c->sin) cudaFree(c->sin);
-        if (c->sout) cudaFree(c->sout);
-        c->sin = c->sout = nullptr;
+        H3D_CHECK(cudaStreamSynchronize(c->cs_h2d));
+        H3D_CHECK(cudaStreamSynchronize(c->cs_d2h));
+        for (double2 **q : {&c->sin, &c->sout[0], &c->sout[1]}) {
+            if (*q) cudaFree(*q);
+            *q = nullptr;
+        }
         c->nstage_io = 0;
         const size_t fe = (size_t)c->n * c->n * c->nh;
         H3D_TRY(ctx_alloc((void **)&c->sin, sizeof(double2) * fe * nf));
-        H3D_TRY(ctx_alloc((void **)&c->sout, sizeof(double2) * fe * nf));
+        H3D_TRY(ctx_alloc((void **)&c->sout[0], sizeof(double2) * fe * nf));
+        H3D_TRY(ctx_alloc((void **)&c->sout[1], sizeof(double2) * fe * nf));
         c->nstage_io = nf;
     }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// restart image in the reference's file layout (restart_io.f90:240-506)
+// ---------------------------------------------------------------------------
+static constexpr int64_t kRestartHeader = 36;  // 5 x int32 + 2 x float64
+
+static int restart_nles(const hit3d_ctx *c) { return les_nles(c->p.les_model); }
+
+extern "C" int64_t hit3d_gpu_restart_bytes(hit3d_ctx *c, int32_t nums)
+{
+    if (!c || nums < 0 || nums > c->p.n_scalars) return -1;
+    return kRestartHeader + (int64_t)(3 + nums + restart_nles(c)) * c->n * c->n * c->n * 8;
+}
+
+extern "C" int hit3d_gpu_restart_pack(hit3d_ctx *c, int32_t nums, double time, double dt, void *image)
+{
+    if (!c || !image) return h3d_set_error_msg(-1, "hit3d_gpu_restart_pack: null argument");
+    if (nums < 0 || nums > c->p.n_scalars)
+        return h3d_set_error_msg(-1, "hit3d_gpu_restart_pack: nums must be 0..n_scalars");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    const int nles = restart_nles(c);
+    unsigned char *img = static_cast<unsigned char *>(image);
+    const int32_t hdr[5] = {c->n, c->n, c->n, nums, nles};
+    memcpy(img, hdr, sizeof hdr);
+    memcpy(img + 20, &time, 8);
+    memcpy(img + 28, &dt, 8);
+    const size_t body = (size_t)c->n * c->n * c->n * 8;
+    // variables in file order: velocity, the nums scalars, the LES fields
+    const int nvar = 3 + nums + nles;
+    for (int v = 0; v < nvar; v++) {
+        const int field = v < 3 + nums ? v : 3 + c->p.n_scalars + (v - 3 - nums);
+        k_dev_to_restart<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->P64, c->U + field * c->fs64, c->stage);
+        H3D_LAUNCH_CHECK();
+        H3D_CHECK(cudaMemcpyAsync(img + kRestartHeader + v * body, c->stage, body, cudaMemcpyDeviceToHost, c->st));
+    }
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    return 0;
+}
+
+extern "C" int hit3d_gpu_restart_unpack(hit3d_ctx *c, const void *image, int64_t bytes, double *time, double *dt,
+                                        int32_t *nums_file, int32_t *nles_file)
+{
+    if (!c || !image) return h3d_set_error_msg(-1, "hit3d_gpu_restart_unpack: null argument");
+    if (bytes < kRestartHeader) return h3d_set_error_msg(-1, "hit3d_gpu_restart_unpack: truncated header");
+    const unsigned char *img = static_cast<const unsigned char *>(image);
+    int32_t hdr[5];
+    double t = 0.0, d = 0.0;
+    memcpy(hdr, img, sizeof hdr);
+    memcpy(&t, img + 20, 8);
+    memcpy(&d, img + 28, 8);
+    if (hdr[0] != c->n || hdr[1] != c->n || hdr[2] != c->n) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "hit3d_gpu_restart_unpack: Dimensions are different: input file %d^3, restart file %d %d %d",
+                 c->n, hdr[0], hdr[1], hdr[2]);
+        return h3d_set_error_msg(-1, buf);
+    }
+    const int nums = hdr[3], nles = hdr[4];
+    if (nums < 0 || nles < 0) return h3d_set_error_msg(-1, "hit3d_gpu_restart_unpack: corrupt header (negative counts)");
+    const size_t body = (size_t)c->n * c->n * c->n * 8;
+    if ((uint64_t)bytes != (uint64_t)kRestartHeader + (uint64_t)(3 + nums + nles) * body)
+        return h3d_set_error_msg(-1, "hit3d_gpu_restart_unpack: size does not match the header");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    const int ns = c->p.n_scalars, nl = restart_nles(c);
+    // the context's fields in order; each from the file or zero
+    // (restart_io.f90:408-448: extra scalars in the file are dropped, missing
+    // ones start from zero for the caller to initialise)
+    for (int f = 0; f < 3 + ns + nl; f++) {
+        int64_t v = -1;
+        if (f < 3) v = f;
+        else if (f < 3 + ns) v = (f - 3) < nums ? f : -1;
+        else v = (f - 3 - ns) < nles ? 3 + nums + (f - 3 - ns) : -1;
+        double2 *dst = c->U + f * c->fs64;
+        if (v < 0) {
+            H3D_CHECK(cudaMemsetAsync(dst, 0, sizeof(double2) * (size_t)c->fs64, c->st));
+            continue;
+        }
+        H3D_CHECK(cudaMemcpyAsync(c->stage, img + kRestartHeader + v * body, body, cudaMemcpyHostToDevice, c->st));
+        k_restart_to_dev<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->P64, c->stage, dst);
+        H3D_LAUNCH_CHECK();
+    }
+    H3D_CHECK(cudaStreamSynchronize(c->st));
+    c->alias_known = 0;
+    if (time) *time = t;
+    if (dt) *dt = d;
+    if (nums_file) *nums_file = nums;
+    if (nles_file) *nles_file = nles;
     return 0;
 }
 
@@ -1113,7 +1208,8 @@ extern "C" int hit3d_gpu_step_host(hit3d_ctx *c, int32_t nio, const double *cons
     };
     // the staging buffers start free
     H3D_CHECK(cudaEventRecord(c->ev_in_free, c->st));
-    H3D_CHECK(cudaEventRecord(c->ev_out_free, c->st));
+    H3D_CHECK(cudaEventRecord(c->ev_out_free[0], c->st));
+    H3D_CHECK(cudaEventRecord(c->ev_out_free[1], c->st));
     H3D_TRY(upload(0));
     int32_t ev = fov ? *fov : 0, es = fos ? *fos : 0;
     for (int i = 0; i < nio; i++) {
@@ -1128,21 +1224,24 @@ extern "C" int hit3d_gpu_step_host(hit3d_ctx *c, int32_t nio, const double *cons
         if (i + 1 < nio) H3D_TRY(upload(i + 1));
         c->alias_known = 0;
         H3D_TRY(hit3d_gpu_step(c, nsteps, &ev, &es, nullptr));
-        // the state -> sout once the previous download has left it, then to the host
-        H3D_CHECK(cudaStreamWaitEvent(c->st, c->ev_out_free, 0));
+        // the state -> output set i % 2 once the download two inputs back has
+        // left it, then to the host
+        const int ob = i & 1;
+        double2 *so = c->sout[ob];
+        H3D_CHECK(cudaStreamWaitEvent(c->st, c->ev_out_free[ob], 0));
         for (int f = 0; f < nf; f++) {
-            k_dev_to_ref<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->U + f * c->fs64, c->sout + f * fe);
+            k_dev_to_ref<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->U + f * c->fs64, so + f * fe);
             H3D_LAUNCH_CHECK();
         }
         H3D_CHECK(cudaEventRecord(c->ev_out_ready, c->st));
         H3D_CHECK(cudaStreamWaitEvent(c->cs_d2h, c->ev_out_ready, 0));
         for (int f = 0; f < nf; f++)
-            H3D_CHECK(copy(out[i] + (size_t)f * ld1 * rows, hp, c->sout + f * fe, width, cudaMemcpyDeviceToHost, c->cs_d2h));
-        H3D_CHECK(cudaEventRecord(c->ev_out_free, c->cs_d2h));
+            H3D_CHECK(copy(out[i] + (size_t)f * ld1 * rows, hp, so + f * fe, width, cudaMemcpyDeviceToHost, c->cs_d2h));
+        H3D_CHECK(cudaEventRecord(c->ev_out_free[ob], c->cs_d2h));
     }
     // the compute stream ends after the last download, so that events recorded
     // on it afterwards time the whole call
-    H3D_CHECK(cudaStreamWaitEvent(c->st, c->ev_out_free, 0));
+    H3D_CHECK(cudaStreamWaitEvent(c->st, c->ev_out_free[(nio - 1) & 1], 0));
     H3D_CHECK(cudaStreamSynchronize(c->st));
     if (fov) *fov = ev;
     if (fos) *fos = es;

@@ -29,10 +29,30 @@ constexpr int MLP_WPAD = (MLP_NPARAM + 3) / 4 * 4;                        // wei
 constexpr size_t MLP_SMEM = sizeof(float) * (MLP_WPAD + MLP_H * MLP_NT);  // + activation columns
 static_assert(MLP_W2 % 4 == 0 && MLP_W3 % 4 == 0, "float4 rows");
 
-H3D_D float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks and Gimpel, "Gaussian Error Linear Units",
+// 2016): gelu(z) = z/2 (1 + tanh(a (z + b z^3))), a = sqrt(2/pi), b = 0.044715;
+// the activation of the network, in training and inference
+constexpr float GELU_A = 0.79788456080286535588f, GELU_B = 0.044715f;
+H3D_D float gelu(float z)
+{
+    const float u = GELU_A * (z + GELU_B * (z * z * z));
+    return 0.5f * z * (1.0f + tanhf(u));
+}
 H3D_D float gelu_d(float z)
 {
-    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * expf(-0.5f * z * z) * 0.39894228040143268f;
+    const float u = GELU_A * (z + GELU_B * (z * z * z)), t = tanhf(u);
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * GELU_A * (1.0f + 3.0f * GELU_B * (z * z));
+}
+// the same with the hardware tanh approximation (tanh.approx.f32, one special
+// function unit instruction), for the tensor-core inference kernel, whose
+// activations are rounded to bf16 afterwards anyway
+H3D_D float gelu_fast(float z)
+{
+    const float u = GELU_A * z * fmaf(GELU_B, z * z, 1.0f);
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+    const float h = 0.5f * z;
+    return fmaf(h, t, h);
 }
 
 struct Feat {

@@ -4,10 +4,10 @@
 // two 64x64 hidden layers (92 % of the multiply-adds) run as
 //   D[128 x 64] (fp32, TMEM) = A[128 x 64] (bf16, smem) * W^T (bf16, smem)
 // with four tcgen05.mma of K = 16 each, issued by one thread and completed
-// through tcgen05.commit on an mbarrier.  The input layer (6 -> 64), the GELUs,
-// the output layer (64 -> 5) and the tensor basis stay on the CUDA cores in
-// fp32.  The activations that feed the tensor cores are rounded to bf16
-// (round to nearest even).
+// through tcgen05.commit on an mbarrier.  The input layer (6 -> 64), the GELUs
+// (tanh form with the hardware tanh approximation), the output layer (64 -> 5)
+// and the tensor basis stay on the CUDA cores in fp32.  The activations that feed
+// the tensor cores are rounded to bf16 (round to nearest even).
 //
 // Shared-memory operands use the no-swizzle K-major canonical layout: 8 x 8
 // "core matrices" of 128 contiguous bytes (row r at 16 r bytes, element k at
@@ -99,8 +99,8 @@ H3D_D void store_act_row(unsigned char *sA, int r, const float *acc, const float
         uint32_t w[4];
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-            const float lo = gelu(acc[8 * c + 2 * e] + b[8 * c + 2 * e]);
-            const float hi = gelu(acc[8 * c + 2 * e + 1] + b[8 * c + 2 * e + 1]);
+            const float lo = gelu_fast(acc[8 * c + 2 * e] + b[8 * c + 2 * e]);
+            const float hi = gelu_fast(acc[8 * c + 2 * e + 1] + b[8 * c + 2 * e + 1]);
             const __nv_bfloat162 h2 = __floats2bfloat162_rn(lo, hi);
             w[e] = *reinterpret_cast<const uint32_t *>(&h2);
         }
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(TC_TILE) k_mlp_apply_tc(int64_t np, int64_t n,
         store_act_row(sm + TC_OFF_A, tid, acc, F + TCF_B2);
         ok &= tc_layer(sm, sW3, tmem, sbar, phase, acc);
 #pragma unroll
-        for (int j = 0; j < MLP_H; j++) acc[j] = gelu(acc[j] + F[TCF_B3 + j]);
+        for (int j = 0; j < MLP_H; j++) acc[j] = gelu_fast(acc[j] + F[TCF_B3 + j]);
         float g[MLP_OUT], tau[MLP_TC];
 #pragma unroll
         for (int q = 0; q < MLP_OUT; q++) {

@@ -1091,6 +1091,33 @@ __global__ void k_sgs_tau(int n, int64_t rp, int64_t fs, const double *__restric
     }
 }
 
+// restart body (restart_io.f90:240-334): each variable's Fourier array without
+// its last two rows (the kx = N/2 pair), i.e. [ky][kz][kx < N/2] complex; to and
+// from the device layout [kz][ky][kx] (pitch P).  The unpacked kx = N/2 modes
+// are zero (every dealiasing rule zeroes them).
+__global__ void k_dev_to_restart(int n, int pitch, const double2 *__restrict__ D, double2 *__restrict__ R)
+{
+    const int nk = n / 2;
+    const int64_t nm = (int64_t)n * n * nk;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        const int kx = (int)(t % nk);
+        const int64_t r = t / nk;
+        const int kzi = (int)(r % n), kyi = (int)(r / n);
+        R[t] = D[((int64_t)kzi * n + kyi) * pitch + kx];
+    }
+}
+__global__ void k_restart_to_dev(int n, int pitch, const double2 *__restrict__ R, double2 *__restrict__ D)
+{
+    const int nk = n / 2, nh = nk + 1;
+    const int64_t nm = (int64_t)n * n * nh;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        const int kx = (int)(t % nh);
+        const int64_t r = t / nh;
+        const int kzi = (int)(r % n), kyi = (int)(r / n);
+        D[((int64_t)kzi * n + kyi) * pitch + kx] = kx < nk ? R[((int64_t)kyi * n + kzi) * nk + kx] : make_double2(0.0, 0.0);
+    }
+}
+
 // layout conversion between the reference's (nx+2, ny, nz) Fourier array
 // [ky][kz][kx] (pitch nh) and the device layout [kz][ky][kx] (pitch P)
 __global__ void k_ref_to_dev(int n, int nh, int pitch, const double2 *__restrict__ R, double2 *__restrict__ D)

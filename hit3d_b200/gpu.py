@@ -111,6 +111,9 @@ SIGNATURES = [
     ("hit3d_gpu_step", C.c_int, [_vp, _i32, C.POINTER(_i32), C.POINTER(_i32), _dp]),
     ("hit3d_gpu_step_host", C.c_int, [_vp, _i32, C.POINTER(_dp), C.POINTER(_dp), _i64, _i32, _i32, C.POINTER(_i32),
                                       C.POINTER(_i32)]),
+    ("hit3d_gpu_restart_bytes", C.c_int64, [_vp, _i32]),
+    ("hit3d_gpu_restart_pack", C.c_int, [_vp, _i32, _d, _d, C.c_void_p]),
+    ("hit3d_gpu_restart_unpack", C.c_int, [_vp, C.c_void_p, _i64, _dp, _dp, C.POINTER(_i32), C.POINTER(_i32)]),
     ("hit3d_gpu_stream", C.c_void_p, [_vp]),
     ("hit3d_gpu_launch_count", C.c_int64, [_vp]),
     ("hit3d_gpu_autotune", C.c_int, [_vp, C.POINTER(_i32), _dp]),
@@ -282,6 +285,28 @@ class Context:
         _check(lib().hit3d_gpu_step_host(self._h, n, pin, pout, self.n + 2, nf, int(nsteps), C.byref(fov),
                                          C.byref(fos)), "step_host")
         self.fov, self.fos = fov.value, fos.value
+
+    def restart_image(self, time: float, dt: float, nums: int | None = None) -> np.ndarray:
+        """The restart file's bytes (header + Fourier body, restart_io.f90:240-334),
+        packed on the device; nums passive scalars (default: all)."""
+        nums = self.p.n_scalars if nums is None else int(nums)
+        nb = int(lib().hit3d_gpu_restart_bytes(self._h, nums))
+        if nb < 0:
+            raise Hit3dError("restart_image: nums out of range")
+        img = np.empty(nb, dtype=np.uint8)
+        _check(lib().hit3d_gpu_restart_pack(self._h, nums, float(time), float(dt), img.ctypes.data_as(C.c_void_p)),
+               "restart_pack")
+        return img
+
+    def restart_load(self, image) -> tuple:
+        """Load a restart file's bytes (restart_io.f90:341-506); returns (time, dt,
+        nums in the file, nles in the file).  Scalars the file lacks are zero."""
+        img = np.ascontiguousarray(np.frombuffer(image, dtype=np.uint8) if not isinstance(image, np.ndarray) else image)
+        t, d = C.c_double(0.0), C.c_double(0.0)
+        nums, nles = C.c_int32(0), C.c_int32(0)
+        _check(lib().hit3d_gpu_restart_unpack(self._h, img.ctypes.data_as(C.c_void_p), img.nbytes, C.byref(t),
+                                              C.byref(d), C.byref(nums), C.byref(nles)), "restart_unpack")
+        return t.value, d.value, nums.value, nles.value
 
     STAGES = ["z_inverse", "y_inverse", "x_fused", "y_forward", "z_forward", "update", "smagorinsky", "other"]
 

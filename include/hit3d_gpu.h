@@ -108,6 +108,26 @@ int hit3d_gpu_download_rhs_old(hit3d_ctx *ctx, double *rhs_old, int64_t ld1, int
  * uploaded, move with the level-n velocity of every step (main.f90:235-247). */
 int hit3d_gpu_step(hit3d_ctx *ctx, int32_t nsteps, int32_t *fov, int32_t *fos, double *courant);
 
+/* Restart image in the reference's file layout, packed on the device
+ * (restart_io.f90:240-334, restart_write_parallel): the 36-byte header (nx, ny,
+ * nz, nums, nles as int32; TIME and DT as float64) followed, per variable, by the
+ * Fourier array's first nx of its nx+2 rows ((nx, ny, nz) float64, column-major),
+ * for the velocity, the first `nums` passive scalars (0..n_scalars; the host loop
+ * writes 0 until the scalars are switched on) and the LES fields.  `image`: host
+ * memory of hit3d_gpu_restart_bytes(ctx, nums) bytes (-1 on bad arguments); one
+ * device-to-host copy per variable, no host re-layout.  The host writes the image
+ * to <run_name>.64.<itime> as is. */
+int64_t hit3d_gpu_restart_bytes(hit3d_ctx *ctx, int32_t nums);
+int hit3d_gpu_restart_pack(hit3d_ctx *ctx, int32_t nums, double time, double dt, void *image);
+/* The inverse (restart_read_parallel, restart_io.f90:341-506): checks the header's
+ * dimensions against the context (the error names both) and the image size
+ * against the header, loads the velocity, min(nums, n_scalars) scalars and
+ * min(nles, the context's) LES fields, and zeroes the fields the image lacks
+ * (the caller initialises added scalars, as init_scalar does in the reference)
+ * and every kx = N/2 mode.  Returns TIME, DT and the header's counts. */
+int hit3d_gpu_restart_unpack(hit3d_ctx *ctx, const void *image, int64_t bytes, double *time, double *dt,
+                             int32_t *nums_file, int32_t *nles_file);
+
 /* Steps with host-owned fields, pipelined over PCIe (no counterpart in the
  * reference, whose host owns `fields` and calls the step between copies,
  * main.f90:124-167).  For i = 0..nio-1: upload in[i] (nf fields in the reference
@@ -117,7 +137,8 @@ int hit3d_gpu_step(hit3d_ctx *ctx, int32_t nsteps, int32_t *fov, int32_t *fos, d
  * streams of their own, so the host-to-device and device-to-host copies overlap.
  * in[i+1] must not share memory with out[i]; every array stays valid until the
  * call returns, and pinned host memory gives the full PCIe rate.  The staging
- * fields (2 nf fields in the reference layout) are allocated on first use. */
+ * fields (3 nf fields in the reference layout: one input set, two output sets
+ * used in turn) are allocated on first use. */
 int hit3d_gpu_step_host(hit3d_ctx *ctx, int32_t nio, const double *const *in, double *const *out, int64_t ld1,
                         int32_t nf, int32_t nsteps, int32_t *fov, int32_t *fos);
 

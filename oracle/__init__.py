@@ -90,6 +90,8 @@ def lib():
         L.oracle_particles_lattice.argtypes = [C.c_int, C.c_int64, dp]
         L.oracle_filter_g.argtypes = [vp, C.c_int, C.c_double, dp]
         L.oracle_apply_filter.argtypes = [vp, dp, dp]
+        L.oracle_read_restart.restype = C.c_int
+        L.oracle_read_restart.argtypes = [vp, C.c_char_p, dp, dp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         _lib = L
     return _lib
 
@@ -255,6 +257,18 @@ class Oracle:
         g = np.zeros((self.n, self.n, self.n + 2))
         lib().oracle_filter_g(self._p, int(kind), float(delta), _dp(g))
         return g
+
+    def read_restart(self, path):
+        """restart_read_parallel (restart_io.f90:341-506) into this oracle's fields;
+        returns (time, dt, nums_in_file, nles_in_file)."""
+        t, d = C.c_double(0.0), C.c_double(0.0)
+        nums, nles = C.c_int(0), C.c_int(0)
+        rc = lib().oracle_read_restart(self._p, os.fsencode(path), C.byref(t), C.byref(d), C.byref(nums), C.byref(nles))
+        if rc == -2:
+            raise ValueError("Dimensions are different")
+        if rc != 0:
+            raise OSError(f"cannot read restart file {path}")
+        return t.value, d.value, nums.value, nles.value
 
     def apply_filter(self, g, a):
         lib().oracle_apply_filter(self._p, _dp(g), _dp(a))

@@ -505,6 +505,54 @@ double *oracle_fields(oracle_t *o) { return o->fields; }
 double *oracle_rhs_old(oracle_t *o) { return o->rhs_old; }
 double *oracle_wrk(oracle_t *o) { return o->wrk; }
 int oracle_nwrk(oracle_t *o) { return o->nwrk; }
+
+/* restart_read_parallel (restart_io.f90:341-506), one task: the 36-byte header
+ * (nx, ny, nz, nums, nles as int32, TIME and DT as float64), a dimension check,
+ * then rows 1..nx of every variable into fields(1:nx, :, :, n) for the velocity
+ * and min(nums, n_scalars) scalars, and the LES variables from after the file's
+ * nums scalars.  Rows nx+1, nx+2 and fields the file lacks are zeroed (the
+ * reference initialises added scalars afterwards; the caller does that here).
+ * Returns 0, or -1 (no file / short read), -2 (dimensions differ). */
+int oracle_read_restart(oracle_t *o, const char *path, double *time, double *dt, int *nums_file, int *nles_file)
+{
+    FILE *f = fopen(path, "rb");
+    if (!f) return -1;
+    int32_t h[5];
+    double td[2];
+    if (fread(h, 4, 5, f) != 5 || fread(td, 8, 2, f) != 2) { fclose(f); return -1; }
+    const int n = o->n;
+    if (h[0] != n || h[1] != n || h[2] != n) { fclose(f); return -2; }
+    const int nums1 = h[3], nles1 = h[4];
+    const size_t fsz = o->fsz, per = (size_t)n * n * n;
+    double *tmp = (double *)malloc(sizeof(double) * per);
+    if (!tmp) { fclose(f); return -1; }
+    memset(o->fields, 0, sizeof(double) * fsz * (size_t)(3 + o->nscal + o->nles));
+    const int nread = 3 + (o->nscal < nums1 ? o->nscal : nums1);
+    int rc = 0;
+    for (int v = 0; v < nread + o->nles && rc == 0; v++) {
+        int field, var;
+        if (v < nread) { field = v; var = v; }
+        else {
+            const int j = v - nread;
+            if (j >= nles1) break;
+            field = 3 + o->nscal + j;
+            var = 3 + nums1 + j;
+        }
+        if (fseek(f, 36 + (long)var * (long)(per * 8), SEEK_SET) != 0 || fread(tmp, 8, per, f) != per) { rc = -1; break; }
+        double *dst = o->fields + (size_t)field * fsz;
+        for (size_t row = 0; row < (size_t)n * n; row++)
+            memcpy(dst + row * (size_t)(n + 2), tmp + row * (size_t)n, sizeof(double) * (size_t)n);
+    }
+    free(tmp);
+    fclose(f);
+    if (rc == 0) {
+        if (time) *time = td[0];
+        if (dt) *dt = td[1];
+        if (nums_file) *nums_file = nums1;
+        if (nles_file) *nles_file = nles1;
+    }
+    return rc;
+}
 void oracle_set_reaction(oracle_t *o, int s, double rate) { o->reac[s] = rate; }
 /* C_T of les_model 5 (c_t.in) and C_mixed of les_models 6, 7 (c_mixed.in) */
 void oracle_set_les_constants(oracle_t *o, double c_t, double c_mixed) { o->c_t = c_t; o->c_mixed = c_mixed; }

@@ -20,7 +20,6 @@ Conventions (shared with the kernels):
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 NIN, NH, NOUT = 6, 64, 5
 SHAPES = [("W1", (NH, NIN)), ("b1", (NH,)), ("W2", (NH, NH)), ("b2", (NH,)), ("W3", (NH, NH)), ("b3", (NH,)),
@@ -55,12 +54,17 @@ def pack(d) -> np.ndarray:
     return np.concatenate([np.asarray(d[name], dtype=np.float64).ravel() for name, _ in SHAPES])
 
 
+GELU_A, GELU_B = np.sqrt(2.0 / np.pi), 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    """GELU in its tanh form (Hendrycks and Gimpel 2016), the network's activation."""
+    return 0.5 * z * (1.0 + np.tanh(GELU_A * (z + GELU_B * z ** 3)))
 
 
 def gelu_d(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(GELU_A * (z + GELU_B * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_A * (1.0 + 3.0 * GELU_B * z * z)
 
 
 def features(A, delta):

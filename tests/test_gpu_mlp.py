@@ -58,8 +58,15 @@ def test_predict_matches_oracle(clip):
 
 def test_tensor_core_predict_matches_oracle():
     """Hidden layers on the tensor cores (bf16 activations, fp32 accumulation in
-    TMEM): against the oracle with the same bf16 rounding of the activations, on a
-    ragged point count that spans several tiles per CTA."""
+    TMEM), GELUs with the hardware tanh approximation: against the oracle with the
+    same bf16 rounding of the activations and the exact tanh, on a ragged point
+    count that spans several tiles per CTA.
+
+    Bound: tanh.approx.f32 differs from tanh by up to about 2^-11, which moves an
+    activation by far less than one bf16 step (2^-8 relative) but decides some
+    bf16 roundings differently; a point's stress then moves by a fraction of a
+    bf16 step.  Stated: 99.9 % of points within 2e-3 of the largest stress, every
+    point within 2e-2."""
     np_ = 300001
     A, _ = mo.synthetic_data(np_, seed=13)
     w = mo.bf16_round(mo.init_params(21)).astype(np.float64)
@@ -68,15 +75,15 @@ def test_tensor_core_predict_matches_oracle():
     ref = mo.predict(w, A, DELTA, act_bf16=True)
     scale = np.abs(ref).max()
     err = np.abs(got - ref).max(axis=0) / scale
-    # a bf16 rounding decided differently by the last fp32 bit of an activation
-    # moves a point by about one bf16 step; everything else agrees to fp32 accuracy
-    assert np.quantile(err, 0.999) < 2e-5 and err.max() < 5e-3, (np.quantile(err, 0.999), err.max())
+    print(f"tensor-core closure vs oracle: median {np.median(err):.2e}, 99.9 % {np.quantile(err, 0.999):.2e}, "
+          f"max {err.max():.2e}")
+    assert np.quantile(err, 0.999) < 2e-3 and err.max() < 2e-2, (np.quantile(err, 0.999), err.max())
     # and the fp32-activation kernel agrees to bf16 accuracy
     exact = m.predict(A, DELTA, clip=False, kernel=0)
     assert np.abs(exact - got).max() < 2e-2 * scale
     got_clip = m.predict(A, DELTA, clip=True, kernel=1)
     ref_clip = mo.predict(w, A, DELTA, clip=True, act_bf16=True)
-    agree = np.all(np.abs(got_clip - ref_clip) <= 5e-3 * scale, axis=0)
+    agree = np.all(np.abs(got_clip - ref_clip) <= 2e-2 * scale, axis=0)
     assert agree.mean() > 0.999
     m.close()
 
