@@ -21,7 +21,7 @@ import numpy as np
 
 from .gpu import Context, les_fields
 from .params import InputFileError, RunConfig, read_input_file
-from .restart import read_restart, restart_name, write_real4, write_restart
+from .restart import read_restart_header, restart_name, write_real4
 from . import particles as _pt
 from .sidecar import GpuSettings, SidecarError, read_sidecar
 
@@ -146,9 +146,12 @@ class Simulation:
             self.io_write_4()
         else:
             self.itime = c.itmin
-            f, self.time, dt, nums1, _ = read_restart(
-                os.path.join(self.wd, restart_name(self.run_name, c.itmin)), c.nx, c.n_scalars, self.n_les)
-            self.ctx.upload_fields(f)
+            path = os.path.join(self.wd, restart_name(self.run_name, c.itmin))
+            # the header is checked on the host first, so that a bad file is
+            # reported by name before anything reaches the device
+            read_restart_header(path, c.nx)
+            with open(path, "rb") as fh:
+                self.time, dt, nums1, _ = self.ctx.restart_load(np.frombuffer(fh.read(), dtype=np.uint8))
             # scalars the .in file has beyond the file's count start from their
             # initial condition (restart_io.f90:419-432)
             for s in range(min(nums1, c.n_scalars), c.n_scalars):
@@ -217,11 +220,14 @@ class Simulation:
         return les_fields(self.cfg.les_model)
 
     def write_restart(self):
+        """restart_write_parallel: the file image is packed on the device
+        (hit3d_gpu_restart_pack) and written as is, through a temporary name."""
         nums = self.cfg.n_scalars if self.int_scalars else 0
-        f = self.ctx.download_fields(self.ctx.nfields)
-        keep = list(range(3 + nums)) + list(range(3 + self.cfg.n_scalars, 3 + self.cfg.n_scalars + self.n_les))
-        write_restart(os.path.join(self.wd, restart_name(self.run_name, self.itime)),
-                      np.ascontiguousarray(f[keep]), self.time, self.cfg.dt, nums, self.n_les)
+        path = os.path.join(self.wd, restart_name(self.run_name, self.itime))
+        img = self.ctx.restart_image(self.time, self.cfg.dt, nums)
+        with open(path + ".part", "wb") as f:
+            f.write(img.tobytes())
+        os.replace(path + ".part", path)
 
     def stat_main(self):
         es, st = self.ctx.stats()

@@ -289,7 +289,7 @@ class Context:
     def restart_image(self, time: float, dt: float, nums: int | None = None) -> np.ndarray:
         """The restart file's bytes (header + Fourier body, restart_io.f90:240-334),
         packed on the device; nums passive scalars (default: all)."""
-        nums = self.p.n_scalars if nums is None else int(nums)
+        nums = self.params.n_scalars if nums is None else int(nums)
         nb = int(lib().hit3d_gpu_restart_bytes(self._h, nums))
         if nb < 0:
             raise Hit3dError("restart_image: nums out of range")

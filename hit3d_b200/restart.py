@@ -39,6 +39,24 @@ def write_restart(path: str, fields: np.ndarray, time: float, dt: float, nums: i
     os.replace(tmp, path)
 
 
+def read_restart_header(path: str, nx: int):
+    """Header of a restart file, checked against the grid and the file size:
+    (nx, ny, nz, nums, nles, time, dt)."""
+    size = os.path.getsize(path)
+    if size < HEADER.size:
+        raise RestartError(f"{path}: truncated header")
+    with open(path, "rb") as f:
+        h = HEADER.unpack(f.read(HEADER.size))
+    nx1, ny1, nz1, nums1, nles1 = h[:5]
+    if (nx1, ny1, nz1) != (nx, nx, nx):
+        raise RestartError(f"Dimensions are different: input file {nx}^3, restart file {nx1} {ny1} {nz1}")
+    if nums1 < 0 or nles1 < 0:
+        raise RestartError("corrupt header (negative counts)")
+    if size != HEADER.size + (3 + nums1 + nles1) * nx * nx * nx * 8:
+        raise RestartError(f"{path}: size {size} does not match its header")
+    return h
+
+
 def read_restart(path: str, nx: int, n_scalars: int, n_les: int = 0):
     """Return (fields (3 + n_scalars + n_les, nx, nx, nx + 2), time, dt, nums_in_file, nles_in_file).
 

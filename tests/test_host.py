@@ -198,3 +198,21 @@ def test_particle_trajectory_line_format(tmp_path):
     vals = [float(line[11 + 16 * k: 11 + 16 * (k + 1)]) for k in range(7)]
     dx = 2 * np.pi / 32
     assert np.allclose(vals, [0.06, 0.0, dx, 2 * dx, 0.5, -0.25, 1e-3], rtol=1e-7)
+
+
+def test_restart_header_checks(tmp_path):
+    from hit3d_b200.restart import read_restart_header
+    f = np.zeros((4, 8, 8, 10))
+    p = str(tmp_path / "r")
+    write_restart(p, f, 2.5, 0.01, 1)
+    assert read_restart_header(p, 8) == (8, 8, 8, 1, 0, 2.5, 0.01)
+    with pytest.raises(RestartError, match="Dimensions"):
+        read_restart_header(p, 16)
+    with open(p, "ab") as fh:
+        fh.write(b"\0" * 8)
+    with pytest.raises(RestartError, match="size"):
+        read_restart_header(p, 8)
+    with open(p, "wb") as fh:
+        fh.write(b"\0" * 12)
+    with pytest.raises(RestartError, match="truncated"):
+        read_restart_header(p, 8)
