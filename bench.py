@@ -618,6 +618,7 @@ def main():
             v32, v32_ms = args.variant, []
         else:
             v32, v32_ms = c32.autotune()
+        t32, t32_ms = getattr(c32, "column_tile", 0), getattr(c32, "column_ms", [])
         c32.step(args.warmup)
         if dist:
             dist.barrier()
@@ -634,7 +635,8 @@ def main():
                 "ek_max_rel_err_vs_fp64": ek_err, "eps_rel_err": abs(st32["eps_v"] - st64["eps_v"]) / st64["eps_v"],
                 "skew_abs_err": abs(st32["skewness"] - st64["skewness"]),
                 "stage_ms": {k: round(v / 3, 3) for k, v in prof32.items() if v > 0},
-                "tuned_variant": v32, "variant_ms": [round(x, 3) for x in v32_ms]}
+                "tuned_variant": v32, "variant_ms": [round(x, 3) for x in v32_ms],
+                "column_tile": t32, "column_ms": [round(x, 3) for x in t32_ms]}
         # error per statistic against the FP64 path every cmp_every steps from the same state
         c32.upload_fields(fields0)
         c32.fov = c32.fos = 1
@@ -691,6 +693,8 @@ def main():
             "stage_ms": {k: round(v, 3) for k, v in prof.items() if v > 0},
             "stage_GBs": stage_gbs,
             "tuned_variant": variant, "variant_ms": [round(x, 3) for x in variant_ms],
+            "column_tile": getattr(ctx, "column_tile", 0),
+            "column_ms": [round(x, 3) for x in getattr(ctx, "column_ms", [])],
             "clocks": clk.summary(),
             "e2e": e2e,
             "fp32_fft": fp32,

@@ -154,7 +154,7 @@ struct hit3d_ctx {
     int nstage_io;           // fields each staging set holds
     cudaEvent_t ev_in_ready, ev_in_free, ev_out_ready, ev_out_free[2];
     int ext_bufs;        // U, RO and W belong to a batch's slab
-    int ctile;           // column-tile shape of the plain strided passes (ColCfgT), grids up to 128
+    int ctile;           // column-tile shape of the plain strided passes (ColCfgT), grids up to 512
     // while a batch class is being stepped through this context (its first
     // run): the number of runs, and the run strides of the state (complex FP64
     // elements) and of the work fields (elements of the transform precision)

@@ -65,19 +65,19 @@ static int zinv_LMC(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_
         io.rs_dst = c->brw;
         nz = nf * c->bruns;
     }
-    auto k = k_colfft<T, L, CF::TC, CF::NT, false, IO>;
+    auto k = k_colfft<T, L, CF::TC, CF::NT, false, IO, CF::MINB>;
     H3D_TRY(set_smem(k, CF::SMEM));
     dim3 g((io.ncol + CF::TC - 1) / CF::TC, rows, nz);
     k<<<g, CF::NT, CF::SMEM, c->st>>>(io, twid<T>(c));
     H3D_LAUNCH_CHECK();
     return 0;
 }
-// the tuned column tile (ctile) applies to the plain copy of grids up to 128
+// the tuned column tile (ctile) applies to the plain copy of grids up to 512
 template <typename T, int L, int MODE>
 static int zinv_LM(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_t src_fs, cx<T> *dst,
                    int64_t dst_fs, int dpitch)
 {
-    if constexpr (L <= 128 && MODE == PRE_COPY) {
+    if constexpr (L <= 512 && MODE == PRE_COPY) {
         if (c->ctile == 1) return zinv_LMC<T, L, MODE, 1>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         if (c->ctile == 2) return zinv_LMC<T, L, MODE, 2>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
     }
@@ -148,11 +148,11 @@ static int spass_LAC(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, 
     }
     dim3 g((io.ncol + CF::TC - 1) / CF::TC, rows, nz);
     if (fwd) {
-        auto k = k_colfft<T, L, CF::TC, CF::NT, true, IOPlain<T, T, T>>;
+        auto k = k_colfft<T, L, CF::TC, CF::NT, true, IOPlain<T, T, T>, CF::MINB>;
         H3D_TRY(set_smem(k, CF::SMEM));
         k<<<g, CF::NT, CF::SMEM, c->st>>>(io, twid<T>(c));
     } else {
-        auto k = k_colfft<T, L, CF::TC, CF::NT, false, IOPlain<T, T, T>>;
+        auto k = k_colfft<T, L, CF::TC, CF::NT, false, IOPlain<T, T, T>, CF::MINB>;
         H3D_TRY(set_smem(k, CF::SMEM));
         k<<<g, CF::NT, CF::SMEM, c->st>>>(io, twid<T>(c));
     }
@@ -162,7 +162,7 @@ static int spass_LAC(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, 
 template <typename T, int L, bool YPASS>
 static int spass_LA(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, int pitch, int nf)
 {
-    if constexpr (L <= 128) {
+    if constexpr (L <= 512) {
         if (c->ctile == 1) return spass_LAC<T, L, YPASS, 1>(c, axis, fwd, base, fs, pitch, nf);
         if (c->ctile == 2) return spass_LAC<T, L, YPASS, 2>(c, axis, fwd, base, fs, pitch, nf);
     }
@@ -1400,6 +1400,60 @@ extern "C" int hit3d_gpu_autotune(hit3d_ctx *c, int32_t *variant, double *ms_out
     return 0;
 }
 
+// time the strided passes of one step (z and y inverse of the velocity, y and z
+// forward of the six products) in the current column tile; the state is read,
+// only the work fields are written
+template <typename T> static int time_columns(hit3d_ctx *c, float *ms)
+{
+    PruneScope prune_scope(c);
+    cx<T> *W = reinterpret_cast<cx<T> *>(c->W);
+    const int64_t wfs = c->wfs;
+    const int wp = c->wpitch;
+    auto go = [&]() -> int {
+        H3D_TRY(zinv<T>(c, 3, PRE_COPY, 0, c->U, c->fs64, W, wfs, wp));
+        H3D_TRY(spass<T>(c, 1, false, W, wfs, wp, 3));
+        H3D_TRY(spass<T>(c, 1, true, W, wfs, wp, 6));
+        H3D_TRY(spass<T>(c, 2, true, W, wfs, wp, 6));
+        return 0;
+    };
+    EventPair ev;
+    H3D_CHECK(ev.create());
+    H3D_TRY(go());  // warm-up
+    H3D_CHECK(cudaEventRecord(ev.e0, c->st));
+    for (int r = 0; r < 3; r++) H3D_TRY(go());
+    H3D_CHECK(cudaEventRecord(ev.e1, c->st));
+    H3D_CHECK(cudaEventSynchronize(ev.e1));
+    H3D_CHECK(cudaEventElapsedTime(ms, ev.e0, ev.e1));
+    *ms /= 3.0f;
+    return 0;
+}
+
+extern "C" int hit3d_gpu_autotune_columns(hit3d_ctx *c, int32_t *tile, double *ms_out)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    H3D_CHECK(cudaSetDevice(c->dev));
+    H3D_TRY(ensure_alias_state(c));
+    if (c->nw < 6) return h3d_set_error_msg(-1, "hit3d_gpu_autotune_columns: the context has fewer than six work fields");
+    int best = 0;
+    float bt = 1e30f;
+    for (int ct = 0; ct < kColTiles; ct++) {
+        if (ms_out) ms_out[ct] = 0.0;
+        if (c->n > 512 && ct > 0) continue;
+        c->ctile = ct;
+        float ms = 0.f;
+        const int rc = c->p.precision == 0 ? time_columns<double>(c, &ms) : time_columns<float>(c, &ms);
+        if (rc) {
+            c->ctile = 0;
+            return rc;
+        }
+        if (ms_out) ms_out[ct] = ms;
+        if (ms < bt) { bt = ms; best = ct; }
+    }
+    c->ctile = best;
+    if (tile) *tile = best;
+    return 0;
+}
+
 extern "C" int hit3d_gpu_check_finite(hit3d_ctx *c, int64_t *nonfinite)
 {
     if (!c || !nonfinite) return h3d_set_error_msg(-1, "hit3d_gpu_check_finite: null argument");
@@ -2285,7 +2339,7 @@ extern "C" int hit3d_batch_autotune(hit3d_batch *b, int32_t *choice, double *ms)
         bt = 1e30f;
         if (mq)
             for (int ct = 0; ct < kColTiles; ct++) mq[kBatchVariants + ct] = 0.0;
-        for (int ct = 0; ct < (c->n <= 128 ? kColTiles : 1); ct++) {
+        for (int ct = 0; ct < (c->n <= 512 ? kColTiles : 1); ct++) {
             c->ctile = ct;
             float t = 0.f;
             H3D_TRY(class_time(b, k, 1, &t));

@@ -2,7 +2,7 @@
 // translation unit that launches them (the context path and the allocation-free
 // entry point), so that both run the configurations the tests cover.
 #pragma once
-#include "fft.cuh"
+#include "passes.cuh"
 
 H3D_HD constexpr int plan_rmax(int L)
 {
@@ -28,7 +28,7 @@ template <typename T, int L> struct RowCfg {
     static constexpr size_t SMEM = (size_t)Lay<L, TC, true>::elems * sizeof(cx<T>);
 };
 
-// Column-tile shapes the batch tuner picks from for grids up to 128 (ct = the
+// Column-tile shapes the tuners pick from for grids up to 512 (ct = the
 // context's `ctile`): 0 the default ColCfg, 1 half as many kx columns per CTA,
 // 2 twice as many; at least one warp per CTA
 constexpr int kColTiles = 3;
@@ -38,4 +38,7 @@ template <typename T, int L, bool YPASS, int CT> struct ColCfgT {
     static constexpr int NT0 = TC * L / plan_rmax(L);
     static constexpr int NT = CT == 0 ? B::NT : NT0 < 32 ? 32 : NT0 > 512 ? 512 : NT0;
     static constexpr size_t SMEM = (size_t)Lay<L, TC, false>::elems * sizeof(cx<T>);
+    // resident CTAs the register cap allows: the default shape's, or four for
+    // the narrow tiles of up to 256 threads and 56 KB
+    static constexpr int MINB = CT == 1 && NT <= 256 && SMEM <= 56 * 1024 ? 4 : ColMinBlocks<T, L, TC, NT>::value;
 };

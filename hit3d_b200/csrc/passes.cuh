@@ -194,8 +194,8 @@ template <typename T, int L, int TC, int NT> struct ColMinBlocks {
     static constexpr int value = (NT >= 128 && (size_t)TC * L * sizeof(cx<T>) <= 112 * 1024) ? 2 : 1;
 };
 
-template <typename T, int L, int TC, int NT, bool FWD, class IO>
-__global__ void __launch_bounds__(NT, (ColMinBlocks<T, L, TC, NT>::value)) k_colfft(const IO io, const cx<T> *__restrict__ tw)
+template <typename T, int L, int TC, int NT, bool FWD, class IO, int MINB = ColMinBlocks<T, L, TC, NT>::value>
+__global__ void __launch_bounds__(NT, MINB) k_colfft(const IO io, const cx<T> *__restrict__ tw)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);

@@ -117,6 +117,7 @@ SIGNATURES = [
     ("hit3d_gpu_stream", C.c_void_p, [_vp]),
     ("hit3d_gpu_launch_count", C.c_int64, [_vp]),
     ("hit3d_gpu_autotune", C.c_int, [_vp, C.POINTER(_i32), _dp]),
+    ("hit3d_gpu_autotune_columns", C.c_int, [_vp, C.POINTER(_i32), _dp]),
     ("hit3d_gpu_set_variant", C.c_int, [_vp, _i32]),
     ("hit3d_gpu_set_pruning", C.c_int, [_vp, _i32]),
     ("hit3d_gpu_set_update_fusion", C.c_int, [_vp, _i32]),
@@ -320,11 +321,21 @@ class Context:
         return dict(zip(self.STAGES, ms.tolist()))
 
     def autotune(self):
-        """Pick the fastest launch shape of the fused x pass; returns (variant, ms per variant)."""
+        """Pick the fastest launch shape of the fused x pass, then the column tile of
+        the strided passes (kept in self.column_tile, times in self.column_ms);
+        returns (variant, ms per variant)."""
         v = C.c_int32(0)
         ms = np.full(N_VARIANTS, np.nan)
         _check(lib().hit3d_gpu_autotune(self._h, C.byref(v), _ptr(ms)), "autotune")
+        self.column_tile, self.column_ms = self.autotune_columns()
         return v.value, [x for x in ms.tolist() if x == x]
+
+    def autotune_columns(self):
+        """Pick the column-tile shape of the strided passes; returns (tile, ms of the 3 shapes)."""
+        t = C.c_int32(0)
+        ms = np.zeros(3)
+        _check(lib().hit3d_gpu_autotune_columns(self._h, C.byref(t), _ptr(ms)), "autotune_columns")
+        return t.value, ms.tolist()
 
     def set_variant(self, v: int):
         _check(lib().hit3d_gpu_set_variant(self._h, int(v)), "set_variant")
