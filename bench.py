@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--config", default=None, choices=CONFIG_NAMES, help="with --configs-only: just this configuration")
     ap.add_argument("--config-steps", type=int, default=0, help="timed steps of --config forced_256 (default 20)")
     ap.add_argument("--cmp-every", type=int, default=50, help="FP32 vs FP64 statistics every this many steps")
-    ap.add_argument("--cmp-points", type=int, default=4)
+    ap.add_argument("--cmp-points", type=int, default=10)
     ap.add_argument("--variant", type=int, default=-1,
                     help="fix the fused x-pass launch shape instead of tuning (profiling runs)")
     ap.add_argument("--update-fusion", type=int, default=-1, choices=(-1, 0, 1),
@@ -467,11 +467,13 @@ def summarize(line):
     other configurations, the learned LES and the CPU baseline."""
     s = {"fp64_steps_per_s": line["value"], "ms_per_step": line["ms_per_step"],
          "roofline_frac": line["roofline"]["frac"], "roofline_kernel": line["roofline"]["kernel"],
-         "e2e_steps_per_s": (line.get("e2e") or {}).get("value")}
+         "e2e_steps_per_s": (line.get("e2e") or {}).get("value"),
+         "e2e_full_arrays_steps_per_s": ((line.get("e2e") or {}).get("full_arrays") or {}).get("value")}
     f = line.get("fp32_fft")
     if f:
         s["fp32"] = {"steps_per_s": f["value"], "speedup_vs_fp64": f["speedup_vs_fp64"],
                      "ek_max_rel_err_over_run": f.get("ek_max_rel_err_over_run"),
+                     "ek_1e-4_crossed_at_step": f.get("ek_1e-4_crossed_at_step"),
                      "per_step": [[c["step"], c["ek_max_rel_err"], c["eps_rel_err"], c["skew_abs_err"]]
                                   for c in f.get("vs_fp64_every_%d_steps" % 50, [])]}
     oc = line.get("other_configs") or {}
@@ -569,29 +571,42 @@ def main():
         hv[:] = fields0
         ho = torch.empty(fields0.size, dtype=torch.float64).pin_memory()
         hov = ho.numpy().reshape(fields0.shape)
-        # warm-up of the pipelined path (staging buffers and copy streams)
+        # warm-up of the pipelined path (staging buffers and copy streams); the
+        # full download also leaves hov zero outside the 2/3-rule band
         ctx.step_host([hv], [hov], nsteps=1)
         stream = torch.cuda.ExternalStream(ctx.stream)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        # every step: upload of that step's fields from pinned host memory, the
-        # step, download of the new state; the next upload overlaps this step
-        # and download (hit3d_gpu_step_host)
-        ctx.step_host([hv] * args.e2e_steps, [hov] * args.e2e_steps, nsteps=1)
-        e1.record(stream)
-        e1.synchronize()
-        te = e0.elapsed_time(e1) / 1000.0
+
+        def e2e_time(band_only):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            # every step: upload of that step's fields from pinned host memory,
+            # the step, download of the new state; the next upload overlaps this
+            # step and download (hit3d_gpu_step_host)
+            ctx.step_host([hv] * args.e2e_steps, [hov] * args.e2e_steps, nsteps=1, band_only=band_only)
+            e1.record(stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1) / 1000.0
+
+        te_full = e2e_time(False)
+        te = e2e_time(True)
         out = hov
         if dist:
             tt = torch.tensor([te], device="cuda")
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             te = float(tt.item())
-        nbytes = fields0.nbytes
+        if dist:
+            tt = torch.tensor([te_full], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te_full = float(tt.item())
+        nbytes = ctx.step_host_bytes(3, True)
         e2e = {"value": world * args.e2e_steps / te, "unit": "timesteps/s", "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps,
-               "api": "hit3d_gpu_step_host (reference-layout host fields, uploads overlapping downloads)"}
+               "api": "hit3d_gpu_step_host, reference-layout host fields, band_only: the 2/3-rule band "
+                      "(every |k_i| <= N/3) crosses PCIe, uploads overlapping downloads",
+               "full_arrays": {"value": world * args.e2e_steps / te_full, "h2d_bytes_per_step": fields0.nbytes,
+                               "d2h_bytes_per_step": fields0.nbytes}}
         del out
 
     # the FP64 trajectory for the per-statistic comparison, recorded before the
@@ -618,7 +633,7 @@ def main():
             v32, v32_ms = args.variant, []
         else:
             v32, v32_ms = c32.autotune()
-        t32, t32_ms = getattr(c32, "column_tile", 0), getattr(c32, "column_ms", [])
+        tile32, tile32_ms = getattr(c32, "column_tile", 0), getattr(c32, "column_ms", [])
         c32.step(args.warmup)
         if dist:
             dist.barrier()
@@ -636,7 +651,7 @@ def main():
                 "skew_abs_err": abs(st32["skewness"] - st64["skewness"]),
                 "stage_ms": {k: round(v / 3, 3) for k, v in prof32.items() if v > 0},
                 "tuned_variant": v32, "variant_ms": [round(x, 3) for x in v32_ms],
-                "column_tile": t32, "column_ms": [round(x, 3) for x in t32_ms]}
+                "column_tile": tile32, "column_ms": [round(x, 3) for x in tile32_ms]}
         # error per statistic against the FP64 path every cmp_every steps from the same state
         c32.upload_fields(fields0)
         c32.fov = c32.fos = 1
@@ -653,6 +668,8 @@ def main():
                         "courant": c32.courant})
         fp32["vs_fp64_every_%d_steps" % args.cmp_every] = cmp
         fp32["ek_max_rel_err_over_run"] = max(c["ek_max_rel_err"] for c in cmp) if cmp else None
+        # the first compared step at which the E(k) error passes 1e-4 (None: not within the run)
+        fp32["ek_1e-4_crossed_at_step"] = next((c["step"] for c in cmp if c["ek_max_rel_err"] > 1e-4), None)
         c32.close()
 
     les = None

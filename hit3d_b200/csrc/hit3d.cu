@@ -1182,12 +1182,59 @@ extern "C" int hit3d_gpu_restart_unpack(hit3d_ctx *c, const void *image, int64_t
 
 extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_t *fos, double *courant);
 
+// the boxes of a field's 2/3-rule band in the reference layout (x = bytes of
+// kx <= kc, y = kz, z = ky): kept kz and ky each form two runs of indices
+struct BandBox {
+    int z0, zb, nz, y0, yb, ny;  // reference-layout start, packed start, count (kz, then ky)
+};
+static int band_boxes(int n, int kc, BandBox *b)
+{
+    const int lo[2] = {0, n - kc}, pk[2] = {0, kc + 1}, cnt[2] = {kc + 1, kc};
+    int q = 0;
+    for (int y = 0; y < 2; y++)
+        for (int z = 0; z < 2; z++)
+            if (cnt[y] > 0 && cnt[z] > 0) b[q++] = BandBox{lo[z], pk[z], cnt[z], lo[y], pk[y], cnt[y]};
+    return q;
+}
+// one field's band between host memory (row pitch hp bytes, n rows per ky slice)
+// and the packed band on the device, as up to four strided box copies
+static cudaError_t band_copy(int n, int kc, double *host, size_t hp, double2 *packed, bool to_device, cudaStream_t s)
+{
+    BandBox b[4];
+    const int nbx = band_boxes(n, kc, b), nb = 2 * kc + 1;
+    const size_t w = (size_t)(kc + 1) * sizeof(double2);
+    for (int q = 0; q < nbx; q++) {
+        cudaMemcpy3DParms m;
+        memset(&m, 0, sizeof m);
+        cudaPitchedPtr hptr = make_cudaPitchedPtr(host, hp, hp, (size_t)n);
+        cudaPitchedPtr dptr = make_cudaPitchedPtr(packed, w, w, (size_t)nb);
+        const cudaPos hpos = make_cudaPos(0, (size_t)b[q].z0, (size_t)b[q].y0);
+        const cudaPos dpos = make_cudaPos(0, (size_t)b[q].zb, (size_t)b[q].yb);
+        if (to_device) { m.srcPtr = hptr; m.srcPos = hpos; m.dstPtr = dptr; m.dstPos = dpos; m.kind = cudaMemcpyHostToDevice; }
+        else { m.srcPtr = dptr; m.srcPos = dpos; m.dstPtr = hptr; m.dstPos = hpos; m.kind = cudaMemcpyDeviceToHost; }
+        m.extent = make_cudaExtent(w, (size_t)b[q].nz, (size_t)b[q].ny);
+        cudaError_t e = cudaMemcpy3DAsync(&m, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+extern "C" int64_t hit3d_gpu_step_host_bytes(hit3d_ctx *c, int32_t nf, int32_t band_only)
+{
+    if (!c || nf < 1 || nf > 3 + c->nsc) return -1;
+    const int kc = c->n / 3;
+    return band_only ? (int64_t)nf * (kc + 1) * (2 * kc + 1) * (2 * kc + 1) * 16
+                     : (int64_t)nf * c->n * c->n * c->nh * 16;
+}
+
 extern "C" int hit3d_gpu_step_host(hit3d_ctx *c, int32_t nio, const double *const *in, double *const *out, int64_t ld1,
-                                   int32_t nf, int32_t nsteps, int32_t *fov, int32_t *fos)
+                                   int32_t nf, int32_t nsteps, int32_t *fov, int32_t *fos, int32_t band_only)
 {
     if (!c || !in || !out || nio < 1 || nsteps < 0) return h3d_set_error_msg(-1, "hit3d_gpu_step_host: bad arguments");
     if (ld1 < c->n + 2) return h3d_set_error_msg(-1, "ld1 must be >= nx+2");
     if (nf < 1 || nf > 3 + c->nsc) return h3d_set_error_msg(-1, "nfields out of range");
+    if (band_only && c->p.dealias != 0)
+        return h3d_set_error_msg(-1, "hit3d_gpu_step_host: band-only transfers need the 2/3 rule (dealias 0)");
     for (int i = 0; i < nio; i++)
         if (!in[i] || !out[i]) return h3d_set_error_msg(-1, "hit3d_gpu_step_host: null field array");
     H3D_CHECK(cudaSetDevice(c->dev));
@@ -1195,14 +1242,18 @@ extern "C" int hit3d_gpu_step_host(hit3d_ctx *c, int32_t nio, const double *cons
     const size_t fe = (size_t)c->n * c->n * c->nh;  // complex elements of one reference-layout field
     const size_t width = (size_t)c->nh * sizeof(double2), hp = (size_t)ld1 * sizeof(double);
     const size_t rows = (size_t)c->n * c->n;
+    const int kc = c->n / 3;
     auto copy = [&](void *dst, size_t dp, const void *src, size_t sp, cudaMemcpyKind kind, cudaStream_t s) {
         return dp == sp && sp == width ? cudaMemcpyAsync(dst, src, width * rows, kind, s)
                                        : cudaMemcpy2DAsync(dst, dp, src, sp, width, rows, kind, s);
     };
     auto upload = [&](int i) -> int {  // host in[i] -> sin, on the copy-in stream
         H3D_CHECK(cudaStreamWaitEvent(c->cs_h2d, c->ev_in_free, 0));
-        for (int f = 0; f < nf; f++)
-            H3D_CHECK(copy(c->sin + f * fe, width, in[i] + (size_t)f * ld1 * rows, hp, cudaMemcpyHostToDevice, c->cs_h2d));
+        for (int f = 0; f < nf; f++) {
+            double *h = const_cast<double *>(in[i]) + (size_t)f * ld1 * rows;
+            if (band_only) H3D_CHECK(band_copy(c->n, kc, h, hp, c->sin + f * fe, true, c->cs_h2d));
+            else H3D_CHECK(copy(c->sin + f * fe, width, h, hp, cudaMemcpyHostToDevice, c->cs_h2d));
+        }
         H3D_CHECK(cudaEventRecord(c->ev_in_ready, c->cs_h2d));
         return 0;
     };
@@ -1217,7 +1268,8 @@ extern "C" int hit3d_gpu_step_host(hit3d_ctx *c, int32_t nio, const double *cons
         // while this state steps and downloads
         H3D_CHECK(cudaStreamWaitEvent(c->st, c->ev_in_ready, 0));
         for (int f = 0; f < nf; f++) {
-            k_ref_to_dev<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->sin + f * fe, c->U + f * c->fs64);
+            if (band_only) k_band_to_dev<<<pw_grid(c), 256, 0, c->st>>>(c->n, kc, c->P64, c->sin + f * fe, c->U + f * c->fs64);
+            else k_ref_to_dev<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->sin + f * fe, c->U + f * c->fs64);
             H3D_LAUNCH_CHECK();
         }
         H3D_CHECK(cudaEventRecord(c->ev_in_free, c->st));
@@ -1230,13 +1282,17 @@ extern "C" int hit3d_gpu_step_host(hit3d_ctx *c, int32_t nio, const double *cons
         double2 *so = c->sout[ob];
         H3D_CHECK(cudaStreamWaitEvent(c->st, c->ev_out_free[ob], 0));
         for (int f = 0; f < nf; f++) {
-            k_dev_to_ref<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->U + f * c->fs64, so + f * fe);
+            if (band_only) k_dev_to_band<<<pw_grid(c), 256, 0, c->st>>>(c->n, kc, c->P64, c->U + f * c->fs64, so + f * fe);
+            else k_dev_to_ref<<<pw_grid(c), 256, 0, c->st>>>(c->n, c->nh, c->P64, c->U + f * c->fs64, so + f * fe);
             H3D_LAUNCH_CHECK();
         }
         H3D_CHECK(cudaEventRecord(c->ev_out_ready, c->st));
         H3D_CHECK(cudaStreamWaitEvent(c->cs_d2h, c->ev_out_ready, 0));
-        for (int f = 0; f < nf; f++)
-            H3D_CHECK(copy(out[i] + (size_t)f * ld1 * rows, hp, so + f * fe, width, cudaMemcpyDeviceToHost, c->cs_d2h));
+        for (int f = 0; f < nf; f++) {
+            double *h = out[i] + (size_t)f * ld1 * rows;
+            if (band_only) H3D_CHECK(band_copy(c->n, kc, h, hp, so + f * fe, false, c->cs_d2h));
+            else H3D_CHECK(copy(h, hp, so + f * fe, width, cudaMemcpyDeviceToHost, c->cs_d2h));
+        }
         H3D_CHECK(cudaEventRecord(c->ev_out_free[ob], c->cs_d2h));
     }
     // the compute stream ends after the last download, so that events recorded

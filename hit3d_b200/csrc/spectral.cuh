@@ -1118,6 +1118,38 @@ __global__ void k_restart_to_dev(int n, int pitch, const double2 *__restrict__ R
     }
 }
 
+// The 2/3-rule band (every |k_i| <= kc = N/3) packed as [ky'][kz'][kx], ky' and
+// kz' in [0, 2 kc] over the kept indices (0..kc, N-kc..N-1), kx in [0, kc]: the
+// part of a dealiased state that is not zero by construction.  band -> the
+// device layout writes every mode of the field (zero outside the band); the
+// device layout -> band reads the band only.
+__global__ void k_band_to_dev(int n, int kc, int pitch, const double2 *__restrict__ B, double2 *__restrict__ D)
+{
+    const int nh = n / 2 + 1, nb = 2 * kc + 1;
+    const int64_t nm = (int64_t)n * n * nh;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        const int kx = (int)(t % nh);
+        const int64_t r = t / nh;
+        const int kyi = (int)(r % n), kzi = (int)(r / n);
+        const int yb = kyi <= kc ? kyi : kyi >= n - kc ? kyi - (n - nb) : -1;
+        const int zb = kzi <= kc ? kzi : kzi >= n - kc ? kzi - (n - nb) : -1;
+        D[r * pitch + kx] =
+            (kx <= kc && yb >= 0 && zb >= 0) ? B[((int64_t)yb * nb + zb) * (kc + 1) + kx] : make_double2(0.0, 0.0);
+    }
+}
+__global__ void k_dev_to_band(int n, int kc, int pitch, const double2 *__restrict__ D, double2 *__restrict__ B)
+{
+    const int nb = 2 * kc + 1;
+    const int64_t nm = (int64_t)nb * nb * (kc + 1);
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nm; t += (int64_t)gridDim.x * blockDim.x) {
+        const int kx = (int)(t % (kc + 1));
+        const int64_t r = t / (kc + 1);
+        const int zb = (int)(r % nb), yb = (int)(r / nb);
+        const int kyi = yb <= kc ? yb : yb + (n - nb), kzi = zb <= kc ? zb : zb + (n - nb);
+        B[t] = D[((int64_t)kzi * n + kyi) * pitch + kx];
+    }
+}
+
 // layout conversion between the reference's (nx+2, ny, nz) Fourier array
 // [ky][kz][kx] (pitch nh) and the device layout [kz][ky][kx] (pitch P)
 __global__ void k_ref_to_dev(int n, int nh, int pitch, const double2 *__restrict__ R, double2 *__restrict__ D)

@@ -110,7 +110,8 @@ SIGNATURES = [
     ("hit3d_gpu_download_rhs_old", C.c_int, [_vp, _dp, _i64, _i32]),
     ("hit3d_gpu_step", C.c_int, [_vp, _i32, C.POINTER(_i32), C.POINTER(_i32), _dp]),
     ("hit3d_gpu_step_host", C.c_int, [_vp, _i32, C.POINTER(_dp), C.POINTER(_dp), _i64, _i32, _i32, C.POINTER(_i32),
-                                      C.POINTER(_i32)]),
+                                      C.POINTER(_i32), _i32]),
+    ("hit3d_gpu_step_host_bytes", C.c_int64, [_vp, _i32, _i32]),
     ("hit3d_gpu_restart_bytes", C.c_int64, [_vp, _i32]),
     ("hit3d_gpu_restart_pack", C.c_int, [_vp, _i32, _d, _d, C.c_void_p]),
     ("hit3d_gpu_restart_unpack", C.c_int, [_vp, C.c_void_p, _i64, _dp, _dp, C.POINTER(_i32), C.POINTER(_i32)]),
@@ -269,10 +270,15 @@ class Context:
         self.fov, self.fos, self.courant = fov.value, fos.value, cour.value
         return self.courant
 
-    def step_host(self, ins, outs, nsteps: int = 1):
+    def step_host_bytes(self, nf: int, band_only: bool = False) -> int:
+        """Bytes hit3d_gpu_step_host moves per input, each way."""
+        return int(lib().hit3d_gpu_step_host_bytes(self._h, int(nf), int(bool(band_only))))
+
+    def step_host(self, ins, outs, nsteps: int = 1, band_only: bool = False):
         """For each (in, out) pair of host arrays (field_shape()), upload `in`,
         advance nsteps and download into `out`, the next upload overlapping this
-        step and download (hit3d_gpu_step_host).  Use pinned arrays for full rate."""
+        step and download (hit3d_gpu_step_host).  Use pinned arrays for full rate.
+        band_only: only the 2/3-rule band crosses PCIe (see the C header)."""
         n = len(ins)
         if n < 1 or len(outs) != n:
             raise ValueError("step_host: ins and outs must be non-empty and of equal length")
@@ -284,7 +290,7 @@ class Context:
         pout = (_dp * n)(*[_ptr(a) for a in outs])
         fov, fos = C.c_int32(self.fov), C.c_int32(self.fos)
         _check(lib().hit3d_gpu_step_host(self._h, n, pin, pout, self.n + 2, nf, int(nsteps), C.byref(fov),
-                                         C.byref(fos)), "step_host")
+                                         C.byref(fos), int(bool(band_only))), "step_host")
         self.fov, self.fos = fov.value, fos.value
 
     def restart_image(self, time: float, dt: float, nums: int | None = None) -> np.ndarray:

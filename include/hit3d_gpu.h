@@ -138,9 +138,16 @@ int hit3d_gpu_restart_unpack(hit3d_ctx *ctx, const void *image, int64_t bytes, d
  * in[i+1] must not share memory with out[i]; every array stays valid until the
  * call returns, and pinned host memory gives the full PCIe rate.  The staging
  * fields (3 nf fields in the reference layout: one input set, two output sets
- * used in turn) are allocated on first use. */
+ * used in turn) are allocated on first use.
+ * band_only = 1 (2/3 rule only): only the modes with every |k_i| <= N/3 cross
+ * PCIe (29.5 % of the array at 512^3), as box copies of the host arrays: the
+ * values of in[i] outside that band are taken as zero, which a dealiased state
+ * has there, and out[i] is written inside the band only (it must hold zeros
+ * outside, e.g. from a download with band_only = 0).  The bytes a call moves
+ * per input: hit3d_gpu_step_host_bytes(ctx, nf, band_only), each way. */
 int hit3d_gpu_step_host(hit3d_ctx *ctx, int32_t nio, const double *const *in, double *const *out, int64_t ld1,
-                        int32_t nf, int32_t nsteps, int32_t *fov, int32_t *fos);
+                        int32_t nf, int32_t nsteps, int32_t *fov, int32_t *fos, int32_t band_only);
+int64_t hit3d_gpu_step_host_bytes(hit3d_ctx *ctx, int32_t nf, int32_t band_only);
 
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, for
  * callers that time or order work around the library (the reference's

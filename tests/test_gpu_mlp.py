@@ -65,8 +65,9 @@ def test_tensor_core_predict_matches_oracle():
     Bound: tanh.approx.f32 differs from tanh by up to about 2^-11, which moves an
     activation by far less than one bf16 step (2^-8 relative) but decides some
     bf16 roundings differently; a point's stress then moves by a fraction of a
-    bf16 step.  Stated: 99.9 % of points within 2e-3 of the largest stress, every
-    point within 2e-2."""
+    bf16 step.  Stated: 99.9 % of points within 2e-4 of the largest stress, every
+    point within 2e-3 (measured on B200: median 1.6e-8, 99.9 % 5.1e-5, max
+    3.8e-4)."""
     np_ = 300001
     A, _ = mo.synthetic_data(np_, seed=13)
     w = mo.bf16_round(mo.init_params(21)).astype(np.float64)
@@ -77,13 +78,13 @@ def test_tensor_core_predict_matches_oracle():
     err = np.abs(got - ref).max(axis=0) / scale
     print(f"tensor-core closure vs oracle: median {np.median(err):.2e}, 99.9 % {np.quantile(err, 0.999):.2e}, "
           f"max {err.max():.2e}")
-    assert np.quantile(err, 0.999) < 2e-3 and err.max() < 2e-2, (np.quantile(err, 0.999), err.max())
+    assert np.quantile(err, 0.999) < 2e-4 and err.max() < 2e-3, (np.quantile(err, 0.999), err.max())
     # and the fp32-activation kernel agrees to bf16 accuracy
     exact = m.predict(A, DELTA, clip=False, kernel=0)
     assert np.abs(exact - got).max() < 2e-2 * scale
     got_clip = m.predict(A, DELTA, clip=True, kernel=1)
     ref_clip = mo.predict(w, A, DELTA, clip=True, act_bf16=True)
-    agree = np.all(np.abs(got_clip - ref_clip) <= 2e-2 * scale, axis=0)
+    agree = np.all(np.abs(got_clip - ref_clip) <= 2e-3 * scale, axis=0)
     assert agree.mean() > 0.999
     m.close()
 

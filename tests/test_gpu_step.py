@@ -227,24 +227,33 @@ def test_unsupported_reaction_type_is_rejected():
         Context(Params(nx=32, dealias=1, n_scalars=1, sc=[1.0], scalar_type=[312]))
 
 
-def test_step_host_pipelined_matches_sequential():
+@pytest.mark.parametrize("band_only", [False, True])
+def test_step_host_pipelined_matches_sequential(band_only):
     """hit3d_gpu_step_host (uploads overlapping the previous step and download)
     gives what upload / step / download calls one after another give, with the
-    AB2 history carried from one input to the next."""
+    AB2 history carried from one input to the next; with band_only only the
+    2/3-rule band crosses PCIe (a dealiased state is zero elsewhere)."""
     from hit3d_b200 import Context, Params
-    p = Params(nx=64, flow_type=1, kfmax=2, nu=1.0 / 400, dt=0.004)
+    p = Params(nx=48, flow_type=1, kfmax=2, nu=1.0 / 400, dt=0.004)
     a = Context(p)
     a.init_velocity(RN1, 2, 4.0, 2.0)
     a.dealias_all()
     a.step(2)
     f0, r0 = a.download_fields(), a.download_rhs_old()
     ins = [np.ascontiguousarray(f0 * s) for s in (1.0, 0.9, 1.1)]
+    if band_only:
+        # values outside the band are ignored on the way in
+        ins[1][:, :, :, 40:] = 7.0
     outs = [np.zeros_like(f0) for _ in ins]
-    a.step_host(ins, outs, nsteps=2)
+    a.step_host(ins, outs, nsteps=2, band_only=band_only)
+    kc = 16
+    assert a.step_host_bytes(3, band_only) == 3 * 16 * ((kc + 1) * (2 * kc + 1) ** 2 if band_only else 48 * 48 * 25)
     b = Context(p)
     b.upload_rhs_old(r0)
     b.fov = b.fos = 0
     for i, x in enumerate(ins):
+        if band_only and i == 1:
+            x = np.ascontiguousarray(f0 * 0.9)
         b.upload_fields(x)
         b.step(2)
         assert np.array_equal(b.download_fields(), outs[i]), i
