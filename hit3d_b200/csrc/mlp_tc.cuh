@@ -1,39 +1,53 @@
 // Tensor-core inference of the learned subgrid closure (sm_100a, tcgen05).
 //
-// A CTA of 128 threads takes tiles of 128 points, one point per thread.  The
-// two 64x64 hidden layers (92 % of the multiply-adds) run as
-//   D[128 x 64] (fp32, TMEM) = A[128 x 64] (bf16, smem) * W^T (bf16, smem)
-// with four tcgen05.mma of K = 16 each, issued by one thread and completed
-// through tcgen05.commit on an mbarrier.  The input layer (6 -> 64), the GELUs
-// (tanh form with the hardware tanh approximation), the output layer (64 -> 5)
-// and the tensor basis stay on the CUDA cores in fp32.  The activations that feed
-// the tensor cores are rounded to bf16 (round to nearest even).
+// A CTA of 128 threads takes tiles of 128 points, one point per thread.  All
+// four layers run on the tensor cores as
+//   D[128 x N] (fp32, TMEM) = A[128 x K] (bf16, smem) * W^T (bf16, smem)
+// with tcgen05.mma of K = 16 each, issued by one thread and completed through
+// tcgen05.commit on an mbarrier:
+//   input layer   K = 16 (the six features, a 1 that carries the bias b1 in
+//                 W1's seventh column, zeros), N = 64, one MMA;
+//   hidden layers K = 64, N = 64, four MMAs each;
+//   output layer  K = 64, N = 16 (W4's five rows, zeros), four MMAs.
+// The features, the GELUs (tanh form with the hardware tanh approximation),
+// the biases b2, b3, b4 and the tensor basis run on the CUDA cores in fp32.
+// The features and every activation that feeds the tensor cores are rounded
+// to bf16 (round to nearest even).
 //
 // Shared-memory operands use the no-swizzle K-major canonical layout: 8 x 8
 // "core matrices" of 128 contiguous bytes (row r at 16 r bytes, element k at
 // 2 k bytes), K chunks of 8 elements LBO bytes apart, 8-row groups SBO bytes
 // apart.  Here every K chunk holds all row groups contiguously, so
-//   A (128 rows): offset(r, k) = ((k/8) 16 + r/8) 128 + (r%8) 16 + (k%8) 2,  LBO 2048, SBO 128
-//   W ( 64 rows): offset(n, k) = ((k/8)  8 + n/8) 128 + (n%8) 16 + (k%8) 2,  LBO 1024, SBO 128
-// and k-step s of an MMA starts 2 chunks further (4096 and 2048 bytes).
+//   A   (128 rows): offset(r, k) = ((k/8) 16 + r/8) 128 + (r%8) 16 + (k%8) 2,  LBO 2048, SBO 128
+//   W   ( 64 rows): offset(n, k) = ((k/8)  8 + n/8) 128 + (n%8) 16 + (k%8) 2,  LBO 1024, SBO 128
+//   W4p ( 16 rows): offset(n, k) = ((k/8)  2 + n/8) 128 + (n%8) 16 + (k%8) 2,  LBO  256, SBO 128
+// and k-step s of an MMA starts 2 chunks further (4096, 2048 and 512 bytes).
+// The input layer's A is the first two chunks of the A tile, its W1p the
+// first two chunks of a 64-row W layout.
 #pragma once
 #include "mlp.cuh"
 
 constexpr int TC_TILE = 128;
-constexpr int TC_COLS = 64;  // TMEM columns: one 128 x 64 fp32 accumulator
+constexpr int TC_COLS = 64;  // TMEM columns: one 128 x 64 fp32 accumulator, reused by every layer
+constexpr int TC_K1 = 16, TC_N4 = 16;  // padded K of the input layer, padded N of the output layer
 constexpr uint32_t TC_A_BYTES = TC_TILE * MLP_H * 2, TC_W_BYTES = MLP_H * MLP_H * 2;
+constexpr uint32_t TC_W1_BYTES = MLP_H * TC_K1 * 2, TC_W4_BYTES = TC_N4 * MLP_H * 2;
 constexpr uint32_t TC_OFF_A = 0, TC_OFF_W2 = TC_A_BYTES, TC_OFF_W3 = TC_OFF_W2 + TC_W_BYTES,
-                   TC_OFF_F = TC_OFF_W3 + TC_W_BYTES;
-// fp32 parameters: W1t[6][64], b1, b2, b3 [64], W4[5][64], b4[5]
-constexpr int TCF_W1 = 0, TCF_B1 = TCF_W1 + MLP_IN * MLP_H, TCF_B2 = TCF_B1 + MLP_H, TCF_B3 = TCF_B2 + MLP_H,
-              TCF_W4 = TCF_B3 + MLP_H, TCF_B4 = TCF_W4 + MLP_OUT * MLP_H, TCF_N = TCF_B4 + 8;
+                   TC_OFF_W1 = TC_OFF_W3 + TC_W_BYTES, TC_OFF_W4 = TC_OFF_W1 + TC_W1_BYTES,
+                   TC_OFF_F = TC_OFF_W4 + TC_W4_BYTES;
+// fp32 parameters kept for the CUDA cores: b2, b3 [64], b4 [5]
+constexpr int TCF_B2 = 0, TCF_B3 = TCF_B2 + MLP_H, TCF_B4 = TCF_B3 + MLP_H, TCF_N = TCF_B4 + 8;
 constexpr uint32_t TC_OFF_BAR = TC_OFF_F + 4 * TCF_N;  // 8-byte mbarrier, then the TMEM address slot
 constexpr size_t TC_SMEM = TC_OFF_BAR + 16;
 static_assert(TC_OFF_BAR % 8 == 0, "mbarrier alignment");
-// kind::f16 instruction descriptor: fp32 accumulator, bf16 A and B, both
-// K-major, N = 64, M = 128
-constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(MLP_H >> 3) << 17) |
-                              ((uint32_t)(TC_TILE >> 4) << 24);
+static_assert(TC_SMEM <= 48 * 1024, "the closure kernel runs with the default shared-memory limit");
+// kind::f16 instruction descriptors: fp32 accumulator, bf16 A and B, both
+// K-major, M = 128; N = 64 (input and hidden layers) or 16 (output layer)
+constexpr uint32_t tc_idesc(int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_TILE >> 4) << 24);
+}
+constexpr uint32_t TC_IDESC = tc_idesc(MLP_H), TC_IDESC_OUT = tc_idesc(TC_N4);
 constexpr uint32_t TC_WAIT_LIMIT = 1u << 22;  // bounded mbarrier polls
 
 H3D_D uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -45,11 +59,11 @@ H3D_D uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-H3D_D void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate)
+H3D_D void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate, uint32_t idesc = TC_IDESC)
 {
     asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-                 "l"(a), "l"(b), "r"(TC_IDESC), "r"(accumulate));
+                 "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
 }
 H3D_D void umma_commit(uint32_t bar)
 {
@@ -91,7 +105,41 @@ H3D_D void tmem_ld32(uint32_t taddr, float *v)
 }
 H3D_D void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// bf16 of gelu(acc[j] + b[j]) into this thread's row of the A tile
+// 16 consecutive TMEM columns of this warp's 32 lanes: thread i gets lane i
+H3D_D void tmem_ld16(uint32_t taddr, float *v)
+{
+    uint32_t r[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                 "%13, %14, %15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                   "=r"(r[15])
+                 : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// row r of the A tile, K chunk c (8 bf16 values)
+H3D_D uint4 *a_chunk(unsigned char *sA, int r, int c)
+{
+    return reinterpret_cast<uint4 *>(sA + ((c * (TC_TILE / 8) + r / 8) * 128 + (r % 8) * 16));
+}
+H3D_D uint32_t pack_bf16(float lo, float hi)
+{
+    const __nv_bfloat162 h2 = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&h2);
+}
+
+// bf16 of the features, then 1 (the bias column of W1p), then zeros: the
+// input layer's A (the first two K chunks of the A tile)
+H3D_D void store_input_row(unsigned char *sA, int r, const float *x)
+{
+    *a_chunk(sA, r, 0) = make_uint4(pack_bf16(x[0], x[1]), pack_bf16(x[2], x[3]), pack_bf16(x[4], x[5]),
+                                    pack_bf16(1.0f, 0.0f));
+    *a_chunk(sA, r, 1) = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// bf16 of gelu(acc[j] + b[j]) (b may be null) into this thread's row of the A tile
 H3D_D void store_act_row(unsigned char *sA, int r, const float *acc, const float *b)
 {
 #pragma unroll
@@ -99,18 +147,20 @@ H3D_D void store_act_row(unsigned char *sA, int r, const float *acc, const float
         uint32_t w[4];
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-            const float lo = gelu_fast(acc[8 * c + 2 * e] + b[8 * c + 2 * e]);
-            const float hi = gelu_fast(acc[8 * c + 2 * e + 1] + b[8 * c + 2 * e + 1]);
-            const __nv_bfloat162 h2 = __floats2bfloat162_rn(lo, hi);
-            w[e] = *reinterpret_cast<const uint32_t *>(&h2);
+            const int j = 8 * c + 2 * e;
+            const float lo = gelu_fast(b ? acc[j] + b[j] : acc[j]);
+            const float hi = gelu_fast(b ? acc[j + 1] + b[j + 1] : acc[j + 1]);
+            w[e] = pack_bf16(lo, hi);
         }
-        *reinterpret_cast<uint4 *>(sA + ((c * (TC_TILE / 8) + r / 8) * 128 + (r % 8) * 16)) =
-            make_uint4(w[0], w[1], w[2], w[3]);
+        *a_chunk(sA, r, c) = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 
-// one hidden layer on the tensor cores: acc (fp32, this thread's row) = A * W^T
-H3D_D bool tc_layer(unsigned char *sm, uint32_t sW, uint32_t tmem, uint32_t bar, uint32_t &phase, float *acc)
+// one layer on the tensor cores: the A tile written by the threads times W^T,
+// nk MMAs of K = 16 (A chunks 2 apart, W chunks `wstep` bytes apart), then this
+// thread's row of the accumulator: ncol (64 or 16) columns into acc
+H3D_D bool tc_layer(unsigned char *sm, uint32_t sW, uint32_t lboW, uint32_t wstep, int nk, uint32_t idesc, int ncol,
+                    uint32_t tmem, uint32_t bar, uint32_t &phase, float *acc)
 {
     proxy_fence();  // the A tile written by the threads, to the tensor cores
     tc_fence_before();
@@ -118,22 +168,25 @@ H3D_D bool tc_layer(unsigned char *sm, uint32_t sW, uint32_t tmem, uint32_t bar,
     tc_fence_after();
     if (threadIdx.x == 0) {
         const uint32_t sA = smem_addr(sm + TC_OFF_A);
-#pragma unroll
-        for (int s = 0; s < MLP_H / 16; s++)
-            umma_bf16(tmem, umma_desc(sA + s * 2 * 2048, 2048, 128), umma_desc(sW + s * 2 * 1024, 1024, 128), s > 0);
+        for (int s = 0; s < nk; s++)
+            umma_bf16(tmem, umma_desc(sA + s * 2 * 2048, 2048, 128), umma_desc(sW + s * wstep, lboW, 128), s > 0, idesc);
         umma_commit(bar);
     }
     const bool ok = mbar_wait(bar, phase);
     phase ^= 1u;
     tc_fence_after();
     const uint32_t ta = tmem + ((uint32_t)(threadIdx.x & ~31) << 16);
-    tmem_ld32(ta, acc);
-    tmem_ld32(ta + 32, acc + 32);
+    if (ncol == MLP_H) {
+        tmem_ld32(ta, acc);
+        tmem_ld32(ta + 32, acc + 32);
+    } else {
+        tmem_ld16(ta, acc);
+    }
     tmem_wait_ld();
     return ok;
 }
 
-// Inference, as k_mlp_apply, with the hidden layers on the tensor cores.
+// Inference, as k_mlp_apply, with all four layers on the tensor cores.
 // err: set to 1 if an MMA completion wait ran out (the results are then invalid).
 template <typename TS>
 __global__ void __launch_bounds__(TC_TILE) k_mlp_apply_tc(int64_t np, int64_t n, int64_t rp, int64_t fs, float delta,
@@ -147,8 +200,7 @@ __global__ void __launch_bounds__(TC_TILE) k_mlp_apply_tc(int64_t np, int64_t n,
     uint32_t *slot = reinterpret_cast<uint32_t *>(sm + TC_OFF_BAR + 8);
     const int tid = threadIdx.x;
 
-    // weights: hidden layers in the K-major core-matrix layout (16-byte copies),
-    // the rest as fp32
+    // weights: hidden layers in the K-major core-matrix layout (16-byte copies)
     const uint4 *w4 = reinterpret_cast<const uint4 *>(wb);
     for (int q = tid; q < 2 * MLP_H * (MLP_H / 8); q += TC_TILE) {
         const int l = q / (MLP_H * MLP_H / 8), e = q % (MLP_H * MLP_H / 8), nrow = e / 8, c = e % 8;
@@ -156,17 +208,25 @@ __global__ void __launch_bounds__(TC_TILE) k_mlp_apply_tc(int64_t np, int64_t n,
         *reinterpret_cast<uint4 *>(sm + (l == 0 ? TC_OFF_W2 : TC_OFF_W3) + (c * (MLP_H / 8) + nrow / 8) * 128 +
                                    (nrow % 8) * 16) = w4[src];
     }
-    for (int q = tid; q < MLP_IN * MLP_H; q += TC_TILE) {
-        const int j = q / MLP_IN, i = q % MLP_IN;
-        F[TCF_W1 + i * MLP_H + j] = __bfloat162float(wb[MLP_W1 + q]);
+    // W1p [64 x 16]: W1's six columns, b1, zeros; W4p [16 x 64]: W4's five rows, zeros
+    const __nv_bfloat16 bz = __float2bfloat16(0.0f);
+    for (int q = tid; q < MLP_H * TC_K1; q += TC_TILE) {
+        const int nrow = q / TC_K1, k = q % TC_K1;
+        const __nv_bfloat16 v = k < MLP_IN ? wb[MLP_W1 + nrow * MLP_IN + k] : k == MLP_IN ? wb[MLP_B1 + nrow] : bz;
+        *reinterpret_cast<__nv_bfloat16 *>(sm + TC_OFF_W1 + ((k / 8) * (MLP_H / 8) + nrow / 8) * 128 + (nrow % 8) * 16 +
+                                           (k % 8) * 2) = v;
+    }
+    for (int q = tid; q < TC_N4 * MLP_H; q += TC_TILE) {
+        const int nrow = q / MLP_H, k = q % MLP_H;
+        const __nv_bfloat16 v = nrow < MLP_OUT ? wb[MLP_W4 + nrow * MLP_H + k] : bz;
+        *reinterpret_cast<__nv_bfloat16 *>(sm + TC_OFF_W4 + ((k / 8) * (TC_N4 / 8) + nrow / 8) * 128 + (nrow % 8) * 16 +
+                                           (k % 8) * 2) = v;
     }
     for (int q = tid; q < MLP_H; q += TC_TILE) {
-        F[TCF_B1 + q] = __bfloat162float(wb[MLP_B1 + q]);
         F[TCF_B2 + q] = __bfloat162float(wb[MLP_B2 + q]);
         F[TCF_B3 + q] = __bfloat162float(wb[MLP_B3 + q]);
     }
-    for (int q = tid; q < MLP_OUT * MLP_H + MLP_OUT; q += TC_TILE)
-        F[TCF_W4 + q] = __bfloat162float(wb[MLP_W4 + q]);  // W4 then b4, contiguous in both layouts
+    if (tid < MLP_OUT) F[TCF_B4 + tid] = __bfloat162float(wb[MLP_B4 + tid]);
     if (tid < 32) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(slot)),
                      "r"(TC_COLS));
@@ -181,7 +241,8 @@ __global__ void __launch_bounds__(TC_TILE) k_mlp_apply_tc(int64_t np, int64_t n,
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *slot, sbar = smem_addr(bar);
-    const uint32_t sW2 = smem_addr(sm + TC_OFF_W2), sW3 = smem_addr(sm + TC_OFF_W3);
+    const uint32_t sW1 = smem_addr(sm + TC_OFF_W1), sW2 = smem_addr(sm + TC_OFF_W2), sW3 = smem_addr(sm + TC_OFF_W3),
+                   sW4 = smem_addr(sm + TC_OFF_W4);
     uint32_t phase = 0;
     bool ok = true;
 
@@ -207,27 +268,17 @@ __global__ void __launch_bounds__(TC_TILE) k_mlp_apply_tc(int64_t np, int64_t n,
         Feat f;
         features(Am, delta, f);
         float acc[MLP_H];
-#pragma unroll
-        for (int j = 0; j < MLP_H; j++) {
-            float s = 0.0f;
-#pragma unroll
-            for (int i = 0; i < MLP_IN; i++) s = fmaf(F[TCF_W1 + i * MLP_H + j], f.x[i], s);
-            acc[j] = s;
-        }
-        store_act_row(sm + TC_OFF_A, tid, acc, F + TCF_B1);
-        ok &= tc_layer(sm, sW2, tmem, sbar, phase, acc);
+        store_input_row(sm + TC_OFF_A, tid, f.x);
+        ok &= tc_layer(sm, sW1, 1024, 2 * 1024, 1, TC_IDESC, MLP_H, tmem, sbar, phase, acc);
+        store_act_row(sm + TC_OFF_A, tid, acc, nullptr);  // b1 came with the input layer
+        ok &= tc_layer(sm, sW2, 1024, 2 * 1024, MLP_H / 16, TC_IDESC, MLP_H, tmem, sbar, phase, acc);
         store_act_row(sm + TC_OFF_A, tid, acc, F + TCF_B2);
-        ok &= tc_layer(sm, sW3, tmem, sbar, phase, acc);
-#pragma unroll
-        for (int j = 0; j < MLP_H; j++) acc[j] = gelu_fast(acc[j] + F[TCF_B3 + j]);
+        ok &= tc_layer(sm, sW3, 1024, 2 * 1024, MLP_H / 16, TC_IDESC, MLP_H, tmem, sbar, phase, acc);
+        store_act_row(sm + TC_OFF_A, tid, acc, F + TCF_B3);
+        ok &= tc_layer(sm, sW4, 256, 2 * 256, MLP_H / 16, TC_IDESC_OUT, TC_N4, tmem, sbar, phase, acc);
         float g[MLP_OUT], tau[MLP_TC];
 #pragma unroll
-        for (int q = 0; q < MLP_OUT; q++) {
-            float s = F[TCF_B4 + q];
-#pragma unroll
-            for (int i = 0; i < MLP_H; i++) s = fmaf(F[TCF_W4 + q * MLP_H + i], acc[i], s);
-            g[q] = s;
-        }
+        for (int q = 0; q < MLP_OUT; q++) g[q] = acc[q] + F[TCF_B4 + q];
         basis_sum(f, g, tau);
         const bool zero = clip && sgs_diss(tau, f.sbar) < 0.f;
         if (valid) {

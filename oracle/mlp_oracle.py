@@ -93,9 +93,12 @@ def _bf16_act(a):
 
 
 def forward(w, x, act_bf16=False):
-    """act_bf16: the inputs of the two hidden 64x64 layers rounded to bf16, as the
-    tensor-core inference kernel feeds them to the MMA."""
+    """act_bf16: every layer's input rounded to bf16 (the features and the three
+    hidden activations), as the tensor-core inference kernel feeds them to the
+    MMAs of its four layers."""
     p = unpack(w)
+    if act_bf16:
+        x = _bf16_act(x)
     z1 = p["W1"] @ x + p["b1"][:, None]
     a1 = gelu(z1)
     if act_bf16:
@@ -106,6 +109,8 @@ def forward(w, x, act_bf16=False):
         a2 = _bf16_act(a2)
     z3 = p["W3"] @ a2 + p["b3"][:, None]
     a3 = gelu(z3)
+    if act_bf16:
+        a3 = _bf16_act(a3)
     g = p["W4"] @ a3 + p["b4"][:, None]
     return g, (x, z1, a1, z2, a2, z3, a3)
 
