@@ -91,14 +91,14 @@ class Batch:
     def autotune(self):
         """Per size class, pick the fused x-pass launch shape (variants 8-14) and
         the column-tile shape of the strided passes by timing them on the class's
-        buffers.  Returns [(variant, tile, ms of the 7 variants, ms of the 3 tiles)]."""
+        buffers.  Returns [(variant, tile, ms of the 7 variants, ms of the 4 tiles)]."""
         k = self.nclasses
         choice = (C.c_int32 * (2 * max(k, 1)))()
-        ms = np.zeros(10 * max(k, 1))
+        ms = np.zeros(11 * max(k, 1))
         _check(lib().hit3d_batch_autotune(self._h, choice, ms.ctypes.data_as(C.POINTER(C.c_double))),
                "hit3d_batch_autotune")
-        return [(int(choice[2 * q]), int(choice[2 * q + 1]), ms[10 * q:10 * q + 7].tolist(),
-                 ms[10 * q + 7:10 * q + 10].tolist()) for q in range(k)]
+        return [(int(choice[2 * q]), int(choice[2 * q + 1]), ms[11 * q:11 * q + 7].tolist(),
+                 ms[11 * q + 7:11 * q + 11].tolist()) for q in range(k)]
 
     def close(self):
         if getattr(self, "_h", None):

@@ -17,6 +17,7 @@
 #include "ctx.cuh"
 #include "passes.cuh"
 #include "launch_cfg.cuh"
+#include "colpipe.cuh"
 #include "spectral.cuh"
 #include "fused_update.cuh"
 
@@ -72,11 +73,52 @@ static int zinv_LMC(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_
     H3D_LAUNCH_CHECK();
     return 0;
 }
-// the tuned column tile (ctile) applies to the plain copy of grids up to 512
+// the pipelined strided pass (k_colfft_pipe): a grid of resident CTAs walking
+// every tile of the pass, with the tile after next in flight
+template <typename T, int L, bool FWD, class IO> static int colpipe_launch(hit3d_ctx *c, const IO &io, int ncol, int rows, int nz)
+{
+    using TI = typename ColIn<IO>::type;
+    using CF = ColPipeCfg<T, TI, L>;
+    auto k = k_colfft_pipe<T, L, CF::TC, CF::NT, FWD, IO, CF::MINB>;
+    H3D_TRY(set_smem(k, CF::SMEM));
+    const ColTiles tl{(ncol + CF::TC - 1) / CF::TC, rows};
+    const int64_t ntiles = (int64_t)tl.nx * rows * nz;
+    if (ntiles > INT32_MAX) return h3d_set_error_msg(-1, "pipelined column pass: too many tiles");
+    int64_t grid = (int64_t)c->nsm * CF::MINB;
+    grid = grid < ntiles ? grid : ntiles;
+    k<<<(unsigned)grid, CF::NT, CF::SMEM, c->st>>>(io, twid<T>(c), tl, (int)ntiles);
+    H3D_LAUNCH_CHECK();
+    return 0;
+}
+
+// the tuned column tile (ctile) applies to the plain copy of grids up to 512;
+// ctile 3 takes the pipelined pass at every size
 template <typename T, int L, int MODE>
 static int zinv_LM(hit3d_ctx *c, int nf, int sfield, const double2 *src, int64_t src_fs, cx<T> *dst,
                    int64_t dst_fs, int dpitch)
 {
+    if constexpr (MODE == PRE_COPY) {
+        if (c->ctile == 3) {
+            IOSpec<T, T, PRE_COPY> io;
+            io.src = src; io.dst = dst; io.fs_src = src_fs; io.fs_dst = dst_fs;
+            io.n = c->n; io.psrc = c->P64; io.pdst = dpitch; io.ncol = c->nh; io.sfield = sfield;
+            io.dx = c->dx;
+            int rows = c->n;
+            if (c->kc_active >= 0) {
+                io.kl = io.ko = c->kc_active;
+                io.ncol = c->kc_active + 1;
+                rows = 2 * c->kc_active + 1;
+            }
+            int nz = nf;
+            if (c->bruns > 0) {
+                io.nfr = nf;
+                io.rs_src = c->bru;
+                io.rs_dst = c->brw;
+                nz = nf * c->bruns;
+            }
+            return colpipe_launch<T, L, false>(c, io, io.ncol, rows, nz);
+        }
+    }
     if constexpr (L <= 512 && MODE == PRE_COPY) {
         if (c->ctile == 1) return zinv_LMC<T, L, MODE, 1>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
         if (c->ctile == 2) return zinv_LMC<T, L, MODE, 2>(c, nf, sfield, src, src_fs, dst, dst_fs, dpitch);
@@ -162,6 +204,30 @@ static int spass_LAC(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, 
 template <typename T, int L, bool YPASS>
 static int spass_LA(hit3d_ctx *c, int axis, bool fwd, cx<T> *base, int64_t fs, int pitch, int nf)
 {
+    if (c->ctile == 3) {
+        IOPlain<T, T, T> io;
+        io.src = base; io.dst = base; io.fs_src = fs; io.fs_dst = fs; io.ncol = c->nh;
+        if (axis == 1) { io.sa_src = io.sa_dst = pitch; io.so_src = io.so_dst = (int64_t)c->n * pitch; }
+        else { io.sa_src = io.sa_dst = (int64_t)c->n * pitch; io.so_src = io.so_dst = pitch; }
+        int rows = c->n;
+        if (c->kc_active >= 0) {
+            io.n = c->n;
+            io.ncol = c->kc_active + 1;
+            if (fwd) io.ks = c->kc_active;
+            else io.kl = c->kc_active;
+            if (axis == 2) {
+                io.ko = c->kc_active;
+                rows = 2 * c->kc_active + 1;
+            }
+        }
+        int nz = nf;
+        if (c->bruns > 0) {
+            io.nfr = nf;
+            io.rs_src = io.rs_dst = c->brw;
+            nz = nf * c->bruns;
+        }
+        return fwd ? colpipe_launch<T, L, true>(c, io, io.ncol, rows, nz) : colpipe_launch<T, L, false>(c, io, io.ncol, rows, nz);
+    }
     if constexpr (L <= 512) {
         if (c->ctile == 1) return spass_LAC<T, L, YPASS, 1>(c, axis, fwd, base, fs, pitch, nf);
         if (c->ctile == 2) return spass_LAC<T, L, YPASS, 2>(c, axis, fwd, base, fs, pitch, nf);
@@ -1494,7 +1560,7 @@ extern "C" int hit3d_gpu_autotune_columns(hit3d_ctx *c, int32_t *tile, double *m
     float bt = 1e30f;
     for (int ct = 0; ct < kColTiles; ct++) {
         if (ms_out) ms_out[ct] = 0.0;
-        if (c->n > 512 && ct > 0) continue;
+        if (c->n > 512 && ct > 0 && ct < 3) continue;
         c->ctile = ct;
         float ms = 0.f;
         const int rc = c->p.precision == 0 ? time_columns<double>(c, &ms) : time_columns<float>(c, &ms);
@@ -1560,6 +1626,15 @@ extern "C" int hit3d_gpu_pruned(hit3d_ctx *c)
     H3D_CHECK(cudaSetDevice(c->dev));
     H3D_TRY(ensure_alias_state(c));
     return c->pruned ? 1 : 0;
+}
+
+extern "C" int hit3d_gpu_set_column_tile(hit3d_ctx *c, int32_t t)
+{
+    if (!c) return h3d_set_error_msg(-1, "null context");
+    if (t < 0 || t >= kColTiles || (c->n > 512 && t > 0 && t < 3))
+        return h3d_set_error_msg(-1, "hit3d_gpu_set_column_tile: no such column tile for this grid");
+    c->ctile = t;
+    return 0;
 }
 
 extern "C" int hit3d_gpu_set_variant(hit3d_ctx *c, int32_t v)
@@ -2395,7 +2470,8 @@ extern "C" int hit3d_batch_autotune(hit3d_batch *b, int32_t *choice, double *ms)
         bt = 1e30f;
         if (mq)
             for (int ct = 0; ct < kColTiles; ct++) mq[kBatchVariants + ct] = 0.0;
-        for (int ct = 0; ct < (c->n <= 512 ? kColTiles : 1); ct++) {
+        for (int ct = 0; ct < kColTiles; ct++) {
+            if (c->n > 512 && ct > 0 && ct < 3) continue;
             c->ctile = ct;
             float t = 0.f;
             H3D_TRY(class_time(b, k, 1, &t));

@@ -28,10 +28,11 @@ template <typename T, int L> struct RowCfg {
     static constexpr size_t SMEM = (size_t)Lay<L, TC, true>::elems * sizeof(cx<T>);
 };
 
-// Column-tile shapes the tuners pick from for grids up to 512 (ct = the
-// context's `ctile`): 0 the default ColCfg, 1 half as many kx columns per CTA,
-// 2 twice as many; at least one warp per CTA
-constexpr int kColTiles = 3;
+// Column-tile shapes the tuners pick from (ct = the context's `ctile`): 0 the
+// default ColCfg, 1 half as many kx columns per CTA, 2 twice as many (grids up
+// to 512; at least one warp per CTA), 3 the pipelined pass (k_colfft_pipe,
+// every grid)
+constexpr int kColTiles = 4;
 template <typename T, int L, bool YPASS, int CT> struct ColCfgT {
     using B = ColCfg<T, L, YPASS>;
     static constexpr int TC = CT == 0 ? B::TC : CT == 1 ? B::TC / 2 : B::TC * 2;

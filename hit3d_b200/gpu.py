@@ -119,6 +119,7 @@ SIGNATURES = [
     ("hit3d_gpu_launch_count", C.c_int64, [_vp]),
     ("hit3d_gpu_autotune", C.c_int, [_vp, C.POINTER(_i32), _dp]),
     ("hit3d_gpu_autotune_columns", C.c_int, [_vp, C.POINTER(_i32), _dp]),
+    ("hit3d_gpu_set_column_tile", C.c_int, [_vp, _i32]),
     ("hit3d_gpu_set_variant", C.c_int, [_vp, _i32]),
     ("hit3d_gpu_set_pruning", C.c_int, [_vp, _i32]),
     ("hit3d_gpu_set_update_fusion", C.c_int, [_vp, _i32]),
@@ -337,11 +338,15 @@ class Context:
         return v.value, [x for x in ms.tolist() if x == x]
 
     def autotune_columns(self):
-        """Pick the column-tile shape of the strided passes; returns (tile, ms of the 3 shapes)."""
+        """Pick the column-tile shape of the strided passes; returns (tile, ms of the 4 shapes)."""
         t = C.c_int32(0)
-        ms = np.zeros(3)
+        ms = np.zeros(4)
         _check(lib().hit3d_gpu_autotune_columns(self._h, C.byref(t), _ptr(ms)), "autotune_columns")
         return t.value, ms.tolist()
+
+    def set_column_tile(self, t: int):
+        _check(lib().hit3d_gpu_set_column_tile(self._h, int(t)), "set_column_tile")
+        self.column_tile = int(t)
 
     def set_variant(self, v: int):
         _check(lib().hit3d_gpu_set_variant(self._h, int(v)), "set_variant")

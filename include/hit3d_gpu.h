@@ -172,11 +172,15 @@ int hit3d_gpu_step_profile(hit3d_ctx *ctx, int32_t nsteps, int32_t *fov, int32_t
 #define HIT3D_FUSED_VARIANTS 15
 int hit3d_gpu_autotune(hit3d_ctx *ctx, int32_t *variant, double *ms);
 /* Column-tile shape of the strided y and z passes (0: the default, 1: half, 2:
- * twice the kx columns per CTA; grids up to 512, larger grids keep 0): times the
- * passes of one step on the context's work fields (the state is read, never
- * written) and keeps the fastest.  *tile receives it, ms[0..3) the times (0 for
- * shapes not tried).  No counterpart in the reference. */
+ * twice the kx columns per CTA, grids up to 512; 3: the pipelined passes, a grid
+ * of resident CTAs that bring the tile after next into shared memory while they
+ * transform the current one, every grid): times the passes of one step on the
+ * context's work fields (the state is read, never written) and keeps the
+ * fastest.  *tile receives it, ms[0..4) the times (0 for shapes not tried).  No
+ * counterpart in the reference. */
 int hit3d_gpu_autotune_columns(hit3d_ctx *ctx, int32_t *tile, double *ms);
+/* Fix the column-tile shape (0-3 as above) instead of tuning it. */
+int hit3d_gpu_set_column_tile(hit3d_ctx *ctx, int32_t tile);
 int hit3d_gpu_set_variant(hit3d_ctx *ctx, int32_t variant);
 
 /* 2/3-rule pruning (no reference counterpart; on by default).  With the 2/3
@@ -349,10 +353,11 @@ int64_t hit3d_batch_graph_launches(hit3d_batch *b);
 int hit3d_batch_nclasses(hit3d_batch *b);
 /* Per size class, time the fused x-pass launch shapes that walk several runs
  * (variants 8-14) and the column-tile shapes of the strided passes (0: the
- * default, 1: half, 2: twice the kx columns per CTA; grids up to 512) on the
+ * default, 1: half, 2: twice the kx columns per CTA, grids up to 512; 3: the
+ * pipelined passes) on the
  * class's own buffers, reading the state without changing it, and keep the
  * fastest of each.  choice[2k], choice[2k+1] receive class k's picks; ms (may
- * be NULL) receives 10 times in ms per class (7 x-pass variants, then 3 tiles,
+ * be NULL) receives 11 times in ms per class (7 x-pass variants, then 4 tiles,
  * NaN-free: tiles not tried report 0).  The next step re-records the graph. */
 int hit3d_batch_autotune(hit3d_batch *b, int32_t *choice, double *ms);
 void hit3d_batch_destroy(hit3d_batch *b);

@@ -144,7 +144,7 @@ def test_batch_refuses_a_learned_closure_run_without_weights():
 
 def test_batch_autotune_picks_shapes_and_keeps_results():
     """The per-class tuner picks a staged x-pass variant (8-14) and a column
-    tile (0-2) per size class without changing the state; afterwards every run
+    tile (0-3) per size class without changing the state; afterwards every run
     equals the same run stepped on its own with that variant (the column tile
     does not change any run's arithmetic)."""
     from hit3d_b200 import Context, Params
@@ -157,7 +157,7 @@ def test_batch_autotune_picks_shapes_and_keeps_results():
     picks = b.autotune()
     assert b.nclasses == 2 and len(picks) == 2
     for v, tile, ms_v, ms_t in picks:
-        assert 8 <= v <= 14 and 0 <= tile <= 2
+        assert 8 <= v <= 14 and 0 <= tile <= 3
         assert all(x > 0 for x in ms_v) and all(x > 0 for x in ms_t)
     for r, c in enumerate(b.contexts):
         assert np.array_equal(c.download_fields(), f0[r])
