@@ -48,11 +48,12 @@ template <class IO> struct ColIn;
 template <typename T, typename TI, typename TO> struct ColIn<IOPlain<T, TI, TO>> { using type = TI; };
 template <typename T, typename TO> struct ColIn<IOSpec<T, TO, PRE_COPY>> { using type = double; };
 
-// launch shape: 128-byte rows of input columns, at most 64 KB per buffer
+// launch shape: 64-byte rows of input columns, at most 32 KB per buffer, so
+// that several CTAs share an SM
 template <typename T, typename TI, int L> struct ColPipeCfg {
     static constexpr int ES = sizeof(cx<TI>) > sizeof(cx<T>) ? (int)sizeof(cx<TI>) : (int)sizeof(cx<T>);
-    static constexpr int TC0 = 128 / (int)sizeof(cx<TI>);
-    static constexpr int TC = (size_t)TC0 * L * ES <= 64 * 1024 ? TC0 : (int)(64 * 1024 / ((size_t)L * ES));
+    static constexpr int TC0 = 64 / (int)sizeof(cx<TI>);
+    static constexpr int TC = (size_t)TC0 * L * ES <= 32 * 1024 ? TC0 : (int)(32 * 1024 / ((size_t)L * ES));
     static constexpr int NT0 = TC * L / plan_rmax(L);
     static constexpr int NT = NT0 > 512 ? 512 : NT0 < 32 ? 32 : NT0;
     static constexpr size_t BUF = (size_t)Lay<L, TC, false>::elems * ES;  // bytes of one buffer
