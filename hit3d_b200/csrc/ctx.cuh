@@ -101,6 +101,8 @@ struct Randu {
 };
 }  // namespace
 
+constexpr int kCopyStreams = 2;  // copy streams per direction of hit3d_gpu_step_host (4 measured slower)
+
 struct hit3d_ctx {
     hit3d_params p;
     int n, nh, P64, P32, nsc, dev, kmax, nsm;
@@ -150,6 +152,11 @@ struct hit3d_ctx {
     // pipelined host transfers (hit3d_gpu_step_host), created on first use: copy
     // streams, staging fields in the reference layout and their events
     cudaStream_t cs_h2d, cs_d2h;
+    // further copy streams per direction (the copies of one transfer are spread
+    // over kCopyStreams streams, so that several copy engines share them) and
+    // the events that join them back
+    cudaStream_t cs_up[kCopyStreams - 1], cs_dn[kCopyStreams - 1];
+    cudaEvent_t ev_up[kCopyStreams - 1], ev_dn[kCopyStreams - 1];
     double2 *sin, *sout[2];  // one input staging set, two output sets used in turn
     int nstage_io;           // fields each staging set holds
     cudaEvent_t ev_in_ready, ev_in_free, ev_out_ready, ev_out_free[2];

@@ -317,20 +317,39 @@ template <typename KF> static dim3 pw_grid(const hit3d_ctx *c, KF kernel)
 
 // z forward pass of the six velocity products (after their y pass, in P) fused
 // with the 2/3-rule update of U and RO
-template <typename T, int L> static int zfwd_update_L(hit3d_ctx *c, const StepArgs &a, const cx<T> *P)
+// with the update of U and RO; zinv: and the z inverse of the new u, v, w into P[0..2]
+template <typename T, int L, bool PRUNED> static int zfwd_update_LP(hit3d_ctx *c, const ZUpdArgs<T> &za)
 {
     using CF = ZUpdCfg<T, L>;
-    auto k = k_zfwd_update<T, L, CF::TC, CF::NT, CF::MINB>;
+    auto k = k_zfwd_update<T, L, CF::TC, CF::NT, CF::NB, CF::MINB, PRUNED>;
     H3D_TRY(set_smem(k, CF::SMEM));
-    const int ncol = c->kc_active >= 0 ? c->kc_active + 1 : c->nh;
-    const int rows = c->kc_active >= 0 ? 2 * c->kc_active + 1 : c->n;
-    k<<<dim3((ncol + CF::TC - 1) / CF::TC, rows), CF::NT, CF::SMEM, c->st>>>(a, P, ncol, c->U, c->RO, twid<T>(c));
+    const int64_t ntiles = (int64_t)((za.ncol + CF::TC - 1) / CF::TC) * za.nrows;
+    int64_t grid = (int64_t)c->nsm * CF::MINB;
+    grid = grid < ntiles ? grid : ntiles;
+    k<<<(unsigned)grid, CF::NT, CF::SMEM, c->st>>>(za, twid<T>(c));
     H3D_LAUNCH_CHECK();
     return 0;
 }
-template <typename T> static int zfwd_update(hit3d_ctx *c, const StepArgs &a, const cx<T> *P)
+template <typename T, int L> static int zfwd_update_L(hit3d_ctx *c, const ZUpdArgs<T> &za)
 {
-#define CALL(L) zfwd_update_L<T, L>(c, a, P)
+    if (c->kc_active >= 0) {
+        if (c->kc_active != L / 3) return h3d_set_error_msg(-1, "fused z pass + update: pruning cutoff is not N/3");
+        return zfwd_update_LP<T, L, true>(c, za);
+    }
+    return zfwd_update_LP<T, L, false>(c, za);
+}
+template <typename T> static int zfwd_update(hit3d_ctx *c, const StepArgs &a, cx<T> *P, bool zinv)
+{
+    if (c->bruns > 0) return h3d_set_error_msg(-1, "fused z pass + update: not for batch classes");
+    ZUpdArgs<T> za;
+    za.a = a;
+    za.W = P;
+    za.U = c->U;
+    za.RO = c->RO;
+    za.ncol = c->kc_active >= 0 ? c->kc_active + 1 : c->nh;
+    za.nrows = c->kc_active >= 0 ? 2 * c->kc_active + 1 : c->n;
+    za.zinv = zinv ? 1 : 0;
+#define CALL(L) zfwd_update_L<T, L>(c, za)
     H3D_DISPATCH(c->n, CALL)
 #undef CALL
 }
@@ -430,7 +449,12 @@ static int ensure_alias_state(hit3d_ctx *c)
     return 0;
 }
 
-template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_s, Prof *prof = nullptr)
+// zin: W[0..2] already hold the z inverse of this state's velocity (written by
+// the previous step's fused z pass + update), so the velocity z inverse is
+// skipped; zout: have the fused z pass + update write the next step's.  Both
+// need the fused path (chain_ok).
+template <typename T>
+static int step_once(hit3d_ctx *c, int euler_v, int euler_s, Prof *prof = nullptr, bool zin = false, bool zout = false)
 {
     PruneScope prune_scope(c);
     const hit3d_params &p = c->p;
@@ -527,7 +551,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
     for (int pass = 0; pass < npass; pass++) {
         const int mode = pass == 0 ? PRE_COPY : PRE_SHIFT;
         MARK(0);
-        H3D_TRY(zinv<T>(c, 3, mode, 0, c->U, c->fs64, Wf(0), wfs, wp));
+        if (!(zin && pass == 0)) H3D_TRY(zinv<T>(c, 3, mode, 0, c->U, c->fs64, Wf(0), wfs, wp));
         for (int s = 0; s < ns; s++)
             H3D_TRY(zinv<T>(c, 1, mode, 0, c->U + (3 + s) * c->fs64, c->fs64, Wf(6 + 3 * s), wfs, wp));
         MARK(1);
@@ -585,7 +609,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
         MARK(4);
         // without LES, the velocity products' z pass runs inside the update
         // kernel (k_zfwd_update); the scalars' products take the plain z pass
-        const bool fuse = c->fuse_update && p.dealias == 0 && p.les_model == 0;
+        const bool fuse = c->fuse_update && p.dealias == 0 && p.les_model == 0 && c->bruns == 0;
         if (fuse) {
             if (nprod > 6) H3D_TRY(spass<T>(c, 2, true, Wf(6), wfs, wp, nprod - 6));
         } else {
@@ -816,7 +840,7 @@ template <typename T> static int step_once(hit3d_ctx *c, int euler_v, int euler_
                 H3D_LAUNCH_CHECK();
             }
             if (fuse) {
-                H3D_TRY(zfwd_update<T>(c, a, Wf(0)));
+                H3D_TRY(zfwd_update<T>(c, a, Wf(0), zout));
             } else {
                 k_update_vel_23<T><<<pw_grid(c, k_update_vel_23<T>), 256, 0, c->st>>>(a, Wf(0), tau, c->U, c->RO);
                 H3D_LAUNCH_CHECK();
@@ -1051,6 +1075,14 @@ extern "C" void hit3d_gpu_finalize(hit3d_ctx *c)
     if (c->cs_h2d) {
         cudaStreamSynchronize(c->cs_h2d);
         cudaStreamSynchronize(c->cs_d2h);
+        for (int q = 0; q < kCopyStreams - 1; q++) {
+            cudaStreamSynchronize(c->cs_up[q]);
+            cudaStreamSynchronize(c->cs_dn[q]);
+            cudaStreamDestroy(c->cs_up[q]);
+            cudaStreamDestroy(c->cs_dn[q]);
+            cudaEventDestroy(c->ev_up[q]);
+            cudaEventDestroy(c->ev_dn[q]);
+        }
         cudaStreamDestroy(c->cs_h2d);
         cudaStreamDestroy(c->cs_d2h);
         cudaEventDestroy(c->ev_in_ready);
@@ -1134,6 +1166,12 @@ static int io_setup(hit3d_ctx *c, int nf)
     if (!c->cs_h2d) {
         H3D_CHECK(cudaStreamCreateWithFlags(&c->cs_h2d, cudaStreamNonBlocking));
         H3D_CHECK(cudaStreamCreateWithFlags(&c->cs_d2h, cudaStreamNonBlocking));
+        for (int q = 0; q < kCopyStreams - 1; q++) {
+            H3D_CHECK(cudaStreamCreateWithFlags(&c->cs_up[q], cudaStreamNonBlocking));
+            H3D_CHECK(cudaStreamCreateWithFlags(&c->cs_dn[q], cudaStreamNonBlocking));
+            H3D_CHECK(cudaEventCreateWithFlags(&c->ev_up[q], cudaEventDisableTiming));
+            H3D_CHECK(cudaEventCreateWithFlags(&c->ev_dn[q], cudaEventDisableTiming));
+        }
         H3D_CHECK(cudaEventCreateWithFlags(&c->ev_in_ready, cudaEventDisableTiming));
         H3D_CHECK(cudaEventCreateWithFlags(&c->ev_in_free, cudaEventDisableTiming));
         H3D_CHECK(cudaEventCreateWithFlags(&c->ev_out_ready, cudaEventDisableTiming));
@@ -1144,6 +1182,10 @@ static int io_setup(hit3d_ctx *c, int nf)
         H3D_CHECK(cudaStreamSynchronize(c->st));
         H3D_CHECK(cudaStreamSynchronize(c->cs_h2d));
         H3D_CHECK(cudaStreamSynchronize(c->cs_d2h));
+        for (int q = 0; q < kCopyStreams - 1; q++) {
+            H3D_CHECK(cudaStreamSynchronize(c->cs_up[q]));
+            H3D_CHECK(cudaStreamSynchronize(c->cs_dn[q]));
+        }
         for (double2 **q : {&c->sin, &c->sout[0], &c->sout[1]}) {
             if (*q) cudaFree(*q);
             *q = nullptr;
@@ -1263,8 +1305,11 @@ static int band_boxes(int n, int kc, BandBox *b)
     return q;
 }
 // one field's band between host memory (row pitch hp bytes, n rows per ky slice)
-// and the packed band on the device, as up to four strided box copies
-static cudaError_t band_copy(int n, int kc, double *host, size_t hp, double2 *packed, bool to_device, cudaStream_t s)
+// and the packed band on the device, as up to four strided box copies, which
+// go round the streams s[] (rr counts the boxes issued), so that several copy
+// engines of the direction share the rows
+static cudaError_t band_copy(int n, int kc, double *host, size_t hp, double2 *packed, bool to_device,
+                             const cudaStream_t (&s)[kCopyStreams], int &rr)
 {
     BandBox b[4];
     const int nbx = band_boxes(n, kc, b), nb = 2 * kc + 1;
@@ -1279,7 +1324,7 @@ static cudaError_t band_copy(int n, int kc, double *host, size_t hp, double2 *pa
         if (to_device) { m.srcPtr = hptr; m.srcPos = hpos; m.dstPtr = dptr; m.dstPos = dpos; m.kind = cudaMemcpyHostToDevice; }
         else { m.srcPtr = dptr; m.srcPos = dpos; m.dstPtr = hptr; m.dstPos = hpos; m.kind = cudaMemcpyDeviceToHost; }
         m.extent = make_cudaExtent(w, (size_t)b[q].nz, (size_t)b[q].ny);
-        cudaError_t e = cudaMemcpy3DAsync(&m, s);
+        cudaError_t e = cudaMemcpy3DAsync(&m, s[rr++ % kCopyStreams]);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -1309,17 +1354,45 @@ extern "C" int hit3d_gpu_step_host(hit3d_ctx *c, int32_t nio, const double *cons
     const size_t width = (size_t)c->nh * sizeof(double2), hp = (size_t)ld1 * sizeof(double);
     const size_t rows = (size_t)c->n * c->n;
     const int kc = c->n / 3;
-    auto copy = [&](void *dst, size_t dp, const void *src, size_t sp, cudaMemcpyKind kind, cudaStream_t s) {
-        return dp == sp && sp == width ? cudaMemcpyAsync(dst, src, width * rows, kind, s)
-                                       : cudaMemcpy2DAsync(dst, dp, src, sp, width, rows, kind, s);
+    // one field as kCopyStreams row ranges, one per copy stream
+    auto copy = [&](void *dst, size_t dp, const void *src, size_t sp, cudaMemcpyKind kind,
+                    const cudaStream_t (&s)[kCopyStreams]) {
+        for (int q = 0; q < kCopyStreams; q++) {
+            const size_t r0 = rows * q / kCopyStreams, r1 = rows * (q + 1) / kCopyStreams;
+            char *d = static_cast<char *>(dst) + r0 * dp;
+            const char *sr = static_cast<const char *>(src) + r0 * sp;
+            cudaError_t e = dp == sp && sp == width ? cudaMemcpyAsync(d, sr, width * (r1 - r0), kind, s[q])
+                                                    : cudaMemcpy2DAsync(d, dp, sr, sp, width, r1 - r0, kind, s[q]);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
     };
-    auto upload = [&](int i) -> int {  // host in[i] -> sin, on the copy-in stream
-        H3D_CHECK(cudaStreamWaitEvent(c->cs_h2d, c->ev_in_free, 0));
+    cudaStream_t up[kCopyStreams], down[kCopyStreams];
+    up[0] = c->cs_h2d;
+    down[0] = c->cs_d2h;
+    for (int q = 1; q < kCopyStreams; q++) { up[q] = c->cs_up[q - 1]; down[q] = c->cs_dn[q - 1]; }
+    // every copy stream of a direction waits for `start`; the first then waits
+    // for the others, so that an event recorded on it covers the whole transfer
+    auto fork = [&](const cudaStream_t (&s)[kCopyStreams], cudaEvent_t start) -> int {
+        for (int q = 0; q < kCopyStreams; q++) H3D_CHECK(cudaStreamWaitEvent(s[q], start, 0));
+        return 0;
+    };
+    auto join = [&](const cudaStream_t (&s)[kCopyStreams], cudaEvent_t *ev) -> int {
+        for (int q = 1; q < kCopyStreams; q++) {
+            H3D_CHECK(cudaEventRecord(ev[q - 1], s[q]));
+            H3D_CHECK(cudaStreamWaitEvent(s[0], ev[q - 1], 0));
+        }
+        return 0;
+    };
+    auto upload = [&](int i) -> int {  // host in[i] -> sin, on the copy-in streams
+        H3D_TRY(fork(up, c->ev_in_free));
+        int rr = 0;
         for (int f = 0; f < nf; f++) {
             double *h = const_cast<double *>(in[i]) + (size_t)f * ld1 * rows;
-            if (band_only) H3D_CHECK(band_copy(c->n, kc, h, hp, c->sin + f * fe, true, c->cs_h2d));
-            else H3D_CHECK(copy(c->sin + f * fe, width, h, hp, cudaMemcpyHostToDevice, c->cs_h2d));
+            if (band_only) H3D_CHECK(band_copy(c->n, kc, h, hp, c->sin + f * fe, true, up, rr));
+            else H3D_CHECK(copy(c->sin + f * fe, width, h, hp, cudaMemcpyHostToDevice, up));
         }
+        H3D_TRY(join(up, c->ev_up));
         H3D_CHECK(cudaEventRecord(c->ev_in_ready, c->cs_h2d));
         return 0;
     };
@@ -1353,12 +1426,14 @@ extern "C" int hit3d_gpu_step_host(hit3d_ctx *c, int32_t nio, const double *cons
             H3D_LAUNCH_CHECK();
         }
         H3D_CHECK(cudaEventRecord(c->ev_out_ready, c->st));
-        H3D_CHECK(cudaStreamWaitEvent(c->cs_d2h, c->ev_out_ready, 0));
+        H3D_TRY(fork(down, c->ev_out_ready));
+        int rr = 0;
         for (int f = 0; f < nf; f++) {
             double *h = out[i] + (size_t)f * ld1 * rows;
-            if (band_only) H3D_CHECK(band_copy(c->n, kc, h, hp, so + f * fe, false, c->cs_d2h));
-            else H3D_CHECK(copy(h, hp, so + f * fe, width, cudaMemcpyDeviceToHost, c->cs_d2h));
+            if (band_only) H3D_CHECK(band_copy(c->n, kc, h, hp, so + f * fe, false, down, rr));
+            else H3D_CHECK(copy(h, hp, so + f * fe, width, cudaMemcpyDeviceToHost, down));
         }
+        H3D_TRY(join(down, c->ev_dn));
         H3D_CHECK(cudaEventRecord(c->ev_out_free[ob], c->cs_d2h));
     }
     // the compute stream ends after the last download, so that events recorded
@@ -1370,6 +1445,14 @@ extern "C" int hit3d_gpu_step_host(hit3d_ctx *c, int32_t nio, const double *cons
     return 0;
 }
 
+// steps of one call chain the velocity z inverse through the fused z pass +
+// update (every step but the first skips it, every step but the last writes
+// the next one's); nothing outside a call sees the difference
+static bool chain_ok(const hit3d_ctx *c)
+{
+    return c->fuse_update && c->p.dealias == 0 && c->p.les_model == 0 && c->bruns == 0;
+}
+
 extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_t *fos, double *courant)
 {
     if (!c) return h3d_set_error_msg(-1, "null context");
@@ -1379,8 +1462,11 @@ extern "C" int hit3d_gpu_step(hit3d_ctx *c, int32_t nsteps, int32_t *fov, int32_
     H3D_CHECK(cudaSetDevice(c->dev));
     H3D_TRY(ensure_alias_state(c));
     int ev = fov ? (*fov != 0) : 0, es = fos ? (*fos != 0) : 0;
+    const bool chain = chain_ok(c);
     for (int it = 0; it < nsteps; it++) {
-        int rc = c->p.precision == 0 ? step_once<double>(c, ev, es) : step_once<float>(c, ev, es);
+        const bool zin = chain && it > 0, zout = chain && it + 1 < nsteps;
+        int rc = c->p.precision == 0 ? step_once<double>(c, ev, es, nullptr, zin, zout)
+                                     : step_once<float>(c, ev, es, nullptr, zin, zout);
         if (rc) return rc;
         ev = 0;
         if (c->int_scalars) es = 0;
@@ -1445,9 +1531,12 @@ extern "C" int hit3d_gpu_step_profile(hit3d_ctx *c, int32_t nsteps, int32_t *fov
     for (int i = 0; i < Prof::MAXM; i++) H3D_CHECK(cudaEventCreate(&prof.ev[i]));
     int ev = fov ? (*fov != 0) : 0, es = fos ? (*fos != 0) : 0;
     int rc = 0;
+    const bool chain = chain_ok(c);
     for (int it = 0; it < nsteps && rc == 0; it++) {
         prof.n = 0;
-        rc = c->p.precision == 0 ? step_once<double>(c, ev, es, &prof) : step_once<float>(c, ev, es, &prof);
+        const bool zin = chain && it > 0, zout = chain && it + 1 < nsteps;
+        rc = c->p.precision == 0 ? step_once<double>(c, ev, es, &prof, zin, zout)
+                                 : step_once<float>(c, ev, es, &prof, zin, zout);
         if (rc) break;
         ev = 0;
         if (c->int_scalars) es = 0;

@@ -150,6 +150,27 @@ struct StepArgs {
     const double *nu_r, *dt_r;
 };
 
+// s = k_x a + k_y b + k_z c rounded in that order (one product, then two fused
+// multiply-adds), so that the separate update and the z pass fused with the
+// update (which adds the products as their transforms come out) agree exactly
+H3D_D double kdot3(double kx, double a, double ky, double b, double kz, double c)
+{
+    return __fma_rn(kz, c, __fma_rn(ky, b, __dmul_rn(kx, a)));
+}
+
+// RHS of one mode with ialias == 0 (rhs_velocity.f90:85-142): -i k_j P_cj - nu k^2 u_c
+// from the sums s_c = k_j P_cj
+H3D_D void vel23_rhs(const ModeIdx &m, const double2 (&s)[3], const double2 (&u)[3], double nu, double2 (&r)[3])
+{
+    const double kx = m.ax, ky = m.ay, kz = m.az;
+    const double t4 = -nu * (kx * kx + ky * ky + kz * kz);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const double2 tt = make_double2(-s[c].x, -s[c].y);
+        r[c] = make_double2(-tt.y + t4 * u[c].x, tt.x + t4 * u[c].y);
+    }
+}
+
 // 2/3 rule (rhs_velocity.f90:85-142) + forcing + AB2 + pressure.
 // P: six product spectra [uu uv uw vv vw ww]; U, RO: velocity state and old RHS
 // TAU (optional, Smagorinsky): six subgrid-stress spectra [t11 t12 t13 t22 t23 t33]
@@ -177,13 +198,10 @@ __global__ void k_update_vel_23(const StepArgs a, const cx<TP> *__restrict__ P, 
             double2 p11 = ld2<TP>(P, po), p12 = ld2<TP>(P, po + a.pfs), p13 = ld2<TP>(P, po + 2 * a.pfs);
             double2 p22 = ld2<TP>(P, po + 3 * a.pfs), p23 = ld2<TP>(P, po + 4 * a.pfs), p33 = ld2<TP>(P, po + 5 * a.pfs);
             double kx = m.ax, ky = m.ay, kz = m.az;
-            double2 t1 = make_double2(-(kx * p11.x + ky * p12.x + kz * p13.x), -(kx * p11.y + ky * p12.y + kz * p13.y));
-            double2 t2 = make_double2(-(kx * p12.x + ky * p22.x + kz * p23.x), -(kx * p12.y + ky * p22.y + kz * p23.y));
-            double2 t3 = make_double2(-(kx * p13.x + ky * p23.x + kz * p33.x), -(kx * p13.y + ky * p23.y + kz * p33.y));
-            double t4 = -nu * (kx * kx + ky * ky + kz * kz);
-            double2 tt[3] = {t1, t2, t3};
-#pragma unroll
-            for (int c = 0; c < 3; c++) r[c] = make_double2(-tt[c].y + t4 * u[c].x, tt[c].x + t4 * u[c].y);
+            const double2 s[3] = {make_double2(kdot3(kx, p11.x, ky, p12.x, kz, p13.x), kdot3(kx, p11.y, ky, p12.y, kz, p13.y)),
+                                  make_double2(kdot3(kx, p12.x, ky, p22.x, kz, p23.x), kdot3(kx, p12.y, ky, p22.y, kz, p23.y)),
+                                  make_double2(kdot3(kx, p13.x, ky, p23.x, kz, p33.x), kdot3(kx, p13.y, ky, p23.y, kz, p33.y))};
+            vel23_rhs(m, s, u, nu, r);
             if (TAU != nullptr) {
                 double2 s11 = ld2<TP>(TAU, po), s12 = ld2<TP>(TAU, po + a.pfs), s13 = ld2<TP>(TAU, po + 2 * a.pfs);
                 double2 s22 = ld2<TP>(TAU, po + 3 * a.pfs), s23 = ld2<TP>(TAU, po + 4 * a.pfs), s33 = ld2<TP>(TAU, po + 5 * a.pfs);

@@ -1,7 +1,9 @@
-"""The z forward pass of the velocity products fused with the update
-(k_zfwd_update) against the separate z pass + k_update_vel_23: the same
-state after several steps, pruned and unpruned, FP64 and FP32 transforms,
-forced and decaying, with passive scalars."""
+"""The z forward pass of the velocity products fused with the update and the
+next step's z inverse (k_zfwd_update) against the separate z passes +
+k_update_vel_23: the same state after several steps of one call (every step
+but the first takes its z inverse from the previous step's fused pass),
+pruned and unpruned, FP64 and FP32 transforms, forced and decaying, with
+passive scalars, up to the 512^3 workload."""
 import numpy as np
 import pytest
 
@@ -17,6 +19,9 @@ pytestmark = pytest.mark.gpu
     (48, 0, dict(n_scalars=2, sc=[0.7, 1.0], scalar_type=[0, 1]), True),
     (128, 0, {}, True),
     (128, 1, {}, False),
+    (256, 0, {}, True),
+    (512, 0, dict(nu=1.0 / 3000.0, dt=2e-4), True),
+    (512, 1, dict(nu=1.0 / 3000.0, dt=2e-4), True),
 ])
 def test_fused_update_matches_separate_passes(n, precision, extra, prune):
     from hit3d_b200 import Context, Params
@@ -33,6 +38,7 @@ def test_fused_update_matches_separate_passes(n, precision, extra, prune):
         out.append((c.download_fields(), c.download_rhs_old()))
         c.close()
     (f1, r1), (f0, r0) = out
+    # the sums k.P are rounded in the same order on both paths
     for a, b in ((f1, f0), (r1, r0)):
         err = np.abs(a - b).max() / np.abs(b).max()
         assert err <= 1e-14, err
