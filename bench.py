@@ -462,6 +462,19 @@ def _sig(x, d=4):
     return x
 
 
+def ek_err_by_decade(e32, e64):
+    """Largest relative E(k) error of the FP32 form per band of shells, banded by
+    the shell's energy over the peak shell's: [1e-2, 1], [1e-4, 1e-2], ...,
+    [1e-12, 1e-10]; None for a band without shells."""
+    r = e64 / e64.max()
+    rel = np.abs(e32 - e64) / np.where(e64 > 0, e64, 1.0)
+    out = {}
+    for d in range(0, 12, 2):
+        m = (r <= 10.0 ** -d) & (r > 10.0 ** -(d + 2))
+        out["1e-%d" % (d + 2)] = float(rel[m].max()) if m.any() else None
+    return out
+
+
 def summarize(line):
     """Compact summary of the bench line: the headline, the FP32 form, the
     other configurations, the learned LES and the CPU baseline."""
@@ -474,6 +487,7 @@ def summarize(line):
         s["fp32"] = {"steps_per_s": f["value"], "speedup_vs_fp64": f["speedup_vs_fp64"],
                      "ek_max_rel_err_over_run": f.get("ek_max_rel_err_over_run"),
                      "ek_1e-4_crossed_at_step": f.get("ek_1e-4_crossed_at_step"),
+                     "ek_max_rel_err_above_1e-6_over_run": f.get("ek_max_rel_err_above_1e-6_over_run"),
                      "per_step": [[c["step"], c["ek_max_rel_err"], c["eps_rel_err"], c["skew_abs_err"]]
                                   for c in f.get("vs_fp64_every_%d_steps" % 50, [])]}
     oc = line.get("other_configs") or {}
@@ -660,8 +674,14 @@ def main():
             c32.step(args.cmp_every)
             e32, s32 = c32.stats()
             mk = e64 > 1e-12 * e64.max()
+            rel = np.abs(e32 - e64) / np.where(e64 > 0, e64, 1.0)
+            mk6 = e64 > 1e-6 * e64.max()
             cmp.append({"step": (k + 1) * args.cmp_every,
-                        "ek_max_rel_err": float(np.max(np.abs(e32[mk] - e64[mk]) / e64[mk])),
+                        "ek_max_rel_err": float(np.max(rel[mk])),
+                        # shells holding at least 1e-6 of the peak shell's energy
+                        "ek_max_rel_err_above_1e-6": float(np.max(rel[mk6])),
+                        "worst_shell": int(np.argmax(np.where(mk, rel, -1.0))) + 1,
+                        "ek_err_by_decade": ek_err_by_decade(e32, e64),
                         "energy_rel_err": abs(s32["energy"] - s64["energy"]) / s64["energy"],
                         "eps_rel_err": abs(s32["eps_v"] - s64["eps_v"]) / s64["eps_v"],
                         "skew_abs_err": abs(s32["skewness"] - s64["skewness"]),
@@ -670,6 +690,7 @@ def main():
         fp32["ek_max_rel_err_over_run"] = max(c["ek_max_rel_err"] for c in cmp) if cmp else None
         # the first compared step at which the E(k) error passes 1e-4 (None: not within the run)
         fp32["ek_1e-4_crossed_at_step"] = next((c["step"] for c in cmp if c["ek_max_rel_err"] > 1e-4), None)
+        fp32["ek_max_rel_err_above_1e-6_over_run"] = max(c["ek_max_rel_err_above_1e-6"] for c in cmp) if cmp else None
         c32.close()
 
     les = None

@@ -61,13 +61,24 @@ template <typename T, bool FWD> H3D_D void dft2(cx<T> &a, cx<T> &b)
     b = t - b;
 }
 
+// d + (-i t) (FWD) or d + i t, and d - (-i t) or d - i t, lane by lane (no
+// swapped pair is formed, so the packed FP32 adds serve only the plain sums)
+template <typename T, bool FWD> H3D_D cx<T> addmi(cx<T> d, cx<T> t)
+{
+    return FWD ? mk<T>(d.x + t.y, d.y - t.x) : mk<T>(d.x - t.y, d.y + t.x);
+}
+template <typename T, bool FWD> H3D_D cx<T> submi(cx<T> d, cx<T> t)
+{
+    return FWD ? mk<T>(d.x - t.y, d.y + t.x) : mk<T>(d.x + t.y, d.y - t.x);
+}
+
 template <typename T, bool FWD> H3D_D void dft4(cx<T> &a0, cx<T> &a1, cx<T> &a2, cx<T> &a3)
 {
-    cx<T> s0 = a0 + a2, d0 = a0 - a2, s1 = a1 + a3, d1 = mul_mi<FWD>(a1 - a3);
+    cx<T> s0 = a0 + a2, d0 = a0 - a2, s1 = a1 + a3, t = a1 - a3;
     a0 = s0 + s1;
     a2 = s0 - s1;
-    a1 = d0 + d1;
-    a3 = d0 - d1;
+    a1 = addmi<T, FWD>(d0, t);
+    a3 = submi<T, FWD>(d0, t);
 }
 
 template <typename T, bool FWD> H3D_D void dft3(cx<T> &a0, cx<T> &a1, cx<T> &a2)
@@ -93,11 +104,10 @@ template <typename T, bool FWD> H3D_D void dft8(cx<T> (&a)[8])
     dft4<T, FWD>(o0, o1, o2, o3);
     // twiddles w8^k, w8 = exp(-+ i pi/4)
     cx<T> t1 = FWD ? mk<T>(r2 * (o1.x + o1.y), r2 * (o1.y - o1.x)) : mk<T>(r2 * (o1.x - o1.y), r2 * (o1.y + o1.x));
-    cx<T> t2 = mul_mi<FWD>(o2);
     cx<T> t3 = FWD ? mk<T>(r2 * (-o3.x + o3.y), r2 * (-o3.y - o3.x)) : mk<T>(r2 * (-o3.x - o3.y), r2 * (-o3.y + o3.x));
     a[0] = e0 + o0; a[4] = e0 - o0;
     a[1] = e1 + t1; a[5] = e1 - t1;
-    a[2] = e2 + t2; a[6] = e2 - t2;
+    a[2] = addmi<T, FWD>(e2, o2); a[6] = submi<T, FWD>(e2, o2);  // e2 +- w8^2 o2
     a[3] = e3 + t3; a[7] = e3 - t3;
 }
 
