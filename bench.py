@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
-    ap.add_argument("--e2e-steps", type=int, default=6)
+    ap.add_argument("--e2e-steps", type=int, default=24,
+                    help="host-buffer steps of the e2e leg (the pipeline fills and drains once per call)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-transform form")
     ap.add_argument("--no-e2e", action="store_true")

@@ -401,6 +401,24 @@ struct Prof {
         if (prof) prof->mark(c->st, (s)); \
     } while (0)
 
+// launch shape of k_forcing_energy: one thread per shell of the band.  Shells
+// beyond the largest a grid has (nint(sqrt(3) N/2) + 1) hold no modes and add
+// nothing, so the band is cut there; one warp at least.
+struct ForcingLaunch {
+    int kfmax, threads;
+    size_t smem;
+};
+static ForcingLaunch forcing_launch(int n, int kfmax)
+{
+    const int shmax = (int)std::lround(std::sqrt(3.0) * (n / 2)) + 1;
+    ForcingLaunch f;
+    f.kfmax = kfmax < shmax ? kfmax : shmax;
+    f.threads = f.kfmax <= kFsmall ? 32 : (f.kfmax + 31) / 32 * 32;
+    if (f.threads > 1024) f.threads = 1024;
+    f.smem = f.kfmax <= kFsmall ? 0 : sizeof(double) * (size_t)f.kfmax;
+    return f;
+}
+
 // ---------------------------------------------------------------------------
 // one time step
 // LES-related transported fields (m_les.f90:111-300): k_sgs for the models with
@@ -523,7 +541,8 @@ static int step_once(hit3d_ctx *c, int euler_v, int euler_s, Prof *prof = nullpt
         }
     }
     if (p.flow_type == 1) {
-        k_forcing_energy<<<1, 32, 0, c->st>>>(c->n, c->P64, c->fs64, p.kfmax, c->U, c->d_fen);
+        const ForcingLaunch fl = forcing_launch(c->n, p.kfmax);
+        k_forcing_energy<<<1, fl.threads, fl.smem, c->st>>>(c->n, c->P64, c->fs64, fl.kfmax, c->U, c->d_fen);
         H3D_LAUNCH_CHECK();
     }
     // reaction sources of type-311 scalars, from this state (phase shift only,
@@ -898,7 +917,7 @@ static int ctx_init(const hit3d_params *p, hit3d_ctx **out, double2 *ext_U, doub
     if (p->n_scalars < 0 || p->n_scalars > HIT3D_MAX_SCALARS) return h3d_set_error_msg(-1, "hit3d_gpu_init: bad n_scalars");
     if (p->dealias != 0 && p->dealias != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: wrong dealias flag");
     if (p->flow_type == 1 && p->force_type != 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: WRONG FORCE TYPE");
-    if (p->flow_type == 1 && (p->kfmax < 1 || p->kfmax > 15)) return h3d_set_error_msg(-1, "hit3d_gpu_init: kfmax must be in 1..15");
+    if (p->flow_type == 1 && p->kfmax < 1) return h3d_set_error_msg(-1, "hit3d_gpu_init: kfmax must be at least 1");
     if (!(p->les_model >= 0 && p->les_model <= 7) && p->les_model != 10 && p->les_model != HIT3D_LES_LEARNED)
         return h3d_set_error_msg(-1, "hit3d_gpu_init: les_model must be 0 (none), 1 (Smagorinsky), 2-3 (dynamic "
                                      "localization), 4-7 (dynamic structure, mixed), 10 (one-equation mixed) or 20 "
@@ -2453,7 +2472,8 @@ template <typename T> static int class_step(hit3d_batch *b, BatchClass &k, int e
     auto Wf = [&](int i) { return W + i * wfs; };
     double *fen = k.tab + 2 * nr;
     if (p.flow_type == 1) {
-        k_forcing_energy<<<nr, 32, 0, c->st>>>(c->n, c->P64, c->fs64, p.kfmax, c->U, fen, k.ru);
+        const ForcingLaunch fl = forcing_launch(c->n, p.kfmax);
+        k_forcing_energy<<<nr, fl.threads, fl.smem, c->st>>>(c->n, c->P64, c->fs64, fl.kfmax, c->U, fen, k.ru);
         H3D_LAUNCH_CHECK();
     }
     H3D_TRY(zinv<T>(c, 3, PRE_COPY, 0, c->U, c->fs64, Wf(0), wfs, wp));

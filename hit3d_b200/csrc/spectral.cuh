@@ -400,44 +400,85 @@ __global__ void k_scalar(const StepArgs a, int mode, int s, double dx, const cx<
     }
 }
 
-// Energy in the forcing band, summed by one thread in the reference's loop
-// order (m_force.f90:266-284) so that the result is reproducible to the bit.
-// Batches launch one CTA per run (run r's state ru elements after run r-1's,
-// its energy in out[r]); one run launches one CTA with ru = 0.
+// Energy in the forcing band (m_force.f90:101-182, summed in the loop order of
+// m_force.f90:266-284): E_f = sum over the shells
+// 1..kfmax of the shell's (|u|^2 + |v|^2 + |w|^2)/N^6, half weight at kx = 0,
+// each mode's real entry and then its imaginary entry added on their own.
+// Bands of up to kFsmall shells: thread 0 sums every shell in one pass over
+// the candidate modes |k_i| <= kfmax + 1, in the reference's loop order (ky,
+// kz, kx).  Wider bands: thread s of the CTA sums shell s + 1 (and s + 1 +
+// blockDim.x, ...) over the same candidates in the same order, and thread 0
+// adds the shells (es, kfmax doubles of dynamic shared memory).  Every shell
+// sum and the final sum over the shells in order are rounded alike in both
+// forms.  One CTA per run of a batch (U advanced by ru per CTA).
+constexpr int kFsmall = 16;
 __global__ void k_forcing_energy(int n, int pitch, int64_t fs, int kfmax, const double2 *__restrict__ U,
                                  double *out, int64_t ru = 0)
 {
-    if (threadIdx.x != 0) return;
+    extern __shared__ double es[];
     U += blockIdx.x * ru;
     out += blockIdx.x;
-    double es[16];
-    for (int s = 0; s < 16; s++) es[s] = 0.0;
     const double n3 = (double)n * n * n;
     const double fac = 1.0 / (n3 * n3);
     const int km = kfmax + 1;
-    // storage indices in increasing order whose |wavenumber| <= km: 0..km, n-km..n-1
-    for (int kq = 0; kq < n; kq++) {
-        if (kq > km && kq < n - km) { kq = n - km - 1; continue; }
-        const int ky = kwave(kq, n);
-        for (int jq = 0; jq < n; jq++) {
-            if (jq > km && jq < n - km) { jq = n - km - 1; continue; }
-            const int kz = kwave(jq, n);
-            for (int kx = 0; kx <= km && kx < n / 2; kx++) {
-                double k2 = (double)kx * kx + (double)ky * ky + (double)kz * kz;
-                int sh = shell32(k2);
-                if (sh <= 0 || sh > kfmax) continue;
-                const int64_t o = ((int64_t)jq * n + kq) * pitch + kx;
-                double2 u = U[o], v = U[fs + o], w = U[2 * fs + o];
-                // real entry then imaginary entry, each added on its own
-                double f2 = __dmul_rn(fac, __dadd_rn(__dadd_rn(__dmul_rn(u.x, u.x), __dmul_rn(v.x, v.x)), __dmul_rn(w.x, w.x)));
-                if (kx == 0) f2 = __dmul_rn(f2, 0.5);
-                es[sh - 1] = __dadd_rn(es[sh - 1], f2);
-                f2 = __dmul_rn(fac, __dadd_rn(__dadd_rn(__dmul_rn(u.y, u.y), __dmul_rn(v.y, v.y)), __dmul_rn(w.y, w.y)));
-                if (kx == 0) f2 = __dmul_rn(f2, 0.5);
-                es[sh - 1] = __dadd_rn(es[sh - 1], f2);
+    if (kfmax <= kFsmall) {
+        if (threadIdx.x != 0) return;
+        double e16[kFsmall];
+        for (int s = 0; s < kFsmall; s++) e16[s] = 0.0;
+        for (int kq = 0; kq < n; kq++) {
+            if (kq > km && kq < n - km) { kq = n - km - 1; continue; }
+            const int ky = kwave(kq, n);
+            for (int jq = 0; jq < n; jq++) {
+                if (jq > km && jq < n - km) { jq = n - km - 1; continue; }
+                const int kz = kwave(jq, n);
+                for (int kx = 0; kx <= km && kx < n / 2; kx++) {
+                    double k2 = (double)kx * kx + (double)ky * ky + (double)kz * kz;
+                    int sh = shell32(k2);
+                    if (sh <= 0 || sh > kfmax) continue;
+                    const int64_t o = ((int64_t)jq * n + kq) * pitch + kx;
+                    double2 u = U[o], v = U[fs + o], w = U[2 * fs + o];
+                    double f2 = __dmul_rn(fac, __dadd_rn(__dadd_rn(__dmul_rn(u.x, u.x), __dmul_rn(v.x, v.x)), __dmul_rn(w.x, w.x)));
+                    if (kx == 0) f2 = __dmul_rn(f2, 0.5);
+                    e16[sh - 1] = __dadd_rn(e16[sh - 1], f2);
+                    f2 = __dmul_rn(fac, __dadd_rn(__dadd_rn(__dmul_rn(u.y, u.y), __dmul_rn(v.y, v.y)), __dmul_rn(w.y, w.y)));
+                    if (kx == 0) f2 = __dmul_rn(f2, 0.5);
+                    e16[sh - 1] = __dadd_rn(e16[sh - 1], f2);
+                }
             }
         }
+        double e = 0.0;
+        for (int s = 0; s < kfmax; s++) e = __dadd_rn(e, e16[s]);
+        *out = e;
+        return;
     }
+    for (int sh0 = threadIdx.x + 1; sh0 <= kfmax; sh0 += blockDim.x) {
+        double e = 0.0;
+        // storage indices in increasing order whose |wavenumber| <= km: 0..km, n-km..n-1
+        for (int kq = 0; kq < n; kq++) {
+            if (kq > km && kq < n - km) { kq = n - km - 1; continue; }
+            const int ky = kwave(kq, n);
+            for (int jq = 0; jq < n; jq++) {
+                if (jq > km && jq < n - km) { jq = n - km - 1; continue; }
+                const int kz = kwave(jq, n);
+                for (int kx = 0; kx <= km && kx < n / 2; kx++) {
+                    double k2 = (double)kx * kx + (double)ky * ky + (double)kz * kz;
+                    if (shell32(k2) != sh0) continue;
+                    const int64_t o = ((int64_t)jq * n + kq) * pitch + kx;
+                    double2 u = U[o], v = U[fs + o], w = U[2 * fs + o];
+                    // real entry then imaginary entry, each added on its own
+                    double f2 = __dmul_rn(fac, __dadd_rn(__dadd_rn(__dmul_rn(u.x, u.x), __dmul_rn(v.x, v.x)), __dmul_rn(w.x, w.x)));
+                    if (kx == 0) f2 = __dmul_rn(f2, 0.5);
+                    e = __dadd_rn(e, f2);
+                    f2 = __dmul_rn(fac, __dadd_rn(__dadd_rn(__dmul_rn(u.y, u.y), __dmul_rn(v.y, v.y)), __dmul_rn(w.y, w.y)));
+                    if (kx == 0) f2 = __dmul_rn(f2, 0.5);
+                    e = __dadd_rn(e, f2);
+                }
+            }
+        }
+        es[sh0 - 1] = e;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
     double e = 0.0;
     for (int s = 0; s < kfmax; s++) e = __dadd_rn(e, es[s]);
     *out = e;

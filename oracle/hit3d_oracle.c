@@ -1554,7 +1554,8 @@ static double forcing_energy(oracle_t *o)
 {
     int n = o->n;
     double fac = 1.0 / (((double)n * n * n) * ((double)n * n * n));
-    double es[64] = {0};
+    /* one sum per shell 1..kfmax (any kfmax the input gives, m_parameters.f90:308) */
+    double *es = (double *)calloc((size_t)(o->kfmax > 0 ? o->kfmax : 1), sizeof(double));
     double *u = F(o, 0), *v = F(o, 1), *w = F(o, 2);
     for (int k = 0; k < n; k++)
         for (int j = 0; j < n; j++)
@@ -1570,6 +1571,7 @@ static double forcing_energy(oracle_t *o)
             }
     double e = 0.0;
     for (int s = 0; s < o->kfmax; s++) e = e + es[s];
+    free(es);
     return e;
 }
 

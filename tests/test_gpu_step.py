@@ -52,6 +52,17 @@ def test_forced_two_thirds():
     _compare(o, g, 3)
 
 
+@pytest.mark.parametrize("kfmax", [20, 40])
+def test_forced_wide_band(kfmax):
+    """Forcing bands of many shells (the reference reads any KFMAX,
+    m_parameters.f90:308): 40 lies beyond the largest shell of a 32^3 grid."""
+    o, g = make_pair(32, dealias=0, flow_type=1, kfmax=kfmax, famp=0.5, nu=1.0 / 100.0, dt=0.002)
+    assert o.nforced() > 0
+    o.step(4)
+    g.step(4)
+    _compare(o, g, 3)
+
+
 def test_forcing_band_energy():
     """Energy in the forcing band (m_force.f90:258-284) agrees with the oracle."""
     o, g = make_pair(32, dealias=0, flow_type=1, kfmax=2)

@@ -244,10 +244,12 @@ def test_pressure_projection_is_divergence_free():
     assert np.abs(o.fields[:3] - before).max() <= 1e-13 * np.abs(before).max()
 
 
-def test_band_forcing_matches_numpy_restatement():
+@pytest.mark.parametrize("kfmax", [2, 20])
+def test_band_forcing_matches_numpy_restatement(kfmax):
     """force_velocity (m_force.f90:101-182): every real entry of shells 1..kfmax
-    gains FAMP / E_band times itself, E_band binned as in the reference."""
-    n, famp, kfmax = 32, 0.5, 2
+    gains FAMP / E_band times itself, E_band binned as in the reference (any
+    band the input file gives, m_parameters.f90:308)."""
+    n, famp = 32, 0.5
     o0 = oracle.Oracle(n, flow_type=0, kfmax=kfmax, famp=famp)
     o1 = oracle.Oracle(n, flow_type=1, kfmax=kfmax, famp=famp)
     o0.init_velocity(RN1, isp_type=1, peak_wavenum=3.0)
