@@ -196,8 +196,10 @@ int hit3d_gpu_pruned(hit3d_ctx *ctx);
 
 /* Without LES and with the 2/3 rule, the z forward pass of the six velocity
  * products runs inside the update kernel, so that the product spectra never
- * reach HBM (the same arithmetic per mode either way; off by default, as the
- * separate z pass + update measured faster). */
+ * reach HBM, and within one hit3d_gpu_step call that kernel also writes the
+ * next step's z inverse of the new velocity (the fields agree with the
+ * separate passes to rounding; off by default, as the separate z passes +
+ * update measured faster).  No counterpart in the reference. */
 int hit3d_gpu_set_update_fusion(hit3d_ctx *ctx, int32_t on);
 
 /* Failure detection (no reference counterpart: a diverged run of the
