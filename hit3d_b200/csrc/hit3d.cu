@@ -413,7 +413,7 @@ static ForcingLaunch forcing_launch(int n, int kfmax)
     const int shmax = (int)std::lround(std::sqrt(3.0) * (n / 2)) + 1;
     ForcingLaunch f;
     f.kfmax = kfmax < shmax ? kfmax : shmax;
-    f.threads = f.kfmax <= kFsmall ? 32 : (f.kfmax + 31) / 32 * 32;
+    f.threads = f.kfmax <= kFsmall ? kFthreads : (f.kfmax + 31) / 32 * 32;
     if (f.threads > 1024) f.threads = 1024;
     f.smem = f.kfmax <= kFsmall ? 0 : sizeof(double) * (size_t)f.kfmax;
     return f;

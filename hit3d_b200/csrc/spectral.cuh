@@ -404,14 +404,17 @@ __global__ void k_scalar(const StepArgs a, int mode, int s, double dx, const cx<
 // m_force.f90:266-284): E_f = sum over the shells
 // 1..kfmax of the shell's (|u|^2 + |v|^2 + |w|^2)/N^6, half weight at kx = 0,
 // each mode's real entry and then its imaginary entry added on their own.
-// Bands of up to kFsmall shells: thread 0 sums every shell in one pass over
-// the candidate modes |k_i| <= kfmax + 1, in the reference's loop order (ky,
-// kz, kx).  Wider bands: thread s of the CTA sums shell s + 1 (and s + 1 +
-// blockDim.x, ...) over the same candidates in the same order, and thread 0
-// adds the shells (es, kfmax doubles of dynamic shared memory).  Every shell
-// sum and the final sum over the shells in order are rounded alike in both
-// forms.  One CTA per run of a batch (U advanced by ru per CTA).
-constexpr int kFsmall = 16;
+// Bands of up to kFsmall shells: the candidate modes |k_i| <= kfmax + 1 in the
+// reference's loop order (ky, kz, kx) go in chunks of kFchunk, every thread
+// computing the contributions of its candidates (its own loads, all in flight
+// at once), and thread 0 adds them, in that order, to the shell sums.  Wider
+// bands: thread s of the CTA sums shell s + 1 (and s + 1 + blockDim.x, ...)
+// over the same candidates in the same order, and thread 0 adds the shells
+// (es, kfmax doubles of dynamic shared memory).  Every shell sum and the final
+// sum over the shells in order are rounded alike in both forms, and as one
+// thread visiting every candidate in order would round them.  One CTA per run
+// of a batch (U advanced by ru per CTA).
+constexpr int kFsmall = 16, kFchunk = 1024, kFthreads = 256;
 __global__ void k_forcing_energy(int n, int pitch, int64_t fs, int kfmax, const double2 *__restrict__ U,
                                  double *out, int64_t ru = 0)
 {
@@ -422,33 +425,60 @@ __global__ void k_forcing_energy(int n, int pitch, int64_t fs, int kfmax, const 
     const double fac = 1.0 / (n3 * n3);
     const int km = kfmax + 1;
     if (kfmax <= kFsmall) {
-        if (threadIdx.x != 0) return;
+        __shared__ double fr[kFchunk], fi[kFchunk];
+        __shared__ unsigned char fsh[kFchunk];
+        // candidate lists: ky and kz storage indices 0..km, n-km..n-1 (all n when
+        // they overlap), kx 0..min(km, n/2 - 1)
+        const int nk = 2 * km + 1 < n ? 2 * km + 1 : n;
+        const int nxc = (km < n / 2 - 1 ? km : n / 2 - 1) + 1;
+        const int64_t nc = (int64_t)nk * nk * nxc;
         double e16[kFsmall];
         for (int s = 0; s < kFsmall; s++) e16[s] = 0.0;
-        for (int kq = 0; kq < n; kq++) {
-            if (kq > km && kq < n - km) { kq = n - km - 1; continue; }
-            const int ky = kwave(kq, n);
-            for (int jq = 0; jq < n; jq++) {
-                if (jq > km && jq < n - km) { jq = n - km - 1; continue; }
-                const int kz = kwave(jq, n);
-                for (int kx = 0; kx <= km && kx < n / 2; kx++) {
-                    double k2 = (double)kx * kx + (double)ky * ky + (double)kz * kz;
-                    int sh = shell32(k2);
-                    if (sh <= 0 || sh > kfmax) continue;
-                    const int64_t o = ((int64_t)jq * n + kq) * pitch + kx;
-                    double2 u = U[o], v = U[fs + o], w = U[2 * fs + o];
-                    double f2 = __dmul_rn(fac, __dadd_rn(__dadd_rn(__dmul_rn(u.x, u.x), __dmul_rn(v.x, v.x)), __dmul_rn(w.x, w.x)));
-                    if (kx == 0) f2 = __dmul_rn(f2, 0.5);
-                    e16[sh - 1] = __dadd_rn(e16[sh - 1], f2);
-                    f2 = __dmul_rn(fac, __dadd_rn(__dadd_rn(__dmul_rn(u.y, u.y), __dmul_rn(v.y, v.y)), __dmul_rn(w.y, w.y)));
-                    if (kx == 0) f2 = __dmul_rn(f2, 0.5);
-                    e16[sh - 1] = __dadd_rn(e16[sh - 1], f2);
+        for (int64_t base = 0; base < nc; base += kFchunk) {
+            for (int q = threadIdx.x; q < kFchunk; q += blockDim.x) {
+                const int64_t t = base + q;
+                unsigned char sh8 = 0;
+                if (t < nc) {
+                    const int kx = (int)(t % nxc);
+                    const int64_t r = t / nxc;
+                    const int b = (int)(r % nk), a = (int)(r / nk);
+                    const int kq = (nk == n || a <= km) ? a : n - (nk - a);
+                    const int jq = (nk == n || b <= km) ? b : n - (nk - b);
+                    const int ky = kwave(kq, n), kz = kwave(jq, n);
+                    const double k2 = (double)kx * kx + (double)ky * ky + (double)kz * kz;
+                    const int sh = shell32(k2);
+                    if (sh > 0 && sh <= kfmax) {
+                        const int64_t o = ((int64_t)jq * n + kq) * pitch + kx;
+                        const double2 u = U[o], v = U[fs + o], w = U[2 * fs + o];
+                        // real entry then imaginary entry, each added on its own
+                        double f2 = __dmul_rn(fac, __dadd_rn(__dadd_rn(__dmul_rn(u.x, u.x), __dmul_rn(v.x, v.x)), __dmul_rn(w.x, w.x)));
+                        if (kx == 0) f2 = __dmul_rn(f2, 0.5);
+                        fr[q] = f2;
+                        f2 = __dmul_rn(fac, __dadd_rn(__dadd_rn(__dmul_rn(u.y, u.y), __dmul_rn(v.y, v.y)), __dmul_rn(w.y, w.y)));
+                        if (kx == 0) f2 = __dmul_rn(f2, 0.5);
+                        fi[q] = f2;
+                        sh8 = (unsigned char)sh;
+                    }
+                }
+                fsh[q] = sh8;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                const int m = nc - base < kFchunk ? (int)(nc - base) : kFchunk;
+                for (int q = 0; q < m; q++) {
+                    const int sh = fsh[q];
+                    if (sh == 0) continue;
+                    e16[sh - 1] = __dadd_rn(e16[sh - 1], fr[q]);
+                    e16[sh - 1] = __dadd_rn(e16[sh - 1], fi[q]);
                 }
             }
+            __syncthreads();
         }
-        double e = 0.0;
-        for (int s = 0; s < kfmax; s++) e = __dadd_rn(e, e16[s]);
-        *out = e;
+        if (threadIdx.x == 0) {
+            double e = 0.0;
+            for (int s = 0; s < kfmax; s++) e = __dadd_rn(e, e16[s]);
+            *out = e;
+        }
         return;
     }
     for (int sh0 = threadIdx.x + 1; sh0 <= kfmax; sh0 += blockDim.x) {
