@@ -139,6 +139,49 @@ H3D_D void store_input_row(unsigned char *sA, int r, const float *x)
     *a_chunk(sA, r, 1) = make_uint4(0u, 0u, 0u, 0u);
 }
 
+// two fp32 lanes in one 64-bit register, and the packed two-lane operations of
+// sm_100 (each lane rounded as the scalar operation rounds it)
+H3D_D uint64_t f2_pack(float lo, float hi)
+{
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+H3D_D void f2_unpack(uint64_t r, float &lo, float &hi) { asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(r)); }
+H3D_D uint64_t f2_add(uint64_t a, uint64_t b)
+{
+    uint64_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+H3D_D uint64_t f2_mul(uint64_t a, uint64_t b)
+{
+    uint64_t r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+H3D_D uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c)
+{
+    uint64_t r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+// gelu_fast of two values, the same operations in the same order on each lane
+// (so the same results), the multiply-adds two lanes per instruction
+H3D_D void gelu_fast2(float z0, float z1, float &g0, float &g1)
+{
+    const uint64_t z = f2_pack(z0, z1);
+    const uint64_t zz = f2_mul(z, z);
+    const uint64_t p = f2_fma(f2_pack(GELU_B, GELU_B), zz, f2_pack(1.0f, 1.0f));
+    const uint64_t u = f2_mul(f2_mul(f2_pack(GELU_A, GELU_A), z), p);
+    float u0, u1, t0, t1;
+    f2_unpack(u, u0, u1);
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t0) : "f"(u0));
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t1) : "f"(u1));
+    const uint64_t h = f2_mul(f2_pack(0.5f, 0.5f), z);
+    f2_unpack(f2_fma(h, f2_pack(t0, t1), h), g0, g1);
+}
+
 // bf16 of gelu(acc[j] + b[j]) (b may be null) into this thread's row of the A tile
 H3D_D void store_act_row(unsigned char *sA, int r, const float *acc, const float *b)
 {
@@ -148,8 +191,11 @@ H3D_D void store_act_row(unsigned char *sA, int r, const float *acc, const float
 #pragma unroll
         for (int e = 0; e < 4; e++) {
             const int j = 8 * c + 2 * e;
-            const float lo = gelu_fast(b ? acc[j] + b[j] : acc[j]);
-            const float hi = gelu_fast(b ? acc[j + 1] + b[j + 1] : acc[j + 1]);
+            uint64_t z = f2_pack(acc[j], acc[j + 1]);
+            if (b) z = f2_add(z, f2_pack(b[j], b[j + 1]));
+            float z0, z1, lo, hi;
+            f2_unpack(z, z0, z1);
+            gelu_fast2(z0, z1, lo, hi);
             w[e] = pack_bf16(lo, hi);
         }
         *a_chunk(sA, r, c) = make_uint4(w[0], w[1], w[2], w[3]);
