@@ -296,9 +296,12 @@ def les_leg(torch, args, dns_rate, dns32_rate, device):
     w[nparam - 5] = -2.0 * 0.18 ** 2 * dx * dx / (delta * delta)
     bits = ((w.view(np.uint32).astype(np.uint64) + 0x7FFF + ((w.view(np.uint32) >> 16) & 1)) >> 16).astype(np.uint16)
     rates = {}
-    for name, model, kernel in (("learned", 20, 1), ("learned_cuda_cores", 20, 0), ("smagorinsky", 1, 0)):
+    # FP64 transforms, and the FP32-transform form (FP64 state and integrator)
+    # with the learned closure and with Smagorinsky
+    for name, model, kernel, prec in (("learned", 20, 1, 0), ("learned_cuda_cores", 20, 0, 0), ("smagorinsky", 1, 0, 0),
+                                      ("learned_fp32_transforms", 20, 1, 1), ("smagorinsky_fp32_transforms", 1, 0, 1)):
         c = Context(Params(nx=n_les, dealias=0, flow_type=1, force_type=1, kfmax=2, famp=0.5, nu=1.0 / RE, dt=dt_les,
-                           les_model=model, device=device))
+                           les_model=model, precision=prec, device=device))
         if model == 20:
             c.les_set_mlp(bits, delta, clip=True, kernel=kernel)
         c.init_velocity(RN1, 2, 4.0, 2.0)
@@ -507,6 +510,7 @@ def summarize(line):
     if le:
         s["learned_les"] = {"steps_per_s": le.get("steps_per_s"),
                             "closure_ms": (le.get("learned_stage_ms") or {}).get("closure"),
+                            "closure_ms_fp32_transforms": (le.get("learned_fp32_transforms_stage_ms") or {}).get("closure"),
                             "speedup_vs_dns_fp64": le.get("speedup_vs_dns_fp64")}
         ap = le.get("aposteriori") or {}
         if "mean_abs_log_spectrum_error" in ap:
