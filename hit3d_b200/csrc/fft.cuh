@@ -72,11 +72,45 @@ template <typename T, bool FWD> H3D_D cx<T> submi(cx<T> d, cx<T> t)
     return FWD ? mk<T>(d.x - t.y, d.y + t.x) : mk<T>(d.x + t.y, d.y - t.x);
 }
 
-template <typename T, bool FWD> H3D_D void dft4(cx<T> &a0, cx<T> &a1, cx<T> &a2, cx<T> &a3)
+// a + b and a - b; PK (FP32 only): one packed two-lane instruction
+// (add/sub.rn.f32x2, each lane rounded as the scalar operation), which the
+// strided passes of the FP32 form use
+template <typename T, bool PK> H3D_D cx<T> cadd(cx<T> a, cx<T> b)
 {
-    cx<T> s0 = a0 + a2, d0 = a0 - a2, s1 = a1 + a3, t = a1 - a3;
-    a0 = s0 + s1;
-    a2 = s0 - s1;
+    if constexpr (PK) {
+        static_assert(sizeof(T) == 4, "packed sums are FP32");
+        unsigned long long pa, pb, r;
+        asm("mov.b64 %0, {%1, %2};" : "=l"(pa) : "f"(a.x), "f"(a.y));
+        asm("mov.b64 %0, {%1, %2};" : "=l"(pb) : "f"(b.x), "f"(b.y));
+        asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pa), "l"(pb));
+        cx<T> o;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(o.x), "=f"(o.y) : "l"(r));
+        return o;
+    } else {
+        return a + b;
+    }
+}
+template <typename T, bool PK> H3D_D cx<T> csub(cx<T> a, cx<T> b)
+{
+    if constexpr (PK) {
+        static_assert(sizeof(T) == 4, "packed sums are FP32");
+        unsigned long long pa, pb, r;
+        asm("mov.b64 %0, {%1, %2};" : "=l"(pa) : "f"(a.x), "f"(a.y));
+        asm("mov.b64 %0, {%1, %2};" : "=l"(pb) : "f"(b.x), "f"(b.y));
+        asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pa), "l"(pb));
+        cx<T> o;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(o.x), "=f"(o.y) : "l"(r));
+        return o;
+    } else {
+        return a - b;
+    }
+}
+
+template <typename T, bool FWD, bool PK = false> H3D_D void dft4(cx<T> &a0, cx<T> &a1, cx<T> &a2, cx<T> &a3)
+{
+    cx<T> s0 = cadd<T, PK>(a0, a2), d0 = csub<T, PK>(a0, a2), s1 = cadd<T, PK>(a1, a3), t = csub<T, PK>(a1, a3);
+    a0 = cadd<T, PK>(s0, s1);
+    a2 = csub<T, PK>(s0, s1);
     a1 = addmi<T, FWD>(d0, t);
     a3 = submi<T, FWD>(d0, t);
 }
@@ -95,32 +129,32 @@ template <typename T, bool FWD> H3D_D void dft3(cx<T> &a0, cx<T> &a1, cx<T> &a2)
     a2 = m - r;
 }
 
-template <typename T, bool FWD> H3D_D void dft8(cx<T> (&a)[8])
+template <typename T, bool FWD, bool PK = false> H3D_D void dft8(cx<T> (&a)[8])
 {
     const T r2 = (T)0.70710678118654752440084436210484904;
     cx<T> e0 = a[0], e1 = a[2], e2 = a[4], e3 = a[6];
     cx<T> o0 = a[1], o1 = a[3], o2 = a[5], o3 = a[7];
-    dft4<T, FWD>(e0, e1, e2, e3);
-    dft4<T, FWD>(o0, o1, o2, o3);
+    dft4<T, FWD, PK>(e0, e1, e2, e3);
+    dft4<T, FWD, PK>(o0, o1, o2, o3);
     // twiddles w8^k, w8 = exp(-+ i pi/4)
     cx<T> t1 = FWD ? mk<T>(r2 * (o1.x + o1.y), r2 * (o1.y - o1.x)) : mk<T>(r2 * (o1.x - o1.y), r2 * (o1.y + o1.x));
     cx<T> t3 = FWD ? mk<T>(r2 * (-o3.x + o3.y), r2 * (-o3.y - o3.x)) : mk<T>(r2 * (-o3.x - o3.y), r2 * (-o3.y + o3.x));
-    a[0] = e0 + o0; a[4] = e0 - o0;
-    a[1] = e1 + t1; a[5] = e1 - t1;
+    a[0] = cadd<T, PK>(e0, o0); a[4] = csub<T, PK>(e0, o0);
+    a[1] = cadd<T, PK>(e1, t1); a[5] = csub<T, PK>(e1, t1);
     a[2] = addmi<T, FWD>(e2, o2); a[6] = submi<T, FWD>(e2, o2);  // e2 +- w8^2 o2
-    a[3] = e3 + t3; a[7] = e3 - t3;
+    a[3] = cadd<T, PK>(e3, t3); a[7] = csub<T, PK>(e3, t3);
 }
 
-template <typename T, int R, bool FWD> H3D_D void dft(cx<T> *a)
+template <typename T, int R, bool FWD, bool PK = false> H3D_D void dft(cx<T> *a)
 {
     if constexpr (R == 2) dft2<T, FWD>(a[0], a[1]);
     else if constexpr (R == 3) dft3<T, FWD>(a[0], a[1], a[2]);
-    else if constexpr (R == 4) dft4<T, FWD>(a[0], a[1], a[2], a[3]);
+    else if constexpr (R == 4) dft4<T, FWD, PK>(a[0], a[1], a[2], a[3]);
     else if constexpr (R == 8) {
         cx<T> t[8];
 #pragma unroll
         for (int m = 0; m < 8; m++) t[m] = a[m];
-        dft8<T, FWD>(t);
+        dft8<T, FWD, PK>(t);
 #pragma unroll
         for (int m = 0; m < 8; m++) a[m] = t[m];
     }
@@ -175,6 +209,10 @@ template <typename T> struct GlobalTw {
         return twid<T, FWD>(tw, k * m * (L / (Ns * R)));
     }
 };
+// packed FP32 sums in the butterflies of the strided passes (COLS layout);
+// the row passes keep scalar sums (measured faster there)
+template <typename T, bool ROWS> constexpr bool kPackSums = !ROWS && sizeof(T) == 4;
+
 template <typename T, int L, int TC, int NT, bool ROWS, bool FWD, bool REV, int s, class TWS>
 H3D_D void fft_mid_stage(cx<T> *sm, const TWS &tws)
 {
@@ -197,7 +235,7 @@ H3D_D void fft_mid_stage(cx<T> *sm, const TWS &tws)
                 if (m > 0) v = cmul(v, tws.template get<L, Ns, R, FWD, s>(i, m, k));
                 a[i * R + m] = v;
             }
-            dft<T, R, FWD>(a + i * R);
+            dft<T, R, FWD, kPackSums<T, ROWS>>(a + i * R);
         }
     }
     __syncthreads();
@@ -296,7 +334,7 @@ struct ColFFT {
             if (TOT0 % NT == 0 || b < TOT0) {
                 int c, j;
                 LY::template bf<R0>(b, c, j);
-                dft<T, R0, FWD>(in + i * R0);
+                dft<T, R0, FWD, kPackSums<T, ROWS>>(in + i * R0);
 #pragma unroll
                 for (int m = 0; m < R0; m++) sm[LY::idx(c, j * R0 + m)] = in[i * R0 + m];
             }
@@ -328,7 +366,7 @@ struct ColFFT {
                     if (m > 0) x = cmul(x, tws.template get<L, NsL, RL, FWD, S - 1>(i, m, k));
                     v[m] = x;
                 }
-                dft<T, RL, FWD>(v);
+                dft<T, RL, FWD, kPackSums<T, ROWS>>(v);
 #pragma unroll
                 for (int m = 0; m < RL; m++) st(c, j + m * nbpc, v[m]);
             }
@@ -357,7 +395,7 @@ struct ColFFT {
                     if (m > 0) x = cmul(x, tws.template get<L, NsL, RL, FWD, S - 1>(i, m, k));
                     v[m] = x;
                 }
-                dft<T, RL, FWD>(v);
+                dft<T, RL, FWD, kPackSums<T, ROWS>>(v);
 #pragma unroll
                 for (int m = 0; m < RL; m++) st(i, m, c, j + m * nbpc, v[m]);
             }
@@ -389,7 +427,7 @@ struct ColFFT {
                 LY::template bf<R0>(b, c, j);
 #pragma unroll
                 for (int f = 0; f < NF; f++) {
-                    dft<T, R0, FWD>(in[f] + i * R0);
+                    dft<T, R0, FWD, kPackSums<T, ROWS>>(in[f] + i * R0);
 #pragma unroll
                     for (int m = 0; m < R0; m++) sm[f * E + LY::idx(c, j * R0 + m)] = in[f][i * R0 + m];
                 }
@@ -424,7 +462,7 @@ struct ColFFT {
                     }
                 }
 #pragma unroll
-                for (int f = 0; f < NF; f++) dft<T, RL, FWD>(out[f] + i * RL);
+                for (int f = 0; f < NF; f++) dft<T, RL, FWD, kPackSums<T, ROWS>>(out[f] + i * RL);
             }
         }
     }
@@ -452,7 +490,7 @@ struct ColFFT {
                     }
                 }
 #pragma unroll
-                for (int f = 0; f < NF; f++) dft<T, R, FWD>(a[f] + i * R);
+                for (int f = 0; f < NF; f++) dft<T, R, FWD, kPackSums<T, ROWS>>(a[f] + i * R);
             }
         }
         __syncthreads();
@@ -493,7 +531,7 @@ struct ColFFT {
                     if (m > 0) x = cmul(x, tws.template get<L, NsL, RL, FWD, S - 1>(i, m, k));
                     out[i * RL + m] = x;
                 }
-                dft<T, RL, FWD>(out + i * RL);
+                dft<T, RL, FWD, kPackSums<T, ROWS>>(out + i * RL);
             }
         }
     }
