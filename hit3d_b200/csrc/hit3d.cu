@@ -316,8 +316,8 @@ template <typename KF> static dim3 pw_grid(const hit3d_ctx *c, KF kernel)
 }
 
 // z forward pass of the six velocity products (after their y pass, in P) fused
-// with the 2/3-rule update of U and RO
-// with the update of U and RO; zinv: and the z inverse of the new u, v, w into P[0..2]
+// with the 2/3-rule update of U and RO and, with zinv, the z inverse of the new
+// u, v, w into P[0..2]
 template <typename T, int L, bool PRUNED> static int zfwd_update_LP(hit3d_ctx *c, const ZUpdArgs<T> &za)
 {
     using CF = ZUpdCfg<T, L>;
@@ -401,9 +401,10 @@ struct Prof {
         if (prof) prof->mark(c->st, (s)); \
     } while (0)
 
-// launch shape of k_forcing_energy: one thread per shell of the band.  Shells
+// launch shape of k_forcing_energy: kFthreads threads loading the candidate
+// modes of a band of up to kFsmall shells, else one thread per shell.  Shells
 // beyond the largest a grid has (nint(sqrt(3) N/2) + 1) hold no modes and add
-// nothing, so the band is cut there; one warp at least.
+// nothing, so the band is cut there.
 struct ForcingLaunch {
     int kfmax, threads;
     size_t smem;
