@@ -466,6 +466,18 @@ def _sig(x, d=4):
     return x
 
 
+def max_over_ranks(dist, t, device="cuda"):
+    """The job's time: the largest of every rank's t (seconds), by one
+    all_reduce(MAX) of the timing scalar (dist None: one process, t itself).
+    device: where the scalar lives for the backend (cuda for NCCL, cpu for gloo)."""
+    if not dist:
+        return t
+    import torch
+    tt = torch.tensor([float(t)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
 def ek_err_by_decade(e32, e64):
     """Largest relative E(k) error of the FP32 form per band of shells, banded by
     the shell's energy over the peak shell's: [1e-2, 1], [1e-4, 1e-2], ...,
@@ -564,10 +576,7 @@ def main():
     with ClockSampler(local) as clk:
         t = timed_steps(torch, ctx, args.steps)
     launches = ctx.launches - launches0
-    if dist:
-        tt = torch.tensor([t], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = float(tt.item())
+    t = max_over_ranks(dist, t)
     value = world * args.steps / t
     ms = 1000.0 * t / args.steps
     es64, st64 = ctx.stats()
@@ -611,14 +620,8 @@ def main():
         te_full = e2e_time(False)
         te = e2e_time(True)
         out = hov
-        if dist:
-            tt = torch.tensor([te], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
-        if dist:
-            tt = torch.tensor([te_full], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te_full = float(tt.item())
+        te = max_over_ranks(dist, te)
+        te_full = max_over_ranks(dist, te_full)
         nbytes = ctx.step_host_bytes(3, True)
         e2e = {"value": world * args.e2e_steps / te, "unit": "timesteps/s", "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps,
@@ -657,10 +660,7 @@ def main():
         if dist:
             dist.barrier()
         t32 = timed_steps(torch, c32, args.steps)
-        if dist:
-            tt = torch.tensor([t32], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t32 = float(tt.item())
+        t32 = max_over_ranks(dist, t32)
         es32, st32 = c32.stats()
         prof32 = c32.step_profile(3)
         mask = es64 > 1e-12 * es64.max()

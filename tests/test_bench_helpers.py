@@ -37,3 +37,40 @@ def test_stage_bytes_fp32_halves_the_work_fields():
     # the update reads and writes the FP64 state in both forms
     assert f32["update"] > 0.5 * f64["update"]
     assert abs(sum(f64.values()) - 27.9) < 0.1
+
+
+def _rank_max(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        # rank r "took" 1.5 + r seconds for 60 steps; the job takes the slowest rank's time
+        t = bench.max_over_ranks(dist, 1.5 + rank, device="cpu")
+        q.put((rank, t, world * 60 / t))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_with_two_gloo_ranks():
+    """The replicas' timing of bench.py --gpus N (one all_reduce(MAX) of the
+    timing scalar, value = N x steps / max time), with two gloo ranks on CPU."""
+    import socket
+
+    import torch.multiprocessing as mp
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_rank_max, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = sorted(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [o[1] for o in out] == [2.5, 2.5]
+    assert all(abs(o[2] - 2 * 60 / 2.5) < 1e-12 for o in out)
+    assert bench.max_over_ranks(None, 3.25) == 3.25
