@@ -504,6 +504,7 @@ def summarize(line):
                      "ek_max_rel_err_over_run": f.get("ek_max_rel_err_over_run"),
                      "ek_1e-4_crossed_at_step": f.get("ek_1e-4_crossed_at_step"),
                      "ek_max_rel_err_above_1e-6_over_run": f.get("ek_max_rel_err_above_1e-6_over_run"),
+                     "ek_max_rel_err_above_1e-10_over_run": f.get("ek_max_rel_err_above_1e-10_over_run"),
                      "per_step": [[c["step"], c["ek_max_rel_err"], c["eps_rel_err"], c["skew_abs_err"]]
                                   for c in f.get("vs_fp64_every_%d_steps" % 50, [])]}
     oc = line.get("other_configs") or {}
@@ -696,6 +697,10 @@ def main():
         # the first compared step at which the E(k) error passes 1e-4 (None: not within the run)
         fp32["ek_1e-4_crossed_at_step"] = next((c["step"] for c in cmp if c["ek_max_rel_err"] > 1e-4), None)
         fp32["ek_max_rel_err_above_1e-6_over_run"] = max(c["ek_max_rel_err_above_1e-6"] for c in cmp) if cmp else None
+        # every shell holding at least 1e-10 of the peak shell's energy
+        fp32["ek_max_rel_err_above_1e-10_over_run"] = max(
+            (v for c in cmp for k, v in c["ek_err_by_decade"].items() if k != "1e-12" and v is not None),
+            default=None)
         c32.close()
 
     les = None
