@@ -72,3 +72,17 @@ def test_reference_les_models_without_a_port_are_rejected():
     for m in (8, 9, 11):
         with pytest.raises(Hit3dError, match="les_model"):
             Context(Params(nx=32, les_model=m))
+
+
+def test_forcing_band_checks_before_device_use():
+    """A forced run needs KFMAX >= 1, and any wider band passes the parameter
+    checks (the reference reads any value, m_parameters.f90:308); without a
+    GPU such a context then fails only at device use."""
+    from hit3d_b200 import Hit3dError, Params, Context
+    with pytest.raises(Hit3dError, match="kfmax"):
+        Context(Params(nx=32, flow_type=1, force_type=1, kfmax=0))
+    import torch
+    if not torch.cuda.is_available():
+        with pytest.raises(Hit3dError) as e:
+            Context(Params(nx=32, flow_type=1, force_type=1, kfmax=100))
+        assert "kfmax" not in str(e.value)
